@@ -1,0 +1,362 @@
+"""Benchmark: points/sec of the 4M-point nonuniform Laplace FMM (eps 1e-6) on B200.
+
+Workload (the headline configuration): lfmm2d on N = 4,000,000 sources drawn
+from a mixture of 16 Gaussians (centres uniform in [0,1]^2, sigma log-uniform
+in [1e-4, 1e-1]), complex charges with N(0,1) real/imaginary parts, dipstr
+N(0,1) (real), unit dipvec at a uniform angle, eps = 1e-6, pg = 2 (potential
+and gradient at the sources); seeded synthetic data (numpy default_rng(1)).
+
+A step is one complete FMM call (tree, lists, all passes, caller-order
+results).  ``value`` times it with inputs resident in HBM (device-pointer C
+ABI b2fmm_lfmm2d_dev) in the mixed-precision mode; ``fp64_value`` is the
+plain FP64 GPU FMM on the same inputs; ``e2e`` calls the reference-named host
+entry point b2fmm_lfmm2d with pinned host buffers (H2D + FMM + D2H per step).
+Every run reports the relative l2 error of pot+grad against the FP64 direct
+sum over 1000 random sources.  ``--impl reference`` times the CPU oracle (the
+C++ restatement of the reference algorithm; the Fortran reference cannot be
+built here) on a bounded sample of the same workload with all host threads.
+
+Multi-GPU (torchrun): every rank evaluates its own independent problem of the
+same size (replicas, no collective in the data path); timings are the max over
+ranks (one all_reduce of the step times) and ``value`` counts all ranks' points.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "points/sec, 4M nonuniform Laplace eps 1e-6: mixed-prec vs FP64 plain, 1 B200"
+WORKLOAD = "lfmm2d 16-Gaussian mixture, complex charges + dipoles, eps=1e-6, pg=2"
+
+
+def make_inputs(n, seed=1):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0, 1, (2, 16))
+    sig = 10 ** rng.uniform(-4, -1, 16)
+    k = rng.integers(0, 16, n)
+    src = c[:, k] + sig[k] * rng.normal(size=(2, n))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    d = rng.normal(size=n) + 0j
+    ph = rng.uniform(0, 2 * np.pi, n)
+    v = np.stack([np.cos(ph), np.sin(ph)])
+    return src, q, d, v
+
+
+def fortran_layout(src, q, d, v):
+    """(2,n)/(n,)/(2,n) user arrays -> the C ABI's column-major layouts."""
+    return (np.ascontiguousarray(src.T), np.ascontiguousarray(q.reshape(-1, 1)),
+            np.ascontiguousarray(d.reshape(-1, 1)), np.ascontiguousarray(v.T.reshape(-1, 2, 1)))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during timing."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"b2fmm_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_baseline(n_sample, reps=1):
+    """Oracle (C++ restatement of the reference algorithm) on a bounded sample."""
+    from oracle import oracle as O
+    O.build()
+    O.set_num_threads(os.cpu_count() or 1)
+    src, q, d, v = make_inputs(n_sample, seed=1)
+    O.lfmm2d(1e-6, src[:, :20000], charges=q[:20000], dipstr=d[:20000], dipvec=v[:, :20000],
+             ifpgh=2)  # warm-up
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
+        ts.append(time.perf_counter() - t0)
+    t = min(ts)
+    return {"value": n_sample / t, "unit": "points/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"{n_sample} points of the same 16-Gaussian mixture (seed 1), one lfmm2d "
+                      f"call, eps=1e-6, pg=2; {t:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    n_sample = args.ref_sample
+    from oracle import oracle as O
+    O.build()
+    O.set_num_threads(os.cpu_count() or 1)
+    src, q, d, v = make_inputs(n_sample, seed=1)
+    for _ in range(args.warmup):
+        O.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
+        ts.append(time.perf_counter() - t0)
+    t = sum(ts) / len(ts)
+    val = n_sample / t
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "points/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD + f"; bounded sample n={n_sample}",
+                                            "n_points": n_sample, "eps": 1e-6},
+            "cpu_baseline": {"value": val, "unit": "points/s", "cores": O.num_threads(),
+                             "kind": "port",
+                             "sample": f"{n_sample} points of the same mixture per step"},
+            "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4_000_000)
+    ap.add_argument("--ref-sample", type=int, default=500_000)
+    ap.add_argument("--cpu-sample", type=int, default=1_000_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    args = ap.parse_args()
+    rank, world, local = dist_info()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    from fmm2d_b200 import _lib
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    L = _lib.lib()
+    n = args.n
+    src, q, d, v = make_inputs(n, seed=1 + rank)
+    hs, hq, hd, hv = fortran_layout(src, q, d, v)
+    ds, dq, dd, dv = (torch.as_tensor(x, device=dev) for x in (hs, hq, hd, hv))
+    pot = torch.empty((n, 1), dtype=torch.complex128, device=dev)
+    grad = torch.empty((n, 2, 1), dtype=torch.complex128, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+
+    def step(precision, timeinfo=None):
+        o = _lib.Options()
+        o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, _lib.PREC[precision]
+        ier = C.c_int(0)
+        ti = timeinfo if timeinfo is not None else np.zeros(8)
+        L.b2fmm_lfmm2d_dev(1, C.c_double(1e-6), C.c_int64(n), ptr(ds), 1, ptr(dq), 1, ptr(dd),
+                           ptr(dv), 2, ptr(pot), ptr(grad), None, C.c_int64(0), None, 0, None,
+                           None, None, C.byref(o), ti.ctypes.data_as(C.c_void_p),
+                           C.c_void_p(stream.cuda_stream), C.byref(ier))
+        if ier.value != 0:
+            raise RuntimeError(f"b2fmm_lfmm2d_dev ier={ier.value}")
+
+    def timed(precision, steps, warmup, with_clocks=False):
+        for _ in range(warmup):
+            step(precision)
+        tis = np.zeros(8)
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        sampler = ClockSampler(local) if with_clocks else None
+        if sampler:
+            sampler.start()
+        L0 = L.b2fmm_kernel_launches()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            ti = np.zeros(8)
+            step(precision, ti)
+            tis += ti
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = L.b2fmm_kernel_launches() - L0
+        clocks = sampler.stop() if sampler else None
+        ms = e0.elapsed_time(e1) / steps
+        if pg:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, tis / steps, launches, clocks
+
+    prec = args.precision
+    ms, ti, launches, clocks = timed(prec, args.steps, args.warmup, with_clocks=True)
+    ms64, ti64, _, _ = timed("fp64", max(2, args.steps // 2), 1) if prec != "fp64" else (ms, ti, 0, None)
+    value = world * n / (ms * 1e-3)
+    value64 = world * n / (ms64 * 1e-3)
+
+    # work counts and roofline of the dominant kernel (from this run)
+    L.b2fmm_set_stats(1)
+    step(prec)
+    L.b2fmm_set_stats(0)
+    st = _lib.get_stats()
+    phases = {"p2m": ti[0], "p2l": ti[1], "m2m": ti[2], "m2l": ti[3], "l2l": ti[4],
+              "leaf_eval(l2p+m2p+p2p)": ti[7]}
+    phases_ms = {k: round(v * 1e3, 4) for k, v in phases.items()}
+    dom = max(phases, key=phases.get)
+    fma_peak = L.b2fmm_fma_peak(1 if prec == "fp64" else 0)
+    nd2 = st["nd_cauchy"]
+    P = st["nterms1"]
+    # algorithmic flops (FMA = 2): P2P charge+dipole pot+grad per pair 15 + 28*nd2
+    # (SURVEY 8d accounting); M2L per translation 2*P*P real MACs x 2 (re,im) x nd2
+    flops = {"leaf_eval(l2p+m2p+p2p)": st["p2p_pairs"] * (15 + 28 * nd2)
+             + st["npts_eval"] * 16 * P * nd2 + st["m2p_evals"] * 16 * P * nd2,
+             "m2l": st["m2l_pairs"] * 4 * P * P * nd2}
+    t_dom = phases[dom]
+    achieved = flops.get(dom, 0.0) / t_dom / 1e12 if t_dom > 0 else 0.0
+    roofline = {"bound": "fma", "kernel": dom, "achieved": achieved,
+                "peak": fma_peak / 1e12, "unit": "TFLOP/s", "frac": achieved / (fma_peak / 1e12),
+                "traffic": None,
+                "peak_source": ("in-run FMA microbenchmark b2fmm_fma_peak "
+                                f"({'FP64' if prec == 'fp64' else 'FP32'}); MEASURED_PEAKS.json "
+                                "holds only HBM copy and bf16 tensor peaks"),
+                "phase_ms": phases_ms, "tree_ms": round(st["tree_ms"], 4),
+                "counts": {k: st[k] for k in ("nboxes", "nlevels", "nleaves", "nterms1",
+                                              "p2p_pairs", "m2l_pairs", "m2p_evals")}}
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        try:
+            roofline["traffic"] = json.load(open(prof)).get(dom)
+        except ValueError:
+            pass
+
+    # accuracy against the FP64 direct sum on 1000 random sources
+    rng = np.random.default_rng(99)
+    idx = np.sort(rng.choice(n, 1000, replace=False))
+    step(prec)
+    pot_h = pot[:, 0].cpu().numpy()
+    grad_h = grad[:, :, 0].cpu().numpy()
+    tsel = torch.as_tensor(np.ascontiguousarray(src[:, idx].T), device=dev)
+    ep = torch.empty((1000, 1), dtype=torch.complex128, device=dev)
+    eg = torch.empty((1000, 2, 1), dtype=torch.complex128, device=dev)
+    ier = C.c_int(0)
+    L.b2fmm_lap_direct_dev(1, 1, C.c_int64(n), ptr(ds), ptr(dq), ptr(dd), ptr(dv),
+                           C.c_int64(1000), ptr(tsel), 2, ptr(ep), ptr(eg), None,
+                           C.c_double(1e-16), C.c_void_p(stream.cuda_stream), C.byref(ier))
+    ex_p = ep[:, 0].cpu().numpy()
+    ex_g = eg[:, :, 0].cpu().numpy()
+    num = np.linalg.norm(pot_h[idx] - ex_p) ** 2 + np.linalg.norm(grad_h[idx] - ex_g) ** 2
+    den = np.linalg.norm(ex_p) ** 2 + np.linalg.norm(ex_g) ** 2
+    err = float(np.sqrt(num / den))
+
+    # end to end through the reference-named host entry point, pinned buffers
+    hsrc = torch.as_tensor(hs).pin_memory()
+    hq_ = torch.as_tensor(hq).pin_memory()
+    hd_ = torch.as_tensor(hd).pin_memory()
+    hv_ = torch.as_tensor(hv).pin_memory()
+    hpot = torch.empty((n, 1), dtype=torch.complex128).pin_memory()
+    hgrad = torch.empty((n, 2, 1), dtype=torch.complex128).pin_memory()
+
+    def e2e_step():
+        ier = C.c_int(0)
+        o = _lib.Options()
+        o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, _lib.PREC[prec]
+        L.b2fmm_lfmm2d_ex(1, C.c_double(1e-6), C.c_int64(n), ptr(hsrc), 1, ptr(hq_), 1, ptr(hd_),
+                          ptr(hv_), 2, ptr(hpot), ptr(hgrad), None, C.c_int64(0), None, 0, None,
+                          None, None, C.byref(o), None, C.byref(ier))
+        return ier.value
+
+    for _ in range(max(1, args.warmup - 1)):
+        e2e_step()
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    te = (time.perf_counter() - t0) / args.steps
+    if pg:
+        t = torch.tensor([te], device=dev, dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        te = float(t.item())
+    h2d = hsrc.numel() * 8 + hq_.numel() * 16 + hd_.numel() * 16 + hv_.numel() * 8
+    d2h = hpot.numel() * 16 + hgrad.numel() * 16
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_sample)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "n_points_per_gpu": n, "eps": 1e-6,
+                           "precision": prec, "parallelism": f"replicas x{world}",
+                           "l2_policy": "inputs (256 MB) and expansions larger than L2"},
+                "fp64_value": value64, "fp64_ms_per_step": ms64,
+                "speedup_vs_fp64": value / value64,
+                "rel_l2_err": err, "err_ref": "FP64 direct sum over 1000 random sources",
+                "e2e": {"value": world * n / te, "unit": "points/s", "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h},
+                "gpu_launches": int(launches),
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

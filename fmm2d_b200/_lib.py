@@ -1,0 +1,92 @@
+"""ctypes binding of ``libfmm2d_b200.so`` (the C ABI of include/fmm2d_b200.h).
+
+The library is built in-tree by ``fmm2d_b200/build.py``.  Loading fails loudly
+when it is missing: there is no CPU fallback behind this package.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libfmm2d_b200.so")
+
+c_int, c_double, c_int64, c_void_p = C.c_int, C.c_double, C.c_int64, C.c_void_p
+P = c_void_p  # all array arguments are raw pointers
+
+
+class Options(C.Structure):
+    """Mirror of ``b2fmm_options``."""
+    _fields_ = [("ndiv", c_int), ("idivflag", c_int), ("ifnear", c_int), ("precision", c_int)]
+
+
+PREC = {"auto": 0, "fp64": 1, "mixed": 2}
+
+_LAP_HOST = [c_int, c_double, c_int64, P, c_int, P, c_int, P]
+_PGH = [c_int, P, P, P, c_int64, P, c_int, P, P, P]
+
+# name -> argtypes, for every symbol declared in include/fmm2d_b200.h
+SIGNATURES = {
+    "b2fmm_version": [],
+    "b2fmm_cfmm2d": _LAP_HOST + [c_int] + _PGH + [P],
+    "b2fmm_lfmm2d": _LAP_HOST + [P, c_int] + _PGH + [P],
+    "b2fmm_rfmm2d": _LAP_HOST + [P, c_int] + _PGH + [P],
+    "b2fmm_cfmm2d_ndiv": _LAP_HOST + [c_int] + _PGH + [c_int, c_int, c_int, P, P],
+    "b2fmm_lfmm2d_ndiv": _LAP_HOST + [P, c_int] + _PGH + [c_int, c_int, c_int, P, P],
+    "b2fmm_rfmm2d_ndiv": _LAP_HOST + [P, c_int] + _PGH + [c_int, c_int, c_int, P, P],
+    "b2fmm_cfmm2d_ex": _LAP_HOST + _PGH + [P, P, P],
+    "b2fmm_lfmm2d_ex": _LAP_HOST + [P] + _PGH + [P, P, P],
+    "b2fmm_rfmm2d_ex": _LAP_HOST + [P] + _PGH + [P, P, P],
+    "b2fmm_cfmm2d_dev": _LAP_HOST + _PGH + [P, P, P, P],
+    "b2fmm_lfmm2d_dev": _LAP_HOST + [P] + _PGH + [P, P, P, P],
+    "b2fmm_rfmm2d_dev": _LAP_HOST + [P] + _PGH + [P, P, P, P],
+    "b2fmm_lap_direct_dev": [c_int, c_int, c_int64, P, P, P, P, c_int64, P, c_int, P, P, P,
+                             c_double, P, P],
+    "b2fmm_tree_build": [P, c_int64, P, c_int64, c_int, c_int, c_int, P, P, P],
+    "b2fmm_tree_get": [P] * 23,
+    "b2fmm_tree_free": [P],
+    "b2fmm_kernel_launches": [],
+    "b2fmm_set_stats": [c_int],
+    "b2fmm_get_stats": [P, c_int],
+    "b2fmm_fma_peak": [c_int],
+}
+
+_lib = None
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+def lib():
+    """Load the CUDA library (raises LibraryMissing when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise LibraryMissing(
+                f"{LIBPATH} not found: build it with `python -m fmm2d_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(LIBPATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = None
+        L.b2fmm_version.restype = C.c_char_p
+        L.b2fmm_tree_build.restype = c_void_p
+        L.b2fmm_kernel_launches.restype = C.c_uint64
+        L.b2fmm_fma_peak.restype = c_double
+        _lib = L
+    return _lib
+
+
+STAT_KEYS = ["nboxes", "nlevels", "nleaves", "nterms1", "p2p_pairs", "m2l_pairs", "m2p_evals",
+             "p2l_sources", "npts_eval", "tree_ms", "fmm_ms", "nd_cauchy"]
+
+
+def get_stats():
+    import numpy as np
+    out = np.zeros(len(STAT_KEYS))
+    lib().b2fmm_get_stats(out.ctypes.data_as(c_void_p), len(STAT_KEYS))
+    return dict(zip(STAT_KEYS, out.tolist()))
+
+
+def version():
+    return lib().b2fmm_version().decode()

@@ -1,0 +1,377 @@
+// extern "C" entry points (include/fmm2d_b200.h).
+#include <cstring>
+#include <vector>
+
+#include "../../include/fmm2d_b200.h"
+#include "direct.cuh"
+#include "laplace.cuh"
+#include "tree.cuh"
+#include "peaks.cuh"
+
+namespace b2 {
+std::atomic<unsigned long long> g_launches{0};
+}
+
+using namespace b2;
+
+namespace {
+
+template <typename F>
+void guarded(int* ier, F&& f) {
+  try {
+    int r = f();
+    if (ier) *ier = r;
+  } catch (const CudaError& e) {
+    fprintf(stderr, "fmm2d_b200: %s\n", e.what());
+    if (ier) *ier = e.ier;
+  } catch (const std::bad_alloc&) {
+    if (ier) *ier = IER_ALLOC;
+  } catch (...) {
+    if (ier) *ier = IER_CUDA;
+  }
+}
+
+LapArgs make_args(int fe, int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+                  int ifpgh, double* pot, double* grad, double* hess, int64_t nt,
+                  const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                  double* hesstarg, const b2fmm_options* o, double* timeinfo) {
+  LapArgs a;
+  a.fe = fe;
+  a.nd = nd;
+  a.eps = eps;
+  a.ns = ns;
+  a.src = sources;
+  a.charge = ifcharge == 1 ? charge : nullptr;
+  a.dipstr = ifdipole == 1 ? dipstr : nullptr;
+  a.dipvec = ifdipole == 1 ? dipvec : nullptr;
+  a.ifpgh = ifpgh;
+  a.pot = pot;
+  a.grad = grad;
+  a.hess = hess;
+  a.nt = nt;
+  a.trg = targ;
+  a.ifpghtarg = ifpghtarg;
+  a.pottarg = pottarg;
+  a.gradtarg = gradtarg;
+  a.hesstarg = hesstarg;
+  if (o) {
+    a.ndiv = o->ndiv;
+    a.idivflag = o->idivflag;
+    a.ifnear = o->ifnear;
+    a.precision = o->precision;
+  }
+  a.timeinfo = timeinfo;
+  return a;
+}
+
+// Host-pointer driver: copies inputs to the device, runs, copies results back.
+int lap_host(LapArgs h) {
+  cudaStream_t st = cudaStreamPerThread;
+  const int nd = h.nd;
+  const long ns = h.ns, nt = h.nt;
+  const int cw = h.fe == FE_REAL ? 1 : 2;
+  const int gw = h.fe == FE_CAUCHY ? 1 : 2, hw = h.fe == FE_CAUCHY ? 1 : 3;
+  const size_t nq = (size_t)cw * nd;
+  DBuf<double> src(st), trg(st), q(st), dp(st), dv(st), po(st), gr(st), he(st), pt(st), gt(st),
+      ht(st);
+  auto up = [&](DBuf<double>& d, const double* hp, size_t n) {
+    if (!hp || n == 0) return (double*)nullptr;
+    d.alloc(n, st);
+    B2_CHECK(cudaMemcpyAsync(d.p, hp, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    return d.p;
+  };
+  auto mk = [&](DBuf<double>& d, size_t n) {
+    if (n == 0) return (double*)nullptr;
+    d.alloc(n, st);
+    return d.p;
+  };
+  LapArgs a = h;
+  a.src = up(src, h.src, 2 * (size_t)ns);
+  a.trg = up(trg, h.ifpghtarg > 0 ? h.trg : nullptr, 2 * (size_t)nt);
+  a.charge = up(q, h.charge, nq * ns);
+  a.dipstr = up(dp, h.dipstr, nq * ns);
+  a.dipvec = h.fe != FE_CAUCHY ? up(dv, h.dipstr ? h.dipvec : nullptr, 2 * (size_t)nd * ns) : nullptr;
+  a.pot = h.ifpgh >= 1 ? mk(po, nq * ns) : nullptr;
+  a.grad = h.ifpgh >= 2 ? mk(gr, nq * gw * ns) : nullptr;
+  a.hess = h.ifpgh >= 3 ? mk(he, nq * hw * ns) : nullptr;
+  a.pottarg = h.ifpghtarg >= 1 ? mk(pt, nq * nt) : nullptr;
+  a.gradtarg = h.ifpghtarg >= 2 ? mk(gt, nq * gw * nt) : nullptr;
+  a.hesstarg = h.ifpghtarg >= 3 ? mk(ht, nq * hw * nt) : nullptr;
+  int r = lap_fmm_device(a, st);
+  if (r != IER_OK) return r;
+  auto down = [&](double* hp, const double* dpp, size_t n) {
+    if (hp && dpp && n) B2_CHECK(cudaMemcpyAsync(hp, dpp, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  };
+  down(h.pot, a.pot, nq * ns);
+  down(h.grad, a.grad, nq * gw * ns);
+  down(h.hess, a.hess, nq * hw * ns);
+  down(h.pottarg, a.pottarg, nq * nt);
+  down(h.gradtarg, a.gradtarg, nq * gw * nt);
+  down(h.hesstarg, a.hesstarg, nq * hw * nt);
+  B2_CHECK(cudaStreamSynchronize(st));
+  return IER_OK;
+}
+
+struct TreeHandle {
+  DeviceTree T;
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* b2fmm_version(void) { return "fmm2d_b200 0.1 (sm_100a)"; }
+
+void b2fmm_cfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr, int iper, int ifpgh,
+                  double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                  int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg, int* ier) {
+  (void)iper;
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_CAUCHY, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              nullptr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, nullptr, nullptr));
+  });
+}
+
+void b2fmm_lfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+                  int iper, int ifpgh, double* pot, double* grad, double* hess, int64_t nt,
+                  const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                  double* hesstarg, int* ier) {
+  (void)iper;
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_LAPLACE, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, nullptr, nullptr));
+  });
+}
+
+void b2fmm_rfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+                  int iper, int ifpgh, double* pot, double* grad, double* hess, int64_t nt,
+                  const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                  double* hesstarg, int* ier) {
+  (void)iper;
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_REAL, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, nullptr, nullptr));
+  });
+}
+
+void b2fmm_cfmm2d_ndiv(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dipstr, int iper,
+                       int ifpgh, double* pot, double* grad, double* hess, int64_t nt,
+                       const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                       double* hesstarg, int ndiv, int idivflag, int ifnear, double* timeinfo,
+                       int* ier) {
+  (void)iper;
+  b2fmm_options o{ndiv, idivflag, ifnear, PREC_AUTO};
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_CAUCHY, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              nullptr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, &o, timeinfo));
+  });
+}
+
+void b2fmm_lfmm2d_ndiv(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dipstr,
+                       const double* dipvec, int iper, int ifpgh, double* pot, double* grad,
+                       double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                       double* pottarg, double* gradtarg, double* hesstarg, int ndiv,
+                       int idivflag, int ifnear, double* timeinfo, int* ier) {
+  (void)iper;
+  b2fmm_options o{ndiv, idivflag, ifnear, PREC_AUTO};
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_LAPLACE, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, &o, timeinfo));
+  });
+}
+
+void b2fmm_rfmm2d_ndiv(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dipstr,
+                       const double* dipvec, int iper, int ifpgh, double* pot, double* grad,
+                       double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                       double* pottarg, double* gradtarg, double* hesstarg, int ndiv,
+                       int idivflag, int ifnear, double* timeinfo, int* ier) {
+  (void)iper;
+  b2fmm_options o{ndiv, idivflag, ifnear, PREC_AUTO};
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_REAL, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, &o, timeinfo));
+  });
+}
+
+void b2fmm_cfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr, int ifpgh,
+                     double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                     int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                     const b2fmm_options* opts, double* timeinfo, int* ier) {
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_CAUCHY, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              nullptr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, opts, timeinfo));
+  });
+}
+
+void b2fmm_lfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr,
+                     const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                     int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                     double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                     double* timeinfo, int* ier) {
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_LAPLACE, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, opts, timeinfo));
+  });
+}
+
+void b2fmm_rfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr,
+                     const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                     int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                     double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                     double* timeinfo, int* ier) {
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_REAL, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, opts, timeinfo));
+  });
+}
+
+void b2fmm_cfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr, int ifpgh,
+                      double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                      int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                      const b2fmm_options* opts, double* timeinfo, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_fmm_device(make_args(FE_CAUCHY, nd, eps, ns, sources, ifcharge, charge, ifdipole,
+                                    dipstr, nullptr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+                                    pottarg, gradtarg, hesstarg, opts, timeinfo),
+                          (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_lfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr,
+                      const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                      int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                      double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                      double* timeinfo, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_fmm_device(make_args(FE_LAPLACE, nd, eps, ns, sources, ifcharge, charge, ifdipole,
+                                    dipstr, dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+                                    pottarg, gradtarg, hesstarg, opts, timeinfo),
+                          (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_rfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr,
+                      const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                      int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                      double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                      double* timeinfo, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_fmm_device(make_args(FE_REAL, nd, eps, ns, sources, ifcharge, charge, ifdipole,
+                                    dipstr, dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+                                    pottarg, gradtarg, hesstarg, opts, timeinfo),
+                          (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_lap_direct_dev(int kind, int nd, int64_t ns, const double* sources,
+                          const double* charge, const double* dipstr, const double* dipvec,
+                          int64_t nt, const double* targ, int ifpgh, double* pot, double* grad,
+                          double* hess, double thresh, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_direct_device(kind, nd, ns, sources, charge, dipstr, dipvec, nt, targ, ifpgh, pot,
+                             grad, hess, thresh, (cudaStream_t)stream);
+  });
+}
+
+void* b2fmm_tree_build(const double* sources_dev, int64_t ns, const double* targ_dev, int64_t nt,
+                       int idivflag, int ndiv, int nlmax, int* nlevels, int* nboxes, int* ier) {
+  TreeHandle* h = nullptr;
+  guarded(ier, [&] {
+    if (ns < 1 || nt < 0 || ndiv < 1 || nlmax < 0 || nlmax > NLMAX) return (int)IER_BADARG;
+    int dev = 0;
+    B2_CHECK(cudaGetDevice(&dev));
+    configure_mempool(dev);
+    h = new TreeHandle();
+    build_device_tree(h->T, sources_dev, ns, targ_dev, nt, idivflag, ndiv, nlmax,
+                      cudaStreamPerThread);
+    *nlevels = h->T.nlevels;
+    *nboxes = h->T.nboxes;
+    return (int)IER_OK;
+  });
+  if (ier && *ier != IER_OK) {
+    delete h;
+    return nullptr;
+  }
+  return h;
+}
+
+void b2fmm_tree_get(void* tree, int* laddr, int* ilevel, int* iparent, int* nchild, int* ichild,
+                    int* ncoll, int* coll, double* centers, double* boxsize, int* isrc,
+                    int* isrcse, int* itarg, int* itargse, int* nlist1, int* list1, int* nlist2,
+                    int* list2, int* nlist3, int* list3, int* nlist4, int* list4, int* ier) {
+  guarded(ier, [&] {
+    TreeHandle* h = (TreeHandle*)tree;
+    DeviceTree& T = h->T;
+    cudaStream_t st = T.st;
+    int nb = T.nboxes;
+    for (int l = 0; l <= T.nlevels; l++) {
+      laddr[2 * l] = T.lfirst[l];
+      laddr[2 * l + 1] = T.llast[l];
+      boxsize[l] = T.boxsize[l];
+    }
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+      if (bytes) B2_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    };
+    cp(ilevel, T.level.p, sizeof(int) * nb);
+    cp(iparent, T.parent.p, sizeof(int) * nb);
+    cp(nchild, T.nchild.p, sizeof(int) * nb);
+    cp(ichild, T.child.p, sizeof(int) * 4 * nb);
+    cp(ncoll, T.ncoll.p, sizeof(int) * nb);
+    cp(coll, T.coll.p, sizeof(int) * 9 * nb);
+    cp(centers, T.center.p, sizeof(double) * 2 * nb);
+    cp(isrc, T.isrc.p, sizeof(int) * T.ns);
+    cp(isrcse, T.srng.p, sizeof(int) * 2 * nb);
+    cp(itarg, T.itarg.p, sizeof(int) * T.nt);
+    cp(itargse, T.trng.p, sizeof(int) * 2 * nb);
+    cp(nlist1, T.nlist1.p, sizeof(int) * nb);
+    cp(list1, T.list1.p, sizeof(int) * MNLIST1 * nb);
+    cp(nlist2, T.nlist2.p, sizeof(int) * nb);
+    cp(list2, T.list2.p, sizeof(int) * MNLIST2 * nb);
+    cp(nlist3, T.nlist3.p, sizeof(int) * nb);
+    cp(list3, T.list3.p, sizeof(int) * MNLIST3 * nb);
+    cp(nlist4, T.nlist4.p, sizeof(int) * nb);
+    cp(list4, T.list4.p, sizeof(int) * MNLIST4 * nb);
+    B2_CHECK(cudaStreamSynchronize(st));
+    return (int)IER_OK;
+  });
+}
+
+void b2fmm_tree_free(void* tree) { delete (TreeHandle*)tree; }
+
+uint64_t b2fmm_kernel_launches(void) { return g_launches.load(); }
+
+void b2fmm_set_stats(int on) { set_stats(on != 0); }
+
+void b2fmm_get_stats(double* out, int n) {
+  const LapStats& S = last_stats();
+  const double v[12] = {S.nboxes,    S.nlevels,     S.nleaves,   S.nterms1,
+                        S.p2p_pairs, S.m2l_pairs,   S.m2p_evals, S.p2l_sources,
+                        S.npts_eval, S.tree_ms,     S.fmm_ms,    S.nd_cauchy};
+  for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
+}
+
+double b2fmm_fma_peak(int fp64) { return fma_peak_flops(fp64 != 0); }
+
+}  // extern "C"

@@ -1,0 +1,1101 @@
+// Cauchy/Laplace FMM on B200 (FP64 path).
+//
+// Follows the step order of cfmm2dmain (src/laplace/cfmm2d.f:442-1341) with
+// the operators of src/laplace/laprouts2d.f and the near field of
+// src/laplace/cauchykernels2d.f.  Layout in HBM: points and densities are
+// gathered once into tree order (sources/targets sorted into leaves), and the
+// multipole / local expansions live in two arrays of nboxes x P x ND complex
+// doubles (P = nterms + 1 coefficients, ND densities of the current chunk),
+// so the coefficients of one box are contiguous.
+//
+// Kernels (one warp per box unless noted):
+//   k_p2m        P2M at leaves (step 1)
+//   k_m2m        upward pass, one launch per level (step 3)
+//   k_p2l        list 4 -> local (step 2)
+//   k_m2l        list 2 multipole -> local (step 4)
+//   k_l2l        downward pass, one launch per level (step 5)
+//   k_leaf       per leaf and 32 evaluation points: L2P + M2P (list 3) +
+//                P2P (list 1) fused, one result write per point (steps 6-8)
+//   k_unpack     caller layout (cfmm / lfmm / rfmm) and inverse permutation
+#include "laplace.cuh"
+
+#include <cmath>
+#include <mutex>
+
+
+namespace b2 {
+
+namespace {
+std::atomic<bool> g_stats_on{false};
+thread_local LapStats g_last_stats;
+}  // namespace
+
+// src/laplace/lndiv2d.f:1-39
+int lap_ndiv(double eps) {
+  if (eps >= 0.5e0) return 3;
+  if (eps >= 0.5e-1) return 5;
+  if (eps >= 0.5e-2) return 8;
+  if (eps >= 0.5e-3) return 10;
+  if (eps >= 0.5e-6) return 15;
+  if (eps >= 0.5e-9) return 20;
+  if (eps >= 0.5e-12) return 25;
+  if (eps >= 0.5e-15) return 45;
+  return -1;  // reference: ns + nt (no refinement)
+}
+
+// src/laplace/l2dterms.f:38-82: smallest j >= 2 with
+// (sqrt2/2)^j / 1.5^(j+1) < eps (worst-case M2L decay), else 1.
+int lap_nterms(double eps) {
+  const double z2 = std::sqrt(2.0) / 2.0;
+  double h = 1.0, jp = 1.0;
+  for (int j = 0; j <= 100; j++) {
+    h *= 1.5;
+    if (j >= 2 && std::fabs(jp * (1.0 / h)) < eps) return j;
+    jp *= z2;
+  }
+  return 1;
+}
+
+void set_stats(bool on) { g_stats_on = on; }
+const LapStats& last_stats() { return g_last_stats; }
+
+const double* device_binomials() {
+  static std::mutex mu;
+  static double* tab[128] = {nullptr};
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (!tab[dev]) {
+    // Pascal recursion as in init_carray (src/common/fmmcommon2d.f:150-165)
+    std::vector<double> c((size_t)BINOM_N * BINOM_N, 0.0);
+    for (int l = 0; l < BINOM_N; l++) c[(size_t)l * BINOM_N] = 1.0;
+    for (int m = 1; m < BINOM_N; m++) {
+      c[(size_t)m * BINOM_N + m] = 1.0;
+      for (int l = m + 1; l < BINOM_N; l++)
+        c[(size_t)l * BINOM_N + m] = c[(size_t)(l - 1) * BINOM_N + m] + c[(size_t)(l - 1) * BINOM_N + m - 1];
+    }
+    double* d = nullptr;
+    B2_CHECK(cudaMalloc(&d, c.size() * sizeof(double)));
+    B2_CHECK(cudaMemcpy(d, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice));
+    tab[dev] = d;
+  }
+  return tab[dev];
+}
+
+void configure_mempool(int device) {
+  static std::mutex mu;
+  static bool done[128] = {false};
+  std::lock_guard<std::mutex> g(mu);
+  if (done[device]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  done[device] = true;
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cpow_int(double2 w, int e) {
+  double2 r = make_double2(1.0, 0.0);
+  double2 b = w;
+  while (e > 0) {
+    if (e & 1) r = cmul(r, b);
+    e >>= 1;
+    if (e) b = cmul(b, b);
+  }
+  return r;
+}
+
+__device__ __forceinline__ double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
+
+// Box and list arrays of the device tree, passed by value to kernels.
+struct TV {
+  const double2* center;
+  const int* level;
+  const int* nchild;
+  const int4* child;
+  const int2* srng;
+  const int2* trng;
+  const int* nl1;
+  const int* l1;
+  const int* nl2;
+  const int* l2;
+  const int* nl3;
+  const int* l3;
+  const int* nl4;
+  const int* l4;
+  const double* boxsize;  // nlevels + 2 entries
+  int ifpgh, ifpghtarg;
+  __device__ __forceinline__ bool has_eval_pts(int b) const {
+    int n = 0;
+    if (ifpghtarg > 0) n += trng[b].y - trng[b].x;
+    if (ifpgh > 0) n += srng[b].y - srng[b].x;
+    return n > 0;
+  }
+};
+
+struct Dens {
+  const double2* q;  // sorted charges (ndc per point) or null
+  const double2* d;  // sorted dipole strengths or null
+  int ndc;           // Cauchy densities per point
+  int d0;            // first density of the current chunk
+};
+
+#define WARP_LOOP(n)                                                                  \
+  const int lane = threadIdx.x & 31;                                                  \
+  const int wib = threadIdx.x >> 5;                                                   \
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;                                   \
+  for (int bi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; bi < (n); bi += nwarps)
+
+// ---------------------------------------------------------------------------
+// step 1: P2M (laprouts2d.f:84-282) at leaves of level >= 2; every other leaf
+// gets a zero expansion so that list 2 / list 3 reads are well defined.
+// m_0 += q,  m_n += -q w^n / n + d w^(n-1) / r,  w = (x - c) / r
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(128) k_p2m(TV t, int first, int n, const double2* __restrict__ xs,
+                                             Dens D, int P, double2* __restrict__ mp) {
+  WARP_LOOP(n) {
+    (void)wib;
+    int b = first + bi;
+    if (t.nchild[b] != 0) continue;
+    double2 acc[2][ND];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    int lev = t.level[b];
+    int2 sr = t.srng[b];
+    if (lev >= 2 && sr.y > sr.x) {
+      double r = t.boxsize[lev];
+      double2 c = t.center[b];
+      for (int j = sr.x; j < sr.y; j++) {
+        double2 x = xs[j];
+        double2 w = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
+        double2 qj[ND], dj[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          qj[d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+          dj[d] = D.d ? D.d[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+        }
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          int k = lane + 32 * s;
+          if (k >= P) break;
+          if (k == 0) {
+#pragma unroll
+            for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], qj[d]);
+          } else {
+            double2 pw = cpow_int(w, k - 1);
+            double2 pn = cmul(pw, w);
+            double2 cq = make_double2(-pn.x / k, -pn.y / k);
+            double2 cd = make_double2(pw.x / r, pw.y / r);
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              cfma(acc[s][d], qj[d], cq);
+              cfma(acc[s][d], dj[d], cd);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      int k = lane + 32 * s;
+      if (k >= P) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) mp[((size_t)b * P + k) * ND + d] = acc[s][d];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// step 3: M2M (laprouts2d.f:905-1015) from the children with sources.
+// z0 = child - parent; t_j = h_j (r1/z0)^j;
+// H_0 = t_0, H_i = (-t_0/i + sum_{j=1..i} t_j C(i-1, j-1)) (z0/r2)^i
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
+                                             const double* __restrict__ binom,
+                                             double2* __restrict__ mp) {
+  extern __shared__ double2 smem[];
+  WARP_LOOP(n) {
+    double2* T = smem + (size_t)wib * P * ND;
+    int b = first + bi;
+    if (t.nchild[b] == 0) continue;
+    int lev = t.level[b];
+    double r2 = t.boxsize[lev], r1 = t.boxsize[lev + 1];
+    double2 c2 = t.center[b];
+    double2 acc[2][ND];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    int4 ch = t.child[b];
+    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    for (int q = 0; q < 4; q++) {
+      int k = cc[q];
+      if (t.srng[k].y <= t.srng[k].x) continue;
+      double2 c1 = t.center[k];
+      double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
+      double2 w1 = crcp(make_double2(z0.x / r1, z0.y / r1));
+      double2 w2 = make_double2(z0.x / r2, z0.y / r2);
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int j = lane + 32 * s;
+        if (j >= P) break;
+        double2 a = cpow_int(w1, j);
+#pragma unroll
+        for (int d = 0; d < ND; d++) T[j * ND + d] = cmul(mp[((size_t)k * P + j) * ND + d], a);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int i = lane + 32 * s;
+        if (i >= P) break;
+        if (i == 0) {
+#pragma unroll
+          for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], T[d]);
+          continue;
+        }
+        double2 v[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) v[d] = make_double2(-T[d].x / i, -T[d].y / i);
+        const double* crow = binom + (size_t)(i - 1) * BINOM_N;
+        for (int j = 1; j <= i; j++) {
+          double cb = crow[j - 1];
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            double2 tj = T[j * ND + d];
+            v[d].x += tj.x * cb;
+            v[d].y += tj.y * cb;
+          }
+        }
+        double2 bi_ = cpow_int(w2, i);
+#pragma unroll
+        for (int d = 0; d < ND; d++) cfma(acc[s][d], v[d], bi_);
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      int i = lane + 32 * s;
+      if (i >= P) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = acc[s][d];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// step 2: P2L from list 4 (laprouts2d.f:501-690), z0 = x - c, w = r/z0:
+// l_0 += q log|z0| - d/z0,  l_n += -q w^n/n - (d/z0) w^n
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(128) k_p2l(TV t, int first, int n, const double2* __restrict__ xs,
+                                             Dens D, int P, double2* __restrict__ lo) {
+  WARP_LOOP(n) {
+    (void)wib;
+    int b = first + bi;
+    int n4 = t.nl4[b];
+    if (n4 == 0 || !t.has_eval_pts(b)) continue;
+    int lev = t.level[b];
+    double r = t.boxsize[lev];
+    double2 c = t.center[b];
+    double2 acc[2][ND];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    for (int e = 0; e < n4; e++) {
+      int jb = t.l4[(size_t)MNLIST4 * b + e];
+      int2 sr = t.srng[jb];
+      for (int j = sr.x; j < sr.y; j++) {
+        double2 x = xs[j];
+        double2 z0 = make_double2(x.x - c.x, x.y - c.y);
+        double2 zi = crcp(z0);
+        double2 w = make_double2(r * zi.x, r * zi.y);
+        double2 qj[ND], dj[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          qj[d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+          dj[d] = D.d ? D.d[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+        }
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          int k = lane + 32 * s;
+          if (k >= P) break;
+          if (k == 0) {
+            double lg = log(hypot(z0.x, z0.y));
+            double2 mzi = cneg(zi);
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              acc[s][d].x += qj[d].x * lg;
+              acc[s][d].y += qj[d].y * lg;
+              cfma(acc[s][d], dj[d], mzi);
+            }
+          } else {
+            double2 wn = cpow_int(w, k);
+            double2 cq = make_double2(-wn.x / k, -wn.y / k);
+            double2 cd = cneg(cmul(zi, wn));
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              cfma(acc[s][d], qj[d], cq);
+              cfma(acc[s][d], dj[d], cd);
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      int k = lane + 32 * s;
+      if (k >= P) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        size_t o = ((size_t)b * P + k) * ND + d;
+        lo[o] = cadd(lo[o], acc[s][d]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// step 4: M2L over list 2 (laprouts2d.f:1130-1244), z0 = c_src - c_tgt,
+// u = r/z0, t_j = h_j (-u)^j:
+//   L_0 += t_0 log|z0| + sum_{j>=1} t_j
+//   L_i += (-t_0/i + sum_{j>=1} C(i+j-1, j-1) t_j) u^i
+// The offset-independent matrix G (G_0j = 1, G_i0 = -1/i, G_ij = C(i+j-1,j-1))
+// sits in shared memory; per pair only the power vectors depend on z0.
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
+                                             const double* __restrict__ binom,
+                                             const double2* __restrict__ mp,
+                                             double2* __restrict__ lo) {
+  extern __shared__ double2 smem[];
+  double* G = (double*)smem;  // G[j * P + i]
+  for (int e = threadIdx.x; e < P * P; e += blockDim.x) {
+    int j = e / P, i = e % P;
+    double g;
+    if (i == 0)
+      g = (j == 0) ? 0.0 : 1.0;
+    else if (j == 0)
+      g = -1.0 / i;
+    else
+      g = binom[(size_t)(i + j - 1) * BINOM_N + (j - 1)];
+    G[e] = g;
+  }
+  __syncthreads();
+  double2* Tbase = smem + (P * P + 1) / 2;
+  WARP_LOOP(n) {
+    double2* T = Tbase + (size_t)wib * P * ND;
+    int b = first + bi;
+    int n2 = t.nl2[b];
+    if (n2 == 0 || !t.has_eval_pts(b)) continue;
+    double r = t.boxsize[t.level[b]];
+    double2 cb = t.center[b];
+    double2 acc[2][ND];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    for (int e = 0; e < n2; e++) {
+      int jb = t.l2[(size_t)MNLIST2 * b + e];
+      double2 cj = t.center[jb];
+      double2 z0 = make_double2(cj.x - cb.x, cj.y - cb.y);
+      double2 zi = crcp(z0);
+      double2 u = make_double2(zi.x * r, zi.y * r);
+      double lg = log(hypot(z0.x, z0.y));
+      double2 ui[2];
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int j = lane + 32 * s;
+        if (j >= P) break;
+        double2 uj = cpow_int(u, j);
+        ui[s] = uj;
+        double2 sj = (j & 1) ? cneg(uj) : uj;
+#pragma unroll
+        for (int d = 0; d < ND; d++) T[j * ND + d] = cmul(mp[((size_t)jb * P + j) * ND + d], sj);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int i = lane + 32 * s;
+        if (i >= P) break;
+        double2 y[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) y[d] = make_double2(0, 0);
+        for (int j = 0; j < P; j++) {
+          double g = G[j * P + i];
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            double2 tj = T[j * ND + d];
+            y[d].x += g * tj.x;
+            y[d].y += g * tj.y;
+          }
+        }
+        if (i == 0) {
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            acc[s][d].x += y[d].x + T[d].x * lg;
+            acc[s][d].y += y[d].y + T[d].y * lg;
+          }
+        } else {
+#pragma unroll
+          for (int d = 0; d < ND; d++) cfma(acc[s][d], y[d], ui[s]);
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      int i = lane + 32 * s;
+      if (i >= P) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        size_t o = ((size_t)b * P + i) * ND + d;
+        lo[o] = cadd(lo[o], acc[s][d]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// step 5: L2L (laprouts2d.f:1020-1123), z0 = child - parent:
+// t_j = l_j (z0/r1)^j, L_i += (sum_{j>=i} t_j C(j, i)) (r2/z0)^i
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int P,
+                                             const double* __restrict__ binom,
+                                             double2* __restrict__ lo) {
+  extern __shared__ double2 smem[];
+  WARP_LOOP(n) {
+    double2* T = smem + (size_t)wib * P * ND;
+    int b = first + bi;
+    if (t.nchild[b] == 0 || !t.has_eval_pts(b)) continue;
+    int lev = t.level[b];
+    double r1 = t.boxsize[lev], r2 = t.boxsize[lev + 1];
+    double2 c1 = t.center[b];
+    int4 ch = t.child[b];
+    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    for (int q = 0; q < 4; q++) {
+      int k = cc[q];
+      double2 ck = t.center[k];
+      double2 z0 = make_double2(ck.x - c1.x, ck.y - c1.y);
+      double2 w1 = make_double2(z0.x / r1, z0.y / r1);
+      double2 w2 = crcp(make_double2(z0.x / r2, z0.y / r2));
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int j = lane + 32 * s;
+        if (j >= P) break;
+        double2 a = cpow_int(w1, j);
+#pragma unroll
+        for (int d = 0; d < ND; d++) T[j * ND + d] = cmul(lo[((size_t)b * P + j) * ND + d], a);
+      }
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int i = lane + 32 * s;
+        if (i >= P) break;
+        double2 v[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
+        for (int j = i; j < P; j++) {
+          double cb = binom[(size_t)j * BINOM_N + i];
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            double2 tj = T[j * ND + d];
+            v[d].x += tj.x * cb;
+            v[d].y += tj.y * cb;
+          }
+        }
+        double2 bi_ = cpow_int(w2, i);
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          size_t o = ((size_t)k * P + i) * ND + d;
+          double2 cur = lo[o];
+          cfma(cur, v[d], bi_);
+          lo[o] = cur;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// steps 6-8 fused per leaf: for 32 evaluation points at a time,
+//   L2P  (laprouts2d.f:696-897)   Horner in (z - c)/r with derivatives
+//   M2P  (laprouts2d.f:289-500)   for each list-3 box, Horner in w = r/(z-c)
+//   P2P  (cauchykernels2d.f)      for each list-1 box, sources staged in smem
+// and one store of pot / grad / hess per point (tree order).
+// ---------------------------------------------------------------------------
+template <int ND>
+struct LeafSmem {
+  double2 coef[64 * ND];  // local or multipole coefficients
+  double2 sx[32];
+  double2 sq[32 * ND];
+  double2 sd[32 * ND];
+};
+
+template <int ND, int IFPGH>
+__global__ void __launch_bounds__(64) k_leaf(TV t, int first, int n, int use_targets,
+                                            const double2* __restrict__ xs,
+                                            const double2* __restrict__ xe, Dens D, int P,
+                                            const double2* __restrict__ mp,
+                                            const double2* __restrict__ lo, double thresh,
+                                            int ifnear, double2* __restrict__ pot,
+                                            double2* __restrict__ grad,
+                                            double2* __restrict__ hess) {
+  extern __shared__ double2 smem[];
+  const double th2 = thresh * thresh;
+  WARP_LOOP(n) {
+    LeafSmem<ND>* S = (LeafSmem<ND>*)smem + wib;
+    int b = first + bi;
+    if (t.nchild[b] != 0) continue;
+    int2 er = use_targets ? t.trng[b] : t.srng[b];
+    if (er.y <= er.x) continue;
+    int lev = t.level[b];
+    double r = t.boxsize[lev];
+    double2 cb = t.center[b];
+    int n3 = t.nl3[b], n1 = ifnear ? t.nl1[b] : 0;
+    for (int k0 = er.x; k0 < er.y; k0 += 32) {
+      int k = k0 + lane;
+      bool act = k < er.y;
+      double2 z = act ? xe[k] : cb;
+      double2 pt[ND], gr[ND], hs[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
+      // L2P
+      __syncwarp();
+      for (int e = lane; e < P * ND; e += 32) S->coef[e] = lo[(size_t)b * P * ND + e];
+      __syncwarp();
+      {
+        double2 zz = make_double2((z.x - cb.x) / r, (z.y - cb.y) / r);
+        double2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          f[d] = S->coef[(P - 1) * ND + d];
+          f1[d] = f2[d] = make_double2(0, 0);
+        }
+        for (int m = P - 2; m >= 0; m--) {
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], zz), f1[d]);
+            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], zz), f[d]);
+            f[d] = cadd(cmul(f[d], zz), S->coef[m * ND + d]);
+          }
+        }
+        double ri = 1.0 / r;
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          pt[d] = f[d];
+          if (IFPGH >= 2) gr[d] = cscale(f1[d], ri);
+          if (IFPGH >= 3) hs[d] = cscale(f2[d], 2.0 * ri * ri);
+        }
+      }
+      // M2P from list 3 (boxes one level finer)
+      for (int e = 0; e < n3; e++) {
+        int jb = t.l3[(size_t)MNLIST3 * b + e];
+        double rj = t.boxsize[lev + 1];
+        double2 cj = t.center[jb];
+        __syncwarp();
+        for (int q = lane; q < P * ND; q += 32) S->coef[q] = mp[(size_t)jb * P * ND + q];
+        __syncwarp();
+        double2 zc = make_double2(z.x - cj.x, z.y - cj.y);
+        double2 zi = crcp(zc);
+        double2 w = make_double2(rj * zi.x, rj * zi.y);
+        double lg = log(hypot(zc.x, zc.y));
+        // S(w) = sum_{m>=1} c_m w^m by Horner, with S' and S''
+        double2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          f[d] = S->coef[(P - 1) * ND + d];
+          f1[d] = f2[d] = make_double2(0, 0);
+        }
+        for (int m = P - 2; m >= 1; m--) {
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], w), f1[d]);
+            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], w), f[d]);
+            f[d] = cadd(cmul(f[d], w), S->coef[m * ND + d]);
+          }
+        }
+        // now f = sum_{m>=1} c_m w^(m-1); shift by one power of w
+        double2 w2 = cmul(w, w);
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          double2 c0 = S->coef[d];
+          // S = w f ; S' = f + w f1 ; S'' = 2 f1 + w f2
+          double2 Sv = cmul(w, f[d]);
+          double2 S1 = cadd(f[d], cmul(w, f1[d]));
+          // f2 holds f''/2 (Horner), so S'' = 2 f' + w f'' = 2 (f1 + w f2)
+          double2 S2 = cscale(cadd(f1[d], cmul(w, f2[d])), 2.0);
+          pt[d].x += Sv.x + c0.x * lg;
+          pt[d].y += Sv.y + c0.y * lg;
+          if (IFPGH >= 2) {
+            // d/dz = S'(w) (-w^2/r) + c0/z
+            double2 g = cmul(S1, w2);
+            g = make_double2(-g.x / rj, -g.y / rj);
+            g = cadd(g, cmul(c0, zi));
+            gr[d] = cadd(gr[d], g);
+          }
+          if (IFPGH >= 3) {
+            // d2/dz2 = S'' w^4/r^2 + S' 2 w^3/r^2 - c0/z^2
+            double2 w3 = cmul(w2, w), w4 = cmul(w2, w2);
+            double ir2 = 1.0 / (rj * rj);
+            double2 h = cadd(cmul(S2, w4), cscale(cmul(S1, w3), 2.0));
+            h = cscale(h, ir2);
+            h = csub(h, cmul(c0, cmul(zi, zi)));
+            hs[d] = cadd(hs[d], h);
+          }
+        }
+      }
+      // P2P from list 1
+      for (int e = 0; e < n1; e++) {
+        int jb = t.l1[(size_t)MNLIST1 * b + e];
+        int2 sr = t.srng[jb];
+        for (int s0 = sr.x; s0 < sr.y; s0 += 32) {
+          int ns = min(32, sr.y - s0);
+          __syncwarp();
+          if (lane < ns) {
+            int j = s0 + lane;
+            S->sx[lane] = xs[j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              if (D.q) S->sq[lane * ND + d] = D.q[(size_t)j * D.ndc + D.d0 + d];
+              if (D.d) S->sd[lane * ND + d] = D.d[(size_t)j * D.ndc + D.d0 + d];
+            }
+          }
+          __syncwarp();
+          if (act) {
+            for (int j = 0; j < ns; j++) {
+              double2 y = S->sx[j];
+              double dx = z.x - y.x, dy = z.y - y.y;
+              double rr = dx * dx + dy * dy;
+              // cauchykernels2d.f: <= for potential-only, < otherwise
+              if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
+              double ir = 1.0 / rr;
+              double2 zi = make_double2(dx * ir, -dy * ir);
+              double lg = 0.5 * log(rr);
+              double2 z2 = (IFPGH >= 2 || D.d) ? cneg(cmul(zi, zi)) : make_double2(0, 0);
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                if (D.q) {
+                  double2 c = S->sq[j * ND + d];
+                  pt[d].x += lg * c.x;
+                  pt[d].y += lg * c.y;
+                  if (IFPGH >= 2) cfma(gr[d], zi, c);
+                  if (IFPGH >= 3) cfma(hs[d], z2, c);
+                }
+                if (D.d) {
+                  double2 c = S->sd[j * ND + d];
+                  cfma(pt[d], zi, c);
+                  if (IFPGH >= 2) cfma(gr[d], z2, c);
+                  if (IFPGH >= 3) {
+                    double2 z3 = cscale(cmul(z2, zi), -2.0);
+                    cfma(hs[d], z3, c);
+                  }
+                }
+              }
+            }
+          }
+        }
+      }
+      if (act) {
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          size_t o = (size_t)k * D.ndc + D.d0 + d;
+          pot[o] = pt[d];
+          if (IFPGH >= 2) grad[o] = gr[d];
+          if (IFPGH >= 3) hess[o] = hs[d];
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// gather / unpack
+// ---------------------------------------------------------------------------
+__global__ void k_gather_pts(const double* __restrict__ xy, const int* __restrict__ perm, long n,
+                             double2* __restrict__ out) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int i = perm[k];
+  out[k] = make_double2(xy[2 * (size_t)i], xy[2 * (size_t)i + 1]);
+}
+
+// Caller densities -> sorted Cauchy densities (lfmm2d.f:139-156, rfmm2d.f:137-151)
+__global__ void k_gather_dens(int fe, int nd, int ndc, const int* __restrict__ perm, long n,
+                              const double* __restrict__ charge, const double* __restrict__ dipstr,
+                              const double* __restrict__ dipvec, double2* __restrict__ qs,
+                              double2* __restrict__ ds) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  size_t i = perm[k];
+  for (int j = 0; j < nd; j++) {
+    if (fe == FE_CAUCHY) {
+      if (qs) qs[k * ndc + j] = ((const double2*)charge)[i * nd + j];
+      if (ds) ds[k * ndc + j] = ((const double2*)dipstr)[i * nd + j];
+    } else {
+      double2 mv = make_double2(0, 0);
+      if (ds) mv = make_double2(-dipvec[(i * 2 + 0) * nd + j], -dipvec[(i * 2 + 1) * nd + j]);
+      if (fe == FE_LAPLACE) {
+        if (qs) {
+          double2 q = ((const double2*)charge)[i * nd + j];
+          qs[k * ndc + 2 * j] = make_double2(q.x, 0);
+          qs[k * ndc + 2 * j + 1] = make_double2(q.y, 0);
+        }
+        if (ds) {
+          double2 dd = ((const double2*)dipstr)[i * nd + j];
+          ds[k * ndc + 2 * j] = cscale(mv, dd.x);
+          ds[k * ndc + 2 * j + 1] = cscale(mv, dd.y);
+        }
+      } else {
+        if (qs) qs[k * ndc + j] = make_double2(charge[i * nd + j], 0);
+        if (ds) ds[k * ndc + j] = cscale(mv, dipstr[i * nd + j]);
+      }
+    }
+  }
+}
+
+// Sorted Cauchy results -> caller layout and order (lfmm2d.f:169-223,
+// rfmm2d.f:158-212; cfmm2d.f:399-432 for the inverse permutation).
+__global__ void k_unpack(int fe, int nd, int ndc, int ifl, const int* __restrict__ perm, long n,
+                         const double2* __restrict__ P1, const double2* __restrict__ G1,
+                         const double2* __restrict__ H1, double* pot, double* grad, double* hess) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  size_t i = perm[k];
+  for (int j = 0; j < nd; j++) {
+    if (fe == FE_CAUCHY) {
+      ((double2*)pot)[i * nd + j] = P1[k * ndc + j];
+      if (ifl >= 2) ((double2*)grad)[i * nd + j] = G1[k * ndc + j];
+      if (ifl >= 3) ((double2*)hess)[i * nd + j] = H1[k * ndc + j];
+    } else if (fe == FE_LAPLACE) {
+      double2 a = P1[k * ndc + 2 * j], bb = P1[k * ndc + 2 * j + 1];
+      ((double2*)pot)[i * nd + j] = make_double2(a.x, bb.x);
+      if (ifl >= 2) {
+        double2 ga = G1[k * ndc + 2 * j], gb = G1[k * ndc + 2 * j + 1];
+        ((double2*)grad)[(i * 2 + 0) * nd + j] = make_double2(ga.x, gb.x);
+        ((double2*)grad)[(i * 2 + 1) * nd + j] = make_double2(-ga.y, -gb.y);
+      }
+      if (ifl >= 3) {
+        double2 ha = H1[k * ndc + 2 * j], hb = H1[k * ndc + 2 * j + 1];
+        ((double2*)hess)[(i * 3 + 0) * nd + j] = make_double2(ha.x, hb.x);
+        ((double2*)hess)[(i * 3 + 1) * nd + j] = make_double2(-ha.y, -hb.y);
+        ((double2*)hess)[(i * 3 + 2) * nd + j] = make_double2(-ha.x, -hb.x);
+      }
+    } else {
+      pot[i * nd + j] = P1[k * ndc + j].x;
+      if (ifl >= 2) {
+        double2 g = G1[k * ndc + j];
+        grad[(i * 2 + 0) * nd + j] = g.x;
+        grad[(i * 2 + 1) * nd + j] = -g.y;
+      }
+      if (ifl >= 3) {
+        double2 h = H1[k * ndc + j];
+        hess[(i * 3 + 0) * nd + j] = h.x;
+        hess[(i * 3 + 1) * nd + j] = -h.y;
+        hess[(i * 3 + 2) * nd + j] = -h.x;
+      }
+    }
+  }
+}
+
+// Work counts for the roofline accounting (enabled by set_stats).
+__global__ void k_stats(TV t, int nb, unsigned long long* out) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long c[6] = {0, 0, 0, 0, 0, 0};
+  if (b < nb) {
+    long ne = 0;
+    if (t.ifpgh > 0) ne += t.srng[b].y - t.srng[b].x;
+    if (t.ifpghtarg > 0) ne += t.trng[b].y - t.trng[b].x;
+    if (t.nchild[b] == 0) {
+      c[0] = 1;
+      long s = 0;
+      for (int e = 0; e < t.nl1[b]; e++) {
+        int j = t.l1[(size_t)MNLIST1 * b + e];
+        s += t.srng[j].y - t.srng[j].x;
+      }
+      c[1] = (unsigned long long)(ne * s);
+      c[3] = (unsigned long long)(ne * t.nl3[b]);
+      c[5] = (unsigned long long)ne;
+    }
+    if (ne > 0 && t.level[b] >= 2) {
+      c[2] = t.nl2[b];
+      long s4 = 0;
+      for (int e = 0; e < t.nl4[b]; e++) {
+        int j = t.l4[(size_t)MNLIST4 * b + e];
+        s4 += t.srng[j].y - t.srng[j].x;
+      }
+      c[4] = (unsigned long long)s4;
+    }
+  }
+  for (int k = 0; k < 6; k++) {
+    unsigned long long v = c[k];
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(~0u, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(&out[k], v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+int warp_grid(long nitems, int warps_per_block) {
+  long blocks = (nitems + warps_per_block - 1) / warps_per_block;
+  return (int)std::max(1L, std::min(blocks, 148L * 64));
+}
+
+template <int ND>
+void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int P,
+               const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
+               double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, double thresh,
+               cudaStream_t st, cudaEvent_t* ev) {
+  const double* binom = device_binomials();
+  const int nb = T.nboxes;
+  const int nl = T.nlevels;
+  B2_CHECK(cudaEventRecord(ev[0], st));
+  k_p2m<ND><<<warp_grid(nb, 4), 128, 0, st>>>(tv, 0, nb, xs, D, P, mp);
+  B2_LAUNCH_CHECK();
+  B2_CHECK(cudaEventRecord(ev[1], st));
+  size_t sm_t = sizeof(double2) * 4 * P * ND;
+  for (int l = nl - 1; l >= 1; l--) {
+    int f = T.lfirst[l], n = T.llast[l] - f + 1;
+    k_m2m<ND><<<warp_grid(n, 4), 128, sm_t, st>>>(tv, f, n, P, binom, mp);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[2], st));
+  B2_CHECK(cudaMemsetAsync(lo, 0, sizeof(double2) * (size_t)nb * P * ND, st));
+  if (nl >= 2) {
+    int f = T.lfirst[2], n = nb - f;
+    k_p2l<ND><<<warp_grid(n, 4), 128, 0, st>>>(tv, f, n, xs, D, P, lo);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[3], st));
+  if (nl >= 2) {
+    int f = T.lfirst[2], n = nb - f;
+    size_t sm = sizeof(double) * (P * P + 1) + sizeof(double2) * 4 * P * ND;
+    if (sm > 48 * 1024)
+      B2_CHECK(cudaFuncSetAttribute(k_m2l<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_m2l<ND><<<warp_grid(n, 4), 128, sm, st>>>(tv, f, n, P, binom, mp, lo);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[4], st));
+  for (int l = 1; l <= nl - 1; l++) {
+    int f = T.lfirst[l], n = T.llast[l] - f + 1;
+    k_l2l<ND><<<warp_grid(n, 4), 128, sm_t, st>>>(tv, f, n, P, binom, lo);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[5], st));
+  size_t sm_leaf = sizeof(LeafSmem<ND>) * 2;
+  auto leaf = [&](int use_t, int ifl, const double2* xe, double2* po, double2* gr, double2* he) {
+    if (ifl <= 0) return;
+    if (ifl == 1) {
+      B2_CHECK(cudaFuncSetAttribute(k_leaf<ND, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_leaf));
+      k_leaf<ND, 1><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
+                                                          thresh, a.ifnear, po, gr, he);
+    } else if (ifl == 2) {
+      B2_CHECK(cudaFuncSetAttribute(k_leaf<ND, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_leaf));
+      k_leaf<ND, 2><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
+                                                          thresh, a.ifnear, po, gr, he);
+    } else {
+      B2_CHECK(cudaFuncSetAttribute(k_leaf<ND, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_leaf));
+      k_leaf<ND, 3><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
+                                                          thresh, a.ifnear, po, gr, he);
+    }
+    B2_LAUNCH_CHECK();
+  };
+  leaf(0, a.ifpgh, xs, ps, gs, hs);
+  leaf(1, a.ifpghtarg, xt, pt, gt, ht);
+  B2_CHECK(cudaEventRecord(ev[6], st));
+}
+
+}  // namespace
+
+int lap_fmm_device(const LapArgs& a, cudaStream_t st) {
+  if (a.nd < 1 || a.ns < 0 || a.nt < 0 || a.ifpgh < 0 || a.ifpgh > 3 || a.ifpghtarg < 0 ||
+      a.ifpghtarg > 3 || a.ns > (1L << 30) || a.nt > (1L << 30))
+    return IER_BADARG;
+  if (a.ns > 0 && !a.src) return IER_BADARG;
+  if (a.nt > 0 && a.ifpghtarg > 0 && !a.trg) return IER_BADARG;
+  if ((a.fe == FE_LAPLACE || a.fe == FE_REAL) && a.dipstr && !a.dipvec) return IER_BADARG;
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  configure_mempool(dev);
+  const int nd = a.nd;
+  const int ndc = a.fe == FE_LAPLACE ? 2 * nd : nd;
+  const long ns = a.ns, nt = a.ifpghtarg > 0 ? a.nt : 0;
+  const bool fc = a.charge != nullptr, fd = a.dipstr != nullptr;
+  if (a.timeinfo)
+    for (int i = 0; i < 8; i++) a.timeinfo[i] = 0;
+  // user output sizes (in doubles)
+  const int cw = a.fe == FE_REAL ? 1 : 2;  // doubles per scalar output
+  const int gw = a.fe == FE_CAUCHY ? 1 : 2, hw = a.fe == FE_CAUCHY ? 1 : 3;
+  if (ns == 0 || (!fc && !fd)) {
+    // nothing interacts: every requested output is zero
+    if (a.ifpgh >= 1 && ns) B2_CHECK(cudaMemsetAsync(a.pot, 0, sizeof(double) * cw * nd * ns, st));
+    if (a.ifpgh >= 2 && ns) B2_CHECK(cudaMemsetAsync(a.grad, 0, sizeof(double) * cw * gw * nd * ns, st));
+    if (a.ifpgh >= 3 && ns) B2_CHECK(cudaMemsetAsync(a.hess, 0, sizeof(double) * cw * hw * nd * ns, st));
+    if (a.ifpghtarg >= 1 && nt) B2_CHECK(cudaMemsetAsync(a.pottarg, 0, sizeof(double) * cw * nd * nt, st));
+    if (a.ifpghtarg >= 2 && nt) B2_CHECK(cudaMemsetAsync(a.gradtarg, 0, sizeof(double) * cw * gw * nd * nt, st));
+    if (a.ifpghtarg >= 3 && nt) B2_CHECK(cudaMemsetAsync(a.hesstarg, 0, sizeof(double) * cw * hw * nd * nt, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    return IER_OK;
+  }
+  int ndiv = a.ndiv > 0 ? a.ndiv : lap_ndiv(a.eps);
+  if (ndiv <= 0) ndiv = (int)std::min<long>(ns + nt, 1L << 30);
+  const int p = lap_nterms(a.eps);
+  const int P = p + 1;
+  if (P > 64) return IER_NTERMS;
+  bool mixed = a.precision == PREC_MIXED || (a.precision == PREC_AUTO && a.eps >= 1e-6);
+
+  cudaEvent_t ev[8];
+  for (int i = 0; i < 8; i++) B2_CHECK(cudaEventCreate(&ev[i]));
+  B2_CHECK(cudaEventRecord(ev[7], st));
+
+  const bool want_stats = g_stats_on.load();
+  cudaEvent_t evt[3];
+  for (int i = 0; i < 3; i++) B2_CHECK(cudaEventCreate(&evt[i]));
+  B2_CHECK(cudaEventRecord(evt[0], st));
+  DeviceTree T;
+  build_device_tree(T, a.src, ns, a.trg, nt, a.idivflag, ndiv, NLMAX, st);
+  B2_CHECK(cudaEventRecord(evt[1], st));
+  const int nb = T.nboxes;
+  if (T.bs0 == 0.0) {
+    // every source and target coincides: all interactions are self
+    // interactions, which the reference omits, so every output is zero
+    if (a.ifpgh >= 1) B2_CHECK(cudaMemsetAsync(a.pot, 0, sizeof(double) * cw * nd * ns, st));
+    if (a.ifpgh >= 2) B2_CHECK(cudaMemsetAsync(a.grad, 0, sizeof(double) * cw * gw * nd * ns, st));
+    if (a.ifpgh >= 3) B2_CHECK(cudaMemsetAsync(a.hess, 0, sizeof(double) * cw * hw * nd * ns, st));
+    if (a.ifpghtarg >= 1 && nt) B2_CHECK(cudaMemsetAsync(a.pottarg, 0, sizeof(double) * cw * nd * nt, st));
+    if (a.ifpghtarg >= 2 && nt) B2_CHECK(cudaMemsetAsync(a.gradtarg, 0, sizeof(double) * cw * gw * nd * nt, st));
+    if (a.ifpghtarg >= 3 && nt) B2_CHECK(cudaMemsetAsync(a.hesstarg, 0, sizeof(double) * cw * hw * nd * nt, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    for (int i = 0; i < 3; i++) cudaEventDestroy(evt[i]);
+    for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+    return IER_OK;
+  }
+
+  std::vector<double> bsx(T.boxsize);
+  bsx.push_back(T.boxsize.back() / 2);
+  DBuf<double> dbs(st);
+  dbs.alloc(bsx.size(), st);
+  B2_CHECK(cudaMemcpyAsync(dbs.p, bsx.data(), sizeof(double) * bsx.size(), cudaMemcpyHostToDevice, st));
+
+  // sorted points and densities
+  DBuf<double2> xs(st), xt(st), qs(st), ds(st);
+  xs.alloc(ns, st);
+  k_gather_pts<<<ceil_div(ns, 256), 256, 0, st>>>(a.src, T.isrc.p, ns, xs.p);
+  B2_LAUNCH_CHECK();
+  if (nt > 0) {
+    xt.alloc(nt, st);
+    k_gather_pts<<<ceil_div(nt, 256), 256, 0, st>>>(a.trg, T.itarg.p, nt, xt.p);
+    B2_LAUNCH_CHECK();
+  }
+  if (fc) qs.alloc((size_t)ns * ndc, st);
+  if (fd) ds.alloc((size_t)ns * ndc, st);
+  k_gather_dens<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, T.isrc.p, ns, a.charge, a.dipstr,
+                                                   a.dipvec, qs.p, ds.p);
+  B2_LAUNCH_CHECK();
+
+  // sorted Cauchy results
+  DBuf<double2> ps(st), gs(st), hs(st), pt(st), gt(st), ht(st);
+  if (a.ifpgh >= 1) ps.alloc((size_t)ns * ndc, st);
+  if (a.ifpgh >= 2) gs.alloc((size_t)ns * ndc, st);
+  if (a.ifpgh >= 3) hs.alloc((size_t)ns * ndc, st);
+  if (a.ifpghtarg >= 1 && nt) pt.alloc((size_t)nt * ndc, st);
+  if (a.ifpghtarg >= 2 && nt) gt.alloc((size_t)nt * ndc, st);
+  if (a.ifpghtarg >= 3 && nt) ht.alloc((size_t)nt * ndc, st);
+
+  TV tv{T.center.p, T.level.p, T.nchild.p, T.child.p, T.srng.p, T.trng.p, T.nlist1.p, T.list1.p,
+        T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p, dbs.p, a.ifpgh,
+        nt > 0 ? a.ifpghtarg : 0};
+  const double thresh = T.bs0 * std::ldexp(1.0, -51);
+  DBuf<unsigned long long> dstat(st);
+  if (want_stats) {
+    dstat.alloc(6, st);
+    dstat.zero(6);
+    k_stats<<<ceil_div(nb, 256), 256, 0, st>>>(tv, nb, dstat.p);
+    B2_LAUNCH_CHECK();
+  }
+  int chunk = ndc >= 8 ? 8 : (ndc >= 4 ? 4 : (ndc >= 2 ? 2 : 1));
+  DBuf<double2> mp(st), lo(st);
+  mp.alloc((size_t)nb * P * chunk, st);
+  lo.alloc((size_t)nb * P * chunk, st);
+  double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int d0 = 0; d0 < ndc;) {
+    int left = ndc - d0;
+    int ND = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
+    Dens D{fc ? qs.p : nullptr, fd ? ds.p : nullptr, ndc, d0};
+    {
+      (void)mixed;
+      switch (ND) {
+        case 8: run_chunk<8>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+        case 4: run_chunk<4>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+        case 2: run_chunk<2>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+        default: run_chunk<1>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+      }
+    }
+    if (a.timeinfo) {
+      B2_CHECK(cudaEventSynchronize(ev[6]));
+      float ms[6];
+      for (int i = 0; i < 6; i++) B2_CHECK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+      // reference buckets: 1 P2M, 2 P2L, 3 M2M, 4 M2L, 5 L2L, 6 M2P, 7 L2P, 8 P2P;
+      // M2P/L2P/P2P run fused in one kernel and are reported in bucket 8.
+      tsum[0] += ms[0] * 1e-3;
+      tsum[2] += ms[1] * 1e-3;
+      tsum[1] += ms[2] * 1e-3;
+      tsum[3] += ms[3] * 1e-3;
+      tsum[4] += ms[4] * 1e-3;
+      tsum[7] += ms[5] * 1e-3;
+    }
+    d0 += ND;
+  }
+  if (a.ifpgh > 0) {
+    k_unpack<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpgh, T.isrc.p, ns, ps.p, gs.p,
+                                                hs.p, a.pot, a.grad, a.hess);
+    B2_LAUNCH_CHECK();
+  }
+  if (a.ifpghtarg > 0 && nt > 0) {
+    k_unpack<<<ceil_div(nt, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpghtarg, T.itarg.p, nt, pt.p,
+                                                gt.p, ht.p, a.pottarg, a.gradtarg, a.hesstarg);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(evt[2], st));
+  B2_CHECK(cudaStreamSynchronize(st));
+  if (a.timeinfo)
+    for (int i = 0; i < 8; i++) a.timeinfo[i] = tsum[i];
+  if (want_stats) {
+    unsigned long long hs6[6];
+    B2_CHECK(cudaMemcpy(hs6, dstat.p, sizeof(hs6), cudaMemcpyDeviceToHost));
+    float t1 = 0, t2 = 0;
+    B2_CHECK(cudaEventElapsedTime(&t1, evt[0], evt[1]));
+    B2_CHECK(cudaEventElapsedTime(&t2, evt[1], evt[2]));
+    LapStats& S = g_last_stats;
+    S.nboxes = nb;
+    S.nlevels = T.nlevels;
+    S.nleaves = (double)hs6[0];
+    S.nterms1 = P;
+    S.p2p_pairs = (double)hs6[1];
+    S.m2l_pairs = (double)hs6[2];
+    S.m2p_evals = (double)hs6[3];
+    S.p2l_sources = (double)hs6[4];
+    S.npts_eval = (double)hs6[5];
+    S.tree_ms = t1;
+    S.fmm_ms = t2;
+    S.nd_cauchy = ndc;
+  }
+  for (int i = 0; i < 3; i++) cudaEventDestroy(evt[i]);
+  for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+  return IER_OK;
+}
+
+}  // namespace b2

@@ -1,0 +1,67 @@
+// Cauchy/Laplace FMM engine (the path of src/laplace/cfmm2d.f, lfmm2d.f,
+// rfmm2d.f) on device memory.
+#pragma once
+#include "common.cuh"
+#include "tree.cuh"
+
+namespace b2 {
+
+// How caller densities map onto Cauchy densities and how results map back.
+enum FrontEnd {
+  FE_CAUCHY = 0,   // cfmm2d: complex charge/dipstr, outputs pot, d/dz, d2/dz2 (nd, n)
+  FE_LAPLACE = 1,  // lfmm2d: complex densities split into 2 Cauchy densities each
+  FE_REAL = 2      // rfmm2d: real densities
+};
+
+enum Precision { PREC_AUTO = 0, PREC_FP64 = 1, PREC_MIXED = 2 };
+
+struct LapArgs {
+  int fe = FE_CAUCHY;
+  int nd = 1;  // caller's number of densities
+  double eps = 1e-6;
+  long ns = 0;
+  const double* src = nullptr;  // (2, ns)
+  const double* charge = nullptr;  // complex (nd, ns) or real (nd, ns)
+  const double* dipstr = nullptr;  // complex or real (nd, ns)
+  const double* dipvec = nullptr;  // (nd, 2, ns) real, lfmm/rfmm only
+  int ifpgh = 0;
+  double *pot = nullptr, *grad = nullptr, *hess = nullptr;
+  long nt = 0;
+  const double* trg = nullptr;  // (2, nt)
+  int ifpghtarg = 0;
+  double *pottarg = nullptr, *gradtarg = nullptr, *hesstarg = nullptr;
+  // tuning (cfmm2d_ndiv.f:23-26)
+  int ndiv = 0;  // <= 0: lndiv2d table
+  int idivflag = 0;
+  int ifnear = 1;
+  int precision = PREC_AUTO;
+  double* timeinfo = nullptr;  // 8 phase times (s), host memory, may be null
+};
+
+// Runs the FMM on device pointers on stream `st`; returns an ier code.
+int lap_fmm_device(const LapArgs& a, cudaStream_t st);
+
+int lap_nterms(double eps);
+int lap_ndiv(double eps);
+
+// Work counts of the last FMM run on this thread (filled when enabled with
+// set_stats(true); costs one extra reduction kernel per call).
+struct LapStats {
+  double nboxes, nlevels, nleaves, nterms1;  // nterms1 = P = nterms + 1
+  double p2p_pairs;                          // sum over leaves: evals x list-1 sources
+  double m2l_pairs;                          // list-2 translations applied
+  double m2p_evals;                          // points x list-3 boxes
+  double p2l_sources;                        // list-4 sources applied
+  double npts_eval;                          // evaluation points (sources + targets)
+  double tree_ms;                            // tree + lists build time (device events)
+  double fmm_ms;                             // everything after the tree
+  double nd_cauchy;                          // Cauchy densities
+};
+void set_stats(bool on);
+const LapStats& last_stats();
+
+// Device binomial table C(l, m), 0 <= m <= l < BINOM_N, row-major (BINOM_N^2).
+constexpr int BINOM_N = 128;
+const double* device_binomials();
+
+}  // namespace b2

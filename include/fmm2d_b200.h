@@ -1,0 +1,172 @@
+/*
+ * fmm2d_b200 -- C ABI of the B200 (sm_100a) implementation of the fmm2d FMM
+ * evaluation path.  Every entry point replaces one routine of the reference
+ * (flatironinstitute/fmm2d); the citation above each declaration names it.
+ *
+ * Conventions (same as the reference's Fortran arrays):
+ *   sources(2,ns), targ(2,nt)          : x/y interleaved doubles
+ *   complex arrays                     : interleaved (re, im) doubles
+ *   charge/dipstr/pot/grad/hess (nd,n) : density index fastest
+ *   lfmm2d/rfmm2d grad (nd,2,n), hess (nd,3,n); dipvec (nd,2,n)
+ *   cfmm2d grad = d/dz, hess = d2/dz2, both (nd,n) complex
+ * Host entry points take host pointers and block until the results are in
+ * the caller's arrays.  The `_dev` entry points take device pointers, run on
+ * the given CUDA stream (NULL = legacy default stream) and return after the
+ * stream has finished the call.
+ * ier: 0 ok, 4 device allocation failure, 13 expansion order too large,
+ *      100 invalid argument, 101 CUDA error.
+ */
+#ifndef FMM2D_B200_H
+#define FMM2D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Tuning knobs of the *_ndiv drivers (src/laplace/cfmm2d_ndiv.f:23-26) plus
+ * the arithmetic mode. */
+typedef struct b2fmm_options {
+  int ndiv;      /* leaf capacity; <= 0 selects the lndiv2d/hndiv2d table  */
+  int idivflag;  /* 0: subdivide on sources, 1: targets, 2: max of both    */
+  int ifnear;    /* 1: include list-1 near field (P2P), 0: far field only  */
+  int precision; /* 0 auto (mixed when eps >= 1e-6), 1 FP64, 2 mixed        */
+} b2fmm_options;
+
+/* Library version string. */
+const char* b2fmm_version(void);
+
+/* ---------------------------------------------------------------- Laplace */
+
+/* cfmm2d: src/laplace/cfmm2d.f:23-26 (Cauchy kernel, complex densities). */
+void b2fmm_cfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr, int iper, int ifpgh,
+                  double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                  int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg, int* ier);
+
+/* lfmm2d: src/laplace/lfmm2d.f:29-32 (complex Laplace, dipvec orientations). */
+void b2fmm_lfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+                  int iper, int ifpgh, double* pot, double* grad, double* hess, int64_t nt,
+                  const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                  double* hesstarg, int* ier);
+
+/* rfmm2d: src/laplace/rfmm2d.f:27-30 (real densities, real outputs). */
+void b2fmm_rfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                  const double* charge, int ifdipole, const double* dipstr, const double* dipvec,
+                  int iper, int ifpgh, double* pot, double* grad, double* hess, int64_t nt,
+                  const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                  double* hesstarg, int* ier);
+
+/* cfmm2d_ndiv / lfmm2d_ndiv / rfmm2d_ndiv: src/laplace/cfmm2d_ndiv.f:23-26,
+ * lfmm2d_ndiv.f:29, rfmm2d_ndiv.f:27.  timeinfo[8] receives the per-step
+ * device times in seconds (P2M, P2L, M2M, M2L, L2L, M2P, L2P, P2P; the
+ * fused leaf kernel reports M2P+L2P+P2P in slot 8). */
+void b2fmm_cfmm2d_ndiv(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dipstr, int iper,
+                       int ifpgh, double* pot, double* grad, double* hess, int64_t nt,
+                       const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                       double* hesstarg, int ndiv, int idivflag, int ifnear, double* timeinfo,
+                       int* ier);
+void b2fmm_lfmm2d_ndiv(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dipstr,
+                       const double* dipvec, int iper, int ifpgh, double* pot, double* grad,
+                       double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                       double* pottarg, double* gradtarg, double* hesstarg, int ndiv,
+                       int idivflag, int ifnear, double* timeinfo, int* ier);
+void b2fmm_rfmm2d_ndiv(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dipstr,
+                       const double* dipvec, int iper, int ifpgh, double* pot, double* grad,
+                       double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                       double* pottarg, double* gradtarg, double* hesstarg, int ndiv,
+                       int idivflag, int ifnear, double* timeinfo, int* ier);
+
+/* Host-pointer variants with options and per-step timings (no reference
+ * counterpart beyond the *_ndiv drivers; used by the python front end). */
+void b2fmm_cfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr, int ifpgh,
+                     double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                     int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                     const b2fmm_options* opts, double* timeinfo, int* ier);
+void b2fmm_lfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr,
+                     const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                     int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                     double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                     double* timeinfo, int* ier);
+void b2fmm_rfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                     const double* charge, int ifdipole, const double* dipstr,
+                     const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                     int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                     double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                     double* timeinfo, int* ier);
+
+/* Device-pointer variants of cfmm2d / lfmm2d / rfmm2d (same argument meaning;
+ * opts may be NULL for the reference defaults; timeinfo may be NULL). */
+void b2fmm_cfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr, int ifpgh,
+                      double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                      int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                      const b2fmm_options* opts, double* timeinfo, void* stream, int* ier);
+void b2fmm_lfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr,
+                      const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                      int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                      double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                      double* timeinfo, void* stream, int* ier);
+void b2fmm_rfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                      const double* charge, int ifdipole, const double* dipstr,
+                      const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                      int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                      double* gradtarg, double* hesstarg, const b2fmm_options* opts,
+                      double* timeinfo, void* stream, int* ier);
+
+/* Direct sums on the device (the python API's c2ddir / l2ddir / r2ddir:
+ * python/fmm2dpy/fmm2d.py:1493-1740 over src/laplace/cauchykernels2d.f,
+ * lapkernels2d.f, rlapkernels2d.f).  Outputs are overwritten.  kind selects
+ * the kernel: 0 Cauchy, 1 complex Laplace, 2 real Laplace. */
+void b2fmm_lap_direct_dev(int kind, int nd, int64_t ns, const double* sources,
+                          const double* charge, const double* dipstr, const double* dipvec,
+                          int64_t nt, const double* targ, int ifpgh, double* pot, double* grad,
+                          double* hess, double thresh, void* stream, int* ier);
+
+/* ------------------------------------------------------------------- tree */
+
+/* Level-restricted tree and lists for (sources, targets), exported for
+ * structural comparison (src/common/pts_tree2d.f:34-655 tree,
+ * pts_tree2d.f:1222-1246 sort, tree_routs2d.f:486-710 lists).
+ * b2fmm_tree_build returns a handle and the sizes; b2fmm_tree_get copies the
+ * arrays to host memory (0-based box/point indices, -1 = none, half-open
+ * point ranges; laddr (nlevels+1, 2) inclusive box ranges per level). */
+void* b2fmm_tree_build(const double* sources_dev, int64_t ns, const double* targ_dev, int64_t nt,
+                       int idivflag, int ndiv, int nlmax, int* nlevels, int* nboxes, int* ier);
+void b2fmm_tree_get(void* tree, int* laddr, int* ilevel, int* iparent, int* nchild, int* ichild,
+                    int* ncoll, int* coll, double* centers, double* boxsize, int* isrc,
+                    int* isrcse, int* itarg, int* itargse, int* nlist1, int* list1, int* nlist2,
+                    int* list2, int* nlist3, int* list3, int* nlist4, int* list4, int* ier);
+void b2fmm_tree_free(void* tree);
+
+/* ----------------------------------------------------------- diagnostics */
+/* These have no counterpart in the reference; they serve the benchmark's
+ * roofline accounting. */
+
+/* Number of kernels this library has launched in the process. */
+uint64_t b2fmm_kernel_launches(void);
+
+/* Enable (1) / disable (0) work counting of subsequent FMM calls on this
+ * thread; b2fmm_get_stats copies up to n of: nboxes, nlevels, nleaves,
+ * nterms+1, P2P pairs, M2L translations, M2P evaluations, P2L sources,
+ * evaluation points, tree build ms, FMM ms after the tree, Cauchy densities. */
+void b2fmm_set_stats(int on);
+void b2fmm_get_stats(double* out, int n);
+
+/* Measured fused-multiply-add throughput of this GPU in flop/s (FP64 when
+ * fp64 != 0, else FP32), from a dependent-free FMA loop over all SMs. */
+double b2fmm_fma_peak(int fp64);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FMM2D_B200_H */
