@@ -1,0 +1,480 @@
+// Mixed-precision Laplace kernels (eps >= 1e-6).
+//
+// * k_m2l_f32: the M2L of laprouts2d.f:1130-1244 in FP32.  Boxes of one
+//   level are translated by integer offsets o (|o|_inf in 2..3) in units of
+//   the box size, so u = r/z0 = 1/o and log|z0| = log r + log|o| come from
+//   49-entry tables; per translation only the gather of the source
+//   multipole (FP64 -> FP32) and the fixed matrix G(i,j) = C(i+j-1, j-1)
+//   remain.  Local expansions are accumulated in FP32 per target box and
+//   added to the FP64 expansion once.
+// * k_leaf_mixed: L2P and M2P in FP64 (as the FP64 path), the near field in
+//   FP32.  Coordinates are stored as x - c0 split into hi + lo floats, so a
+//   difference (xt_hi - xs_hi) + (xt_lo - xs_lo) keeps the relative accuracy
+//   of the FP64 difference even for nearly coincident points; log and 1/r^2
+//   use the SFU.  Per-pair terms are summed in FP32 over at most 32 sources
+//   and the partial sums in FP64.  Small leaves split their sources between
+//   2 or 4 lane groups so that the warp stays busy.
+#include "lap_mixed.cuh"
+#include "laplace.cuh"
+
+namespace b2 {
+
+namespace {
+
+using namespace lapk;
+
+__global__ void k_prep_pts(const double2* __restrict__ x, long n, double cx0, double cy0,
+                           float4* __restrict__ out) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double dx = x[k].x - cx0, dy = x[k].y - cy0;
+  float hx = (float)dx, hy = (float)dy;
+  out[k] = make_float4(hx, hy, (float)(dx - (double)hx), (float)(dy - (double)hy));
+}
+
+__global__ void k_prep_dens(const double2* __restrict__ in, long m, float2* __restrict__ out) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k < m) out[k] = make_float2((float)in[k].x, (float)in[k].y);
+}
+
+// utab[o][k] = (1/o)^k for o = (ox, oy), ox, oy in -3..3; lgtab[o] = log|o|
+__global__ void k_utab(int P, float2* utab, float* lgtab) {
+  int i = blockIdx.x, k = threadIdx.x;
+  int ox = i / 7 - 3, oy = i % 7 - 3;
+  if (k >= P) return;
+  if (ox == 0 && oy == 0) {
+    utab[i * P + k] = make_float2(0.f, 0.f);
+    if (k == 0) lgtab[i] = 0.f;
+    return;
+  }
+  double2 u = crcp(make_double2((double)ox, (double)oy));
+  double2 p = cpow_int(u, k);
+  utab[i * P + k] = make_float2((float)p.x, (float)p.y);
+  if (k == 0) lgtab[i] = (float)log(hypot((double)ox, (double)oy));
+}
+
+__device__ __forceinline__ float2 cmulf_(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ void cfmaf_(float2& a, float2 b, float2 c) {
+  a.x = fmaf(b.x, c.x, fmaf(-b.y, c.y, a.x));
+  a.y = fmaf(b.x, c.y, fmaf(b.y, c.x, a.y));
+}
+
+template <int ND>
+__global__ void __launch_bounds__(128) k_m2l_f32(TV t, int first, int n, int P,
+                                                 const double* __restrict__ binom,
+                                                 const float2* __restrict__ utab_g,
+                                                 const float* __restrict__ lgtab_g,
+                                                 const double2* __restrict__ mp,
+                                                 double2* __restrict__ lo) {
+  extern __shared__ float smf[];
+  float* G = smf;                                  // G[j * P + i]
+  float2* U = (float2*)(smf + ((P * P + 1) & ~1));  // U[o * P + k]
+  float* LG = (float*)(U + 49 * P);
+  float2* Tb = (float2*)(LG + 50);
+  for (int e = threadIdx.x; e < P * P; e += blockDim.x) {
+    int j = e / P, i = e % P;
+    float g;
+    if (i == 0)
+      g = (j == 0) ? 0.f : 1.f;
+    else if (j == 0)
+      g = -1.f / i;
+    else
+      g = (float)binom[(size_t)(i + j - 1) * BINOM_N + (j - 1)];
+    G[e] = g;
+  }
+  for (int e = threadIdx.x; e < 49 * P; e += blockDim.x) U[e] = utab_g[e];
+  for (int e = threadIdx.x; e < 49; e += blockDim.x) LG[e] = lgtab_g[e];
+  __syncthreads();
+  WARP_LOOP(n) {
+    float2* T = Tb + (size_t)wib * P * ND;
+    int b = first + bi;
+    int n2 = t.nl2[b];
+    if (n2 == 0 || !t.has_eval_pts(b)) continue;
+    double r = t.boxsize[t.level[b]];
+    double2 cb = t.center[b];
+    float lgr = (float)log(r);
+    double rinv = 1.0 / r;
+    float2 acc[2][ND];
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_float2(0.f, 0.f);
+    for (int e = 0; e < n2; e++) {
+      int jb = t.l2[(size_t)MNLIST2 * b + e];
+      double2 cj = t.center[jb];
+      int ox = __double2int_rn((cj.x - cb.x) * rinv), oy = __double2int_rn((cj.y - cb.y) * rinv);
+      int oi = (ox + 3) * 7 + (oy + 3);
+      float lg = lgr + LG[oi];
+      const float2* Uo = U + oi * P;
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int j = lane + 32 * s;
+        if (j >= P) break;
+        float2 sj = Uo[j];
+        if (j & 1) sj = make_float2(-sj.x, -sj.y);
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          double2 h = mp[((size_t)jb * P + j) * ND + d];
+          T[j * ND + d] = cmulf_(make_float2((float)h.x, (float)h.y), sj);
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        int i = lane + 32 * s;
+        if (i >= P) break;
+        float2 y[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) y[d] = make_float2(0.f, 0.f);
+        for (int j = 0; j < P; j++) {
+          float g = G[j * P + i];
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            float2 tj = T[j * ND + d];
+            y[d].x = fmaf(g, tj.x, y[d].x);
+            y[d].y = fmaf(g, tj.y, y[d].y);
+          }
+        }
+        if (i == 0) {
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            acc[s][d].x += y[d].x + T[d].x * lg;
+            acc[s][d].y += y[d].y + T[d].y * lg;
+          }
+        } else {
+          float2 ui = Uo[i];
+#pragma unroll
+          for (int d = 0; d < ND; d++) cfmaf_(acc[s][d], y[d], ui);
+        }
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      int i = lane + 32 * s;
+      if (i >= P) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        size_t o = ((size_t)b * P + i) * ND + d;
+        double2 cur = lo[o];
+        lo[o] = make_double2(cur.x + acc[s][d].x, cur.y + acc[s][d].y);
+      }
+    }
+  }
+}
+
+template <int ND, int IFPGH>
+__global__ void __launch_bounds__(128) k_leaf_mixed(
+    TV t, int nb, int use_targets, const float4* __restrict__ xs32,
+    const float4* __restrict__ xe32, const double2* __restrict__ xe64,
+    const float2* __restrict__ q32, const float2* __restrict__ d32, int ndc, int d0, int P,
+    const double2* __restrict__ mp, const double2* __restrict__ lo, float th2, int ifnear,
+    double2* __restrict__ pot, double2* __restrict__ grad, double2* __restrict__ hess) {
+  extern __shared__ double2 smd[];
+  const bool hq = q32 != nullptr, hd = d32 != nullptr;
+  WARP_LOOP(nb) {
+    double2* coef = smd + (size_t)wib * (P * ND + 32 + 32 * ND);
+    float4* SX = (float4*)(coef + P * ND);
+    float2* SQ = (float2*)(SX + 32);
+    float2* SD = SQ + 32 * ND;
+    int b = bi;
+    if (t.nchild[b] != 0) continue;
+    int2 er = use_targets ? t.trng[b] : t.srng[b];
+    int ne = er.y - er.x;
+    if (ne <= 0) continue;
+    const int LG2G = ne <= 8 ? 2 : (ne <= 16 ? 1 : 0);  // log2 of the lane groups
+    const int G = 1 << LG2G, TW = 32 >> LG2G;
+    const int g = lane / TW, tl = lane % TW;
+    int lev = t.level[b];
+    double r = t.boxsize[lev];
+    double2 cb = t.center[b];
+    int n3 = t.nl3[b], n1 = ifnear ? t.nl1[b] : 0;
+    // list-1 sources as one concatenated index range
+    int l1s[MNLIST1], cum[MNLIST1 + 1];
+    cum[0] = 0;
+    for (int e = 0; e < MNLIST1; e++) {
+      int2 sr = e < n1 ? t.srng[t.l1[(size_t)MNLIST1 * b + e]] : make_int2(0, 0);
+      l1s[e] = sr.x;
+      cum[e + 1] = cum[e] + (sr.y - sr.x);
+    }
+    const int tot = cum[MNLIST1];
+    for (int k0 = er.x; k0 < er.y; k0 += TW) {
+      int k = k0 + tl;
+      bool act = k < er.y;
+      double2 z = act ? xe64[k] : cb;
+      float4 zf = act ? xe32[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+      double2 pt[ND], gr[ND], hs[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
+      // L2P (FP64) by lane group 0
+      __syncwarp();
+      for (int e = lane; e < P * ND; e += 32) coef[e] = lo[(size_t)b * P * ND + e];
+      __syncwarp();
+      if (g == 0) {
+        double2 zz = make_double2((z.x - cb.x) / r, (z.y - cb.y) / r);
+        double2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          f[d] = coef[(P - 1) * ND + d];
+          f1[d] = f2[d] = make_double2(0, 0);
+        }
+        for (int m = P - 2; m >= 0; m--) {
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], zz), f1[d]);
+            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], zz), f[d]);
+            f[d] = cadd(cmul(f[d], zz), coef[m * ND + d]);
+          }
+        }
+        double ri = 1.0 / r;
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          pt[d] = f[d];
+          if (IFPGH >= 2) gr[d] = cscale(f1[d], ri);
+          if (IFPGH >= 3) hs[d] = cscale(f2[d], 2.0 * ri * ri);
+        }
+      }
+      // M2P (FP64), list-3 box e by lane group e mod G
+      for (int e = 0; e < n3; e++) {
+        int jb = t.l3[(size_t)MNLIST3 * b + e];
+        __syncwarp();
+        for (int q = lane; q < P * ND; q += 32) coef[q] = mp[(size_t)jb * P * ND + q];
+        __syncwarp();
+        if ((e & (G - 1)) != g) continue;
+        double rj = t.boxsize[lev + 1];
+        double2 cj = t.center[jb];
+        double2 zc = make_double2(z.x - cj.x, z.y - cj.y);
+        double2 zi = crcp(zc);
+        double2 w = make_double2(rj * zi.x, rj * zi.y);
+        double lg = log(hypot(zc.x, zc.y));
+        double2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          f[d] = coef[(P - 1) * ND + d];
+          f1[d] = f2[d] = make_double2(0, 0);
+        }
+        for (int m = P - 2; m >= 1; m--) {
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], w), f1[d]);
+            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], w), f[d]);
+            f[d] = cadd(cmul(f[d], w), coef[m * ND + d]);
+          }
+        }
+        double2 w2 = cmul(w, w);
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          double2 c0 = coef[d];
+          double2 Sv = cmul(w, f[d]);
+          double2 S1 = cadd(f[d], cmul(w, f1[d]));
+          pt[d].x += Sv.x + c0.x * lg;
+          pt[d].y += Sv.y + c0.y * lg;
+          if (IFPGH >= 2) {
+            double2 gg = cmul(S1, w2);
+            gg = make_double2(-gg.x / rj, -gg.y / rj);
+            gr[d] = cadd(gr[d], cadd(gg, cmul(c0, zi)));
+          }
+          if (IFPGH >= 3) {
+            double2 S2 = cscale(cadd(f1[d], cmul(w, f2[d])), 2.0);
+            double2 w3 = cmul(w2, w), w4 = cmul(w2, w2);
+            double2 h = cadd(cmul(S2, w4), cscale(cmul(S1, w3), 2.0));
+            h = cscale(h, 1.0 / (rj * rj));
+            hs[d] = cadd(hs[d], csub(h, cmul(c0, cmul(zi, zi))));
+          }
+        }
+      }
+      // P2P (FP32) over the concatenated list-1 sources, 32 staged at a time
+      for (int g0 = 0; g0 < tot; g0 += 32) {
+        int m = min(32, tot - g0);
+        __syncwarp();
+        if (lane < m) {
+          int gi = g0 + lane, e = 0;
+          while (gi >= cum[e + 1]) e++;
+          int j = l1s[e] + (gi - cum[e]);
+          SX[lane] = xs32[j];
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            if (hq) SQ[lane * ND + d] = q32[(size_t)j * ndc + d0 + d];
+            if (hd) SD[lane * ND + d] = d32[(size_t)j * ndc + d0 + d];
+          }
+        }
+        __syncwarp();
+        float2 fp[ND], fg[ND], fh[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
+        if (act) {
+          for (int jj = g; jj < m; jj += G) {
+            float4 s = SX[jj];
+            float dx = (zf.x - s.x) + (zf.z - s.z);
+            float dy = (zf.y - s.y) + (zf.w - s.w);
+            float rr = fmaf(dx, dx, dy * dy);
+            // cauchykernels2d.f: <= for potential-only, < otherwise
+            if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
+            float ir = __fdividef(1.0f, rr);
+            float2 zi = make_float2(dx * ir, -dy * ir);
+            float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
+            if (hq) {
+              float lg = 0.5f * __logf(rr);
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                float2 c = SQ[jj * ND + d];
+                fp[d].x = fmaf(lg, c.x, fp[d].x);
+                fp[d].y = fmaf(lg, c.y, fp[d].y);
+                if (IFPGH >= 2) cfmaf_(fg[d], zi, c);
+                if (IFPGH >= 3) cfmaf_(fh[d], z2, c);
+              }
+            }
+            if (hd) {
+              float2 z3 = make_float2(0.f, 0.f);
+              if (IFPGH >= 3) {
+                z3 = cmulf_(z2, zi);
+                z3 = make_float2(-2.f * z3.x, -2.f * z3.y);
+              }
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                float2 c = SD[jj * ND + d];
+                cfmaf_(fp[d], zi, c);
+                if (IFPGH >= 2) cfmaf_(fg[d], z2, c);
+                if (IFPGH >= 3) cfmaf_(fh[d], z3, c);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          pt[d].x += fp[d].x;
+          pt[d].y += fp[d].y;
+          if (IFPGH >= 2) {
+            gr[d].x += fg[d].x;
+            gr[d].y += fg[d].y;
+          }
+          if (IFPGH >= 3) {
+            hs[d].x += fh[d].x;
+            hs[d].y += fh[d].y;
+          }
+        }
+      }
+      // combine the lane groups (same target in lanes tl, tl+TW, ...)
+      for (int off = TW; off < 32; off <<= 1) {
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          pt[d].x += __shfl_xor_sync(~0u, pt[d].x, off);
+          pt[d].y += __shfl_xor_sync(~0u, pt[d].y, off);
+          if (IFPGH >= 2) {
+            gr[d].x += __shfl_xor_sync(~0u, gr[d].x, off);
+            gr[d].y += __shfl_xor_sync(~0u, gr[d].y, off);
+          }
+          if (IFPGH >= 3) {
+            hs[d].x += __shfl_xor_sync(~0u, hs[d].x, off);
+            hs[d].y += __shfl_xor_sync(~0u, hs[d].y, off);
+          }
+        }
+      }
+      if (act && g == 0) {
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          size_t o = (size_t)k * ndc + d0 + d;
+          pot[o] = pt[d];
+          if (IFPGH >= 2) grad[o] = gr[d];
+          if (IFPGH >= 3) hess[o] = hs[d];
+        }
+      }
+    }
+  }
+}
+
+int grid_for(long nitems, int wpb) {
+  long blocks = (nitems + wpb - 1) / wpb;
+  return (int)std::max(1L, std::min(blocks, 148L * 32));
+}
+
+template <int ND>
+void m2l_launch(const TV& t, int first, int n, int P, const double* binom, const MixedData& M,
+                const double2* mp, double2* lo, cudaStream_t st) {
+  size_t sm = sizeof(float) * (((P * P + 1) & ~1) + 2 * 49 * P + 50) + sizeof(float2) * 4 * P * ND;
+  B2_CHECK(cudaFuncSetAttribute(k_m2l_f32<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_m2l_f32<ND><<<grid_for(n, 4), 128, sm, st>>>(t, first, n, P, binom, M.utab.p, M.lgtab.p, mp, lo);
+  B2_LAUNCH_CHECK();
+}
+
+template <int ND, int IFPGH>
+void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const double2* xe64,
+                 int ndc, int d0, int P, const double2* mp, const double2* lo, double thresh,
+                 int ifnear, double2* pot, double2* grad, double2* hess, cudaStream_t st) {
+  size_t sm = sizeof(double2) * 4 * (P * ND + 32 + 32 * ND);
+  B2_CHECK(cudaFuncSetAttribute(k_leaf_mixed<ND, IFPGH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sm));
+  k_leaf_mixed<ND, IFPGH><<<grid_for(nb, 4), 128, sm, st>>>(
+      t, nb, use_targets, M.xs.p, use_targets ? M.xt.p : M.xs.p, xe64, M.q.p, M.d.p, ndc, d0, P,
+      mp, lo, (float)(thresh * thresh), ifnear, pot, grad, hess);
+  B2_LAUNCH_CHECK();
+}
+
+template <int ND>
+void leaf_dispatch(int ifl, const TV& t, int nb, int use_targets, const MixedData& M,
+                   const double2* xe64, int ndc, int d0, int P, const double2* mp,
+                   const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
+                   double2* hess, cudaStream_t st) {
+  if (ifl == 1)
+    leaf_launch<ND, 1>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+  else if (ifl == 2)
+    leaf_launch<ND, 2>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+  else
+    leaf_launch<ND, 3>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+}
+
+}  // namespace
+
+void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* xt, long nt,
+                       const double2* qs, const double2* ds, int ndc, double cx0, double cy0,
+                       int P, cudaStream_t st) {
+  M.xs.alloc(ns, st);
+  k_prep_pts<<<ceil_div(ns, 256), 256, 0, st>>>(xs, ns, cx0, cy0, M.xs.p);
+  B2_LAUNCH_CHECK();
+  if (nt > 0) {
+    M.xt.alloc(nt, st);
+    k_prep_pts<<<ceil_div(nt, 256), 256, 0, st>>>(xt, nt, cx0, cy0, M.xt.p);
+    B2_LAUNCH_CHECK();
+  }
+  long m = ns * (long)ndc;
+  if (qs) {
+    M.q.alloc(m, st);
+    k_prep_dens<<<ceil_div(m, 256), 256, 0, st>>>(qs, m, M.q.p);
+    B2_LAUNCH_CHECK();
+  }
+  if (ds) {
+    M.d.alloc(m, st);
+    k_prep_dens<<<ceil_div(m, 256), 256, 0, st>>>(ds, m, M.d.p);
+    B2_LAUNCH_CHECK();
+  }
+  M.utab.alloc(49 * (size_t)P, st);
+  M.lgtab.alloc(49, st);
+  k_utab<<<49, 64, 0, st>>>(P, M.utab.p, M.lgtab.p);
+  B2_LAUNCH_CHECK();
+}
+
+void lap_mixed_m2l(int ND, const TV& t, int first, int n, int P, const double* binom,
+                   const MixedData& M, const double2* mp, double2* lo, cudaStream_t st) {
+  switch (ND) {
+    case 8: m2l_launch<8>(t, first, n, P, binom, M, mp, lo, st); break;
+    case 4: m2l_launch<4>(t, first, n, P, binom, M, mp, lo, st); break;
+    case 2: m2l_launch<2>(t, first, n, P, binom, M, mp, lo, st); break;
+    default: m2l_launch<1>(t, first, n, P, binom, M, mp, lo, st); break;
+  }
+}
+
+void lap_mixed_leaf(int ND, int ifl, const TV& t, int nb, int use_targets, const MixedData& M,
+                    const double2* xe64, int ndc, int d0, int P, const double2* mp,
+                    const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
+                    double2* hess, cudaStream_t st) {
+  switch (ND) {
+    case 8: leaf_dispatch<8>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
+    case 4: leaf_dispatch<4>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
+    case 2: leaf_dispatch<2>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
+    default: leaf_dispatch<1>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
+  }
+}
+
+}  // namespace b2

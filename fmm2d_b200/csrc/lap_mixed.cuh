@@ -1,0 +1,32 @@
+// Mixed-precision kernels of the Laplace FMM (used when eps >= 1e-6 or when
+// requested): FP32 M2L and a FP32 near field with double-float coordinate
+// differences; expansions, shifts, L2P and M2P stay FP64.
+#pragma once
+#include "lap_common.cuh"
+
+namespace b2 {
+
+// FP32 copies of the sorted points (x - c0 split into hi/lo floats, so that
+// coordinate differences keep FP64-level relative accuracy) and densities.
+struct MixedData {
+  DBuf<float4> xs, xt;  // (xhi, yhi, xlo, ylo)
+  DBuf<float2> q, d;    // all Cauchy densities, ndc per point
+  DBuf<float2> utab;    // (1/o)^k for the 7x7 integer offsets o, k < P
+  DBuf<float> lgtab;    // log|o|
+};
+
+void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* xt, long nt,
+                       const double2* qs, const double2* ds, int ndc, double cx0, double cy0,
+                       int P, cudaStream_t st);
+
+// M2L over list 2 for boxes [first, first+n) of one density chunk (FP32).
+void lap_mixed_m2l(int ND, const lapk::TV& t, int first, int n, int P, const double* binom,
+                   const MixedData& M, const double2* mp, double2* lo, cudaStream_t st);
+
+// Fused leaf evaluation (L2P + M2P in FP64, P2P in FP32) for one chunk.
+void lap_mixed_leaf(int ND, int ifl, const lapk::TV& t, int nb, int use_targets,
+                    const MixedData& M, const double2* xe64, int ndc, int d0, int P,
+                    const double2* mp, const double2* lo, double thresh, int ifnear,
+                    double2* pot, double2* grad, double2* hess, cudaStream_t st);
+
+}  // namespace b2

@@ -18,6 +18,8 @@
 //                P2P (list 1) fused, one result write per point (steps 6-8)
 //   k_unpack     caller layout (cfmm / lfmm / rfmm) and inverse permutation
 #include "laplace.cuh"
+#include "lap_common.cuh"
+#include "lap_mixed.cuh"
 
 #include <cmath>
 #include <mutex>
@@ -97,71 +99,25 @@ void configure_mempool(int device) {
 
 namespace {
 
+using namespace lapk;
+
 // ---------------------------------------------------------------------------
-// device helpers
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double2 cpow_int(double2 w, int e) {
-  double2 r = make_double2(1.0, 0.0);
-  double2 b = w;
-  while (e > 0) {
-    if (e & 1) r = cmul(r, b);
-    e >>= 1;
-    if (e) b = cmul(b, b);
-  }
-  return r;
-}
-
-__device__ __forceinline__ double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
-
-// Box and list arrays of the device tree, passed by value to kernels.
-struct TV {
-  const double2* center;
-  const int* level;
-  const int* nchild;
-  const int4* child;
-  const int2* srng;
-  const int2* trng;
-  const int* nl1;
-  const int* l1;
-  const int* nl2;
-  const int* l2;
-  const int* nl3;
-  const int* l3;
-  const int* nl4;
-  const int* l4;
-  const double* boxsize;  // nlevels + 2 entries
-  int ifpgh, ifpghtarg;
-  __device__ __forceinline__ bool has_eval_pts(int b) const {
-    int n = 0;
-    if (ifpghtarg > 0) n += trng[b].y - trng[b].x;
-    if (ifpgh > 0) n += srng[b].y - srng[b].x;
-    return n > 0;
-  }
-};
-
-struct Dens {
-  const double2* q;  // sorted charges (ndc per point) or null
-  const double2* d;  // sorted dipole strengths or null
-  int ndc;           // Cauchy densities per point
-  int d0;            // first density of the current chunk
-};
-
-#define WARP_LOOP(n)                                                                  \
-  const int lane = threadIdx.x & 31;                                                  \
-  const int wib = threadIdx.x >> 5;                                                   \
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;                                   \
-  for (int bi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; bi < (n); bi += nwarps)
-
+// Shared-memory staging used by P2M and P2L: 32 sources at a time, one per
+// lane, each lane writing the power table w^0..w^(P-1) of its source and its
+// (pre-scaled) densities; then the lanes switch to one coefficient each and
+// accumulate over the staged sources.
 // ---------------------------------------------------------------------------
 // step 1: P2M (laprouts2d.f:84-282) at leaves of level >= 2; every other leaf
 // gets a zero expansion so that list 2 / list 3 reads are well defined.
-// m_0 += q,  m_n += -q w^n / n + d w^(n-1) / r,  w = (x - c) / r
-// ---------------------------------------------------------------------------
+// m_0 += q,  m_n += -q w^n / n + (d/r) w^(n-1),  w = (x - c) / r
 template <int ND>
-__global__ void __launch_bounds__(128) k_p2m(TV t, int first, int n, const double2* __restrict__ xs,
-                                             Dens D, int P, double2* __restrict__ mp) {
+__global__ void __launch_bounds__(64) k_p2m(TV t, int first, int n, const double2* __restrict__ xs,
+                                            Dens D, int P, double2* __restrict__ mp) {
+  extern __shared__ double2 smem[];
   WARP_LOOP(n) {
-    (void)wib;
+    double2* W = smem + (size_t)wib * (32 * P + 64 * ND);
+    double2* Q = W + 32 * P;
+    double2* Dd = Q + 32 * ND;
     int b = first + bi;
     if (t.nchild[b] != 0) continue;
     double2 acc[2][ND];
@@ -173,32 +129,46 @@ __global__ void __launch_bounds__(128) k_p2m(TV t, int first, int n, const doubl
     int2 sr = t.srng[b];
     if (lev >= 2 && sr.y > sr.x) {
       double r = t.boxsize[lev];
+      double ri = 1.0 / r;
       double2 c = t.center[b];
-      for (int j = sr.x; j < sr.y; j++) {
-        double2 x = xs[j];
-        double2 w = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
-        double2 qj[ND], dj[ND];
+      for (int s0 = sr.x; s0 < sr.y; s0 += 32) {
+        int m = min(32, sr.y - s0);
+        __syncwarp();
+        if (lane < m) {
+          int j = s0 + lane;
+          double2 x = xs[j];
+          double2 w = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
+          double2 pw = make_double2(1.0, 0.0);
+          for (int k = 0; k < P; k++) {
+            W[lane * P + k] = pw;
+            pw = cmul(pw, w);
+          }
 #pragma unroll
-        for (int d = 0; d < ND; d++) {
-          qj[d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
-          dj[d] = D.d ? D.d[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+          for (int d = 0; d < ND; d++) {
+            Q[lane * ND + d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+            Dd[lane * ND + d] =
+                D.d ? cscale(D.d[(size_t)j * D.ndc + D.d0 + d], ri) : make_double2(0, 0);
+          }
         }
+        __syncwarp();
 #pragma unroll
         for (int s = 0; s < 2; s++) {
           int k = lane + 32 * s;
           if (k >= P) break;
           if (k == 0) {
+            for (int j = 0; j < m; j++)
 #pragma unroll
-            for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], qj[d]);
+              for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], Q[j * ND + d]);
           } else {
-            double2 pw = cpow_int(w, k - 1);
-            double2 pn = cmul(pw, w);
-            double2 cq = make_double2(-pn.x / k, -pn.y / k);
-            double2 cd = make_double2(pw.x / r, pw.y / r);
+            double mik = -1.0 / k;
+            for (int j = 0; j < m; j++) {
+              double2 wk = W[j * P + k], wk1 = W[j * P + k - 1];
+              double2 cq = cscale(wk, mik);
 #pragma unroll
-            for (int d = 0; d < ND; d++) {
-              cfma(acc[s][d], qj[d], cq);
-              cfma(acc[s][d], dj[d], cd);
+              for (int d = 0; d < ND; d++) {
+                cfma(acc[s][d], Q[j * ND + d], cq);
+                cfma(acc[s][d], Dd[j * ND + d], wk1);
+              }
             }
           }
         }
@@ -294,59 +264,89 @@ __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
 
 // ---------------------------------------------------------------------------
 // step 2: P2L from list 4 (laprouts2d.f:501-690), z0 = x - c, w = r/z0:
-// l_0 += q log|z0| - d/z0,  l_n += -q w^n/n - (d/z0) w^n
+// l_0 += q log|z0| - d/z0,  l_n += -q w^n/n - (d/z0) w^n.
+// The sources of the (at most 5) list-4 boxes are taken 32 at a time from
+// their concatenation; each lane computes 1/z0, log|z0| and the powers of
+// its source once.
 // ---------------------------------------------------------------------------
 template <int ND>
-__global__ void __launch_bounds__(128) k_p2l(TV t, int first, int n, const double2* __restrict__ xs,
-                                             Dens D, int P, double2* __restrict__ lo) {
+__global__ void __launch_bounds__(64) k_p2l(TV t, int first, int n, const double2* __restrict__ xs,
+                                            Dens D, int P, double2* __restrict__ lo) {
+  extern __shared__ double2 smem[];
   WARP_LOOP(n) {
-    (void)wib;
+    double2* W = smem + (size_t)wib * (32 * P + 64 * ND + 32);
+    double2* Q = W + 32 * P;
+    double2* Dd = Q + 32 * ND;
+    double* LG = (double*)(Dd + 32 * ND);
     int b = first + bi;
     int n4 = t.nl4[b];
     if (n4 == 0 || !t.has_eval_pts(b)) continue;
     int lev = t.level[b];
     double r = t.boxsize[lev];
     double2 c = t.center[b];
+    int bs[5], be[5], tot = 0;
+    for (int e = 0; e < 5; e++) {
+      bs[e] = be[e] = 0;
+      if (e < n4) {
+        int2 sr = t.srng[t.l4[(size_t)MNLIST4 * b + e]];
+        bs[e] = sr.x;
+        be[e] = tot;  // offset of box e in the concatenation
+        tot += sr.y - sr.x;
+      }
+    }
     double2 acc[2][ND];
 #pragma unroll
     for (int s = 0; s < 2; s++)
 #pragma unroll
       for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
-    for (int e = 0; e < n4; e++) {
-      int jb = t.l4[(size_t)MNLIST4 * b + e];
-      int2 sr = t.srng[jb];
-      for (int j = sr.x; j < sr.y; j++) {
+    for (int g0 = 0; g0 < tot; g0 += 32) {
+      int m = min(32, tot - g0);
+      __syncwarp();
+      if (lane < m) {
+        int g = g0 + lane, e = 0;
+        while (e + 1 < n4 && g >= be[e + 1]) e++;
+        int j = bs[e] + (g - be[e]);
         double2 x = xs[j];
         double2 z0 = make_double2(x.x - c.x, x.y - c.y);
         double2 zi = crcp(z0);
         double2 w = make_double2(r * zi.x, r * zi.y);
-        double2 qj[ND], dj[ND];
+        double2 pw = make_double2(1.0, 0.0);
+        for (int k = 0; k < P; k++) {
+          W[lane * P + k] = pw;
+          pw = cmul(pw, w);
+        }
+        LG[lane] = log(hypot(z0.x, z0.y));
+        double2 mzi = cneg(zi);
 #pragma unroll
         for (int d = 0; d < ND; d++) {
-          qj[d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
-          dj[d] = D.d ? D.d[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+          Q[lane * ND + d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+          Dd[lane * ND + d] = D.d ? cmul(D.d[(size_t)j * D.ndc + D.d0 + d], mzi) : make_double2(0, 0);
         }
+      }
+      __syncwarp();
 #pragma unroll
-        for (int s = 0; s < 2; s++) {
-          int k = lane + 32 * s;
-          if (k >= P) break;
-          if (k == 0) {
-            double lg = log(hypot(z0.x, z0.y));
-            double2 mzi = cneg(zi);
+      for (int s = 0; s < 2; s++) {
+        int k = lane + 32 * s;
+        if (k >= P) break;
+        if (k == 0) {
+          for (int j = 0; j < m; j++) {
+            double lg = LG[j];
 #pragma unroll
             for (int d = 0; d < ND; d++) {
-              acc[s][d].x += qj[d].x * lg;
-              acc[s][d].y += qj[d].y * lg;
-              cfma(acc[s][d], dj[d], mzi);
+              double2 q = Q[j * ND + d];
+              acc[s][d].x += q.x * lg + Dd[j * ND + d].x;
+              acc[s][d].y += q.y * lg + Dd[j * ND + d].y;
             }
-          } else {
-            double2 wn = cpow_int(w, k);
-            double2 cq = make_double2(-wn.x / k, -wn.y / k);
-            double2 cd = cneg(cmul(zi, wn));
+          }
+        } else {
+          double mik = -1.0 / k;
+          for (int j = 0; j < m; j++) {
+            double2 wk = W[j * P + k];
+            double2 cq = cscale(wk, mik);
 #pragma unroll
             for (int d = 0; d < ND; d++) {
-              cfma(acc[s][d], qj[d], cq);
-              cfma(acc[s][d], dj[d], cd);
+              cfma(acc[s][d], Q[j * ND + d], cq);
+              cfma(acc[s][d], Dd[j * ND + d], wk);
             }
           }
         }
@@ -411,7 +411,8 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
       double2 z0 = make_double2(cj.x - cb.x, cj.y - cb.y);
       double2 zi = crcp(z0);
       double2 u = make_double2(zi.x * r, zi.y * r);
-      double lg = log(hypot(z0.x, z0.y));
+      double lg = lane == 0 ? log(hypot(z0.x, z0.y)) : 0.0;
+      lg = __shfl_sync(~0u, lg, 0);
       double2 ui[2];
       __syncwarp();
 #pragma unroll
@@ -858,12 +859,16 @@ template <int ND>
 void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int P,
                const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
                double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, double thresh,
-               cudaStream_t st, cudaEvent_t* ev) {
+               cudaStream_t st, cudaEvent_t* ev, const MixedData* M) {
   const double* binom = device_binomials();
   const int nb = T.nboxes;
   const int nl = T.nlevels;
   B2_CHECK(cudaEventRecord(ev[0], st));
-  k_p2m<ND><<<warp_grid(nb, 4), 128, 0, st>>>(tv, 0, nb, xs, D, P, mp);
+  size_t sm_p2m = sizeof(double2) * 2 * (32 * (size_t)P + 64 * ND);
+  size_t sm_p2l = sm_p2m + sizeof(double2) * 2 * 32;
+  B2_CHECK(cudaFuncSetAttribute(k_p2m<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2m));
+  B2_CHECK(cudaFuncSetAttribute(k_p2l<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2l));
+  k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, 0, nb, xs, D, P, mp);
   B2_LAUNCH_CHECK();
   B2_CHECK(cudaEventRecord(ev[1], st));
   size_t sm_t = sizeof(double2) * 4 * P * ND;
@@ -876,11 +881,14 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   B2_CHECK(cudaMemsetAsync(lo, 0, sizeof(double2) * (size_t)nb * P * ND, st));
   if (nl >= 2) {
     int f = T.lfirst[2], n = nb - f;
-    k_p2l<ND><<<warp_grid(n, 4), 128, 0, st>>>(tv, f, n, xs, D, P, lo);
+    k_p2l<ND><<<warp_grid(n, 2), 64, sm_p2l, st>>>(tv, f, n, xs, D, P, lo);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[3], st));
-  if (nl >= 2) {
+  if (nl >= 2 && M) {
+    int f = T.lfirst[2], n = nb - f;
+    lap_mixed_m2l(ND, tv, f, n, P, binom, *M, mp, lo, st);
+  } else if (nl >= 2) {
     int f = T.lfirst[2], n = nb - f;
     size_t sm = sizeof(double) * (P * P + 1) + sizeof(double2) * 4 * P * ND;
     if (sm > 48 * 1024)
@@ -898,6 +906,11 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   size_t sm_leaf = sizeof(LeafSmem<ND>) * 2;
   auto leaf = [&](int use_t, int ifl, const double2* xe, double2* po, double2* gr, double2* he) {
     if (ifl <= 0) return;
+    if (M) {
+      lap_mixed_leaf(ND, ifl, tv, nb, use_t, *M, xe, D.ndc, D.d0, P, mp, lo, thresh, a.ifnear, po,
+                     gr, he, st);
+      return;
+    }
     if (ifl == 1) {
       B2_CHECK(cudaFuncSetAttribute(k_leaf<ND, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_leaf));
       k_leaf<ND, 1><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
@@ -1031,18 +1044,20 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st) {
   mp.alloc((size_t)nb * P * chunk, st);
   lo.alloc((size_t)nb * P * chunk, st);
   double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  MixedData MD;
+  if (mixed)
+    lap_mixed_prepare(MD, xs.p, ns, xt.p, nt, fc ? qs.p : nullptr, fd ? ds.p : nullptr, ndc, T.cx0,
+                      T.cy0, P, st);
+  const MixedData* Mp = mixed ? &MD : nullptr;
   for (int d0 = 0; d0 < ndc;) {
     int left = ndc - d0;
     int ND = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
     Dens D{fc ? qs.p : nullptr, fd ? ds.p : nullptr, ndc, d0};
-    {
-      (void)mixed;
-      switch (ND) {
-        case 8: run_chunk<8>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
-        case 4: run_chunk<4>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
-        case 2: run_chunk<2>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
-        default: run_chunk<1>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
-      }
+    switch (ND) {
+      case 8: run_chunk<8>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
+      case 4: run_chunk<4>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
+      case 2: run_chunk<2>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
+      default: run_chunk<1>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
     }
     if (a.timeinfo) {
       B2_CHECK(cudaEventSynchronize(ev[6]));
