@@ -40,6 +40,8 @@ SIGNATURES = {
     "b2fmm_rfmm2d_dev": _LAP_HOST + [P] + _PGH + [P, P, P, P],
     "b2fmm_lap_direct_dev": [c_int, c_int, c_int64, P, P, P, P, c_int64, P, c_int, P, P, P,
                              c_double, P, P],
+    "b2fmm_lap_direct_noalloc_dev": [c_int, c_int, c_int64, P, P, P, P, c_int64, P, c_int, P, P,
+                                     P, c_double, P, P],
     "b2fmm_tree_build": [P, c_int64, P, c_int64, c_int, c_int, c_int, P, P, P],
     "b2fmm_tree_get": [P] * 23,
     "b2fmm_tree_free": [P],

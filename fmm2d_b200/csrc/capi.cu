@@ -295,6 +295,17 @@ void b2fmm_lap_direct_dev(int kind, int nd, int64_t ns, const double* sources,
   });
 }
 
+void b2fmm_lap_direct_noalloc_dev(int kind, int nd, int64_t ns, const double* sources,
+                                  const double* charge, const double* dipstr,
+                                  const double* dipvec, int64_t nt, const double* targ,
+                                  int ifpgh, double* pot, double* grad, double* hess,
+                                  double thresh, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_direct_device_noalloc(kind, nd, ns, sources, charge, dipstr, dipvec, nt, targ,
+                                     ifpgh, pot, grad, hess, thresh, (cudaStream_t)stream);
+  });
+}
+
 void* b2fmm_tree_build(const double* sources_dev, int64_t ns, const double* targ_dev, int64_t nt,
                        int idivflag, int ndiv, int nlmax, int* nlevels, int* nboxes, int* ier) {
   TreeHandle* h = nullptr;

@@ -18,7 +18,8 @@ enum {
   IER_NTERMS = 13,
   IER_BADARG = 100,  // invalid argument (sizes, flags)
   IER_CUDA = 101,    // CUDA runtime error
-  IER_TIMEOUT = 102  // a bounded device wait gave up
+  IER_TIMEOUT = 102,  // a bounded device wait gave up
+  IER_NOALLOC_TOO_LARGE = 103  // problem exceeds a fixed static scratch array
 };
 
 struct CudaError : public std::runtime_error {

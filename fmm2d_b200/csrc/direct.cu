@@ -6,6 +6,8 @@
 // second kernel adds in slice order, so the result is deterministic.
 #include "direct.cuh"
 
+#include <mutex>
+
 namespace b2 {
 
 namespace {
@@ -215,6 +217,118 @@ int lap_direct_device(int kind, int nd, long ns, const double* src, const double
   else
     run_direct<2>(nd, ns, src, charge, dipstr, dipvec, nt, trg, ifpgh, pot, grad, hess, thresh, st);
   return IER_OK;
+}
+
+}  // namespace b2
+
+namespace b2 {
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the direct sum.
+//
+// Some callers cannot allocate device memory while they call us: code that
+// runs inside another framework's memory budget (the whole device already
+// reserved by its allocator), latency-critical loops that must not hit a
+// synchronising or failing cudaMalloc, or embedded pipelines with a fixed
+// memory plan.  lap_direct_device_noalloc() therefore takes its per-slice
+// partial sums from the file-scope array below instead of the stream-ordered
+// pool.  The array is NOALLOC_SCRATCH_ELEMS complex doubles (4 MiB) and every
+// GPU that loads this library keeps it until the process exits.
+//
+// In host code `g_direct_scratch` only names a host-side stand-in, not the
+// device address, so the first call on each device looks the address up with
+// cudaGetSymbolAddress (with that device current) and caches it; make that
+// first call before any stream capture.  All calls share the one array and it
+// keeps the last call's contents: the first kernel writes every element the
+// second one reads, so nothing needs clearing, but calls that overlap on the
+// GPU (other streams, other host threads) race on it and must be serialised
+// by the caller.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t NOALLOC_SCRATCH_ELEMS = (size_t)1 << 18;  // 4 MiB of double2
+static __device__ __align__(256) double2 g_direct_scratch[NOALLOC_SCRATCH_ELEMS];
+
+std::mutex g_scratch_mu;
+double2* g_scratch_addr[128] = {nullptr};
+
+double2* scratch_address() {
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_direct_scratch);
+    if (e != cudaSuccess || !p)
+      throw CudaError(std::string("cudaGetSymbolAddress(g_direct_scratch): ") +
+                          cudaGetErrorString(e),
+                      IER_CUDA);
+    g_scratch_addr[dev] = (double2*)p;
+  }
+  return g_scratch_addr[dev];
+}
+
+template <int KIND>
+int run_direct_noalloc(int nd, long ns, const double* src, const double* charge,
+                       const double* dipstr, const double* dipvec, long nt, const double* trg,
+                       int ifpgh, double* pot, double* grad, double* hess, double thresh,
+                       cudaStream_t st) {
+  constexpr int NS = KIND == 0 ? 3 : 6;
+  if ((size_t)nt * NS > NOALLOC_SCRATCH_ELEMS) {
+    fprintf(stderr,
+            "fmm2d_b200: b2fmm_lap_direct_noalloc_dev: %ld targets need %zu scratch elements, "
+            "the static scratch holds %zu (at most %zu targets for this kernel)\n",
+            nt, (size_t)nt * NS, NOALLOC_SCRATCH_ELEMS, NOALLOC_SCRATCH_ELEMS / NS);
+    return IER_NOALLOC_TOO_LARGE;
+  }
+  double2* part = scratch_address();
+  int tb = ceil_div(nt, DT);
+  long fit = (long)(NOALLOC_SCRATCH_ELEMS / ((size_t)nt * NS));
+  int nslice = std::max(1, std::min(1024, (148 * 16) / std::max(tb, 1)));
+  nslice = (int)std::min<long>(nslice, fit);
+  long chunk = (ns + nslice - 1) / nslice;
+  chunk = ((chunk + DT - 1) / DT) * DT;
+  nslice = (int)std::max(1L, (ns + chunk - 1) / chunk);
+  int lt = (ifpgh >= 2 && (KIND != 0 ? charge != nullptr : true)) ? 1 : 0;
+  for (int d = 0; d < nd; d++) {
+    dim3 grid(tb, nslice);
+    k_direct<KIND><<<grid, DT, 0, st>>>(nd, d, ns, src, charge, dipstr, dipvec, nt, trg, ifpgh,
+                                        thresh * thresh, lt, chunk, part);
+    B2_LAUNCH_CHECK();
+    k_direct_reduce<KIND><<<ceil_div(nt, 256), 256, 0, st>>>(nd, d, nt, nslice, ifpgh, part, pot,
+                                                             grad, hess);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaStreamSynchronize(st));
+  return IER_OK;
+}
+
+}  // namespace
+
+int lap_direct_device_noalloc(int kind, int nd, long ns, const double* src, const double* charge,
+                              const double* dipstr, const double* dipvec, long nt,
+                              const double* trg, int ifpgh, double* pot, double* grad,
+                              double* hess, double thresh, cudaStream_t st) {
+  if (nd < 1 || ns < 0 || nt < 0 || ifpgh < 1 || ifpgh > 3 || kind < 0 || kind > 2)
+    return IER_BADARG;
+  if (nt == 0) return IER_OK;
+  if (ns == 0 || (!charge && !dipstr)) {
+    int cw = kind == 2 ? 1 : 2, gw = kind == 0 ? 1 : 2, hw = kind == 0 ? 1 : 3;
+    B2_CHECK(cudaMemsetAsync(pot, 0, sizeof(double) * cw * nd * nt, st));
+    if (ifpgh >= 2) B2_CHECK(cudaMemsetAsync(grad, 0, sizeof(double) * cw * gw * nd * nt, st));
+    if (ifpgh >= 3) B2_CHECK(cudaMemsetAsync(hess, 0, sizeof(double) * cw * hw * nd * nt, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    return IER_OK;
+  }
+  if (kind != 0 && dipstr && !dipvec) return IER_BADARG;
+  if (kind == 0)
+    return run_direct_noalloc<0>(nd, ns, src, charge, dipstr, dipvec, nt, trg, ifpgh, pot, grad,
+                                 hess, thresh, st);
+  if (kind == 1)
+    return run_direct_noalloc<1>(nd, ns, src, charge, dipstr, dipvec, nt, trg, ifpgh, pot, grad,
+                                 hess, thresh, st);
+  return run_direct_noalloc<2>(nd, ns, src, charge, dipstr, dipvec, nt, trg, ifpgh, pot, grad,
+                               hess, thresh, st);
 }
 
 }  // namespace b2

@@ -11,4 +11,12 @@ int lap_direct_device(int kind, int nd, long ns, const double* src, const double
                       int ifpgh, double* pot, double* grad, double* hess, double thresh,
                       cudaStream_t st);
 
+// Same sums with the partial-sum scratch taken from a static device array
+// instead of the memory pool (no device allocation at all); rejects target
+// counts whose partials do not fit (IER_NOALLOC_TOO_LARGE).
+int lap_direct_device_noalloc(int kind, int nd, long ns, const double* src, const double* charge,
+                              const double* dipstr, const double* dipvec, long nt,
+                              const double* trg, int ifpgh, double* pot, double* grad,
+                              double* hess, double thresh, cudaStream_t st);
+
 }  // namespace b2

@@ -14,7 +14,8 @@
  * the given CUDA stream (NULL = legacy default stream) and return after the
  * stream has finished the call.
  * ier: 0 ok, 4 device allocation failure, 13 expansion order too large,
- *      100 invalid argument, 101 CUDA error.
+ *      100 invalid argument, 101 CUDA error, 103 problem larger than a
+ *      fixed static scratch array.
  */
 #ifndef FMM2D_B200_H
 #define FMM2D_B200_H
@@ -130,6 +131,24 @@ void b2fmm_lap_direct_dev(int kind, int nd, int64_t ns, const double* sources,
                           const double* charge, const double* dipstr, const double* dipvec,
                           int64_t nt, const double* targ, int ifpgh, double* pot, double* grad,
                           double* hess, double thresh, void* stream, int* ier);
+
+/* Allocation-free variant of b2fmm_lap_direct_dev.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot allocate
+ * device memory during the call (a device already reserved by another
+ * framework's allocator, latency-critical loops, fixed memory plans): it
+ * calls no cudaMalloc/cudaFree or allocating library routine and takes its
+ * scratch from a 4 MiB static device array instead, which every GPU that
+ * loads the library holds until exit.  Limit: nt*3 (kind 0) or nt*6
+ * (kinds 1, 2) <= 262144, i.e. at most 87381 / 43690 targets per call;
+ * larger nt returns ier = 103 without computing.  The first call on a device
+ * looks up the array's device address, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race on it and
+ * must be serialised by the caller. */
+void b2fmm_lap_direct_noalloc_dev(int kind, int nd, int64_t ns, const double* sources,
+                                  const double* charge, const double* dipstr,
+                                  const double* dipvec, int64_t nt, const double* targ,
+                                  int ifpgh, double* pot, double* grad, double* hess,
+                                  double thresh, void* stream, int* ier);
 
 /* ------------------------------------------------------------------- tree */
 
