@@ -61,34 +61,50 @@ __device__ __forceinline__ void cfmaf_(float2& a, float2 b, float2 c) {
   a.y = fmaf(b.x, c.y, fmaf(b.y, c.x, a.y));
 }
 
+// Register-tiled FP32 M2L.  Per target box (one warp) and translation e:
+// y = G t_e with t_e(j) = h_j (-u)^j, u = 1/o, followed by L_i += u^i y_i
+// (L_0 += y_0 + t_0 log|z0|).  Lane = (row block rb of 4 rows, translation
+// group eg): the warp takes EG translations at a time; each lane multiplies
+// its 4 rows of G (a float4 per j from shared memory) with the 2*ND real
+// columns of its translation (one broadcast load per j), i.e. 8*ND FMAs per
+// two shared loads.  Partial locals of the EG groups are summed through
+// shared memory at the end of the box.
 template <int ND>
-__global__ void __launch_bounds__(128) k_m2l_f32(TV t, int first, int n, int P,
+__global__ void __launch_bounds__(128) k_m2l_f32(TV t, int first, int n, int P, int RB, int EG,
                                                  const double* __restrict__ binom,
                                                  const float2* __restrict__ utab_g,
                                                  const float* __restrict__ lgtab_g,
                                                  const double2* __restrict__ mp,
                                                  double2* __restrict__ lo) {
-  extern __shared__ float smf[];
-  float* G = smf;                                  // G[j * P + i]
-  float2* U = (float2*)(smf + ((P * P + 1) & ~1));  // U[o * P + k]
-  float* LG = (float*)(U + 49 * P);
-  float2* Tb = (float2*)(LG + 50);
-  for (int e = threadIdx.x; e < P * P; e += blockDim.x) {
-    int j = e / P, i = e % P;
-    float g;
-    if (i == 0)
-      g = (j == 0) ? 0.f : 1.f;
-    else if (j == 0)
-      g = -1.f / i;
-    else
-      g = (float)binom[(size_t)(i + j - 1) * BINOM_N + (j - 1)];
-    G[e] = g;
+  extern __shared__ float4 sm4[];
+  const int CW = 2 * ND;  // real columns per translation
+  // per-warp scratch first (16-byte aligned blocks), then the tables
+  const size_t warp_floats = (size_t)EG * P * CW * 2 + ((2 * EG + 3) & ~3);
+  float* wbase = (float*)sm4;
+  float4* G4 = (float4*)(wbase + 4 * warp_floats);  // [P][RB]: rows 4rb..4rb+3 of column j
+  float2* U = (float2*)(G4 + (size_t)P * RB);      // [49][P]
+  float* LG = (float*)(U + 49 * P);                // [49]
+  for (int e = threadIdx.x; e < P * RB * 4; e += blockDim.x) {
+    int j = e / (RB * 4), i = e % (RB * 4);
+    float g = 0.f;
+    if (i < P) {
+      if (i == 0)
+        g = (j == 0) ? 0.f : 1.f;
+      else if (j == 0)
+        g = -1.f / i;
+      else
+        g = (float)binom[(size_t)(i + j - 1) * BINOM_N + (j - 1)];
+    }
+    ((float*)G4)[e] = g;
   }
   for (int e = threadIdx.x; e < 49 * P; e += blockDim.x) U[e] = utab_g[e];
   for (int e = threadIdx.x; e < 49; e += blockDim.x) LG[e] = lgtab_g[e];
   __syncthreads();
   WARP_LOOP(n) {
-    float2* T = Tb + (size_t)wib * P * ND;
+    float* Tw = wbase + (size_t)wib * warp_floats;   // [EG][P][CW]
+    float* Rw = Tw + (size_t)EG * P * CW;            // [EG][P][CW] partial locals
+    int* OI = (int*)(Rw + (size_t)EG * P * CW);      // [EG] offsets
+    float* LGE = (float*)(OI + EG);                  // [EG] log|z0|
     int b = first + bi;
     int n2 = t.nl2[b];
     if (n2 == 0 || !t.has_eval_pts(b)) continue;
@@ -96,71 +112,118 @@ __global__ void __launch_bounds__(128) k_m2l_f32(TV t, int first, int n, int P,
     double2 cb = t.center[b];
     float lgr = (float)log(r);
     double rinv = 1.0 / r;
-    float2 acc[2][ND];
+    const int rb = lane % RB, eg = lane / RB;
+    const bool act = eg < EG;
+    float acc[4][2 * ND];
 #pragma unroll
-    for (int s = 0; s < 2; s++)
+    for (int q = 0; q < 4; q++)
 #pragma unroll
-      for (int d = 0; d < ND; d++) acc[s][d] = make_float2(0.f, 0.f);
-    for (int e = 0; e < n2; e++) {
-      int jb = t.l2[(size_t)MNLIST2 * b + e];
-      double2 cj = t.center[jb];
-      int ox = __double2int_rn((cj.x - cb.x) * rinv), oy = __double2int_rn((cj.y - cb.y) * rinv);
-      int oi = (ox + 3) * 7 + (oy + 3);
-      float lg = lgr + LG[oi];
-      const float2* Uo = U + oi * P;
+      for (int c = 0; c < 2 * ND; c++) acc[q][c] = 0.f;
+    for (int e0 = 0; e0 < n2; e0 += EG) {
+      int cnt = min(EG, n2 - e0);
       __syncwarp();
-#pragma unroll
-      for (int s = 0; s < 2; s++) {
-        int j = lane + 32 * s;
-        if (j >= P) break;
-        float2 sj = Uo[j];
-        if (j & 1) sj = make_float2(-sj.x, -sj.y);
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          double2 h = mp[((size_t)jb * P + j) * ND + d];
-          T[j * ND + d] = cmulf_(make_float2((float)h.x, (float)h.y), sj);
-        }
+      if (lane < cnt) {
+        int jb = t.l2[(size_t)MNLIST2 * b + e0 + lane];
+        double2 cj = t.center[jb];
+        int ox = __double2int_rn((cj.x - cb.x) * rinv), oy = __double2int_rn((cj.y - cb.y) * rinv);
+        int oi = (ox + 3) * 7 + (oy + 3);
+        OI[lane] = oi;
+        LGE[lane] = lgr + LG[oi];
       }
       __syncwarp();
+      // gather t_e(j) = h_j (-u)^j in FP32
+      for (int k = lane; k < cnt * P * ND; k += 32) {
+        int e = k / (P * ND), rem = k % (P * ND), j = rem / ND, d = rem % ND;
+        int jb = t.l2[(size_t)MNLIST2 * b + e0 + e];
+        float2 sj = U[OI[e] * P + j];
+        if (j & 1) sj = make_float2(-sj.x, -sj.y);
+        double2 h = mp[((size_t)jb * P + j) * ND + d];
+        float2 v = cmulf_(make_float2((float)h.x, (float)h.y), sj);
+        Tw[((size_t)e * P + j) * CW + 2 * d] = v.x;
+        Tw[((size_t)e * P + j) * CW + 2 * d + 1] = v.y;
+      }
+      __syncwarp();
+      if (act && eg < cnt) {
+        float y[4][2 * ND];
 #pragma unroll
-      for (int s = 0; s < 2; s++) {
-        int i = lane + 32 * s;
-        if (i >= P) break;
-        float2 y[ND];
+        for (int q = 0; q < 4; q++)
 #pragma unroll
-        for (int d = 0; d < ND; d++) y[d] = make_float2(0.f, 0.f);
+          for (int c = 0; c < 2 * ND; c++) y[q][c] = 0.f;
+        const float* Te = Tw + (size_t)eg * P * CW;
         for (int j = 0; j < P; j++) {
-          float g = G[j * P + i];
+          float4 g = G4[j * RB + rb];
+          float tv[2 * ND];
+          if (ND % 2 == 0) {
 #pragma unroll
-          for (int d = 0; d < ND; d++) {
-            float2 tj = T[j * ND + d];
-            y[d].x = fmaf(g, tj.x, y[d].x);
-            y[d].y = fmaf(g, tj.y, y[d].y);
+            for (int c = 0; c < ND / 2; c++) {
+              float4 v4 = ((const float4*)(Te + j * CW))[c];
+              tv[4 * c] = v4.x;
+              tv[4 * c + 1] = v4.y;
+              tv[4 * c + 2] = v4.z;
+              tv[4 * c + 3] = v4.w;
+            }
+          } else {
+#pragma unroll
+            for (int c = 0; c < ND; c++) {
+              float2 v2 = ((const float2*)(Te + j * CW))[c];
+              tv[2 * c] = v2.x;
+              tv[2 * c + 1] = v2.y;
+            }
+          }
+#pragma unroll
+          for (int c = 0; c < 2 * ND; c++) {
+            y[0][c] = fmaf(g.x, tv[c], y[0][c]);
+            y[1][c] = fmaf(g.y, tv[c], y[1][c]);
+            y[2][c] = fmaf(g.z, tv[c], y[2][c]);
+            y[3][c] = fmaf(g.w, tv[c], y[3][c]);
           }
         }
-        if (i == 0) {
+        const int oi = OI[eg];
+        const float lge = LGE[eg];
 #pragma unroll
-          for (int d = 0; d < ND; d++) {
-            acc[s][d].x += y[d].x + T[d].x * lg;
-            acc[s][d].y += y[d].y + T[d].y * lg;
+        for (int q = 0; q < 4; q++) {
+          int i = 4 * rb + q;
+          if (i >= P) break;
+          if (i == 0) {
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              acc[q][2 * d] += y[q][2 * d] + Te[2 * d] * lge;
+              acc[q][2 * d + 1] += y[q][2 * d + 1] + Te[2 * d + 1] * lge;
+            }
+          } else {
+            float2 ui = U[oi * P + i];
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              float yr = y[q][2 * d], yi = y[q][2 * d + 1];
+              acc[q][2 * d] += yr * ui.x - yi * ui.y;
+              acc[q][2 * d + 1] += yr * ui.y + yi * ui.x;
+            }
           }
-        } else {
-          float2 ui = Uo[i];
-#pragma unroll
-          for (int d = 0; d < ND; d++) cfmaf_(acc[s][d], y[d], ui);
         }
       }
     }
+    // sum the translation groups and add to the FP64 local expansion
+    __syncwarp();
+    if (act) {
 #pragma unroll
-    for (int s = 0; s < 2; s++) {
-      int i = lane + 32 * s;
-      if (i >= P) break;
+      for (int q = 0; q < 4; q++) {
+        int i = 4 * rb + q;
+        if (i >= P) break;
 #pragma unroll
-      for (int d = 0; d < ND; d++) {
-        size_t o = ((size_t)b * P + i) * ND + d;
-        double2 cur = lo[o];
-        lo[o] = make_double2(cur.x + acc[s][d].x, cur.y + acc[s][d].y);
+        for (int c = 0; c < 2 * ND; c++) Rw[((size_t)eg * P + i) * CW + c] = acc[q][c];
       }
+    }
+    __syncwarp();
+    for (int k = lane; k < P * ND; k += 32) {
+      int i = k / ND, d = k % ND;
+      float sr = 0.f, si = 0.f;
+      for (int g = 0; g < EG; g++) {
+        sr += Rw[((size_t)g * P + i) * CW + 2 * d];
+        si += Rw[((size_t)g * P + i) * CW + 2 * d + 1];
+      }
+      size_t o = ((size_t)b * P + i) * ND + d;
+      double2 cur = lo[o];
+      lo[o] = make_double2(cur.x + sr, cur.y + si);
     }
   }
 }
@@ -393,9 +456,13 @@ int grid_for(long nitems, int wpb) {
 template <int ND>
 void m2l_launch(const TV& t, int first, int n, int P, const double* binom, const MixedData& M,
                 const double2* mp, double2* lo, cudaStream_t st) {
-  size_t sm = sizeof(float) * (((P * P + 1) & ~1) + 2 * 49 * P + 50) + sizeof(float2) * 4 * P * ND;
+  const int RB = (P + 3) / 4, EG = 32 / RB;
+  const size_t warp_floats = (size_t)EG * P * 2 * ND * 2 + ((2 * EG + 3) & ~3);
+  size_t sm = sizeof(float) * 4 * warp_floats + sizeof(float4) * (size_t)P * RB +
+              sizeof(float2) * 49 * P + sizeof(float) * 52;
   B2_CHECK(cudaFuncSetAttribute(k_m2l_f32<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  k_m2l_f32<ND><<<grid_for(n, 4), 128, sm, st>>>(t, first, n, P, binom, M.utab.p, M.lgtab.p, mp, lo);
+  k_m2l_f32<ND><<<grid_for(n, 4), 128, sm, st>>>(t, first, n, P, RB, EG, binom, M.utab.p,
+                                                  M.lgtab.p, mp, lo);
   B2_LAUNCH_CHECK();
 }
 

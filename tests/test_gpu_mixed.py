@@ -1,0 +1,65 @@
+"""Mixed-precision Laplace path (FP32 near field and M2L, FP64 expansions)
+against the FP64 direct sum (error below eps) and against the oracle."""
+import numpy as np
+import pytest
+
+import fmm2d_b200 as fmm
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _gauss16(rng, n):
+    c = rng.uniform(0, 1, (2, 16))
+    sig = 10 ** rng.uniform(-4, -1, 16)
+    k = rng.integers(0, 16, n)
+    return c[:, k] + sig[k] * rng.normal(size=(2, n))
+
+
+@pytest.mark.parametrize("eps", [1e-3, 1e-6])
+def test_mixed_lfmm_vs_direct(gpu, oracle, eps):
+    rng = np.random.default_rng(21)
+    n = 40000
+    src = _gauss16(rng, n)
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    d = rng.normal(size=n) + 0j
+    ph = rng.uniform(0, 2 * np.pi, n)
+    v = np.stack([np.cos(ph), np.sin(ph)])
+    out = fmm.lfmm2d(eps=eps, sources=src, charges=q, dipstr=d, dipvec=v, pg=2,
+                     precision="mixed")
+    assert out.ier == 0
+    idx = rng.choice(n, 300, replace=False)
+    ex = oracle.l2ddir(src, src[:, idx], charges=q, dipstr=d, dipvec=v, ifpgh=2)
+    err = np.sqrt((np.linalg.norm(out.pot[idx] - ex["pottarg"][0]) ** 2 +
+                   np.linalg.norm(out.grad[:, idx] - ex["gradtarg"][0]) ** 2) /
+                  (np.linalg.norm(ex["pottarg"][0]) ** 2 + np.linalg.norm(ex["gradtarg"][0]) ** 2))
+    assert err < eps
+
+
+@pytest.mark.parametrize("pg", [1, 2, 3])
+def test_mixed_st_vs_oracle(gpu, oracle, pg):
+    rng = np.random.default_rng(30 + pg)
+    n, nt, nd = 6000, 2500, 2
+    src = rng.uniform(0, 1, (2, n))
+    trg = rng.uniform(0, 1, (2, nt))
+    q = rng.normal(size=(nd, n)) + 1j * rng.normal(size=(nd, n))
+    d = rng.normal(size=(nd, n)) + 1j * rng.normal(size=(nd, n))
+    v = rng.uniform(-1, 1, (nd, 2, n))
+    out = fmm.lfmm2d(eps=1e-6, sources=src, charges=q, dipstr=d, dipvec=v, targets=trg, pg=pg,
+                     pgt=pg, nd=nd, precision="mixed")
+    ref = oracle.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, targets=trg, ifpgh=pg,
+                        ifpghtarg=pg, nd=nd)
+    for k in ["pot", "grad", "hess"][:pg]:
+        assert rel_l2(getattr(out, k), ref[k]) < 1e-6, k
+        assert rel_l2(getattr(out, k + "targ"), ref[k + "targ"]) < 1e-6, k + "targ"
+
+
+def test_mixed_cfmm_nd3_and_auto(gpu, oracle):
+    rng = np.random.default_rng(8)
+    n = 8000
+    src = _gauss16(rng, n)
+    q = rng.normal(size=(3, n)) + 0j
+    out = fmm.cfmm2d(eps=1e-6, sources=src, charges=q, pg=2, nd=3)  # auto -> mixed
+    ref = oracle.cfmm2d(1e-6, src, charges=q, ifpgh=2, nd=3)
+    assert rel_l2(out.pot.real, ref["pot"].real) < 1e-6
+    assert rel_l2(out.grad, ref["grad"]) < 1e-6
