@@ -957,6 +957,889 @@ int run_cfmm(const CfmmArgs& A, Tree* keep_tree) {
   return 0;
 }
 
+// ===========================================================================
+// Helmholtz (src/helmholtz/): hfmm2d low-frequency path
+// ===========================================================================
+
+// H0^(1)(z), H1^(1)(z).  The oracle evaluates them independently of the
+// CUDA library: real arguments with libstdc++'s cylindrical Bessel functions,
+// complex arguments with the ascending series (DLMF 10.2.2, 10.8.1) in long
+// double for |z| <= 17 and the Hankel asymptotic expansion (DLMF 10.17.5)
+// beyond.  (The reference uses its own hank103, src/common/hank103.f.)
+typedef std::complex<long double> cld;
+
+void hankel01_series(cld z, cld& h0, cld& h1) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  const long double eg = 0.577215664901532860606512090082402431L;
+  cld q = -(z * z) / 4.0L;
+  cld t0 = 1.0L, t1 = 1.0L;  // (-z^2/4)^k / (k!)^2 and / (k!(k+1)!)
+  cld j0 = 0.0L, j1s = 0.0L, y0s = 0.0L, y1s = 0.0L;
+  long double hk = 0.0L;  // harmonic number H_k
+  for (int k = 0; k < 200; k++) {
+    if (k > 0) {
+      t0 *= q / ((long double)k * k);
+      t1 *= q / ((long double)k * (k + 1));
+      hk += 1.0L / k;
+    }
+    j0 += t0;
+    j1s += t1;
+    y0s += hk * t0;                               // sum H_k (-z^2/4)^k/(k!)^2
+    y1s += (2 * (hk - eg) + 1.0L / (k + 1)) * t1;  // psi(k+1)+psi(k+2)
+    if (k > 5 && std::abs(t0) < 1e-30L * std::abs(j0) && std::abs(t1) < 1e-30L) break;
+  }
+  cld lz = std::log(z / 2.0L);
+  cld j1 = (z / 2.0L) * j1s;
+  cld y0 = (2.0L / pi) * (lz + eg) * j0 - (2.0L / pi) * y0s;
+  cld y1 = -2.0L / (pi * z) + (2.0L / pi) * lz * j1 - (z / (2.0L * pi)) * y1s;
+  cld I(0.0L, 1.0L);
+  h0 = j0 + I * y0;
+  h1 = j1 + I * y1;
+}
+
+void hankel01_asym(cld z, cld& h0, cld& h1) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  cld I(0.0L, 1.0L);
+  cld pre = std::sqrt(2.0L / (pi * z));
+  cld out[2];
+  for (int nu = 0; nu <= 1; nu++) {
+    long double m = 4.0L * nu * nu;
+    cld sum = 1.0L, term = 1.0L;
+    long double last = 1e300L;
+    for (int k = 1; k < 200; k++) {
+      long double a = (m - (2.0L * k - 1) * (2.0L * k - 1)) / (k * 8.0L);
+      cld nt = term * (I * a / z);
+      if (std::abs(nt) > last) break;  // optimal truncation
+      last = std::abs(nt);
+      term = nt;
+      sum += term;
+      if (last < 1e-21L) break;
+    }
+    out[nu] = pre * std::exp(I * (z - nu * pi / 2.0L - pi / 4.0L)) * sum;
+  }
+  h0 = out[0];
+  h1 = out[1];
+}
+
+void hankel01(cdbl z, cdbl& h0, cdbl& h1) {
+  if (z.imag() == 0.0 && z.real() > 0.0) {
+    double x = z.real();
+    h0 = cdbl(std::cyl_bessel_j(0.0, x), std::cyl_neumann(0.0, x));
+    h1 = cdbl(std::cyl_bessel_j(1.0, x), std::cyl_neumann(1.0, x));
+    return;
+  }
+  cld zl((long double)z.real(), (long double)z.imag()), a, b;
+  if (std::abs(zl) <= 17.0L)
+    hankel01_series(zl, a, b);
+  else
+    hankel01_asym(zl, a, b);
+  h0 = cdbl((double)a.real(), (double)a.imag());
+  h1 = cdbl((double)b.real(), (double)b.imag());
+}
+
+// h2dall (src/helmholtz/h2dcommon.f:71-178): hvec(n) = H_n(z) rscale^n,
+// n = 0..nterms, by upward recurrence from H0, H1 (zero for |z| < 1e-200).
+void h2dall(int nterms, cdbl z, double rscale, cdbl* hv) {
+  if (std::abs(z) < 1e-200) {
+    for (int i = 0; i <= nterms; i++) hv[i] = 0.0;
+    return;
+  }
+  cdbl h0, h1;
+  hankel01(z, h0, h1);
+  hv[0] = h0;
+  if (nterms >= 1) hv[1] = h1 * rscale;
+  double s2 = rscale * rscale;
+  cdbl zinv = rscale / z;
+  for (int i = 1; i < nterms; i++) hv[i + 1] = (zinv * (2.0 * i)) * hv[i] - s2 * hv[i - 1];
+}
+
+// jbessel2d (src/common/cdjseval2d.f:5-204): fjs(n) = J_n(z) / rscale^n,
+// n = 0..nterms, by Miller's backward recurrence started where the forward
+// recurrence exceeds 1e20, normalised with exp(-/+ i z) = sum (-/+i)^n ...
+void jbessel2d(int nterms, cdbl z, double rscale, cdbl* fjs) {
+  if (std::abs(z) < 1e-200) {
+    fjs[0] = 1.0;
+    for (int i = 1; i <= nterms; i++) fjs[i] = 0.0;
+    return;
+  }
+  const double upb2 = 1e40, upb2inv = 1e-40;
+  cdbl zinv = 1.0 / z;
+  cdbl fn = 1.0, fnm1 = 0.0;
+  int ntop = nterms + 10000;
+  for (int i = nterms; i <= nterms + 10000; i++) {
+    cdbl t = (2.0 * i) * zinv * fn - fnm1;
+    if (std::norm(t) > upb2) {
+      ntop = i + 1;
+      break;
+    }
+    fnm1 = fn;
+    fn = t;
+  }
+  std::vector<cdbl> f(ntop + 1, 0.0);
+  std::vector<char> isc(ntop + 1, 0);
+  f[ntop] = 0.0;
+  f[ntop - 1] = 1.0;
+  for (int i = ntop - 1; i >= 1; i--) {
+    cdbl t = (2.0 * i) * zinv * f[i] - f[i + 1];
+    f[i - 1] = t;
+    if (std::norm(t) > upb2) {
+      f[i] *= upb2inv;
+      f[i - 1] *= upb2inv;
+      isc[i] = 1;
+    }
+  }
+  double sinv = 1.0 / rscale, sctot = 1.0;
+  for (int i = 1; i <= ntop; i++) {
+    sctot *= sinv;
+    if (isc[i - 1]) sctot *= upb2inv;
+    f[i] *= sctot;
+  }
+  cdbl I(0, 1);
+  cdbl zmul = z.imag() < 0 ? I : -I;
+  cdbl zsn = std::pow(zmul, ntop % 4);
+  cdbl zmi = 1.0 / zmul;
+  cdbl psi = 0.0;
+  for (int i = ntop; i >= 1; i--) {
+    psi = rscale * psi + f[i] * zsn;
+    zsn *= zmi;
+  }
+  psi = 2.0 * psi * rscale + f[0];
+  cdbl zs = (z.imag() < 0 ? std::exp(I * z) : std::exp(-I * z)) / psi;
+  for (int i = 0; i <= nterms; i++) fjs[i] = f[i] * zs;
+}
+
+// h2dterms (src/helmholtz/h2dterms.f:35-97): first j with
+// (|J_j H_j| + |J_(j-1) H_(j-1)|) |H_0| < eps (|J_0 H_0| + |J_1 H_1|).
+int h2dterms(double bsize, cdbl zk, double eps, int* ier) {
+  const double pi2 = 8 * std::atan(1.0);
+  cdbl z1 = (zk * bsize) * 1.5;
+  double rscale = 1.0;
+  if (std::abs(zk * bsize) < pi2) rscale = std::abs(zk * bsize);
+  const int nt = 2000;
+  std::vector<cdbl> hf(nt + 1), jf(nt + 1);
+  h2dall(nt, z1, rscale, hf.data());
+  cdbl z2 = (zk * bsize) * (std::sqrt(2.0) / 2.0);
+  jbessel2d(nt, z2, rscale, jf.data());
+  double x0 = std::abs(jf[0] * hf[0]) + std::abs(jf[1] * hf[1]);
+  for (int j = 2; j <= nt; j++) {
+    double x1 = std::abs(jf[j] * hf[j]), x2 = std::abs(jf[j - 1] * hf[j - 1]);
+    if ((x1 + x2) * std::abs(hf[0]) < eps * x0) return j + 1;
+  }
+  *ier = 13;
+  return 10001;
+}
+
+int helm_ndiv(double eps, long ns, long nt) { return lap_ndiv(eps, ns, nt); }  // hndiv2d.f
+
+inline void polar(double x, double y, double& r, double& th) {  // h2cart2polar
+  r = std::sqrt(x * x + y * y);
+  th = (x == 0 && y == 0) ? 0.0 : std::atan2(y, x);
+}
+
+// Expansions are (nd, -p:p): element (d, n) at [(n + p) * nd + d].
+struct HExp {
+  int p, nd;
+  cdbl* a;
+  cdbl& at(int n, int d) { return a[(size_t)(n + p) * nd + d]; }
+};
+
+// ctompole / dtompole (helmrouts2d.f:1383-1492): add one source's charge and
+// dipole terms given jv(n) = Z_n (J or H, scaled) and zmul = exp(-i theta).
+void add_src_terms(int nd, cdbl zk, double rs, cdbl zmul, const cdbl* jv, const cdbl* q,
+                   const cdbl* dst, const double* dv, int ldv, HExp E) {
+  cdbl I(0, 1), zinv = std::conj(zmul);
+  if (q) {
+    for (int d = 0; d < nd; d++) E.at(0, d) += q[d] * jv[0];
+    cdbl t1 = zmul, t2 = -zinv;
+    for (int n = 1; n <= E.p; n++) {
+      for (int d = 0; d < nd; d++) {
+        E.at(n, d) += jv[n] * t1 * q[d];
+        E.at(-n, d) += jv[n] * t2 * q[d];
+      }
+      t1 *= zmul;
+      t2 = -t2 * zinv;
+    }
+  }
+  if (dst) {
+    cdbl z3 = zinv / rs, z4 = zmul * rs, z5 = zmul / rs, z6 = zinv * rs;
+    for (int d = 0; d < nd; d++) {
+      double v1 = dv[d], v2 = dv[ldv + d];
+      E.at(0, d) -= dst[d] * jv[1] * zk / 2.0 * rs * ((zmul + zinv) * v1 + (zmul - zinv) * I * v2);
+    }
+    cdbl t1 = -zmul * zk / 2.0, t2 = zinv * zk / 2.0;
+    for (int n = 1; n <= E.p; n++) {
+      for (int d = 0; d < nd; d++) {
+        double v1 = dv[d], v2 = dv[ldv + d];
+        cdbl a7 = z3 * cdbl(-v1, v2), a8 = z4 * cdbl(v1, v2), a9 = z5 * cdbl(-v1, -v2),
+             a10 = z6 * cdbl(v1, -v2);
+        E.at(n, d) += (jv[n - 1] * a7 + jv[n + 1] * a8) * t1 * dst[d];
+        E.at(-n, d) += (jv[n - 1] * a9 + jv[n + 1] * a10) * t2 * dst[d];
+      }
+      t1 *= zmul;
+      t2 = -t2 * zinv;
+    }
+  }
+}
+
+// mk_mpoleg (helmrouts2d.f): derivative expansions (x and y) of order p+1.
+void mk_grad_exp(int nd, cdbl zk, double rs, HExp M, HExp X, HExp Y) {
+  cdbl I(0, 1);
+  cdbl s1 = zk / 2.0 / rs, s2 = zk / 2.0 * rs, s3 = zk / 2.0 / rs * I, s4 = zk / 2.0 * rs * I;
+  for (int n = -X.p; n <= X.p; n++)
+    for (int d = 0; d < nd; d++) X.at(n, d) = Y.at(n, d) = 0.0;
+  for (int d = 0; d < nd; d++) {
+    X.at(-1, d) += s1 * M.at(0, d);
+    Y.at(-1, d) += s3 * M.at(0, d);
+    X.at(1, d) -= s1 * M.at(0, d);
+    Y.at(1, d) += s3 * M.at(0, d);
+  }
+  for (int i = 1; i <= M.p; i++)
+    for (int d = 0; d < nd; d++) {
+      X.at(i - 1, d) += s2 * M.at(i, d);
+      Y.at(i - 1, d) += s4 * M.at(i, d);
+      X.at(i + 1, d) -= s1 * M.at(i, d);
+      Y.at(i + 1, d) += s3 * M.at(i, d);
+    }
+  for (int i = -M.p; i <= -1; i++)
+    for (int d = 0; d < nd; d++) {
+      X.at(i - 1, d) += s1 * M.at(i, d);
+      Y.at(i - 1, d) += s3 * M.at(i, d);
+      X.at(i + 1, d) -= s2 * M.at(i, d);
+      Y.at(i + 1, d) += s4 * M.at(i, d);
+    }
+}
+
+// mk_mpoleh: second derivatives (xx from x, xy from x, yy from y), order p+2.
+void mk_hess_exp(int nd, cdbl zk, double rs, HExp X, HExp Y, HExp XX, HExp XY, HExp YY) {
+  cdbl I(0, 1);
+  cdbl s1 = zk / 2.0 / rs, s2 = zk / 2.0 * rs, s3 = zk / 2.0 / rs * I, s4 = zk / 2.0 * rs * I;
+  for (int n = -XX.p; n <= XX.p; n++)
+    for (int d = 0; d < nd; d++) XX.at(n, d) = XY.at(n, d) = YY.at(n, d) = 0.0;
+  for (int d = 0; d < nd; d++) {
+    XX.at(-1, d) += s1 * X.at(0, d);
+    XY.at(-1, d) += s3 * X.at(0, d);
+    YY.at(-1, d) += s3 * Y.at(0, d);
+    XX.at(1, d) -= s1 * X.at(0, d);
+    XY.at(1, d) += s3 * X.at(0, d);
+    YY.at(1, d) += s3 * Y.at(0, d);
+  }
+  for (int i = 1; i <= X.p; i++)
+    for (int d = 0; d < nd; d++) {
+      XX.at(i - 1, d) += s2 * X.at(i, d);
+      XY.at(i - 1, d) += s4 * X.at(i, d);
+      YY.at(i - 1, d) += s4 * Y.at(i, d);
+      XX.at(i + 1, d) -= s1 * X.at(i, d);
+      XY.at(i + 1, d) += s3 * X.at(i, d);
+      YY.at(i + 1, d) += s3 * Y.at(i, d);
+    }
+  for (int i = -X.p; i <= -1; i++)
+    for (int d = 0; d < nd; d++) {
+      XX.at(i - 1, d) += s1 * X.at(i, d);
+      XY.at(i - 1, d) += s3 * X.at(i, d);
+      YY.at(i - 1, d) += s3 * Y.at(i, d);
+      XX.at(i + 1, d) -= s2 * X.at(i, d);
+      XY.at(i + 1, d) += s4 * X.at(i, d);
+      YY.at(i + 1, d) += s4 * Y.at(i, d);
+    }
+}
+
+// mpole_evalp: sum_n E(n) mt(n) with mt(n) = (i/4) Z_|n| exp(i n theta) (-1)^... 
+void eval_exp(int nd, HExp E, const cdbl* mt, int mtoff, cdbl* out) {
+  cdbl I4(0, 0.25);
+  for (int d = 0; d < nd; d++) out[d] += mt[mtoff] * E.at(0, d) * I4;
+  for (int n = 1; n <= E.p; n++)
+    for (int d = 0; d < nd; d++) out[d] += E.at(n, d) * mt[mtoff + n] + E.at(-n, d) * mt[mtoff - n];
+}
+
+// table mt(-m..m): mt(0) = Z_0, mt(+-n) = (i/4) Z_n zmul^n, (-i/4)(-zinv)^.. as mpole_evalp
+void make_mt(int m, cdbl zmul, const cdbl* zv, std::vector<cdbl>& mt) {
+  cdbl I4(0, 0.25);
+  mt.assign(2 * m + 1, 0.0);
+  mt[m] = zv[0];
+  cdbl t1 = zmul * I4, t2 = -std::conj(zmul) * I4;
+  for (int j = 1; j <= m; j++) {
+    mt[m + j] = t1 * zv[j];
+    mt[m - j] = t2 * zv[j];
+    t1 *= zmul;
+    t2 = -t2 * std::conj(zmul);
+  }
+}
+
+// Evaluate an expansion (multipole with H, local with J) at points with
+// derivatives (h2dmpeval*, h2dtaeval*; helmrouts2d.f:274-966).
+void helm_eval(int nd, cdbl zk, double rs, const double* c, HExp E, bool mpole, const double* xy,
+               int n, int ifpgh, cdbl* pot, cdbl* grad, cdbl* hess) {
+  int p = E.p;
+  double rsg = mpole ? rs : 1.0 / rs;  // mk_mpoleg scale: rscale for H, 1/rscale for J
+  std::vector<cdbl> bx((2 * p + 3) * nd), by((2 * p + 3) * nd), bxx((2 * p + 5) * nd),
+      bxy((2 * p + 5) * nd), byy((2 * p + 5) * nd);
+  HExp X{p + 1, nd, bx.data()}, Y{p + 1, nd, by.data()};
+  HExp XX{p + 2, nd, bxx.data()}, XY{p + 2, nd, bxy.data()}, YY{p + 2, nd, byy.data()};
+  if (ifpgh >= 2) mk_grad_exp(nd, zk, rsg, E, X, Y);
+  if (ifpgh >= 3) mk_hess_exp(nd, zk, rsg, X, Y, XX, XY, YY);
+  std::vector<cdbl> zv(p + 12), mt;
+  cdbl I(0, 1);
+  for (int k = 0; k < n; k++) {
+    double r, th;
+    polar(xy[2 * k] - c[0], xy[2 * k + 1] - c[1], r, th);
+    cdbl z = zk * r;
+    if (mpole)
+      h2dall(p + 3, z, rs, zv.data());
+    else
+      jbessel2d(p + 3, z, rs, zv.data());
+    cdbl zmul = std::exp(I * th);
+    make_mt(p + 2, zmul, zv.data(), mt);
+    eval_exp(nd, E, mt.data(), p + 2, pot + (size_t)k * nd);
+    if (ifpgh >= 2) {
+      std::vector<cdbl> g(nd, 0.0), h(nd, 0.0);
+      eval_exp(nd, X, mt.data(), p + 2, g.data());
+      eval_exp(nd, Y, mt.data(), p + 2, h.data());
+      for (int d = 0; d < nd; d++) {
+        grad[((size_t)k * 2 + 0) * nd + d] += g[d];
+        grad[((size_t)k * 2 + 1) * nd + d] += h[d];
+      }
+    }
+    if (ifpgh >= 3) {
+      std::vector<cdbl> a(nd, 0.0), b(nd, 0.0), e(nd, 0.0);
+      eval_exp(nd, XX, mt.data(), p + 2, a.data());
+      eval_exp(nd, XY, mt.data(), p + 2, b.data());
+      eval_exp(nd, YY, mt.data(), p + 2, e.data());
+      for (int d = 0; d < nd; d++) {
+        hess[((size_t)k * 3 + 0) * nd + d] += a[d];
+        hess[((size_t)k * 3 + 1) * nd + d] += b[d];
+        hess[((size_t)k * 3 + 2) * nd + d] += e[d];
+      }
+    }
+  }
+}
+
+// Form an expansion from sources: multipole (J, h2dformmp*) or local
+// (H, h2dformta*) about c.
+void helm_form(int nd, cdbl zk, double rs, const double* src, int ns, const cdbl* q,
+               const cdbl* dst, const double* dv, const double* c, HExp E, bool mpole) {
+  cdbl I(0, 1);
+  std::vector<cdbl> zv(E.p + 12);
+  for (int j = 0; j < ns; j++) {
+    double r, th;
+    polar(src[2 * j] - c[0], src[2 * j + 1] - c[1], r, th);
+    cdbl z = zk * r;
+    if (mpole)
+      jbessel2d(E.p + 1, z, rs, zv.data());
+    else
+      h2dall(E.p + 2, z, rs, zv.data());
+    cdbl zmul = std::exp(-I * th);
+    add_src_terms(nd, zk, mpole ? rs : 1.0 / rs, zmul, zv.data(), q ? q + (size_t)j * nd : nullptr,
+                  dst ? dst + (size_t)j * nd : nullptr, dv ? dv + (size_t)j * 2 * nd : nullptr, nd,
+                  E);
+  }
+}
+
+// Translation kernels table ztab(-m..m) = Z_|j| * exp(-i j theta) with the
+// (-1)^j sign on negative indices (h2dmpmp / h2dlocloc / h2dmploc).
+void shift_table(int m, cdbl zmul, const cdbl* zv, std::vector<cdbl>& t) {
+  t.assign(2 * m + 1, 0.0);
+  t[m] = zv[0];
+  cdbl a = zmul, b = -std::conj(zmul);
+  for (int j = 1; j <= m; j++) {
+    t[m + j] = a * zv[j];
+    t[m - j] = b * zv[j];
+    a *= zmul;
+    b = -b * std::conj(zmul);
+  }
+}
+
+// h2dmpmp (helmrouts2d.f:967-1095)
+void h2dmpmp(int nd, cdbl zk, double rs1, const double* c1, HExp H1, double rs2, const double* c2,
+             HExp H2) {
+  const double pi = 4 * std::atan(1.0);
+  int p1 = H1.p, p2 = H2.p, nt = p1 + p2;
+  double r, th;
+  polar(c2[0] - c1[0], c2[1] - c1[1], r, th);
+  th -= pi;
+  std::vector<cdbl> jv(nt + 12), T;
+  jbessel2d(nt + 3, zk * r, rs1, jv.data());
+  cdbl I(0, 1);
+  shift_table(nt, std::exp(-I * th), jv.data(), T);
+  auto J = [&](int j) { return T[nt + j]; };
+  for (int d = 0; d < nd; d++) H2.at(0, d) += H1.at(0, d) * J(0);
+  double rsj2 = rs1 * rs1, rsj = rsj2;
+  for (int j = 1; j <= p1; j++) {
+    for (int d = 0; d < nd; d++) {
+      H2.at(0, d) += (H1.at(j, d) * J(-j)) * rsj;
+      H2.at(0, d) += (H1.at(-j, d) * J(j)) * rsj;
+    }
+    rsj *= rsj2;
+  }
+  double rsi5 = rs1 / rs2;
+  for (int i = 1; i <= p2; i++) {
+    for (int d = 0; d < nd; d++) {
+      H2.at(i, d) += H1.at(0, d) * J(i) * rsi5;
+      H2.at(-i, d) += H1.at(0, d) * J(-i) * rsi5;
+    }
+    rsi5 *= rs1 / rs2;
+  }
+  rsi5 = rs1 / rs2;
+  for (int i = 1; i <= p2; i++) {
+    rsj = rsj2;
+    for (int j = 1; j <= std::min(p1, i); j++) {
+      double fs3 = rsi5 * rsj;
+      for (int d = 0; d < nd; d++) {
+        H2.at(i, d) += (H1.at(j, d) * J(i - j)) * rsi5;
+        H2.at(i, d) += (H1.at(-j, d) * J(i + j)) * fs3;
+        H2.at(-i, d) += (H1.at(j, d) * J(-i - j)) * fs3;
+        H2.at(-i, d) += (H1.at(-j, d) * J(-i + j)) * rsi5;
+      }
+      rsj *= rsj2;
+    }
+    rsj = std::pow(rsj2, i + 1);
+    double fs2 = rsi5 * rsj2, fs3 = rsi5 * rsj;
+    for (int j = i + 1; j <= p1; j++) {
+      for (int d = 0; d < nd; d++) {
+        H2.at(i, d) += (H1.at(j, d) * J(i - j)) * fs2;
+        H2.at(i, d) += (H1.at(-j, d) * J(i + j)) * fs3;
+        H2.at(-i, d) += (H1.at(j, d) * J(-i - j)) * fs3;
+        H2.at(-i, d) += (H1.at(-j, d) * J(-i + j)) * fs2;
+      }
+      fs3 *= rsj2;
+      fs2 *= rsj2;
+    }
+    rsi5 *= rs1 / rs2;
+  }
+}
+
+// h2dlocloc (helmrouts2d.f:1096-1220)
+void h2dlocloc(int nd, cdbl zk, double rs1, const double* c1, HExp J1, double rs2,
+               const double* c2, HExp J2) {
+  const double pi = 4 * std::atan(1.0);
+  int p1 = J1.p, p2 = J2.p, nt = p1 + p2;
+  double r, th;
+  polar(c2[0] - c1[0], c2[1] - c1[1], r, th);
+  th -= pi;
+  std::vector<cdbl> jv(nt + 12), T;
+  jbessel2d(nt + 3, zk * r, rs1, jv.data());
+  cdbl I(0, 1);
+  shift_table(nt, std::exp(-I * th), jv.data(), T);
+  auto J = [&](int j) { return T[nt + j]; };
+  for (int d = 0; d < nd; d++) J2.at(0, d) += J1.at(0, d) * J(0);
+  for (int j = 1; j <= p1; j++)
+    for (int d = 0; d < nd; d++) {
+      J2.at(0, d) += J1.at(j, d) * J(-j);
+      J2.at(0, d) += J1.at(-j, d) * J(j);
+    }
+  double rsi = rs1, rsi7 = rs2;
+  for (int i = 1; i <= p2; i++) {
+    for (int d = 0; d < nd; d++) {
+      J2.at(i, d) += J1.at(0, d) * J(i) * rsi7 * rsi;
+      J2.at(-i, d) += J1.at(0, d) * J(-i) * rsi7 * rsi;
+    }
+    rsi *= rs1;
+    rsi7 *= rs2;
+  }
+  rsi = rs1;
+  rsi7 = rs2;
+  double rsi5 = rs2 / rs1;
+  for (int i = 1; i <= p2; i++) {
+    double fs2 = rsi5;
+    if (p1 <= i) fs2 = fs2 * std::pow(rs1, 2 * (i - p1));
+    for (int j = std::min(p1, i); j >= 1; j--) {
+      for (int d = 0; d < nd; d++) {
+        J2.at(i, d) += (J1.at(j, d) * J(i - j)) * fs2;
+        J2.at(i, d) += (J1.at(-j, d) * J(i + j)) * rsi7 * rsi;
+        J2.at(-i, d) += (J1.at(j, d) * J(-i - j)) * rsi7 * rsi;
+        J2.at(-i, d) += (J1.at(-j, d) * J(-i + j)) * fs2;
+      }
+      fs2 *= rs1 * rs1;
+    }
+    for (int j = i + 1; j <= p1; j++) {
+      for (int d = 0; d < nd; d++) {
+        J2.at(i, d) += (J1.at(j, d) * J(i - j)) * rsi5;
+        J2.at(i, d) += (J1.at(-j, d) * J(i + j)) * rsi7 * rsi;
+        J2.at(-i, d) += (J1.at(j, d) * J(-i - j)) * rsi7 * rsi;
+        J2.at(-i, d) += (J1.at(-j, d) * J(-i + j)) * rsi5;
+      }
+    }
+    rsi *= rs1;
+    rsi7 *= rs2;
+    rsi5 *= rs2 / rs1;
+  }
+}
+
+// h2dmploc (helmrouts2d.f:1221-1382)
+void h2dmploc(int nd, cdbl zk, double rs1, const double* c1, HExp H, double rs2,
+              const double* c2, HExp L) {
+  const double pi = 4 * std::atan(1.0);
+  int p1 = H.p, p2 = L.p, nt = p1 + p2;
+  double r, th;
+  polar(c2[0] - c1[0], c2[1] - c1[1], r, th);
+  th -= pi;
+  std::vector<cdbl> hv(nt + 12), T;
+  h2dall(nt + 1, zk * r, rs1, hv.data());
+  cdbl I(0, 1);
+  shift_table(nt, std::exp(-I * th), hv.data(), T);
+  auto Hh = [&](int j) { return T[nt + j]; };
+  std::vector<cdbl> tmp((2 * p2 + 1) * nd, 0.0);
+  HExp Tm{p2, nd, tmp.data()};
+  std::vector<double> rs2pow(p2 + 1);
+  double rfac = rs1 * rs1;
+  if (p2 >= 1) rs2pow[1] = rfac;
+  for (int i = 2; i <= p2; i++) rs2pow[i] = rs2pow[i - 1] * rfac;
+  for (int d = 0; d < nd; d++) Tm.at(0, d) += H.at(0, d) * Hh(0);
+  for (int j = 1; j <= p1; j++)
+    for (int d = 0; d < nd; d++) {
+      Tm.at(0, d) += H.at(j, d) * Hh(-j);
+      Tm.at(0, d) += H.at(-j, d) * Hh(j);
+    }
+  for (int i = 1; i <= p2; i++) {
+    for (int d = 0; d < nd; d++) {
+      Tm.at(i, d) += H.at(0, d) * Hh(i);
+      Tm.at(-i, d) += H.at(0, d) * Hh(-i);
+    }
+    for (int j = 1; j <= std::min(p1, i); j++)
+      for (int d = 0; d < nd; d++) {
+        Tm.at(i, d) += (H.at(j, d) * Hh(i - j)) * rs2pow[j];
+        Tm.at(i, d) += H.at(-j, d) * Hh(i + j);
+        Tm.at(-i, d) += H.at(j, d) * Hh(-i - j);
+        Tm.at(-i, d) += (H.at(-j, d) * Hh(-i + j)) * rs2pow[j];
+      }
+    for (int j = i + 1; j <= p1; j++)
+      for (int d = 0; d < nd; d++) {
+        Tm.at(i, d) += (H.at(j, d) * Hh(i - j)) * rs2pow[i];
+        Tm.at(i, d) += H.at(-j, d) * Hh(i + j);
+        Tm.at(-i, d) += H.at(j, d) * Hh(-i - j);
+        Tm.at(-i, d) += (H.at(-j, d) * Hh(-i + j)) * rs2pow[i];
+      }
+  }
+  double f = rs2 / rs1, rs12 = f;
+  for (int d = 0; d < nd; d++) L.at(0, d) += Tm.at(0, d);
+  for (int i = 1; i <= p2; i++) {
+    for (int d = 0; d < nd; d++) {
+      L.at(i, d) += Tm.at(i, d) * rs12;
+      L.at(-i, d) += Tm.at(-i, d) * rs12;
+    }
+    rs12 *= f;
+  }
+}
+
+// Helmholtz direct interaction (helmkernels2d.f:3-904): pot += (i/4)[H0 q
+// + k H1 (v.r)/r d]; gradients and Hessians as h2d_directcdh.  Pairs with
+// |k r| below thresh are skipped (<= for the charge potential-only variant).
+void h2d_direct(int nd, cdbl zk, const double* src, int ns, const cdbl* q, const cdbl* dst,
+                const double* dv, const double* trg, int nt, int ifpgh, cdbl* pot, cdbl* grad,
+                cdbl* hess, double thresh) {
+  cdbl I4(0, 0.25);
+  bool le = (ifpgh == 1 && q && !dst);
+  for (int j = 0; j < nt; j++)
+    for (int i = 0; i < ns; i++) {
+      double xd = trg[2 * j] - src[2 * i], yd = trg[2 * j + 1] - src[2 * i + 1];
+      double rr = xd * xd + yd * yd, r = std::sqrt(rr);
+      cdbl z = zk * r;
+      if (le ? (std::abs(z) <= thresh) : (std::abs(z) < thresh)) continue;
+      cdbl h0, h1;
+      hankel01(z, h0, h1);
+      double ct = xd / r, st = yd / r;
+      cdbl h2 = 2.0 * h1 / z - h0, h3 = 4.0 * h2 / z - h1;
+      for (int d = 0; d < nd; d++) {
+        cdbl P = 0.0, gx = 0.0, gy = 0.0, hxx = 0.0, hxy = 0.0, hyy = 0.0;
+        if (q) {
+          cdbl c = q[(size_t)i * nd + d];
+          P += h0 * c * I4;
+          cdbl cd = -h1 * (zk * c * I4 / r);
+          gx += cd * xd;
+          gy += cd * yd;
+          cdbl ch = (zk * c * I4 / r) / rr;
+          cdbl h2z = -z * h0 + 2.0 * h1;
+          hxx += ch * (h2z * xd * xd - rr * h1);
+          hxy += ch * (h2z * xd * yd);
+          hyy += ch * (h2z * yd * yd - rr * h1);
+        }
+        if (dst) {
+          cdbl c = dst[(size_t)i * nd + d];
+          double v1 = dv[((size_t)i * 2 + 0) * nd + d], v2 = dv[((size_t)i * 2 + 1) * nd + d];
+          P += h1 / r * zk * I4 * c * (xd * v1 + yd * v2);
+          cdbl c2 = -zk * zk * I4 * c;
+          cdbl f1 = h2 * (ct * ct - 0.5) - h0 / 2.0, f2 = h2 * ct * st,
+               f3 = h2 * (st * st - 0.5) - h0 / 2.0;
+          gx += c2 * f1 * v1 + c2 * f2 * v2;
+          gy += c2 * f2 * v1 + c2 * f3 * v2;
+          cdbl a1 = (-h1 / 2.0 * (-1.5) - h3 / 2.0 * (ct * ct - 0.5 - st * st)) * ct;
+          cdbl a2 = (-h1 / 2.0 * (-0.5) - h3 / 2.0 * (1.5 * ct * ct - 0.5 * st * st)) * st;
+          cdbl a3 = (-h1 / 2.0 * (-0.5) - h3 / 2.0 * (1.5 * st * st - 0.5 * ct * ct)) * ct;
+          cdbl a4 = (-h1 / 2.0 * (-1.5) - h3 / 2.0 * (st * st - 0.5 - ct * ct)) * st;
+          cdbl c3 = -zk * zk * zk * c * I4;
+          hxx += c3 * a1 * v1 + c3 * a2 * v2;
+          hxy += c3 * a2 * v1 + c3 * a3 * v2;
+          hyy += c3 * a3 * v1 + c3 * a4 * v2;
+        }
+        pot[(size_t)j * nd + d] += P;
+        if (ifpgh >= 2) {
+          grad[((size_t)j * 2 + 0) * nd + d] += gx;
+          grad[((size_t)j * 2 + 1) * nd + d] += gy;
+        }
+        if (ifpgh >= 3) {
+          hess[((size_t)j * 3 + 0) * nd + d] += hxx;
+          hess[((size_t)j * 3 + 1) * nd + d] += hxy;
+          hess[((size_t)j * 3 + 2) * nd + d] += hyy;
+        }
+      }
+    }
+}
+
+// hfmm2d (src/helmholtz/hfmm2d.f:19-450) and hfmm2dmain (456-1580), low
+// frequency: every level where M2L runs has box size <= 16 wavelengths.
+// Returns 13 if an expansion order exceeds the table, 20 when the
+// high-frequency (wideband) branch would be needed.
+int run_hfmm(int nd, double eps, cdbl zk, int ns, const double* src, const cdbl* charge,
+             const cdbl* dipstr, const double* dipvec, int ifpgh, cdbl* pot, cdbl* grad,
+             cdbl* hess, int nt, const double* targ, int ifpghtarg, cdbl* pottarg,
+             cdbl* gradtarg, cdbl* hesstarg, int ndiv_in, double* timeinfo) {
+  const double pi = 4 * std::atan(1.0);
+  double tinfo[8] = {0};
+  auto zero_out = [&]() {
+    if (ifpgh >= 1) std::fill(pot, pot + (size_t)nd * ns, cdbl(0));
+    if (ifpgh >= 2) std::fill(grad, grad + (size_t)2 * nd * ns, cdbl(0));
+    if (ifpgh >= 3) std::fill(hess, hess + (size_t)3 * nd * ns, cdbl(0));
+    if (ifpghtarg >= 1) std::fill(pottarg, pottarg + (size_t)nd * nt, cdbl(0));
+    if (ifpghtarg >= 2) std::fill(gradtarg, gradtarg + (size_t)2 * nd * nt, cdbl(0));
+    if (ifpghtarg >= 3) std::fill(hesstarg, hesstarg + (size_t)3 * nd * nt, cdbl(0));
+  };
+  if (ns <= 0) {
+    zero_out();
+    return 0;
+  }
+  int ndiv = ndiv_in > 0 ? ndiv_in : helm_ndiv(eps, ns, nt);
+  Tree T;
+  build_tree(src, ns, targ, nt, 0, ndiv, 51, T);
+  if (T.boxsize[0] == 0.0) {
+    zero_out();
+    return 0;
+  }
+  sort_points(T, src, ns, T.isrc, T.isrcse);
+  sort_points(T, targ, nt, T.itarg, T.itargse);
+  compute_lists(T);
+  const int nl = T.nlevels, nb = T.nboxes();
+  std::vector<double> rsc(nl + 1);
+  std::vector<int> nterms(nl + 1);
+  int ier = 0;
+  for (int l = 0; l <= nl; l++) {
+    rsc[l] = std::min(std::abs(zk * T.boxsize[l] / (2.0 * pi)), 1.0);
+    nterms[l] = h2dterms(T.boxsize[l], zk, eps, &ier);
+  }
+  if (ier) return ier;
+  double zi = zk.imag();
+  const double zkiup = 40.0;
+  // high-frequency levels are not restated: the M2L/M2M levels must be
+  // at most 16 wavelengths (hfmm2d.f:1001-1013, 1119-1124)
+  for (int l = 1; l <= nl; l++) {
+    double dlam = 1.0 / std::real(zk / (2 * pi));
+    if (zi * T.boxsize[l] < zkiup && T.boxsize[l] / dlam > 16.0) return 20;
+  }
+  // expansion storage: per box (2p+1) nd complex
+  std::vector<size_t> off(nb);
+  size_t tot = 0;
+  for (int l = 0; l <= nl; l++)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++) {
+      off[b] = tot;
+      tot += (size_t)(2 * nterms[l] + 1) * nd;
+    }
+  std::vector<cdbl> mp(tot, 0.0), lo(tot, 0.0);
+  auto MP = [&](int b) { return HExp{nterms[T.ilevel[b]], nd, &mp[off[b]]}; };
+  auto LO = [&](int b) { return HExp{nterms[T.ilevel[b]], nd, &lo[off[b]]}; };
+  auto CEN = [&](int b) { return &T.centers[2 * (size_t)b]; };
+  // sorted copies
+  std::vector<double> ss(2 * (size_t)ns), ts(2 * (size_t)nt), dvs(dipstr ? 2 * (size_t)nd * ns : 0);
+  std::vector<cdbl> qs(charge ? (size_t)nd * ns : 0), ds(dipstr ? (size_t)nd * ns : 0);
+  for (int k = 0; k < ns; k++) {
+    int i = T.isrc[k];
+    ss[2 * k] = src[2 * i];
+    ss[2 * k + 1] = src[2 * i + 1];
+    for (int d = 0; d < nd; d++) {
+      if (charge) qs[(size_t)k * nd + d] = charge[(size_t)i * nd + d];
+      if (dipstr) {
+        ds[(size_t)k * nd + d] = dipstr[(size_t)i * nd + d];
+        dvs[((size_t)k * 2 + 0) * nd + d] = dipvec[((size_t)i * 2 + 0) * nd + d];
+        dvs[((size_t)k * 2 + 1) * nd + d] = dipvec[((size_t)i * 2 + 1) * nd + d];
+      }
+    }
+  }
+  for (int k = 0; k < nt; k++) {
+    int i = T.itarg[k];
+    ts[2 * k] = targ[2 * i];
+    ts[2 * k + 1] = targ[2 * i + 1];
+  }
+  const cdbl* qp = charge ? qs.data() : nullptr;
+  const cdbl* dpp = dipstr ? ds.data() : nullptr;
+  const double* dvp = dipstr ? dvs.data() : nullptr;
+  std::vector<cdbl> po((size_t)nd * ns), gr((size_t)2 * nd * ns), he((size_t)3 * nd * ns);
+  std::vector<cdbl> pt((size_t)nd * nt), gt((size_t)2 * nd * nt), ht((size_t)3 * nd * nt);
+  auto nsrc = [&](int b) { return T.isrcse[2 * b + 1] - T.isrcse[2 * b]; };
+  auto ntrg = [&](int b) { return T.itargse[2 * b + 1] - T.itargse[2 * b]; };
+  auto has_eval = [&](int b) {
+    return (ifpghtarg > 0 ? ntrg(b) : 0) + (ifpgh > 0 ? nsrc(b) : 0) > 0;
+  };
+  auto lev_ok = [&](int l) { return zi * T.boxsize[l] < zkiup; };
+  double t0 = wtime();
+  // step 1: P2M at leaves
+  for (int l = 2; l <= nl; l++) {
+    if (!lev_ok(l)) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++) {
+      int s = T.isrcse[2 * b];
+      if (T.nchild[b] == 0 && nsrc(b) > 0)
+        helm_form(nd, zk, rsc[l], &ss[2 * (size_t)s], nsrc(b), qp ? qp + (size_t)s * nd : nullptr,
+                  dpp ? dpp + (size_t)s * nd : nullptr, dvp ? dvp + (size_t)s * 2 * nd : nullptr,
+                  CEN(b), MP(b), true);
+    }
+  }
+  tinfo[0] = wtime() - t0;
+  // step 2: P2L from list 4
+  t0 = wtime();
+  for (int l = 2; l <= nl; l++) {
+    if (!lev_ok(l)) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++) {
+      if (!has_eval(b)) continue;
+      for (int i = 0; i < T.nl4[b]; i++) {
+        int j = T.l4[(size_t)MNL4 * b + i];
+        int s = T.isrcse[2 * j];
+        helm_form(nd, zk, rsc[l], &ss[2 * (size_t)s], nsrc(j), qp ? qp + (size_t)s * nd : nullptr,
+                  dpp ? dpp + (size_t)s * nd : nullptr, dvp ? dvp + (size_t)s * 2 * nd : nullptr,
+                  CEN(b), LO(b), false);
+      }
+    }
+  }
+  tinfo[1] = wtime() - t0;
+  // step 3: M2M
+  t0 = wtime();
+  for (int l = nl - 1; l >= 1; l--) {
+    if (!lev_ok(l)) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++)
+      for (int i = 0; i < T.nchild[b]; i++) {
+        int c = T.ichild[4 * b + i];
+        if (nsrc(c) > 0) h2dmpmp(nd, zk, rsc[l + 1], CEN(c), MP(c), rsc[l], CEN(b), MP(b));
+      }
+  }
+  tinfo[2] = wtime() - t0;
+  // step 4: M2L
+  t0 = wtime();
+  for (int l = 2; l <= nl; l++) {
+    if (!lev_ok(l)) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++) {
+      if (!has_eval(b)) continue;
+      for (int i = 0; i < T.nl2[b]; i++) {
+        int j = T.l2[(size_t)MNL2 * b + i];
+        h2dmploc(nd, zk, rsc[l], CEN(j), MP(j), rsc[l], CEN(b), LO(b));
+      }
+    }
+  }
+  tinfo[3] = wtime() - t0;
+  // step 5: L2L
+  t0 = wtime();
+  for (int l = 1; l <= nl - 1; l++) {
+    if (!lev_ok(l)) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++) {
+      if (!has_eval(b)) continue;
+      for (int i = 0; i < T.nchild[b]; i++) {
+        int c = T.ichild[4 * b + i];
+        h2dlocloc(nd, zk, rsc[l], CEN(b), LO(b), rsc[l + 1], CEN(c), LO(c));
+      }
+    }
+  }
+  tinfo[4] = wtime() - t0;
+  // step 6: M2P from list 3
+  t0 = wtime();
+  for (int l = 1; l <= nl - 1; l++) {
+    if (!lev_ok(l + 1)) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++)
+      for (int i = 0; i < T.nl3[b]; i++) {
+        int j = T.l3[(size_t)MNL3 * b + i];
+        if (ifpghtarg > 0) {
+          int s = T.itargse[2 * b];
+          helm_eval(nd, zk, rsc[l + 1], CEN(j), MP(j), true, &ts[2 * (size_t)s], ntrg(b),
+                    ifpghtarg, &pt[(size_t)s * nd], &gt[(size_t)s * 2 * nd], &ht[(size_t)s * 3 * nd]);
+        }
+        if (ifpgh > 0) {
+          int s = T.isrcse[2 * b];
+          helm_eval(nd, zk, rsc[l + 1], CEN(j), MP(j), true, &ss[2 * (size_t)s], nsrc(b), ifpgh,
+                    &po[(size_t)s * nd], &gr[(size_t)s * 2 * nd], &he[(size_t)s * 3 * nd]);
+        }
+      }
+  }
+  tinfo[5] = wtime() - t0;
+  // step 7: L2P at leaves
+  t0 = wtime();
+  for (int l = 0; l <= nl; l++) {
+    if (!lev_ok(l)) continue;
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++) {
+      if (T.nchild[b] != 0) continue;
+      if (ifpghtarg > 0) {
+        int s = T.itargse[2 * b];
+        helm_eval(nd, zk, rsc[l], CEN(b), LO(b), false, &ts[2 * (size_t)s], ntrg(b), ifpghtarg,
+                  &pt[(size_t)s * nd], &gt[(size_t)s * 2 * nd], &ht[(size_t)s * 3 * nd]);
+      }
+      if (ifpgh > 0) {
+        int s = T.isrcse[2 * b];
+        helm_eval(nd, zk, rsc[l], CEN(b), LO(b), false, &ss[2 * (size_t)s], nsrc(b), ifpgh,
+                  &po[(size_t)s * nd], &gr[(size_t)s * 2 * nd], &he[(size_t)s * 3 * nd]);
+      }
+    }
+  }
+  tinfo[6] = wtime() - t0;
+  // step 8: P2P
+  t0 = wtime();
+  double thresh = std::abs(zk) * T.boxsize[0] * std::pow(2.0, -51);
+  for (int l = 0; l <= nl; l++) {
+#pragma omp parallel for schedule(dynamic)
+    for (int b = T.lfirst[l]; b <= T.llast[l]; b++)
+      for (int i = 0; i < T.nl1[b]; i++) {
+        int j = T.l1[(size_t)MNL1 * b + i];
+        int s = T.isrcse[2 * j], n = nsrc(j);
+        const cdbl* qj = qp ? qp + (size_t)s * nd : nullptr;
+        const cdbl* dj = dpp ? dpp + (size_t)s * nd : nullptr;
+        const double* vj = dvp ? dvp + (size_t)s * 2 * nd : nullptr;
+        if (ifpghtarg > 0) {
+          int t = T.itargse[2 * b];
+          h2d_direct(nd, zk, &ss[2 * (size_t)s], n, qj, dj, vj, &ts[2 * (size_t)t], ntrg(b),
+                     ifpghtarg, &pt[(size_t)t * nd], &gt[(size_t)t * 2 * nd],
+                     &ht[(size_t)t * 3 * nd], thresh);
+        }
+        if (ifpgh > 0) {
+          int t = T.isrcse[2 * b];
+          h2d_direct(nd, zk, &ss[2 * (size_t)s], n, qj, dj, vj, &ss[2 * (size_t)t], nsrc(b), ifpgh,
+                     &po[(size_t)t * nd], &gr[(size_t)t * 2 * nd], &he[(size_t)t * 3 * nd],
+                     thresh);
+        }
+      }
+  }
+  tinfo[7] = wtime() - t0;
+  for (int k = 0; k < ns; k++) {
+    int i = T.isrc[k];
+    for (int d = 0; d < nd; d++) {
+      if (ifpgh >= 1) pot[(size_t)i * nd + d] = po[(size_t)k * nd + d];
+      for (int c = 0; c < 2 && ifpgh >= 2; c++)
+        grad[((size_t)i * 2 + c) * nd + d] = gr[((size_t)k * 2 + c) * nd + d];
+      for (int c = 0; c < 3 && ifpgh >= 3; c++)
+        hess[((size_t)i * 3 + c) * nd + d] = he[((size_t)k * 3 + c) * nd + d];
+    }
+  }
+  for (int k = 0; k < nt; k++) {
+    int i = T.itarg[k];
+    for (int d = 0; d < nd; d++) {
+      if (ifpghtarg >= 1) pottarg[(size_t)i * nd + d] = pt[(size_t)k * nd + d];
+      for (int c = 0; c < 2 && ifpghtarg >= 2; c++)
+        gradtarg[((size_t)i * 2 + c) * nd + d] = gt[((size_t)k * 2 + c) * nd + d];
+      for (int c = 0; c < 3 && ifpghtarg >= 3; c++)
+        hesstarg[((size_t)i * 3 + c) * nd + d] = ht[((size_t)k * 3 + c) * nd + d];
+    }
+  }
+  if (timeinfo)
+    for (int i = 0; i < 8; i++) timeinfo[i] = tinfo[i];
+  return 0;
+}
+
 // Output unpacking shared by lfmm2d / rfmm2d:
 // pot = Re, grad = (Re g, -Im g), hess = (Re h, -Im h, -Re h)
 // (lfmm2d.f:169-223, rfmm2d.f:158-212)
@@ -1257,6 +2140,57 @@ void orc_r2ddir(int nd, const double* src, int ns, const double* charge, const d
     for (size_t k = 0; k < (size_t)nd * 2 * nt; k++) grad[k] = G[k].real();
   if (ifpgh >= 3)
     for (size_t k = 0; k < (size_t)nd * 3 * nt; k++) hess[k] = H[k].real();
+}
+
+// hfmm2d (src/helmholtz/hfmm2d.f:19-22); zk as (re, im).
+void orc_hfmm2d(int nd, double eps, double zkr, double zki, int ns, const double* sources,
+                int ifcharge, const double* charge, int ifdipole, const double* dipstr,
+                const double* dipvec, int ifpgh, double* pot, double* grad, double* hess, int nt,
+                const double* targ, int ifpghtarg, double* pottarg, double* gradtarg,
+                double* hesstarg, int ndiv, double* timeinfo, int* ier) {
+  *ier = run_hfmm(nd, eps, cdbl(zkr, zki), ns, sources, ifcharge ? (const cdbl*)charge : nullptr,
+                  ifdipole ? (const cdbl*)dipstr : nullptr, ifdipole ? dipvec : nullptr, ifpgh,
+                  (cdbl*)pot, (cdbl*)grad, (cdbl*)hess, nt, targ, ifpghtarg, (cdbl*)pottarg,
+                  (cdbl*)gradtarg, (cdbl*)hesstarg, ndiv, timeinfo);
+}
+
+// Helmholtz direct sum (helmkernels2d.f); outputs overwritten.
+void orc_h2ddir(int nd, double zkr, double zki, const double* src, int ns, const double* charge,
+                const double* dipstr, const double* dipvec, const double* trg, int nt, int ifpgh,
+                double* pot, double* grad, double* hess, double thresh) {
+  cdbl zk(zkr, zki);
+  cdbl* P = (cdbl*)pot;
+  cdbl* G = (cdbl*)grad;
+  cdbl* H = (cdbl*)hess;
+  std::fill(P, P + (size_t)nd * nt, cdbl(0));
+  if (ifpgh >= 2) std::fill(G, G + (size_t)2 * nd * nt, cdbl(0));
+  if (ifpgh >= 3) std::fill(H, H + (size_t)3 * nd * nt, cdbl(0));
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < nt; j++)
+    h2d_direct(nd, zk, src, ns, (const cdbl*)charge, (const cdbl*)dipstr, dipvec,
+               trg + 2 * (size_t)j, 1, ifpgh, P + (size_t)j * nd,
+               ifpgh >= 2 ? G + (size_t)j * 2 * nd : nullptr,
+               ifpgh >= 3 ? H + (size_t)j * 3 * nd : nullptr, thresh);
+}
+
+// H0, H1 and the helpers' sequences for the fixture tests.
+void orc_hankel01(double zr, double zi, double* h0h1) {
+  cdbl a, b;
+  hankel01(cdbl(zr, zi), a, b);
+  h0h1[0] = a.real();
+  h0h1[1] = a.imag();
+  h0h1[2] = b.real();
+  h0h1[3] = b.imag();
+}
+void orc_jbessel2d(int nterms, double zr, double zi, double rscale, double* out) {
+  jbessel2d(nterms, cdbl(zr, zi), rscale, (cdbl*)out);
+}
+void orc_h2dall(int nterms, double zr, double zi, double rscale, double* out) {
+  h2dall(nterms, cdbl(zr, zi), rscale, (cdbl*)out);
+}
+int orc_h2dterms(double bsize, double zkr, double zki, double eps) {
+  int ier = 0;
+  return h2dterms(bsize, cdbl(zkr, zki), eps, &ier);
 }
 
 // LAPACK dlaran (src/common/dlaran.f) behind hkrand (src/common/hkrand.f):

@@ -212,3 +212,83 @@ def hkrand(n, seed=None):
     out = np.zeros(n)
     lib().orc_hkrand_fill(_p(out), C.c_long(n))
     return out
+
+
+# ---------------------------------------------------------------- Helmholtz
+def hfmm2d(eps, zk, sources, charges=None, dipstr=None, dipvec=None, targets=None, ifpgh=0,
+           ifpghtarg=0, nd=1, ndiv=0):
+    """Oracle hfmm2d; outputs pot (nd,n), grad (nd,2,n), hess (nd,3,n) complex."""
+    s = _f64(sources.T)
+    ns = s.shape[0]
+    t = _f64(np.zeros((0, 2)) if targets is None else targets.T)
+    nt = t.shape[0]
+    cv = (lambda a: np.ascontiguousarray(np.asarray(a).reshape(nd, ns).T, dtype=np.complex128))
+    q = None if charges is None else cv(charges)
+    d = None if dipstr is None else cv(dipstr)
+    v = None if dipvec is None else _f64(np.asarray(dipvec).reshape(nd, 2, ns).transpose(2, 1, 0))
+    pot = np.zeros((max(ns, 1), nd), np.complex128)
+    grad = np.zeros((max(ns, 1), 2, nd), np.complex128)
+    hess = np.zeros((max(ns, 1), 3, nd), np.complex128)
+    pt = np.zeros((max(nt, 1), nd), np.complex128)
+    gt = np.zeros((max(nt, 1), 2, nd), np.complex128)
+    ht = np.zeros((max(nt, 1), 3, nd), np.complex128)
+    tinfo = np.zeros(8)
+    ier = C.c_int(0)
+    zk = complex(zk)
+    lib().orc_hfmm2d(C.c_int(nd), C.c_double(eps), C.c_double(zk.real), C.c_double(zk.imag),
+                     C.c_int(ns), _p(s), C.c_int(q is not None), _p(q), C.c_int(d is not None),
+                     _p(d), _p(v), C.c_int(ifpgh), _p(pot), _p(grad), _p(hess), C.c_int(nt), _p(t),
+                     C.c_int(ifpghtarg), _p(pt), _p(gt), _p(ht), C.c_int(ndiv), _p(tinfo),
+                     C.byref(ier))
+    return dict(pot=pot[:ns].T, grad=grad[:ns].transpose(2, 1, 0),
+                hess=hess[:ns].transpose(2, 1, 0), pottarg=pt[:nt].T,
+                gradtarg=gt[:nt].transpose(2, 1, 0), hesstarg=ht[:nt].transpose(2, 1, 0),
+                timeinfo=tinfo, ier=ier.value)
+
+
+def h2ddir(zk, sources, targets, charges=None, dipstr=None, dipvec=None, ifpgh=1, nd=1,
+           thresh=1e-16):
+    s = _f64(sources.T)
+    t = _f64(targets.T)
+    ns, nt = s.shape[0], t.shape[0]
+    cv = (lambda a: np.ascontiguousarray(np.asarray(a).reshape(nd, ns).T, dtype=np.complex128))
+    q = None if charges is None else cv(charges)
+    d = None if dipstr is None else cv(dipstr)
+    v = None if dipvec is None else _f64(np.asarray(dipvec).reshape(nd, 2, ns).transpose(2, 1, 0))
+    pot = np.zeros((nt, nd), np.complex128)
+    grad = np.zeros((nt, 2, nd), np.complex128)
+    hess = np.zeros((nt, 3, nd), np.complex128)
+    zk = complex(zk)
+    lib().orc_h2ddir(C.c_int(nd), C.c_double(zk.real), C.c_double(zk.imag), _p(s), C.c_int(ns),
+                     _p(q), _p(d), _p(v), _p(t), C.c_int(nt), C.c_int(ifpgh), _p(pot), _p(grad),
+                     _p(hess), C.c_double(thresh))
+    return dict(pottarg=pot.T, gradtarg=grad.transpose(2, 1, 0), hesstarg=hess.transpose(2, 1, 0))
+
+
+def hankel01(z):
+    out = np.zeros(4)
+    lib().orc_hankel01(C.c_double(complex(z).real), C.c_double(complex(z).imag), _p(out))
+    return complex(out[0], out[1]), complex(out[2], out[3])
+
+
+def jbessel2d(nterms, z, rscale):
+    out = np.zeros(nterms + 1, np.complex128)
+    z = complex(z)
+    lib().orc_jbessel2d(C.c_int(nterms), C.c_double(z.real), C.c_double(z.imag),
+                        C.c_double(rscale), _p(out))
+    return out
+
+
+def h2dall(nterms, z, rscale):
+    out = np.zeros(nterms + 1, np.complex128)
+    z = complex(z)
+    lib().orc_h2dall(C.c_int(nterms), C.c_double(z.real), C.c_double(z.imag), C.c_double(rscale),
+                     _p(out))
+    return out
+
+
+def h2dterms(bsize, zk, eps):
+    zk = complex(zk)
+    lib().orc_h2dterms.restype = C.c_int
+    return lib().orc_h2dterms(C.c_double(bsize), C.c_double(zk.real), C.c_double(zk.imag),
+                              C.c_double(eps))
