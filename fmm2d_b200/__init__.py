@@ -7,9 +7,9 @@
 See fmm2d_b200/fmm2d.py for the entry points; the CUDA library's C ABI is
 include/fmm2d_b200.h.
 """
-from .fmm2d import (Output, c2ddir, cfmm2d, comperr, l2ddir, lfmm2d, r2ddir,  # noqa: F401
-                    rfmm2d)
+from .fmm2d import (Output, c2ddir, cfmm2d, comperr, h2ddir, hfmm2d, l2ddir,  # noqa: F401
+                    lfmm2d, r2ddir, rfmm2d)
 from ._lib import version  # noqa: F401
 
-__all__ = ["Output", "lfmm2d", "rfmm2d", "cfmm2d", "l2ddir", "r2ddir", "c2ddir", "comperr",
-           "version"]
+__all__ = ["Output", "hfmm2d", "lfmm2d", "rfmm2d", "cfmm2d", "h2ddir", "l2ddir", "r2ddir",
+           "c2ddir", "comperr", "version"]

@@ -22,6 +22,7 @@ PREC = {"auto": 0, "fp64": 1, "mixed": 2}
 
 _LAP_HOST = [c_int, c_double, c_int64, P, c_int, P, c_int, P]
 _PGH = [c_int, P, P, P, c_int64, P, c_int, P, P, P]
+_HELM_HOST = [c_int, c_double, c_double, c_double, c_int64, P, c_int, P, c_int, P, P]
 
 # name -> argtypes, for every symbol declared in include/fmm2d_b200.h
 SIGNATURES = {
@@ -42,6 +43,13 @@ SIGNATURES = {
                              c_double, P, P],
     "b2fmm_lap_direct_noalloc_dev": [c_int, c_int, c_int64, P, P, P, P, c_int64, P, c_int, P, P,
                                      P, c_double, P, P],
+    "b2fmm_hfmm2d": _HELM_HOST + [c_int] + _PGH + [P],
+    "b2fmm_hfmm2d_ndiv": _HELM_HOST + [c_int] + _PGH + [c_int, c_int, c_int, P, P],
+    "b2fmm_hfmm2d_dev": _HELM_HOST + _PGH + [P, P, P, P],
+    "b2fmm_h2ddir_dev": [c_int, c_double, c_double, c_int64, P, P, P, P, c_int64, P, c_int, P,
+                         P, P, c_double, P, P],
+    "b2fmm_h2dterms": [c_double, c_double, c_double, c_double, P],
+    "b2fmm_helm_special": [c_int, c_int, c_double, c_double, c_double, P],
     "b2fmm_tree_build": [P, c_int64, P, c_int64, c_int, c_int, c_int, P, P, P],
     "b2fmm_tree_get": [P] * 23,
     "b2fmm_tree_free": [P],
@@ -75,6 +83,7 @@ def lib():
         L.b2fmm_tree_build.restype = c_void_p
         L.b2fmm_kernel_launches.restype = C.c_uint64
         L.b2fmm_fma_peak.restype = c_double
+        L.b2fmm_h2dterms.restype = c_int
         _lib = L
     return _lib
 

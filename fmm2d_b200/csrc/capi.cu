@@ -4,6 +4,8 @@
 
 #include "../../include/fmm2d_b200.h"
 #include "direct.cuh"
+#include "helm_special.cuh"
+#include "helmholtz.cuh"
 #include "laplace.cuh"
 #include "tree.cuh"
 #include "peaks.cuh"
@@ -109,6 +111,86 @@ int lap_host(LapArgs h) {
   down(h.pottarg, a.pottarg, nq * nt);
   down(h.gradtarg, a.gradtarg, nq * gw * nt);
   down(h.hesstarg, a.hesstarg, nq * hw * nt);
+  B2_CHECK(cudaStreamSynchronize(st));
+  return IER_OK;
+}
+
+HelmArgs make_hargs(int nd, double eps, double zkr, double zki, int64_t ns, const double* sources,
+                    int ifcharge, const double* charge, int ifdipole, const double* dipstr,
+                    const double* dipvec, int ifpgh, double* pot, double* grad, double* hess,
+                    int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+                    double* gradtarg, double* hesstarg, const b2fmm_options* o,
+                    double* timeinfo) {
+  HelmArgs a;
+  a.nd = nd;
+  a.eps = eps;
+  a.zkr = zkr;
+  a.zki = zki;
+  a.ns = ns;
+  a.src = sources;
+  a.charge = ifcharge == 1 ? charge : nullptr;
+  a.dipstr = ifdipole == 1 ? dipstr : nullptr;
+  a.dipvec = ifdipole == 1 ? dipvec : nullptr;
+  a.ifpgh = ifpgh;
+  a.pot = pot;
+  a.grad = grad;
+  a.hess = hess;
+  a.nt = nt;
+  a.trg = targ;
+  a.ifpghtarg = ifpghtarg;
+  a.pottarg = pottarg;
+  a.gradtarg = gradtarg;
+  a.hesstarg = hesstarg;
+  if (o) {
+    a.ndiv = o->ndiv;
+    a.ifnear = o->ifnear;
+  }
+  a.timeinfo = timeinfo;
+  return a;
+}
+
+// Host-pointer Helmholtz driver (complex values interleaved re/im).
+int helm_host(HelmArgs h) {
+  cudaStream_t st = cudaStreamPerThread;
+  const int nd = h.nd;
+  const long ns = h.ns, nt = h.ifpghtarg > 0 ? h.nt : 0;
+  const size_t nq = 2 * (size_t)nd;
+  DBuf<double> src(st), trg(st), q(st), dp(st), dv(st), po(st), gr(st), he(st), pt(st), gt(st),
+      ht(st);
+  auto up = [&](DBuf<double>& d, const double* hp, size_t n) {
+    if (!hp || n == 0) return (double*)nullptr;
+    d.alloc(n, st);
+    B2_CHECK(cudaMemcpyAsync(d.p, hp, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    return d.p;
+  };
+  auto mk = [&](DBuf<double>& d, size_t n) {
+    if (n == 0) return (double*)nullptr;
+    d.alloc(n, st);
+    return d.p;
+  };
+  HelmArgs a = h;
+  a.src = up(src, h.src, 2 * (size_t)ns);
+  a.trg = up(trg, nt > 0 ? h.trg : nullptr, 2 * (size_t)nt);
+  a.charge = up(q, h.charge, nq * ns);
+  a.dipstr = up(dp, h.dipstr, nq * ns);
+  a.dipvec = up(dv, h.dipstr ? h.dipvec : nullptr, 2 * (size_t)nd * ns);
+  a.pot = h.ifpgh >= 1 ? mk(po, nq * ns) : nullptr;
+  a.grad = h.ifpgh >= 2 ? mk(gr, nq * 2 * ns) : nullptr;
+  a.hess = h.ifpgh >= 3 ? mk(he, nq * 3 * ns) : nullptr;
+  a.pottarg = h.ifpghtarg >= 1 ? mk(pt, nq * nt) : nullptr;
+  a.gradtarg = h.ifpghtarg >= 2 ? mk(gt, nq * 2 * nt) : nullptr;
+  a.hesstarg = h.ifpghtarg >= 3 ? mk(ht, nq * 3 * nt) : nullptr;
+  int r = helm_fmm_device(a, st);
+  if (r != IER_OK) return r;
+  auto down = [&](double* hp, const double* dpp, size_t n) {
+    if (hp && dpp && n) B2_CHECK(cudaMemcpyAsync(hp, dpp, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  };
+  down(h.pot, a.pot, nq * ns);
+  down(h.grad, a.grad, nq * 2 * ns);
+  down(h.hess, a.hess, nq * 3 * ns);
+  down(h.pottarg, a.pottarg, nq * nt);
+  down(h.gradtarg, a.gradtarg, nq * 2 * nt);
+  down(h.hesstarg, a.hesstarg, nq * 3 * nt);
   B2_CHECK(cudaStreamSynchronize(st));
   return IER_OK;
 }
@@ -304,6 +386,84 @@ void b2fmm_lap_direct_noalloc_dev(int kind, int nd, int64_t ns, const double* so
     return lap_direct_device_noalloc(kind, nd, ns, sources, charge, dipstr, dipvec, nt, targ,
                                      ifpgh, pot, grad, hess, thresh, (cudaStream_t)stream);
   });
+}
+
+void b2fmm_hfmm2d(int nd, double eps, double zk_re, double zk_im, int64_t ns,
+                  const double* sources, int ifcharge, const double* charge, int ifdipole,
+                  const double* dipstr, const double* dipvec, int iper, int ifpgh, double* pot,
+                  double* grad, double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                  double* pottarg, double* gradtarg, double* hesstarg, int* ier) {
+  (void)iper;
+  guarded(ier, [&] {
+    return helm_host(make_hargs(nd, eps, zk_re, zk_im, ns, sources, ifcharge, charge, ifdipole,
+                                dipstr, dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+                                pottarg, gradtarg, hesstarg, nullptr, nullptr));
+  });
+}
+
+void b2fmm_hfmm2d_ndiv(int nd, double eps, double zk_re, double zk_im, int64_t ns,
+                       const double* sources, int ifcharge, const double* charge, int ifdipole,
+                       const double* dipstr, const double* dipvec, int iper, int ifpgh,
+                       double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                       int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                       int ndiv, int idivflag, int ifnear, double* timeinfo, int* ier) {
+  (void)iper;
+  (void)idivflag;
+  b2fmm_options o{ndiv, 0, ifnear, PREC_FP64};
+  guarded(ier, [&] {
+    return helm_host(make_hargs(nd, eps, zk_re, zk_im, ns, sources, ifcharge, charge, ifdipole,
+                                dipstr, dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+                                pottarg, gradtarg, hesstarg, &o, timeinfo));
+  });
+}
+
+void b2fmm_hfmm2d_dev(int nd, double eps, double zk_re, double zk_im, int64_t ns,
+                      const double* sources, int ifcharge, const double* charge, int ifdipole,
+                      const double* dipstr, const double* dipvec, int ifpgh, double* pot,
+                      double* grad, double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                      double* pottarg, double* gradtarg, double* hesstarg,
+                      const b2fmm_options* opts, double* timeinfo, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return helm_fmm_device(make_hargs(nd, eps, zk_re, zk_im, ns, sources, ifcharge, charge,
+                                      ifdipole, dipstr, dipvec, ifpgh, pot, grad, hess, nt, targ,
+                                      ifpghtarg, pottarg, gradtarg, hesstarg, opts, timeinfo),
+                           (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_h2ddir_dev(int nd, double zk_re, double zk_im, int64_t ns, const double* sources,
+                      const double* charge, const double* dipstr, const double* dipvec,
+                      int64_t nt, const double* targ, int ifpgh, double* pot, double* grad,
+                      double* hess, double thresh, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return helm_direct_device(nd, zk_re, zk_im, ns, sources, charge, dipstr, dipvec, nt, targ,
+                              ifpgh, pot, grad, hess, thresh, (cudaStream_t)stream);
+  });
+}
+
+int b2fmm_h2dterms(double bsize, double zk_re, double zk_im, double eps, int* ier) {
+  int e = 0, p = 0;
+  guarded(ier, [&] {
+    p = helm_nterms(bsize, zk_re, zk_im, eps, &e);
+    return e;
+  });
+  return p;
+}
+
+void b2fmm_helm_special(int kind, int n, double z_re, double z_im, double rscale, double* out) {
+  double2 z = make_double2(z_re, z_im);
+  if (kind == 0) {
+    double2 h0, h1;
+    helm::hank01(z, h0, h1);
+    out[0] = h0.x;
+    out[1] = h0.y;
+    out[2] = h1.x;
+    out[3] = h1.y;
+  } else if (kind == 1) {
+    helm::jscaled(n, z, rscale, (double2*)out);
+  } else {
+    helm::hscaled(n, z, rscale, (double2*)out);
+  }
 }
 
 void* b2fmm_tree_build(const double* sources_dev, int64_t ns, const double* targ_dev, int64_t nt,

@@ -16,6 +16,7 @@ enum {
   IER_OK = 0,
   IER_ALLOC = 4,
   IER_NTERMS = 13,
+  IER_HIGHFREQ = 20,  // Helmholtz boxes above 16 wavelengths (wideband translations)
   IER_BADARG = 100,  // invalid argument (sizes, flags)
   IER_CUDA = 101,    // CUDA runtime error
   IER_TIMEOUT = 102,  // a bounded device wait gave up

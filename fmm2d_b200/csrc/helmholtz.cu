@@ -1,0 +1,1302 @@
+// Helmholtz FMM on B200 (FP64): the low-frequency path of hfmm2dmain
+// (src/helmholtz/hfmm2d.f:456-1580) with the operators of
+// src/helmholtz/helmrouts2d.f and the near field of helmkernels2d.f.
+//
+// Expansions have 2p_l+1 coefficients (n = -p_l..p_l) per density, with a
+// per-level order p_l (h2dterms) and scale rs_l = min(|zk bs_l / 2pi|, 1);
+// box b of level l stores them at off_l + (b - lfirst_l) (2p_l+1) ND.
+// Centres of boxes of one level differ by multiples of the box size, so the
+// translation kernels of M2L (per integer offset) and of M2M / L2L (per
+// child slot) are tabulated once per level; M2L and the shifts then become
+// Toeplitz convolutions with per-lane rscale factors:
+//   M2M: H2(i) += sum_j H1(j) T(i-j) (rs1/rs2)^|i| rs1^(2e),
+//        e = max(0,|j|-|i|) for j of the sign of i, else |j|   (h2dmpmp)
+//   L2L: J2(i) += sum_j J1(j) T(i-j) F(i,j)                     (h2dlocloc)
+//   M2L: L(i)  += sum_j H(j) T(i-j) rs^(2 min(|j|,|i|)) [same sign] (h2dmploc)
+#include "helmholtz.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "helm_special.cuh"
+#include "lap_common.cuh"
+#include "laplace.cuh"
+#include "tree.cuh"
+
+namespace b2 {
+
+namespace helm {
+const SerTab& helm_tables() {
+  static SerTab T;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    double f = 1.0;  // k!
+    double hk = 0.0;
+    const double eg = 0.57721566490153286061;
+    for (int k = 0; k < NSER; k++) {
+      if (k > 0) {
+        f *= k;
+        hk += 1.0 / k;
+      }
+      double fk1 = f * (k + 1);
+      T.c0[k] = 1.0 / (f * f);
+      T.c1[k] = 1.0 / (f * fk1);
+      T.cy0[k] = hk / (f * f);
+      T.cy1[k] = (2.0 * (hk - eg) + 1.0 / (k + 1)) / (f * fk1);
+    }
+    T.a0[0] = T.a1[0] = 1.0;
+    for (int k = 1; k < NSER; k++) {
+      double m = (2.0 * k - 1) * (2.0 * k - 1);
+      T.a0[k] = T.a0[k - 1] * (0.0 - m) / (8.0 * k);
+      T.a1[k] = T.a1[k - 1] * (4.0 - m) / (8.0 * k);
+    }
+  });
+  return T;
+}
+}  // namespace helm
+
+namespace {
+
+using namespace lapk;
+using helm::hscaled;
+using helm::jscaled;
+
+void ensure_device_tables() {
+  static std::mutex mu;
+  static bool done[128] = {false};
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (done[dev]) return;
+  const helm::SerTab& T = helm::helm_tables();
+  B2_CHECK(cudaMemcpyToSymbol(helm::c_ser, &T, sizeof(T)));
+  done[dev] = true;
+}
+
+constexpr int HMAXP = 63;  // largest supported expansion order (2p+1 <= 4 x 32 lanes)
+
+struct HLev {
+  int lfirst, p, P, ok;  // ok: expansions formed at this level (zkiupbound test)
+  double rs, bs;
+  long off;              // expansion offset (double2 units, times ND inside kernels)
+  int nsh;               // half width of the M2M/L2L tables towards level l+1
+  long tm2l, tm2m, tl2l; // table offsets (double2 units)
+};
+
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// T[k], k = -nt..nt: T(0) = Z_0, T(j) = e^j Z_j, T(-j) = (-conj e)^j Z_j with
+// e = exp(-i theta) (the jtemp/htemp tables of h2dmpmp / h2dmploc).
+__device__ void phase_table(int nt, double theta, const double2* Z, double2* T) {
+  double2 e = make_double2(cos(theta), -sin(theta));
+  double2 ec = cconj(e);
+  T[nt] = Z[0];
+  double2 a = e, b = make_double2(-ec.x, -ec.y);
+  for (int j = 1; j <= nt; j++) {
+    T[nt + j] = cmul(a, Z[j]);
+    T[nt - j] = cmul(b, Z[j]);
+    a = cmul(a, e);
+    b = cmul(b, make_double2(-ec.x, -ec.y));
+  }
+}
+
+// One thread per (level, table): M2L tables for 49 offsets at levels >= 2,
+// M2M and L2L tables for the 4 child slots below every level.
+__global__ void k_h_tables(const HLev* __restrict__ lv, int nl, double zkr, double zki,
+                           double2* __restrict__ tabs, double2* __restrict__ scratch,
+                           int scratch_stride) {
+  int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const double pi = 3.14159265358979323846;
+  int nper = 49 + 8;
+  int l = tid / nper, k = tid % nper;
+  if (l > nl) return;
+  double2 zk = make_double2(zkr, zki);
+  double2* Z = scratch + (size_t)tid * scratch_stride;
+  HLev L = lv[l];
+  if (k < 49) {
+    if (l < 2 || !L.ok) return;
+    int ox = k / 7 - 3, oy = k % 7 - 3;
+    if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) return;
+    // z0 = c_tgt - c_src = o bs; theta - pi as in h2dmploc
+    double x = ox * L.bs, y = oy * L.bs;
+    double r = sqrt(x * x + y * y), th = atan2(y, x) - pi;
+    int nt = 2 * L.p;
+    hscaled(nt + 1, make_double2(zk.x * r, zk.y * r), L.rs, Z);
+    phase_table(nt, th, Z, tabs + L.tm2l + (size_t)k * (2 * nt + 1));
+    return;
+  }
+  if (l >= nl || l < 2) return;  // shifts run between levels >= 2
+  HLev C = lv[l + 1];
+  int slot = (k - 49) % 4, kind = (k - 49) / 4;  // kind 0: M2M, 1: L2L
+  if (!(kind == 0 ? C.ok : L.ok)) return;
+  double h = C.bs / 2;
+  double cx = (slot & 1) ? h : -h, cy = (slot < 2) ? -h : h;  // child - parent
+  int nt = L.nsh;
+  // M2M: z0 = parent - child, scaled by rs(child); L2L: child - parent, rs(parent)
+  double x = kind == 0 ? -cx : cx, y = kind == 0 ? -cy : cy;
+  double r = sqrt(x * x + y * y), th = atan2(y, x) - pi;
+  double rs1 = kind == 0 ? C.rs : L.rs;
+  jscaled(nt + 3, make_double2(zk.x * r, zk.y * r), rs1, Z);
+  phase_table(nt, th, Z, tabs + (kind == 0 ? L.tm2m : L.tl2l) + (size_t)slot * (2 * nt + 1));
+}
+
+struct HDens {
+  const double2* q;   // sorted charges (nd per point)
+  const double2* d;   // sorted dipole strengths
+  const double* v;    // sorted dipvec (2*nd per point)
+  int nd, d0;
+};
+
+// Per-source expansion terms (ctompole / dtompole, helmrouts2d.f:1383-1492)
+// for coefficient n of one density: Z = scaled J (multipole) or H (local),
+// E = powers of e = exp(-i theta) of the source, q, dipole d with (v1, v2).
+__device__ __forceinline__ double2 src_term(int n, const double2* Z, const double2* E, double2 q,
+                                            double2 d, double v1, double v2, bool hq, bool hd,
+                                            double2 zk, double rs) {
+  int m = n < 0 ? -n : n;
+  double2 res = make_double2(0, 0);
+  double2 em = E[m];
+  double2 eneg = cconj(em);  // e^{+i m theta}
+  if (hq) {
+    if (n == 0)
+      res = cmul(q, Z[0]);
+    else if (n > 0)
+      res = cmul(cmul(Z[m], em), q);
+    else {
+      double2 t = cmul(Z[m], eneg);
+      if (m & 1) t = make_double2(-t.x, -t.y);
+      res = cmul(t, q);
+    }
+  }
+  if (hd) {
+    double2 e1 = E[1], ei = cconj(E[1]);  // zmul, zinv
+    double2 hzk = make_double2(0.5 * zk.x, 0.5 * zk.y);
+    if (n == 0) {
+      double2 sp = cadd(e1, ei), sm = csub(e1, ei);
+      double2 u = cadd(cscale(sp, v1), cscale(make_double2(-sm.y, sm.x), v2));  // (e+ei) v1 + (e-ei) i v2
+      double2 t = cmul(cmul(cscale(Z[1], rs), hzk), u);
+      res = csub(res, cmul(d, t));
+    } else if (n > 0) {
+      double2 z7 = cmul(cscale(ei, 1.0 / rs), make_double2(-v1, v2));
+      double2 z8 = cmul(cscale(e1, rs), make_double2(v1, v2));
+      double2 t1 = cmul(make_double2(-hzk.x, -hzk.y), E[m]);  // -(zk/2) e^m
+      double2 s = cadd(cmul(Z[m - 1], z7), cmul(Z[m + 1], z8));
+      res = cadd(res, cmul(cmul(s, t1), d));
+    } else {
+      double2 z9 = cmul(cscale(e1, 1.0 / rs), make_double2(-v1, -v2));
+      double2 z10 = cmul(cscale(ei, rs), make_double2(v1, -v2));
+      double2 t2 = cmul(hzk, eneg);  // (zk/2) zinv^m (-1)^(m-1)
+      if (!(m & 1)) t2 = make_double2(-t2.x, -t2.y);
+      double2 s = cadd(cmul(Z[m - 1], z9), cmul(Z[m + 1], z10));
+      res = cadd(res, cmul(cmul(s, t2), d));
+    }
+  }
+  return res;
+}
+
+// Form expansions from sources (P2M with J, P2L with H).  Warp per box;
+// 16 sources staged at a time (tables Z and E in shared memory), then lanes
+// take coefficients n = -p..p.
+template <int ND>
+__device__ void form_from_sources(int lane, double2* Zs, double2* Es, double* Ps, int sbeg,
+                                  int send, const double2* __restrict__ xs, const HDens& D,
+                                  double2 c, double2 zk, double rs, int p, bool mpole,
+                                  double2 acc[4][ND]) {
+  const int W = p + 3;  // table width (orders 0..p+2)
+  const bool hq = D.q != nullptr, hd = D.d != nullptr;
+  for (int s0 = sbeg; s0 < send; s0 += 16) {
+    int m = min(16, send - s0);
+    __syncwarp();
+    if (lane < m) {
+      int j = s0 + lane;
+      double2 x = xs[j];
+      double dx = x.x - c.x, dy = x.y - c.y;
+      double r = sqrt(dx * dx + dy * dy);
+      double th = (dx == 0 && dy == 0) ? 0.0 : atan2(dy, dx);
+      double2 z = make_double2(zk.x * r, zk.y * r);
+      double2* Z = Zs + lane * W;
+      if (mpole)
+        jscaled(p + 1, z, rs, Z);
+      else
+        hscaled(p + 2, z, rs, Z);
+      double2 e = make_double2(cos(th), -sin(th));
+      double2* E = Es + lane * W;
+      E[0] = make_double2(1, 0);
+      for (int k = 1; k <= p + 1; k++) E[k] = cmul(E[k - 1], e);
+      double* Pp = Ps + lane * (4 * ND + 2 * ND);
+      for (int d = 0; d < ND; d++) {
+        double2 q = hq ? D.q[(size_t)j * D.nd + D.d0 + d] : make_double2(0, 0);
+        double2 dd = hd ? D.d[(size_t)j * D.nd + D.d0 + d] : make_double2(0, 0);
+        Pp[4 * d] = q.x;
+        Pp[4 * d + 1] = q.y;
+        Pp[4 * d + 2] = dd.x;
+        Pp[4 * d + 3] = dd.y;
+        Pp[4 * ND + 2 * d] = hd ? D.v[((size_t)j * 2 + 0) * D.nd + D.d0 + d] : 0.0;
+        Pp[4 * ND + 2 * d + 1] = hd ? D.v[((size_t)j * 2 + 1) * D.nd + D.d0 + d] : 0.0;
+      }
+    }
+    __syncwarp();
+    double rsd = mpole ? rs : 1.0 / rs;
+#pragma unroll
+    for (int sl = 0; sl < 4; sl++) {
+      int n = lane + 32 * sl - p;
+      if (n > p) break;
+      for (int jj = 0; jj < m; jj++) {
+        const double* Pp = Ps + jj * (4 * ND + 2 * ND);
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          double2 q = make_double2(Pp[4 * d], Pp[4 * d + 1]);
+          double2 dd = make_double2(Pp[4 * d + 2], Pp[4 * d + 3]);
+          acc[sl][d] = cadd(acc[sl][d],
+                            src_term(n, Zs + jj * W, Es + jj * W, q, dd, Pp[4 * ND + 2 * d],
+                                     Pp[4 * ND + 2 * d + 1], hq, hd, zk, rsd));
+        }
+      }
+    }
+  }
+}
+
+#define HLOOP(n)                                                                      \
+  const int lane = threadIdx.x & 31;                                                  \
+  const int wib = threadIdx.x >> 5;                                                   \
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;                                   \
+  for (int bi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; bi < (n); bi += nwarps)
+
+__device__ __forceinline__ double2* hexp(double2* base, const HLev& L, int b, int ND) {
+  return base + (L.off + (size_t)(b - L.lfirst) * L.P) * ND;
+}
+
+// step 1: P2M at leaves of levels >= 2 (zero expansions elsewhere)
+template <int ND>
+__global__ void __launch_bounds__(64) k_h_p2m(TV t, const HLev* __restrict__ lv, int nb,
+                                              const double2* __restrict__ xs, HDens D, double zkr,
+                                              double zki, double2* __restrict__ mp, int maxp) {
+  extern __shared__ double2 hsm[];
+  HLOOP(nb) {
+    int b = bi;
+    if (t.nchild[b] != 0) continue;
+    int lev = t.level[b];
+    if (lev < 2) continue;  // multipoles of levels 0 and 1 are never used
+    HLev L = lv[lev];
+    int W = L.p + 3;
+    double2* Zs = hsm + (size_t)wib * (32 * (maxp + 3) + 16 * 3 * ND);
+    double2* Es = Zs + 16 * W;
+    double* Ps = (double*)(Es + 16 * W);
+    double2 acc[4][ND];
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    int2 sr = t.srng[b];
+    if (L.ok && sr.y > sr.x)
+      form_from_sources<ND>(lane, Zs, Es, Ps, sr.x, sr.y, xs, D, t.center[b],
+                            make_double2(zkr, zki), L.rs, L.p, true, acc);
+    double2* M = hexp(mp, L, b, ND);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      int n = lane + 32 * s - L.p;
+      if (n > L.p) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) M[(n + L.p) * ND + d] = acc[s][d];
+    }
+  }
+}
+
+// step 2: P2L from list 4
+template <int ND>
+__global__ void __launch_bounds__(64) k_h_p2l(TV t, const HLev* __restrict__ lv, int first, int n,
+                                              const double2* __restrict__ xs, HDens D, double zkr,
+                                              double zki, double2* __restrict__ lo, int maxp) {
+  extern __shared__ double2 hsm[];
+  HLOOP(n) {
+    int b = first + bi;
+    int n4 = t.nl4[b];
+    if (n4 == 0 || !t.has_eval_pts(b)) continue;
+    int lev = t.level[b];
+    HLev L = lv[lev];
+    if (!L.ok) continue;
+    int W = L.p + 3;
+    double2* Zs = hsm + (size_t)wib * (32 * (maxp + 3) + 16 * 3 * ND);
+    double2* Es = Zs + 16 * W;
+    double* Ps = (double*)(Es + 16 * W);
+    double2 acc[4][ND];
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    for (int e = 0; e < n4; e++) {
+      int2 sr = t.srng[t.l4[(size_t)MNLIST4 * b + e]];
+      form_from_sources<ND>(lane, Zs, Es, Ps, sr.x, sr.y, xs, D, t.center[b],
+                            make_double2(zkr, zki), L.rs, L.p, false, acc);
+    }
+    double2* Lo = hexp(lo, L, b, ND);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      int nn = lane + 32 * s - L.p;
+      if (nn > L.p) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) Lo[(nn + L.p) * ND + d] = cadd(Lo[(nn + L.p) * ND + d], acc[s][d]);
+    }
+  }
+}
+
+// step 3: M2M, parents of one level
+template <int ND>
+__global__ void __launch_bounds__(64) k_h_m2m(TV t, const HLev* __restrict__ lv, int lev, int first,
+                                              int n, const double2* __restrict__ tabs,
+                                              double2* __restrict__ mp) {
+  extern __shared__ double2 hsm[];
+  HLev L = lv[lev], C = lv[lev + 1];
+  HLOOP(n) {
+    double2* H1s = hsm + (size_t)wib * ((2 * C.p + 1) * ND + HMAXP + 1);
+    double* R1 = (double*)(H1s + (2 * C.p + 1) * ND);  // rs1^(2e)
+    int b = first + bi;
+    if (t.nchild[b] == 0) continue;
+    double rs1 = C.rs, rs2 = L.rs;
+    for (int e = lane; e <= C.p; e += 32) R1[e] = pow(rs1, 2.0 * e);
+    double2 acc[4][ND];
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    int4 ch = t.child[b];
+    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    const int p1 = C.p, p2 = L.p, nt = L.nsh;
+    for (int q = 0; q < 4; q++) {
+      int k = cc[q];
+      if (t.srng[k].y <= t.srng[k].x) continue;
+      const double2* H1 = hexp((double2*)mp, C, k, ND);
+      __syncwarp();
+      for (int e = lane; e < (2 * p1 + 1) * ND; e += 32) H1s[e] = H1[e];
+      __syncwarp();
+      const double2* T = tabs + L.tm2m + (size_t)q * (2 * nt + 1) + nt;  // T[k], k=-nt..nt
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        int i = lane + 32 * s - p2;
+        if (i > p2) break;
+        int ai = i < 0 ? -i : i;
+        double fi = pow(rs1 / rs2, (double)ai);
+        double2 v[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
+        for (int j = -p1; j <= p1; j++) {
+          int aj = j < 0 ? -j : j;
+          bool same = (i == 0) || (j > 0 && i > 0) || (j < 0 && i < 0);
+          int e = same ? max(0, aj - ai) : aj;
+          if (i == 0) e = aj;
+          double2 tt = cscale(T[i - j], R1[e]);
+#pragma unroll
+          for (int d = 0; d < ND; d++) cfma(v[d], H1s[(j + p1) * ND + d], tt);
+        }
+#pragma unroll
+        for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], cscale(v[d], fi));
+      }
+    }
+    double2* M = hexp(mp, L, b, ND);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      int i = lane + 32 * s - p2;
+      if (i > p2) break;
+#pragma unroll
+      for (int d = 0; d < ND; d++) M[(i + p2) * ND + d] = acc[s][d];
+    }
+  }
+}
+
+// step 4: M2L over list 2 (same level: rs1 = rs2, (rs2/rs1)^|i| = 1)
+template <int ND>
+__global__ void __launch_bounds__(64) k_h_m2l(TV t, const HLev* __restrict__ lv, int first, int n,
+                                              const double2* __restrict__ tabs,
+                                              const double2* __restrict__ mp,
+                                              double2* __restrict__ lo, int maxp) {
+  extern __shared__ double2 hsm[];
+  HLOOP(n) {
+    int b = first + bi;
+    int n2 = t.nl2[b];
+    if (n2 == 0 || !t.has_eval_pts(b)) continue;
+    int lev = t.level[b];
+    HLev L = lv[lev];
+    if (!L.ok) continue;
+    const int p = L.p, np = 2 * p + 1, nt = 2 * p;
+    double2* Hs = hsm + (size_t)wib * (2 * (2 * maxp + 1) * ND);
+    double2* Hsc = Hs + np * ND;  // H(j) rs^(2|j|)
+    double rs = L.rs;
+    double2 acc1[4][ND], acc2[4][ND];
+#pragma unroll
+    for (int s = 0; s < 4; s++)
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc1[s][d] = acc2[s][d] = make_double2(0, 0);
+    double2 cb = t.center[b];
+    double rinv = 1.0 / L.bs;
+    for (int e = 0; e < n2; e++) {
+      int jb = t.l2[(size_t)MNLIST2 * b + e];
+      double2 cj = t.center[jb];
+      int ox = __double2int_rn((cb.x - cj.x) * rinv), oy = __double2int_rn((cb.y - cj.y) * rinv);
+      const double2* T = tabs + L.tm2l + (size_t)((ox + 3) * 7 + (oy + 3)) * (2 * nt + 1) + nt;
+      const double2* H = hexp((double2*)mp, L, jb, ND);
+      __syncwarp();
+      for (int k = lane; k < np * ND; k += 32) {
+        double2 h = H[k];
+        int j = k / ND - p;
+        Hs[k] = h;
+        Hsc[k] = cscale(h, pow(rs, 2.0 * (j < 0 ? -j : j)));
+      }
+      __syncwarp();
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        int i = lane + 32 * s - p;
+        if (i > p) break;
+        if (i >= 0) {
+          for (int j = -p; j <= 0; j++) {
+            double2 tt = T[i - j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hs[(j + p) * ND + d], tt);
+          }
+          for (int j = 1; j <= i; j++) {
+            double2 tt = T[i - j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hsc[(j + p) * ND + d], tt);
+          }
+          for (int j = i + 1; j <= p; j++) {
+            double2 tt = T[i - j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) cfma(acc2[s][d], Hs[(j + p) * ND + d], tt);
+          }
+        } else {
+          int m = -i;
+          for (int j = 0; j <= p; j++) {
+            double2 tt = T[i - j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hs[(j + p) * ND + d], tt);
+          }
+          for (int j = -m; j <= -1; j++) {
+            double2 tt = T[i - j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hsc[(j + p) * ND + d], tt);
+          }
+          for (int j = -p; j <= -m - 1; j++) {
+            double2 tt = T[i - j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) cfma(acc2[s][d], Hs[(j + p) * ND + d], tt);
+          }
+        }
+      }
+    }
+    double2* Lo = hexp(lo, L, b, ND);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+      int i = lane + 32 * s - p;
+      if (i > p) break;
+      double f = pow(rs, 2.0 * (i < 0 ? -i : i));
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        double2 v = cadd(acc1[s][d], cscale(acc2[s][d], f));
+        Lo[(i + p) * ND + d] = cadd(Lo[(i + p) * ND + d], v);
+      }
+    }
+  }
+}
+
+// step 5: L2L from the parents of one level
+template <int ND>
+__global__ void __launch_bounds__(64) k_h_l2l(TV t, const HLev* __restrict__ lv, int lev, int first,
+                                              int n, const double2* __restrict__ tabs,
+                                              double2* __restrict__ lo) {
+  extern __shared__ double2 hsm[];
+  HLev L = lv[lev], C = lv[lev + 1];
+  HLOOP(n) {
+    double2* J1s = hsm + (size_t)wib * ((2 * L.p + 1) * ND);
+    int b = first + bi;
+    if (t.nchild[b] == 0 || !t.has_eval_pts(b)) continue;
+    const int p1 = L.p, p2 = C.p, nt = L.nsh;
+    double rs1 = L.rs, rs2 = C.rs;
+    const double2* J1 = hexp(lo, L, b, ND);
+    __syncwarp();
+    for (int e = lane; e < (2 * p1 + 1) * ND; e += 32) J1s[e] = J1[e];
+    __syncwarp();
+    int4 ch = t.child[b];
+    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    for (int q = 0; q < 4; q++) {
+      int k = cc[q];
+      const double2* T = tabs + L.tl2l + (size_t)q * (2 * nt + 1) + nt;
+      double2* J2 = hexp(lo, C, k, ND);
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        int i = lane + 32 * s - p2;
+        if (i > p2) break;
+        int ai = i < 0 ? -i : i;
+        double A = pow(rs2 / rs1, (double)ai), Cf = pow(rs1 * rs2, (double)ai);
+        double2 v[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
+        for (int j = -p1; j <= p1; j++) {
+          int aj = j < 0 ? -j : j;
+          bool same = (j > 0 && i > 0) || (j < 0 && i < 0);
+          double f;
+          if (i == 0)
+            f = 1.0;
+          else if (!same)
+            f = Cf;
+          else
+            f = A * pow(rs1, 2.0 * max(0, ai - aj));
+          double2 tt = cscale(T[i - j], f);
+#pragma unroll
+          for (int d = 0; d < ND; d++) cfma(v[d], J1s[(j + p1) * ND + d], tt);
+        }
+#pragma unroll
+        for (int d = 0; d < ND; d++) J2[(i + p2) * ND + d] = cadd(J2[(i + p2) * ND + d], v[d]);
+      }
+    }
+  }
+}
+
+// Derivative expansions of an expansion E of order p (mk_mpoleg / mk_mpoleh,
+// helmrouts2d.f): X, Y of order p+1 and XX, XY, YY of order p+2, scale s.
+template <int ND>
+__device__ void derivative_exps(int lane, const double2* E, int p, double2 zk, double s,
+                                double2* X, double2* Y, double2* XX, double2* XY, double2* YY,
+                                int ifpgh) {
+  double2 s1 = cscale(zk, 0.5 / s), s2 = cscale(zk, 0.5 * s);
+  double2 s3 = make_double2(-s1.y, s1.x), s4 = make_double2(-s2.y, s2.x);  // times i
+  // X(n), n = -(p+1)..p+1: contributions from E(n+1) and E(n-1)
+  auto Ev = [&](int n, int d) {
+    return (n >= -p && n <= p) ? E[(n + p) * ND + d] : make_double2(0, 0);
+  };
+  for (int k = lane; k < (2 * p + 3) * ND; k += 32) {
+    int n = k / ND - (p + 1), d = k % ND;
+    double2 x = make_double2(0, 0), y = make_double2(0, 0);
+    // from E(m) with m = n+1 (E(m) adds to index m-1 = n): m >= 1 -> s2/s4,
+    // m == 0 -> s1/s3 (to -1), m <= -1 -> s1/s3
+    int m = n + 1;
+    double2 em = Ev(m, d);
+    if (m >= 1) {
+      x = cadd(x, cmul(s2, em));
+      y = cadd(y, cmul(s4, em));
+    } else {
+      x = cadd(x, cmul(s1, em));
+      y = cadd(y, cmul(s3, em));
+    }
+    // from E(m) with m = n-1 (adds to index m+1 = n): m >= 0 -> -s1 / +s3,
+    // m <= -1 -> -s2 / +s4
+    m = n - 1;
+    em = Ev(m, d);
+    if (m >= 0) {
+      x = csub(x, cmul(s1, em));
+      y = cadd(y, cmul(s3, em));
+    } else {
+      x = csub(x, cmul(s2, em));
+      y = cadd(y, cmul(s4, em));
+    }
+    X[k] = x;
+    Y[k] = y;
+  }
+  if (ifpgh < 3) return;
+  __syncwarp();
+  int q = p + 1;
+  auto Xv = [&](int n, int d) {
+    return (n >= -q && n <= q) ? X[(n + q) * ND + d] : make_double2(0, 0);
+  };
+  auto Yv = [&](int n, int d) {
+    return (n >= -q && n <= q) ? Y[(n + q) * ND + d] : make_double2(0, 0);
+  };
+  for (int k = lane; k < (2 * p + 5) * ND; k += 32) {
+    int n = k / ND - (p + 2), d = k % ND;
+    double2 xx = make_double2(0, 0), xy = make_double2(0, 0), yy = make_double2(0, 0);
+    int m = n + 1;
+    double2 ex = Xv(m, d), ey = Yv(m, d);
+    if (m >= 1) {
+      xx = cadd(xx, cmul(s2, ex));
+      xy = cadd(xy, cmul(s4, ex));
+      yy = cadd(yy, cmul(s4, ey));
+    } else {
+      xx = cadd(xx, cmul(s1, ex));
+      xy = cadd(xy, cmul(s3, ex));
+      yy = cadd(yy, cmul(s3, ey));
+    }
+    m = n - 1;
+    ex = Xv(m, d);
+    ey = Yv(m, d);
+    if (m >= 0) {
+      xx = csub(xx, cmul(s1, ex));
+      xy = cadd(xy, cmul(s3, ex));
+      yy = cadd(yy, cmul(s3, ey));
+    } else {
+      xx = csub(xx, cmul(s2, ex));
+      xy = cadd(xy, cmul(s4, ex));
+      yy = cadd(yy, cmul(s4, ey));
+    }
+    XX[k] = xx;
+    XY[k] = xy;
+    YY[k] = yy;
+  }
+}
+
+// sum_n E(n) mt(n), mt(0) = (i/4) Z_0, mt(+-n) = (i/4) Z_n (e^{i th})^n,
+// (i/4) Z_n (-e^{-i th})^n (mpole_evalp, helmrouts2d.f:1493-1530).
+template <int ND>
+__device__ __forceinline__ void eval_sum(const double2* E, int q, const double2* Z, double2 ep,
+                                         double2 out[ND]) {
+  double2 i4 = make_double2(0.0, 0.25);
+  double2 m0 = cmul(Z[0], i4);
+#pragma unroll
+  for (int d = 0; d < ND; d++) out[d] = cadd(out[d], cmul(E[q * ND + d], m0));
+  double2 a = cmul(ep, i4), bneg = make_double2(-ep.x, ep.y);  // -exp(-i theta)
+  double2 b = cmul(bneg, i4);  // (-e^{-i th}) i/4
+  for (int n = 1; n <= q; n++) {
+    double2 tp = cmul(a, Z[n]), tm = cmul(b, Z[n]);
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      out[d] = cadd(out[d], cmul(E[(q + n) * ND + d], tp));
+      out[d] = cadd(out[d], cmul(E[(q - n) * ND + d], tm));
+    }
+    a = cmul(a, ep);
+    b = cmul(b, bneg);
+  }
+}
+
+// Pair term of the near field (helmkernels2d.f h2d_directcdh, cdg, ...).
+template <int ND, int IFPGH>
+__device__ __forceinline__ void h_pair(double xd, double yd, double2 zk, const double2* q,
+                                       const double2* dd, const double* v, bool hq, bool hd,
+                                       double2 pot[ND], double2 g1[ND], double2 g2[ND],
+                                       double2 hh[ND][3]) {
+  double rr = xd * xd + yd * yd, r = sqrt(rr);
+  double2 z = make_double2(zk.x * r, zk.y * r);
+  double2 h0, h1;
+  helm::hank01(z, h0, h1);
+  const double2 i4 = make_double2(0, 0.25);
+  double ir = 1.0 / r;
+  double ct = xd * ir, st = yd * ir;
+  double2 zki4 = cmul(zk, i4);
+  if (hq) {
+    double2 cdd = cscale(cmul(h1, zki4), -ir);  // -h1 zk i/4 / r
+    double2 h2z = csub(cscale(h1, 2.0), cmul(z, h0));
+    double2 chs = cscale(zki4, ir / rr);
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      pot[d] = cadd(pot[d], cmul(cmul(h0, i4), q[d]));
+      if (IFPGH >= 2) {
+        double2 c = cmul(cdd, q[d]);
+        g1[d] = cadd(g1[d], cscale(c, xd));
+        g2[d] = cadd(g2[d], cscale(c, yd));
+      }
+      if (IFPGH >= 3) {
+        double2 c = cmul(chs, q[d]);
+        hh[d][0] = cadd(hh[d][0], cmul(c, csub(cscale(h2z, xd * xd), cscale(h1, rr))));
+        hh[d][1] = cadd(hh[d][1], cmul(c, cscale(h2z, xd * yd)));
+        hh[d][2] = cadd(hh[d][2], cmul(c, csub(cscale(h2z, yd * yd), cscale(h1, rr))));
+      }
+    }
+  }
+  if (hd) {
+    double2 zi = crcp(z);
+    double2 h2 = csub(cscale(cmul(h1, zi), 2.0), h0);
+    double2 cdd = cscale(cmul(h1, zki4), ir);      // h1 / r zk i/4
+    double2 cdd2 = cmul(cmul(zk, zk), make_double2(0, -0.25));  // -zk^2 i/4
+    double2 f1 = csub(cscale(h2, ct * ct - 0.5), cscale(h0, 0.5));
+    double2 f2 = cscale(h2, ct * st);
+    double2 f3 = csub(cscale(h2, st * st - 0.5), cscale(h0, 0.5));
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      double v1 = v[2 * d], v2 = v[2 * d + 1];
+      pot[d] = cadd(pot[d], cscale(cmul(cdd, dd[d]), xd * v1 + yd * v2));
+      if (IFPGH >= 2) {
+        double2 c = cmul(cdd2, dd[d]);
+        double2 hxx = cmul(c, f1), hxy = cmul(c, f2), hyy = cmul(c, f3);
+        g1[d] = cadd(g1[d], cadd(cscale(hxx, v1), cscale(hxy, v2)));
+        g2[d] = cadd(g2[d], cadd(cscale(hxy, v1), cscale(hyy, v2)));
+      }
+      if (IFPGH >= 3) {
+        double2 h3 = csub(cscale(cmul(h2, zi), 4.0), h1);
+        double2 a1 = cscale(csub(cscale(h1, 0.75), cscale(h3, 0.5 * (ct * ct - 0.5 - st * st))), ct);
+        double2 a2 = cscale(csub(cscale(h1, 0.25), cscale(h3, 0.5 * (1.5 * ct * ct - 0.5 * st * st))), st);
+        double2 a3 = cscale(csub(cscale(h1, 0.25), cscale(h3, 0.5 * (1.5 * st * st - 0.5 * ct * ct))), ct);
+        double2 a4 = cscale(csub(cscale(h1, 0.75), cscale(h3, 0.5 * (st * st - 0.5 - ct * ct))), st);
+        double2 c3 = cmul(cmul(cmul(zk, zk), zk), make_double2(0, -0.25));
+        double2 c = cmul(c3, dd[d]);
+        hh[d][0] = cadd(hh[d][0], cmul(c, cadd(cscale(a1, v1), cscale(a2, v2))));
+        hh[d][1] = cadd(hh[d][1], cmul(c, cadd(cscale(a2, v1), cscale(a3, v2))));
+        hh[d][2] = cadd(hh[d][2], cmul(c, cadd(cscale(a3, v1), cscale(a4, v2))));
+      }
+    }
+  }
+}
+
+// steps 6-8 fused per leaf: L2P (J tables), M2P (H tables) and P2P for 32
+// evaluation points at a time; one result write per point (tree order).
+template <int ND, int IFPGH>
+__global__ void __launch_bounds__(64) k_h_leaf(TV t, const HLev* __restrict__ lv, int nb,
+                                               int use_targets, const double2* __restrict__ xs,
+                                               const double2* __restrict__ xe, HDens D,
+                                               double zkr, double zki, const double2* __restrict__ mp,
+                                               const double2* __restrict__ lo, double thresh,
+                                               int ifnear, double2* __restrict__ pot,
+                                               double2* __restrict__ grad,
+                                               double2* __restrict__ hess, int maxp) {
+  extern __shared__ double2 hsm[];
+  const double2 zk = make_double2(zkr, zki);
+  const int ES = (2 * maxp + 1) + 2 * (2 * maxp + 3) + 3 * (2 * maxp + 5);
+  HLOOP(nb) {
+    double2* E = hsm + (size_t)wib * (ES * ND + 32 * (1 + 3 * ND));
+    double2* X = E + (2 * maxp + 1) * ND;
+    double2* Y = X + (2 * maxp + 3) * ND;
+    double2* XX = Y + (2 * maxp + 3) * ND;
+    double2* XY = XX + (2 * maxp + 5) * ND;
+    double2* YY = XY + (2 * maxp + 5) * ND;
+    double2* SX = YY + (2 * maxp + 5) * ND;  // staged sources
+    double2* SQ = SX + 32;
+    double2* SD = SQ + 32 * ND;
+    double* SV = (double*)(SD + 32 * ND);  // 2 ND doubles per staged source
+    int b = bi;
+    if (t.nchild[b] != 0) continue;
+    int2 er = use_targets ? t.trng[b] : t.srng[b];
+    if (er.y <= er.x) continue;
+    int lev = t.level[b];
+    HLev L = lv[lev];
+    double2 cb = t.center[b];
+    int n3 = t.nl3[b], n1 = ifnear ? t.nl1[b] : 0;
+    double2 Zt[HMAXP + 4];
+    for (int k0 = er.x; k0 < er.y; k0 += 32) {
+      int k = k0 + lane;
+      bool act = k < er.y;
+      double2 z = act ? xe[k] : cb;
+      double2 po[ND], g1[ND], g2[ND], hh[ND][3];
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        po[d] = g1[d] = g2[d] = make_double2(0, 0);
+        hh[d][0] = hh[d][1] = hh[d][2] = make_double2(0, 0);
+      }
+      // L2P: local of the leaf with J tables, derivatives via rs^-1 expansions
+      // (local expansions of levels 0 and 1 are zero)
+      if (L.ok && lev >= 2) {
+        int p = L.p;
+        __syncwarp();
+        const double2* Lb = hexp((double2*)lo, L, b, ND);
+        for (int e = lane; e < (2 * p + 1) * ND; e += 32) E[e] = Lb[e];
+        __syncwarp();
+        if (IFPGH >= 2) derivative_exps<ND>(lane, E, p, zk, 1.0 / L.rs, X, Y, XX, XY, YY, IFPGH);
+        __syncwarp();
+        double dx = z.x - cb.x, dy = z.y - cb.y;
+        double r = sqrt(dx * dx + dy * dy), th = (dx == 0 && dy == 0) ? 0.0 : atan2(dy, dx);
+        jscaled(p + 3, make_double2(zk.x * r, zk.y * r), L.rs, Zt);
+        double2 ep = make_double2(cos(th), sin(th));
+        eval_sum<ND>(E, p, Zt, ep, po);
+        if (IFPGH >= 2) {
+          eval_sum<ND>(X, p + 1, Zt, ep, g1);
+          eval_sum<ND>(Y, p + 1, Zt, ep, g2);
+        }
+        if (IFPGH >= 3) {
+          double2 t0[ND], t1[ND], t2[ND];
+#pragma unroll
+          for (int d = 0; d < ND; d++) t0[d] = t1[d] = t2[d] = make_double2(0, 0);
+          eval_sum<ND>(XX, p + 2, Zt, ep, t0);
+          eval_sum<ND>(XY, p + 2, Zt, ep, t1);
+          eval_sum<ND>(YY, p + 2, Zt, ep, t2);
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            hh[d][0] = cadd(hh[d][0], t0[d]);
+            hh[d][1] = cadd(hh[d][1], t1[d]);
+            hh[d][2] = cadd(hh[d][2], t2[d]);
+          }
+        }
+      }
+      // M2P from list 3 (boxes of level lev+1)
+      for (int e = 0; e < n3; e++) {
+        HLev C = lv[lev + 1];
+        if (!C.ok) break;
+        int jb = t.l3[(size_t)MNLIST3 * b + e];
+        int p = C.p;
+        __syncwarp();
+        const double2* Mb = hexp((double2*)mp, C, jb, ND);
+        for (int q = lane; q < (2 * p + 1) * ND; q += 32) E[q] = Mb[q];
+        __syncwarp();
+        if (IFPGH >= 2) derivative_exps<ND>(lane, E, p, zk, C.rs, X, Y, XX, XY, YY, IFPGH);
+        __syncwarp();
+        double2 cj = t.center[jb];
+        double dx = z.x - cj.x, dy = z.y - cj.y;
+        double r = sqrt(dx * dx + dy * dy), th = (dx == 0 && dy == 0) ? 0.0 : atan2(dy, dx);
+        hscaled(p + 3, make_double2(zk.x * r, zk.y * r), C.rs, Zt);
+        double2 ep = make_double2(cos(th), sin(th));
+        eval_sum<ND>(E, p, Zt, ep, po);
+        if (IFPGH >= 2) {
+          eval_sum<ND>(X, p + 1, Zt, ep, g1);
+          eval_sum<ND>(Y, p + 1, Zt, ep, g2);
+        }
+        if (IFPGH >= 3) {
+          double2 t0[ND], t1[ND], t2[ND];
+#pragma unroll
+          for (int d = 0; d < ND; d++) t0[d] = t1[d] = t2[d] = make_double2(0, 0);
+          eval_sum<ND>(XX, p + 2, Zt, ep, t0);
+          eval_sum<ND>(XY, p + 2, Zt, ep, t1);
+          eval_sum<ND>(YY, p + 2, Zt, ep, t2);
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            hh[d][0] = cadd(hh[d][0], t0[d]);
+            hh[d][1] = cadd(hh[d][1], t1[d]);
+            hh[d][2] = cadd(hh[d][2], t2[d]);
+          }
+        }
+      }
+      // P2P from list 1
+      const bool hq = D.q != nullptr, hd = D.d != nullptr;
+      for (int e = 0; e < n1; e++) {
+        int jb = t.l1[(size_t)MNLIST1 * b + e];
+        int2 sr = t.srng[jb];
+        for (int s0 = sr.x; s0 < sr.y; s0 += 32) {
+          int ns = min(32, sr.y - s0);
+          __syncwarp();
+          if (lane < ns) {
+            int j = s0 + lane;
+            SX[lane] = xs[j];
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              if (hq) SQ[lane * ND + d] = D.q[(size_t)j * D.nd + D.d0 + d];
+              if (hd) {
+                SD[lane * ND + d] = D.d[(size_t)j * D.nd + D.d0 + d];
+                SV[lane * 2 * ND + 2 * d] = D.v[((size_t)j * 2 + 0) * D.nd + D.d0 + d];
+                SV[lane * 2 * ND + 2 * d + 1] = D.v[((size_t)j * 2 + 1) * D.nd + D.d0 + d];
+              }
+            }
+          }
+          __syncwarp();
+          if (act) {
+            for (int jj = 0; jj < ns; jj++) {
+              double2 y = SX[jj];
+              double xd = z.x - y.x, yd = z.y - y.y;
+              double az = hypot(zk.x, zk.y) * sqrt(xd * xd + yd * yd);
+              // helmkernels2d.f: <= for the charge potential-only kernel, < otherwise
+              bool le = (IFPGH == 1) && hq && !hd;
+              if (le ? (az <= thresh) : (az < thresh)) continue;
+              h_pair<ND, IFPGH>(xd, yd, zk, SQ + jj * ND, SD + jj * ND, SV + jj * 2 * ND, hq, hd,
+                                po, g1, g2, hh);
+            }
+          }
+        }
+      }
+      if (act) {
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          pot[(size_t)k * D.nd + D.d0 + d] = po[d];
+          if (IFPGH >= 2) {
+            grad[((size_t)k * 2 + 0) * D.nd + D.d0 + d] = g1[d];
+            grad[((size_t)k * 2 + 1) * D.nd + D.d0 + d] = g2[d];
+          }
+          if (IFPGH >= 3)
+            for (int c = 0; c < 3; c++) hess[((size_t)k * 3 + c) * D.nd + D.d0 + d] = hh[d][c];
+        }
+      }
+    }
+  }
+}
+
+__global__ void k_h_gather(const double* __restrict__ xy, const int* __restrict__ perm, long n,
+                           int nd, const double* __restrict__ charge,
+                           const double* __restrict__ dipstr, const double* __restrict__ dipvec,
+                           double2* __restrict__ xs, double2* __restrict__ qs,
+                           double2* __restrict__ ds, double* __restrict__ vs) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  size_t i = perm[k];
+  xs[k] = make_double2(xy[2 * i], xy[2 * i + 1]);
+  for (int d = 0; d < nd; d++) {
+    if (qs) qs[k * nd + d] = ((const double2*)charge)[i * nd + d];
+    if (ds) {
+      ds[k * nd + d] = ((const double2*)dipstr)[i * nd + d];
+      vs[(k * 2 + 0) * nd + d] = dipvec[(i * 2 + 0) * nd + d];
+      vs[(k * 2 + 1) * nd + d] = dipvec[(i * 2 + 1) * nd + d];
+    }
+  }
+}
+
+__global__ void k_h_unpack(const int* __restrict__ perm, long n, int w,
+                           const double2* __restrict__ in, double2* __restrict__ out) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  size_t i = perm[k];
+  for (int c = 0; c < w; c++) out[i * w + c] = in[k * w + c];
+}
+
+// direct sums
+template <int IFPGH>
+__global__ void __launch_bounds__(128) k_h_direct(int nd, int d, long ns, const double* __restrict__ src,
+                                                 const double* __restrict__ charge,
+                                                 const double* __restrict__ dipstr,
+                                                 const double* __restrict__ dipvec, long nt,
+                                                 const double* __restrict__ trg, double zkr,
+                                                 double zki, double thresh, long chunk,
+                                                 double2* __restrict__ part) {
+  __shared__ double sx[128], sy[128], sv[256];
+  __shared__ double2 sq[128], sd[128];
+  long tix = blockIdx.x * 128L + threadIdx.x;
+  bool act = tix < nt;
+  double x = act ? trg[2 * tix] : 0, y = act ? trg[2 * tix + 1] : 0;
+  double2 po[1] = {make_double2(0, 0)}, g1[1] = {make_double2(0, 0)}, g2[1] = {make_double2(0, 0)};
+  double2 hh[1][3] = {{make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)}};
+  long s0 = blockIdx.y * chunk, s1 = min(ns, s0 + chunk);
+  bool hq = charge != nullptr, hd = dipstr != nullptr;
+  double2 zk = make_double2(zkr, zki);
+  double azk = hypot(zkr, zki);
+  for (long b0 = s0; b0 < s1; b0 += 128) {
+    __syncthreads();
+    long j = b0 + threadIdx.x;
+    if (j < s1) {
+      sx[threadIdx.x] = src[2 * j];
+      sy[threadIdx.x] = src[2 * j + 1];
+      if (hq) sq[threadIdx.x] = ((const double2*)charge)[j * nd + d];
+      if (hd) {
+        sd[threadIdx.x] = ((const double2*)dipstr)[j * nd + d];
+        sv[2 * threadIdx.x] = dipvec[(j * 2 + 0) * nd + d];
+        sv[2 * threadIdx.x + 1] = dipvec[(j * 2 + 1) * nd + d];
+      }
+    }
+    __syncthreads();
+    int m = (int)min(128L, s1 - b0);
+    if (act)
+      for (int i = 0; i < m; i++) {
+        double xd = x - sx[i], yd = y - sy[i];
+        double az = azk * sqrt(xd * xd + yd * yd);
+        bool le = (IFPGH == 1) && hq && !hd;
+        if (le ? (az <= thresh) : (az < thresh)) continue;
+        h_pair<1, IFPGH>(xd, yd, zk, &sq[i], &sd[i], &sv[2 * i], hq, hd, po, g1, g2, hh);
+      }
+  }
+  if (act) {
+    double2* o = part + ((size_t)blockIdx.y * nt + tix) * 6;
+    o[0] = po[0];
+    o[1] = g1[0];
+    o[2] = g2[0];
+    o[3] = hh[0][0];
+    o[4] = hh[0][1];
+    o[5] = hh[0][2];
+  }
+}
+
+__global__ void k_h_direct_reduce(int nd, int d, long nt, int nslice, int ifpgh,
+                                  const double2* __restrict__ part, double2* pot, double2* grad,
+                                  double2* hess) {
+  long tix = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (tix >= nt) return;
+  double2 o[6];
+  for (int c = 0; c < 6; c++) o[c] = make_double2(0, 0);
+  for (int s = 0; s < nslice; s++)
+    for (int c = 0; c < 6; c++) o[c] = cadd(o[c], part[((size_t)s * nt + tix) * 6 + c]);
+  pot[tix * nd + d] = o[0];
+  if (ifpgh >= 2) {
+    grad[(tix * 2 + 0) * nd + d] = o[1];
+    grad[(tix * 2 + 1) * nd + d] = o[2];
+  }
+  if (ifpgh >= 3)
+    for (int c = 0; c < 3; c++) hess[(tix * 3 + c) * nd + d] = o[3 + c];
+}
+
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024)
+    B2_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
+int grid_w(long nitems, int wpb) {
+  long blocks = (nitems + wpb - 1) / wpb;
+  return (int)std::max(1L, std::min(blocks, 148L * 32));
+}
+
+template <int ND>
+void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
+                const HLev* dlv, const std::vector<HLev>& hl, int maxp, const double2* tabs,
+                const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
+                double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, double thresh,
+                cudaStream_t st, cudaEvent_t* ev) {
+  const int nb = T.nboxes, nl = T.nlevels;
+  B2_CHECK(cudaEventRecord(ev[0], st));
+  size_t sm_form = sizeof(double2) * 2 * (32 * (size_t)(maxp + 3) + 16 * 3 * ND);
+  set_smem(k_h_p2m<ND>, sm_form);
+  set_smem(k_h_p2l<ND>, sm_form);
+  k_h_p2m<ND><<<grid_w(nb, 2), 64, sm_form, st>>>(tv, dlv, nb, xs, D, a.zkr, a.zki, mp, maxp);
+  B2_LAUNCH_CHECK();
+  B2_CHECK(cudaEventRecord(ev[1], st));
+  for (int l = nl - 1; l >= 2; l--) {
+    if (!hl[l].ok) continue;
+    int f = T.lfirst[l], n = T.llast[l] - f + 1;
+    size_t sm = sizeof(double2) * 2 * ((2 * hl[l + 1].p + 1) * ND + HMAXP + 1);
+    set_smem(k_h_m2m<ND>, sm);
+    k_h_m2m<ND><<<grid_w(n, 2), 64, sm, st>>>(tv, dlv, l, f, n, tabs, mp);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[2], st));
+  if (nl >= 2) {
+    int f = T.lfirst[2], n = nb - f;
+    k_h_p2l<ND><<<grid_w(n, 2), 64, sm_form, st>>>(tv, dlv, f, n, xs, D, a.zkr, a.zki, lo, maxp);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[3], st));
+  if (nl >= 2) {
+    int f = T.lfirst[2], n = nb - f;
+    size_t sm = sizeof(double2) * 2 * (2 * (2 * maxp + 1) * ND);
+    set_smem(k_h_m2l<ND>, sm);
+    k_h_m2l<ND><<<grid_w(n, 2), 64, sm, st>>>(tv, dlv, f, n, tabs, mp, lo, maxp);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[4], st));
+  for (int l = 2; l <= nl - 1; l++) {
+    if (!hl[l].ok) continue;
+    int f = T.lfirst[l], n = T.llast[l] - f + 1;
+    size_t sm = sizeof(double2) * 2 * ((2 * hl[l].p + 1) * ND);
+    set_smem(k_h_l2l<ND>, sm);
+    k_h_l2l<ND><<<grid_w(n, 2), 64, sm, st>>>(tv, dlv, l, f, n, tabs, lo);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[5], st));
+  const int ES = (2 * maxp + 1) + 2 * (2 * maxp + 3) + 3 * (2 * maxp + 5);
+  size_t sm_leaf = sizeof(double2) * 2 * (ES * ND + 32 * (1 + 3 * ND));
+  auto leaf = [&](int use_t, int ifl, const double2* xe, double2* po, double2* gr, double2* he) {
+    if (ifl <= 0) return;
+    if (ifl == 1) {
+      set_smem(k_h_leaf<ND, 1>, sm_leaf);
+      k_h_leaf<ND, 1><<<grid_w(nb, 2), 64, sm_leaf, st>>>(tv, dlv, nb, use_t, xs, xe, D, a.zkr, a.zki,
+                                                         mp, lo, thresh, a.ifnear, po, gr, he, maxp);
+    } else if (ifl == 2) {
+      set_smem(k_h_leaf<ND, 2>, sm_leaf);
+      k_h_leaf<ND, 2><<<grid_w(nb, 2), 64, sm_leaf, st>>>(tv, dlv, nb, use_t, xs, xe, D, a.zkr, a.zki,
+                                                         mp, lo, thresh, a.ifnear, po, gr, he, maxp);
+    } else {
+      set_smem(k_h_leaf<ND, 3>, sm_leaf);
+      k_h_leaf<ND, 3><<<grid_w(nb, 2), 64, sm_leaf, st>>>(tv, dlv, nb, use_t, xs, xe, D, a.zkr, a.zki,
+                                                         mp, lo, thresh, a.ifnear, po, gr, he, maxp);
+    }
+    B2_LAUNCH_CHECK();
+  };
+  leaf(0, a.ifpgh, xs, ps, gs, hs);
+  leaf(1, a.ifpghtarg, xt, pt, gt, ht);
+  B2_CHECK(cudaEventRecord(ev[6], st));
+}
+
+}  // namespace
+
+int helm_nterms(double bsize, double zkr, double zki, double eps, int* ier) {
+  // h2dterms: first j with (|J_j H_j| + |J_(j-1) H_(j-1)|) |H_0| < eps (|J_0 H_0| + |J_1 H_1|)
+  const double pi2 = 8 * std::atan(1.0);
+  double2 zb = make_double2(zkr * bsize, zki * bsize);
+  double rscale = 1.0;
+  if (std::hypot(zb.x, zb.y) < pi2) rscale = std::hypot(zb.x, zb.y);
+  const int NT = 400;
+  std::vector<double2> hf(NT + 1), jf(NT + 1);
+  helm::hscaled(NT, make_double2(1.5 * zb.x, 1.5 * zb.y), rscale, hf.data());
+  double c = std::sqrt(2.0) / 2.0;
+  helm::jscaled(NT, make_double2(c * zb.x, c * zb.y), rscale, jf.data());
+  auto ab = [](double2 a, double2 b) { double2 m = cmul(a, b); return std::hypot(m.x, m.y); };
+  double x0 = ab(jf[0], hf[0]) + ab(jf[1], hf[1]);
+  double h0 = std::hypot(hf[0].x, hf[0].y);
+  for (int j = 2; j <= NT; j++) {
+    double v = (ab(jf[j], hf[j]) + ab(jf[j - 1], hf[j - 1])) * h0;
+    if (v < eps * x0) return j + 1;
+  }
+  *ier = IER_NTERMS;
+  return 10001;
+}
+
+int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
+  if (a.nd < 1 || a.ns < 0 || a.nt < 0 || a.ifpgh < 0 || a.ifpgh > 3 || a.ifpghtarg < 0 ||
+      a.ifpghtarg > 3 || a.ns > (1L << 30) || a.nt > (1L << 30))
+    return IER_BADARG;
+  if (a.ns > 0 && !a.src) return IER_BADARG;
+  if (a.nt > 0 && a.ifpghtarg > 0 && !a.trg) return IER_BADARG;
+  if (a.dipstr && !a.dipvec) return IER_BADARG;
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  configure_mempool(dev);
+  ensure_device_tables();
+  const int nd = a.nd;
+  const long ns = a.ns, nt = a.ifpghtarg > 0 ? a.nt : 0;
+  const bool fc = a.charge != nullptr, fd = a.dipstr != nullptr;
+  if (a.timeinfo)
+    for (int i = 0; i < 8; i++) a.timeinfo[i] = 0;
+  auto zero_outputs = [&]() {
+    if (a.ifpgh >= 1 && ns) B2_CHECK(cudaMemsetAsync(a.pot, 0, sizeof(double2) * nd * ns, st));
+    if (a.ifpgh >= 2 && ns) B2_CHECK(cudaMemsetAsync(a.grad, 0, sizeof(double2) * 2 * nd * ns, st));
+    if (a.ifpgh >= 3 && ns) B2_CHECK(cudaMemsetAsync(a.hess, 0, sizeof(double2) * 3 * nd * ns, st));
+    if (a.ifpghtarg >= 1 && nt) B2_CHECK(cudaMemsetAsync(a.pottarg, 0, sizeof(double2) * nd * nt, st));
+    if (a.ifpghtarg >= 2 && nt) B2_CHECK(cudaMemsetAsync(a.gradtarg, 0, sizeof(double2) * 2 * nd * nt, st));
+    if (a.ifpghtarg >= 3 && nt) B2_CHECK(cudaMemsetAsync(a.hesstarg, 0, sizeof(double2) * 3 * nd * nt, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+  };
+  if (ns == 0 || (!fc && !fd)) {
+    zero_outputs();
+    return IER_OK;
+  }
+  int ndiv = a.ndiv > 0 ? a.ndiv : lap_ndiv(a.eps);  // hndiv2d.f: same table as lndiv2d
+  if (ndiv <= 0) ndiv = (int)std::min<long>(ns + nt, 1L << 30);
+  DeviceTree T;
+  build_device_tree(T, a.src, ns, a.trg, nt, 0, ndiv, NLMAX, st);
+  if (T.bs0 == 0.0) {
+    zero_outputs();
+    return IER_OK;
+  }
+  const int nl = T.nlevels;
+  const double pi = 4 * std::atan(1.0);
+  const double zkabs = std::hypot(a.zkr, a.zki);
+  // per-level order and scale (hfmm2d.f:317-326), high-frequency test
+  // (hfmm2d.f:1001-1013): box > 16 wavelengths needs the wideband path
+  std::vector<HLev> hl(nl + 1);
+  int maxp = 0, ier = 0;
+  for (int l = 0; l <= nl; l++) {
+    double bs = T.boxsize[l];
+    hl[l].lfirst = T.lfirst[l];
+    hl[l].rs = std::min(zkabs * bs / (2.0 * pi), 1.0);
+    hl[l].bs = bs;
+    hl[l].p = helm_nterms(bs, a.zkr, a.zki, a.eps, &ier);
+    hl[l].P = 2 * hl[l].p + 1;
+    hl[l].ok = (a.zki * bs < 40.0) ? 1 : 0;
+    if (hl[l].ok && l >= 1 && bs / (1.0 / (a.zkr / (2.0 * pi))) > 16.0) return IER_HIGHFREQ;
+    if (l >= 2) maxp = std::max(maxp, hl[l].p);
+  }
+  if (ier) return ier;
+  if (maxp > HMAXP) return IER_NTERMS;
+  // expansion and table layout
+  long off = 0, toff = 0;
+  for (int l = 0; l <= nl; l++) {
+    hl[l].off = off;
+    off += (long)(T.llast[l] - T.lfirst[l] + 1) * hl[l].P;
+    hl[l].nsh = l < nl ? hl[l].p + hl[l + 1].p : 0;
+    hl[l].tm2l = toff;
+    if (l >= 2) toff += 49L * (4 * hl[l].p + 1);
+    hl[l].tm2m = toff;
+    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
+    hl[l].tl2l = toff;
+    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
+  }
+  DBuf<HLev> dlv(st);
+  dlv.alloc(nl + 1, st);
+  B2_CHECK(cudaMemcpyAsync(dlv.p, hl.data(), sizeof(HLev) * (nl + 1), cudaMemcpyHostToDevice, st));
+  DBuf<double2> tabs(st), scratch(st);
+  tabs.alloc(std::max(toff, 1L), st);
+  const int nthreads = (nl + 1) * 57, sstride = 2 * (2 * HMAXP) + 8;
+  scratch.alloc((size_t)nthreads * sstride, st);
+  k_h_tables<<<ceil_div(nthreads, 64), 64, 0, st>>>(dlv.p, nl, a.zkr, a.zki, tabs.p, scratch.p, sstride);
+  B2_LAUNCH_CHECK();
+  std::vector<double> bsx(T.boxsize);
+  bsx.push_back(T.boxsize.back() / 2);
+  DBuf<double> dbs(st);
+  dbs.alloc(bsx.size(), st);
+  B2_CHECK(cudaMemcpyAsync(dbs.p, bsx.data(), sizeof(double) * bsx.size(), cudaMemcpyHostToDevice, st));
+  // sorted inputs
+  DBuf<double2> xs(st), xt(st), qs(st), ds(st);
+  DBuf<double> vs(st);
+  xs.alloc(ns, st);
+  if (fc) qs.alloc((size_t)ns * nd, st);
+  if (fd) {
+    ds.alloc((size_t)ns * nd, st);
+    vs.alloc((size_t)ns * 2 * nd, st);
+  }
+  k_h_gather<<<ceil_div(ns, 256), 256, 0, st>>>(a.src, T.isrc.p, ns, nd, a.charge, a.dipstr,
+                                               a.dipvec, xs.p, qs.p, ds.p, vs.p);
+  B2_LAUNCH_CHECK();
+  if (nt > 0) {
+    xt.alloc(nt, st);
+    k_h_gather<<<ceil_div(nt, 256), 256, 0, st>>>(a.trg, T.itarg.p, nt, 0, nullptr, nullptr,
+                                                 nullptr, xt.p, nullptr, nullptr, nullptr);
+    B2_LAUNCH_CHECK();
+  }
+  DBuf<double2> ps(st), gs(st), hs(st), pt(st), gt(st), ht(st);
+  if (a.ifpgh >= 1) ps.alloc((size_t)ns * nd, st);
+  if (a.ifpgh >= 2) gs.alloc((size_t)ns * 2 * nd, st);
+  if (a.ifpgh >= 3) hs.alloc((size_t)ns * 3 * nd, st);
+  if (a.ifpghtarg >= 1 && nt) pt.alloc((size_t)nt * nd, st);
+  if (a.ifpghtarg >= 2 && nt) gt.alloc((size_t)nt * 2 * nd, st);
+  if (a.ifpghtarg >= 3 && nt) ht.alloc((size_t)nt * 3 * nd, st);
+  TV tv{T.center.p, T.level.p, T.nchild.p, T.child.p, T.srng.p, T.trng.p, T.nlist1.p, T.list1.p,
+        T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p, dbs.p, a.ifpgh,
+        nt > 0 ? a.ifpghtarg : 0};
+  const double thresh = zkabs * T.bs0 * std::ldexp(1.0, -51);
+  int chunk = nd >= 4 ? 4 : (nd >= 2 ? 2 : 1);
+  DBuf<double2> mp(st), lo(st);
+  mp.alloc((size_t)off * chunk, st);
+  lo.alloc((size_t)off * chunk, st);
+  cudaEvent_t ev[8];
+  for (int i = 0; i < 8; i++) B2_CHECK(cudaEventCreate(&ev[i]));
+  double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int d0 = 0; d0 < nd;) {
+    int left = nd - d0;
+    int ND = left >= 4 ? 4 : (left >= 2 ? 2 : 1);
+    HDens D{fc ? qs.p : nullptr, fd ? ds.p : nullptr, fd ? vs.p : nullptr, nd, d0};
+    B2_CHECK(cudaMemsetAsync(lo.p, 0, sizeof(double2) * (size_t)off * ND, st));
+    switch (ND) {
+      case 4: helm_chunk<4>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+      case 2: helm_chunk<2>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+      default: helm_chunk<1>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+    }
+    if (a.timeinfo) {
+      B2_CHECK(cudaEventSynchronize(ev[6]));
+      float ms[6];
+      for (int i = 0; i < 6; i++) B2_CHECK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+      tsum[0] += ms[0] * 1e-3;
+      tsum[2] += ms[1] * 1e-3;
+      tsum[1] += ms[2] * 1e-3;
+      tsum[3] += ms[3] * 1e-3;
+      tsum[4] += ms[4] * 1e-3;
+      tsum[7] += ms[5] * 1e-3;
+    }
+    d0 += ND;
+  }
+  auto unpack = [&](const int* perm, long n, int w, const double2* in, double* out) {
+    if (!out || !n) return;
+    k_h_unpack<<<ceil_div(n, 256), 256, 0, st>>>(perm, n, w, in, (double2*)out);
+    B2_LAUNCH_CHECK();
+  };
+  if (a.ifpgh >= 1) unpack(T.isrc.p, ns, nd, ps.p, a.pot);
+  if (a.ifpgh >= 2) unpack(T.isrc.p, ns, 2 * nd, gs.p, a.grad);
+  if (a.ifpgh >= 3) unpack(T.isrc.p, ns, 3 * nd, hs.p, a.hess);
+  if (a.ifpghtarg >= 1) unpack(T.itarg.p, nt, nd, pt.p, a.pottarg);
+  if (a.ifpghtarg >= 2) unpack(T.itarg.p, nt, 2 * nd, gt.p, a.gradtarg);
+  if (a.ifpghtarg >= 3) unpack(T.itarg.p, nt, 3 * nd, ht.p, a.hesstarg);
+  B2_CHECK(cudaStreamSynchronize(st));
+  if (a.timeinfo)
+    for (int i = 0; i < 8; i++) a.timeinfo[i] = tsum[i];
+  for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+  return IER_OK;
+}
+
+int helm_direct_device(int nd, double zkr, double zki, long ns, const double* src,
+                       const double* charge, const double* dipstr, const double* dipvec, long nt,
+                       const double* trg, int ifpgh, double* pot, double* grad, double* hess,
+                       double thresh, cudaStream_t st) {
+  if (nd < 1 || ns < 0 || nt < 0 || ifpgh < 1 || ifpgh > 3) return IER_BADARG;
+  if (nt == 0) return IER_OK;
+  if (dipstr && !dipvec) return IER_BADARG;
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  configure_mempool(dev);
+  ensure_device_tables();
+  if (ns == 0 || (!charge && !dipstr)) {
+    B2_CHECK(cudaMemsetAsync(pot, 0, sizeof(double2) * nd * nt, st));
+    if (ifpgh >= 2) B2_CHECK(cudaMemsetAsync(grad, 0, sizeof(double2) * 2 * nd * nt, st));
+    if (ifpgh >= 3) B2_CHECK(cudaMemsetAsync(hess, 0, sizeof(double2) * 3 * nd * nt, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    return IER_OK;
+  }
+  int tb = ceil_div(nt, 128);
+  int nslice = std::max(1, std::min(1024, (148 * 16) / std::max(tb, 1)));
+  long chunk = (ns + nslice - 1) / nslice;
+  chunk = ((chunk + 127) / 128) * 128;
+  nslice = (int)std::max(1L, (ns + chunk - 1) / chunk);
+  DBuf<double2> part(st);
+  part.alloc((size_t)nslice * nt * 6, st);
+  for (int d = 0; d < nd; d++) {
+    dim3 grid(tb, nslice);
+    if (ifpgh == 1)
+      k_h_direct<1><<<grid, 128, 0, st>>>(nd, d, ns, src, charge, dipstr, dipvec, nt, trg, zkr, zki, thresh, chunk, part.p);
+    else if (ifpgh == 2)
+      k_h_direct<2><<<grid, 128, 0, st>>>(nd, d, ns, src, charge, dipstr, dipvec, nt, trg, zkr, zki, thresh, chunk, part.p);
+    else
+      k_h_direct<3><<<grid, 128, 0, st>>>(nd, d, ns, src, charge, dipstr, dipvec, nt, trg, zkr, zki, thresh, chunk, part.p);
+    B2_LAUNCH_CHECK();
+    k_h_direct_reduce<<<ceil_div(nt, 256), 256, 0, st>>>(nd, d, nt, nslice, ifpgh, part.p,
+                                                         (double2*)pot, (double2*)grad,
+                                                         (double2*)hess);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaStreamSynchronize(st));
+  return IER_OK;
+}
+
+}  // namespace b2

@@ -1,0 +1,40 @@
+// Helmholtz FMM engine (the low-frequency path of src/helmholtz/hfmm2d.f).
+#pragma once
+#include "common.cuh"
+
+namespace b2 {
+
+struct HelmArgs {
+  int nd = 1;
+  double eps = 1e-9;
+  double zkr = 1.0, zki = 0.0;  // zk
+  long ns = 0;
+  const double* src = nullptr;     // (2, ns)
+  const double* charge = nullptr;  // complex (nd, ns)
+  const double* dipstr = nullptr;  // complex (nd, ns)
+  const double* dipvec = nullptr;  // (nd, 2, ns)
+  int ifpgh = 0;
+  double *pot = nullptr, *grad = nullptr, *hess = nullptr;  // complex (nd,n),(nd,2,n),(nd,3,n)
+  long nt = 0;
+  const double* trg = nullptr;
+  int ifpghtarg = 0;
+  double *pottarg = nullptr, *gradtarg = nullptr, *hesstarg = nullptr;
+  int ndiv = 0;
+  int ifnear = 1;
+  double* timeinfo = nullptr;
+};
+
+// ier: 0 ok, 13 expansion order too large, 20 the problem needs the
+// high-frequency (box larger than 16 wavelengths) translations.
+int helm_fmm_device(const HelmArgs& a, cudaStream_t st);
+
+// All-pairs Helmholtz sums (h2d_direct*, src/helmholtz/helmkernels2d.f).
+int helm_direct_device(int nd, double zkr, double zki, long ns, const double* src,
+                       const double* charge, const double* dipstr, const double* dipvec, long nt,
+                       const double* trg, int ifpgh, double* pot, double* grad, double* hess,
+                       double thresh, cudaStream_t st);
+
+// Expansion order of a box of size bsize (h2dterms, src/helmholtz/h2dterms.f:35-97).
+int helm_nterms(double bsize, double zkr, double zki, double eps, int* ier);
+
+}  // namespace b2

@@ -1,8 +1,9 @@
 """fmm2dpy-compatible front end (python/fmm2dpy/fmm2d.py of the reference).
 
 Same keyword-only signatures, argument meaning, output shapes, assertion
-messages and dispatch as ``fmm2dpy.lfmm2d / rfmm2d / cfmm2d`` and the direct
-sums ``l2ddir / r2ddir / c2ddir``, plus ``comperr`` and ``Output``.  Arrays
+messages and dispatch as ``fmm2dpy.hfmm2d / lfmm2d / rfmm2d / cfmm2d`` and
+the direct sums ``h2ddir / l2ddir / r2ddir / c2ddir``, plus ``comperr`` and
+``Output``.  Arrays
 may be numpy arrays (host; results come back as numpy) or CUDA torch tensors
 (device; zero host copies, results are CUDA tensors).  Every evaluation runs
 in ``libfmm2d_b200.so`` on the GPU; there is no CPU fallback.
@@ -342,6 +343,145 @@ def r2ddir(*, sources, targets, charges=None, dipstr=None, dipvec=None, pgt=0, n
 def c2ddir(*, sources, targets, charges=None, dipstr=None, pgt=0, nd=1, thresh=1e-16):
     """Cauchy direct sum (fmm2d.py:1616-1740)."""
     return _direct_front(0, sources, targets, charges, dipstr, None, pgt, nd, thresh)
+
+
+# ---------------------------------------------------------------------------
+# Helmholtz (python/fmm2dpy/fmm2d.py:20-199, 1250-1368)
+# ---------------------------------------------------------------------------
+def _helm_run(eps, zk, sources, charges, dipstr, dipvec, targets, ifpgh, ifpghtarg, nd,
+              ndiv=None, timeinfo=None, **_ignored):
+    """One Helmholtz FMM call; returns user-shaped outputs and ier."""
+    torch_mode = _is_torch(sources)
+    B = _TH if torch_mode else _NP
+    ns = _ns_of(sources)
+    zk = complex(zk)
+    dt = np.complex128
+    s = B.prep(sources, (2, ns), (1, 0), np.float64)
+    q = None if charges is None else B.prep(charges, (nd, ns), (1, 0), dt)
+    d = None if dipstr is None else B.prep(dipstr, (nd, ns), (1, 0), dt)
+    v = None if dipstr is None else B.prep(dipvec, (nd, 2, ns), (2, 1, 0), np.float64)
+    nt = 0
+    t = None
+    if targets is not None and ifpghtarg > 0:
+        nt = _ns_of(targets)
+        t = B.prep(targets, (2, nt), (1, 0), np.float64)
+    kw = dict(device=sources.device) if torch_mode else {}
+    pot = B.empty((ns, nd), dt, **kw) if ifpgh >= 1 else None
+    grad = B.empty((ns, 2, nd), dt, **kw) if ifpgh >= 2 else None
+    hess = B.empty((ns, 3, nd), dt, **kw) if ifpgh >= 3 else None
+    pott = B.empty((nt, nd), dt, **kw) if ifpghtarg >= 1 and nt else None
+    gradt = B.empty((nt, 2, nd), dt, **kw) if ifpghtarg >= 2 and nt else None
+    hesst = B.empty((nt, 3, nd), dt, **kw) if ifpghtarg >= 3 and nt else None
+    ti = np.zeros(8) if timeinfo is None else timeinfo
+    ier = C.c_int(0)
+    L = _lib.lib()
+    head = [C.c_int(nd), C.c_double(eps), C.c_double(zk.real), C.c_double(zk.imag), C.c_int64(ns),
+            _ptr(s), C.c_int(q is not None), _ptr(q), C.c_int(d is not None), _ptr(d), _ptr(v)]
+    pgh = [C.c_int(ifpgh), _ptr(pot), _ptr(grad), _ptr(hess), C.c_int64(nt), _ptr(t),
+           C.c_int(ifpghtarg), _ptr(pott), _ptr(gradt), _ptr(hesst)]
+    if torch_mode:
+        import torch
+        opts = _options("fp64", ndiv)
+        stream = torch.cuda.current_stream(sources.device).cuda_stream
+        L.b2fmm_hfmm2d_dev(*head, *pgh, C.byref(opts), ti.ctypes.data_as(C.c_void_p),
+                           C.c_void_p(stream), C.byref(ier))
+    else:
+        L.b2fmm_hfmm2d_ndiv(*head, C.c_int(0), *pgh, C.c_int(int(ndiv) if ndiv else 0),
+                            C.c_int(0), C.c_int(1), ti.ctypes.data_as(C.c_void_p), C.byref(ier))
+
+    def user(a, kind):
+        if a is None:
+            return None
+        if kind == "p":
+            return a[:, 0] if nd == 1 else B.T(a, (1, 0))
+        return B.T(a[:, :, 0], (1, 0)) if nd == 1 else B.T(a, (2, 1, 0))
+
+    return dict(pot=user(pot, "p"), grad=user(grad, "g"), hess=user(hess, "h"),
+                pottarg=user(pott, "p"), gradtarg=user(gradt, "g"), hesstarg=user(hesst, "h"),
+                ier=ier.value)
+
+
+_HST_MSG = ("if both potential or potential at gradient are requested at sources and targets, "
+            "then the same pg must be equal to pgt")
+
+
+def hfmm2d(*, eps, zk, sources, charges=None, dipstr=None, dipvec=None, targets=None, pg=0,
+           pgt=0, nd=1, **ext):
+    """Helmholtz FMM (python/fmm2dpy/fmm2d.py:20-199).
+
+    u(x) = (i/4) sum_j c_j H0(k|x - x_j|) + k d_j v_j.(x - x_j)/|x - x_j|
+    H1(k|x - x_j|), with gradients; pg / pgt take 1 (potential) or 2
+    (potential and gradient) as in the reference front end.  Self
+    interactions are omitted.  ``out.ier`` is 20 when some level that
+    translates expansions has boxes larger than 16 wavelengths.
+    """
+    out = Output()
+    ns, ifcharge, ifdipole = _check_common(sources, charges, dipstr, dipvec, targets, nd)
+    if pg == 0 and pgt == 0:
+        print("Nothing to compute, set either pg or pgt to non-zero")
+        return out
+    if not (ifcharge or ifdipole):
+        return out
+    q = charges if ifcharge else None
+    d = dipstr if ifdipole else None
+    v = dipvec if ifdipole else None
+    res = None
+    if pg in (1, 2) and targets is not None:
+        assert pg == pgt, _HST_MSG
+        res = _helm_run(eps, zk, sources, q, d, v, targets, pgt, pgt, nd, **ext)
+    elif pg in (1, 2):
+        res = _helm_run(eps, zk, sources, q, d, v, None, pg, 0, nd, **ext)
+    elif targets is not None and pgt in (1, 2):
+        res = _helm_run(eps, zk, sources, q, d, v, targets, 0, pgt, nd, **ext)
+    if res is not None:
+        for k in ("pot", "grad", "pottarg", "gradtarg"):
+            if res[k] is not None:
+                setattr(out, k, res[k])
+        out.ier = res["ier"]
+    return out
+
+
+def h2ddir(*, zk, sources, targets, charges=None, dipstr=None, dipvec=None, pgt=0, nd=1,
+           thresh=1e-16):
+    """Helmholtz direct sum (python/fmm2dpy/fmm2d.py:1250-1368); pgt 1 or 2.
+    A source is skipped at targets where |zk| |x - x_j| is below thresh
+    (at or below for the charge potential-only kernel)."""
+    import torch
+    assert sources.shape[0] == 2, "The first dimension of sources must be 2"
+    out = Output()
+    if pgt == 0:
+        print("Nothing to compute, set either pg or pgt to non-zero")
+        return out
+    ns, ifcharge, ifdipole = _check_common(sources, charges, dipstr, dipvec, None, nd)
+    assert targets.shape[0] == 2, "The first dimension of targets must be 2"
+    if pgt not in (1, 2) or not (ifcharge or ifdipole):
+        return out
+    torch_mode = _is_torch(sources)
+    zk = complex(zk)
+    nt = _ns_of(targets)
+    s = _to_dev(sources, torch.float64).reshape(2, ns).T.contiguous()
+    t = _to_dev(targets, torch.float64).reshape(2, nt).T.contiguous()
+    cd = torch.complex128
+    q = _to_dev(charges, cd).reshape(nd, ns).T.contiguous() if ifcharge else None
+    d = _to_dev(dipstr, cd).reshape(nd, ns).T.contiguous() if ifdipole else None
+    v = (_to_dev(dipvec, torch.float64).reshape(nd, 2, ns).permute(2, 1, 0).contiguous()
+         if ifdipole else None)
+    pot = torch.zeros((nt, nd), dtype=cd, device="cuda")
+    grad = torch.zeros((nt, 2, nd), dtype=cd, device="cuda") if pgt >= 2 else None
+    ier = C.c_int(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    _lib.lib().b2fmm_h2ddir_dev(C.c_int(nd), C.c_double(zk.real), C.c_double(zk.imag),
+                                C.c_int64(ns), _ptr(s), _ptr(q), _ptr(d), _ptr(v),
+                                C.c_int64(nt), _ptr(t), C.c_int(pgt), _ptr(pot), _ptr(grad),
+                                None, C.c_double(thresh), C.c_void_p(stream), C.byref(ier))
+    if ier.value != 0:
+        raise RuntimeError(f"direct sum failed, ier={ier.value}")
+    potu = pot[:, 0] if nd == 1 else pot.T
+    out.pottarg = potu if torch_mode else potu.cpu().numpy()
+    if pgt >= 2:
+        g = grad[:, :, 0].T if nd == 1 else grad.permute(2, 1, 0)
+        out.gradtarg = g if torch_mode else g.cpu().numpy()
+    return out
 
 
 # ---------------------------------------------------------------------------

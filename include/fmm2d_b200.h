@@ -14,8 +14,9 @@
  * the given CUDA stream (NULL = legacy default stream) and return after the
  * stream has finished the call.
  * ier: 0 ok, 4 device allocation failure, 13 expansion order too large,
- *      100 invalid argument, 101 CUDA error, 103 problem larger than a
- *      fixed static scratch array.
+ *      20 Helmholtz problem needing the high-frequency (box > 16
+ *      wavelengths) translations, 100 invalid argument, 101 CUDA error,
+ *      103 problem larger than a fixed static scratch array.
  */
 #ifndef FMM2D_B200_H
 #define FMM2D_B200_H
@@ -149,6 +150,56 @@ void b2fmm_lap_direct_noalloc_dev(int kind, int nd, int64_t ns, const double* so
                                   const double* dipvec, int64_t nt, const double* targ,
                                   int ifpgh, double* pot, double* grad, double* hess,
                                   double thresh, void* stream, int* ier);
+
+/* -------------------------------------------------------------- Helmholtz */
+
+/* hfmm2d: src/helmholtz/hfmm2d.f:19-22.  zk is passed as (zk_re, zk_im);
+ * charge, dipstr and all outputs are complex, grad (nd,2,n), hess (nd,3,n),
+ * dipvec (nd,2,n) real.  Low-frequency path: ier 20 when a level where
+ * translations run has boxes larger than 16 wavelengths
+ * (hfmm2d.f:1001-1013, the wideband branch of src/helmholtz/wideband2d.f). */
+void b2fmm_hfmm2d(int nd, double eps, double zk_re, double zk_im, int64_t ns,
+                  const double* sources, int ifcharge, const double* charge, int ifdipole,
+                  const double* dipstr, const double* dipvec, int iper, int ifpgh, double* pot,
+                  double* grad, double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                  double* pottarg, double* gradtarg, double* hesstarg, int* ier);
+
+/* hfmm2d_ndiv: src/helmholtz/hfmm2d_ndiv.f:19-22 (idivflag is accepted and
+ * ignored, as hfmm2dmain always subdivides on sources). */
+void b2fmm_hfmm2d_ndiv(int nd, double eps, double zk_re, double zk_im, int64_t ns,
+                       const double* sources, int ifcharge, const double* charge, int ifdipole,
+                       const double* dipstr, const double* dipvec, int iper, int ifpgh,
+                       double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                       int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                       int ndiv, int idivflag, int ifnear, double* timeinfo, int* ier);
+
+/* Device-pointer hfmm2d (FP64; opts->precision is ignored). */
+void b2fmm_hfmm2d_dev(int nd, double eps, double zk_re, double zk_im, int64_t ns,
+                      const double* sources, int ifcharge, const double* charge, int ifdipole,
+                      const double* dipstr, const double* dipvec, int ifpgh, double* pot,
+                      double* grad, double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                      double* pottarg, double* gradtarg, double* hesstarg,
+                      const b2fmm_options* opts, double* timeinfo, void* stream, int* ier);
+
+/* h2d_direct{c,d,cd}{p,g,h}: src/helmholtz/helmkernels2d.f:3-904.  Device
+ * pointers; charge / dipstr NULL when absent; pairs with |zk r| < thresh
+ * (<= for the charge potential-only kernel) are skipped.  Outputs are
+ * overwritten (the reference adds into them). */
+void b2fmm_h2ddir_dev(int nd, double zk_re, double zk_im, int64_t ns, const double* sources,
+                      const double* charge, const double* dipstr, const double* dipvec,
+                      int64_t nt, const double* targ, int ifpgh, double* pot, double* grad,
+                      double* hess, double thresh, void* stream, int* ier);
+
+/* h2dterms: src/helmholtz/h2dterms.f:35-97 (expansion order of a box). */
+int b2fmm_h2dterms(double bsize, double zk_re, double zk_im, double eps, int* ier);
+
+/* Host evaluation of the special functions the Helmholtz kernels use (the
+ * same source is compiled for the device): kind 0 writes H0, H1 of z
+ * (hank103, src/common/hank103.f:116) as 4 doubles; kind 1 writes
+ * J_k(z)/rscale^k, k = 0..n (jbessel2d, src/common/cdjseval2d.f:5-204);
+ * kind 2 writes H_k(z) rscale^k (h2dall, src/helmholtz/h2dcommon.f:71-178).
+ * out holds 2(n+1) doubles for kinds 1 and 2. */
+void b2fmm_helm_special(int kind, int n, double z_re, double z_im, double rscale, double* out);
 
 /* ------------------------------------------------------------------- tree */
 
