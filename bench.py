@@ -16,6 +16,14 @@ sum over 1000 random sources.  ``--impl reference`` times the CPU oracle (the
 C++ restatement of the reference algorithm; the Fortran reference cannot be
 built here) on a bounded sample of the same workload with all host threads.
 
+``helmholtz_c4`` adds the Helmholtz configuration: hfmm2d with zk = 40 on
+2,000,000 sources at uniform random angles on the curve
+r(t) = 0.3 (1 + 0.2 cos 5t) about (0.5, 0.5) and 1,000,000 uniform targets,
+complex charges and dipole strengths CN(0,1), unit dipvec at a uniform angle,
+eps = 1e-9, pgt = 2 (FP64 throughout), timed the same way with its relative
+l2 error against the FP64 direct sum on 1000 targets.  ``--c4-only`` prints
+just that object (``--c4-scale`` shrinks it for profiling).
+
 Multi-GPU (torchrun): every rank evaluates its own independent problem of the
 same size (replicas, no collective in the data path); timings are the max over
 ranks (one all_reduce of the step times) and ``value`` counts all ranks' points.
@@ -51,6 +59,86 @@ def make_inputs(n, seed=1):
     return src, q, d, v
 
 
+def make_c4_inputs(ns, nt, seed=4):
+    """Helmholtz configuration: closed smooth curve + uniform targets."""
+    rng = np.random.default_rng(seed)
+    th = rng.uniform(0, 2 * np.pi, ns)
+    r = 0.3 * (1 + 0.2 * np.cos(5 * th))
+    src = np.stack([0.5 + r * np.cos(th), 0.5 + r * np.sin(th)])
+    trg = rng.uniform(0, 1, (2, nt))
+    q = (rng.normal(size=ns) + 1j * rng.normal(size=ns)) / np.sqrt(2)
+    d = (rng.normal(size=ns) + 1j * rng.normal(size=ns)) / np.sqrt(2)
+    ph = rng.uniform(0, 2 * np.pi, ns)
+    v = np.stack([np.cos(ph), np.sin(ph)])
+    return src, trg, q, d, v
+
+
+def helmholtz_c4(L, dev, stream, scale=1.0, steps=3, warmup=1):
+    """hfmm2d, zk=40, 2M curve sources + 1M targets, eps=1e-9, pgt=2."""
+    import torch
+    from fmm2d_b200 import _lib
+    ns, nt = int(2_000_000 * scale), int(1_000_000 * scale)
+    src, trg, q, d, v = make_c4_inputs(ns, nt)
+    hs, hq, hd, hv = fortran_layout(src, q, d, v)
+    ds, dq, dd, dv = (torch.as_tensor(x, device=dev) for x in (hs, hq, hd, hv))
+    dt = torch.as_tensor(np.ascontiguousarray(trg.T), device=dev)
+    pt = torch.empty((nt, 1), dtype=torch.complex128, device=dev)
+    gt = torch.empty((nt, 2, 1), dtype=torch.complex128, device=dev)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    zk, eps = 40.0, 1e-9
+
+    def step(ti=None):
+        o = _lib.Options()
+        o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, 1
+        ier = C.c_int(0)
+        ti = ti if ti is not None else np.zeros(8)
+        L.b2fmm_hfmm2d_dev(1, eps, zk, 0.0, ns, ptr(ds), 1, ptr(dq), 1, ptr(dd), ptr(dv), 0,
+                           None, None, None, nt, ptr(dt), 2, ptr(pt), ptr(gt), None, C.byref(o),
+                           ti.ctypes.data_as(C.c_void_p), C.c_void_p(stream.cuda_stream),
+                           C.byref(ier))
+        if ier.value != 0:
+            raise RuntimeError(f"b2fmm_hfmm2d_dev ier={ier.value}")
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    tis = np.zeros(8)
+    e0.record(stream)
+    for _ in range(steps):
+        ti = np.zeros(8)
+        step(ti)
+        tis += ti
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    tis /= steps
+    rng = np.random.default_rng(98)
+    idx = np.sort(rng.choice(nt, min(1000, nt), replace=False))
+    tsel = torch.as_tensor(np.ascontiguousarray(trg[:, idx].T), device=dev)
+    m = len(idx)
+    ep = torch.empty((m, 1), dtype=torch.complex128, device=dev)
+    eg = torch.empty((m, 2, 1), dtype=torch.complex128, device=dev)
+    ier = C.c_int(0)
+    L.b2fmm_h2ddir_dev(1, zk, 0.0, ns, ptr(ds), ptr(dq), ptr(dd), ptr(dv), m, ptr(tsel), 2,
+                       ptr(ep), ptr(eg), None, C.c_double(1e-16),
+                       C.c_void_p(stream.cuda_stream), C.byref(ier))
+    ia = torch.as_tensor(idx, device=dev)
+    a_p, a_g = pt[ia, 0].cpu().numpy(), gt[ia, :, 0].cpu().numpy()
+    e_p, e_g = ep[:, 0].cpu().numpy(), eg[:, :, 0].cpu().numpy()
+    err = float(np.sqrt((np.linalg.norm(a_p - e_p) ** 2 + np.linalg.norm(a_g - e_g) ** 2)
+                        / (np.linalg.norm(e_p) ** 2 + np.linalg.norm(e_g) ** 2)))
+    return {"workload": "hfmm2d zk=40, curve r=0.3(1+0.2cos5t) sources + uniform targets, "
+                        "charges+dipoles CN(0,1), eps=1e-9, pgt=2, FP64",
+            "ns": ns, "nt": nt, "value": (ns + nt) / (ms * 1e-3), "unit": "points/s",
+            "ms_per_step": ms, "steps": steps, "rel_l2_err": err,
+            "err_ref": f"FP64 direct sum over {m} random targets",
+            "phase_ms": {k: round(tis[i] * 1e3, 3) for k, i in
+                         (("p2m", 0), ("m2m", 2), ("p2l", 1), ("m2l", 3), ("l2l", 4),
+                          ("leaf_eval(l2p+m2p+p2p)", 7))}}
+
+
 def fortran_layout(src, q, d, v):
     """(2,n)/(n,)/(2,n) user arrays -> the C ABI's column-major layouts."""
     return (np.ascontiguousarray(src.T), np.ascontiguousarray(q.reshape(-1, 1)),
@@ -73,7 +161,7 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-i", str(self.gpu), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
 
@@ -166,7 +254,7 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=4_000_000)
@@ -174,6 +262,9 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1_000_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-c4", action="store_true", help="skip the Helmholtz configuration")
+    ap.add_argument("--c4-only", action="store_true", help="run only the Helmholtz configuration")
+    ap.add_argument("--c4-scale", type=float, default=1.0)
     args = ap.parse_args()
     rank, world, local = dist_info()
     if args.impl == "reference":
@@ -191,6 +282,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     L = _lib.lib()
+    if args.c4_only:
+        res = helmholtz_c4(L, dev, torch.cuda.current_stream(dev), args.c4_scale,
+                           max(1, args.steps), max(1, args.warmup))
+        if rank == 0:
+            print(json.dumps({"helmholtz_c4": res}), flush=True)
+        return
     n = args.n
     src, q, d, v = make_inputs(n, seed=1 + rank)
     hs, hq, hd, hv = fortran_layout(src, q, d, v)
@@ -246,6 +343,12 @@ def main():
     ms64, ti64, _, _ = timed("fp64", max(2, args.steps // 2), 1) if prec != "fp64" else (ms, ti, 0, None)
     value = world * n / (ms * 1e-3)
     value64 = world * n / (ms64 * 1e-3)
+    # the same mixed step with the M2L on the CUDA cores instead of tcgen05
+    ms_cc = None
+    if prec == "mixed":
+        L.b2fmm_set_m2l_tensor_cores(0)
+        ms_cc, _, _, _ = timed(prec, max(2, args.steps // 4), 1)
+        L.b2fmm_set_m2l_tensor_cores(1)
 
     # work counts and roofline of the dominant kernel (from this run)
     L.b2fmm_set_stats(1)
@@ -333,6 +436,10 @@ def main():
     h2d = hsrc.numel() * 8 + hq_.numel() * 16 + hd_.numel() * 16 + hv_.numel() * 8
     d2h = hpot.numel() * 16 + hgrad.numel() * 16
 
+    c4 = None
+    if not args.no_c4:
+        c4 = helmholtz_c4(L, dev, stream, args.c4_scale)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_sample)
@@ -344,14 +451,18 @@ def main():
                 "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "n_points_per_gpu": n, "eps": 1e-6,
                            "precision": prec, "parallelism": f"replicas x{world}",
+                           "m2l_engine": ("tcgen05 split-TF32 (FP32 accumulate in TMEM)"
+                                          if prec == "mixed" else "FP64 CUDA cores"),
                            "l2_policy": "inputs (256 MB) and expansions larger than L2"},
                 "fp64_value": value64, "fp64_ms_per_step": ms64,
+                "mixed_cuda_core_m2l_ms_per_step": ms_cc,
                 "speedup_vs_fp64": value / value64,
                 "rel_l2_err": err, "err_ref": "FP64 direct sum over 1000 random sources",
                 "e2e": {"value": world * n / te, "unit": "points/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": int(launches),
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+                "helmholtz_c4": c4}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
