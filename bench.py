@@ -24,6 +24,14 @@ eps = 1e-9, pgt = 2 (FP64 throughout), timed the same way with its relative
 l2 error against the FP64 direct sum on 1000 targets.  ``--c4-only`` prints
 just that object (``--c4-scale`` shrinks it for profiling).
 
+``batched_c3`` is the batched configuration: 256 independent cfmm2d problems
+with N log-uniform in [2e3, 2e5], uniform or single-Gaussian clouds, nd in
+{1, 2, 4} complex densities, eps = 1e-6, pg = 1.  It times 256 sequential
+plain calls (b2fmm_cfmm2d_dev, tree included in every call) against one
+launch of a CUDA graph that evaluates all 256 plans (trees built once,
+b2fmm_plan_create; their build time is reported separately), and checks
+the graph's results against the sequential ones.
+
 Multi-GPU (torchrun): every rank evaluates its own independent problem of the
 same size (replicas, no collective in the data path); timings are the max over
 ranks (one all_reduce of the step times) and ``value`` counts all ranks' points.
@@ -137,6 +145,86 @@ def helmholtz_c4(L, dev, stream, scale=1.0, steps=3, warmup=1):
             "phase_ms": {k: round(tis[i] * 1e3, 3) for k, i in
                          (("p2m", 0), ("m2m", 2), ("p2l", 1), ("m2l", 3), ("l2l", 4),
                           ("leaf_eval(l2p+m2p+p2p)", 7))}}
+
+
+def batched_c3(L, dev, nprob=256, seed=3, nbranch=16, launches=5):
+    """256 cfmm2d problems: sequential plain calls vs one captured graph."""
+    import torch
+    from fmm2d_b200 import _lib
+    from fmm2d_b200.plan import BatchGraph, Plan
+    rng = np.random.default_rng(seed)
+    probs = []
+    for i in range(nprob):
+        n = int(round(10 ** rng.uniform(np.log10(2e3), np.log10(2e5))))
+        nd = int(rng.choice([1, 2, 4]))
+        if rng.uniform() < 0.5:
+            src = rng.uniform(0, 1, (2, n))
+        else:
+            c = rng.uniform(0.25, 0.75, 2)
+            src = c[:, None] + 10 ** rng.uniform(-3, -1) * rng.normal(size=(2, n))
+        q = rng.normal(size=(nd, n)) + 1j * rng.normal(size=(nd, n))
+        ts = torch.as_tensor(np.ascontiguousarray(src.T), device=dev)
+        tq = torch.as_tensor(np.ascontiguousarray(q.T), device=dev)
+        probs.append((n, nd, ts, tq, torch.empty((n, nd), dtype=torch.complex128, device=dev)))
+    npts = sum(p[0] for p in probs)
+    stream = torch.cuda.current_stream(dev)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    o = _lib.Options()
+    o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, 0
+
+    def sequential():
+        for n, nd, ts, tq, pot in probs:
+            ier = C.c_int(0)
+            L.b2fmm_cfmm2d_dev(nd, C.c_double(1e-6), C.c_int64(n), ptr(ts), 1, ptr(tq), 0, None, 1,
+                               ptr(pot), None, None, C.c_int64(0), None, 0, None, None, None,
+                               C.byref(o), None, C.c_void_p(stream.cuda_stream), C.byref(ier))
+            if ier.value != 0:
+                raise RuntimeError(f"b2fmm_cfmm2d_dev ier={ier.value}")
+
+    sequential()  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sequential()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    seq_ms = e0.elapsed_time(e1)
+    seq_pot = [p[4].clone() for p in probs]
+    t0 = time.perf_counter()
+    plans = [Plan("cfmm2d", eps=1e-6, sources=ts, charges=True, pg=1, nd=nd)
+             for n, nd, ts, tq, pot in probs]
+    torch.cuda.synchronize()
+    plan_ms = (time.perf_counter() - t0) * 1e3
+    t0 = time.perf_counter()
+    g = BatchGraph(plans, charges=[p[3] for p in probs], nbranch=nbranch)
+    torch.cuda.synchronize()
+    graph_build_ms = (time.perf_counter() - t0) * 1e3
+    g.launch()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(launches):
+        g.launch(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    graph_ms = e0.elapsed_time(e1) / launches
+    st = g.status()
+    err = 0.0
+    for (n, nd, ts, tq, pot), ref, out in zip(probs, seq_pot, g.outs):
+        a, b = out["pot"], ref
+        err = max(err, float(torch.linalg.norm(a - b) / torch.linalg.norm(b)))
+    nodes = g.nodes
+    g.close()
+    for p in plans:
+        p.close()
+    return {"workload": "256 cfmm2d problems, N log-uniform [2e3, 2e5], uniform or "
+                        "single-Gaussian clouds, nd in {1,2,4}, eps=1e-6, pg=1",
+            "problems": nprob, "points": npts, "unit": "points/s",
+            "sequential_ms": seq_ms, "sequential_value": npts / (seq_ms * 1e-3),
+            "graph_ms": graph_ms, "graph_value": npts / (graph_ms * 1e-3),
+            "graph_speedup": seq_ms / graph_ms, "graph_branches": nbranch, "graph_nodes": nodes,
+            "plan_build_ms": plan_ms, "graph_build_ms": graph_build_ms,
+            "graph_plus_plans_value": npts / ((graph_ms + plan_ms) * 1e-3),
+            "max_rel_diff_graph_vs_sequential": err, "status": st}
 
 
 def fortran_layout(src, q, d, v):
@@ -265,6 +353,8 @@ def main():
     ap.add_argument("--no-c4", action="store_true", help="skip the Helmholtz configuration")
     ap.add_argument("--c4-only", action="store_true", help="run only the Helmholtz configuration")
     ap.add_argument("--c4-scale", type=float, default=1.0)
+    ap.add_argument("--no-c3", action="store_true", help="skip the batched configuration")
+    ap.add_argument("--c3-only", action="store_true", help="run only the batched configuration")
     args = ap.parse_args()
     rank, world, local = dist_info()
     if args.impl == "reference":
@@ -282,6 +372,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     L = _lib.lib()
+    if args.c3_only:
+        res = batched_c3(L, dev)
+        if rank == 0:
+            print(json.dumps({"batched_c3": res}), flush=True)
+        return
     if args.c4_only:
         res = helmholtz_c4(L, dev, torch.cuda.current_stream(dev), args.c4_scale,
                            max(1, args.steps), max(1, args.warmup))
@@ -436,6 +531,9 @@ def main():
     h2d = hsrc.numel() * 8 + hq_.numel() * 16 + hd_.numel() * 16 + hv_.numel() * 8
     d2h = hpot.numel() * 16 + hgrad.numel() * 16
 
+    c3 = None
+    if not args.no_c3:
+        c3 = batched_c3(L, dev)
     c4 = None
     if not args.no_c4:
         c4 = helmholtz_c4(L, dev, stream, args.c4_scale)
@@ -462,7 +560,7 @@ def main():
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": int(launches),
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-                "helmholtz_c4": c4}
+                "helmholtz_c4": c4, "batched_c3": c3}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

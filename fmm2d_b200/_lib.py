@@ -57,6 +57,18 @@ SIGNATURES = {
     "b2fmm_set_stats": [c_int],
     "b2fmm_get_stats": [P, c_int],
     "b2fmm_fma_peak": [c_int],
+    "b2fmm_set_m2l_tensor_cores": [c_int],
+    "b2fmm_tc_gemm_probe": [P, P, c_int, c_int, P, P, P],
+    "b2fmm_plan_create": [c_int, c_int, c_double, c_int64, P, c_int, c_int, c_int, c_int64, P,
+                          c_int, P, P, P],
+    "b2fmm_plan_eval": [P] * 12,
+    "b2fmm_plan_status": [P],
+    "b2fmm_plan_free": [P],
+    "b2fmm_batch_graph_create": [c_int] + [P] * 10 + [c_int, P],
+    "b2fmm_batch_graph_launch": [P, P, P],
+    "b2fmm_batch_graph_status": [P],
+    "b2fmm_batch_graph_nodes": [P],
+    "b2fmm_batch_graph_free": [P],
 }
 
 _lib = None
@@ -84,6 +96,11 @@ def lib():
         L.b2fmm_kernel_launches.restype = C.c_uint64
         L.b2fmm_fma_peak.restype = c_double
         L.b2fmm_h2dterms.restype = c_int
+        L.b2fmm_plan_create.restype = c_void_p
+        L.b2fmm_plan_status.restype = c_int
+        L.b2fmm_batch_graph_create.restype = c_void_p
+        L.b2fmm_batch_graph_status.restype = c_int
+        L.b2fmm_batch_graph_nodes.restype = C.c_int64
         _lib = L
     return _lib
 

@@ -3,12 +3,15 @@
 #include <vector>
 
 #include "../../include/fmm2d_b200.h"
+#include "batch.cuh"
 #include "direct.cuh"
 #include "helm_special.cuh"
 #include "helmholtz.cuh"
 #include "laplace.cuh"
 #include "tree.cuh"
 #include "peaks.cuh"
+#include "lap_mixed.cuh"
+#include "tc_m2l.cuh"
 
 namespace b2 {
 std::atomic<unsigned long long> g_launches{0};
@@ -441,6 +444,94 @@ void b2fmm_h2ddir_dev(int nd, double zk_re, double zk_im, int64_t ns, const doub
   });
 }
 
+void* b2fmm_plan_create(int fe, int nd, double eps, int64_t ns, const double* sources,
+                        int ifcharge, int ifdipole, int ifpgh, int64_t nt, const double* targ,
+                        int ifpghtarg, const b2fmm_options* opts, void* stream, int* ier) {
+  static const double present = 0.0;  // marks a density kind the evaluations will pass
+  LapPlan* p = nullptr;
+  guarded(ier, [&] {
+    LapArgs a;
+    a.fe = fe;
+    a.nd = nd;
+    a.eps = eps;
+    a.ns = ns;
+    a.src = sources;
+    a.charge = ifcharge == 1 ? &present : nullptr;
+    a.dipstr = ifdipole == 1 ? &present : nullptr;
+    a.ifpgh = ifpgh;
+    a.nt = nt;
+    a.trg = targ;
+    a.ifpghtarg = ifpghtarg;
+    if (opts) {
+      a.ndiv = opts->ndiv;
+      a.idivflag = opts->idivflag;
+      a.ifnear = opts->ifnear;
+      a.precision = opts->precision;
+    }
+    return lap_plan_create(a, (cudaStream_t)stream, true, &p);
+  });
+  if (ier && *ier != IER_OK && p) {
+    lap_plan_free(p);
+    p = nullptr;
+  }
+  return p;
+}
+
+void b2fmm_plan_eval(void* plan, const double* charge, const double* dipstr, const double* dipvec,
+                     double* pot, double* grad, double* hess, double* pottarg, double* gradtarg,
+                     double* hesstarg, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_plan_eval((LapPlan*)plan, charge, dipstr, dipvec, pot, grad, hess, pottarg,
+                         gradtarg, hesstarg, (cudaStream_t)stream, false, nullptr);
+  });
+}
+
+int b2fmm_plan_status(void* plan) {
+  int ier = 0;
+  guarded(&ier, [&] { return lap_plan_status((LapPlan*)plan); });
+  return ier;
+}
+
+void b2fmm_plan_free(void* plan) { lap_plan_free((LapPlan*)plan); }
+
+void* b2fmm_batch_graph_create(int n, void* const* plans, const double* const* charge,
+                               const double* const* dipstr, const double* const* dipvec,
+                               double* const* pot, double* const* grad, double* const* hess,
+                               double* const* pottarg, double* const* gradtarg,
+                               double* const* hesstarg, int nbranch, int* ier) {
+  BatchGraph* g = nullptr;
+  guarded(ier, [&] {
+    BatchIO io;
+    io.charge = charge;
+    io.dipstr = dipstr;
+    io.dipvec = dipvec;
+    io.pot = pot;
+    io.grad = grad;
+    io.hess = hess;
+    io.pottarg = pottarg;
+    io.gradtarg = gradtarg;
+    io.hesstarg = hesstarg;
+    return batch_graph_create(n, (LapPlan* const*)plans, io, nbranch, &g);
+  });
+  return g;
+}
+
+void b2fmm_batch_graph_launch(void* graph, void* stream, int* ier) {
+  guarded(ier, [&] { return batch_graph_launch((BatchGraph*)graph, (cudaStream_t)stream); });
+}
+
+int b2fmm_batch_graph_status(void* graph) {
+  int ier = 0;
+  guarded(&ier, [&] { return batch_graph_status((BatchGraph*)graph); });
+  return ier;
+}
+
+int64_t b2fmm_batch_graph_nodes(void* graph) {
+  return (int64_t)batch_graph_nodes((const BatchGraph*)graph);
+}
+
+void b2fmm_batch_graph_free(void* graph) { batch_graph_free((BatchGraph*)graph); }
+
 int b2fmm_h2dterms(double bsize, double zk_re, double zk_im, double eps, int* ier) {
   int e = 0, p = 0;
   guarded(ier, [&] {
@@ -544,5 +635,12 @@ void b2fmm_get_stats(double* out, int n) {
 }
 
 double b2fmm_fma_peak(int fp64) { return fma_peak_flops(fp64 != 0); }
+
+void b2fmm_set_m2l_tensor_cores(int on) { set_m2l_tensor_cores(on != 0); }
+
+void b2fmm_tc_gemm_probe(const float* a_dev, const float* b_dev, int k, int n, float* d_dev,
+                         void* stream, int* ier) {
+  guarded(ier, [&] { return tc_gemm_probe(a_dev, b_dev, k, n, d_dev, (cudaStream_t)stream); });
+}
 
 }  // extern "C"

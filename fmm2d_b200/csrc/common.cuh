@@ -1,5 +1,8 @@
 // Shared helpers for the fmm2d_b200 CUDA library (sm_100a).
 #pragma once
+#include <mutex>
+#include <utility>
+#include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -95,6 +98,23 @@ struct DBuf {
     if (count) B2_CHECK(cudaMemsetAsync(p, v, count * sizeof(T), s));
   }
 };
+
+// Raise a kernel's dynamic shared-memory limit when a launch needs more than
+// the default 48 KB.  Each (kernel, device) pair is set once per size, so
+// repeated launches (and launches under stream capture) make no further calls.
+template <typename K>
+void set_smem_attr(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<const void*, int>, size_t>> done;
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  for (auto& e : done)
+    if (e.first.first == (const void*)kernel && e.first.second == dev && e.second >= bytes) return;
+  B2_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  done.push_back({{(const void*)kernel, dev}, bytes});
+}
 
 // Keep freed memory in the pool between calls so repeated FMMs do not pay
 // for cudaMalloc (the pool is per device and shared by all streams).

@@ -993,7 +993,7 @@ __global__ void k_h_direct_reduce(int nd, int d, long nt, int nslice, int ifpgh,
 template <typename K>
 void set_smem(K kernel, size_t bytes) {
   if (bytes > 48 * 1024)
-    B2_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    set_smem_attr(kernel, bytes);
 }
 
 int grid_w(long nitems, int wpb) {

@@ -15,6 +15,8 @@
 //   and the partial sums in FP64.  Small leaves split their sources between
 //   2 or 4 lane groups so that the warp stays busy.
 #include "lap_mixed.cuh"
+
+#include <atomic>
 #include "laplace.cuh"
 
 namespace b2 {
@@ -460,7 +462,7 @@ void m2l_launch(const TV& t, int first, int n, int P, const double* binom, const
   const size_t warp_floats = (size_t)EG * P * 2 * ND * 2 + ((2 * EG + 3) & ~3);
   size_t sm = sizeof(float) * 4 * warp_floats + sizeof(float4) * (size_t)P * RB +
               sizeof(float2) * 49 * P + sizeof(float) * 52;
-  B2_CHECK(cudaFuncSetAttribute(k_m2l_f32<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  set_smem_attr(k_m2l_f32<ND>, sm);
   k_m2l_f32<ND><<<grid_for(n, 4), 128, sm, st>>>(t, first, n, P, RB, EG, binom, M.utab.p,
                                                   M.lgtab.p, mp, lo);
   B2_LAUNCH_CHECK();
@@ -471,8 +473,7 @@ void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const
                  int ndc, int d0, int P, const double2* mp, const double2* lo, double thresh,
                  int ifnear, double2* pot, double2* grad, double2* hess, cudaStream_t st) {
   size_t sm = sizeof(double2) * 4 * (P * ND + 32 + 32 * ND);
-  B2_CHECK(cudaFuncSetAttribute(k_leaf_mixed<ND, IFPGH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sm));
+  set_smem_attr(k_leaf_mixed<ND, IFPGH>, sm);
   k_leaf_mixed<ND, IFPGH><<<grid_for(nb, 4), 128, sm, st>>>(
       t, nb, use_targets, M.xs.p, use_targets ? M.xt.p : M.xs.p, xe64, M.q.p, M.d.p, ndc, d0, P,
       mp, lo, (float)(thresh * thresh), ifnear, pot, grad, hess);
@@ -495,8 +496,8 @@ void leaf_dispatch(int ifl, const TV& t, int nb, int use_targets, const MixedDat
 }  // namespace
 
 void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* xt, long nt,
-                       const double2* qs, const double2* ds, int ndc, double cx0, double cy0,
-                       int P, cudaStream_t st) {
+                       bool has_q, bool has_d, int ndc, double cx0, double cy0, int P,
+                       cudaStream_t st) {
   M.xs.alloc(ns, st);
   k_prep_pts<<<ceil_div(ns, 256), 256, 0, st>>>(xs, ns, cx0, cy0, M.xs.p);
   B2_LAUNCH_CHECK();
@@ -506,24 +507,44 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
     B2_LAUNCH_CHECK();
   }
   long m = ns * (long)ndc;
-  if (qs) {
-    M.q.alloc(m, st);
-    k_prep_dens<<<ceil_div(m, 256), 256, 0, st>>>(qs, m, M.q.p);
-    B2_LAUNCH_CHECK();
-  }
-  if (ds) {
-    M.d.alloc(m, st);
-    k_prep_dens<<<ceil_div(m, 256), 256, 0, st>>>(ds, m, M.d.p);
-    B2_LAUNCH_CHECK();
-  }
+  if (has_q) M.q.alloc(m, st);
+  if (has_d) M.d.alloc(m, st);
   M.utab.alloc(49 * (size_t)P, st);
   M.lgtab.alloc(49, st);
   k_utab<<<49, 64, 0, st>>>(P, M.utab.p, M.lgtab.p);
   B2_LAUNCH_CHECK();
 }
 
+void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, long ns, int ndc,
+                         cudaStream_t st) {
+  long m = ns * (long)ndc;
+  if (qs && M.q.p) {
+    k_prep_dens<<<ceil_div(m, 256), 256, 0, st>>>(qs, m, M.q.p);
+    B2_LAUNCH_CHECK();
+  }
+  if (ds && M.d.p) {
+    k_prep_dens<<<ceil_div(m, 256), 256, 0, st>>>(ds, m, M.d.p);
+    B2_LAUNCH_CHECK();
+  }
+}
+
+namespace {
+std::atomic<bool> g_m2l_tc{true};
+}
+
+void set_m2l_tensor_cores(bool on) { g_m2l_tc.store(on); }
+bool m2l_tensor_cores() { return g_m2l_tc.load(); }
+
 void lap_mixed_m2l(int ND, const TV& t, int first, int n, int P, const double* binom,
                    const MixedData& M, const double2* mp, double2* lo, cudaStream_t st) {
+  if (M.tc && M.pairs.usable && m2l_tc_supported(P) && M.err) {
+    long nmp = (long)M.nboxes * P * ND;
+    if ((long)M.mp32.n < nmp) throw CudaError("tensor-core M2L: scratch too small", IER_BADARG);
+    int r = m2l_tc_run(ND, t, M.pairs, P, binom, M.utab.p, M.lgtab.p, mp, M.mp32.p, nmp, lo,
+                       M.nlev, M.err, st);
+    if (r != IER_OK) throw CudaError("tensor-core M2L: invalid arguments", r);
+    return;
+  }
   switch (ND) {
     case 8: m2l_launch<8>(t, first, n, P, binom, M, mp, lo, st); break;
     case 4: m2l_launch<4>(t, first, n, P, binom, M, mp, lo, st); break;

@@ -3,6 +3,7 @@
 // differences; expansions, shifts, L2P and M2P stay FP64.
 #pragma once
 #include "lap_common.cuh"
+#include "tc_m2l.cuh"
 
 namespace b2 {
 
@@ -13,11 +14,27 @@ struct MixedData {
   DBuf<float2> q, d;    // all Cauchy densities, ndc per point
   DBuf<float2> utab;    // (1/o)^k for the 7x7 integer offsets o, k < P
   DBuf<float> lgtab;    // log|o|
+  M2LPairs pairs;       // flattened list-2 pairs for the tensor-core M2L
+  DBuf<float2> mp32;    // FP32 copy of one chunk's multipoles (tensor-core M2L)
+  bool tc = false;      // run M2L on the tensor cores
+  int nlev = 0;         // tree levels + 1
+  int nboxes = 0;
+  int* err = nullptr;   // device flag set by a tensor-core wait that gave up
 };
 
+// Tensor-core M2L switch (default on); off selects the FP32 CUDA-core M2L.
+void set_m2l_tensor_cores(bool on);
+bool m2l_tensor_cores();
+
+// Geometry part (FP32 coordinates, offset tables) and allocation of the FP32
+// density copies for ndc densities per source.
 void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* xt, long nt,
-                       const double2* qs, const double2* ds, int ndc, double cx0, double cy0,
-                       int P, cudaStream_t st);
+                       bool has_q, bool has_d, int ndc, double cx0, double cy0, int P,
+                       cudaStream_t st);
+
+// FP32 copies of the sorted densities (every evaluation).
+void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, long ns, int ndc,
+                         cudaStream_t st);
 
 // M2L over list 2 for boxes [first, first+n) of one density chunk (FP32).
 void lap_mixed_m2l(int ND, const lapk::TV& t, int first, int n, int P, const double* binom,

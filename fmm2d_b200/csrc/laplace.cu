@@ -18,6 +18,8 @@
 //                P2P (list 1) fused, one result write per point (steps 6-8)
 //   k_unpack     caller layout (cfmm / lfmm / rfmm) and inverse permutation
 #include "laplace.cuh"
+
+#include <memory>
 #include "lap_common.cuh"
 #include "lap_mixed.cuh"
 
@@ -866,8 +868,8 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   B2_CHECK(cudaEventRecord(ev[0], st));
   size_t sm_p2m = sizeof(double2) * 2 * (32 * (size_t)P + 64 * ND);
   size_t sm_p2l = sm_p2m + sizeof(double2) * 2 * 32;
-  B2_CHECK(cudaFuncSetAttribute(k_p2m<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2m));
-  B2_CHECK(cudaFuncSetAttribute(k_p2l<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_p2l));
+  set_smem_attr(k_p2m<ND>, sm_p2m);
+  set_smem_attr(k_p2l<ND>, sm_p2l);
   k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, 0, nb, xs, D, P, mp);
   B2_LAUNCH_CHECK();
   B2_CHECK(cudaEventRecord(ev[1], st));
@@ -892,7 +894,7 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
     int f = T.lfirst[2], n = nb - f;
     size_t sm = sizeof(double) * (P * P + 1) + sizeof(double2) * 4 * P * ND;
     if (sm > 48 * 1024)
-      B2_CHECK(cudaFuncSetAttribute(k_m2l<ND>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      set_smem_attr(k_m2l<ND>, sm);
     k_m2l<ND><<<warp_grid(n, 4), 128, sm, st>>>(tv, f, n, P, binom, mp, lo);
     B2_LAUNCH_CHECK();
   }
@@ -912,15 +914,15 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
       return;
     }
     if (ifl == 1) {
-      B2_CHECK(cudaFuncSetAttribute(k_leaf<ND, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_leaf));
+      set_smem_attr(k_leaf<ND, 1>, sm_leaf);
       k_leaf<ND, 1><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
                                                           thresh, a.ifnear, po, gr, he);
     } else if (ifl == 2) {
-      B2_CHECK(cudaFuncSetAttribute(k_leaf<ND, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_leaf));
+      set_smem_attr(k_leaf<ND, 2>, sm_leaf);
       k_leaf<ND, 2><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
                                                           thresh, a.ifnear, po, gr, he);
     } else {
-      B2_CHECK(cudaFuncSetAttribute(k_leaf<ND, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_leaf));
+      set_smem_attr(k_leaf<ND, 3>, sm_leaf);
       k_leaf<ND, 3><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
                                                           thresh, a.ifnear, po, gr, he);
     }
@@ -933,136 +935,234 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
 
 }  // namespace
 
-int lap_fmm_device(const LapArgs& a, cudaStream_t st) {
+struct LapPlan {
+  LapArgs a;                      // geometry and flags (density/output pointers unused)
+  cudaStream_t st = nullptr;      // stream owning the buffers
+  bool own = false;               // st was created by the plan
+  int nd = 1, ndc = 1, P = 0, chunk = 1;
+  long ns = 0, nt = 0;
+  bool fc = false, fd = false, mixed = false;
+  bool zero = false;              // nothing interacts: every output is zero
+  double thresh = 0;
+  float tree_ms = 0;
+  DeviceTree T;
+  DBuf<double> dbs;
+  DBuf<double2> xs, xt, qs, ds, ps, gs, hs, pt, gt, ht, mp, lo;
+  DBuf<int> err;
+  MixedData MD;
+  TV tv{};
+  cudaEvent_t ev[8] = {};
+  ~LapPlan() {
+    for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
+namespace {
+
+// Element counts (doubles) of the caller's output arrays.
+struct OutSizes {
+  size_t pot, grad, hess, pott, gradt, hesst;
+};
+
+OutSizes out_sizes(const LapPlan& p) {
+  const LapArgs& a = p.a;
+  const size_t cw = a.fe == FE_REAL ? 1 : 2;
+  const size_t gw = a.fe == FE_CAUCHY ? 1 : 2, hw = a.fe == FE_CAUCHY ? 1 : 3;
+  const size_t nd = p.nd, ns = p.ns, nt = p.nt;
+  OutSizes o{};
+  o.pot = a.ifpgh >= 1 ? cw * nd * ns : 0;
+  o.grad = a.ifpgh >= 2 ? cw * gw * nd * ns : 0;
+  o.hess = a.ifpgh >= 3 ? cw * hw * nd * ns : 0;
+  o.pott = a.ifpghtarg >= 1 ? cw * nd * nt : 0;
+  o.gradt = a.ifpghtarg >= 2 ? cw * gw * nd * nt : 0;
+  o.hesst = a.ifpghtarg >= 3 ? cw * hw * nd * nt : 0;
+  return o;
+}
+
+// Reads and clears the plan's device error flag after `st` has finished.
+int read_err(LapPlan& p, cudaStream_t st) {
+  int* h = pinned_ints(1);
+  B2_CHECK(cudaMemcpyAsync(h, p.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  B2_CHECK(cudaStreamSynchronize(st));
+  if (h[0]) {
+    B2_CHECK(cudaMemsetAsync(p.err.p, 0, sizeof(int), st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    return IER_TIMEOUT;
+  }
+  return IER_OK;
+}
+
+}  // namespace
+
+int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPlan** out) {
+  *out = nullptr;
   if (a.nd < 1 || a.ns < 0 || a.nt < 0 || a.ifpgh < 0 || a.ifpgh > 3 || a.ifpghtarg < 0 ||
-      a.ifpghtarg > 3 || a.ns > (1L << 30) || a.nt > (1L << 30))
+      a.ifpghtarg > 3 || a.ns > (1L << 30) || a.nt > (1L << 30) || a.fe < 0 || a.fe > 2)
     return IER_BADARG;
   if (a.ns > 0 && !a.src) return IER_BADARG;
   if (a.nt > 0 && a.ifpghtarg > 0 && !a.trg) return IER_BADARG;
-  if ((a.fe == FE_LAPLACE || a.fe == FE_REAL) && a.dipstr && !a.dipvec) return IER_BADARG;
   int dev = 0;
   B2_CHECK(cudaGetDevice(&dev));
   configure_mempool(dev);
-  const int nd = a.nd;
-  const int ndc = a.fe == FE_LAPLACE ? 2 * nd : nd;
-  const long ns = a.ns, nt = a.ifpghtarg > 0 ? a.nt : 0;
-  const bool fc = a.charge != nullptr, fd = a.dipstr != nullptr;
-  if (a.timeinfo)
-    for (int i = 0; i < 8; i++) a.timeinfo[i] = 0;
-  // user output sizes (in doubles)
-  const int cw = a.fe == FE_REAL ? 1 : 2;  // doubles per scalar output
-  const int gw = a.fe == FE_CAUCHY ? 1 : 2, hw = a.fe == FE_CAUCHY ? 1 : 3;
-  if (ns == 0 || (!fc && !fd)) {
-    // nothing interacts: every requested output is zero
-    if (a.ifpgh >= 1 && ns) B2_CHECK(cudaMemsetAsync(a.pot, 0, sizeof(double) * cw * nd * ns, st));
-    if (a.ifpgh >= 2 && ns) B2_CHECK(cudaMemsetAsync(a.grad, 0, sizeof(double) * cw * gw * nd * ns, st));
-    if (a.ifpgh >= 3 && ns) B2_CHECK(cudaMemsetAsync(a.hess, 0, sizeof(double) * cw * hw * nd * ns, st));
-    if (a.ifpghtarg >= 1 && nt) B2_CHECK(cudaMemsetAsync(a.pottarg, 0, sizeof(double) * cw * nd * nt, st));
-    if (a.ifpghtarg >= 2 && nt) B2_CHECK(cudaMemsetAsync(a.gradtarg, 0, sizeof(double) * cw * gw * nd * nt, st));
-    if (a.ifpghtarg >= 3 && nt) B2_CHECK(cudaMemsetAsync(a.hesstarg, 0, sizeof(double) * cw * hw * nd * nt, st));
+  std::unique_ptr<LapPlan> pl(new LapPlan());
+  LapPlan& p = *pl;
+  p.a = a;
+  p.a.charge = p.a.dipstr = p.a.dipvec = nullptr;
+  p.a.pot = p.a.grad = p.a.hess = p.a.pottarg = p.a.gradtarg = p.a.hesstarg = nullptr;
+  p.a.timeinfo = nullptr;
+  p.nd = a.nd;
+  p.ndc = a.fe == FE_LAPLACE ? 2 * a.nd : a.nd;
+  p.ns = a.ns;
+  p.nt = a.ifpghtarg > 0 ? a.nt : 0;
+  p.a.nt = p.nt;
+  p.fc = a.charge != nullptr;
+  p.fd = a.dipstr != nullptr;
+  if (own_stream) {
+    B2_CHECK(cudaStreamCreateWithFlags(&p.st, cudaStreamNonBlocking));
+    p.own = true;
+    // the plan's stream starts after the work already queued on the caller's
+    cudaEvent_t e;
+    B2_CHECK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    B2_CHECK(cudaEventRecord(e, st_in));
+    B2_CHECK(cudaStreamWaitEvent(p.st, e, 0));
+    B2_CHECK(cudaEventDestroy(e));
+  } else {
+    p.st = st_in;
+  }
+  cudaStream_t st = p.st;
+  for (auto& e : p.ev) B2_CHECK(cudaEventCreate(&e));
+  p.err.alloc(1, st);
+  p.err.zero(1);
+  if (p.ns == 0 || (!p.fc && !p.fd)) {
+    p.zero = true;
     B2_CHECK(cudaStreamSynchronize(st));
+    *out = pl.release();
     return IER_OK;
   }
   int ndiv = a.ndiv > 0 ? a.ndiv : lap_ndiv(a.eps);
-  if (ndiv <= 0) ndiv = (int)std::min<long>(ns + nt, 1L << 30);
-  const int p = lap_nterms(a.eps);
-  const int P = p + 1;
-  if (P > 64) return IER_NTERMS;
-  bool mixed = a.precision == PREC_MIXED || (a.precision == PREC_AUTO && a.eps >= 1e-6);
+  if (ndiv <= 0) ndiv = (int)std::min<long>(p.ns + p.nt, 1L << 30);
+  p.P = lap_nterms(a.eps) + 1;
+  if (p.P > 64) return IER_NTERMS;
+  p.mixed = a.precision == PREC_MIXED || (a.precision == PREC_AUTO && a.eps >= 1e-6);
 
-  cudaEvent_t ev[8];
-  for (int i = 0; i < 8; i++) B2_CHECK(cudaEventCreate(&ev[i]));
-  B2_CHECK(cudaEventRecord(ev[7], st));
-
-  const bool want_stats = g_stats_on.load();
-  cudaEvent_t evt[3];
-  for (int i = 0; i < 3; i++) B2_CHECK(cudaEventCreate(&evt[i]));
-  B2_CHECK(cudaEventRecord(evt[0], st));
-  DeviceTree T;
-  build_device_tree(T, a.src, ns, a.trg, nt, a.idivflag, ndiv, NLMAX, st);
-  B2_CHECK(cudaEventRecord(evt[1], st));
-  const int nb = T.nboxes;
+  cudaEvent_t e0, e1;
+  B2_CHECK(cudaEventCreate(&e0));
+  B2_CHECK(cudaEventCreate(&e1));
+  B2_CHECK(cudaEventRecord(e0, st));
+  build_device_tree(p.T, a.src, p.ns, a.trg, p.nt, a.idivflag, ndiv, NLMAX, st);
+  B2_CHECK(cudaEventRecord(e1, st));
+  DeviceTree& T = p.T;
   if (T.bs0 == 0.0) {
     // every source and target coincides: all interactions are self
     // interactions, which the reference omits, so every output is zero
-    if (a.ifpgh >= 1) B2_CHECK(cudaMemsetAsync(a.pot, 0, sizeof(double) * cw * nd * ns, st));
-    if (a.ifpgh >= 2) B2_CHECK(cudaMemsetAsync(a.grad, 0, sizeof(double) * cw * gw * nd * ns, st));
-    if (a.ifpgh >= 3) B2_CHECK(cudaMemsetAsync(a.hess, 0, sizeof(double) * cw * hw * nd * ns, st));
-    if (a.ifpghtarg >= 1 && nt) B2_CHECK(cudaMemsetAsync(a.pottarg, 0, sizeof(double) * cw * nd * nt, st));
-    if (a.ifpghtarg >= 2 && nt) B2_CHECK(cudaMemsetAsync(a.gradtarg, 0, sizeof(double) * cw * gw * nd * nt, st));
-    if (a.ifpghtarg >= 3 && nt) B2_CHECK(cudaMemsetAsync(a.hesstarg, 0, sizeof(double) * cw * hw * nd * nt, st));
+    p.zero = true;
     B2_CHECK(cudaStreamSynchronize(st));
-    for (int i = 0; i < 3; i++) cudaEventDestroy(evt[i]);
-    for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *out = pl.release();
     return IER_OK;
   }
-
+  const int nb = T.nboxes;
   std::vector<double> bsx(T.boxsize);
   bsx.push_back(T.boxsize.back() / 2);
-  DBuf<double> dbs(st);
-  dbs.alloc(bsx.size(), st);
-  B2_CHECK(cudaMemcpyAsync(dbs.p, bsx.data(), sizeof(double) * bsx.size(), cudaMemcpyHostToDevice, st));
-
-  // sorted points and densities
-  DBuf<double2> xs(st), xt(st), qs(st), ds(st);
-  xs.alloc(ns, st);
-  k_gather_pts<<<ceil_div(ns, 256), 256, 0, st>>>(a.src, T.isrc.p, ns, xs.p);
+  p.dbs.alloc(bsx.size(), st);
+  B2_CHECK(cudaMemcpyAsync(p.dbs.p, bsx.data(), sizeof(double) * bsx.size(),
+                           cudaMemcpyHostToDevice, st));
+  p.xs.alloc(p.ns, st);
+  k_gather_pts<<<ceil_div(p.ns, 256), 256, 0, st>>>(a.src, T.isrc.p, p.ns, p.xs.p);
   B2_LAUNCH_CHECK();
-  if (nt > 0) {
-    xt.alloc(nt, st);
-    k_gather_pts<<<ceil_div(nt, 256), 256, 0, st>>>(a.trg, T.itarg.p, nt, xt.p);
+  if (p.nt > 0) {
+    p.xt.alloc(p.nt, st);
+    k_gather_pts<<<ceil_div(p.nt, 256), 256, 0, st>>>(a.trg, T.itarg.p, p.nt, p.xt.p);
     B2_LAUNCH_CHECK();
   }
-  if (fc) qs.alloc((size_t)ns * ndc, st);
-  if (fd) ds.alloc((size_t)ns * ndc, st);
-  k_gather_dens<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, T.isrc.p, ns, a.charge, a.dipstr,
-                                                   a.dipvec, qs.p, ds.p);
-  B2_LAUNCH_CHECK();
-
-  // sorted Cauchy results
-  DBuf<double2> ps(st), gs(st), hs(st), pt(st), gt(st), ht(st);
-  if (a.ifpgh >= 1) ps.alloc((size_t)ns * ndc, st);
-  if (a.ifpgh >= 2) gs.alloc((size_t)ns * ndc, st);
-  if (a.ifpgh >= 3) hs.alloc((size_t)ns * ndc, st);
-  if (a.ifpghtarg >= 1 && nt) pt.alloc((size_t)nt * ndc, st);
-  if (a.ifpghtarg >= 2 && nt) gt.alloc((size_t)nt * ndc, st);
-  if (a.ifpghtarg >= 3 && nt) ht.alloc((size_t)nt * ndc, st);
-
-  TV tv{T.center.p, T.level.p, T.nchild.p, T.child.p, T.srng.p, T.trng.p, T.nlist1.p, T.list1.p,
-        T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p, dbs.p, a.ifpgh,
-        nt > 0 ? a.ifpghtarg : 0};
-  const double thresh = T.bs0 * std::ldexp(1.0, -51);
-  DBuf<unsigned long long> dstat(st);
-  if (want_stats) {
-    dstat.alloc(6, st);
-    dstat.zero(6);
-    k_stats<<<ceil_div(nb, 256), 256, 0, st>>>(tv, nb, dstat.p);
-    B2_LAUNCH_CHECK();
+  const size_t nsd = (size_t)p.ns * p.ndc, ntd = (size_t)p.nt * p.ndc;
+  if (p.fc) p.qs.alloc(nsd, st);
+  if (p.fd) p.ds.alloc(nsd, st);
+  if (a.ifpgh >= 1) p.ps.alloc(nsd, st);
+  if (a.ifpgh >= 2) p.gs.alloc(nsd, st);
+  if (a.ifpgh >= 3) p.hs.alloc(nsd, st);
+  if (a.ifpghtarg >= 1 && p.nt) p.pt.alloc(ntd, st);
+  if (a.ifpghtarg >= 2 && p.nt) p.gt.alloc(ntd, st);
+  if (a.ifpghtarg >= 3 && p.nt) p.ht.alloc(ntd, st);
+  p.tv = TV{T.center.p, T.level.p, T.nchild.p, T.child.p, T.srng.p, T.trng.p, T.nlist1.p,
+            T.list1.p, T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p,
+            p.dbs.p, a.ifpgh, p.nt > 0 ? a.ifpghtarg : 0};
+  p.thresh = T.bs0 * std::ldexp(1.0, -51);
+  p.chunk = p.ndc >= 8 ? 8 : (p.ndc >= 4 ? 4 : (p.ndc >= 2 ? 2 : 1));
+  p.mp.alloc((size_t)nb * p.P * p.chunk, st);
+  p.lo.alloc((size_t)nb * p.P * p.chunk, st);
+  if (p.mixed) {
+    lap_mixed_prepare(p.MD, p.xs.p, p.ns, p.xt.p, p.nt, p.fc, p.fd, p.ndc, T.cx0, T.cy0, p.P, st);
+    p.MD.err = p.err.p;
+    if (T.nlevels >= 2 && T.nlevels < 64 && m2l_tensor_cores() && m2l_tc_supported(p.P)) {
+      p.MD.tc = true;
+      p.MD.nlev = T.nlevels + 1;
+      p.MD.nboxes = nb;
+      m2l_tc_build_pairs(p.MD.pairs, p.tv, T.lfirst[2], nb - T.lfirst[2], nb, st);
+      if (p.MD.pairs.npairs > 0) p.MD.mp32.alloc((size_t)nb * p.P * p.chunk, st);
+    }
   }
-  int chunk = ndc >= 8 ? 8 : (ndc >= 4 ? 4 : (ndc >= 2 ? 2 : 1));
-  DBuf<double2> mp(st), lo(st);
-  mp.alloc((size_t)nb * P * chunk, st);
-  lo.alloc((size_t)nb * P * chunk, st);
+  device_binomials();
+  B2_CHECK(cudaStreamSynchronize(st));
+  B2_CHECK(cudaEventElapsedTime(&p.tree_ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *out = pl.release();
+  return IER_OK;
+}
+
+int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const double* dipvec,
+                  double* pot, double* grad, double* hess, double* pottarg, double* gradtarg,
+                  double* hesstarg, cudaStream_t st, bool sync, double* timeinfo) {
+  if (!pp) return IER_BADARG;
+  LapPlan& p = *pp;
+  const LapArgs& a = p.a;
+  if ((charge != nullptr) != p.fc || (dipstr != nullptr) != p.fd) return IER_BADARG;
+  if ((a.fe == FE_LAPLACE || a.fe == FE_REAL) && dipstr && !dipvec) return IER_BADARG;
+  const OutSizes o = out_sizes(p);
+  if ((o.pot && !pot) || (o.grad && !grad) || (o.hess && !hess) || (o.pott && !pottarg) ||
+      (o.gradt && !gradtarg) || (o.hesst && !hesstarg))
+    return IER_BADARG;
+  if (timeinfo)
+    for (int i = 0; i < 8; i++) timeinfo[i] = 0;
+  if (p.zero) {
+    auto z = [&](double* d, size_t n) {
+      if (n) B2_CHECK(cudaMemsetAsync(d, 0, sizeof(double) * n, st));
+    };
+    z(pot, o.pot);
+    z(grad, o.grad);
+    z(hess, o.hess);
+    z(pottarg, o.pott);
+    z(gradtarg, o.gradt);
+    z(hesstarg, o.hesst);
+    if (sync) B2_CHECK(cudaStreamSynchronize(st));
+    return IER_OK;
+  }
+  DeviceTree& T = p.T;
+  const long ns = p.ns, nt = p.nt;
+  const int nd = p.nd, ndc = p.ndc, P = p.P;
+  k_gather_dens<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, T.isrc.p, ns, charge, dipstr,
+                                                   dipvec, p.qs.p, p.ds.p);
+  B2_LAUNCH_CHECK();
+  if (p.mixed) lap_mixed_densities(p.MD, p.qs.p, p.ds.p, ns, ndc, st);
+  const MixedData* Mp = p.mixed ? &p.MD : nullptr;
   double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  MixedData MD;
-  if (mixed)
-    lap_mixed_prepare(MD, xs.p, ns, xt.p, nt, fc ? qs.p : nullptr, fd ? ds.p : nullptr, ndc, T.cx0,
-                      T.cy0, P, st);
-  const MixedData* Mp = mixed ? &MD : nullptr;
   for (int d0 = 0; d0 < ndc;) {
     int left = ndc - d0;
     int ND = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
-    Dens D{fc ? qs.p : nullptr, fd ? ds.p : nullptr, ndc, d0};
+    Dens D{p.fc ? p.qs.p : nullptr, p.fd ? p.ds.p : nullptr, ndc, d0};
     switch (ND) {
-      case 8: run_chunk<8>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
-      case 4: run_chunk<4>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
-      case 2: run_chunk<2>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
-      default: run_chunk<1>(tv, T, a, D, P, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev, Mp); break;
+      case 8: run_chunk<8>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
+      case 4: run_chunk<4>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
+      case 2: run_chunk<2>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
+      default: run_chunk<1>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
     }
-    if (a.timeinfo) {
-      B2_CHECK(cudaEventSynchronize(ev[6]));
+    if (timeinfo) {
+      B2_CHECK(cudaEventSynchronize(p.ev[6]));
       float ms[6];
-      for (int i = 0; i < 6; i++) B2_CHECK(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+      for (int i = 0; i < 6; i++) B2_CHECK(cudaEventElapsedTime(&ms[i], p.ev[i], p.ev[i + 1]));
       // reference buckets: 1 P2M, 2 P2L, 3 M2M, 4 M2L, 5 L2L, 6 M2P, 7 L2P, 8 P2P;
       // M2P/L2P/P2P run fused in one kernel and are reported in bucket 8.
       tsum[0] += ms[0] * 1e-3;
@@ -1075,42 +1175,86 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st) {
     d0 += ND;
   }
   if (a.ifpgh > 0) {
-    k_unpack<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpgh, T.isrc.p, ns, ps.p, gs.p,
-                                                hs.p, a.pot, a.grad, a.hess);
+    k_unpack<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpgh, T.isrc.p, ns, p.ps.p,
+                                                p.gs.p, p.hs.p, pot, grad, hess);
     B2_LAUNCH_CHECK();
   }
   if (a.ifpghtarg > 0 && nt > 0) {
-    k_unpack<<<ceil_div(nt, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpghtarg, T.itarg.p, nt, pt.p,
-                                                gt.p, ht.p, a.pottarg, a.gradtarg, a.hesstarg);
+    k_unpack<<<ceil_div(nt, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpghtarg, T.itarg.p, nt, p.pt.p,
+                                                p.gt.p, p.ht.p, pottarg, gradtarg, hesstarg);
     B2_LAUNCH_CHECK();
   }
-  B2_CHECK(cudaEventRecord(evt[2], st));
-  B2_CHECK(cudaStreamSynchronize(st));
-  if (a.timeinfo)
-    for (int i = 0; i < 8; i++) a.timeinfo[i] = tsum[i];
-  if (want_stats) {
+  if (timeinfo)
+    for (int i = 0; i < 8; i++) timeinfo[i] = tsum[i];
+  if (sync) {
+    B2_CHECK(cudaStreamSynchronize(st));
+    return read_err(p, st);
+  }
+  return IER_OK;
+}
+
+int lap_plan_status(LapPlan* p) {
+  if (!p) return IER_BADARG;
+  B2_CHECK(cudaDeviceSynchronize());
+  return read_err(*p, p->st);
+}
+
+void lap_plan_free(LapPlan* p) {
+  if (!p) return;
+  cudaStream_t st = p->st;
+  bool own = p->own;
+  if (own) cudaDeviceSynchronize();  // evaluations may have run on other streams
+  delete p;                          // buffers are released on the plan's stream
+  if (own) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+}
+
+int lap_fmm_device(const LapArgs& a, cudaStream_t st) {
+  if ((a.fe == FE_LAPLACE || a.fe == FE_REAL) && a.dipstr && !a.dipvec) return IER_BADARG;
+  LapPlan* p = nullptr;
+  int r = lap_plan_create(a, st, false, &p);
+  if (r != IER_OK) return r;
+  std::unique_ptr<LapPlan, void (*)(LapPlan*)> guard(p, lap_plan_free);
+  const bool want_stats = g_stats_on.load();
+  DBuf<unsigned long long> dstat(st);
+  if (want_stats && !p->zero) {
+    dstat.alloc(6, st);
+    dstat.zero(6);
+    k_stats<<<ceil_div(p->T.nboxes, 256), 256, 0, st>>>(p->tv, p->T.nboxes, dstat.p);
+    B2_LAUNCH_CHECK();
+  }
+  cudaEvent_t e0, e1;
+  B2_CHECK(cudaEventCreate(&e0));
+  B2_CHECK(cudaEventCreate(&e1));
+  B2_CHECK(cudaEventRecord(e0, st));
+  r = lap_plan_eval(p, a.charge, a.dipstr, a.dipvec, a.pot, a.grad, a.hess, a.pottarg, a.gradtarg,
+                    a.hesstarg, st, true, a.timeinfo);
+  B2_CHECK(cudaEventRecord(e1, st));
+  B2_CHECK(cudaEventSynchronize(e1));
+  if (want_stats && !p->zero && r == IER_OK) {
     unsigned long long hs6[6];
     B2_CHECK(cudaMemcpy(hs6, dstat.p, sizeof(hs6), cudaMemcpyDeviceToHost));
-    float t1 = 0, t2 = 0;
-    B2_CHECK(cudaEventElapsedTime(&t1, evt[0], evt[1]));
-    B2_CHECK(cudaEventElapsedTime(&t2, evt[1], evt[2]));
+    float t2 = 0;
+    B2_CHECK(cudaEventElapsedTime(&t2, e0, e1));
     LapStats& S = g_last_stats;
-    S.nboxes = nb;
-    S.nlevels = T.nlevels;
+    S.nboxes = p->T.nboxes;
+    S.nlevels = p->T.nlevels;
     S.nleaves = (double)hs6[0];
-    S.nterms1 = P;
+    S.nterms1 = p->P;
     S.p2p_pairs = (double)hs6[1];
     S.m2l_pairs = (double)hs6[2];
     S.m2p_evals = (double)hs6[3];
     S.p2l_sources = (double)hs6[4];
     S.npts_eval = (double)hs6[5];
-    S.tree_ms = t1;
+    S.tree_ms = p->tree_ms;
     S.fmm_ms = t2;
-    S.nd_cauchy = ndc;
+    S.nd_cauchy = p->ndc;
   }
-  for (int i = 0; i < 3; i++) cudaEventDestroy(evt[i]);
-  for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
-  return IER_OK;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return r;
 }
 
 }  // namespace b2

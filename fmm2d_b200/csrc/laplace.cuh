@@ -41,6 +41,24 @@ struct LapArgs {
 // Runs the FMM on device pointers on stream `st`; returns an ier code.
 int lap_fmm_device(const LapArgs& a, cudaStream_t st);
 
+// A plan holds everything of an FMM call that depends only on the points:
+// the tree and lists, the sorted points, the operator tables and every work
+// buffer.  lap_plan_eval then runs the density-dependent part (gather, the
+// eight FMM steps, unsort) as stream work only: no allocation, no host
+// synchronisation unless `sync` is set, so it can be captured in a CUDA
+// graph.  One plan must not be evaluated on two streams at the same time.
+// `a` gives the geometry and flags; its charge / dipstr pointers only mark
+// which densities later evaluations pass (non-null = present).
+struct LapPlan;
+int lap_plan_create(const LapArgs& a, cudaStream_t st, bool own_stream, LapPlan** out);
+int lap_plan_eval(LapPlan* p, const double* charge, const double* dipstr, const double* dipvec,
+                  double* pot, double* grad, double* hess, double* pottarg, double* gradtarg,
+                  double* hesstarg, cudaStream_t st, bool sync, double* timeinfo);
+// IER_TIMEOUT when a bounded tensor-core wait of an earlier evaluation gave
+// up, else IER_OK; clears the flag.  Synchronises the device.
+int lap_plan_status(LapPlan* p);
+void lap_plan_free(LapPlan* p);
+
 int lap_nterms(double eps);
 int lap_ndiv(double eps);
 

@@ -201,6 +201,62 @@ int b2fmm_h2dterms(double bsize, double zk_re, double zk_im, double eps, int* ie
  * out holds 2(n+1) doubles for kinds 1 and 2. */
 void b2fmm_helm_special(int kind, int n, double z_re, double z_im, double rscale, double* out);
 
+/* ------------------------------------------- plans and batches (no reference counterpart) */
+
+/* A plan is the point-dependent part of a Laplace / Cauchy FMM call (fe: 0
+ * cfmm2d, 1 lfmm2d, 2 rfmm2d): tree, lists, sorted points and every work
+ * buffer, built once for fixed sources / targets / flags (the reference
+ * rebuilds them in every call of cfmm2d.f:23-436).  Device pointers;
+ * ifcharge / ifdipole fix which densities the evaluations pass.  The plan
+ * has its own stream; NULL is returned (and *ier set) on error. */
+void* b2fmm_plan_create(int fe, int nd, double eps, int64_t ns, const double* sources,
+                        int ifcharge, int ifdipole, int ifpgh, int64_t nt, const double* targ,
+                        int ifpghtarg, const b2fmm_options* opts, void* stream, int* ier);
+
+/* Enqueue one evaluation of a plan for new densities on `stream` (device
+ * pointers, the layouts of the matching b2fmm_*fmm2d_dev call).  Stream work
+ * only: no allocation and no host synchronisation, so it may be captured in a
+ * CUDA graph; *ier reports argument errors.  A plan must not run on two
+ * streams at once. */
+void b2fmm_plan_eval(void* plan, const double* charge, const double* dipstr, const double* dipvec,
+                     double* pot, double* grad, double* hess, double* pottarg, double* gradtarg,
+                     double* hesstarg, void* stream, int* ier);
+
+/* Synchronises the device; 102 if a bounded tensor-core wait of an earlier
+ * evaluation gave up (clears the flag), else 0. */
+int b2fmm_plan_status(void* plan);
+void b2fmm_plan_free(void* plan);
+
+/* One CUDA graph holding one evaluation of each of n plans, spread over
+ * nbranch concurrent branches.  The arrays hold one device pointer per plan
+ * (NULL array = argument absent for all).  Every plan is evaluated once,
+ * synchronously, before the capture.  Plans and pointers must outlive the
+ * graph. */
+void* b2fmm_batch_graph_create(int n, void* const* plans, const double* const* charge,
+                               const double* const* dipstr, const double* const* dipvec,
+                               double* const* pot, double* const* grad, double* const* hess,
+                               double* const* pottarg, double* const* gradtarg,
+                               double* const* hesstarg, int nbranch, int* ier);
+void b2fmm_batch_graph_launch(void* graph, void* stream, int* ier);
+int b2fmm_batch_graph_status(void* graph);
+int64_t b2fmm_batch_graph_nodes(void* graph);
+void b2fmm_batch_graph_free(void* graph);
+
+/* ------------------------------------------------- tensor-core M2L (no reference counterpart) */
+
+/* Mixed-precision Laplace M2L engine switch: 1 (default) runs the list-2
+ * translations (laprouts2d.f:1130-1244) as split-TF32 tcgen05 tensor-core
+ * tiles; 0 runs the FP32 CUDA-core kernel.  Process-wide. */
+void b2fmm_set_m2l_tensor_cores(int on);
+
+/* Check of the tensor-core tile path: D = A B^T for A 128 x k and B n x k
+ * (row-major FP32 device arrays; k in {8,16,24,32}, n in {16,32}) through the
+ * same shared-memory layout, split-TF32 tcgen05.mma and tcgen05.ld read-back
+ * as the M2L kernel.  D is 128 x n row-major.  ier 102 if the bounded wait
+ * for the tensor cores expired. */
+void b2fmm_tc_gemm_probe(const float* a_dev, const float* b_dev, int k, int n, float* d_dev,
+                         void* stream, int* ier);
+
 /* ------------------------------------------------------------------- tree */
 
 /* Level-restricted tree and lists for (sources, targets), exported for

@@ -1,0 +1,90 @@
+"""Tensor-core (tcgen05) M2L: the tile path against an FP64 GEMM, and the
+mixed-precision FMM with the tensor-core M2L against the CUDA-core M2L, the
+FP64 FMM and the direct sum."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import fmm2d_b200 as fmm
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def tc_on():
+    L = fmm._lib.lib()
+    L.b2fmm_set_m2l_tensor_cores(1)
+    yield L
+    L.b2fmm_set_m2l_tensor_cores(1)
+
+
+@pytest.mark.parametrize("k", [8, 16, 24, 32])
+@pytest.mark.parametrize("n", [16, 32])
+def test_tc_gemm_probe_split_tf32(gpu, k, n):
+    """D = A B^T through the shared-memory layout, split-TF32 tcgen05.mma and
+    tcgen05.ld of the M2L kernel: FP32-level accuracy."""
+    import torch
+    rng = np.random.default_rng(k * 100 + n)
+    a = rng.normal(size=(128, k)).astype(np.float32)
+    b = rng.normal(size=(n, k)).astype(np.float32)
+    ta = torch.as_tensor(a, device=gpu)
+    tb = torch.as_tensor(b, device=gpu)
+    td = torch.full((128, n), np.nan, dtype=torch.float32, device=gpu)
+    ier = C.c_int(-1)
+    fmm._lib.lib().b2fmm_tc_gemm_probe(C.c_void_p(ta.data_ptr()), C.c_void_p(tb.data_ptr()), k, n,
+                                       C.c_void_p(td.data_ptr()),
+                                       C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                       C.byref(ier))
+    assert ier.value == 0
+    d = td.cpu().numpy().astype(np.float64)
+    ref = a.astype(np.float64) @ b.astype(np.float64).T
+    scale = np.abs(a).astype(np.float64) @ np.abs(b).astype(np.float64).T
+    assert np.all(np.isfinite(d))
+    assert np.max(np.abs(d - ref) / scale) < 2e-6
+
+
+def _cloud(seed, n):
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0, 1, (2, 8))
+    sig = 10 ** rng.uniform(-3, -1, 8)
+    k = rng.integers(0, 8, n)
+    src = c[:, k] + sig[k] * rng.normal(size=(2, n))
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    d = rng.normal(size=n) + 1j * rng.normal(size=n)
+    v = rng.uniform(-1, 1, (2, n))
+    return src, q, d, v
+
+
+@pytest.mark.parametrize("eps", [1e-3, 1e-6])
+@pytest.mark.parametrize("nd", [1, 3])
+def test_mixed_tc_matches_cuda_core_m2l(gpu, tc_on, eps, nd):
+    src, q, d, v = _cloud(3, 40000)
+    if nd > 1:
+        rng = np.random.default_rng(4)
+        q = rng.normal(size=(nd, 40000)) + 1j * rng.normal(size=(nd, 40000))
+        d = v = None
+    kw = dict(eps=eps, sources=src, charges=q, dipstr=d, dipvec=v, pg=2, nd=nd,
+              precision="mixed")
+    out_tc = fmm.lfmm2d(**kw)
+    tc_on.b2fmm_set_m2l_tensor_cores(0)
+    out_cc = fmm.lfmm2d(**kw)
+    tc_on.b2fmm_set_m2l_tensor_cores(1)
+    out_64 = fmm.lfmm2d(**{**kw, "precision": "fp64"})
+    assert out_tc.ier == 0 and out_cc.ier == 0
+    # both mixed engines agree with the FP64 FMM far below eps
+    assert rel_l2(out_tc.pot, out_64.pot) < 1e-6
+    assert rel_l2(out_tc.grad, out_64.grad) < 1e-6
+    assert rel_l2(out_tc.pot, out_cc.pot) < 1e-6
+
+
+def test_mixed_tc_vs_direct_4_densities(gpu, tc_on):
+    """nd = 2 complex -> 4 Cauchy densities per chunk (ND = 4 tiles)."""
+    src, q, d, v = _cloud(5, 60000)
+    rng = np.random.default_rng(6)
+    q2 = rng.normal(size=(2, 60000)) + 1j * rng.normal(size=(2, 60000))
+    out = fmm.lfmm2d(eps=1e-6, sources=src, charges=q2, pg=2, nd=2, precision="mixed")
+    ex = fmm.l2ddir(sources=src, targets=src[:, :500], charges=q2, pgt=2, nd=2)
+    assert rel_l2(out.pot[:, :500], ex.pottarg) < 1e-6
+    assert rel_l2(out.grad[:, :, :500], ex.gradtarg) < 1e-6
