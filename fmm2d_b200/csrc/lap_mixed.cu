@@ -7,13 +7,13 @@
 //   multipole (FP64 -> FP32) and the fixed matrix G(i,j) = C(i+j-1, j-1)
 //   remain.  Local expansions are accumulated in FP32 per target box and
 //   added to the FP64 expansion once.
-// * k_leaf_mixed: L2P and M2P in FP64 (as the FP64 path), the near field in
-//   FP32.  Coordinates are stored as x - c0 split into hi + lo floats, so a
-//   difference (xt_hi - xs_hi) + (xt_lo - xs_lo) keeps the relative accuracy
-//   of the FP64 difference even for nearly coincident points; log and 1/r^2
-//   use the SFU.  Per-pair terms are summed in FP32 over at most 32 sources
-//   and the partial sums in FP64.  Small leaves split their sources between
-//   2 or 4 lane groups so that the warp stays busy.
+// * k_far_mixed / k_p2p_mixed: one evaluation point per thread.  L2P and M2P
+//   in FP64 (as the FP64 path), then the near field in FP32.  Coordinates are
+//   stored as x - c0 split into hi + lo floats, so a difference
+//   (xt_hi - xs_hi) + (xt_lo - xs_lo) keeps the relative accuracy of the FP64
+//   difference even for nearly coincident points; log and 1/r^2 use the SFU.
+//   Per-pair terms are summed in FP32 over at most 32 sources and the
+//   partial sums in FP64.
 #include "lap_mixed.cuh"
 
 #include <atomic>
@@ -230,222 +230,207 @@ __global__ void __launch_bounds__(128) k_m2l_f32(TV t, int first, int n, int P, 
   }
 }
 
+// Leaf box of every evaluation point (points are in tree order).
+__global__ void k_point_leaf(TV t, int nb, int use_targets, int* __restrict__ leaf) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb || t.nchild[b] != 0) return;
+  int2 r = use_targets ? t.trng[b] : t.srng[b];
+  for (int k = r.x; k < r.y; k++) leaf[k] = b;
+}
+
+// Far field of one evaluation point per thread, FP64: L2P from the local
+// expansion of its leaf and M2P from the leaf's list-3 boxes (the
+// coefficients of one box are shared by the neighbouring threads of the same
+// leaf through the L1 cache).  Writes pot / grad / hess of the point.
 template <int ND, int IFPGH>
-__global__ void __launch_bounds__(128) k_leaf_mixed(
-    TV t, int nb, int use_targets, const float4* __restrict__ xs32,
-    const float4* __restrict__ xe32, const double2* __restrict__ xe64,
-    const float2* __restrict__ q32, const float2* __restrict__ d32, int ndc, int d0, int P,
-    const double2* __restrict__ mp, const double2* __restrict__ lo, float th2, int ifnear,
+__global__ void __launch_bounds__(128) k_far_mixed(
+    TV t, long n, const int* __restrict__ leaf, const double2* __restrict__ xe64, int ndc, int d0,
+    int P, const double2* __restrict__ mp, const double2* __restrict__ lo,
     double2* __restrict__ pot, double2* __restrict__ grad, double2* __restrict__ hess) {
-  extern __shared__ double2 smd[];
-  const bool hq = q32 != nullptr, hd = d32 != nullptr;
-  WARP_LOOP(nb) {
-    double2* coef = smd + (size_t)wib * (P * ND + 32 + 32 * ND);
-    float4* SX = (float4*)(coef + P * ND);
-    float2* SQ = (float2*)(SX + 32);
-    float2* SD = SQ + 32 * ND;
-    int b = bi;
-    if (t.nchild[b] != 0) continue;
-    int2 er = use_targets ? t.trng[b] : t.srng[b];
-    int ne = er.y - er.x;
-    if (ne <= 0) continue;
-    const int LG2G = ne <= 8 ? 2 : (ne <= 16 ? 1 : 0);  // log2 of the lane groups
-    const int G = 1 << LG2G, TW = 32 >> LG2G;
-    const int g = lane / TW, tl = lane % TW;
-    int lev = t.level[b];
-    double r = t.boxsize[lev];
-    double2 cb = t.center[b];
-    int n3 = t.nl3[b], n1 = ifnear ? t.nl1[b] : 0;
-    // list-1 sources as one concatenated index range
-    int l1s[MNLIST1], cum[MNLIST1 + 1];
-    cum[0] = 0;
-    for (int e = 0; e < MNLIST1; e++) {
-      int2 sr = e < n1 ? t.srng[t.l1[(size_t)MNLIST1 * b + e]] : make_int2(0, 0);
-      l1s[e] = sr.x;
-      cum[e + 1] = cum[e] + (sr.y - sr.x);
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int b = leaf[k];
+  const int lev = t.level[b];
+  const double r = t.boxsize[lev];
+  const double2 cb = t.center[b];
+  const double2 z = xe64[k];
+  double2 pt[ND], gr[ND], hs[ND];
+  {
+    // L2P: sum_m L_m ((z - c) / r)^m and derivatives (Horner)
+    const double2* L = lo + (size_t)b * P * ND;
+    double2 zz = make_double2((z.x - cb.x) / r, (z.y - cb.y) / r);
+    double2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      f[d] = L[(P - 1) * ND + d];
+      f1[d] = f2[d] = make_double2(0, 0);
     }
-    const int tot = cum[MNLIST1];
-    for (int k0 = er.x; k0 < er.y; k0 += TW) {
-      int k = k0 + tl;
-      bool act = k < er.y;
-      double2 z = act ? xe64[k] : cb;
-      float4 zf = act ? xe32[k] : make_float4(0.f, 0.f, 0.f, 0.f);
-      double2 pt[ND], gr[ND], hs[ND];
+    for (int m = P - 2; m >= 0; m--) {
 #pragma unroll
-      for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
-      // L2P (FP64) by lane group 0
-      __syncwarp();
-      for (int e = lane; e < P * ND; e += 32) coef[e] = lo[(size_t)b * P * ND + e];
-      __syncwarp();
-      if (g == 0) {
-        double2 zz = make_double2((z.x - cb.x) / r, (z.y - cb.y) / r);
-        double2 f[ND], f1[ND], f2[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          f[d] = coef[(P - 1) * ND + d];
-          f1[d] = f2[d] = make_double2(0, 0);
-        }
-        for (int m = P - 2; m >= 0; m--) {
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], zz), f1[d]);
-            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], zz), f[d]);
-            f[d] = cadd(cmul(f[d], zz), coef[m * ND + d]);
-          }
-        }
-        double ri = 1.0 / r;
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          pt[d] = f[d];
-          if (IFPGH >= 2) gr[d] = cscale(f1[d], ri);
-          if (IFPGH >= 3) hs[d] = cscale(f2[d], 2.0 * ri * ri);
-        }
+      for (int d = 0; d < ND; d++) {
+        if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], zz), f1[d]);
+        if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], zz), f[d]);
+        f[d] = cadd(cmul(f[d], zz), L[m * ND + d]);
       }
-      // M2P (FP64), list-3 box e by lane group e mod G
-      for (int e = 0; e < n3; e++) {
-        int jb = t.l3[(size_t)MNLIST3 * b + e];
-        __syncwarp();
-        for (int q = lane; q < P * ND; q += 32) coef[q] = mp[(size_t)jb * P * ND + q];
-        __syncwarp();
-        if ((e & (G - 1)) != g) continue;
-        double rj = t.boxsize[lev + 1];
-        double2 cj = t.center[jb];
-        double2 zc = make_double2(z.x - cj.x, z.y - cj.y);
-        double2 zi = crcp(zc);
-        double2 w = make_double2(rj * zi.x, rj * zi.y);
-        double lg = log(hypot(zc.x, zc.y));
-        double2 f[ND], f1[ND], f2[ND];
+    }
+    double ri = 1.0 / r;
 #pragma unroll
-        for (int d = 0; d < ND; d++) {
-          f[d] = coef[(P - 1) * ND + d];
-          f1[d] = f2[d] = make_double2(0, 0);
-        }
-        for (int m = P - 2; m >= 1; m--) {
+    for (int d = 0; d < ND; d++) {
+      pt[d] = f[d];
+      gr[d] = IFPGH >= 2 ? cscale(f1[d], ri) : make_double2(0, 0);
+      hs[d] = IFPGH >= 3 ? cscale(f2[d], 2.0 * ri * ri) : make_double2(0, 0);
+    }
+  }
+  const int n3 = t.nl3[b];
+  for (int e = 0; e < n3; e++) {
+    // M2P: c_0 log(z - c) + sum_{m>=1} c_m (r_j / (z - c))^m
+    int jb = t.l3[(size_t)MNLIST3 * b + e];
+    const double2* M = mp + (size_t)jb * P * ND;
+    double rj = t.boxsize[lev + 1];
+    double2 cj = t.center[jb];
+    double2 zc = make_double2(z.x - cj.x, z.y - cj.y);
+    double2 zi = crcp(zc);
+    double2 w = make_double2(rj * zi.x, rj * zi.y);
+    double lg = log(hypot(zc.x, zc.y));
+    double2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      f[d] = M[(P - 1) * ND + d];
+      f1[d] = f2[d] = make_double2(0, 0);
+    }
+    for (int m = P - 2; m >= 1; m--) {
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], w), f1[d]);
+        if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], w), f[d]);
+        f[d] = cadd(cmul(f[d], w), M[m * ND + d]);
+      }
+    }
+    double2 w2 = cmul(w, w);
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      double2 c0 = M[d];
+      double2 Sv = cmul(w, f[d]);
+      double2 S1 = cadd(f[d], cmul(w, f1[d]));
+      pt[d].x += Sv.x + c0.x * lg;
+      pt[d].y += Sv.y + c0.y * lg;
+      if (IFPGH >= 2) {
+        double2 gg = cmul(S1, w2);
+        gg = make_double2(-gg.x / rj, -gg.y / rj);
+        gr[d] = cadd(gr[d], cadd(gg, cmul(c0, zi)));
+      }
+      if (IFPGH >= 3) {
+        double2 S2 = cscale(cadd(f1[d], cmul(w, f2[d])), 2.0);
+        double2 w3 = cmul(w2, w), w4 = cmul(w2, w2);
+        double2 h = cadd(cmul(S2, w4), cscale(cmul(S1, w3), 2.0));
+        h = cscale(h, 1.0 / (rj * rj));
+        hs[d] = cadd(hs[d], csub(h, cmul(c0, cmul(zi, zi))));
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    size_t o = (size_t)k * ndc + d0 + d;
+    pot[o] = pt[d];
+    if (IFPGH >= 2) grad[o] = gr[d];
+    if (IFPGH >= 3) hess[o] = hs[d];
+  }
+}
+
+// Near field of one evaluation point per thread, FP32 (cauchykernels2d.f):
+// all sources of the leaf's list-1 boxes; coordinate differences from the
+// hi/lo float pairs, per-pair terms summed in FP32 over at most 32 sources,
+// the partial sums in FP64, added to the far field already in the outputs.
+template <int ND, int IFPGH>
+__global__ void __launch_bounds__(128) k_p2p_mixed(
+    TV t, long n, const int* __restrict__ leaf, const float4* __restrict__ xs32,
+    const float4* __restrict__ xe32, const float2* __restrict__ q32,
+    const float2* __restrict__ d32, int ndc, int d0, float th2, double2* __restrict__ pot,
+    double2* __restrict__ grad, double2* __restrict__ hess) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const bool hq = q32 != nullptr, hd = d32 != nullptr;
+  const int b = leaf[k];
+  const float4 zf = xe32[k];
+  double2 pt[ND], gr[ND], hs[ND];
+#pragma unroll
+  for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
+  float2 fp[ND], fg[ND], fh[ND];
+#pragma unroll
+  for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
+  int cnt = 0;
+  const int n1 = t.nl1[b];
+  for (int e = 0; e < n1; e++) {
+    int2 sr = t.srng[t.l1[(size_t)MNLIST1 * b + e]];
+    for (int j = sr.x; j < sr.y; j++) {
+      float4 s = xs32[j];
+      float dx = (zf.x - s.x) + (zf.z - s.z);
+      float dy = (zf.y - s.y) + (zf.w - s.w);
+      float rr = fmaf(dx, dx, dy * dy);
+      // cauchykernels2d.f: <= for potential-only, < otherwise
+      if (!(IFPGH == 1 ? (rr <= th2) : (rr < th2))) {
+        float ir = __fdividef(1.0f, rr);
+        float2 zi = make_float2(dx * ir, -dy * ir);
+        float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
+        if (hq) {
+          float lg = 0.5f * __logf(rr);
 #pragma unroll
           for (int d = 0; d < ND; d++) {
-            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], w), f1[d]);
-            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], w), f[d]);
-            f[d] = cadd(cmul(f[d], w), coef[m * ND + d]);
+            float2 c = q32[(size_t)j * ndc + d0 + d];
+            fp[d].x = fmaf(lg, c.x, fp[d].x);
+            fp[d].y = fmaf(lg, c.y, fp[d].y);
+            if (IFPGH >= 2) cfmaf_(fg[d], zi, c);
+            if (IFPGH >= 3) cfmaf_(fh[d], z2, c);
           }
         }
-        double2 w2 = cmul(w, w);
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          double2 c0 = coef[d];
-          double2 Sv = cmul(w, f[d]);
-          double2 S1 = cadd(f[d], cmul(w, f1[d]));
-          pt[d].x += Sv.x + c0.x * lg;
-          pt[d].y += Sv.y + c0.y * lg;
-          if (IFPGH >= 2) {
-            double2 gg = cmul(S1, w2);
-            gg = make_double2(-gg.x / rj, -gg.y / rj);
-            gr[d] = cadd(gr[d], cadd(gg, cmul(c0, zi)));
-          }
+        if (hd) {
+          float2 z3 = make_float2(0.f, 0.f);
           if (IFPGH >= 3) {
-            double2 S2 = cscale(cadd(f1[d], cmul(w, f2[d])), 2.0);
-            double2 w3 = cmul(w2, w), w4 = cmul(w2, w2);
-            double2 h = cadd(cmul(S2, w4), cscale(cmul(S1, w3), 2.0));
-            h = cscale(h, 1.0 / (rj * rj));
-            hs[d] = cadd(hs[d], csub(h, cmul(c0, cmul(zi, zi))));
+            z3 = cmulf_(z2, zi);
+            z3 = make_float2(-2.f * z3.x, -2.f * z3.y);
+          }
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            float2 c = d32[(size_t)j * ndc + d0 + d];
+            cfmaf_(fp[d], zi, c);
+            if (IFPGH >= 2) cfmaf_(fg[d], z2, c);
+            if (IFPGH >= 3) cfmaf_(fh[d], z3, c);
           }
         }
       }
-      // P2P (FP32) over the concatenated list-1 sources, 32 staged at a time
-      for (int g0 = 0; g0 < tot; g0 += 32) {
-        int m = min(32, tot - g0);
-        __syncwarp();
-        if (lane < m) {
-          int gi = g0 + lane, e = 0;
-          while (gi >= cum[e + 1]) e++;
-          int j = l1s[e] + (gi - cum[e]);
-          SX[lane] = xs32[j];
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            if (hq) SQ[lane * ND + d] = q32[(size_t)j * ndc + d0 + d];
-            if (hd) SD[lane * ND + d] = d32[(size_t)j * ndc + d0 + d];
-          }
-        }
-        __syncwarp();
-        float2 fp[ND], fg[ND], fh[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
-        if (act) {
-          for (int jj = g; jj < m; jj += G) {
-            float4 s = SX[jj];
-            float dx = (zf.x - s.x) + (zf.z - s.z);
-            float dy = (zf.y - s.y) + (zf.w - s.w);
-            float rr = fmaf(dx, dx, dy * dy);
-            // cauchykernels2d.f: <= for potential-only, < otherwise
-            if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
-            float ir = __fdividef(1.0f, rr);
-            float2 zi = make_float2(dx * ir, -dy * ir);
-            float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
-            if (hq) {
-              float lg = 0.5f * __logf(rr);
-#pragma unroll
-              for (int d = 0; d < ND; d++) {
-                float2 c = SQ[jj * ND + d];
-                fp[d].x = fmaf(lg, c.x, fp[d].x);
-                fp[d].y = fmaf(lg, c.y, fp[d].y);
-                if (IFPGH >= 2) cfmaf_(fg[d], zi, c);
-                if (IFPGH >= 3) cfmaf_(fh[d], z2, c);
-              }
-            }
-            if (hd) {
-              float2 z3 = make_float2(0.f, 0.f);
-              if (IFPGH >= 3) {
-                z3 = cmulf_(z2, zi);
-                z3 = make_float2(-2.f * z3.x, -2.f * z3.y);
-              }
-#pragma unroll
-              for (int d = 0; d < ND; d++) {
-                float2 c = SD[jj * ND + d];
-                cfmaf_(fp[d], zi, c);
-                if (IFPGH >= 2) cfmaf_(fg[d], z2, c);
-                if (IFPGH >= 3) cfmaf_(fh[d], z3, c);
-              }
-            }
-          }
-        }
+      if (++cnt == 32) {
+        cnt = 0;
 #pragma unroll
         for (int d = 0; d < ND; d++) {
           pt[d].x += fp[d].x;
           pt[d].y += fp[d].y;
+          fp[d] = make_float2(0.f, 0.f);
           if (IFPGH >= 2) {
             gr[d].x += fg[d].x;
             gr[d].y += fg[d].y;
+            fg[d] = make_float2(0.f, 0.f);
           }
           if (IFPGH >= 3) {
             hs[d].x += fh[d].x;
             hs[d].y += fh[d].y;
+            fh[d] = make_float2(0.f, 0.f);
           }
         }
       }
-      // combine the lane groups (same target in lanes tl, tl+TW, ...)
-      for (int off = TW; off < 32; off <<= 1) {
+    }
+  }
 #pragma unroll
-        for (int d = 0; d < ND; d++) {
-          pt[d].x += __shfl_xor_sync(~0u, pt[d].x, off);
-          pt[d].y += __shfl_xor_sync(~0u, pt[d].y, off);
-          if (IFPGH >= 2) {
-            gr[d].x += __shfl_xor_sync(~0u, gr[d].x, off);
-            gr[d].y += __shfl_xor_sync(~0u, gr[d].y, off);
-          }
-          if (IFPGH >= 3) {
-            hs[d].x += __shfl_xor_sync(~0u, hs[d].x, off);
-            hs[d].y += __shfl_xor_sync(~0u, hs[d].y, off);
-          }
-        }
-      }
-      if (act && g == 0) {
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          size_t o = (size_t)k * ndc + d0 + d;
-          pot[o] = pt[d];
-          if (IFPGH >= 2) grad[o] = gr[d];
-          if (IFPGH >= 3) hess[o] = hs[d];
-        }
-      }
+  for (int d = 0; d < ND; d++) {
+    size_t o = (size_t)k * ndc + d0 + d;
+    double2 v = pot[o];
+    pot[o] = make_double2(v.x + pt[d].x + fp[d].x, v.y + pt[d].y + fp[d].y);
+    if (IFPGH >= 2) {
+      v = grad[o];
+      grad[o] = make_double2(v.x + gr[d].x + fg[d].x, v.y + gr[d].y + fg[d].y);
+    }
+    if (IFPGH >= 3) {
+      v = hess[o];
+      hess[o] = make_double2(v.x + hs[d].x + fh[d].x, v.y + hs[d].y + fh[d].y);
     }
   }
 }
@@ -472,11 +457,17 @@ template <int ND, int IFPGH>
 void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const double2* xe64,
                  int ndc, int d0, int P, const double2* mp, const double2* lo, double thresh,
                  int ifnear, double2* pot, double2* grad, double2* hess, cudaStream_t st) {
-  size_t sm = sizeof(double2) * 4 * (P * ND + 32 + 32 * ND);
-  set_smem_attr(k_leaf_mixed<ND, IFPGH>, sm);
-  k_leaf_mixed<ND, IFPGH><<<grid_for(nb, 4), 128, sm, st>>>(
-      t, nb, use_targets, M.xs.p, use_targets ? M.xt.p : M.xs.p, xe64, M.q.p, M.d.p, ndc, d0, P,
-      mp, lo, (float)(thresh * thresh), ifnear, pot, grad, hess);
+  (void)nb;
+  const long n = use_targets ? M.nt : M.ns;
+  if (n <= 0) return;
+  const int* leaf = use_targets ? M.leaf_t.p : M.leaf_s.p;
+  k_far_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(t, n, leaf, xe64, ndc, d0, P, mp, lo,
+                                                          pot, grad, hess);
+  B2_LAUNCH_CHECK();
+  if (!ifnear) return;
+  k_p2p_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(
+      t, n, leaf, M.xs.p, use_targets ? M.xt.p : M.xs.p, M.q.p, M.d.p, ndc, d0,
+      (float)(thresh * thresh), pot, grad, hess);
   B2_LAUNCH_CHECK();
 }
 
@@ -513,6 +504,19 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
   M.lgtab.alloc(49, st);
   k_utab<<<49, 64, 0, st>>>(P, M.utab.p, M.lgtab.p);
   B2_LAUNCH_CHECK();
+}
+
+void lap_mixed_leaves(MixedData& M, const TV& t, int nb, long ns, long nt, cudaStream_t st) {
+  M.ns = ns;
+  M.nt = nt;
+  M.leaf_s.alloc(ns, st);
+  k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, nb, 0, M.leaf_s.p);
+  B2_LAUNCH_CHECK();
+  if (nt > 0) {
+    M.leaf_t.alloc(nt, st);
+    k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, nb, 1, M.leaf_t.p);
+    B2_LAUNCH_CHECK();
+  }
 }
 
 void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, long ns, int ndc,

@@ -19,6 +19,8 @@ struct MixedData {
   bool tc = false;      // run M2L on the tensor cores
   int nlev = 0;         // tree levels + 1
   int nboxes = 0;
+  long ns = 0, nt = 0;
+  DBuf<int> leaf_s, leaf_t;  // leaf box of every sorted source / target
   int* err = nullptr;   // device flag set by a tensor-core wait that gave up
 };
 
@@ -31,6 +33,9 @@ bool m2l_tensor_cores();
 void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* xt, long nt,
                        bool has_q, bool has_d, int ndc, double cx0, double cy0, int P,
                        cudaStream_t st);
+
+// Leaf box of every sorted evaluation point (once per tree).
+void lap_mixed_leaves(MixedData& M, const lapk::TV& t, int nb, long ns, long nt, cudaStream_t st);
 
 // FP32 copies of the sorted densities (every evaluation).
 void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, long ns, int ndc,

@@ -1096,6 +1096,7 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   if (p.mixed) {
     lap_mixed_prepare(p.MD, p.xs.p, p.ns, p.xt.p, p.nt, p.fc, p.fd, p.ndc, T.cx0, T.cy0, p.P, st);
     p.MD.err = p.err.p;
+    lap_mixed_leaves(p.MD, p.tv, nb, p.ns, p.nt, st);
     if (T.nlevels >= 2 && T.nlevels < 64 && m2l_tensor_cores() && m2l_tc_supported(p.P)) {
       p.MD.tc = true;
       p.MD.nlev = T.nlevels + 1;
