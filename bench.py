@@ -32,6 +32,13 @@ launch of a CUDA graph that evaluates all 256 plans (trees built once,
 b2fmm_plan_create; their build time is reported separately), and checks
 the graph's results against the sequential ones.
 
+``costmodel_c5`` is the learned-cost-model sweep: 40 rfmm2d problems with N
+log-uniform in [1e4, 8e6] over three distributions (uniform; the 16-Gaussian
+mixture; the curve above with density graded over 1e3), real N(0,1)
+charges, eps in {1e-3, 1e-6}, pg = 2: total time with the leaf size chosen by
+the trained network (fmm2d_b200/costmodel.py) against the lndiv2d table,
+both error-checked against the FP64 direct sum.
+
 Multi-GPU (torchrun): every rank evaluates its own independent problem of the
 same size (replicas, no collective in the data path); timings are the max over
 ranks (one all_reduce of the step times) and ``value`` counts all ranks' points.
@@ -354,6 +361,7 @@ def main():
     ap.add_argument("--c4-only", action="store_true", help="run only the Helmholtz configuration")
     ap.add_argument("--c4-scale", type=float, default=1.0)
     ap.add_argument("--no-c3", action="store_true", help="skip the batched configuration")
+    ap.add_argument("--no-c5", action="store_true", help="skip the cost-model sweep")
     ap.add_argument("--c3-only", action="store_true", help="run only the batched configuration")
     args = ap.parse_args()
     rank, world, local = dist_info()
@@ -534,6 +542,16 @@ def main():
     c3 = None
     if not args.no_c3:
         c3 = batched_c3(L, dev)
+    c5 = None
+    if not args.no_c5:
+        from fmm2d_b200 import costmodel as cm
+        model = cm.CostModel.load()
+        if model is not None:
+            res = cm.evaluate(model, cm.sweep_problems(40, seed0=5000))
+            c5 = {k: v for k, v in res.items() if k != "rows"}
+            c5["workload"] = ("40 rfmm2d problems, N log-uniform [1e4, 8e6], uniform / "
+                              "16-Gaussian mixture / graded curve, eps in {1e-3, 1e-6}, pg=2")
+            c5["ndiv_mlp"] = [r["ndiv_mlp"] for r in res["rows"]]
     c4 = None
     if not args.no_c4:
         c4 = helmholtz_c4(L, dev, stream, args.c4_scale)
@@ -560,7 +578,7 @@ def main():
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": int(launches),
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-                "helmholtz_c4": c4, "batched_c3": c3}
+                "helmholtz_c4": c4, "batched_c3": c3, "costmodel_c5": c5}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()

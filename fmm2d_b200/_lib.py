@@ -58,6 +58,11 @@ SIGNATURES = {
     "b2fmm_get_stats": [P, c_int],
     "b2fmm_fma_peak": [c_int],
     "b2fmm_set_m2l_tensor_cores": [c_int],
+    "b2fmm_mlp_param_count": [c_int, c_int, c_int],
+    "b2fmm_mlp_forward": [P, c_int, c_int, c_int, c_int, P, P, P, P],
+    "b2fmm_mlp_gradient": [P, P, c_int, c_int, c_int, c_int, P, P, P, P, P],
+    "b2fmm_mlp_train": [P, P, c_int, c_int, c_int, c_int, P, c_int, C.c_float, P, P, P],
+    "b2fmm_point_stats": [P, c_int64, P, c_int64, P, P, P],
     "b2fmm_tc_gemm_probe": [P, P, c_int, c_int, P, P, P],
     "b2fmm_plan_create": [c_int, c_int, c_double, c_int64, P, c_int, c_int, c_int, c_int64, P,
                           c_int, P, P, P],
@@ -97,6 +102,7 @@ def lib():
         L.b2fmm_fma_peak.restype = c_double
         L.b2fmm_h2dterms.restype = c_int
         L.b2fmm_plan_create.restype = c_void_p
+        L.b2fmm_mlp_param_count.restype = c_int
         L.b2fmm_plan_status.restype = c_int
         L.b2fmm_batch_graph_create.restype = c_void_p
         L.b2fmm_batch_graph_status.restype = c_int

@@ -11,6 +11,7 @@
 #include "tree.cuh"
 #include "peaks.cuh"
 #include "lap_mixed.cuh"
+#include "mlp.cuh"
 #include "tc_m2l.cuh"
 
 namespace b2 {
@@ -635,6 +636,36 @@ void b2fmm_get_stats(double* out, int n) {
 }
 
 double b2fmm_fma_peak(int fp64) { return fma_peak_flops(fp64 != 0); }
+
+int b2fmm_mlp_param_count(int nin, int h1, int h2) { return mlp_param_count(nin, h1, h2); }
+
+void b2fmm_mlp_forward(const float* x, int batch, int nin, int h1, int h2, const float* params,
+                       float* y, void* stream, int* ier) {
+  guarded(ier, [&] { return mlp_forward(x, batch, nin, h1, h2, params, y, (cudaStream_t)stream); });
+}
+
+void b2fmm_mlp_gradient(const float* x, const float* target, int batch, int nin, int h1, int h2,
+                        const float* params, float* grad, float* loss, void* stream, int* ier) {
+  guarded(ier, [&] {
+    int r = mlp_gradient(x, target, batch, nin, h1, h2, params, grad, loss, (cudaStream_t)stream);
+    if (r == IER_OK) B2_CHECK(cudaStreamSynchronize((cudaStream_t)stream));
+    return r;
+  });
+}
+
+void b2fmm_mlp_train(const float* x, const float* target, int batch, int nin, int h1, int h2,
+                     float* params, int steps, float lr, float* loss_history, void* stream,
+                     int* ier) {
+  guarded(ier, [&] {
+    return mlp_train(x, target, batch, nin, h1, h2, params, steps, lr, loss_history,
+                     (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_point_stats(const double* sources, int64_t ns, const double* targ, int64_t nt,
+                       unsigned* hist, void* stream, int* ier) {
+  guarded(ier, [&] { return point_stats(sources, ns, targ, nt, hist, (cudaStream_t)stream); });
+}
 
 void b2fmm_set_m2l_tensor_cores(int on) { set_m2l_tensor_cores(on != 0); }
 

@@ -8,12 +8,12 @@
 //   remain.  Local expansions are accumulated in FP32 per target box and
 //   added to the FP64 expansion once.
 // * k_far_mixed / k_p2p_mixed: one evaluation point per thread.  L2P and M2P
-//   in FP64 (as the FP64 path), then the near field in FP32.  Coordinates are
-//   stored as x - c0 split into hi + lo floats, so a difference
-//   (xt_hi - xs_hi) + (xt_lo - xs_lo) keeps the relative accuracy of the FP64
-//   difference even for nearly coincident points; log and 1/r^2 use the SFU.
-//   Per-pair terms are summed in FP32 over at most 32 sources and the
-//   partial sums in FP64.
+//   in FP64 (as the FP64 path), then the near field in FP32.  The coordinate
+//   difference of a pair is formed in FP64 and rounded once to FP32, so it
+//   keeps the relative accuracy of the FP64 path's difference even for nearly
+//   coincident points (separations of 1e-12 occur in graded distributions);
+//   log and 1/r^2 use the SFU.  Per-pair terms are summed in FP32 over at
+//   most 32 sources and the partial sums in FP64.
 #include "lap_mixed.cuh"
 
 #include <atomic>
@@ -24,15 +24,6 @@ namespace b2 {
 namespace {
 
 using namespace lapk;
-
-__global__ void k_prep_pts(const double2* __restrict__ x, long n, double cx0, double cy0,
-                           float4* __restrict__ out) {
-  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  double dx = x[k].x - cx0, dy = x[k].y - cy0;
-  float hx = (float)dx, hy = (float)dy;
-  out[k] = make_float4(hx, hy, (float)(dx - (double)hx), (float)(dy - (double)hy));
-}
 
 __global__ void k_prep_dens(const double2* __restrict__ in, long m, float2* __restrict__ out) {
   long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -343,15 +334,15 @@ __global__ void __launch_bounds__(128) k_far_mixed(
 // the partial sums in FP64, added to the far field already in the outputs.
 template <int ND, int IFPGH>
 __global__ void __launch_bounds__(128) k_p2p_mixed(
-    TV t, long n, const int* __restrict__ leaf, const float4* __restrict__ xs32,
-    const float4* __restrict__ xe32, const float2* __restrict__ q32,
+    TV t, long n, const int* __restrict__ leaf, const double2* __restrict__ xs64,
+    const double2* __restrict__ xe64, const float2* __restrict__ q32,
     const float2* __restrict__ d32, int ndc, int d0, float th2, double2* __restrict__ pot,
     double2* __restrict__ grad, double2* __restrict__ hess) {
   long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (k >= n) return;
   const bool hq = q32 != nullptr, hd = d32 != nullptr;
   const int b = leaf[k];
-  const float4 zf = xe32[k];
+  const double2 z = xe64[k];
   double2 pt[ND], gr[ND], hs[ND];
 #pragma unroll
   for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
@@ -363,9 +354,11 @@ __global__ void __launch_bounds__(128) k_p2p_mixed(
   for (int e = 0; e < n1; e++) {
     int2 sr = t.srng[t.l1[(size_t)MNLIST1 * b + e]];
     for (int j = sr.x; j < sr.y; j++) {
-      float4 s = xs32[j];
-      float dx = (zf.x - s.x) + (zf.z - s.z);
-      float dy = (zf.y - s.y) + (zf.w - s.w);
+      // the difference in FP64 (as the FP64 path forms it), the kernel in FP32:
+      // sources closer than ~1e-15 of the coordinates keep their relative accuracy
+      double2 s = xs64[j];
+      float dx = (float)(z.x - s.x);
+      float dy = (float)(z.y - s.y);
       float rr = fmaf(dx, dx, dy * dy);
       // cauchykernels2d.f: <= for potential-only, < otherwise
       if (!(IFPGH == 1 ? (rr <= th2) : (rr < th2))) {
@@ -466,8 +459,7 @@ void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const
   B2_LAUNCH_CHECK();
   if (!ifnear) return;
   k_p2p_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(
-      t, n, leaf, M.xs.p, use_targets ? M.xt.p : M.xs.p, M.q.p, M.d.p, ndc, d0,
-      (float)(thresh * thresh), pot, grad, hess);
+      t, n, leaf, M.xs64, xe64, M.q.p, M.d.p, ndc, d0, (float)(thresh * thresh), pot, grad, hess);
   B2_LAUNCH_CHECK();
 }
 
@@ -489,14 +481,10 @@ void leaf_dispatch(int ifl, const TV& t, int nb, int use_targets, const MixedDat
 void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* xt, long nt,
                        bool has_q, bool has_d, int ndc, double cx0, double cy0, int P,
                        cudaStream_t st) {
-  M.xs.alloc(ns, st);
-  k_prep_pts<<<ceil_div(ns, 256), 256, 0, st>>>(xs, ns, cx0, cy0, M.xs.p);
-  B2_LAUNCH_CHECK();
-  if (nt > 0) {
-    M.xt.alloc(nt, st);
-    k_prep_pts<<<ceil_div(nt, 256), 256, 0, st>>>(xt, nt, cx0, cy0, M.xt.p);
-    B2_LAUNCH_CHECK();
-  }
+  (void)xt;
+  (void)cx0;
+  (void)cy0;
+  M.xs64 = xs;
   long m = ns * (long)ndc;
   if (has_q) M.q.alloc(m, st);
   if (has_d) M.d.alloc(m, st);

@@ -7,10 +7,10 @@
 
 namespace b2 {
 
-// FP32 copies of the sorted points (x - c0 split into hi/lo floats, so that
-// coordinate differences keep FP64-level relative accuracy) and densities.
+// Data of the mixed-precision kernels: FP32 copies of the sorted densities,
+// offset tables, the tensor-core M2L pair list and per-point leaf maps.
 struct MixedData {
-  DBuf<float4> xs, xt;  // (xhi, yhi, xlo, ylo)
+  const double2* xs64 = nullptr;  // sorted sources (FP64, owned by the caller)
   DBuf<float2> q, d;    // all Cauchy densities, ndc per point
   DBuf<float2> utab;    // (1/o)^k for the 7x7 integer offsets o, k < P
   DBuf<float> lgtab;    // log|o|
@@ -28,7 +28,7 @@ struct MixedData {
 void set_m2l_tensor_cores(bool on);
 bool m2l_tensor_cores();
 
-// Geometry part (FP32 coordinates, offset tables) and allocation of the FP32
+// Geometry part (source pointer, offset tables) and allocation of the FP32
 // density copies for ndc densities per source.
 void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* xt, long nt,
                        bool has_q, bool has_d, int ndc, double cx0, double cy0, int P,

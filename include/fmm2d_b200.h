@@ -242,6 +242,29 @@ int b2fmm_batch_graph_status(void* graph);
 int64_t b2fmm_batch_graph_nodes(void* graph);
 void b2fmm_batch_graph_free(void* graph);
 
+/* -------------------------------------- learned cost model (no reference counterpart) */
+
+/* The reference picks the leaf size from a fixed table (lndiv2d.f:1-39);
+ * these entry points carry the small MLP that predicts the FMM's time from
+ * point-distribution statistics and the leaf size, with hand-written
+ * forward, backward and Adam kernels.  Parameters are one flat FP32 array
+ * W1 [h1][nin], b1 [h1], W2 [h2][h1], b2 [h2], w3 [h2], b3; tanh hidden
+ * layers, linear output; nin <= 32, h1, h2 <= 64.  Device pointers. */
+int b2fmm_mlp_param_count(int nin, int h1, int h2);
+void b2fmm_mlp_forward(const float* x, int batch, int nin, int h1, int h2, const float* params,
+                       float* y, void* stream, int* ier);
+/* Gradient of mean_b (y_b - target_b)^2; loss (device, may be NULL). */
+void b2fmm_mlp_gradient(const float* x, const float* target, int batch, int nin, int h1, int h2,
+                        const float* params, float* grad, float* loss, void* stream, int* ier);
+/* `steps` full-batch Adam steps in place; loss_history: host, may be NULL. */
+void b2fmm_mlp_train(const float* x, const float* target, int batch, int nin, int h1, int h2,
+                     float* params, int steps, float lr, float* loss_history, void* stream,
+                     int* ier);
+/* 128 x 128 occupancy histogram (device, row-major) of sources and targets
+ * over the square that holds them, the input of the cost-model features. */
+void b2fmm_point_stats(const double* sources, int64_t ns, const double* targ, int64_t nt,
+                       unsigned* hist, void* stream, int* ier);
+
 /* ------------------------------------------------- tensor-core M2L (no reference counterpart) */
 
 /* Mixed-precision Laplace M2L engine switch: 1 (default) runs the list-2

@@ -63,3 +63,20 @@ def test_mixed_cfmm_nd3_and_auto(gpu, oracle):
     ref = oracle.cfmm2d(1e-6, src, charges=q, ifpgh=2, nd=3)
     assert rel_l2(out.pot.real, ref["pot"].real) < 1e-6
     assert rel_l2(out.grad, ref["grad"]) < 1e-6
+
+
+def test_mixed_graded_curve_nearly_coincident_sources(gpu):
+    """Sources on a curve with density graded over 1e3 (separations down to
+    ~1e-11): the mixed path stays within eps for the potential and the
+    gradient (pair differences are formed in FP64)."""
+    from fmm2d_b200.costmodel import make_problem
+    src, q = make_problem("curve", 400000, 11)
+    d = np.sort(np.hypot(*np.diff(src[:, np.argsort(np.arctan2(src[1] - 0.5, src[0] - 0.5))],
+                                  axis=1)))
+    assert d[0] < 1e-10
+    out = fmm.rfmm2d(eps=1e-6, sources=src, charges=q, pg=2, precision="mixed")
+    rng = np.random.default_rng(0)
+    idx = np.sort(rng.choice(400000, 300, replace=False))
+    ex = fmm.r2ddir(sources=src, targets=src[:, idx], charges=q, pgt=2)
+    assert rel_l2(out.pot[idx], ex.pottarg) < 1e-6
+    assert rel_l2(out.grad[:, idx], ex.gradtarg) < 1e-6
