@@ -10,7 +10,8 @@ in ``libfmm2d_b200.so`` on the GPU; there is no CPU fallback.
 
 Optional keyword extensions (not in the reference, defaults reproduce it):
 ``precision`` ('auto' = mixed when eps >= 1e-6, 'fp64', 'mixed'), ``ndiv``
-(leaf capacity override) and ``timeinfo`` (a length-8 float64 numpy array
+(leaf capacity override, or 'auto' for the learned cost model of
+fmm2d_b200/costmodel.py) and ``timeinfo`` (a length-8 float64 numpy array
 that receives the per-step device times).
 """
 import ctypes as C
@@ -124,6 +125,13 @@ def _lap_run(fe, eps, sources, charges, dipstr, dipvec, targets, ifpgh, ifpghtar
     pott = B.empty((nt, nd), dt, **kw) if ifpghtarg >= 1 and nt else None
     gradt = B.empty(gshape(nt), dt, **kw) if ifpghtarg >= 2 and nt else None
     hesst = B.empty(hshape(nt), dt, **kw) if ifpghtarg >= 3 and nt else None
+    if ndiv == "auto":
+        # leaf size from the learned cost model (lndiv2d table without weights)
+        import torch
+        from . import costmodel
+        dsrc = s if torch_mode else torch.as_tensor(s, device="cuda")
+        dtrg = None if t is None else (t if torch_mode else torch.as_tensor(t, device="cuda"))
+        ndiv = costmodel.auto_ndiv(dsrc, dtrg, eps)
     opts = _options(precision, ndiv)
     ti = np.zeros(8) if timeinfo is None else timeinfo
     ier = C.c_int(0)

@@ -123,3 +123,15 @@ def test_trained_model_beats_table_on_held_out_problems(gpu):
     res = cm.evaluate(model, cm.sweep_problems(6, seed0=9000, nmin=2e5, nmax=2e6))
     assert res["max_err_over_eps_mlp"] < 1.0 and res["max_err_over_eps_table"] < 1.0
     assert res["total_ms_mlp"] <= 1.05 * res["total_ms_table"]
+
+
+def test_front_end_auto_ndiv(gpu):
+    """ndiv='auto' through the fmm2dpy-style front end gives the same
+    result as the table's leaf size, within eps."""
+    import fmm2d_b200 as fmm
+    from conftest import rel_l2
+    src, q = cm.make_problem("mixture", 200000, 3)
+    a = fmm.rfmm2d(eps=1e-6, sources=src, charges=q, pg=2, ndiv="auto")
+    b = fmm.rfmm2d(eps=1e-6, sources=src, charges=q, pg=2)
+    assert a.ier == 0
+    assert rel_l2(a.pot, b.pot) < 1e-6 and rel_l2(a.grad, b.grad) < 1e-6
