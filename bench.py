@@ -46,6 +46,7 @@ ranks (one all_reduce of the step times) and ``value`` counts all ranks' points.
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -472,15 +473,42 @@ def main():
              "m2l": st["m2l_pairs"] * 4 * P * P * nd2}
     t_dom = phases[dom]
     achieved = flops.get(dom, 0.0) / t_dom / 1e12 if t_dom > 0 else 0.0
-    roofline = {"bound": "fma", "kernel": dom, "achieved": achieved,
-                "peak": fma_peak / 1e12, "unit": "TFLOP/s", "frac": achieved / (fma_peak / 1e12),
-                "traffic": None,
-                "peak_source": ("in-run FMA microbenchmark b2fmm_fma_peak "
-                                f"({'FP64' if prec == 'fp64' else 'FP32'}); MEASURED_PEAKS.json "
-                                "holds only HBM copy and bf16 tensor peaks"),
-                "phase_ms": phases_ms, "tree_ms": round(st["tree_ms"], 4),
-                "counts": {k: st[k] for k in ("nboxes", "nlevels", "nleaves", "nterms1",
-                                              "p2p_pairs", "m2l_pairs", "m2p_evals")}}
+    counts = {k: st[k] for k in ("nboxes", "nlevels", "nleaves", "nterms1", "p2p_pairs",
+                                 "m2l_pairs", "m2p_evals")}
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) \
+        if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    if dom == "m2l" and prec == "mixed":
+        # tensor-core M2L: useful flops against the measured dense bf16 peak
+        # (MEASURED_PEAKS.json); TF32 issues at half that rate, and the split
+        # products issue 3x the useful work on K, N padded to the MMA shape
+        K = (int(P) + 7) // 8 * 8
+        N = 16 if P <= 16 else 32
+        tiles = math.ceil(st["m2l_pairs"] * nd2 / 128)
+        issued = tiles * 2 * (K // 8) * 3 * (128 * N * 8 * 2)
+        peak = peaks.get("bf16_tflops", 1590.0)
+        roofline = {"bound": "tensor", "kernel": "m2l (k_m2l_tc, tcgen05 kind::tf32)",
+                    "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "issued_tensor_tflops": issued / t_dom / 1e12,
+                    "issued_frac_of_tf32_peak": issued / t_dom / 1e12 / (peak / 2),
+                    "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else
+                                    "fallback 1590 TFLOP/s bf16")}
+    else:
+        roofline = {"bound": "fma", "kernel": dom, "achieved": achieved,
+                    "peak": fma_peak / 1e12, "unit": "TFLOP/s",
+                    "frac": achieved / (fma_peak / 1e12), "traffic": None,
+                    "peak_source": ("in-run FMA microbenchmark b2fmm_fma_peak "
+                                    f"({'FP64' if prec == 'fp64' else 'FP32'})")}
+    t_leaf = phases["leaf_eval(l2p+m2p+p2p)"]
+    p2p_fl = st["p2p_pairs"] * (15 + 28 * nd2)
+    roofline["near_field"] = {"bound": "fma", "pairs": st["p2p_pairs"],
+                              "achieved": p2p_fl / t_leaf / 1e12 if t_leaf > 0 else 0.0,
+                              "peak": fma_peak / 1e12, "unit": "TFLOP/s",
+                              "note": "P2P flops over the whole leaf phase (L2P and M2P "
+                                      "included in the time)"}
+    roofline["near_field"]["frac"] = roofline["near_field"]["achieved"] / (fma_peak / 1e12)
+    roofline.update({"phase_ms": phases_ms, "tree_ms": round(st["tree_ms"], 4),
+                     "counts": counts})
     prof = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(prof):
         try:

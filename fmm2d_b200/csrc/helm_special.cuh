@@ -295,17 +295,16 @@ __host__ __device__ inline void hscaled(int N, double2 z, double rs, double2* ou
   }
 }
 
-// out[n] = J_n(z) / rs^n, n = 0..N.  The recurrence starts at order
-// S >= max(N, |z| + 10, |z|^2 / 10), where the series of F_S has little
-// cancellation, or at
-// the highest order whose leading factor (|z| / 2 rs)^n / n! is above 1e-250.
-__host__ __device__ inline void jscaled(int N, double2 z, double rs, double2* out) {
+// Start of the downward recurrence for F_n = J_n(z) / rs^n, n <= N: the
+// highest order M kept (S >= max(N, |z| + 10, |z|^2 / 10), where the series of
+// F_S has little cancellation, or the highest order whose leading factor
+// (|z| / 2 rs)^n / n! is above 1e-250; orders above M are 0) and F_M, F_{M-1}
+// from their power series.  False for |z| < 1e-200 (F_0 = 1, the rest 0).
+// The caller continues with F_{n-1} = (2 n rs / z) F_n - rs^2 F_{n+1}.
+__host__ __device__ inline bool jstart(int N, double2 z, double rs, int& M, double2& f_hi,
+                                       double2& f_lo) {
   double az = hypot(z.x, z.y);
-  if (az < 1e-200) {
-    out[0] = make_double2(1, 0);
-    for (int i = 1; i <= N; i++) out[i] = make_double2(0, 0);
-    return;
-  }
+  if (az < 1e-200) return false;
   double2 w = cscale(z, 0.5 / rs);
   double aw = 0.5 * az / rs;
   // the series of F_S sums terms up to ~exp(|z|^2 / 4S) times its value:
@@ -313,19 +312,18 @@ __host__ __device__ inline void jscaled(int N, double2 z, double rs, double2* ou
   int S = N > (int)az + 10 ? N : (int)az + 10;
   if (az < 200.0 && S < (int)(0.1 * az * az) + 1) S = (int)(0.1 * az * az) + 1;
   if (S < 1) S = 1;
-  int M = S;
+  M = S;
   {
-    double lt = 0.0, lw = log10(aw);  // log10 of the leading factor
+    double lt = 1.0;  // the leading factor (|z| / 2 rs)^n / n!
     for (int n = 1; n <= S; n++) {
-      lt += lw - log10((double)n);
-      if (lt < -250.0) {
+      lt *= aw / n;
+      if (lt < 1e-250) {
         M = n - 1;
         break;
       }
     }
   }
   if (M < 1) M = 1;
-  for (int n = M + 1; n <= N; n++) out[n] = make_double2(0, 0);
   // F_m = t_m sum_k (-z^2/4)^k m! / (k! (m+k)!), t_m = w^m / m!, m = M, M-1
   double2 q = cmul(z, z);
   q = make_double2(-0.25 * q.x, -0.25 * q.y);
@@ -342,8 +340,21 @@ __host__ __device__ inline void jscaled(int N, double2 z, double rs, double2* ou
     }
     sr[s] = sum;
   }
-  double2 f_hi = cmul(tM, sr[0]);                                   // F_M
-  double2 f_lo = cmul(cscale(cmul(tM, crcp(w)), (double)M), sr[1]);  // F_{M-1}
+  f_hi = cmul(tM, sr[0]);                                   // F_M
+  f_lo = cmul(cscale(cmul(tM, crcp(w)), (double)M), sr[1]);  // F_{M-1}
+  return true;
+}
+
+// out[n] = J_n(z) / rs^n, n = 0..N (jstart + the downward recurrence).
+__host__ __device__ inline void jscaled(int N, double2 z, double rs, double2* out) {
+  int M = 0;
+  double2 f_hi, f_lo;
+  if (!jstart(N, z, rs, M, f_hi, f_lo)) {
+    out[0] = make_double2(1, 0);
+    for (int i = 1; i <= N; i++) out[i] = make_double2(0, 0);
+    return;
+  }
+  for (int n = M + 1; n <= N; n++) out[n] = make_double2(0, 0);
   if (M <= N) out[M] = f_hi;
   if (M - 1 <= N) out[M - 1] = f_lo;
   double2 c = cscale(crcp(z), 2.0 * rs);

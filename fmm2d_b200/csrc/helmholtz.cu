@@ -551,110 +551,6 @@ __global__ void __launch_bounds__(64) k_h_l2l(TV t, const HLev* __restrict__ lv,
   }
 }
 
-// Derivative expansions of an expansion E of order p (mk_mpoleg / mk_mpoleh,
-// helmrouts2d.f): X, Y of order p+1 and XX, XY, YY of order p+2, scale s.
-template <int ND>
-__device__ void derivative_exps(int lane, const double2* E, int p, double2 zk, double s,
-                                double2* X, double2* Y, double2* XX, double2* XY, double2* YY,
-                                int ifpgh) {
-  double2 s1 = cscale(zk, 0.5 / s), s2 = cscale(zk, 0.5 * s);
-  double2 s3 = make_double2(-s1.y, s1.x), s4 = make_double2(-s2.y, s2.x);  // times i
-  // X(n), n = -(p+1)..p+1: contributions from E(n+1) and E(n-1)
-  auto Ev = [&](int n, int d) {
-    return (n >= -p && n <= p) ? E[(n + p) * ND + d] : make_double2(0, 0);
-  };
-  for (int k = lane; k < (2 * p + 3) * ND; k += 32) {
-    int n = k / ND - (p + 1), d = k % ND;
-    double2 x = make_double2(0, 0), y = make_double2(0, 0);
-    // from E(m) with m = n+1 (E(m) adds to index m-1 = n): m >= 1 -> s2/s4,
-    // m == 0 -> s1/s3 (to -1), m <= -1 -> s1/s3
-    int m = n + 1;
-    double2 em = Ev(m, d);
-    if (m >= 1) {
-      x = cadd(x, cmul(s2, em));
-      y = cadd(y, cmul(s4, em));
-    } else {
-      x = cadd(x, cmul(s1, em));
-      y = cadd(y, cmul(s3, em));
-    }
-    // from E(m) with m = n-1 (adds to index m+1 = n): m >= 0 -> -s1 / +s3,
-    // m <= -1 -> -s2 / +s4
-    m = n - 1;
-    em = Ev(m, d);
-    if (m >= 0) {
-      x = csub(x, cmul(s1, em));
-      y = cadd(y, cmul(s3, em));
-    } else {
-      x = csub(x, cmul(s2, em));
-      y = cadd(y, cmul(s4, em));
-    }
-    X[k] = x;
-    Y[k] = y;
-  }
-  if (ifpgh < 3) return;
-  __syncwarp();
-  int q = p + 1;
-  auto Xv = [&](int n, int d) {
-    return (n >= -q && n <= q) ? X[(n + q) * ND + d] : make_double2(0, 0);
-  };
-  auto Yv = [&](int n, int d) {
-    return (n >= -q && n <= q) ? Y[(n + q) * ND + d] : make_double2(0, 0);
-  };
-  for (int k = lane; k < (2 * p + 5) * ND; k += 32) {
-    int n = k / ND - (p + 2), d = k % ND;
-    double2 xx = make_double2(0, 0), xy = make_double2(0, 0), yy = make_double2(0, 0);
-    int m = n + 1;
-    double2 ex = Xv(m, d), ey = Yv(m, d);
-    if (m >= 1) {
-      xx = cadd(xx, cmul(s2, ex));
-      xy = cadd(xy, cmul(s4, ex));
-      yy = cadd(yy, cmul(s4, ey));
-    } else {
-      xx = cadd(xx, cmul(s1, ex));
-      xy = cadd(xy, cmul(s3, ex));
-      yy = cadd(yy, cmul(s3, ey));
-    }
-    m = n - 1;
-    ex = Xv(m, d);
-    ey = Yv(m, d);
-    if (m >= 0) {
-      xx = csub(xx, cmul(s1, ex));
-      xy = cadd(xy, cmul(s3, ex));
-      yy = cadd(yy, cmul(s3, ey));
-    } else {
-      xx = csub(xx, cmul(s2, ex));
-      xy = cadd(xy, cmul(s4, ex));
-      yy = cadd(yy, cmul(s4, ey));
-    }
-    XX[k] = xx;
-    XY[k] = xy;
-    YY[k] = yy;
-  }
-}
-
-// sum_n E(n) mt(n), mt(0) = (i/4) Z_0, mt(+-n) = (i/4) Z_n (e^{i th})^n,
-// (i/4) Z_n (-e^{-i th})^n (mpole_evalp, helmrouts2d.f:1493-1530).
-template <int ND>
-__device__ __forceinline__ void eval_sum(const double2* E, int q, const double2* Z, double2 ep,
-                                         double2 out[ND]) {
-  double2 i4 = make_double2(0.0, 0.25);
-  double2 m0 = cmul(Z[0], i4);
-#pragma unroll
-  for (int d = 0; d < ND; d++) out[d] = cadd(out[d], cmul(E[q * ND + d], m0));
-  double2 a = cmul(ep, i4), bneg = make_double2(-ep.x, ep.y);  // -exp(-i theta)
-  double2 b = cmul(bneg, i4);  // (-e^{-i th}) i/4
-  for (int n = 1; n <= q; n++) {
-    double2 tp = cmul(a, Z[n]), tm = cmul(b, Z[n]);
-#pragma unroll
-    for (int d = 0; d < ND; d++) {
-      out[d] = cadd(out[d], cmul(E[(q + n) * ND + d], tp));
-      out[d] = cadd(out[d], cmul(E[(q - n) * ND + d], tm));
-    }
-    a = cmul(a, ep);
-    b = cmul(b, bneg);
-  }
-}
-
 // Pair term of the near field (helmkernels2d.f h2d_directcdh, cdg, ...).
 template <int ND, int IFPGH>
 __device__ __forceinline__ void h_pair(double xd, double yd, double2 zk, const double2* q,
@@ -723,170 +619,251 @@ __device__ __forceinline__ void h_pair(double xd, double yd, double2 zk, const d
   }
 }
 
-// steps 6-8 fused per leaf: L2P (J tables), M2P (H tables) and P2P for 32
-// evaluation points at a time; one result write per point (tree order).
+// Leaf box of every evaluation point (points are in tree order).
+__global__ void k_h_point_leaf(TV t, int nb, int use_targets, int* __restrict__ leaf) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb || t.nchild[b] != 0) return;
+  int2 r = use_targets ? t.trng[b] : t.srng[b];
+  for (int k = r.x; k < r.y; k++) leaf[k] = b;
+}
+
+// Coefficient n of the derivative expansions of mk_mpoleg / mk_mpoleh
+// (helmrouts2d.f): with s1 = zk/(2s), s2 = zk s/2, s3 = i s1, s4 = i s2,
+//   X(n) = [n+1 >= 1 ? s2 : s1] F(n+1) - [n-1 >= 0 ? s1 : s2] F(n-1),
+//   Y(n) = [n+1 >= 1 ? s4 : s3] F(n+1) + [n-1 >= 0 ? s3 : s4] F(n-1);
+// XX, XY come from X and YY from Y by the same rules.
+struct DerivCoef {
+  double2 s1, s2, s3, s4;
+};
+
+template <typename F>
+__device__ __forceinline__ double2 rule_x(F f, int n, const DerivCoef& c) {
+  double2 a = f(n + 1), b = f(n - 1);
+  return csub(cmul(n + 1 >= 1 ? c.s2 : c.s1, a), cmul(n - 1 >= 0 ? c.s1 : c.s2, b));
+}
+template <typename F>
+__device__ __forceinline__ double2 rule_y(F f, int n, const DerivCoef& c) {
+  double2 a = f(n + 1), b = f(n - 1);
+  return cadd(cmul(n + 1 >= 1 ? c.s4 : c.s3, a), cmul(n - 1 >= 0 ? c.s3 : c.s4, b));
+}
+
+// Adds sum_n V(n) mt(n) for V = E (and its derivative expansions) at one
+// point, mt(0) = (i/4) Z_0, mt(n) = (i/4) Z_n e^{i n th}, mt(-n) = (i/4) Z_n
+// (-e^{-i th})^n (mpole_evalp / h2dtaevalp, helmrouts2d.f:274-966), with the
+// scaled Bessel (local, mpole = false) or Hankel (multipole) sequence Z of
+// argument zz = zk r generated by its recurrence on the fly, no tables.
 template <int ND, int IFPGH>
-__global__ void __launch_bounds__(64) k_h_leaf(TV t, const HLev* __restrict__ lv, int nb,
-                                               int use_targets, const double2* __restrict__ xs,
-                                               const double2* __restrict__ xe, HDens D,
-                                               double zkr, double zki, const double2* __restrict__ mp,
-                                               const double2* __restrict__ lo, double thresh,
-                                               int ifnear, double2* __restrict__ pot,
-                                               double2* __restrict__ grad,
-                                               double2* __restrict__ hess, int maxp) {
-  extern __shared__ double2 hsm[];
-  const double2 zk = make_double2(zkr, zki);
-  const int ES = (2 * maxp + 1) + 2 * (2 * maxp + 3) + 3 * (2 * maxp + 5);
-  HLOOP(nb) {
-    double2* E = hsm + (size_t)wib * (ES * ND + 32 * (1 + 3 * ND));
-    double2* X = E + (2 * maxp + 1) * ND;
-    double2* Y = X + (2 * maxp + 3) * ND;
-    double2* XX = Y + (2 * maxp + 3) * ND;
-    double2* XY = XX + (2 * maxp + 5) * ND;
-    double2* YY = XY + (2 * maxp + 5) * ND;
-    double2* SX = YY + (2 * maxp + 5) * ND;  // staged sources
-    double2* SQ = SX + 32;
-    double2* SD = SQ + 32 * ND;
-    double* SV = (double*)(SD + 32 * ND);  // 2 ND doubles per staged source
-    int b = bi;
-    if (t.nchild[b] != 0) continue;
-    int2 er = use_targets ? t.trng[b] : t.srng[b];
-    if (er.y <= er.x) continue;
-    int lev = t.level[b];
-    HLev L = lv[lev];
-    double2 cb = t.center[b];
-    int n3 = t.nl3[b], n1 = ifnear ? t.nl1[b] : 0;
-    double2 Zt[HMAXP + 4];
-    for (int k0 = er.x; k0 < er.y; k0 += 32) {
-      int k = k0 + lane;
-      bool act = k < er.y;
-      double2 z = act ? xe[k] : cb;
-      double2 po[ND], g1[ND], g2[ND], hh[ND][3];
+__device__ void eval_at_point(const double2* __restrict__ E, int p, double2 zk, double rs,
+                              bool mpole, double2 zz, double2 ep, double2 po[ND], double2 g1[ND],
+                              double2 g2[ND], double2 hh[ND][3]) {
+  const int q = p + IFPGH - 1;  // highest order that contributes
+  const double s = mpole ? rs : 1.0 / rs;
+  DerivCoef c;
+  c.s1 = cscale(zk, 0.5 / s);
+  c.s2 = cscale(zk, 0.5 * s);
+  c.s3 = make_double2(-c.s1.y, c.s1.x);
+  c.s4 = make_double2(-c.s2.y, c.s2.x);
+  const double2 i4 = make_double2(0.0, 0.25);
+  auto contribute = [&](int m, double2 Zm, double2 epm) {
+    // orders +m and -m share Z_m
+    double2 base = cmul(Zm, i4);
+    for (int sgn = 1; sgn >= -1; sgn -= 2) {
+      if (m == 0 && sgn < 0) break;
+      int n = sgn * m;
+      double2 ph = sgn > 0 ? epm : cconj(epm);
+      if (sgn < 0 && (m & 1)) ph = make_double2(-ph.x, -ph.y);
+      double2 mt = cmul(base, ph);
 #pragma unroll
       for (int d = 0; d < ND; d++) {
-        po[d] = g1[d] = g2[d] = make_double2(0, 0);
-        hh[d][0] = hh[d][1] = hh[d][2] = make_double2(0, 0);
-      }
-      // L2P: local of the leaf with J tables, derivatives via rs^-1 expansions
-      // (local expansions of levels 0 and 1 are zero)
-      if (L.ok && lev >= 2) {
-        int p = L.p;
-        __syncwarp();
-        const double2* Lb = hexp((double2*)lo, L, b, ND);
-        for (int e = lane; e < (2 * p + 1) * ND; e += 32) E[e] = Lb[e];
-        __syncwarp();
-        if (IFPGH >= 2) derivative_exps<ND>(lane, E, p, zk, 1.0 / L.rs, X, Y, XX, XY, YY, IFPGH);
-        __syncwarp();
-        double dx = z.x - cb.x, dy = z.y - cb.y;
-        double r = sqrt(dx * dx + dy * dy), th = (dx == 0 && dy == 0) ? 0.0 : atan2(dy, dx);
-        jscaled(p + 3, make_double2(zk.x * r, zk.y * r), L.rs, Zt);
-        double2 ep = make_double2(cos(th), sin(th));
-        eval_sum<ND>(E, p, Zt, ep, po);
+        auto Ef = [&](int k) {
+          return (k >= -p && k <= p) ? E[(size_t)(k + p) * ND + d] : make_double2(0, 0);
+        };
+        if (m <= p) po[d] = cadd(po[d], cmul(Ef(n), mt));
         if (IFPGH >= 2) {
-          eval_sum<ND>(X, p + 1, Zt, ep, g1);
-          eval_sum<ND>(Y, p + 1, Zt, ep, g2);
+          g1[d] = cadd(g1[d], cmul(rule_x(Ef, n, c), mt));
+          g2[d] = cadd(g2[d], cmul(rule_y(Ef, n, c), mt));
         }
         if (IFPGH >= 3) {
-          double2 t0[ND], t1[ND], t2[ND];
-#pragma unroll
-          for (int d = 0; d < ND; d++) t0[d] = t1[d] = t2[d] = make_double2(0, 0);
-          eval_sum<ND>(XX, p + 2, Zt, ep, t0);
-          eval_sum<ND>(XY, p + 2, Zt, ep, t1);
-          eval_sum<ND>(YY, p + 2, Zt, ep, t2);
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            hh[d][0] = cadd(hh[d][0], t0[d]);
-            hh[d][1] = cadd(hh[d][1], t1[d]);
-            hh[d][2] = cadd(hh[d][2], t2[d]);
-          }
-        }
-      }
-      // M2P from list 3 (boxes of level lev+1)
-      for (int e = 0; e < n3; e++) {
-        HLev C = lv[lev + 1];
-        if (!C.ok) break;
-        int jb = t.l3[(size_t)MNLIST3 * b + e];
-        int p = C.p;
-        __syncwarp();
-        const double2* Mb = hexp((double2*)mp, C, jb, ND);
-        for (int q = lane; q < (2 * p + 1) * ND; q += 32) E[q] = Mb[q];
-        __syncwarp();
-        if (IFPGH >= 2) derivative_exps<ND>(lane, E, p, zk, C.rs, X, Y, XX, XY, YY, IFPGH);
-        __syncwarp();
-        double2 cj = t.center[jb];
-        double dx = z.x - cj.x, dy = z.y - cj.y;
-        double r = sqrt(dx * dx + dy * dy), th = (dx == 0 && dy == 0) ? 0.0 : atan2(dy, dx);
-        hscaled(p + 3, make_double2(zk.x * r, zk.y * r), C.rs, Zt);
-        double2 ep = make_double2(cos(th), sin(th));
-        eval_sum<ND>(E, p, Zt, ep, po);
-        if (IFPGH >= 2) {
-          eval_sum<ND>(X, p + 1, Zt, ep, g1);
-          eval_sum<ND>(Y, p + 1, Zt, ep, g2);
-        }
-        if (IFPGH >= 3) {
-          double2 t0[ND], t1[ND], t2[ND];
-#pragma unroll
-          for (int d = 0; d < ND; d++) t0[d] = t1[d] = t2[d] = make_double2(0, 0);
-          eval_sum<ND>(XX, p + 2, Zt, ep, t0);
-          eval_sum<ND>(XY, p + 2, Zt, ep, t1);
-          eval_sum<ND>(YY, p + 2, Zt, ep, t2);
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            hh[d][0] = cadd(hh[d][0], t0[d]);
-            hh[d][1] = cadd(hh[d][1], t1[d]);
-            hh[d][2] = cadd(hh[d][2], t2[d]);
-          }
-        }
-      }
-      // P2P from list 1
-      const bool hq = D.q != nullptr, hd = D.d != nullptr;
-      for (int e = 0; e < n1; e++) {
-        int jb = t.l1[(size_t)MNLIST1 * b + e];
-        int2 sr = t.srng[jb];
-        for (int s0 = sr.x; s0 < sr.y; s0 += 32) {
-          int ns = min(32, sr.y - s0);
-          __syncwarp();
-          if (lane < ns) {
-            int j = s0 + lane;
-            SX[lane] = xs[j];
-#pragma unroll
-            for (int d = 0; d < ND; d++) {
-              if (hq) SQ[lane * ND + d] = D.q[(size_t)j * D.nd + D.d0 + d];
-              if (hd) {
-                SD[lane * ND + d] = D.d[(size_t)j * D.nd + D.d0 + d];
-                SV[lane * 2 * ND + 2 * d] = D.v[((size_t)j * 2 + 0) * D.nd + D.d0 + d];
-                SV[lane * 2 * ND + 2 * d + 1] = D.v[((size_t)j * 2 + 1) * D.nd + D.d0 + d];
-              }
-            }
-          }
-          __syncwarp();
-          if (act) {
-            for (int jj = 0; jj < ns; jj++) {
-              double2 y = SX[jj];
-              double xd = z.x - y.x, yd = z.y - y.y;
-              double az = hypot(zk.x, zk.y) * sqrt(xd * xd + yd * yd);
-              // helmkernels2d.f: <= for the charge potential-only kernel, < otherwise
-              bool le = (IFPGH == 1) && hq && !hd;
-              if (le ? (az <= thresh) : (az < thresh)) continue;
-              h_pair<ND, IFPGH>(xd, yd, zk, SQ + jj * ND, SD + jj * ND, SV + jj * 2 * ND, hq, hd,
-                                po, g1, g2, hh);
-            }
-          }
-        }
-      }
-      if (act) {
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          pot[(size_t)k * D.nd + D.d0 + d] = po[d];
-          if (IFPGH >= 2) {
-            grad[((size_t)k * 2 + 0) * D.nd + D.d0 + d] = g1[d];
-            grad[((size_t)k * 2 + 1) * D.nd + D.d0 + d] = g2[d];
-          }
-          if (IFPGH >= 3)
-            for (int c = 0; c < 3; c++) hess[((size_t)k * 3 + c) * D.nd + D.d0 + d] = hh[d][c];
+          auto Xf = [&](int k) { return rule_x(Ef, k, c); };
+          auto Yf = [&](int k) { return rule_y(Ef, k, c); };
+          hh[d][0] = cadd(hh[d][0], cmul(rule_x(Xf, n, c), mt));
+          hh[d][1] = cadd(hh[d][1], cmul(rule_y(Xf, n, c), mt));
+          hh[d][2] = cadd(hh[d][2], cmul(rule_y(Yf, n, c), mt));
         }
       }
     }
+  };
+  if (!mpole) {
+    // scaled J, downward from the series start
+    int M = 0;
+    double2 f_hi, f_lo;
+    if (!helm::jstart(q, zz, rs, M, f_hi, f_lo)) {
+      contribute(0, make_double2(1, 0), make_double2(1, 0));
+      return;
+    }
+    const int mtop = min(M, q);
+    double2 epm = make_double2(1, 0);
+    for (int k = 0; k < mtop; k++) epm = cmul(epm, ep);
+    const double2 epc = cconj(ep);
+    auto visit = [&](int m, double2 Zm) {
+      if (m > q) return;
+      contribute(m, Zm, epm);
+      epm = cmul(epm, epc);
+    };
+    visit(M, f_hi);
+    visit(M - 1, f_lo);
+    const double2 cz = cscale(crcp(zz), 2.0 * rs);
+    const double s2r = rs * rs;
+    for (int n = M - 1; n >= 1; n--) {
+      double2 nx = csub(cmul(cscale(cz, (double)n), f_lo), cscale(f_hi, s2r));
+      f_hi = f_lo;
+      f_lo = nx;
+      visit(n - 1, nx);
+    }
+  } else {
+    // scaled H, upward from H0, H1
+    if (hypot(zz.x, zz.y) < 1e-200) return;
+    double2 h0, h1;
+    helm::hank01(zz, h0, h1);
+    double2 zm1 = h0, zm = cscale(h1, rs);  // Z_0, Z_1
+    contribute(0, h0, make_double2(1, 0));
+    double2 epm = ep;
+    if (q >= 1) contribute(1, zm, epm);
+    const double2 cz = cscale(crcp(zz), 2.0 * rs);
+    const double s2r = rs * rs;
+    for (int m = 1; m < q; m++) {
+      double2 nx = csub(cmul(cscale(cz, (double)m), zm), cscale(zm1, s2r));
+      zm1 = zm;
+      zm = nx;
+      epm = cmul(epm, ep);
+      contribute(m + 1, zm, epm);
+    }
+  }
+}
+
+// steps 6 and 7, one evaluation point per thread: L2P from its leaf's local
+// expansion and M2P from the leaf's list-3 boxes; writes the outputs.
+template <int ND, int IFPGH>
+__global__ void __launch_bounds__(128) k_h_far(TV t, const HLev* __restrict__ lv, long n,
+                                               const int* __restrict__ leaf,
+                                               const double2* __restrict__ xe, HDens D, double zkr,
+                                               double zki, const double2* __restrict__ mp,
+                                               const double2* __restrict__ lo,
+                                               double2* __restrict__ pot,
+                                               double2* __restrict__ grad,
+                                               double2* __restrict__ hess) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double2 zk = make_double2(zkr, zki);
+  const double azk = hypot(zkr, zki);
+  const int b = leaf[k];
+  const int lev = t.level[b];
+  const double2 z = xe[k];
+  double2 po[ND], g1[ND], g2[ND], hh[ND][3];
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    po[d] = g1[d] = g2[d] = make_double2(0, 0);
+    hh[d][0] = hh[d][1] = hh[d][2] = make_double2(0, 0);
+  }
+  auto polar = [&](double2 c, double2& zz, double2& ep) {
+    double dx = z.x - c.x, dy = z.y - c.y;
+    double r = sqrt(dx * dx + dy * dy);
+    double th = (dx == 0 && dy == 0) ? 0.0 : atan2(dy, dx);
+    zz = make_double2(zk.x * r, zk.y * r);
+    double sn, cs;
+    sincos(th, &sn, &cs);
+    ep = make_double2(cs, sn);
+  };
+  (void)azk;
+  const HLev L = lv[lev];
+  if (L.ok && lev >= 2) {
+    double2 zz, ep;
+    polar(t.center[b], zz, ep);
+    eval_at_point<ND, IFPGH>(hexp(const_cast<double2*>(lo), L, b, ND), L.p, zk, L.rs, false, zz,
+                             ep, po, g1, g2, hh);
+  }
+  const int n3 = t.nl3[b];
+  for (int e = 0; e < n3; e++) {
+    const HLev C = lv[lev + 1];
+    if (!C.ok) break;
+    int jb = t.l3[(size_t)MNLIST3 * b + e];
+    double2 zz, ep;
+    polar(t.center[jb], zz, ep);
+    eval_at_point<ND, IFPGH>(hexp(const_cast<double2*>(mp), C, jb, ND), C.p, zk, C.rs, true, zz,
+                             ep, po, g1, g2, hh);
+  }
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    size_t o = (size_t)k * D.nd + D.d0 + d;
+    pot[o] = po[d];
+    if (IFPGH >= 2) {
+      grad[((size_t)k * 2 + 0) * D.nd + D.d0 + d] = g1[d];
+      grad[((size_t)k * 2 + 1) * D.nd + D.d0 + d] = g2[d];
+    }
+    if (IFPGH >= 3)
+      for (int c = 0; c < 3; c++) hess[((size_t)k * 3 + c) * D.nd + D.d0 + d] = hh[d][c];
+  }
+}
+
+// step 8, one evaluation point per thread: the sources of its leaf's list-1
+// boxes (h2d_direct*), added to the far field already in the outputs.
+template <int ND, int IFPGH>
+__global__ void __launch_bounds__(128) k_h_p2p(TV t, long n, const int* __restrict__ leaf,
+                                               const double2* __restrict__ xs,
+                                               const double2* __restrict__ xe, HDens D,
+                                               double zkr, double zki, double thresh,
+                                               double2* __restrict__ pot,
+                                               double2* __restrict__ grad,
+                                               double2* __restrict__ hess) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double2 zk = make_double2(zkr, zki);
+  const double azk = hypot(zkr, zki);
+  const bool hq = D.q != nullptr, hd = D.d != nullptr;
+  const int b = leaf[k];
+  const double2 z = xe[k];
+  double2 po[ND], g1[ND], g2[ND], hh[ND][3];
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    po[d] = g1[d] = g2[d] = make_double2(0, 0);
+    hh[d][0] = hh[d][1] = hh[d][2] = make_double2(0, 0);
+  }
+  // helmkernels2d.f: <= for the charge potential-only kernel, < otherwise
+  const bool le = (IFPGH == 1) && hq && !hd;
+  const int n1 = t.nl1[b];
+  for (int e = 0; e < n1; e++) {
+    int2 sr = t.srng[t.l1[(size_t)MNLIST1 * b + e]];
+    for (int j = sr.x; j < sr.y; j++) {
+      double2 y = xs[j];
+      double xd = z.x - y.x, yd = z.y - y.y;
+      double az = azk * sqrt(xd * xd + yd * yd);
+      if (le ? (az <= thresh) : (az < thresh)) continue;
+      double2 qv[ND], dv[ND];
+      double vv[2 * ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        qv[d] = hq ? D.q[(size_t)j * D.nd + D.d0 + d] : make_double2(0, 0);
+        dv[d] = hd ? D.d[(size_t)j * D.nd + D.d0 + d] : make_double2(0, 0);
+        vv[2 * d] = hd ? D.v[((size_t)j * 2 + 0) * D.nd + D.d0 + d] : 0.0;
+        vv[2 * d + 1] = hd ? D.v[((size_t)j * 2 + 1) * D.nd + D.d0 + d] : 0.0;
+      }
+      h_pair<ND, IFPGH>(xd, yd, zk, qv, dv, vv, hq, hd, po, g1, g2, hh);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    size_t o = (size_t)k * D.nd + D.d0 + d;
+    pot[o] = cadd(pot[o], po[d]);
+    if (IFPGH >= 2) {
+      size_t o1 = ((size_t)k * 2 + 0) * D.nd + D.d0 + d, o2 = ((size_t)k * 2 + 1) * D.nd + D.d0 + d;
+      grad[o1] = cadd(grad[o1], g1[d]);
+      grad[o2] = cadd(grad[o2], g2[d]);
+    }
+    if (IFPGH >= 3)
+      for (int c = 0; c < 3; c++) {
+        size_t oc = ((size_t)k * 3 + c) * D.nd + D.d0 + d;
+        hess[oc] = cadd(hess[oc], hh[d][c]);
+      }
   }
 }
 
@@ -1006,7 +983,8 @@ void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
                 const HLev* dlv, const std::vector<HLev>& hl, int maxp, const double2* tabs,
                 const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
                 double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, double thresh,
-                cudaStream_t st, cudaEvent_t* ev) {
+                const int* leaf_s, const int* leaf_t, long ns_pts, long nt_pts, cudaStream_t st,
+                cudaEvent_t* ev) {
   const int nb = T.nboxes, nl = T.nlevels;
   B2_CHECK(cudaEventRecord(ev[0], st));
   size_t sm_form = sizeof(double2) * 2 * (32 * (size_t)(maxp + 3) + 16 * 3 * ND);
@@ -1047,24 +1025,27 @@ void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[5], st));
-  const int ES = (2 * maxp + 1) + 2 * (2 * maxp + 3) + 3 * (2 * maxp + 5);
-  size_t sm_leaf = sizeof(double2) * 2 * (ES * ND + 32 * (1 + 3 * ND));
   auto leaf = [&](int use_t, int ifl, const double2* xe, double2* po, double2* gr, double2* he) {
-    if (ifl <= 0) return;
+    const long n = use_t ? nt_pts : ns_pts;
+    if (ifl <= 0 || n <= 0) return;
+    const int* lf = use_t ? leaf_t : leaf_s;
+    const int g = ceil_div(n, 128);
+#define B2_H_LEAF(IFL)                                                                        \
+  k_h_far<ND, IFL><<<g, 128, 0, st>>>(tv, dlv, n, lf, xe, D, a.zkr, a.zki, mp, lo, po, gr, he); \
+  B2_LAUNCH_CHECK();                                                                          \
+  if (a.ifnear) {                                                                             \
+    k_h_p2p<ND, IFL><<<g, 128, 0, st>>>(tv, n, lf, xs, xe, D, a.zkr, a.zki, thresh, po, gr,   \
+                                        he);                                                  \
+    B2_LAUNCH_CHECK();                                                                        \
+  }
     if (ifl == 1) {
-      set_smem(k_h_leaf<ND, 1>, sm_leaf);
-      k_h_leaf<ND, 1><<<grid_w(nb, 2), 64, sm_leaf, st>>>(tv, dlv, nb, use_t, xs, xe, D, a.zkr, a.zki,
-                                                         mp, lo, thresh, a.ifnear, po, gr, he, maxp);
+      B2_H_LEAF(1)
     } else if (ifl == 2) {
-      set_smem(k_h_leaf<ND, 2>, sm_leaf);
-      k_h_leaf<ND, 2><<<grid_w(nb, 2), 64, sm_leaf, st>>>(tv, dlv, nb, use_t, xs, xe, D, a.zkr, a.zki,
-                                                         mp, lo, thresh, a.ifnear, po, gr, he, maxp);
+      B2_H_LEAF(2)
     } else {
-      set_smem(k_h_leaf<ND, 3>, sm_leaf);
-      k_h_leaf<ND, 3><<<grid_w(nb, 2), 64, sm_leaf, st>>>(tv, dlv, nb, use_t, xs, xe, D, a.zkr, a.zki,
-                                                         mp, lo, thresh, a.ifnear, po, gr, he, maxp);
+      B2_H_LEAF(3)
     }
-    B2_LAUNCH_CHECK();
+#undef B2_H_LEAF
   };
   leaf(0, a.ifpgh, xs, ps, gs, hs);
   leaf(1, a.ifpghtarg, xt, pt, gt, ht);
@@ -1208,6 +1189,16 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
         T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p, dbs.p, a.ifpgh,
         nt > 0 ? a.ifpghtarg : 0};
   const double thresh = zkabs * T.bs0 * std::ldexp(1.0, -51);
+  // leaf box of every sorted point, for the one-point-per-thread leaf kernels
+  DBuf<int> leafs(st), leaft(st);
+  leafs.alloc(ns, st);
+  k_h_point_leaf<<<ceil_div(T.nboxes, 128), 128, 0, st>>>(tv, T.nboxes, 0, leafs.p);
+  B2_LAUNCH_CHECK();
+  if (nt > 0) {
+    leaft.alloc(nt, st);
+    k_h_point_leaf<<<ceil_div(T.nboxes, 128), 128, 0, st>>>(tv, T.nboxes, 1, leaft.p);
+    B2_LAUNCH_CHECK();
+  }
   int chunk = nd >= 4 ? 4 : (nd >= 2 ? 2 : 1);
   DBuf<double2> mp(st), lo(st);
   mp.alloc((size_t)off * chunk, st);
@@ -1221,9 +1212,9 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
     HDens D{fc ? qs.p : nullptr, fd ? ds.p : nullptr, fd ? vs.p : nullptr, nd, d0};
     B2_CHECK(cudaMemsetAsync(lo.p, 0, sizeof(double2) * (size_t)off * ND, st));
     switch (ND) {
-      case 4: helm_chunk<4>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
-      case 2: helm_chunk<2>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
-      default: helm_chunk<1>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, st, ev); break;
+      case 4: helm_chunk<4>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
+      case 2: helm_chunk<2>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
+      default: helm_chunk<1>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
     }
     if (a.timeinfo) {
       B2_CHECK(cudaEventSynchronize(ev[6]));
