@@ -341,211 +341,232 @@ __global__ void __launch_bounds__(64) k_h_p2l(TV t, const HLev* __restrict__ lv,
   }
 }
 
-// step 3: M2M, parents of one level
+// step 3: M2M, parents of one level.  One block per parent, one thread per
+// output coefficient i; each child's multipole (plain and scaled by
+// rs1^(2|j|)) and its child-slot kernel table are staged in shared memory:
+//   H2(i) += (rs1/rs2)^|i| sum_j H1(j) T(i-j) rs1^(2e),
+//   e = max(0, |j| - |i|) for j of the sign of i, else |j|   (h2dmpmp)
 template <int ND>
-__global__ void __launch_bounds__(64) k_h_m2m(TV t, const HLev* __restrict__ lv, int lev, int first,
-                                              int n, const double2* __restrict__ tabs,
-                                              double2* __restrict__ mp) {
+__global__ void __launch_bounds__(128) k_h_m2m(TV t, const HLev* __restrict__ lv, int lev, int first,
+                                               int n, const double2* __restrict__ tabs,
+                                               double2* __restrict__ mp) {
   extern __shared__ double2 hsm[];
-  HLev L = lv[lev], C = lv[lev + 1];
-  HLOOP(n) {
-    double2* H1s = hsm + (size_t)wib * ((2 * C.p + 1) * ND + HMAXP + 1);
-    double* R1 = (double*)(H1s + (2 * C.p + 1) * ND);  // rs1^(2e)
-    int b = first + bi;
+  const HLev L = lv[lev], C = lv[lev + 1];
+  const int p1 = C.p, p2 = L.p, nt = L.nsh, np1 = 2 * p1 + 1;
+  double2* Hs = hsm;                    // [np1 ND]
+  double2* Hsc = Hs + np1 * ND;         // H1(j) rs1^(2|j|)
+  double2* Ts = Hsc + np1 * ND;         // [2 nt + 1]
+  double* R1 = reinterpret_cast<double*>(Ts + 2 * nt + 1);  // rs1^(2k), k <= max(p1, p2)
+  const int tid = threadIdx.x, i = tid - p2;
+  const bool act = tid < 2 * p2 + 1;
+  const int ai = i < 0 ? -i : i;
+  const int kmax = p1 > p2 ? p1 : p2;
+  for (int k = tid; k <= kmax; k += blockDim.x) R1[k] = pow(C.rs, 2.0 * k);
+  const double fi = pow(C.rs / L.rs, (double)ai);
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
     if (t.nchild[b] == 0) continue;
-    double rs1 = C.rs, rs2 = L.rs;
-    for (int e = lane; e <= C.p; e += 32) R1[e] = pow(rs1, 2.0 * e);
-    double2 acc[4][ND];
+    double2 acc[ND];
 #pragma unroll
-    for (int s = 0; s < 4; s++)
-#pragma unroll
-      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
-    int4 ch = t.child[b];
-    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
-    const int p1 = C.p, p2 = L.p, nt = L.nsh;
+    for (int d = 0; d < ND; d++) acc[d] = make_double2(0, 0);
+    const int4 ch = t.child[b];
+    const int cc[4] = {ch.x, ch.y, ch.z, ch.w};
     for (int q = 0; q < 4; q++) {
-      int k = cc[q];
-      if (t.srng[k].y <= t.srng[k].x) continue;
-      const double2* H1 = hexp((double2*)mp, C, k, ND);
-      __syncwarp();
-      for (int e = lane; e < (2 * p1 + 1) * ND; e += 32) H1s[e] = H1[e];
-      __syncwarp();
-      const double2* T = tabs + L.tm2m + (size_t)q * (2 * nt + 1) + nt;  // T[k], k=-nt..nt
+      const int k = cc[q];
+      if (t.srng[k].y <= t.srng[k].x) continue;  // block-uniform
+      const double2* H1 = hexp(mp, C, k, ND);
+      const double2* Tg = tabs + L.tm2m + (size_t)q * (2 * nt + 1);
+      __syncthreads();  // R1 ready / the previous child is consumed
+      for (int e = tid; e < np1 * ND; e += blockDim.x) {
+        double2 h = H1[e];
+        int jj = e / ND - p1;
+        Hs[e] = h;
+        Hsc[e] = cscale(h, R1[jj < 0 ? -jj : jj]);
+      }
+      for (int e = tid; e <= 2 * nt; e += blockDim.x) Ts[e] = Tg[e];
+      __syncthreads();
+      if (!act) continue;
+      const double2* T = Ts + nt;
+      if (i == 0) {
+        for (int jj = -p1; jj <= p1; jj++) {
 #pragma unroll
-      for (int s = 0; s < 4; s++) {
-        int i = lane + 32 * s - p2;
-        if (i > p2) break;
-        int ai = i < 0 ? -i : i;
-        double fi = pow(rs1 / rs2, (double)ai);
-        double2 v[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
-        for (int j = -p1; j <= p1; j++) {
-          int aj = j < 0 ? -j : j;
-          bool same = (i == 0) || (j > 0 && i > 0) || (j < 0 && i < 0);
-          int e = same ? max(0, aj - ai) : aj;
-          if (i == 0) e = aj;
-          double2 tt = cscale(T[i - j], R1[e]);
-#pragma unroll
-          for (int d = 0; d < ND; d++) cfma(v[d], H1s[(j + p1) * ND + d], tt);
+          for (int d = 0; d < ND; d++) cfma(acc[d], Hsc[(jj + p1) * ND + d], T[-jj]);
         }
+        continue;
+      }
+      // opposite sign or j = 0: rs1^(2|j|); same sign, |j| <= |i|: 1;
+      // same sign, |j| > |i|: rs1^(2(|j| - |i|))
+      const int sg = i > 0 ? 1 : -1;
+      for (int aj = 0; aj <= p1; aj++) {
+        int jj = -sg * aj;
 #pragma unroll
-        for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], cscale(v[d], fi));
+        for (int d = 0; d < ND; d++) cfma(acc[d], Hsc[(jj + p1) * ND + d], T[i - jj]);
+      }
+      for (int aj = 1; aj <= p1; aj++) {
+        int jj = sg * aj;
+        double2 tt = T[i - jj];
+        if (aj > ai) tt = cscale(tt, R1[aj - ai]);
+#pragma unroll
+        for (int d = 0; d < ND; d++) cfma(acc[d], Hs[(jj + p1) * ND + d], tt);
       }
     }
-    double2* M = hexp(mp, L, b, ND);
+    if (act) {
+      double2* M = hexp(mp, L, b, ND);
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      int i = lane + 32 * s - p2;
-      if (i > p2) break;
-#pragma unroll
-      for (int d = 0; d < ND; d++) M[(i + p2) * ND + d] = acc[s][d];
+      for (int d = 0; d < ND; d++) M[(i + p2) * ND + d] = cscale(acc[d], fi);
     }
+    __syncthreads();
   }
 }
 
-// step 4: M2L over list 2 (same level: rs1 = rs2, (rs2/rs1)^|i| = 1)
+// step 4: M2L over list 2 (same level: rs1 = rs2, (rs2/rs1)^|i| = 1).
+// One block per target box, one thread per output coefficient i; for every
+// list-2 source the block stages its multipole (plain and scaled by
+// rs^(2|j|)) and the (level, offset) kernel table in shared memory, then
+//   L(i) += sum_j H(j) T(i-j) rs^(2 min(|i|,|j|)) [i, j of the same sign]
+// with the rscale factor folded into three j ranges (h2dmploc).
 template <int ND>
-__global__ void __launch_bounds__(64) k_h_m2l(TV t, const HLev* __restrict__ lv, int first, int n,
-                                              const double2* __restrict__ tabs,
-                                              const double2* __restrict__ mp,
-                                              double2* __restrict__ lo, int maxp) {
+__global__ void __launch_bounds__(128) k_h_m2l(TV t, const HLev* __restrict__ lv, int first, int n,
+                                               const double2* __restrict__ tabs,
+                                               const double2* __restrict__ mp,
+                                               double2* __restrict__ lo, int maxp) {
   extern __shared__ double2 hsm[];
-  HLOOP(n) {
-    int b = first + bi;
-    int n2 = t.nl2[b];
+  double2* Hs = hsm;                               // [(2 maxp + 1) ND]
+  double2* Hsc = Hs + (2 * maxp + 1) * ND;         // H(j) rs^(2|j|)
+  double2* Ts = Hsc + (2 * maxp + 1) * ND;         // [4 maxp + 1]
+  double* RS2 = reinterpret_cast<double*>(Ts + 4 * maxp + 1);  // rs^(2k), k <= maxp
+  const int tid = threadIdx.x;
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
+    const int n2 = t.nl2[b];
     if (n2 == 0 || !t.has_eval_pts(b)) continue;
-    int lev = t.level[b];
-    HLev L = lv[lev];
+    const int lev = t.level[b];
+    const HLev L = lv[lev];
     if (!L.ok) continue;
     const int p = L.p, np = 2 * p + 1, nt = 2 * p;
-    double2* Hs = hsm + (size_t)wib * (2 * (2 * maxp + 1) * ND);
-    double2* Hsc = Hs + np * ND;  // H(j) rs^(2|j|)
-    double rs = L.rs;
-    double2 acc1[4][ND], acc2[4][ND];
+    const int i = tid - p;
+    const bool act = tid < np;
+    __syncthreads();  // the previous box is done with the shared arrays
+    for (int k = tid; k <= p; k += blockDim.x) RS2[k] = pow(L.rs, 2.0 * k);
+    double2 acc1[ND], acc2[ND];
 #pragma unroll
-    for (int s = 0; s < 4; s++)
-#pragma unroll
-      for (int d = 0; d < ND; d++) acc1[s][d] = acc2[s][d] = make_double2(0, 0);
-    double2 cb = t.center[b];
-    double rinv = 1.0 / L.bs;
+    for (int d = 0; d < ND; d++) acc1[d] = acc2[d] = make_double2(0, 0);
+    const double2 cb = t.center[b];
+    const double rinv = 1.0 / L.bs;
     for (int e = 0; e < n2; e++) {
-      int jb = t.l2[(size_t)MNLIST2 * b + e];
-      double2 cj = t.center[jb];
-      int ox = __double2int_rn((cb.x - cj.x) * rinv), oy = __double2int_rn((cb.y - cj.y) * rinv);
-      const double2* T = tabs + L.tm2l + (size_t)((ox + 3) * 7 + (oy + 3)) * (2 * nt + 1) + nt;
-      const double2* H = hexp((double2*)mp, L, jb, ND);
-      __syncwarp();
-      for (int k = lane; k < np * ND; k += 32) {
+      const int jb = t.l2[(size_t)MNLIST2 * b + e];
+      const double2 cj = t.center[jb];
+      const int ox = __double2int_rn((cb.x - cj.x) * rinv);
+      const int oy = __double2int_rn((cb.y - cj.y) * rinv);
+      const double2* Tg = tabs + L.tm2l + (size_t)((ox + 3) * 7 + (oy + 3)) * (2 * nt + 1);
+      const double2* H = hexp(const_cast<double2*>(mp), L, jb, ND);
+      __syncthreads();  // RS2 written / previous source consumed
+      for (int k = tid; k < np * ND; k += blockDim.x) {
         double2 h = H[k];
-        int j = k / ND - p;
+        int jj = k / ND - p;
         Hs[k] = h;
-        Hsc[k] = cscale(h, pow(rs, 2.0 * (j < 0 ? -j : j)));
+        Hsc[k] = cscale(h, RS2[jj < 0 ? -jj : jj]);
       }
-      __syncwarp();
-#pragma unroll
-      for (int s = 0; s < 4; s++) {
-        int i = lane + 32 * s - p;
-        if (i > p) break;
+      for (int k = tid; k <= 2 * nt; k += blockDim.x) Ts[k] = Tg[k];
+      __syncthreads();
+      if (act) {
+        const double2* T = Ts + nt;  // T[k], k = -nt..nt
+        int a0, a1, b0, b1, c0, c1;  // plain, scaled, constant-factor j ranges
         if (i >= 0) {
-          for (int j = -p; j <= 0; j++) {
-            double2 tt = T[i - j];
-#pragma unroll
-            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hs[(j + p) * ND + d], tt);
-          }
-          for (int j = 1; j <= i; j++) {
-            double2 tt = T[i - j];
-#pragma unroll
-            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hsc[(j + p) * ND + d], tt);
-          }
-          for (int j = i + 1; j <= p; j++) {
-            double2 tt = T[i - j];
-#pragma unroll
-            for (int d = 0; d < ND; d++) cfma(acc2[s][d], Hs[(j + p) * ND + d], tt);
-          }
+          a0 = -p; a1 = 0; b0 = 1; b1 = i; c0 = i + 1; c1 = p;
         } else {
-          int m = -i;
-          for (int j = 0; j <= p; j++) {
-            double2 tt = T[i - j];
+          a0 = 0; a1 = p; b0 = i; b1 = -1; c0 = -p; c1 = i - 1;
+        }
+        for (int jj = a0; jj <= a1; jj++) {
+          double2 tt = T[i - jj];
 #pragma unroll
-            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hs[(j + p) * ND + d], tt);
-          }
-          for (int j = -m; j <= -1; j++) {
-            double2 tt = T[i - j];
+          for (int d = 0; d < ND; d++) cfma(acc1[d], Hs[(jj + p) * ND + d], tt);
+        }
+        for (int jj = b0; jj <= b1; jj++) {
+          double2 tt = T[i - jj];
 #pragma unroll
-            for (int d = 0; d < ND; d++) cfma(acc1[s][d], Hsc[(j + p) * ND + d], tt);
-          }
-          for (int j = -p; j <= -m - 1; j++) {
-            double2 tt = T[i - j];
+          for (int d = 0; d < ND; d++) cfma(acc1[d], Hsc[(jj + p) * ND + d], tt);
+        }
+        for (int jj = c0; jj <= c1; jj++) {
+          double2 tt = T[i - jj];
 #pragma unroll
-            for (int d = 0; d < ND; d++) cfma(acc2[s][d], Hs[(j + p) * ND + d], tt);
-          }
+          for (int d = 0; d < ND; d++) cfma(acc2[d], Hs[(jj + p) * ND + d], tt);
         }
       }
     }
-    double2* Lo = hexp(lo, L, b, ND);
+    if (act) {
+      double2* Lo = hexp(lo, L, b, ND);
+      const double f = RS2[i < 0 ? -i : i];
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      int i = lane + 32 * s - p;
-      if (i > p) break;
-      double f = pow(rs, 2.0 * (i < 0 ? -i : i));
-#pragma unroll
-      for (int d = 0; d < ND; d++) {
-        double2 v = cadd(acc1[s][d], cscale(acc2[s][d], f));
-        Lo[(i + p) * ND + d] = cadd(Lo[(i + p) * ND + d], v);
-      }
+      for (int d = 0; d < ND; d++)
+        Lo[(i + p) * ND + d] = cadd(Lo[(i + p) * ND + d], cadd(acc1[d], cscale(acc2[d], f)));
     }
   }
 }
 
-// step 5: L2L from the parents of one level
+// step 5: L2L from the parents of one level.  One block per parent, one
+// thread per output coefficient i of the children; the parent's local
+// expansion is staged once, each child slot's kernel table per child:
+//   J2(i) += sum_j J1(j) T(i-j) F(i, j),  F = 1 for i = 0,
+//   (rs1 rs2)^|i| for j of the other sign or j = 0,
+//   (rs2/rs1)^|i| rs1^(2 max(0, |i| - |j|)) for j of the sign of i  (h2dlocloc)
 template <int ND>
-__global__ void __launch_bounds__(64) k_h_l2l(TV t, const HLev* __restrict__ lv, int lev, int first,
-                                              int n, const double2* __restrict__ tabs,
-                                              double2* __restrict__ lo) {
+__global__ void __launch_bounds__(128) k_h_l2l(TV t, const HLev* __restrict__ lv, int lev, int first,
+                                               int n, const double2* __restrict__ tabs,
+                                               double2* __restrict__ lo) {
   extern __shared__ double2 hsm[];
-  HLev L = lv[lev], C = lv[lev + 1];
-  HLOOP(n) {
-    double2* J1s = hsm + (size_t)wib * ((2 * L.p + 1) * ND);
-    int b = first + bi;
+  const HLev L = lv[lev], C = lv[lev + 1];
+  const int p1 = L.p, p2 = C.p, nt = L.nsh, np1 = 2 * p1 + 1;
+  double2* Js = hsm;                    // [np1 ND]
+  double2* Ts = Js + np1 * ND;          // [4][2 nt + 1]
+  double* R1 = reinterpret_cast<double*>(Ts + 4 * (2 * nt + 1));  // rs1^(2k), k <= p2
+  const int tid = threadIdx.x, i = tid - p2;
+  const bool act = tid < 2 * p2 + 1;
+  const int ai = i < 0 ? -i : i;
+  const double rs1 = L.rs, rs2 = C.rs;
+  for (int k = tid; k <= p2; k += blockDim.x) R1[k] = pow(rs1, 2.0 * k);
+  for (int e = tid; e < 4 * (2 * nt + 1); e += blockDim.x) Ts[e] = tabs[L.tl2l + e];
+  const double A = pow(rs2 / rs1, (double)ai), Cf = pow(rs1 * rs2, (double)ai);
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
     if (t.nchild[b] == 0 || !t.has_eval_pts(b)) continue;
-    const int p1 = L.p, p2 = C.p, nt = L.nsh;
-    double rs1 = L.rs, rs2 = C.rs;
     const double2* J1 = hexp(lo, L, b, ND);
-    __syncwarp();
-    for (int e = lane; e < (2 * p1 + 1) * ND; e += 32) J1s[e] = J1[e];
-    __syncwarp();
-    int4 ch = t.child[b];
-    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    __syncthreads();  // tables ready / the previous parent is consumed
+    for (int e = tid; e < np1 * ND; e += blockDim.x) Js[e] = J1[e];
+    __syncthreads();
+    if (!act) continue;
+    const int4 ch = t.child[b];
+    const int cc[4] = {ch.x, ch.y, ch.z, ch.w};
     for (int q = 0; q < 4; q++) {
-      int k = cc[q];
-      const double2* T = tabs + L.tl2l + (size_t)q * (2 * nt + 1) + nt;
-      double2* J2 = hexp(lo, C, k, ND);
+      const double2* T = Ts + (size_t)q * (2 * nt + 1) + nt;
+      double2 acc[ND], accc[ND], acca[ND];
 #pragma unroll
-      for (int s = 0; s < 4; s++) {
-        int i = lane + 32 * s - p2;
-        if (i > p2) break;
-        int ai = i < 0 ? -i : i;
-        double A = pow(rs2 / rs1, (double)ai), Cf = pow(rs1 * rs2, (double)ai);
-        double2 v[ND];
+      for (int d = 0; d < ND; d++) acc[d] = accc[d] = acca[d] = make_double2(0, 0);
+      if (i == 0) {
+        for (int jj = -p1; jj <= p1; jj++) {
 #pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
-        for (int j = -p1; j <= p1; j++) {
-          int aj = j < 0 ? -j : j;
-          bool same = (j > 0 && i > 0) || (j < 0 && i < 0);
-          double f;
-          if (i == 0)
-            f = 1.0;
-          else if (!same)
-            f = Cf;
-          else
-            f = A * pow(rs1, 2.0 * max(0, ai - aj));
-          double2 tt = cscale(T[i - j], f);
-#pragma unroll
-          for (int d = 0; d < ND; d++) cfma(v[d], J1s[(j + p1) * ND + d], tt);
+          for (int d = 0; d < ND; d++) cfma(acc[d], Js[(jj + p1) * ND + d], T[-jj]);
         }
+      } else {
+        const int sg = i > 0 ? 1 : -1;
+        for (int aj = 0; aj <= p1; aj++) {  // other sign and j = 0
+          int jj = -sg * aj;
 #pragma unroll
-        for (int d = 0; d < ND; d++) J2[(i + p2) * ND + d] = cadd(J2[(i + p2) * ND + d], v[d]);
+          for (int d = 0; d < ND; d++) cfma(accc[d], Js[(jj + p1) * ND + d], T[i - jj]);
+        }
+        for (int aj = 1; aj <= p1; aj++) {  // same sign
+          int jj = sg * aj;
+          double2 tt = T[i - jj];
+          if (aj < ai) tt = cscale(tt, R1[ai - aj]);
+#pragma unroll
+          for (int d = 0; d < ND; d++) cfma(acca[d], Js[(jj + p1) * ND + d], tt);
+        }
+      }
+      double2* J2 = hexp(lo, C, cc[q], ND);
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        double2 v = cadd(acc[d], cadd(cscale(accc[d], Cf), cscale(acca[d], A)));
+        J2[(i + p2) * ND + d] = cadd(J2[(i + p2) * ND + d], v);
       }
     }
   }
@@ -996,9 +1017,10 @@ void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
   for (int l = nl - 1; l >= 2; l--) {
     if (!hl[l].ok) continue;
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    size_t sm = sizeof(double2) * 2 * ((2 * hl[l + 1].p + 1) * ND + HMAXP + 1);
+    size_t sm = sizeof(double2) * (2 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
+                sizeof(double) * (HMAXP + 1);
     set_smem(k_h_m2m<ND>, sm);
-    k_h_m2m<ND><<<grid_w(n, 2), 64, sm, st>>>(tv, dlv, l, f, n, tabs, mp);
+    k_h_m2m<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, dlv, l, f, n, tabs, mp);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[2], st));
@@ -1010,18 +1032,21 @@ void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
   B2_CHECK(cudaEventRecord(ev[3], st));
   if (nl >= 2) {
     int f = T.lfirst[2], n = nb - f;
-    size_t sm = sizeof(double2) * 2 * (2 * (2 * maxp + 1) * ND);
+    size_t sm = sizeof(double2) * (2 * (2 * maxp + 1) * ND + 4 * maxp + 1) +
+                sizeof(double) * (maxp + 1);
     set_smem(k_h_m2l<ND>, sm);
-    k_h_m2l<ND><<<grid_w(n, 2), 64, sm, st>>>(tv, dlv, f, n, tabs, mp, lo, maxp);
+    k_h_m2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, dlv, f, n, tabs, mp, lo,
+                                                                   maxp);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[4], st));
   for (int l = 2; l <= nl - 1; l++) {
     if (!hl[l].ok) continue;
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    size_t sm = sizeof(double2) * 2 * ((2 * hl[l].p + 1) * ND);
+    size_t sm = sizeof(double2) * ((2 * hl[l].p + 1) * ND + 4 * (2 * hl[l].nsh + 1)) +
+                sizeof(double) * (HMAXP + 1);
     set_smem(k_h_l2l<ND>, sm);
-    k_h_l2l<ND><<<grid_w(n, 2), 64, sm, st>>>(tv, dlv, l, f, n, tabs, lo);
+    k_h_l2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, dlv, l, f, n, tabs, lo);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[5], st));
