@@ -291,6 +291,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(x, dist, device):
+    """Largest value of x over the ranks (one all-reduce; x itself when not
+    distributed).  The step time of the slowest rank bounds the job."""
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_info():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -435,11 +446,7 @@ def main():
         torch.cuda.synchronize()
         launches = L.b2fmm_kernel_launches() - L0
         clocks = sampler.stop() if sampler else None
-        ms = e0.elapsed_time(e1) / steps
-        if pg:
-            t = torch.tensor([ms], device=dev, dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, pg, dev)
         return ms, tis / steps, launches, clocks
 
     prec = args.precision
@@ -559,11 +566,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    te = (time.perf_counter() - t0) / args.steps
-    if pg:
-        t = torch.tensor([te], device=dev, dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        te = float(t.item())
+    te = max_over_ranks((time.perf_counter() - t0) / args.steps, pg, dev)
     h2d = hsrc.numel() * 8 + hq_.numel() * 16 + hd_.numel() * 16 + hv_.numel() * 8
     d2h = hpot.numel() * 16 + hgrad.numel() * 16
 
