@@ -486,17 +486,19 @@ def main():
         if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     if dom == "m2l" and prec == "mixed":
         # tensor-core M2L: useful flops against the measured dense bf16 peak
-        # (MEASURED_PEAKS.json); TF32 issues at half that rate, and the split
-        # products issue 3x the useful work on K, N padded to the MMA shape
-        K = (int(P) + 7) // 8 * 8
-        N = 16 if P <= 16 else 32
-        tiles = math.ceil(st["m2l_pairs"] * nd2 / 128)
-        issued = tiles * 2 * (K // 8) * 3 * (128 * N * 8 * 2)
+        # (MEASURED_PEAKS.json); TF32 issues at half that rate.  Issued work:
+        # per tile offset step, 3 split products x K/8 MMAs of 128 x N x 8
+        # (K = 2 KH, N = 2 KH + 2 rounded to 16, KH = P rounded to 4)
+        KH = (int(P) + 3) // 4 * 4
+        K, N = 2 * KH, (2 * KH + 2 + 15) // 16 * 16
+        mma = st["m2l_tc_steps"] * 3 * (K // 8)
+        issued = mma * (128 * N * 8 * 2)
         peak = peaks.get("bf16_tflops", 1590.0)
         roofline = {"bound": "tensor", "kernel": "m2l (k_m2l_tc, tcgen05 kind::tf32)",
                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": None,
                     "issued_tensor_tflops": issued / t_dom / 1e12,
+                    "offset_steps": st["m2l_tc_steps"], "mma_instructions": mma,
                     "issued_frac_of_tf32_peak": issued / t_dom / 1e12 / (peak / 2),
                     "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else
                                     "fallback 1590 TFLOP/s bf16")}

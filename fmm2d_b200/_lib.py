@@ -112,7 +112,7 @@ def lib():
 
 
 STAT_KEYS = ["nboxes", "nlevels", "nleaves", "nterms1", "p2p_pairs", "m2l_pairs", "m2p_evals",
-             "p2l_sources", "npts_eval", "tree_ms", "fmm_ms", "nd_cauchy"]
+             "p2l_sources", "npts_eval", "tree_ms", "fmm_ms", "nd_cauchy", "m2l_tc_steps"]
 
 
 def get_stats():

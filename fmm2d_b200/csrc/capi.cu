@@ -629,10 +629,11 @@ void b2fmm_set_stats(int on) { set_stats(on != 0); }
 
 void b2fmm_get_stats(double* out, int n) {
   const LapStats& S = last_stats();
-  const double v[12] = {S.nboxes,    S.nlevels,     S.nleaves,   S.nterms1,
+  const double v[13] = {S.nboxes,    S.nlevels,     S.nleaves,   S.nterms1,
                         S.p2p_pairs, S.m2l_pairs,   S.m2p_evals, S.p2l_sources,
-                        S.npts_eval, S.tree_ms,     S.fmm_ms,    S.nd_cauchy};
-  for (int i = 0; i < n && i < 12; i++) out[i] = v[i];
+                        S.npts_eval, S.tree_ms,     S.fmm_ms,    S.nd_cauchy,
+                        S.m2l_tc_steps};
+  for (int i = 0; i < n && i < 13; i++) out[i] = v[i];
 }
 
 double b2fmm_fma_peak(int fp64) { return fma_peak_flops(fp64 != 0); }

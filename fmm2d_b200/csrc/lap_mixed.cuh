@@ -14,7 +14,7 @@ struct MixedData {
   DBuf<float2> q, d;    // all Cauchy densities, ndc per point
   DBuf<float2> utab;    // (1/o)^k for the 7x7 integer offsets o, k < P
   DBuf<float> lgtab;    // log|o|
-  M2LPairs pairs;       // flattened list-2 pairs for the tensor-core M2L
+  M2LPairs pairs;       // list-2 targets and entries for the tensor-core M2L
   DBuf<float2> mp32;    // FP32 copy of one chunk's multipoles (tensor-core M2L)
   bool tc = false;      // run M2L on the tensor cores
   int nlev = 0;         // tree levels + 1

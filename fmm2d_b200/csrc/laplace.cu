@@ -1101,8 +1101,8 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
       p.MD.tc = true;
       p.MD.nlev = T.nlevels + 1;
       p.MD.nboxes = nb;
-      m2l_tc_build_pairs(p.MD.pairs, p.tv, T.lfirst[2], nb - T.lfirst[2], nb, st);
-      if (p.MD.pairs.npairs > 0) p.MD.mp32.alloc((size_t)nb * p.P * p.chunk, st);
+      m2l_tc_build(p.MD.pairs, p.tv, T.lfirst[2], nb - T.lfirst[2], nb, p.P, p.chunk, st);
+      if (p.MD.pairs.npairs > 0) p.MD.mp32.alloc(m2l_tc_scratch(p.MD.pairs, nb, p.chunk), st);
     }
   }
   device_binomials();
@@ -1252,6 +1252,12 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st) {
     S.tree_ms = p->tree_ms;
     S.fmm_ms = t2;
     S.nd_cauchy = p->ndc;
+    S.m2l_tc_steps = 0;
+    if (p->mixed && p->MD.tc && p->MD.pairs.steps.p) {
+      unsigned long long hsteps = 0;
+      B2_CHECK(cudaMemcpy(&hsteps, p->MD.pairs.steps.p, sizeof(hsteps), cudaMemcpyDeviceToHost));
+      S.m2l_tc_steps = (double)hsteps;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

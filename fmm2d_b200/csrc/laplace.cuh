@@ -74,6 +74,7 @@ struct LapStats {
   double tree_ms;                            // tree + lists build time (device events)
   double fmm_ms;                             // everything after the tree
   double nd_cauchy;                          // Cauchy densities
+  double m2l_tc_steps;                       // tensor-core M2L: offset steps of all tiles (0: not used)
 };
 void set_stats(bool on);
 const LapStats& last_stats();

@@ -5,31 +5,40 @@
 
 namespace b2 {
 
-// Flattened list-2 pairs of all boxes of levels >= 2 that have evaluation
-// points, ordered by target box:
-// (target | level << 26, source | offset_index << 26).
+// M2L targets (boxes of levels >= 2 with list-2 boxes and evaluation
+// points, in box order) and their list-2 entries sorted by offset index:
+// the input of the offset-accumulating tensor-core kernel.
 struct M2LPairs {
-  DBuf<int2> pairs;
-  long npairs = 0;
-  bool usable = false;  // false: box indices do not fit the packed format
+  DBuf<int> tbox;                   // box | level << 26
+  DBuf<int> tstart;                 // ntgt + 1 offsets into ent
+  DBuf<unsigned long long> tmask;   // bit o: a list-2 box at offset index o
+  DBuf<int> ent;                    // source | offset index << 26
+  DBuf<float> btab;                 // resident operator image (7 base offsets)
+  DBuf<unsigned long long> steps;   // offset steps of all tiles (tensor-core work)
+  long ntgt = 0, npairs = 0;
+  int P = 0;
+  bool usable = false;  // false: box indices do not fit the packed format or P too large
 };
 
-void m2l_tc_build_pairs(M2LPairs& L, const lapk::TV& t, int first, int n, int nboxes,
-                        cudaStream_t st);
+// Builds L for boxes [first, first+n) (P coefficients; chunk = densities of
+// the main chunk, used only for the step count).
+void m2l_tc_build(M2LPairs& L, const lapk::TV& t, int first, int n, int nboxes, int P, int chunk,
+                  cudaStream_t st);
 
 // True when the tensor-core M2L supports P (expansion length).
 bool m2l_tc_supported(int P);
 
-// Enqueues the M2L contributions of all pairs into lo (FP64, [box][P][ND])
-// on st without synchronising (capturable in a CUDA graph).
-// utab/lgtab: (1/o)^k and log|o| tables of the 7x7 integer offsets; nlev:
-// number of tree levels (entries of t.boxsize that are read), <= 64; mp32:
-// scratch of nmp = nboxes * P * ND float2 for the FP32 copy of mp.  A bounded
-// wait for the tensor cores that gives up sets *err_dev to 1 (the caller
-// reports IER_TIMEOUT after synchronising).
-int m2l_tc_run(int ND, const lapk::TV& t, const M2LPairs& L, int P, const double* binom,
-               const float2* utab, const float* lgtab, const double2* mp, float2* mp32,
-               long nmp, double2* lo, int nlev, int* err_dev, cudaStream_t st);
+// float2 elements of the FP32 multipole scratch for ND densities.
+long m2l_tc_scratch(const M2LPairs& L, int nboxes, int ND);
+
+// Enqueues the M2L contributions of all list-2 boxes into lo (FP64,
+// [box][P][ND]) on st without synchronising (capturable in a CUDA graph).
+// mp32: scratch of nmp32 >= m2l_tc_scratch() float2 for the FP32 copy of mp;
+// boxsize: nlev (<= 64) box sizes by level.  A bounded wait for the tensor
+// cores that gives up sets *err_dev to 1 (the caller reports IER_TIMEOUT
+// after synchronising).
+int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long nmp32, int nboxes,
+               double2* lo, const double* boxsize, int nlev, int* err_dev, cudaStream_t st);
 
 // Probe of the tensor-core tile path: D = A B^T for a 128 x K (A) and an
 // N x K (B) FP32 matrix (row-major, device pointers), K in {8,16,24,32},

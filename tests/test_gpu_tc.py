@@ -88,3 +88,31 @@ def test_mixed_tc_vs_direct_4_densities(gpu, tc_on):
     ex = fmm.l2ddir(sources=src, targets=src[:, :500], charges=q2, pgt=2, nd=2)
     assert rel_l2(out.pot[:, :500], ex.pottarg) < 1e-6
     assert rel_l2(out.grad[:, :, :500], ex.gradtarg) < 1e-6
+
+
+@pytest.mark.parametrize("eps", [0.1, 0.01, 1e-3, 1e-4, 1e-6, 3e-7])
+@pytest.mark.parametrize("kind", ["cfmm_nd1", "lfmm_nd4"])
+def test_tc_every_expansion_length(gpu, tc_on, eps, kind):
+    """All operator sizes of the offset-accumulating kernel (P = 4, 7, 10,
+    13, 19 -> 4, 8, 12, 16, 20 coefficients per half row) with 1 and 8
+    densities per tile row group; P = 21 (eps 3e-7) runs the CUDA-core M2L.
+    The tensor-core result equals the CUDA-core FP32 M2L and the FP64 FMM to
+    FP32 accuracy."""
+    src, q, d, v = _cloud(11, 30000)
+    if kind == "cfmm_nd1":
+        f = fmm.cfmm2d
+        kw = dict(eps=eps, sources=src, charges=q, dipstr=d, pg=2)
+    else:
+        rng = np.random.default_rng(12)
+        q4 = rng.normal(size=(4, 30000)) + 1j * rng.normal(size=(4, 30000))
+        f = fmm.lfmm2d
+        kw = dict(eps=eps, sources=src, charges=q4, pg=2, nd=4)
+    out_tc = f(**kw, precision="mixed")
+    tc_on.b2fmm_set_m2l_tensor_cores(0)
+    out_cc = f(**kw, precision="mixed")
+    tc_on.b2fmm_set_m2l_tensor_cores(1)
+    out_64 = f(**kw, precision="fp64")
+    assert out_tc.ier == 0 and out_cc.ier == 0 and out_64.ier == 0
+    assert rel_l2(out_tc.pot, out_cc.pot) < 1e-6
+    assert rel_l2(out_tc.grad, out_cc.grad) < 1e-6
+    assert rel_l2(out_tc.pot, out_64.pot) < 1e-6
