@@ -71,7 +71,32 @@ LapArgs make_args(int fe, int nd, double eps, int64_t ns, const double* sources,
   return a;
 }
 
+// Second stream of the calling thread for host->device copies that overlap
+// the tree build, with the events that order it against the main stream.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t alloc_done = nullptr, copies_done = nullptr;
+  ~SideStream() {
+    if (copies_done) cudaEventDestroy(copies_done);
+    if (alloc_done) cudaEventDestroy(alloc_done);
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+SideStream& side_stream() {
+  thread_local SideStream ss;
+  if (!ss.s) {
+    B2_CHECK(cudaStreamCreateWithFlags(&ss.s, cudaStreamNonBlocking));
+    B2_CHECK(cudaEventCreateWithFlags(&ss.alloc_done, cudaEventDisableTiming));
+    B2_CHECK(cudaEventCreateWithFlags(&ss.copies_done, cudaEventDisableTiming));
+  }
+  return ss;
+}
+
 // Host-pointer driver: copies inputs to the device, runs, copies results back.
+// The point coordinates go first on the main stream (the tree needs them);
+// the densities follow on a side stream while the tree is being built, and
+// the evaluation waits for them.
 int lap_host(LapArgs h) {
   cudaStream_t st = cudaStreamPerThread;
   const int nd = h.nd;
@@ -95,16 +120,38 @@ int lap_host(LapArgs h) {
   LapArgs a = h;
   a.src = up(src, h.src, 2 * (size_t)ns);
   a.trg = up(trg, h.ifpghtarg > 0 ? h.trg : nullptr, 2 * (size_t)nt);
-  a.charge = up(q, h.charge, nq * ns);
-  a.dipstr = up(dp, h.dipstr, nq * ns);
-  a.dipvec = h.fe != FE_CAUCHY ? up(dv, h.dipstr ? h.dipvec : nullptr, 2 * (size_t)nd * ns) : nullptr;
+  // densities: allocated on the main stream, copied on the side stream
+  SideStream& ss = side_stream();
+  const double* hq = h.charge;
+  const double* hd = h.dipstr;
+  const double* hv = h.fe != FE_CAUCHY && h.dipstr ? h.dipvec : nullptr;
+  a.charge = hq ? mk(q, nq * ns) : nullptr;
+  a.dipstr = hd ? mk(dp, nq * ns) : nullptr;
+  a.dipvec = hv ? mk(dv, 2 * (size_t)nd * ns) : nullptr;
+  B2_CHECK(cudaEventRecord(ss.alloc_done, st));
+  B2_CHECK(cudaStreamWaitEvent(ss.s, ss.alloc_done, 0));
+  auto side_up = [&](const double* dst, const double* hp, size_t n) {
+    if (dst && hp && n)
+      B2_CHECK(cudaMemcpyAsync((void*)dst, hp, n * sizeof(double), cudaMemcpyHostToDevice, ss.s));
+  };
+  side_up(a.charge, hq, nq * ns);
+  side_up(a.dipstr, hd, nq * ns);
+  side_up(a.dipvec, hv, 2 * (size_t)nd * ns);
+  B2_CHECK(cudaEventRecord(ss.copies_done, ss.s));
+  // whatever happens below, the main stream (on which the buffers are freed)
+  // waits for the side copies first
+  struct WaitOnExit {
+    cudaStream_t st;
+    cudaEvent_t e;
+    ~WaitOnExit() { cudaStreamWaitEvent(st, e, 0); }
+  } wait_guard{st, ss.copies_done};
   a.pot = h.ifpgh >= 1 ? mk(po, nq * ns) : nullptr;
   a.grad = h.ifpgh >= 2 ? mk(gr, nq * gw * ns) : nullptr;
   a.hess = h.ifpgh >= 3 ? mk(he, nq * hw * ns) : nullptr;
   a.pottarg = h.ifpghtarg >= 1 ? mk(pt, nq * nt) : nullptr;
   a.gradtarg = h.ifpghtarg >= 2 ? mk(gt, nq * gw * nt) : nullptr;
   a.hesstarg = h.ifpghtarg >= 3 ? mk(ht, nq * hw * nt) : nullptr;
-  int r = lap_fmm_device(a, st);
+  int r = lap_fmm_device(a, st, ss.copies_done);
   if (r != IER_OK) return r;
   auto down = [&](double* hp, const double* dpp, size_t n) {
     if (hp && dpp && n) B2_CHECK(cudaMemcpyAsync(hp, dpp, n * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -1212,11 +1212,12 @@ void lap_plan_free(LapPlan* p) {
   }
 }
 
-int lap_fmm_device(const LapArgs& a, cudaStream_t st) {
+int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
   if ((a.fe == FE_LAPLACE || a.fe == FE_REAL) && a.dipstr && !a.dipvec) return IER_BADARG;
   LapPlan* p = nullptr;
   int r = lap_plan_create(a, st, false, &p);
   if (r != IER_OK) return r;
+  if (dens_ready) B2_CHECK(cudaStreamWaitEvent(st, dens_ready, 0));
   std::unique_ptr<LapPlan, void (*)(LapPlan*)> guard(p, lap_plan_free);
   const bool want_stats = g_stats_on.load();
   DBuf<unsigned long long> dstat(st);

@@ -39,7 +39,10 @@ struct LapArgs {
 };
 
 // Runs the FMM on device pointers on stream `st`; returns an ier code.
-int lap_fmm_device(const LapArgs& a, cudaStream_t st);
+// dens_ready (optional): an event the evaluation waits for before it reads
+// the densities (they may still be arriving on another stream while the tree
+// is built).
+int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready = nullptr);
 
 // A plan holds everything of an FMM call that depends only on the points:
 // the tree and lists, the sorted points, the operator tables and every work
