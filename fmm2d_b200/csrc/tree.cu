@@ -9,12 +9,18 @@
 // searches of the sorted keys.  Box creation, level restriction and the
 // interaction lists follow the reference's own passes and box numbering so
 // that the resulting tree is identical to the reference's, array for array.
+// All passes from the root to the final point ranges run in one persistent
+// (cooperative) kernel whose blocks step through the levels together behind
+// bounded grid barriers; box creation order comes from grid-wide exclusive
+// scans over the boxes in number order.  The host reads the level table back
+// once, then builds the lists with one more kernel.
 #include "tree.cuh"
 
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cfloat>
+#include <mutex>
 
 namespace b2 {
 
@@ -203,7 +209,7 @@ __device__ __forceinline__ void split_range(int2 r, const uint64_t* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// box kernels
+// box data
 // ---------------------------------------------------------------------------
 struct BoxPtrs {
   double2* center;
@@ -223,30 +229,19 @@ BoxPtrs ptrs(DeviceTree& T) {
                  T.iflag.p,  T.ncoll.p, T.coll.p,   T.srng.p,   T.trng.p};
 }
 
-__global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt) {
-  B.center[0] = make_double2(root[0], root[1]);
-  B.level[0] = 0;
-  B.parent[0] = -1;
-  B.nchild[0] = 0;
-  B.child[0] = make_int4(-1, -1, -1, -1);
-  B.iflag[0] = 0;
-  B.srng[0] = make_int2(0, ns);
-  B.trng[0] = make_int2(0, nt);
-}
-
-// refine if the relevant count exceeds ndiv (pts_tree2d.f:538-560)
-__global__ void k_refine_flags(BoxPtrs B, int first, int n, int idivflag, int ndiv, int* flags) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int b = first + i;
-  int nss = B.srng[b].y - B.srng[b].x, ntt = B.trng[b].y - B.trng[b].x;
-  int nn = idivflag == 0 ? nss : (idivflag == 1 ? ntt : max(nss, ntt));
-  flags[i] = nn > ndiv ? 1 : 0;
-}
-
-__global__ void k_total(const int* flags, const int* scan, int n, int* out) {
-  out[0] = n > 0 ? scan[n - 1] + flags[n - 1] : 0;
-}
+// Device control block of the tree build: level table, box count, status
+// and the grid barrier / scan scratch of the persistent build kernel.
+constexpr int TB_MAXG = 1024;  // most blocks of the build kernel
+struct TreeCtl {
+  int nboxes, nlevels, cap, status;
+  int lfirst[NLMAX + 2], llast[NLMAX + 2];
+  int tf[NLMAX + 2], tl[NLMAX + 2], newf[NLMAX + 2];
+  double bs[NLMAX + 3];
+  unsigned bar_count, bar_gen;
+  int total;
+  int tot[TB_MAXG];
+};
+enum : int { TB_OK = 0, TB_OVERFLOW = 1, TB_DEEP = 2, TB_TIMEOUT = 3 };
 
 // Create the four children of parent b as boxes base..base+3 with the
 // reference's child order (-,-), (+,-), (-,+), (+,+).
@@ -269,29 +264,41 @@ __device__ __forceinline__ void create_children(BoxPtrs& B, int b, int base, dou
   B.child[b] = make_int4(base, base + 1, base + 2, base + 3);
 }
 
-// Adaptive refinement of one level, with the children's point ranges.
-__global__ void k_make_children_t0(BoxPtrs B, int first, int n, const int* flags, const int* scan,
-                                   int child_base, double bs_child, int lev_child,
-                                   const uint64_t* skhi, const uint64_t* sklo,
-                                   const uint64_t* tkhi, const uint64_t* tklo) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !flags[i]) return;
-  int b = first + i;
-  int base = child_base + 4 * scan[i];
-  int2 sr = B.srng[b], tr = B.trng[b];
-  create_children(B, b, base, bs_child, lev_child, 0);
-  int2 r[4];
-  split_range(sr, skhi, sklo, lev_child, r);
-  for (int j = 0; j < 4; j++) B.srng[base + j] = r[j];
-  split_range(tr, tkhi, tklo, lev_child, r);
-  for (int j = 0; j < 4; j++) B.trng[base + j] = r[j];
+__global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt, TreeCtl* C, int cap) {
+  B.center[0] = make_double2(root[0], root[1]);
+  B.level[0] = 0;
+  B.parent[0] = -1;
+  B.nchild[0] = 0;
+  B.child[0] = make_int4(-1, -1, -1, -1);
+  B.iflag[0] = 0;
+  B.srng[0] = make_int2(0, ns);
+  B.trng[0] = make_int2(0, nt);
+  B.ncoll[0] = 1;
+  B.coll[0] = 0;
+  for (int q = 1; q < 9; q++) B.coll[q] = -1;
+  C->nboxes = 1;
+  C->nlevels = 0;
+  C->cap = cap;
+  C->status = TB_OK;
+  C->lfirst[0] = 0;
+  C->llast[0] = 0;
+  C->bs[0] = root[2];
+  C->bar_count = 0;
+  C->bar_gen = 0;
+}
+
+// ---------------------------------------------------------------------------
+// per-box steps of the build (pts_tree2d.f, tree_routs2d.f)
+// ---------------------------------------------------------------------------
+// refine if the relevant count exceeds ndiv (pts_tree2d.f:538-560)
+__device__ __forceinline__ int refine_flag(const BoxPtrs& B, int b, int idivflag, int ndiv) {
+  int nss = B.srng[b].y - B.srng[b].x, ntt = B.trng[b].y - B.trng[b].x;
+  int nn = idivflag == 0 ? nss : (idivflag == 1 ? ntt : max(nss, ntt));
+  return nn > ndiv ? 1 : 0;
 }
 
 // Colleagues from the parent's colleagues' children (tree_routs2d.f:160-206).
-__global__ void k_colleagues(BoxPtrs B, int first, int n, double tol) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int b = first + i;
+__device__ void colleagues(BoxPtrs& B, int b, double tol) {
   int* cl = B.coll + 9 * (size_t)b;
   int cnt = 0;
   if (B.level[b] == 0) {
@@ -322,15 +329,7 @@ __global__ void k_colleagues(BoxPtrs B, int first, int n, double tol) {
 
 // Level restriction, pass 1 ("flag"): a leaf colleague of a box's
 // grandparent that touches the box's parent (pts_tree2d.f:805-842).
-// The outcome does not depend on the order of the boxes, so all levels >= 2
-// run in one launch.
-__global__ void k_flag_pass(BoxPtrs B, int first, int n, const double* distest) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int b = first + i;
-  int lev = B.level[b];
-  if (lev < 2) return;
-  double dt = distest[lev];
+__device__ void flag_pass(BoxPtrs& B, int b, double dt) {
   int dad = B.parent[b], gd = B.parent[dad];
   double2 cd = B.center[dad];
   int ng = B.ncoll[gd];
@@ -343,11 +342,8 @@ __global__ void k_flag_pass(BoxPtrs B, int first, int n, const double* distest) 
 }
 
 // Pass 2 ("flag+"): a leaf colleague of the parent of a flagged or flag+
-// box that touches that box (pts_tree2d.f:852-890); one level per launch.
-__global__ void k_flagplus(BoxPtrs B, int first, int n, double dt) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int b = first + i;
+// box that touches that box (pts_tree2d.f:852-890).
+__device__ void flagplus(BoxPtrs& B, int b, double dt) {
   int f = B.iflag[b];
   if (f != 1 && f != 2) return;
   int dad = B.parent[b];
@@ -361,47 +357,9 @@ __global__ void k_flagplus(BoxPtrs B, int first, int n, double dt) {
   }
 }
 
-// Mark boxes (over one contiguous range, or two concatenated ranges) whose
-// flag is > 0.
-__global__ void k_mark2(const int* iflag, int f1, int n1, int f2, int n2, int* flags) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n1 + n2) return;
-  int b = i < n1 ? f1 + i : f2 + (i - n1);
-  flags[i] = iflag[b] > 0 ? 1 : 0;
-}
-
-// Refine flagged boxes of one or two concatenated ranges; children of flag-1
-// boxes become flag++ (3), of flag+ boxes 0 (tree_routs2d.f:355-385).
-__global__ void k_make_children_flag(BoxPtrs B, int f1, int n1, int f2, int n2, const int* flags,
-                                     const int* scan, int child_base, const double* boxsize) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n1 + n2 || !flags[i]) return;
-  int b = i < n1 ? f1 + i : f2 + (i - n1);
-  int lev_child = B.level[b] + 1;
-  int pf = B.iflag[b];
-  create_children(B, b, child_base + 4 * scan[i], boxsize[lev_child], lev_child, pf == 1 ? 3 : 0);
-}
-
-// Per-level counts of flagged boxes inside [lf[l], ll[l]] (T0 layout).
-__global__ void k_level_counts(const int* flags, const int* scan, int base, const int* lf,
-                               const int* ll, int l0, int l1, int* cnt) {
-  int l = l0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (l > l1) return;
-  int a = lf[l] - base, e = ll[l] - base;
-  cnt[l] = scan[e] + flags[e] - scan[a];
-}
-
-__global__ void k_keep_flag3(int* iflag, int n) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && iflag[i] != 3) iflag[i] = 0;
-}
-
 // A flag++ box is refined if a child (with children) of one of its
 // colleagues touches it (tree_routs2d.f:217-326).
-__global__ void k_update_flags(BoxPtrs B, int f1, int n1, int f2, int n2, double dt, int* flags) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n1 + n2) return;
-  int b = i < n1 ? f1 + i : f2 + (i - n1);
+__device__ int update_flag(BoxPtrs& B, int b, double dt) {
   int f = B.iflag[b];
   if (f == 3) {
     f = 0;
@@ -423,41 +381,12 @@ __global__ void k_update_flags(BoxPtrs B, int f1, int n1, int f2, int n2, double
     }
     B.iflag[b] = f;
   }
-  flags[i] = (f == 1) ? 1 : 0;
+  return f == 1 ? 1 : 0;
 }
 
-// Renumbering: per level, the level's current range, then its tail
-// (pts_tree2d.f:1066-1215).  lv = [lf, ll, tf, tl, newf] x (nl+1).
-__global__ void k_reorg_map(const int* level, int n, const int* lv, int nl1, int* map) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
-  int l = level[b];
-  int lf = lv[l], ll = lv[nl1 + l], tf = lv[2 * nl1 + l], newf = lv[4 * nl1 + l];
-  map[b] = (b >= lf && b <= ll) ? newf + (b - lf) : newf + (ll - lf + 1) + (b - tf);
-}
-
-__global__ void k_reorg_apply(BoxPtrs S, BoxPtrs D, const int* map, int n) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= n) return;
-  int m = map[b];
-  D.center[m] = S.center[b];
-  D.level[m] = S.level[b];
-  D.nchild[m] = S.nchild[b];
-  D.iflag[m] = S.iflag[b];
-  int p = S.parent[b];
-  D.parent[m] = p < 0 ? -1 : map[p];
-  int4 c = S.child[b];
-  D.child[m] = make_int4(c.x < 0 ? -1 : map[c.x], c.y < 0 ? -1 : map[c.y],
-                         c.z < 0 ? -1 : map[c.z], c.w < 0 ? -1 : map[c.w]);
-}
-
-// Point ranges of the children of every refined box of one level.
-__global__ void k_split_ranges(BoxPtrs B, int first, int n, int lev_child, const uint64_t* skhi,
+// Point ranges of the four children of refined box b.
+__device__ void split_children(BoxPtrs& B, int b, int lev_child, const uint64_t* skhi,
                                const uint64_t* sklo, const uint64_t* tkhi, const uint64_t* tklo) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int b = first + i;
-  if (B.nchild[b] == 0) return;
   int4 ch = B.child[b];
   int cc[4] = {ch.x, ch.y, ch.z, ch.w};
   int2 r[4];
@@ -467,9 +396,339 @@ __global__ void k_split_ranges(BoxPtrs B, int first, int n, int lev_child, const
   for (int j = 0; j < 4; j++) B.trng[cc[j]] = r[j];
 }
 
-__global__ void k_set_root_range(BoxPtrs B, int ns, int nt) {
-  B.srng[0] = make_int2(0, ns);
-  B.trng[0] = make_int2(0, nt);
+// ---------------------------------------------------------------------------
+// grid-wide primitives of the persistent build kernel (cooperative launch:
+// all blocks are resident).  Every wait is bounded; a barrier that gives up
+// sets TB_TIMEOUT, which releases the other blocks too.
+// ---------------------------------------------------------------------------
+constexpr long TB_BAR_LIMIT = 1L << 22;
+
+__device__ __forceinline__ int ctl_status(const TreeCtl* C) {
+  return *reinterpret_cast<const volatile int*>(&C->status);
+}
+
+// Grid barrier with release/acquire ordering at GPU scope: the arrival is
+// an atom.add.release and the wait an ld.acquire loop on the generation
+// word, so every write made before the barrier by any block is visible to
+// every block after it.
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v)
+               : "memory");
+  return old;
+}
+
+__device__ bool gbar(TreeCtl* C) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g0 = ld_acquire(&C->bar_gen);
+    if (atom_add_release(&C->bar_count, 1u) + 1 == gridDim.x) {
+      C->bar_count = 0;
+      atom_add_release(&C->bar_gen, 1u);
+    } else {
+      for (long it = 0; ld_acquire(&C->bar_gen) == g0; it++) {
+        if (it > TB_BAR_LIMIT || ctl_status(C) == TB_TIMEOUT) {
+          atomicExch(&C->status, TB_TIMEOUT);
+          break;
+        }
+        if (it > 32) __nanosleep(64);
+      }
+    }
+  }
+  __syncthreads();
+  return ctl_status(C) != TB_TIMEOUT;
+}
+
+// Item i of one box range [f1, f1+n1) or of two concatenated ranges.
+struct Items {
+  int f1, n1, f2, n;
+  __device__ __forceinline__ int box(int i) const { return i < n1 ? f1 + i : f2 + (i - n1); }
+};
+
+// Block-level exclusive scan of one 0/1 flag per thread; returns the
+// thread's exclusive rank and sets *sum to the block total.
+__device__ __forceinline__ int block_excl_scan(int f, int* wsum, int* sum) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const unsigned bal = __ballot_sync(~0u, f);
+  const int in_warp = __popc(bal & ((1u << lane) - 1u));
+  __syncthreads();
+  if (lane == 0) wsum[w] = __popc(bal);
+  __syncthreads();
+  int pre = 0, tot = 0;
+  for (int q = 0; q < nw; q++) {
+    const int v = wsum[q];
+    if (q < w) pre += v;
+    tot += v;
+  }
+  *sum = tot;
+  return pre + in_warp;
+}
+
+// Grid-wide exclusive scan of flag[i] (i < n, flags already stored) in item
+// order: rank[i] = number of flagged items before i.  Returns the total
+// (the same on every block).  Two grid barriers: after the block counts, and
+// at the end, so that every block may read any rank afterwards.
+__device__ int grid_scan(TreeCtl* C, int n, const int* flag, int* rank, int* wsum, int* red) {
+  const int G = gridDim.x, chunk = (n + G - 1) / G;
+  const int c0 = min(n, blockIdx.x * chunk), c1 = min(n, c0 + chunk);
+  int cnt = 0;
+  for (int i = c0 + threadIdx.x; i < c1 + (int)threadIdx.x; i += blockDim.x)
+    cnt += __syncthreads_count(i < c1 && flag[i]);
+  if (threadIdx.x == 0) C->tot[blockIdx.x] = cnt;
+  if (!gbar(C)) return 0;
+  if (threadIdx.x == 0) red[0] = red[1] = 0;
+  __syncthreads();
+  int pre = 0, all = 0;
+  for (int q = threadIdx.x; q < G; q += blockDim.x) {
+    const int v = *reinterpret_cast<volatile int*>(&C->tot[q]);
+    if (q < (int)blockIdx.x) pre += v;
+    all += v;
+  }
+  atomicAdd(&red[0], pre);
+  atomicAdd(&red[1], all);
+  __syncthreads();
+  int run = red[0];
+  const int total = red[1];
+  for (int i0 = c0; i0 < c1; i0 += blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const int f = i < c1 ? flag[i] : 0;
+    int s;
+    const int r = block_excl_scan(f, wsum, &s);
+    if (i < c1) rank[i] = run + r;
+    run += s;
+  }
+  // the ranks are read by other blocks (grid-stride loops) after this
+  if (!gbar(C)) return 0;
+  return total;
+}
+
+struct TreeKeys {
+  const uint64_t *skhi, *sklo, *tkhi, *tklo;
+};
+
+// Renumber the boxes: per level, the level's current range, then its tail
+// [tf, tl] (pts_tree2d.f:1066-1215), through the scratch arrays S.
+__device__ bool reorganize(TreeCtl* C, BoxPtrs& B, BoxPtrs& S, int* map, int nl) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  const int nb = C->nboxes;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int cur = 0;
+    for (int l = 0; l <= nl; l++) {
+      C->newf[l] = cur;
+      cur += (C->llast[l] - C->lfirst[l] + 1) + max(C->tl[l] - C->tf[l] + 1, 0);
+    }
+  }
+  if (!gbar(C)) return false;
+  for (int b = gt; b < nb; b += gs) {
+    const int l = B.level[b];
+    const int lf = C->lfirst[l], ll = C->llast[l];
+    map[b] = (b >= lf && b <= ll) ? C->newf[l] + (b - lf) : C->newf[l] + (ll - lf + 1) + (b - C->tf[l]);
+  }
+  if (!gbar(C)) return false;
+  for (int b = gt; b < nb; b += gs) {
+    const int m = map[b];
+    S.center[m] = B.center[b];
+    S.level[m] = B.level[b];
+    S.nchild[m] = B.nchild[b];
+    S.iflag[m] = B.iflag[b];
+    const int p = B.parent[b];
+    S.parent[m] = p < 0 ? -1 : map[p];
+    const int4 c = B.child[b];
+    S.child[m] = make_int4(c.x < 0 ? -1 : map[c.x], c.y < 0 ? -1 : map[c.y],
+                           c.z < 0 ? -1 : map[c.z], c.w < 0 ? -1 : map[c.w]);
+  }
+  if (!gbar(C)) return false;
+  for (int b = gt; b < nb; b += gs) {
+    B.center[b] = S.center[b];
+    B.level[b] = S.level[b];
+    B.nchild[b] = S.nchild[b];
+    B.iflag[b] = S.iflag[b];
+    B.parent[b] = S.parent[b];
+    B.child[b] = S.child[b];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int l = 0; l <= nl; l++) {
+      const int no = C->llast[l] - C->lfirst[l] + 1, nt = max(C->tl[l] - C->tf[l] + 1, 0);
+      C->lfirst[l] = C->newf[l];
+      C->llast[l] = C->newf[l] + no + nt - 1;
+    }
+  }
+  return gbar(C);
+}
+
+__device__ bool colleagues_all(TreeCtl* C, BoxPtrs& B, int nl) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  for (int l = 0; l <= nl; l++) {
+    const double tol = (double)1.05f * C->bs[l];
+    for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs) colleagues(B, b, tol);
+    if (!gbar(C)) return false;
+  }
+  return true;
+}
+
+// The whole level-restricted tree on the device: adaptive refinement level by
+// level (pts_tree2d.f:538-755), level restriction (pts_tree2d.f:760-1060,
+// tree_routs2d.f:217-388), renumbering and the point ranges of every box, with
+// the reference's box numbering.  Scratch: flag, rank (cap ints each) and the
+// reorganisation copies S.  Outcome in C->status (TB_OVERFLOW: more than
+// C->cap boxes; TB_DEEP: levels beyond 32 need the 51-level keys).
+__global__ void __launch_bounds__(256, 2)
+    k_tree_build(BoxPtrs B, BoxPtrs S, TreeCtl* C, int* flag, int* rank, TreeKeys K,
+                 int idivflag, int ndiv, int nlmax, int deep) {
+  __shared__ int wsum[32];
+  __shared__ int red[2];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  const int cap = C->cap;
+  // A zero-size root (all points coincide) cannot be subdivided: the
+  // children would coincide with it forever.  Keep the root as the only box.
+  if (C->bs[0] == 0.0) nlmax = 0;
+  // --- adaptive refinement ---------------------------------------------
+  int lev = 0;
+  for (; lev < nlmax; lev++) {
+    const int f = C->lfirst[lev], n = C->llast[lev] - f + 1, nb = C->nboxes;
+    for (int i = gt; i < n; i += gs) flag[i] = refine_flag(B, f + i, idivflag, ndiv);
+    if (!gbar(C)) return;
+    const int tot = grid_scan(C, n, flag, rank, wsum, red);
+    if (ctl_status(C) == TB_TIMEOUT) return;
+    if (tot == 0) break;
+    if (lev + 1 > 32 && !deep) {
+      if (gt == 0) C->status = TB_DEEP;
+      return;
+    }
+    if (nb + 4 * tot > cap) {
+      if (gt == 0) C->status = TB_OVERFLOW;
+      return;
+    }
+    const double bsc = C->bs[lev] / 2;
+    for (int i = gt; i < n; i += gs) {
+      if (!flag[i]) continue;
+      const int b = f + i, base = nb + 4 * rank[i];
+      create_children(B, b, base, bsc, lev + 1, 0);
+      split_children(B, b, lev + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
+    }
+    if (!gbar(C)) return;
+    if (gt == 0) {
+      C->bs[lev + 1] = bsc;
+      C->lfirst[lev + 1] = nb;
+      C->llast[lev + 1] = nb + 4 * tot - 1;
+      C->nboxes = nb + 4 * tot;
+    }
+    if (!gbar(C)) return;
+    const double tol = (double)1.05f * bsc;
+    for (int b = C->lfirst[lev + 1] + gt; b <= C->llast[lev + 1]; b += gs) colleagues(B, b, tol);
+    if (!gbar(C)) return;
+  }
+  const int nl = lev;
+  if (gt == 0) {
+    C->nlevels = nl;
+    C->bs[nl + 1] = C->bs[nl] / 2;
+  }
+  if (nl >= 2) {
+    // --- level restriction ---------------------------------------------
+    // pass 1: flag (levels >= 2, one pass)
+    for (int b = C->lfirst[2] + gt; b < C->nboxes; b += gs) {
+      const int l = B.level[b];
+      flag_pass(B, b, 1.05 * (C->bs[l - 1] + C->bs[l - 2]) / 2.0);
+    }
+    if (!gbar(C)) return;
+    // pass 2: flag+, finest level first
+    for (int l = nl; l >= 1; l--) {
+      const double dt = 1.05 * (C->bs[l] + C->bs[l - 1]) / 2.0;
+      for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs) flagplus(B, b, dt);
+      if (!gbar(C)) return;
+    }
+    if (gt == 0)
+      for (int l = 0; l <= nl; l++) {
+        C->tf[l] = 0;
+        C->tl[l] = -1;
+      }
+    // subdivide the flag and flag+ boxes of levels 1..nl-2
+    if (nl - 2 >= 1) {
+      const int f = C->lfirst[1], n = C->llast[nl - 2] - f + 1, nb = C->nboxes;
+      for (int i = gt; i < n; i += gs) flag[i] = B.iflag[f + i] > 0 ? 1 : 0;
+      if (!gbar(C)) return;
+      const int tot = grid_scan(C, n, flag, rank, wsum, red);
+      if (ctl_status(C) == TB_TIMEOUT) return;
+      if (tot > 0) {
+        if (nb + 4 * tot > cap) {
+          if (gt == 0) C->status = TB_OVERFLOW;
+          return;
+        }
+        for (int i = gt; i < n; i += gs) {
+          if (!flag[i]) continue;
+          const int b = f + i, lc = B.level[b] + 1;
+          create_children(B, b, nb + 4 * rank[i], C->bs[lc], lc, B.iflag[b] == 1 ? 3 : 0);
+        }
+        if (!gbar(C)) return;
+        if (gt == 0) {
+          int base = nb;
+          for (int l = 1; l <= nl - 2; l++) {
+            const int a = C->lfirst[l] - f, e = C->llast[l] - f;
+            const int c = rank[e] + flag[e] - rank[a];
+            C->tf[l + 1] = base;
+            C->tl[l + 1] = base + 4 * c - 1;
+            base += 4 * c;
+          }
+          C->nboxes = nb + 4 * tot;
+        }
+        if (!gbar(C)) return;
+      }
+    }
+    if (!reorganize(C, B, S, rank, nl)) return;
+    if (!colleagues_all(C, B, nl)) return;
+    for (int b = gt; b < C->nboxes; b += gs)
+      if (B.iflag[b] != 3) B.iflag[b] = 0;
+    if (gt == 0)
+      for (int l = 0; l <= nl; l++) {
+        C->tf[l] = 0;
+        C->tl[l] = -1;
+      }
+    if (!gbar(C)) return;
+    // pass 3: flag++ boxes, coarsest level first, refining as needed
+    for (int l = 2; l <= nl - 2; l++) {
+      const Items it{C->lfirst[l], C->llast[l] - C->lfirst[l] + 1, C->tf[l],
+                     (C->llast[l] - C->lfirst[l] + 1) + max(C->tl[l] - C->tf[l] + 1, 0)};
+      const int nb = C->nboxes;
+      const double dt = 1.05 * (C->bs[l] + C->bs[l + 1]) / 2.0;
+      for (int i = gt; i < it.n; i += gs) flag[i] = update_flag(B, it.box(i), dt);
+      if (!gbar(C)) return;
+      const int tot = grid_scan(C, it.n, flag, rank, wsum, red);
+      if (ctl_status(C) == TB_TIMEOUT) return;
+      if (tot == 0) continue;
+      if (nb + 4 * tot > cap) {
+        if (gt == 0) C->status = TB_OVERFLOW;
+        return;
+      }
+      for (int i = gt; i < it.n; i += gs) {
+        if (!flag[i]) continue;
+        const int b = it.box(i), lc = B.level[b] + 1;
+        create_children(B, b, nb + 4 * rank[i], C->bs[lc], lc, B.iflag[b] == 1 ? 3 : 0);
+      }
+      if (!gbar(C)) return;
+      if (gt == 0) {
+        C->tf[l + 1] = nb;
+        C->tl[l + 1] = nb + 4 * tot - 1;
+        C->nboxes = nb + 4 * tot;
+      }
+      if (!gbar(C)) return;
+      const double tol = (double)1.05f * C->bs[l + 1];
+      for (int b = C->tf[l + 1] + gt; b <= C->tl[l + 1]; b += gs) colleagues(B, b, tol);
+      if (!gbar(C)) return;
+    }
+    if (!reorganize(C, B, S, rank, nl)) return;
+    if (!colleagues_all(C, B, nl)) return;
+  }
+  // --- point ranges of every box of the final tree ----------------------
+  for (int l = 0; l < nl; l++) {
+    for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs)
+      if (B.nchild[b] != 0) split_children(B, b, l + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
+    if (!gbar(C)) return;
+  }
 }
 
 // Lists 1-4 of every box (tree_routs2d.f:486-710), as a gather: a box's
@@ -578,49 +837,8 @@ __global__ void k_lists(BoxPtrs B, int nb, const double* boxsize, int* nl1, int*
 }
 
 // ---------------------------------------------------------------------------
-// host helpers
+// host side
 // ---------------------------------------------------------------------------
-struct Scanner {
-  DBuf<char> tmp;
-  size_t bytes = 0;
-  DBuf<int> total;
-  // exclusive scan of flags[0..n) into scan; returns the total (synchronises)
-  int run(const int* flags, int* scan, int n, cudaStream_t st) {
-    if (n <= 0) return 0;
-    size_t need = 0;
-    B2_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, need, flags, scan, n, st));
-    if (need > bytes) {
-      tmp.alloc(need, st);
-      bytes = need;
-    }
-    B2_CHECK(cub::DeviceScan::ExclusiveSum(tmp.p, need, flags, scan, n, st));
-    if (!total.p) total.alloc(1, st);
-    k_total<<<1, 1, 0, st>>>(flags, scan, n, total.p);
-    B2_LAUNCH_CHECK();
-    int* h = (int*)pinned_bytes(sizeof(int));
-    B2_CHECK(cudaMemcpyAsync(h, total.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    B2_CHECK(cudaStreamSynchronize(st));
-    return h[0];
-  }
-};
-
-void ensure_cap(DeviceTree& T, int need) {
-  if (need <= T.cap) return;
-  int nc = std::max(need, T.cap * 2);
-  size_t keep = T.nboxes;
-  T.center.grow(nc, keep);
-  T.level.grow(nc, keep);
-  T.parent.grow(nc, keep);
-  T.nchild.grow(nc, keep);
-  T.child.grow(nc, keep);
-  T.iflag.grow(nc, keep);
-  T.ncoll.grow(nc, keep);
-  T.coll.grow((size_t)9 * nc, (size_t)9 * keep);
-  T.srng.grow(nc, keep);
-  T.trng.grow(nc, keep);
-  T.cap = nc;
-}
-
 void alloc_boxes(DeviceTree& T, int cap) {
   cudaStream_t st = T.st;
   T.center.alloc(cap, st);
@@ -636,172 +854,22 @@ void alloc_boxes(DeviceTree& T, int cap) {
   T.cap = cap;
 }
 
-void colleagues_level(DeviceTree& T, int lev, int first, int n) {
-  if (n <= 0) return;
-  double tol = (double)1.05f * T.boxsize[lev];
-  k_colleagues<<<ceil_div(n, 128), 128, 0, T.st>>>(ptrs(T), first, n, tol);
-  B2_LAUNCH_CHECK();
-}
-
-void colleagues_all(DeviceTree& T) {
-  for (int l = 0; l <= T.nlevels; l++)
-    colleagues_level(T, l, T.lfirst[l], T.llast[l] - T.lfirst[l] + 1);
-}
-
-void reorganize(DeviceTree& T, const std::vector<int>& tf, const std::vector<int>& tl) {
-  int nl1 = T.nlevels + 1;
-  std::vector<int> lv(5 * nl1);
-  int cur = 0;
-  for (int l = 0; l < nl1; l++) {
-    int no = T.llast[l] - T.lfirst[l] + 1;
-    int nt = tl[l] - tf[l] + 1;
-    lv[l] = T.lfirst[l];
-    lv[nl1 + l] = T.llast[l];
-    lv[2 * nl1 + l] = tf[l];
-    lv[3 * nl1 + l] = tl[l];
-    lv[4 * nl1 + l] = cur;
-    cur += no + std::max(nt, 0);
+// Resident blocks of the persistent build kernel on this device.
+int tree_grid() {
+  static std::mutex mu;
+  static int grid[128] = {0};
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  if (!grid[dev]) {
+    int nsm = 0, per = 0, coop = 0;
+    B2_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    B2_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) throw CudaError("tree build: cooperative launch not supported", IER_CUDA);
+    B2_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_build, 256, 0));
+    grid[dev] = std::max(1, std::min(per * nsm, TB_MAXG));
   }
-  cudaStream_t st = T.st;
-  int* hp = (int*)pinned_bytes(sizeof(int) * lv.size());
-  B2_CHECK(cudaStreamSynchronize(st));  // the pinned scratch may still be in flight
-  std::copy(lv.begin(), lv.end(), hp);
-  DBuf<int> dlv(st), map(st);
-  dlv.alloc(lv.size(), st);
-  B2_CHECK(cudaMemcpyAsync(dlv.p, hp, sizeof(int) * lv.size(), cudaMemcpyHostToDevice, st));
-  int nb = T.nboxes;
-  map.alloc(nb, st);
-  k_reorg_map<<<ceil_div(nb, 256), 256, 0, st>>>(T.level.p, nb, dlv.p, nl1, map.p);
-  B2_LAUNCH_CHECK();
-  DeviceTree N;
-  N.st = st;
-  alloc_boxes(N, T.cap);
-  k_reorg_apply<<<ceil_div(nb, 256), 256, 0, st>>>(ptrs(T), ptrs(N), map.p, nb);
-  B2_LAUNCH_CHECK();
-  std::swap(T.center, N.center);
-  std::swap(T.level, N.level);
-  std::swap(T.parent, N.parent);
-  std::swap(T.nchild, N.nchild);
-  std::swap(T.child, N.child);
-  std::swap(T.iflag, N.iflag);
-  for (int l = 0; l < nl1; l++) {
-    int no = T.llast[l] - T.lfirst[l] + 1;
-    int nt = std::max(tl[l] - tf[l] + 1, 0);
-    T.lfirst[l] = lv[4 * nl1 + l];
-    T.llast[l] = lv[4 * nl1 + l] + no + nt - 1;
-  }
-  B2_CHECK(cudaStreamSynchronize(st));  // keep `hp` valid until the upload is done
-}
-
-DBuf<double> upload_doubles(const std::vector<double>& v, cudaStream_t st) {
-  DBuf<double> d(st);
-  d.alloc(v.size(), st);
-  double* hp = (double*)pinned_bytes(sizeof(double) * v.size());
-  B2_CHECK(cudaStreamSynchronize(st));
-  std::copy(v.begin(), v.end(), hp);
-  B2_CHECK(cudaMemcpyAsync(d.p, hp, sizeof(double) * v.size(), cudaMemcpyHostToDevice, st));
-  B2_CHECK(cudaStreamSynchronize(st));
-  return d;
-}
-
-void fix_level_restriction(DeviceTree& T, Scanner& sc) {
-  cudaStream_t st = T.st;
-  const int nl = T.nlevels;
-  std::vector<double> dflag(nl + 1, 0.0);
-  for (int l = 2; l <= nl; l++) dflag[l] = 1.05 * (T.boxsize[l - 1] + T.boxsize[l - 2]) / 2.0;
-  DBuf<double> ddflag = upload_doubles(dflag, st);
-  DBuf<double> dbs = upload_doubles(T.boxsize, st);
-  // pass 1: flag
-  {
-    int f = T.lfirst[2], n = T.nboxes - f;
-    k_flag_pass<<<ceil_div(n, 128), 128, 0, st>>>(ptrs(T), f, n, ddflag.p);
-    B2_LAUNCH_CHECK();
-  }
-  // pass 2: flag+, finest level first
-  for (int l = nl; l >= 1; l--) {
-    double dt = 1.05 * (T.boxsize[l] + T.boxsize[l - 1]) / 2.0;
-    int n = T.llast[l] - T.lfirst[l] + 1;
-    k_flagplus<<<ceil_div(n, 128), 128, 0, st>>>(ptrs(T), T.lfirst[l], n, dt);
-    B2_LAUNCH_CHECK();
-  }
-  std::vector<int> tf(nl + 1, 0), tl(nl + 1, -1);
-  // subdivide flag and flag+ boxes of levels 1..nl-2
-  if (nl - 2 >= 1) {
-    int f = T.lfirst[1], n = T.llast[nl - 2] - f + 1;
-    DBuf<int> flags(st), scan(st), cnt(st);
-    flags.alloc(n, st);
-    scan.alloc(n, st);
-    k_mark2<<<ceil_div(n, 256), 256, 0, st>>>(T.iflag.p, f, n, 0, 0, flags.p);
-    B2_LAUNCH_CHECK();
-    int tot = sc.run(flags.p, scan.p, n, st);
-    if (tot > 0) {
-      std::vector<int> lfl(nl + 1), lll(nl + 1);
-      for (int l = 0; l <= nl; l++) {
-        lfl[l] = T.lfirst[l];
-        lll[l] = T.llast[l];
-      }
-      DBuf<int> dlf(st), dll(st);
-      dlf.alloc(nl + 1, st);
-      dll.alloc(nl + 1, st);
-      int* hp = (int*)pinned_bytes(sizeof(int) * 2 * (nl + 1));
-      std::copy(lfl.begin(), lfl.end(), hp);
-      std::copy(lll.begin(), lll.end(), hp + nl + 1);
-      B2_CHECK(cudaMemcpyAsync(dlf.p, hp, sizeof(int) * (nl + 1), cudaMemcpyHostToDevice, st));
-      B2_CHECK(cudaMemcpyAsync(dll.p, hp + nl + 1, sizeof(int) * (nl + 1), cudaMemcpyHostToDevice,
-                               st));
-      cnt.alloc(nl + 1, st);
-      cnt.zero(nl + 1);
-      k_level_counts<<<1, 64, 0, st>>>(flags.p, scan.p, f, dlf.p, dll.p, 1, nl - 2, cnt.p);
-      B2_LAUNCH_CHECK();
-      int* hc = (int*)pinned_bytes(sizeof(int) * (nl + 1) * 3);
-      B2_CHECK(cudaStreamSynchronize(st));
-      B2_CHECK(cudaMemcpyAsync(hc, cnt.p, sizeof(int) * (nl + 1), cudaMemcpyDeviceToHost, st));
-      B2_CHECK(cudaStreamSynchronize(st));
-      std::vector<int> c(hc, hc + nl + 1);
-      ensure_cap(T, T.nboxes + 4 * tot);
-      k_make_children_flag<<<ceil_div(n, 128), 128, 0, st>>>(ptrs(T), f, n, 0, 0, flags.p, scan.p,
-                                                              T.nboxes, dbs.p);
-      B2_LAUNCH_CHECK();
-      int base = T.nboxes;
-      for (int l = 1; l <= nl - 2; l++) {
-        tf[l + 1] = base;
-        tl[l + 1] = base + 4 * c[l] - 1;
-        base += 4 * c[l];
-      }
-      T.nboxes += 4 * tot;
-    }
-  }
-  reorganize(T, tf, tl);
-  colleagues_all(T);
-  k_keep_flag3<<<ceil_div(T.nboxes, 256), 256, 0, st>>>(T.iflag.p, T.nboxes);
-  B2_LAUNCH_CHECK();
-  std::fill(tf.begin(), tf.end(), 0);
-  std::fill(tl.begin(), tl.end(), -1);
-  // pass 3: flag++ boxes, coarsest level first, refining as needed
-  DBuf<int> flags(st), scan(st);
-  for (int l = 2; l <= nl - 2; l++) {
-    int f1 = T.lfirst[l], n1 = T.llast[l] - f1 + 1;
-    int f2 = tf[l], n2 = std::max(tl[l] - tf[l] + 1, 0);
-    int n = n1 + n2;
-    if (n <= 0) continue;
-    flags.grow(n, 0);
-    scan.grow(n, 0);
-    double dt = 1.05 * (T.boxsize[l] + T.boxsize[l + 1]) / 2.0;
-    k_update_flags<<<ceil_div(n, 128), 128, 0, st>>>(ptrs(T), f1, n1, f2, n2, dt, flags.p);
-    B2_LAUNCH_CHECK();
-    int tot = sc.run(flags.p, scan.p, n, st);
-    if (tot == 0) continue;
-    ensure_cap(T, T.nboxes + 4 * tot);
-    k_make_children_flag<<<ceil_div(n, 128), 128, 0, st>>>(ptrs(T), f1, n1, f2, n2, flags.p,
-                                                            scan.p, T.nboxes, dbs.p);
-    B2_LAUNCH_CHECK();
-    tf[l + 1] = T.nboxes;
-    tl[l + 1] = T.nboxes + 4 * tot - 1;
-    T.nboxes += 4 * tot;
-    colleagues_level(T, l + 1, tf[l + 1], 4 * tot);
-  }
-  reorganize(T, tf, tl);
-  colleagues_all(T);
+  return grid[dev];
 }
 
 }  // namespace
@@ -827,64 +895,70 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   // sort points along the virtual complete tree
   sort_by_key(src, ns, T.root.p, false, T.skhi, T.sklo, T.isrc, st);
   sort_by_key(trg, nt, T.root.p, false, T.tkhi, T.tklo, T.itarg, st);
-  // boxes
-  int cap0 = (int)std::min<long>(8 + 3 * (ns + nt) / std::max(ndiv, 1), 1L << 30);
-  alloc_boxes(T, std::max(cap0, 64));
-  k_init_root<<<1, 1, 0, st>>>(ptrs(T), T.root.p, (int)ns, (int)nt);
-  B2_LAUNCH_CHECK();
-  double* hr = (double*)pinned_bytes(3 * sizeof(double));
-  B2_CHECK(cudaMemcpyAsync(hr, T.root.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-  B2_CHECK(cudaStreamSynchronize(st));
-  T.cx0 = hr[0];
-  T.cy0 = hr[1];
-  T.bs0 = hr[2];
-  T.boxsize.assign(1, T.bs0);
-  T.lfirst.assign(1, 0);
-  T.llast.assign(1, 0);
-  T.nboxes = 1;
-  Scanner sc;
-  DBuf<int> flags(st), scan(st);
-  int lev;
-  // A zero-size root (all points coincide) cannot be subdivided: the
-  // children would coincide with it forever.  Keep the root as the only box.
-  if (T.bs0 == 0.0) nlmax = 0;
-  for (lev = 0; lev < nlmax; lev++) {
-    int f = T.lfirst[lev], n = T.llast[lev] - f + 1;
-    flags.grow(n, 0);
-    scan.grow(n, 0);
-    k_refine_flags<<<ceil_div(n, 256), 256, 0, st>>>(ptrs(T), f, n, idivflag, ndiv, flags.p);
+  // boxes: one persistent kernel builds the whole tree; it is re-run with
+  // more capacity (or with the 51-level keys) when it reports that need
+  int cap = (int)std::min<long>(8 + 3 * (ns + nt) / std::max(ndiv, 1), 1L << 30);
+  cap = std::max(cap, 64);
+  DBuf<TreeCtl> ctl(st);
+  ctl.alloc(1, st);
+  const int grid = tree_grid();
+  TreeCtl* hc = (TreeCtl*)pinned_bytes(sizeof(TreeCtl));
+  for (;;) {
+    alloc_boxes(T, cap);
+    DBuf<double2> sc(st);
+    DBuf<int> sl(st), sp(st), sn(st), sf(st), flag(st), rank(st);
+    DBuf<int4> sch(st);
+    sc.alloc(cap, st);
+    sl.alloc(cap, st);
+    sp.alloc(cap, st);
+    sn.alloc(cap, st);
+    sf.alloc(cap, st);
+    sch.alloc(cap, st);
+    flag.alloc(cap, st);
+    rank.alloc(cap, st);
+    BoxPtrs B = ptrs(T);
+    BoxPtrs S{sc.p, sl.p, sp.p, sn.p, sch.p, sf.p, nullptr, nullptr, nullptr, nullptr};
+    k_init_root<<<1, 1, 0, st>>>(B, T.root.p, (int)ns, (int)nt, ctl.p, cap);
     B2_LAUNCH_CHECK();
-    int nref = sc.run(flags.p, scan.p, n, st);
-    if (nref == 0) break;
-    if (lev + 1 > 32 && !T.deep_sorted) {
+    TreeKeys K{T.skhi.p, T.sklo.p, T.tkhi.p, T.tklo.p};
+    TreeCtl* C = ctl.p;
+    int* fp = flag.p;
+    int* rp = rank.p;
+    int deep = T.deep_sorted ? 1 : 0;
+    void* args[] = {&B, &S, &C, &fp, &rp, &K, &idivflag, &ndiv, &nlmax, &deep};
+    B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(256), args, 0,
+                                         st));
+    B2_CHECK(cudaMemcpyAsync(hc, ctl.p, sizeof(TreeCtl), cudaMemcpyDeviceToHost, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    if (hc->status == TB_DEEP && !T.deep_sorted) {
       // levels beyond 32 need the points ordered by all key digits
       sort_by_key(src, ns, T.root.p, true, T.skhi, T.sklo, T.isrc, st);
       sort_by_key(trg, nt, T.root.p, true, T.tkhi, T.tklo, T.itarg, st);
       T.deep_sorted = true;
+      continue;
     }
-    T.boxsize.push_back(T.boxsize[lev] / 2);
-    ensure_cap(T, T.nboxes + 4 * nref);
-    k_make_children_t0<<<ceil_div(n, 128), 128, 0, st>>>(
-        ptrs(T), f, n, flags.p, scan.p, T.nboxes, T.boxsize[lev + 1], lev + 1, T.skhi.p, T.sklo.p,
-        T.tkhi.p, T.tklo.p);
-    B2_LAUNCH_CHECK();
-    T.lfirst.push_back(T.nboxes);
-    T.nboxes += 4 * nref;
-    T.llast.push_back(T.nboxes - 1);
+    if (hc->status == TB_OVERFLOW) {
+      if (cap >= (1 << 29)) throw CudaError("tree build: too many boxes", IER_ALLOC);
+      cap = (int)std::min<long>(2L * cap, 1L << 30);
+      continue;
+    }
+    if (hc->status != TB_OK) throw CudaError("tree build: grid barrier timed out", IER_TIMEOUT);
+    break;
   }
-  T.nlevels = lev;
-  colleagues_all(T);
-  if (T.nlevels >= 2) fix_level_restriction(T, sc);
-  // point ranges of every box of the final tree
-  k_set_root_range<<<1, 1, 0, st>>>(ptrs(T), (int)ns, (int)nt);
-  B2_LAUNCH_CHECK();
-  for (int l = 0; l < T.nlevels; l++) {
-    int n = T.llast[l] - T.lfirst[l] + 1;
-    k_split_ranges<<<ceil_div(n, 128), 128, 0, st>>>(ptrs(T), T.lfirst[l], n, l + 1, T.skhi.p,
-                                                     T.sklo.p, T.tkhi.p, T.tklo.p);
-    B2_LAUNCH_CHECK();
+  T.nlevels = hc->nlevels;
+  T.nboxes = hc->nboxes;
+  T.lfirst.assign(hc->lfirst, hc->lfirst + T.nlevels + 1);
+  T.llast.assign(hc->llast, hc->llast + T.nlevels + 1);
+  T.boxsize.assign(hc->bs, hc->bs + T.nlevels + 1);
+  T.bs0 = hc->bs[0];
+  {
+    double* hr = (double*)pinned_bytes(3 * sizeof(double));
+    B2_CHECK(cudaMemcpyAsync(hr, T.root.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    T.cx0 = hr[0];
+    T.cy0 = hr[1];
   }
-  // interaction lists
+  // interaction lists (boxsize(nlevels+1) for the leaf tests is in the control block)
   int nb = T.nboxes;
   T.nlist1.alloc(nb, st);
   T.list1.alloc((size_t)MNLIST1 * nb, st);
@@ -894,10 +968,7 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   T.list3.alloc((size_t)MNLIST3 * nb, st);
   T.nlist4.alloc(nb, st);
   T.list4.alloc((size_t)MNLIST4 * nb, st);
-  std::vector<double> bsx(T.boxsize);
-  bsx.push_back(T.boxsize.back() / 2);  // boxsize(nlevels+1) for the leaf tests
-  DBuf<double> dbs = upload_doubles(bsx, st);
-  k_lists<<<ceil_div(nb, 128), 128, 0, st>>>(ptrs(T), nb, dbs.p, T.nlist1.p, T.list1.p,
+  k_lists<<<ceil_div(nb, 128), 128, 0, st>>>(ptrs(T), nb, &ctl.p->bs[0], T.nlist1.p, T.list1.p,
                                              T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p,
                                              T.nlist4.p, T.list4.p);
   B2_LAUNCH_CHECK();
