@@ -186,28 +186,6 @@ void sort_by_key(const double* xy, long n, const double* root, bool deep, DBuf<u
   B2_LAUNCH_CHECK();
 }
 
-// Split the sorted range r of a box at level lev-1 into its four children
-// at level lev (digit 0..3 is non-decreasing inside the range).
-__device__ __forceinline__ void split_range(int2 r, const uint64_t* __restrict__ khi,
-                                            const uint64_t* __restrict__ klo, int lev,
-                                            int2 out[4]) {
-  int b[5];
-  b[0] = r.x;
-  b[4] = r.y;
-  for (int d = 1; d <= 3; d++) {
-    int lo = b[d - 1], hi = r.y;
-    while (lo < hi) {
-      int m = (lo + hi) >> 1;
-      if (key_digit(khi[m], klo[m], lev) < d)
-        lo = m + 1;
-      else
-        hi = m;
-    }
-    b[d] = lo;
-  }
-  for (int d = 0; d < 4; d++) out[d] = make_int2(b[d], b[d + 1]);
-}
-
 // ---------------------------------------------------------------------------
 // box data
 // ---------------------------------------------------------------------------
@@ -218,6 +196,7 @@ struct BoxPtrs {
   int* nchild;
   int4* child;
   int* iflag;
+  uint64_t* pkey;  // path from the root, 2 bits per level (build scratch)
   int* ncoll;
   int* coll;
   int2* srng;
@@ -225,21 +204,23 @@ struct BoxPtrs {
 };
 
 BoxPtrs ptrs(DeviceTree& T) {
-  return BoxPtrs{T.center.p, T.level.p, T.parent.p, T.nchild.p, T.child.p,
-                 T.iflag.p,  T.ncoll.p, T.coll.p,   T.srng.p,   T.trng.p};
+  return BoxPtrs{T.center.p, T.level.p, T.parent.p, T.nchild.p, T.child.p, T.iflag.p,
+                 nullptr,    T.ncoll.p, T.coll.p,   T.srng.p,   T.trng.p};
 }
 
 // Device control block of the tree build: level table, box count, status
 // and the grid barrier / scan scratch of the persistent build kernel.
-constexpr int TB_MAXG = 1024;  // most blocks of the build kernel
+constexpr int TB_MAXG = 1024;    // most blocks of the build kernel
+constexpr int TB_THREADS = 512;  // threads per block (one block per SM)
+constexpr int TB_GROUPS = 8;     // first-level arrival counters of the grid barrier
 struct TreeCtl {
   int nboxes, nlevels, cap, status;
   int lfirst[NLMAX + 2], llast[NLMAX + 2];
-  int tf[NLMAX + 2], tl[NLMAX + 2], newf[NLMAX + 2];
+  int tf[NLMAX + 2], tl[NLMAX + 2], lcnt[NLMAX + 2];
   double bs[NLMAX + 3];
-  unsigned bar_count, bar_gen;
-  int total;
-  int tot[TB_MAXG];
+  unsigned bar_sub[TB_GROUPS * 32];  // one 128-byte line per group
+  unsigned bar_top, bar_gen;
+  int tot[2][TB_MAXG];  // per-block counts of the scans, alternating
 };
 enum : int { TB_OK = 0, TB_OVERFLOW = 1, TB_DEEP = 2, TB_TIMEOUT = 3 };
 
@@ -249,6 +230,7 @@ __device__ __forceinline__ void create_children(BoxPtrs& B, int b, int base, dou
                                                 int lev_child, int child_flag) {
   double2 c = B.center[b];
   double h = bs_child / 2;
+  const uint64_t pk = B.pkey[b];
   for (int j = 0; j < 4; j++) {
     int k = base + j;
     B.center[k] = make_double2(c.x + ((j & 1) ? h : -h), c.y + ((j < 2) ? -h : h));
@@ -257,6 +239,7 @@ __device__ __forceinline__ void create_children(BoxPtrs& B, int b, int base, dou
     B.nchild[k] = 0;
     B.child[k] = make_int4(-1, -1, -1, -1);
     B.iflag[k] = child_flag;
+    B.pkey[k] = pk * 4 + (uint64_t)j;
     B.srng[k] = make_int2(0, 0);
     B.trng[k] = make_int2(0, 0);
   }
@@ -271,6 +254,7 @@ __global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt, TreeC
   B.nchild[0] = 0;
   B.child[0] = make_int4(-1, -1, -1, -1);
   B.iflag[0] = 0;
+  B.pkey[0] = 0;
   B.srng[0] = make_int2(0, ns);
   B.trng[0] = make_int2(0, nt);
   B.ncoll[0] = 1;
@@ -283,7 +267,8 @@ __global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt, TreeC
   C->lfirst[0] = 0;
   C->llast[0] = 0;
   C->bs[0] = root[2];
-  C->bar_count = 0;
+  for (int q = 0; q < TB_GROUPS * 32; q++) C->bar_sub[q] = 0;
+  C->bar_top = 0;
   C->bar_gen = 0;
 }
 
@@ -384,16 +369,73 @@ __device__ int update_flag(BoxPtrs& B, int b, double dt) {
   return f == 1 ? 1 : 0;
 }
 
-// Point ranges of the four children of refined box b.
+// Point ranges of the four children of refined box b: the three digit
+// boundaries in the source range and the three in the target range are six
+// independent binary searches, stepped together so that their loads overlap.
 __device__ void split_children(BoxPtrs& B, int b, int lev_child, const uint64_t* skhi,
                                const uint64_t* sklo, const uint64_t* tkhi, const uint64_t* tklo) {
-  int4 ch = B.child[b];
-  int cc[4] = {ch.x, ch.y, ch.z, ch.w};
-  int2 r[4];
-  split_range(B.srng[b], skhi, sklo, lev_child, r);
-  for (int j = 0; j < 4; j++) B.srng[cc[j]] = r[j];
-  split_range(B.trng[b], tkhi, tklo, lev_child, r);
-  for (int j = 0; j < 4; j++) B.trng[cc[j]] = r[j];
+  const int2 rs = B.srng[b], rt = B.trng[b];
+  int lo[6], hi[6];
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    lo[q] = q < 3 ? rs.x : rt.x;
+    hi[q] = q < 3 ? rs.y : rt.y;
+  }
+  for (;;) {
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      if (lo[q] < hi[q]) {
+        any = true;
+        const int m = (lo[q] + hi[q]) >> 1;
+        const int dg = q < 3 ? key_digit(skhi[m], sklo[m], lev_child)
+                             : key_digit(tkhi[m], tklo[m], lev_child);
+        if (dg < (q % 3) + 1)
+          lo[q] = m + 1;
+        else
+          hi[q] = m;
+      }
+    }
+    if (!any) break;
+  }
+  const int4 ch = B.child[b];
+  const int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+  const int bs_[5] = {rs.x, lo[0], lo[1], lo[2], rs.y};
+  const int bt_[5] = {rt.x, lo[3], lo[4], lo[5], rt.y};
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    B.srng[cc[j]] = make_int2(bs_[j], bs_[j + 1]);
+    B.trng[cc[j]] = make_int2(bt_[j], bt_[j + 1]);
+  }
+}
+
+// Ranges of the sorted source and target keys (first 32 levels) whose top
+// 2*lev bits equal the box path pk: the points of the box.  The four binary
+// searches (first key with prefix >= pk, first with prefix > pk, in both
+// arrays) are stepped together.
+__device__ void prefix_ranges(const uint64_t* __restrict__ skhi, int ns,
+                              const uint64_t* __restrict__ tkhi, int nt, uint64_t pk, int lev,
+                              int2& rs, int2& rt) {
+  const int sh = 64 - 2 * lev;
+  int lo[4] = {0, 0, 0, 0}, hi[4] = {ns, ns, nt, nt};
+  for (;;) {
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      if (lo[q] < hi[q]) {
+        any = true;
+        const int m = (lo[q] + hi[q]) >> 1;
+        const uint64_t v = (q < 2 ? skhi[m] : tkhi[m]) >> sh;
+        if ((q & 1) ? v <= pk : v < pk)
+          lo[q] = m + 1;
+        else
+          hi[q] = m;
+      }
+    }
+    if (!any) break;
+  }
+  rs = make_int2(lo[0], lo[1]);
+  rt = make_int2(lo[2], lo[3]);
 }
 
 // ---------------------------------------------------------------------------
@@ -401,24 +443,25 @@ __device__ void split_children(BoxPtrs& B, int b, int lev_child, const uint64_t*
 // all blocks are resident).  Every wait is bounded; a barrier that gives up
 // sets TB_TIMEOUT, which releases the other blocks too.
 // ---------------------------------------------------------------------------
-constexpr long TB_BAR_LIMIT = 1L << 22;
+constexpr long long TB_BAR_CYCLES = 1LL << 30;  // about half a second
 
 __device__ __forceinline__ int ctl_status(const TreeCtl* C) {
   return *reinterpret_cast<const volatile int*>(&C->status);
 }
 
-// Grid barrier with release/acquire ordering at GPU scope: the arrival is
-// an atom.add.release and the wait an ld.acquire loop on the generation
-// word, so every write made before the barrier by any block is visible to
-// every block after it.
+// Two-level grid barrier with acquire-release ordering at GPU scope: a block
+// arrives on its group counter, the last arrival of a group on the top
+// counter, and the last arrival there advances the generation word the
+// blocks wait on (ld.acquire), so every write made before the barrier by any
+// block is visible to every block after it.
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ unsigned atom_add_release(unsigned* p, unsigned v) {
+__device__ __forceinline__ unsigned atom_add_acqrel(unsigned* p, unsigned v) {
   unsigned old;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v)
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v)
                : "memory");
   return old;
 }
@@ -427,16 +470,23 @@ __device__ bool gbar(TreeCtl* C) {
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned g0 = ld_acquire(&C->bar_gen);
-    if (atom_add_release(&C->bar_count, 1u) + 1 == gridDim.x) {
-      C->bar_count = 0;
-      atom_add_release(&C->bar_gen, 1u);
-    } else {
-      for (long it = 0; ld_acquire(&C->bar_gen) == g0; it++) {
-        if (it > TB_BAR_LIMIT || ctl_status(C) == TB_TIMEOUT) {
+    const int G = gridDim.x, ng = min(TB_GROUPS, G), grp = blockIdx.x % ng;
+    const unsigned members = (unsigned)((G - grp + ng - 1) / ng);
+    unsigned* sub = &C->bar_sub[grp * 32];
+    if (atom_add_acqrel(sub, 1u) + 1 == members) {
+      *sub = 0;
+      if (atom_add_acqrel(&C->bar_top, 1u) + 1 == (unsigned)ng) {
+        C->bar_top = 0;
+        atom_add_acqrel(&C->bar_gen, 1u);
+      }
+    }
+    if (ld_acquire(&C->bar_gen) == g0) {
+      const long long t0 = clock64();
+      while (ld_acquire(&C->bar_gen) == g0) {
+        if (clock64() - t0 > TB_BAR_CYCLES || ctl_status(C) == TB_TIMEOUT) {
           atomicExch(&C->status, TB_TIMEOUT);
           break;
         }
-        if (it > 32) __nanosleep(64);
       }
     }
   }
@@ -449,6 +499,16 @@ struct Items {
   int f1, n1, f2, n;
   __device__ __forceinline__ int box(int i) const { return i < n1 ? f1 + i : f2 + (i - n1); }
 };
+
+// The block's contiguous chunk of n items (item order = box order).
+struct Chunk {
+  int c0, c1;
+};
+__device__ __forceinline__ Chunk chunk_of(int n) {
+  const int G = gridDim.x, ch = (n + G - 1) / G;
+  const int c0 = min(n, (int)blockIdx.x * ch);
+  return Chunk{c0, min(n, c0 + ch)};
+}
 
 // Block-level exclusive scan of one 0/1 flag per thread; returns the
 // thread's exclusive rank and sets *sum to the block total.
@@ -469,42 +529,23 @@ __device__ __forceinline__ int block_excl_scan(int f, int* wsum, int* sum) {
   return pre + in_warp;
 }
 
-// Grid-wide exclusive scan of flag[i] (i < n, flags already stored) in item
-// order: rank[i] = number of flagged items before i.  Returns the total
-// (the same on every block).  Two grid barriers: after the block counts, and
-// at the end, so that every block may read any rank afterwards.
-__device__ int grid_scan(TreeCtl* C, int n, const int* flag, int* rank, int* wsum, int* red) {
-  const int G = gridDim.x, chunk = (n + G - 1) / G;
-  const int c0 = min(n, blockIdx.x * chunk), c1 = min(n, c0 + chunk);
-  int cnt = 0;
-  for (int i = c0 + threadIdx.x; i < c1 + (int)threadIdx.x; i += blockDim.x)
-    cnt += __syncthreads_count(i < c1 && flag[i]);
-  if (threadIdx.x == 0) C->tot[blockIdx.x] = cnt;
-  if (!gbar(C)) return 0;
+// After the barrier that follows the block counts in tot[buf]: the number
+// of flagged items in the chunks before this block's, and in all chunks.
+__device__ void block_prefix(const TreeCtl* C, int buf, int* red, int& pre, int& total) {
   if (threadIdx.x == 0) red[0] = red[1] = 0;
   __syncthreads();
-  int pre = 0, all = 0;
-  for (int q = threadIdx.x; q < G; q += blockDim.x) {
-    const int v = *reinterpret_cast<volatile int*>(&C->tot[q]);
-    if (q < (int)blockIdx.x) pre += v;
-    all += v;
+  int p = 0, a = 0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += blockDim.x) {
+    const int v = C->tot[buf][q];
+    if (q < (int)blockIdx.x) p += v;
+    a += v;
   }
-  atomicAdd(&red[0], pre);
-  atomicAdd(&red[1], all);
+  atomicAdd(&red[0], p);
+  atomicAdd(&red[1], a);
   __syncthreads();
-  int run = red[0];
-  const int total = red[1];
-  for (int i0 = c0; i0 < c1; i0 += blockDim.x) {
-    const int i = i0 + threadIdx.x;
-    const int f = i < c1 ? flag[i] : 0;
-    int s;
-    const int r = block_excl_scan(f, wsum, &s);
-    if (i < c1) rank[i] = run + r;
-    run += s;
-  }
-  // the ranks are read by other blocks (grid-stride loops) after this
-  if (!gbar(C)) return 0;
-  return total;
+  pre = red[0];
+  total = red[1];
+  __syncthreads();
 }
 
 struct TreeKeys {
@@ -512,57 +553,71 @@ struct TreeKeys {
 };
 
 // Renumber the boxes: per level, the level's current range, then its tail
-// [tf, tl] (pts_tree2d.f:1066-1215), through the scratch arrays S.
-__device__ bool reorganize(TreeCtl* C, BoxPtrs& B, BoxPtrs& S, int* map, int nl) {
+// [tf, tl] (pts_tree2d.f:1066-1215).  The permuted arrays are written into
+// the alternate buffers `alt`, which then become current.
+__device__ bool reorganize(TreeCtl* C, BoxPtrs& cur, BoxPtrs& alt, int* map, int nl, int nb,
+                           int* newf) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
-  const int nb = C->nboxes;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    int cur = 0;
+  if (threadIdx.x == 0) {
+    int c = 0;
     for (int l = 0; l <= nl; l++) {
-      C->newf[l] = cur;
-      cur += (C->llast[l] - C->lfirst[l] + 1) + max(C->tl[l] - C->tf[l] + 1, 0);
+      newf[l] = c;
+      c += (C->llast[l] - C->lfirst[l] + 1) + max(C->tl[l] - C->tf[l] + 1, 0);
     }
   }
-  if (!gbar(C)) return false;
+  __syncthreads();
   for (int b = gt; b < nb; b += gs) {
-    const int l = B.level[b];
+    const int l = cur.level[b];
     const int lf = C->lfirst[l], ll = C->llast[l];
-    map[b] = (b >= lf && b <= ll) ? C->newf[l] + (b - lf) : C->newf[l] + (ll - lf + 1) + (b - C->tf[l]);
+    map[b] = (b >= lf && b <= ll) ? newf[l] + (b - lf) : newf[l] + (ll - lf + 1) + (b - C->tf[l]);
   }
   if (!gbar(C)) return false;
   for (int b = gt; b < nb; b += gs) {
     const int m = map[b];
-    S.center[m] = B.center[b];
-    S.level[m] = B.level[b];
-    S.nchild[m] = B.nchild[b];
-    S.iflag[m] = B.iflag[b];
-    const int p = B.parent[b];
-    S.parent[m] = p < 0 ? -1 : map[p];
-    const int4 c = B.child[b];
-    S.child[m] = make_int4(c.x < 0 ? -1 : map[c.x], c.y < 0 ? -1 : map[c.y],
-                           c.z < 0 ? -1 : map[c.z], c.w < 0 ? -1 : map[c.w]);
-  }
-  if (!gbar(C)) return false;
-  for (int b = gt; b < nb; b += gs) {
-    B.center[b] = S.center[b];
-    B.level[b] = S.level[b];
-    B.nchild[b] = S.nchild[b];
-    B.iflag[b] = S.iflag[b];
-    B.parent[b] = S.parent[b];
-    B.child[b] = S.child[b];
+    alt.center[m] = cur.center[b];
+    alt.level[m] = cur.level[b];
+    alt.nchild[m] = cur.nchild[b];
+    alt.iflag[m] = cur.iflag[b];
+    alt.pkey[m] = cur.pkey[b];
+    const int p = cur.parent[b];
+    alt.parent[m] = p < 0 ? -1 : map[p];
+    const int4 c = cur.child[b];
+    alt.child[m] = make_int4(c.x < 0 ? -1 : map[c.x], c.y < 0 ? -1 : map[c.y],
+                             c.z < 0 ? -1 : map[c.z], c.w < 0 ? -1 : map[c.w]);
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     for (int l = 0; l <= nl; l++) {
       const int no = C->llast[l] - C->lfirst[l] + 1, nt = max(C->tl[l] - C->tf[l] + 1, 0);
-      C->lfirst[l] = C->newf[l];
-      C->llast[l] = C->newf[l] + no + nt - 1;
+      C->lfirst[l] = newf[l];
+      C->llast[l] = newf[l] + no + nt - 1;
     }
   }
-  return gbar(C);
+  if (!gbar(C)) return false;
+  // the permuted arrays become current (the others are recomputed later)
+  BoxPtrs t = cur;
+  cur.center = alt.center;
+  cur.level = alt.level;
+  cur.parent = alt.parent;
+  cur.nchild = alt.nchild;
+  cur.child = alt.child;
+  cur.iflag = alt.iflag;
+  cur.pkey = alt.pkey;
+  alt.center = t.center;
+  alt.level = t.level;
+  alt.parent = t.parent;
+  alt.nchild = t.nchild;
+  alt.child = t.child;
+  alt.iflag = t.iflag;
+  alt.pkey = t.pkey;
+  return true;
 }
 
-__device__ bool colleagues_all(TreeCtl* C, BoxPtrs& B, int nl) {
+// Colleagues of all levels, top down; the first level's pass also runs
+// `extra` over all boxes (work that only has to precede the next phase).
+template <class F>
+__device__ bool colleagues_all(TreeCtl* C, BoxPtrs& B, int nl, int nb, F extra) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  for (int b = gt; b < nb; b += gs) extra(b);
   for (int l = 0; l <= nl; l++) {
     const double tol = (double)1.05f * C->bs[l];
     for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs) colleagues(B, b, tol);
@@ -574,27 +629,51 @@ __device__ bool colleagues_all(TreeCtl* C, BoxPtrs& B, int nl) {
 // The whole level-restricted tree on the device: adaptive refinement level by
 // level (pts_tree2d.f:538-755), level restriction (pts_tree2d.f:760-1060,
 // tree_routs2d.f:217-388), renumbering and the point ranges of every box, with
-// the reference's box numbering.  Scratch: flag, rank (cap ints each) and the
-// reorganisation copies S.  Outcome in C->status (TB_OVERFLOW: more than
+// the reference's box numbering.  A refinement step is two phases: every
+// block flags the boxes of its contiguous chunk of the level (and computes
+// colleagues of the level), then after one barrier every block knows the
+// flagged counts of all chunks and creates the children of its own chunk in
+// box order.  Scratch: flag (cap ints; also the renumbering map) and the
+// alternate box arrays S.  Outcome in C->status (TB_OVERFLOW: more than
 // C->cap boxes; TB_DEEP: levels beyond 32 need the 51-level keys).
-__global__ void __launch_bounds__(256, 2)
-    k_tree_build(BoxPtrs B, BoxPtrs S, TreeCtl* C, int* flag, int* rank, TreeKeys K,
+__global__ void __launch_bounds__(TB_THREADS, 1)
+    k_tree_build(BoxPtrs B, BoxPtrs S, TreeCtl* C, int* flag, TreeKeys K, int ns, int nt,
                  int idivflag, int ndiv, int nlmax, int deep) {
   __shared__ int wsum[32];
   __shared__ int red[2];
+  __shared__ int newf[NLMAX + 2];
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   const int cap = C->cap;
+  BoxPtrs cur = B, alt = S;
+  int buf = 0;  // tot[] buffer of the next scan
   // A zero-size root (all points coincide) cannot be subdivided: the
   // children would coincide with it forever.  Keep the root as the only box.
   if (C->bs[0] == 0.0) nlmax = 0;
   // --- adaptive refinement ---------------------------------------------
-  int lev = 0;
-  for (; lev < nlmax; lev++) {
-    const int f = C->lfirst[lev], n = C->llast[lev] - f + 1, nb = C->nboxes;
-    for (int i = gt; i < n; i += gs) flag[i] = refine_flag(B, f + i, idivflag, ndiv);
+  int f = 0, n = 1, nb = 1, lev = 0;
+  for (;; lev++) {
+    // phase A: colleagues of the level, refine flags and counts of own chunk
+    if (lev >= 1) {
+      const double tol = (double)1.05f * C->bs[lev];
+      for (int b = f + gt; b < f + n; b += gs) colleagues(cur, b, tol);
+    }
+    const bool more = lev < nlmax;
+    const Chunk ch = chunk_of(n);
+    int cnt = 0;
+    if (more)
+      for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const int fl = i < ch.c1 ? refine_flag(cur, f + i, idivflag, ndiv) : 0;
+        if (i < ch.c1) flag[i] = fl;
+        cnt += __syncthreads_count(fl);
+      }
+    if (threadIdx.x == 0) C->tot[buf][blockIdx.x] = cnt;
     if (!gbar(C)) return;
-    const int tot = grid_scan(C, n, flag, rank, wsum, red);
-    if (ctl_status(C) == TB_TIMEOUT) return;
+    if (!more) break;
+    // phase B: children of the flagged boxes of own chunk, in box order
+    int pre, tot;
+    block_prefix(C, buf, red, pre, tot);
+    buf ^= 1;
     if (tot == 0) break;
     if (lev + 1 > 32 && !deep) {
       if (gt == 0) C->status = TB_DEEP;
@@ -605,22 +684,27 @@ __global__ void __launch_bounds__(256, 2)
       return;
     }
     const double bsc = C->bs[lev] / 2;
-    for (int i = gt; i < n; i += gs) {
-      if (!flag[i]) continue;
-      const int b = f + i, base = nb + 4 * rank[i];
-      create_children(B, b, base, bsc, lev + 1, 0);
-      split_children(B, b, lev + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
+    int run = pre;
+    for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
+      const int i = i0 + threadIdx.x;
+      const int fl = i < ch.c1 ? flag[i] : 0;
+      int s;
+      const int r = block_excl_scan(fl, wsum, &s);
+      if (fl) {
+        create_children(cur, f + i, nb + 4 * (run + r), bsc, lev + 1, 0);
+        split_children(cur, f + i, lev + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
+      }
+      run += s;
     }
-    if (!gbar(C)) return;
     if (gt == 0) {
       C->bs[lev + 1] = bsc;
       C->lfirst[lev + 1] = nb;
       C->llast[lev + 1] = nb + 4 * tot - 1;
       C->nboxes = nb + 4 * tot;
     }
-    if (!gbar(C)) return;
-    const double tol = (double)1.05f * bsc;
-    for (int b = C->lfirst[lev + 1] + gt; b <= C->llast[lev + 1]; b += gs) colleagues(B, b, tol);
+    f = nb;
+    n = 4 * tot;
+    nb += 4 * tot;
     if (!gbar(C)) return;
   }
   const int nl = lev;
@@ -630,104 +714,153 @@ __global__ void __launch_bounds__(256, 2)
   }
   if (nl >= 2) {
     // --- level restriction ---------------------------------------------
-    // pass 1: flag (levels >= 2, one pass)
-    for (int b = C->lfirst[2] + gt; b < C->nboxes; b += gs) {
-      const int l = B.level[b];
-      flag_pass(B, b, 1.05 * (C->bs[l - 1] + C->bs[l - 2]) / 2.0);
+    // pass 1: flag (levels >= 2, one pass); zero the per-level counts and tails
+    if (gt == 0)
+      for (int l = 0; l <= nl; l++) {
+        C->lcnt[l] = 0;
+        C->tf[l] = 0;
+        C->tl[l] = -1;
+      }
+    for (int b = C->lfirst[2] + gt; b < nb; b += gs) {
+      const int l = cur.level[b];
+      flag_pass(cur, b, 1.05 * (C->bs[l - 1] + C->bs[l - 2]) / 2.0);
     }
     if (!gbar(C)) return;
     // pass 2: flag+, finest level first
     for (int l = nl; l >= 1; l--) {
       const double dt = 1.05 * (C->bs[l] + C->bs[l - 1]) / 2.0;
-      for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs) flagplus(B, b, dt);
+      for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs) flagplus(cur, b, dt);
       if (!gbar(C)) return;
     }
-    if (gt == 0)
-      for (int l = 0; l <= nl; l++) {
-        C->tf[l] = 0;
-        C->tl[l] = -1;
-      }
     // subdivide the flag and flag+ boxes of levels 1..nl-2
     if (nl - 2 >= 1) {
-      const int f = C->lfirst[1], n = C->llast[nl - 2] - f + 1, nb = C->nboxes;
-      for (int i = gt; i < n; i += gs) flag[i] = B.iflag[f + i] > 0 ? 1 : 0;
+      const int f1 = C->lfirst[1], n1 = C->llast[nl - 2] - f1 + 1;
+      const Chunk ch = chunk_of(n1);
+      int cnt = 0;
+      for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const int fl = i < ch.c1 ? (cur.iflag[f1 + i] > 0 ? 1 : 0) : 0;
+        if (i < ch.c1) flag[i] = fl;
+        if (fl) atomicAdd(&C->lcnt[cur.level[f1 + i]], 1);
+        cnt += __syncthreads_count(fl);
+      }
+      if (threadIdx.x == 0) C->tot[buf][blockIdx.x] = cnt;
       if (!gbar(C)) return;
-      const int tot = grid_scan(C, n, flag, rank, wsum, red);
-      if (ctl_status(C) == TB_TIMEOUT) return;
+      int pre, tot;
+      block_prefix(C, buf, red, pre, tot);
+      buf ^= 1;
       if (tot > 0) {
         if (nb + 4 * tot > cap) {
           if (gt == 0) C->status = TB_OVERFLOW;
           return;
         }
-        for (int i = gt; i < n; i += gs) {
-          if (!flag[i]) continue;
-          const int b = f + i, lc = B.level[b] + 1;
-          create_children(B, b, nb + 4 * rank[i], C->bs[lc], lc, B.iflag[b] == 1 ? 3 : 0);
+        int run = pre;
+        for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
+          const int i = i0 + threadIdx.x;
+          const int fl = i < ch.c1 ? flag[i] : 0;
+          int s;
+          const int r = block_excl_scan(fl, wsum, &s);
+          if (fl) {
+            const int b = f1 + i, lc = cur.level[b] + 1;
+            create_children(cur, b, nb + 4 * (run + r), C->bs[lc], lc, cur.iflag[b] == 1 ? 3 : 0);
+          }
+          run += s;
         }
-        if (!gbar(C)) return;
         if (gt == 0) {
           int base = nb;
           for (int l = 1; l <= nl - 2; l++) {
-            const int a = C->lfirst[l] - f, e = C->llast[l] - f;
-            const int c = rank[e] + flag[e] - rank[a];
+            const int c = C->lcnt[l];
             C->tf[l + 1] = base;
             C->tl[l + 1] = base + 4 * c - 1;
             base += 4 * c;
           }
           C->nboxes = nb + 4 * tot;
         }
+        nb += 4 * tot;
         if (!gbar(C)) return;
       }
     }
-    if (!reorganize(C, B, S, rank, nl)) return;
-    if (!colleagues_all(C, B, nl)) return;
-    for (int b = gt; b < C->nboxes; b += gs)
-      if (B.iflag[b] != 3) B.iflag[b] = 0;
-    if (gt == 0)
-      for (int l = 0; l <= nl; l++) {
-        C->tf[l] = 0;
-        C->tl[l] = -1;
+    if (!reorganize(C, cur, alt, flag, nl, nb, newf)) return;
+    // colleagues of the renumbered tree; flag++ boxes keep their flag (3),
+    // all others are cleared; the tails are cleared for pass 3
+    auto keep3 = [&](int b) {
+      if (cur.iflag[b] != 3) cur.iflag[b] = 0;
+      if (b <= nl) {
+        C->tf[b] = 0;
+        C->tl[b] = -1;
       }
-    if (!gbar(C)) return;
-    // pass 3: flag++ boxes, coarsest level first, refining as needed
+    };
+    if (!colleagues_all(C, cur, nl, nb, keep3)) return;
+    // pass 3: flag++ boxes, coarsest level first, refining as needed; the
+    // colleagues of a level's new boxes (its tail) are computed in the same
+    // phase as the level's flags, by the thread that then flags the box
     for (int l = 2; l <= nl - 2; l++) {
-      const Items it{C->lfirst[l], C->llast[l] - C->lfirst[l] + 1, C->tf[l],
-                     (C->llast[l] - C->lfirst[l] + 1) + max(C->tl[l] - C->tf[l] + 1, 0)};
-      const int nb = C->nboxes;
+      const int lf = C->lfirst[l], n1 = C->llast[l] - lf + 1, tf = C->tf[l];
+      const Items it{lf, n1, tf, n1 + max(C->tl[l] - tf + 1, 0)};
       const double dt = 1.05 * (C->bs[l] + C->bs[l + 1]) / 2.0;
-      for (int i = gt; i < it.n; i += gs) flag[i] = update_flag(B, it.box(i), dt);
+      const double ctol = (double)1.05f * C->bs[l];
+      const Chunk ch = chunk_of(it.n);
+      int cnt = 0;
+      for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        int fl = 0;
+        if (i < ch.c1) {
+          const int b = it.box(i);
+          if (i >= n1) colleagues(cur, b, ctol);
+          fl = update_flag(cur, b, dt);
+          flag[i] = fl;
+        }
+        cnt += __syncthreads_count(fl);
+      }
+      if (threadIdx.x == 0) C->tot[buf][blockIdx.x] = cnt;
       if (!gbar(C)) return;
-      const int tot = grid_scan(C, it.n, flag, rank, wsum, red);
-      if (ctl_status(C) == TB_TIMEOUT) return;
+      int pre, tot;
+      block_prefix(C, buf, red, pre, tot);
+      buf ^= 1;
       if (tot == 0) continue;
       if (nb + 4 * tot > cap) {
         if (gt == 0) C->status = TB_OVERFLOW;
         return;
       }
-      for (int i = gt; i < it.n; i += gs) {
-        if (!flag[i]) continue;
-        const int b = it.box(i), lc = B.level[b] + 1;
-        create_children(B, b, nb + 4 * rank[i], C->bs[lc], lc, B.iflag[b] == 1 ? 3 : 0);
+      int run = pre;
+      for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
+        const int i = i0 + threadIdx.x;
+        const int fl = i < ch.c1 ? flag[i] : 0;
+        int s;
+        const int r = block_excl_scan(fl, wsum, &s);
+        if (fl) {
+          const int b = it.box(i), lc = cur.level[b] + 1;
+          create_children(cur, b, nb + 4 * (run + r), C->bs[lc], lc, cur.iflag[b] == 1 ? 3 : 0);
+        }
+        run += s;
       }
-      if (!gbar(C)) return;
       if (gt == 0) {
         C->tf[l + 1] = nb;
         C->tl[l + 1] = nb + 4 * tot - 1;
         C->nboxes = nb + 4 * tot;
       }
-      if (!gbar(C)) return;
-      const double tol = (double)1.05f * C->bs[l + 1];
-      for (int b = C->tf[l + 1] + gt; b <= C->tl[l + 1]; b += gs) colleagues(B, b, tol);
+      nb += 4 * tot;
       if (!gbar(C)) return;
     }
-    if (!reorganize(C, B, S, rank, nl)) return;
-    if (!colleagues_all(C, B, nl)) return;
+    if (!reorganize(C, cur, alt, flag, nl, nb, newf)) return;
+    if (!colleagues_all(C, cur, nl, nb, [](int) {})) return;
   }
   // --- point ranges of every box of the final tree ----------------------
-  for (int l = 0; l < nl; l++) {
-    for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs)
-      if (B.nchild[b] != 0) split_children(B, b, l + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
-    if (!gbar(C)) return;
+  if (nl <= 32) {
+    // a box's points are the keys with its path as prefix (one pass)
+    for (int b = gt + 1; b < nb; b += gs) {
+      const int l = cur.level[b];
+      int2 rs, rt;
+      prefix_ranges(K.skhi, ns, K.tkhi, nt, cur.pkey[b], l, rs, rt);
+      cur.srng[b] = rs;
+      cur.trng[b] = rt;
+    }
+  } else {
+    for (int l = 0; l < nl; l++) {
+      for (int b = C->lfirst[l] + gt; b <= C->llast[l]; b += gs)
+        if (cur.nchild[b] != 0) split_children(cur, b, l + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
+      if (!gbar(C)) return;
+    }
   }
 }
 
@@ -866,7 +999,7 @@ int tree_grid() {
     B2_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     B2_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     if (!coop) throw CudaError("tree build: cooperative launch not supported", IER_CUDA);
-    B2_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_build, 256, 0));
+    B2_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_tree_build, TB_THREADS, 0));
     grid[dev] = std::max(1, std::min(per * nsm, TB_MAXG));
   }
   return grid[dev];
@@ -906,8 +1039,9 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   for (;;) {
     alloc_boxes(T, cap);
     DBuf<double2> sc(st);
-    DBuf<int> sl(st), sp(st), sn(st), sf(st), flag(st), rank(st);
+    DBuf<int> sl(st), sp(st), sn(st), sf(st), flag(st);
     DBuf<int4> sch(st);
+    DBuf<uint64_t> pk1(st), pk2(st);
     sc.alloc(cap, st);
     sl.alloc(cap, st);
     sp.alloc(cap, st);
@@ -915,19 +1049,21 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
     sf.alloc(cap, st);
     sch.alloc(cap, st);
     flag.alloc(cap, st);
-    rank.alloc(cap, st);
+    pk1.alloc(cap, st);
+    pk2.alloc(cap, st);
     BoxPtrs B = ptrs(T);
-    BoxPtrs S{sc.p, sl.p, sp.p, sn.p, sch.p, sf.p, nullptr, nullptr, nullptr, nullptr};
+    B.pkey = pk1.p;
+    BoxPtrs S{sc.p, sl.p, sp.p, sn.p, sch.p, sf.p, pk2.p, nullptr, nullptr, nullptr, nullptr};
     k_init_root<<<1, 1, 0, st>>>(B, T.root.p, (int)ns, (int)nt, ctl.p, cap);
     B2_LAUNCH_CHECK();
     TreeKeys K{T.skhi.p, T.sklo.p, T.tkhi.p, T.tklo.p};
     TreeCtl* C = ctl.p;
     int* fp = flag.p;
-    int* rp = rank.p;
+    int nsi = (int)ns, nti = (int)nt;
     int deep = T.deep_sorted ? 1 : 0;
-    void* args[] = {&B, &S, &C, &fp, &rp, &K, &idivflag, &ndiv, &nlmax, &deep};
-    B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(256), args, 0,
-                                         st));
+    void* args[] = {&B, &S, &C, &fp, &K, &nsi, &nti, &idivflag, &ndiv, &nlmax, &deep};
+    B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(TB_THREADS),
+                                         args, 0, st));
     B2_CHECK(cudaMemcpyAsync(hc, ctl.p, sizeof(TreeCtl), cudaMemcpyDeviceToHost, st));
     B2_CHECK(cudaStreamSynchronize(st));
     if (hc->status == TB_DEEP && !T.deep_sorted) {
