@@ -190,6 +190,9 @@ __global__ void __launch_bounds__(64) k_p2m(TV t, int first, int n, const double
 // step 3: M2M (laprouts2d.f:905-1015) from the children with sources.
 // z0 = child - parent; t_j = h_j (r1/z0)^j;
 // H_0 = t_0, H_i = (-t_0/i + sum_{j=1..i} t_j C(i-1, j-1)) (z0/r2)^i
+// One warp per parent: the lanes first stage t for all four children at
+// once (lane = (child, j)), so the children's loads overlap, then each lane
+// sums its coefficients over the children.
 // ---------------------------------------------------------------------------
 template <int ND>
 __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
@@ -197,69 +200,71 @@ __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
                                              double2* __restrict__ mp) {
   extern __shared__ double2 smem[];
   WARP_LOOP(n) {
-    double2* T = smem + (size_t)wib * P * ND;
+    // per warp: t[child][j][density] (zero for children without sources),
+    // then z0 / r2 of each child
+    double2* T = smem + (size_t)wib * (4 * P * ND + 4);
+    double2* W2 = T + 4 * P * ND;
     int b = first + bi;
     if (t.nchild[b] == 0) continue;
     int lev = t.level[b];
     double r2 = t.boxsize[lev], r1 = t.boxsize[lev + 1];
     double2 c2 = t.center[b];
-    double2 acc[2][ND];
-#pragma unroll
-    for (int s = 0; s < 2; s++)
-#pragma unroll
-      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
     int4 ch = t.child[b];
-    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
-    for (int q = 0; q < 4; q++) {
-      int k = cc[q];
-      if (t.srng[k].y <= t.srng[k].x) continue;
-      double2 c1 = t.center[k];
-      double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
-      double2 w1 = crcp(make_double2(z0.x / r1, z0.y / r1));
-      double2 w2 = make_double2(z0.x / r2, z0.y / r2);
-      __syncwarp();
-#pragma unroll
-      for (int s = 0; s < 2; s++) {
-        int j = lane + 32 * s;
-        if (j >= P) break;
-        double2 a = cpow_int(w1, j);
-#pragma unroll
-        for (int d = 0; d < ND; d++) T[j * ND + d] = cmul(mp[((size_t)k * P + j) * ND + d], a);
+    __syncwarp();
+    for (int e = lane; e < 4 * P; e += 32) {
+      const int c = e / P, j = e % P;
+      const int k = c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
+      const bool has = t.srng[k].y > t.srng[k].x;
+      double2 a = make_double2(0, 0);
+      if (has) {
+        double2 c1 = t.center[k];
+        double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
+        double2 w1 = crcp(make_double2(z0.x / r1, z0.y / r1));
+        a = cpow_int(w1, j);
+        if (j == 0) W2[c] = make_double2(z0.x / r2, z0.y / r2);
+      } else if (j == 0) {
+        W2[c] = make_double2(0, 0);
       }
-      __syncwarp();
 #pragma unroll
-      for (int s = 0; s < 2; s++) {
-        int i = lane + 32 * s;
-        if (i >= P) break;
+      for (int d = 0; d < ND; d++)
+        T[(c * P + j) * ND + d] = has ? cmul(mp[((size_t)k * P + j) * ND + d], a) : make_double2(0, 0);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < 2; s++) {
+      int i = lane + 32 * s;
+      if (i >= P) break;
+      double2 acc[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) acc[d] = make_double2(0, 0);
+      const double* crow = binom + (size_t)(i > 0 ? i - 1 : 0) * BINOM_N;
+      for (int c = 0; c < 4; c++) {
         if (i == 0) {
 #pragma unroll
-          for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], T[d]);
+          for (int d = 0; d < ND; d++) acc[d] = cadd(acc[d], T[c * P * ND + d]);
           continue;
         }
+        const double2 w2 = W2[c];
+        if (w2.x == 0.0 && w2.y == 0.0) continue;  // child without sources
+        const double2* tc = T + (size_t)c * P * ND;
         double2 v[ND];
 #pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = make_double2(-T[d].x / i, -T[d].y / i);
-        const double* crow = binom + (size_t)(i - 1) * BINOM_N;
+        for (int d = 0; d < ND; d++) v[d] = make_double2(-tc[d].x / i, -tc[d].y / i);
         for (int j = 1; j <= i; j++) {
           double cb = crow[j - 1];
 #pragma unroll
           for (int d = 0; d < ND; d++) {
-            double2 tj = T[j * ND + d];
+            double2 tj = tc[j * ND + d];
             v[d].x += tj.x * cb;
             v[d].y += tj.y * cb;
           }
         }
         double2 bi_ = cpow_int(w2, i);
 #pragma unroll
-        for (int d = 0; d < ND; d++) cfma(acc[s][d], v[d], bi_);
+        for (int d = 0; d < ND; d++) cfma(acc[d], v[d], bi_);
       }
-    }
 #pragma unroll
-    for (int s = 0; s < 2; s++) {
-      int i = lane + 32 * s;
-      if (i >= P) break;
-#pragma unroll
-      for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = acc[s][d];
+      for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = acc[d];
     }
   }
 }
@@ -472,6 +477,8 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
 // ---------------------------------------------------------------------------
 // step 5: L2L (laprouts2d.f:1020-1123), z0 = child - parent:
 // t_j = l_j (z0/r1)^j, L_i += (sum_{j>=i} t_j C(j, i)) (r2/z0)^i
+// One warp per parent: lanes stage t for all four children at once (lane =
+// (child, j)), then each lane produces one (child, i) coefficient.
 // ---------------------------------------------------------------------------
 template <int ND>
 __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int P,
@@ -479,54 +486,51 @@ __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int P,
                                              double2* __restrict__ lo) {
   extern __shared__ double2 smem[];
   WARP_LOOP(n) {
-    double2* T = smem + (size_t)wib * P * ND;
+    // per warp: t[child][j][density], then r2 / z0 of each child
+    double2* T = smem + (size_t)wib * (4 * P * ND + 4);
+    double2* W2 = T + 4 * P * ND;
     int b = first + bi;
     if (t.nchild[b] == 0 || !t.has_eval_pts(b)) continue;
     int lev = t.level[b];
     double r1 = t.boxsize[lev], r2 = t.boxsize[lev + 1];
     double2 c1 = t.center[b];
     int4 ch = t.child[b];
-    int cc[4] = {ch.x, ch.y, ch.z, ch.w};
-    for (int q = 0; q < 4; q++) {
-      int k = cc[q];
+    __syncwarp();
+    for (int e = lane; e < 4 * P; e += 32) {
+      const int c = e / P, j = e % P;
+      const int k = c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
       double2 ck = t.center[k];
       double2 z0 = make_double2(ck.x - c1.x, ck.y - c1.y);
       double2 w1 = make_double2(z0.x / r1, z0.y / r1);
-      double2 w2 = crcp(make_double2(z0.x / r2, z0.y / r2));
-      __syncwarp();
+      if (j == 0) W2[c] = crcp(make_double2(z0.x / r2, z0.y / r2));
+      double2 a = cpow_int(w1, j);
 #pragma unroll
-      for (int s = 0; s < 2; s++) {
-        int j = lane + 32 * s;
-        if (j >= P) break;
-        double2 a = cpow_int(w1, j);
+      for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(lo[((size_t)b * P + j) * ND + d], a);
+    }
+    __syncwarp();
+    for (int e = lane; e < 4 * P; e += 32) {
+      const int c = e / P, i = e % P;
+      const int k = c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
+      double2 v[ND];
 #pragma unroll
-        for (int d = 0; d < ND; d++) T[j * ND + d] = cmul(lo[((size_t)b * P + j) * ND + d], a);
-      }
-      __syncwarp();
-#pragma unroll
-      for (int s = 0; s < 2; s++) {
-        int i = lane + 32 * s;
-        if (i >= P) break;
-        double2 v[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
-        for (int j = i; j < P; j++) {
-          double cb = binom[(size_t)j * BINOM_N + i];
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            double2 tj = T[j * ND + d];
-            v[d].x += tj.x * cb;
-            v[d].y += tj.y * cb;
-          }
-        }
-        double2 bi_ = cpow_int(w2, i);
+      for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
+      const double2* tc = T + (size_t)c * P * ND;
+      for (int j = i; j < P; j++) {
+        double cb = binom[(size_t)j * BINOM_N + i];
 #pragma unroll
         for (int d = 0; d < ND; d++) {
-          size_t o = ((size_t)k * P + i) * ND + d;
-          double2 cur = lo[o];
-          cfma(cur, v[d], bi_);
-          lo[o] = cur;
+          double2 tj = tc[j * ND + d];
+          v[d].x += tj.x * cb;
+          v[d].y += tj.y * cb;
         }
+      }
+      double2 bi_ = cpow_int(W2[c], i);
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        size_t o = ((size_t)k * P + i) * ND + d;
+        double2 cur = lo[o];
+        cfma(cur, v[d], bi_);
+        lo[o] = cur;
       }
     }
   }
@@ -873,10 +877,12 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, 0, nb, xs, D, P, mp);
   B2_LAUNCH_CHECK();
   B2_CHECK(cudaEventRecord(ev[1], st));
-  size_t sm_t = sizeof(double2) * 4 * P * ND;
+  const size_t sm_m2m = sizeof(double2) * (4 * (size_t)P * ND + 4) * 4, sm_l2l = sm_m2m;
+  set_smem_attr(k_m2m<ND>, sm_m2m);
+  set_smem_attr(k_l2l<ND>, sm_l2l);
   for (int l = nl - 1; l >= 1; l--) {
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    k_m2m<ND><<<warp_grid(n, 4), 128, sm_t, st>>>(tv, f, n, P, binom, mp);
+    k_m2m<ND><<<warp_grid(n, 4), 128, sm_m2m, st>>>(tv, f, n, P, binom, mp);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[2], st));
@@ -901,7 +907,7 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   B2_CHECK(cudaEventRecord(ev[4], st));
   for (int l = 1; l <= nl - 1; l++) {
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    k_l2l<ND><<<warp_grid(n, 4), 128, sm_t, st>>>(tv, f, n, P, binom, lo);
+    k_l2l<ND><<<warp_grid(n, 4), 128, sm_l2l, st>>>(tv, f, n, P, binom, lo);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[5], st));
