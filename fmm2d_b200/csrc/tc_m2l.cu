@@ -131,6 +131,39 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   }
 }
 
+// Non-blocking test of a barrier phase.
+__device__ __forceinline__ bool mbar_test(uint32_t mbar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// The same bounded wait for threads that are usually early (the row builders
+// run stages ahead of the tensor cores): each failed try backs off, so the
+// waiting warps leave the issue slots to the MMA-issuing thread.
+__device__ __forceinline__ bool mbar_wait_backoff(uint32_t mbar, uint32_t parity) {
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > TC_WAIT_CYCLES) return false;
+    __nanosleep(256);
+  }
+}
+
 __device__ __forceinline__ void tc_fence_before() {
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -417,7 +450,7 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         }
         const int s = (int)(g % OT_STAGES);
         if (g >= OT_STAGES && !*s_fail) {
-          if (!mbar_wait(empty0 + 8 * s, (g / OT_STAGES - 1) & 1)) *s_fail = 1;
+          if (!mbar_wait_backoff(empty0 + 8 * s, (g / OT_STAGES - 1) & 1)) *s_fail = 1;
           tc_fence_after();
         }
         // coefficient k = 4 part + j, so k = j (mod 4): input phase i^(-m j)
@@ -470,40 +503,56 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         if (lane == 0) mbar_arrive(full0 + 8 * pend);
       }
     } else if (lane == 0) {
-      // MMA issuer
+      // MMA issuer.  After the blocking wait for the next stage it also takes
+      // the following stages that are already full, so that one tcgen05 fence
+      // covers several steps (the fence costs a few hundred clocks), and it
+      // reads the next step's class ahead of time.
       const uint32_t idesc = idesc_tf32(TC_ROWS, N);
       unsigned touched = 0;
+      bool fail = *s_fail != 0;
       unsigned long long mm = mask;
-      while (mm) {
-        const int oi = __ffsll((long long)mm) - 1;
-        mm &= mm - 1;
-        const int s = (int)(g % OT_STAGES);
-        if (!*s_fail && !mbar_wait(full0 + 8 * s, (g / OT_STAGES) & 1)) *s_fail = 1;
-        tc_fence_after();
-        const int cl = CLS[oi];
-        if (cl == 255) *s_fail = 1;  // not an interaction offset: its MMA is not issued
-        if (!*s_fail) {
-          const int m = cl & 3;
-          const uint32_t a_hi = taddr + L::A_COL + (uint32_t)(s * 2 * K), a_lo = a_hi + K;
-          // descriptors of the matrix's hi and lo tiles; a K step of 8 columns
-          // advances the start address by 256 bytes (16 in descriptor units)
-          const uint64_t bh = umma_desc(sbase + L::B0 + (uint32_t)(cl >> 2) * 2 * L::SB, 128,
-                                        (uint32_t)K * 32);
-          const uint64_t bl = bh + (L::SB >> 4);
-          const uint32_t dt = taddr + (uint32_t)(m * N);
-          const uint32_t acc0 = ((touched >> m) & 1u) ? 1u : 0u;
-#pragma unroll
-          for (int ks = 0; ks < K / 8; ks++) {
-            umma_tf32_ts(dt, a_hi + 8 * ks, bh + 16 * ks, idesc, ks == 0 ? acc0 : 1u);
-            umma_tf32_ts(dt, a_hi + 8 * ks, bl + 16 * ks, idesc, 1u);
-            umma_tf32_ts(dt, a_lo + 8 * ks, bh + 16 * ks, idesc, 1u);
-          }
-          touched |= 1u << m;
+      int cl_next = mm ? CLS[__ffsll((long long)mm) - 1] : 255;
+      uint32_t left = nsteps;
+      while (left > 0) {
+        if (!fail && !mbar_wait(full0 + 8 * (g % OT_STAGES), (g / OT_STAGES) & 1)) fail = true;
+        uint32_t ready = 1;
+        while (!fail && ready < left && ready < OT_STAGES) {
+          const uint32_t gn = g + ready;
+          if (!mbar_test(full0 + 8 * (gn % OT_STAGES), (gn / OT_STAGES) & 1)) break;
+          ++ready;
         }
-        // the commit also releases the stage when nothing was issued
-        umma_commit(empty0 + 8 * s);
-        ++g;
+        tc_fence_after();
+        for (uint32_t q = 0; q < ready; q++) {
+          mm &= mm - 1;
+          const int cl = cl_next;
+          cl_next = mm ? CLS[__ffsll((long long)mm) - 1] : 255;
+          const int s = (int)(g % OT_STAGES);
+          if (cl == 255) fail = true;  // not an interaction offset: its MMA is not issued
+          if (!fail) {
+            const int m = cl & 3;
+            const uint32_t a_hi = taddr + L::A_COL + (uint32_t)(s * 2 * K), a_lo = a_hi + K;
+            // descriptors of the matrix's hi and lo tiles; a K step of 8 columns
+            // advances the start address by 256 bytes (16 in descriptor units)
+            const uint64_t bh = umma_desc(sbase + L::B0 + (uint32_t)(cl >> 2) * 2 * L::SB, 128,
+                                          (uint32_t)K * 32);
+            const uint64_t bl = bh + (L::SB >> 4);
+            const uint32_t dt = taddr + (uint32_t)(m * N);
+            const uint32_t acc0 = ((touched >> m) & 1u) ? 1u : 0u;
+#pragma unroll
+            for (int ks = 0; ks < K / 8; ks++) {
+              umma_tf32_ts(dt, a_hi + 8 * ks, bh + 16 * ks, idesc, ks == 0 ? acc0 : 1u);
+              umma_tf32_ts(dt, a_hi + 8 * ks, bl + 16 * ks, idesc, 1u);
+              umma_tf32_ts(dt, a_lo + 8 * ks, bh + 16 * ks, idesc, 1u);
+            }
+            touched |= 1u << m;
+          }
+          // the commit also releases the stage when nothing was issued
+          umma_commit(empty0 + 8 * s);
+          ++g;
+        }
+        left -= ready;
       }
+      if (fail) *s_fail = 1;
     }
     g = g0 + nsteps;
     // rotation classes present in the tile (the same on every thread)
