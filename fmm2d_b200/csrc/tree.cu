@@ -612,6 +612,113 @@ __device__ bool reorganize(TreeCtl* C, BoxPtrs& cur, BoxPtrs& alt, int* map, int
   return true;
 }
 
+// Colleagues through a hash table of (level, path key) -> box.  The
+// colleagues of a box are the existing boxes of its level in its 3x3
+// neighbourhood; the reference collects them from the children of the
+// parent's colleagues (tree_routs2d.f:160-206), parent colleagues in their
+// own order and children in child order, which is the order of the path
+// keys (Morton order), so the neighbours are sorted by key.  Paths of at
+// most 31 levels fit the 64-bit table key (a sentinel bit above the path).
+struct BoxHash {
+  unsigned long long* key;  // 0 = empty
+  int* box;
+  unsigned mask;            // capacity - 1 (power of two)
+};
+
+__device__ __forceinline__ unsigned long long hash_key(int lev, uint64_t pk) {
+  return (1ull << (2 * lev)) | pk;
+}
+__device__ __forceinline__ unsigned hash_slot(unsigned long long k, unsigned mask) {
+  return (unsigned)((k * 0x9E3779B97F4A7C15ull) >> 32) & mask;
+}
+__device__ __forceinline__ uint64_t spread_bits(uint32_t x) {
+  uint64_t v = x;
+  v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+  v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+  v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+  v = (v | (v << 2)) & 0x3333333333333333ull;
+  v = (v | (v << 1)) & 0x5555555555555555ull;
+  return v;
+}
+__device__ __forceinline__ uint32_t compact_bits(uint64_t v) {
+  v &= 0x5555555555555555ull;
+  v = (v | (v >> 1)) & 0x3333333333333333ull;
+  v = (v | (v >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+  v = (v | (v >> 4)) & 0x00FF00FF00FF00FFull;
+  v = (v | (v >> 8)) & 0x0000FFFF0000FFFFull;
+  v = (v | (v >> 16)) & 0x00000000FFFFFFFFull;
+  return (uint32_t)v;
+}
+
+__device__ void hash_insert(const BoxHash& H, unsigned long long k, int b) {
+  unsigned h = hash_slot(k, H.mask);
+  for (unsigned it = 0; it <= H.mask; it++) {
+    const unsigned long long prev = atomicCAS(&H.key[h], 0ull, k);
+    if (prev == 0ull || prev == k) {
+      H.box[h] = b;
+      return;
+    }
+    h = (h + 1) & H.mask;
+  }
+}
+
+__device__ int hash_find(const BoxHash& H, unsigned long long k) {
+  unsigned h = hash_slot(k, H.mask);
+  for (unsigned it = 0; it <= H.mask; it++) {
+    const unsigned long long v = H.key[h];
+    if (v == k) return H.box[h];
+    if (v == 0ull) return -1;
+    h = (h + 1) & H.mask;
+  }
+  return -1;
+}
+
+// Colleagues of every box of the current tree (levels <= 31): clear the
+// table, insert every box, look up the 3x3 neighbourhoods; three phases.
+// `extra` runs over all boxes in the first phase.
+template <class F>
+__device__ bool colleagues_hashed(TreeCtl* C, BoxPtrs& B, const BoxHash& H, int nb, F extra) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
+  for (unsigned h = gt; h <= H.mask; h += gs) H.key[h] = 0ull;
+  for (int b = gt; b < nb; b += gs) extra(b);
+  if (!gbar(C)) return false;
+  for (int b = gt; b < nb; b += gs) hash_insert(H, hash_key(B.level[b], B.pkey[b]), b);
+  if (!gbar(C)) return false;
+  for (int b = gt; b < nb; b += gs) {
+    int* cl = B.coll + 9 * (size_t)b;
+    const int l = B.level[b];
+    if (l == 0) {
+      cl[0] = b;
+      for (int q = 1; q < 9; q++) cl[q] = -1;
+      B.ncoll[b] = 1;
+      continue;
+    }
+    const uint64_t pk = B.pkey[b];
+    const long ix = compact_bits(pk), iy = compact_bits(pk >> 1), side = 1L << l;
+    uint64_t fk[9];
+    int fb[9], cnt = 0;
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        const long x = ix + dx, y = iy + dy;
+        if (x < 0 || y < 0 || x >= side || y >= side) continue;
+        const uint64_t nk = (spread_bits((uint32_t)y) << 1) | spread_bits((uint32_t)x);
+        const int nbx = (dx == 0 && dy == 0) ? b : hash_find(H, hash_key(l, nk));
+        if (nbx < 0) continue;
+        int q = cnt++;
+        while (q > 0 && fk[q - 1] > nk) {
+          fk[q] = fk[q - 1];
+          fb[q] = fb[q - 1];
+          q--;
+        }
+        fk[q] = nk;
+        fb[q] = nbx;
+      }
+    for (int q = 0; q < 9; q++) cl[q] = q < cnt ? fb[q] : -1;
+    B.ncoll[b] = cnt;
+  }
+  return gbar(C);
+}
+
 // Colleagues of all levels, top down; the first level's pass also runs
 // `extra` over all boxes (work that only has to precede the next phase).
 template <class F>
@@ -630,15 +737,15 @@ __device__ bool colleagues_all(TreeCtl* C, BoxPtrs& B, int nl, int nb, F extra) 
 // level (pts_tree2d.f:538-755), level restriction (pts_tree2d.f:760-1060,
 // tree_routs2d.f:217-388), renumbering and the point ranges of every box, with
 // the reference's box numbering.  A refinement step is two phases: every
-// block flags the boxes of its contiguous chunk of the level (and computes
-// colleagues of the level), then after one barrier every block knows the
+// block flags the boxes of its contiguous chunk of the level, then after one
+// barrier every block knows the
 // flagged counts of all chunks and creates the children of its own chunk in
 // box order.  Scratch: flag (cap ints; also the renumbering map) and the
 // alternate box arrays S.  Outcome in C->status (TB_OVERFLOW: more than
 // C->cap boxes; TB_DEEP: levels beyond 32 need the 51-level keys).
 __global__ void __launch_bounds__(TB_THREADS, 1)
-    k_tree_build(BoxPtrs B, BoxPtrs S, TreeCtl* C, int* flag, TreeKeys K, int ns, int nt,
-                 int idivflag, int ndiv, int nlmax, int deep) {
+    k_tree_build(BoxPtrs B, BoxPtrs S, TreeCtl* C, int* flag, TreeKeys K, BoxHash H, int ns,
+                 int nt, int idivflag, int ndiv, int nlmax, int deep) {
   __shared__ int wsum[32];
   __shared__ int red[2];
   __shared__ int newf[NLMAX + 2];
@@ -652,11 +759,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
   // --- adaptive refinement ---------------------------------------------
   int f = 0, n = 1, nb = 1, lev = 0;
   for (;; lev++) {
-    // phase A: colleagues of the level, refine flags and counts of own chunk
-    if (lev >= 1) {
-      const double tol = (double)1.05f * C->bs[lev];
-      for (int b = f + gt; b < f + n; b += gs) colleagues(cur, b, tol);
-    }
+    // phase A: refine flags and counts of own chunk
     const bool more = lev < nlmax;
     const Chunk ch = chunk_of(n);
     int cnt = 0;
@@ -712,6 +815,11 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
     C->nlevels = nl;
     C->bs[nl + 1] = C->bs[nl] / 2;
   }
+  // colleagues of the refined tree (the level restriction and the lists use them)
+  const bool hashed = nl <= 31;
+  if (!(hashed ? colleagues_hashed(C, cur, H, nb, [](int) {})
+               : colleagues_all(C, cur, nl, nb, [](int) {})))
+    return;
   if (nl >= 2) {
     // --- level restriction ---------------------------------------------
     // pass 1: flag (levels >= 2, one pass); zero the per-level counts and tails
@@ -790,7 +898,8 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
         C->tl[b] = -1;
       }
     };
-    if (!colleagues_all(C, cur, nl, nb, keep3)) return;
+    if (!(hashed ? colleagues_hashed(C, cur, H, nb, keep3) : colleagues_all(C, cur, nl, nb, keep3)))
+      return;
     // pass 3: flag++ boxes, coarsest level first, refining as needed; the
     // colleagues of a level's new boxes (its tail) are computed in the same
     // phase as the level's flags, by the thread that then flags the box
@@ -843,7 +952,9 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
       if (!gbar(C)) return;
     }
     if (!reorganize(C, cur, alt, flag, nl, nb, newf)) return;
-    if (!colleagues_all(C, cur, nl, nb, [](int) {})) return;
+    if (!(hashed ? colleagues_hashed(C, cur, H, nb, [](int) {})
+                 : colleagues_all(C, cur, nl, nb, [](int) {})))
+      return;
   }
   // --- point ranges of every box of the final tree ----------------------
   if (nl <= 32) {
@@ -1042,6 +1153,13 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
     DBuf<int> sl(st), sp(st), sn(st), sf(st), flag(st);
     DBuf<int4> sch(st);
     DBuf<uint64_t> pk1(st), pk2(st);
+    DBuf<unsigned long long> hkey(st);
+    DBuf<int> hbox(st);
+    unsigned hcap = 1;
+    while (hcap < 2u * (unsigned)cap) hcap <<= 1;
+    hkey.alloc(hcap, st);
+    hbox.alloc(hcap, st);
+    BoxHash H{hkey.p, hbox.p, hcap - 1};
     sc.alloc(cap, st);
     sl.alloc(cap, st);
     sp.alloc(cap, st);
@@ -1061,7 +1179,7 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
     int* fp = flag.p;
     int nsi = (int)ns, nti = (int)nt;
     int deep = T.deep_sorted ? 1 : 0;
-    void* args[] = {&B, &S, &C, &fp, &K, &nsi, &nti, &idivflag, &ndiv, &nlmax, &deep};
+    void* args[] = {&B, &S, &C, &fp, &K, &H, &nsi, &nti, &idivflag, &ndiv, &nlmax, &deep};
     B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(TB_THREADS),
                                          args, 0, st));
     B2_CHECK(cudaMemcpyAsync(hc, ctl.p, sizeof(TreeCtl), cudaMemcpyDeviceToHost, st));
