@@ -487,10 +487,10 @@ def main():
     if dom == "m2l" and prec == "mixed":
         # tensor-core M2L: useful flops against the measured dense bf16 peak
         # (MEASURED_PEAKS.json); TF32 issues at half that rate.  Issued work:
-        # per tile offset step, 3 split products x K/8 MMAs of 128 x N x 8
-        # (K = 2 KH, N = 2 KH + 2 rounded to 16, KH = P rounded to 4)
+        # per tile step, 3 split products x K/8 MMAs of 128 x N x 8
+        # (K = 2 KH, N = 2 KH rounded to 16, KH = P rounded to 4)
         KH = (int(P) + 3) // 4 * 4
-        K, N = 2 * KH, (2 * KH + 2 + 15) // 16 * 16
+        K, N = 2 * KH, (2 * KH + 15) // 16 * 16
         mma = st["m2l_tc_steps"] * 3 * (K // 8)
         issued = mma * (128 * N * 8 * 2)
         peak = peaks.get("bf16_tflops", 1590.0)
@@ -498,7 +498,7 @@ def main():
                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                     "frac": achieved / peak, "traffic": None,
                     "issued_tensor_tflops": issued / t_dom / 1e12,
-                    "offset_steps": st["m2l_tc_steps"], "mma_instructions": mma,
+                    "tile_steps": st["m2l_tc_steps"], "mma_instructions": mma,
                     "issued_frac_of_tf32_peak": issued / t_dom / 1e12 / (peak / 2),
                     "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else
                                     "fallback 1590 TFLOP/s bf16")}

@@ -2,54 +2,44 @@
 //
 // On scaled expansions (rscale = box size of the level, laprouts2d.f:1130-1244)
 // the translation from a source box at integer offset o = (c_src - c_tgt)/bs
-// is a complex matrix of the offset alone,
-//     L_i += sum_k T_o[i][k] h_k,     T_o[i][k] = u^i G_ik (-u)^k,  u = 1/o,
-// G_0k = 1 (k > 0), G_i0 = -1/i, G_ik = C(i+k-1, k-1), T_o[0][0] = log|o|,
-// plus the level term L_0 += log(bs) h_0.  A target box has at most one
-// list-2 source per offset, so the M2L of a tile of 128 rows (target box,
-// density) is a sum over the <= 40 offsets of one GEMM each,
-//     Y[rows, :] += A_o[rows, :] B_o^T,
-// with A_o the multipole of every row's source at offset o (a zero row where
-// the target has none).  The accumulator stays in tensor memory across the
-// offsets and the result is written once per target: no per-pair scaling, no
-// reduction over pairs and no atomics.
+// (u = 1/o) factors into two diagonal scalings around one real matrix:
+//     t_k = h_k (-u)^k,   y = G t,   L_i += u^i y_i  (i >= 1),
+//     L_0 += y_0 + h_0 (log bs + log|o|),
+// G_00 = 0, G_0k = 1 (k > 0), G_i0 = -1/i, G_ik = C(i+k-1, k-1).  G is the
+// same for every offset and level, so the product y = G t of all pairs is
+// one GEMM with a resident B operand; the scalings are FP32 complex
+// multiplies by 49-entry tables in shared memory.
 //
-// The 40 offsets are images of 7 base offsets b (2,0) (2,1) (2,2) (3,0)
-// (3,1) (3,2) (3,3) under the 8 symmetries of the square, o = w b or
-// o = w conj(b) with w = i^m.  With u = conj(w) u_b (or conj(w) conj(u_b)),
-//     T_o h = conj(w)^i (T'_b h'),   h'_k = conj(w)^k h_k,   T'_b = T_b or conj(T_b):
-// the row builders apply the input phases (exact swaps and sign changes of
-// the FP32 values), each rotation class m accumulates in its own
-// tensor-memory columns, and the epilogue applies the output phases and sums
-// the 4 classes.  The 14 operators T_b, conj(T_b) (TF32 hi + lo) stay
-// resident in shared memory for the whole kernel.
+// Tiles of 128 rows (target box, density): step j takes every row's j-th
+// list-2 source (a target has at most 27), so a tile runs <= 27 steps with
+// one 128 x N x K MMA chain each (K = 2 KH real columns of t, real and
+// imaginary parts interleaved; N = 2 KH rounded to 16).  Split TF32
+// (cvt.rna on both parts): G t = A_hi B_hi + A_hi B_lo + A_lo B_hi with
+// 22-bit operands, products in FP32 in tensor memory.
 //
-// Complex products as real GEMMs, real and imaginary parts interleaved:
-// A row = (Re, Im) h'_0 .. h'_{KH-1} (K = 2 KH), Y row = (Re, Im) L_0 ..
-// L_{KH-1}, then (Re, Im) S0 with S0 = sum of h_0 over the row's sources
-// (for the log(bs) term), B = 2x2 blocks [[Re T, -Im T], [Im T, Re T]] plus
-// the two S0 rows.  Split TF32 (cvt.rna): A B = A_hi B_hi + A_hi B_lo +
-// A_lo B_hi, FP32-level accuracy, accumulated in FP32 in tensor memory.
+// Accumulation: the tensor cores round the FP32 sum of every MMA
+// instruction toward zero.  Summed in place over a tile (27 offsets x 3
+// passes x K/8 instructions) that bias reaches ~1e-5 of the locals, so each
+// step has its own product in tensor memory, started by the two small terms
+// (only the K/8 instructions of A_hi B_hi truncate at full magnitude), and
+// the builders read it back (tcgen05.ld), scale it by u^i and sum the steps
+// in FP32 registers with round-to-nearest: ~2e-7 relative, near a plain FP32
+// M2L.
 //
-// B tiles in shared memory use the canonical K-major layout without
-// swizzle: element (r, k) of a tile with K columns sits at byte
-// (r/8)*SBO + (k/4)*128 + (r%8)*16 + (k%4)*4, SBO = 32 K (8x16-byte core
-// matrices, K-adjacent core matrices 128 bytes apart).  The A rows live in
-// tensor memory (lane = row), written by the builders with tcgen05.st.
+// Layouts: A (per stage, hi and lo) and B in shared memory use the canonical
+// K-major layout without swizzle: element (r, k) of a tile with K columns
+// sits at byte (r/8)*SBO + (k/4)*128 + (r%8)*16 + (k%4)*4, SBO = 32 K
+// (8x16-byte core matrices, K-adjacent core matrices 128 bytes apart).
 //
 // Roles: builder warps (thread = one row x 4 coefficients) gather the
-// source multipoles two offset steps ahead, apply the phases, split and
-// write the rows of a step into one of 4 tensor-memory stages; one issuer
-// thread waits for the stage (mbarrier) and issues the step's tcgen05.mma
-// (M = 128, N = 2 KH + 2 rounded to 16, K = 8 per instruction, A from
-// tensor memory, B from shared memory), whose commit releases the stage.
-// Targets are grouped by their position in the parent box, which fixes the
-// set of offsets a target can have (at most 27 of the 40), so a tile runs
-// few offset steps.  At the end of a tile every builder thread reads back
-// its coefficients of the 4 class accumulators (tcgen05.ld) and adds them to
-// the FP64 locals; each target row is written by exactly one thread.
-// Every wait on the tensor cores is bounded; on time-out the kernel records
-// an error flag (reported as IER_TIMEOUT), frees its tensor memory and ends.
+// source multipoles two steps ahead, scale and split them and write the A
+// rows of a step into one of 4 shared-memory stages; one issuer thread waits
+// for the stage (mbarrier) and issues the step's tcgen05.mma (M = 128, K = 8
+// per instruction), whose commit releases the stage and its product.  At the
+// end of a tile each builder thread adds its 4 coefficients to the FP64
+// locals; each target row is written by exactly one thread.  Every wait on
+// the tensor cores is bounded; on time-out the kernel records an error flag
+// (reported as IER_TIMEOUT), frees its tensor memory and ends.
 #include "tc_m2l.cuh"
 
 #include <cub/cub.cuh>
@@ -199,6 +189,18 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float* v) {
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
+// 8 consecutive FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, float* v) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
+      : "r"(addr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -220,7 +222,8 @@ __device__ __forceinline__ void store_split4(char* hi, char* lo, int r, int k0, 
   float h0 = tf32_rna(a0), h1 = tf32_rna(a1), h2 = tf32_rna(a2), h3 = tf32_rna(a3);
   uint32_t o = tile_off(r, k0, K);
   *reinterpret_cast<float4*>(hi + o) = make_float4(h0, h1, h2, h3);
-  *reinterpret_cast<float4*>(lo + o) = make_float4(a0 - h0, a1 - h1, a2 - h2, a3 - h3);
+  *reinterpret_cast<float4*>(lo + o) = make_float4(tf32_rna(a0 - h0), tf32_rna(a1 - h1),
+                                                   tf32_rna(a2 - h2), tf32_rna(a3 - h3));
 }
 
 // Issue D (+)= A_hi B_hi + A_hi B_lo + A_lo B_hi over K / 8 steps.
@@ -238,126 +241,94 @@ __device__ __forceinline__ void issue_split_mma(uint32_t d_tmem, uint32_t a_hi, 
 }
 
 // ---------------------------------------------------------------------------
-// offset-accumulating M2L
+// M2L on the tensor cores
 // ---------------------------------------------------------------------------
-constexpr int NBASE = 7;
-constexpr int NBMAT = 2 * NBASE;  // the base operators and their conjugates
-constexpr int OT_STAGES = 4;      // A stages in tensor memory (power of 2)
-__host__ __device__ constexpr int base_ox(int b) { return b < 3 ? 2 : 3; }
-__host__ __device__ constexpr int base_oy(int b) { return b < 3 ? b : b - 3; }
+constexpr int OT_STAGES = 4;  // pipeline stages (power of 2)
+constexpr int NOFF = 49;      // offset index (ox + 3) * 7 + (oy + 3), |ox|, |oy| <= 3
+constexpr int NO_OFFSET = 63; // a row without a list-2 entry at this step
 
 // Sizes and layouts for KH complex coefficients per row.  Columns of A and
-// of the accumulators interleave real and imaginary parts: A col 2k + c =
-// (Re, Im) h'_k, Y col 2i + c = (Re, Im) L_i, Y cols 2 KH, 2 KH + 1 = S0.
+// of the products interleave real and imaginary parts: A col 2k + c =
+// (Re, Im) t_k, D col 2i + c = (Re, Im) y_i.
 template <int KH>
 struct OT {
-  static constexpr int K = 2 * KH;                       // A columns
-  static constexpr int N = (2 * KH + 2 + 15) / 16 * 16;  // accumulator columns per class
-  static constexpr int PARTS = KH / 4;                   // builder threads per row
+  static constexpr int K = 2 * KH;                   // A columns
+  static constexpr int N = (2 * KH + 15) / 16 * 16;  // product columns
+  static constexpr int PARTS = KH / 4;               // builder threads per row
   static constexpr int BUILDERS = 128 * PARTS;
   static constexpr int BWARPS = BUILDERS / 32;
-  static constexpr int THREADS = BUILDERS + 32;          // + the MMA issuer warp
-  static constexpr uint32_t SB = (uint32_t)N * K * 4;    // one B tile (hi or lo)
-  static constexpr uint32_t B0 = 0;                      // resident B: [matrix][hi, lo]
-  static constexpr uint32_t MISC = NBMAT * 2 * SB;       // mbarriers, tmem address, flags
-  static constexpr uint32_t WM = MISC + 128;             // per-warp offset masks (u64 x 4)
-  static constexpr uint32_t LGL = WM + 32;               // float[64] log(box size)
-  static constexpr uint32_t CLS = LGL + 256;             // uchar[64] offset classes
-  static constexpr uint32_t TOTAL = CLS + 64;
-  // tensor memory: 4 rotation-class accumulators, then OT_STAGES A stages [hi, lo]
-  static constexpr uint32_t A_COL = 4 * N;
-  static constexpr uint32_t TMEM_USED = A_COL + OT_STAGES * 2 * K;
-  static constexpr uint32_t TMEM_COLS = TMEM_USED <= 128 ? 128 : (TMEM_USED <= 256 ? 256 : 512);
+  static constexpr int THREADS = BUILDERS + 32;      // + the MMA issuer warp
+  static constexpr uint32_t SA = 128u * K * 4;       // one A tile (hi or lo)
+  static constexpr uint32_t SB = (uint32_t)N * K * 4;  // one B tile (hi or lo)
+  static constexpr uint32_t A0 = 0;                  // A stages: [stage][hi, lo]
+  static constexpr uint32_t B0 = OT_STAGES * 2 * SA; // G: [hi, lo]
+  static constexpr uint32_t UP = B0 + 2 * SB;        // float2 [NOFF][KH]: (-u)^k
+  static constexpr uint32_t UO = UP + NOFF * KH * 8; // float2 [NOFF][KH]: u^i
+  static constexpr uint32_t LGO = UO + NOFF * KH * 8;  // float [64]: log|o|
+  static constexpr uint32_t LGL = LGO + 256;         // double [64]: log(box size) by level
+  static constexpr uint32_t MISC = LGL + 512;        // mbarriers, tmem address, flags
+  static constexpr uint32_t TOTAL = MISC + 128;
+  // tensor memory: one product D per stage
+  static constexpr uint32_t TMEM_USED = OT_STAGES * N;
+  static constexpr uint32_t TMEM_COLS =
+      TMEM_USED <= 32 ? 32 : (TMEM_USED <= 64 ? 64 : (TMEM_USED <= 128 ? 128 : 256));
 };
 
-// Gather this thread's 4 coefficients of the row's source multipole at
-// offset oi, if the row's next list-2 entry is at that offset.
-template <int KH>
-__device__ __forceinline__ bool ot_fetch(int oi, unsigned& ecur, int& ep, int ee,
-                                         const int* __restrict__ ent,
-                                         const float4* __restrict__ mp32, int ND, int d, int part,
-                                         float4 (&v)[2]) {
-  if ((int)(ecur >> 26) != oi) return false;
-  const float4* h = mp32 + ((size_t)(ecur & 0x3FFFFFFu) * ND + d) * (KH / 2) + 2 * part;
-  v[0] = h[0];
-  v[1] = h[1];
-  ++ep;
-  ecur = ep < ee ? (unsigned)ent[ep] : 0xFFFFFFFFu;
-  return true;
+// float elements of the table image: G (hi, lo), then (-u)^k and u^i per
+// offset (float2), then log|o| (64 floats).
+__host__ __device__ constexpr long m2l_tab_floats(int KH) {
+  return 2L * ((2 * KH + 15) / 16 * 16) * (2 * KH) + 4L * NOFF * KH + 64;
 }
 
-// (x, y) times i^e
-__device__ __forceinline__ void rot_ie(float x, float y, int e, float& a, float& b) {
-  a = (e & 1) ? -y : x;
-  b = (e & 1) ? x : y;
-  if (e & 2) {
-    a = -a;
-    b = -b;
+// This thread's 4 coefficients of the row's j-th list-2 source multipole
+// (entry e = source | offset index << 26; none: e = ~0).
+template <int KH>
+__device__ __forceinline__ void ot_fetch(int j, int ep, int ee, const int* __restrict__ ent,
+                                         const float4* __restrict__ mp32, int ND, int d, int part,
+                                         unsigned& e, float4 (&v)[2]) {
+  if (ep + j < ee) {
+    e = (unsigned)ent[ep + j];
+    const float4* h = mp32 + ((size_t)(e & 0x3FFFFFFu) * ND + d) * (KH / 2) + 2 * part;
+    v[0] = h[0];
+    v[1] = h[1];
+  } else {
+    e = 0xFFFFFFFFu;
   }
 }
 
-// MMA with A from tensor memory and B from shared memory.
-__device__ __forceinline__ void umma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b,
-                                             uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
-          d_tmem),
-      "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-      : "memory");
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-
-// 8 consecutive FP32 columns of this thread's tensor-memory lane.
-__device__ __forceinline__ void tmem_st8(uint32_t addr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(addr),
-      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
-      : "memory");
-}
-__device__ __forceinline__ void tmem_ld8(uint32_t addr, float* v) {
-  uint32_t r[8];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7])
-      : "r"(addr)
-      : "memory");
-#pragma unroll
-  for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmem_wait_st() {
-  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-
-struct OffsetClasses {
-  unsigned char c[52];  // per offset index (ox+3)*7 + (oy+3): matrix*4 + m; 255: none
-};
 
 // One CTA per SM (persistent); a tile = 128 rows = 128/ND target boxes x ND
 // densities.  tbox: box | level << 26 per target; tstart: CSR offsets into
-// ent (source | offset index << 26, sorted by offset index); tmask: offsets
-// present per target; btab: the resident B image; mp32: FP32 multipoles
-// [box][ND][KH] (zero beyond P); lo: FP64 locals [box][P][ND].
+// ent (source | offset index << 26); tab: the table image; mp32: FP32
+// multipoles [box][ND][KH] (zero beyond P); lo: FP64 locals [box][P][ND].
 //
-// Pipeline per tile, one step per offset present in the tile: the builder
-// warps (thread = row x 4 coefficients) write the A rows of step g into
-// tensor-memory stage g % 4 with tcgen05.st once the MMAs of step g - 4
-// have released it (empty barrier, tcgen05.commit) and arrive on the
-// stage's full barrier; the issuer warp waits for it and issues the step's
-// MMAs (A from tensor memory, B from shared memory).  The builders' global
-// loads run two steps ahead; no CTA-wide barrier sits between the steps of
-// a tile.  At the end of a tile every builder thread reads back its 4
-// coefficients of the 4 class accumulators and updates the FP64 locals.
+// Step j of a tile handles the j-th list-2 entry of every row (rows with
+// fewer entries get zeros), so a tile runs max(list-2 size) <= 27 steps.
+// Per step, with o the row's offset and u = 1/o:
+//     t_k = h_k (-u)^k                        (builders, FP32)
+//     y   = G t                               (tensor cores, split TF32)
+//     L_i += u^i y_i,  L_0 += h_0 log|o|      (builders, FP32 registers)
+// and at the end of the tile L_0 += log(bs) sum h_0 and the FP64 update.
+//
+// Pipeline: the builder warps write the A rows (hi, lo) of step g into
+// shared-memory stage g % 4 once the MMAs of step g - 4 have released it
+// (empty barrier, tcgen05.commit); before that they read back the product of
+// step g - 4 from the stage's tensor-memory columns (tcgen05.ld).  They
+// arrive on the stage's full barrier one step later (after the proxy fence
+// and the wait for the read), and the issuer thread then issues the step's
+// MMAs: A_hi B_lo (starting the product), A_lo B_hi, A_hi B_hi.  The tensor
+// cores truncate each instruction's FP32 sum toward zero; with the two small
+// terms first only the K/8 instructions of the main term truncate at full
+// magnitude, and the steps are summed with round-to-nearest in registers.
 template <int KH>
 __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
     k_m2l_tc(const int* __restrict__ tbox, const int* __restrict__ tstart,
-             const unsigned long long* __restrict__ tmask, const int* __restrict__ ent, int ntgt,
-             int ndsh, int P, const float4* __restrict__ btab, OffsetClasses oc,
-             const double* __restrict__ boxsize, int nlev, const float4* __restrict__ mp32,
-             double2* __restrict__ lo, int* __restrict__ err) {
+             const int* __restrict__ ent, int ntgt, int ndsh, int P,
+             const float4* __restrict__ tab, const double* __restrict__ boxsize, int nlev,
+             const float4* __restrict__ mp32, double2* __restrict__ lo, int* __restrict__ err) {
   using L = OT<KH>;
   constexpr int K = L::K, N = L::N;
   extern __shared__ __align__(1024) char smem[];
@@ -369,19 +340,19 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
   const uint32_t full0 = smem_u32(misc), empty0 = full0 + 8 * OT_STAGES;
   volatile uint32_t* s_taddr = misc + 4 * OT_STAGES;
   volatile int* s_fail = reinterpret_cast<volatile int*>(misc + 4 * OT_STAGES + 1);
-  unsigned long long* s_wm = reinterpret_cast<unsigned long long*>(smem + L::WM);
-  float* LGL = reinterpret_cast<float*>(smem + L::LGL);
-  unsigned char* CLS = reinterpret_cast<unsigned char*>(smem + L::CLS);
+  volatile int* s_wmax = reinterpret_cast<volatile int*>(misc + 4 * OT_STAGES + 2);  // [4]
+  const float2* UP = reinterpret_cast<const float2*>(smem + L::UP);
+  const float2* UO = reinterpret_cast<const float2*>(smem + L::UO);
+  const float* LGO = reinterpret_cast<const float*>(smem + L::LGO);
+  double* LGL = reinterpret_cast<double*>(smem + L::LGL);
 
   {
+    // G and the offset tables are contiguous in the image and in shared memory
     float4* dst = reinterpret_cast<float4*>(smem + L::B0);
-    constexpr int nv = (int)(NBMAT * 2 * L::SB / 16);
-    for (int e = tid; e < nv; e += L::THREADS) dst[e] = btab[e];
+    constexpr int nv = (int)(m2l_tab_floats(KH) / 4);
+    for (int e = tid; e < nv; e += L::THREADS) dst[e] = tab[e];
   }
-  for (int e = tid; e < 64; e += L::THREADS) {
-    LGL[e] = e < nlev ? (float)log(boxsize[e]) : 0.f;
-    CLS[e] = e < 49 ? oc.c[e] : (unsigned char)255;
-  }
+  for (int e = tid; e < 64; e += L::THREADS) LGL[e] = e < nlev ? log(boxsize[e]) : 0.0;
   if (tid == 0) {
     for (int q = 0; q < OT_STAGES; q++) {
       mbar_init(full0 + 8 * q, L::BWARPS);
@@ -400,118 +371,147 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
   const uint32_t sbase = smem_u32(smem);
   const long ntiles = (ntgt + tpt - 1) / tpt;
   const bool builder = warp < L::BWARPS;
-  uint32_t g = 0;  // offset steps of this CTA so far; stage g % OT_STAGES
-  int zmask = 0;   // bit s: this thread's columns of stage s hold zeros
+  uint32_t g = 0;  // steps of this CTA so far; stage g % OT_STAGES
 
   for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long ti = tile * tpt + (r >> ndsh);
     const bool valid = builder && ti < ntgt;
     int ep = 0, ee = 0;
-    unsigned long long msk = 0;
     if (valid) {
       ep = tstart[ti];
       ee = tstart[ti + 1];
-      msk = tmask[ti];
     }
     {
-      unsigned a = __reduce_or_sync(~0u, (unsigned)msk);
-      unsigned b = __reduce_or_sync(~0u, (unsigned)(msk >> 32));
-      if (lane == 0 && warp < 4) s_wm[warp] = ((unsigned long long)b << 32) | a;
+      const int m = __reduce_max_sync(~0u, ee - ep);
+      if (lane == 0 && warp < 4) s_wmax[warp] = m;
     }
     __syncthreads();
     if (*s_fail) break;
-    const unsigned long long mask = s_wm[0] | s_wm[1] | s_wm[2] | s_wm[3];
-    const uint32_t g0 = g, nsteps = (uint32_t)__popcll(mask);
+    const uint32_t g0 = g;
+    const uint32_t nsteps =
+        (uint32_t)max(max(s_wmax[0], s_wmax[1]), max(s_wmax[2], s_wmax[3]));
 
     if (builder) {
-      unsigned ecur = ep < ee ? (unsigned)ent[ep] : 0xFFFFFFFFu;
-      unsigned long long fm = mask;  // offsets not fetched yet
-      float4 va[2], vb[2], vc[2];
-      int oa = -1, ob = -1;
-      bool ha = false, hb = false;
-      if (fm) {
-        oa = __ffsll((long long)fm) - 1;
-        fm &= fm - 1;
-        ha = ot_fetch<KH>(oa, ecur, ep, ee, ent, mp32, ND, d, part, va);
-      }
-      if (fm) {
-        ob = __ffsll((long long)fm) - 1;
-        fm &= fm - 1;
-        hb = ot_fetch<KH>(ob, ecur, ep, ee, ent, mp32, ND, d, part, vb);
-      }
-      int pend = -1;  // stage whose stores are in flight (arrival deferred by one step)
-      while (oa >= 0) {
-        bool hc = false;
-        int ocn = -1;
-        if (fm) {
-          ocn = __ffsll((long long)fm) - 1;
-          fm &= fm - 1;
-          hc = ot_fetch<KH>(ocn, ecur, ep, ee, ent, mp32, ND, d, part, vc);
+      // this thread's coefficients i = 4 part + q of the tile's locals, and
+      // (part 0) the sum of h_0 for the level term
+      float acc[8], s0[2] = {0.f, 0.f};
+#pragma unroll
+      for (int q = 0; q < 8; q++) acc[q] = 0.f;
+      uint32_t oring = 0;  // bits 6s .. 6s + 5: offset index of the step in stage s
+      auto take = [&](const float (&y)[8], int oi) {
+        if (oi == NO_OFFSET) return;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const float2 v = cmulf(make_float2(y[2 * q], y[2 * q + 1]), UO[oi * KH + 4 * part + q]);
+          acc[2 * q] += v.x;
+          acc[2 * q + 1] += v.y;
         }
+      };
+      unsigned ea, eb, ec;
+      float4 va[2], vb[2], vc[2];
+      ot_fetch<KH>(0, ep, ee, ent, mp32, ND, d, part, ea, va);
+      ot_fetch<KH>(1, ep, ee, ent, mp32, ND, d, part, eb, vb);
+      int pend = -1;  // stage whose rows are written but not yet published
+      for (uint32_t j = 0; j < nsteps; j++) {
+        ot_fetch<KH>((int)j + 2, ep, ee, ent, mp32, ND, d, part, ec, vc);
         const int s = (int)(g % OT_STAGES);
         if (g >= OT_STAGES && !*s_fail) {
           if (!mbar_wait_backoff(empty0 + 8 * s, (g / OT_STAGES - 1) & 1)) *s_fail = 1;
           tc_fence_after();
         }
-        // coefficient k = 4 part + j, so k = j (mod 4): input phase i^(-m j)
-        float hi[8], lw[8];
+        // the product of step g - 4 when that step is this tile's
+        const bool rd = g >= g0 + OT_STAGES;
+        float y[8];
+        if (rd) tmem_ld8(lane_base + (uint32_t)(s * N + 8 * part), y);
+        const int oi = ea == 0xFFFFFFFFu ? NO_OFFSET : (int)(ea >> 26);
+        float t[8];
         {
-          const int m = CLS[oa] & 3;
-          const float x[4] = {va[0].x, va[0].z, va[1].x, va[1].z};
-          const float y[4] = {va[0].y, va[0].w, va[1].y, va[1].w};
+          const float2 h[4] = {make_float2(va[0].x, va[0].y), make_float2(va[0].z, va[0].w),
+                               make_float2(va[1].x, va[1].y), make_float2(va[1].z, va[1].w)};
 #pragma unroll
-          for (int j = 0; j < 4; j++) {
-            float a = 0.f, b = 0.f;
-            if (ha) rot_ie(x[j], y[j], (-(m * j)) & 3, a, b);
-            hi[2 * j] = tf32_rna(a);
-            hi[2 * j + 1] = tf32_rna(b);
-            lw[2 * j] = a - hi[2 * j];
-            lw[2 * j + 1] = b - hi[2 * j + 1];
+          for (int q = 0; q < 4; q++) {
+            float2 v = make_float2(0.f, 0.f);
+            if (oi != NO_OFFSET) v = cmulf(h[q], UP[oi * KH + 4 * part + q]);
+            t[2 * q] = v.x;
+            t[2 * q + 1] = v.y;
+          }
+          if (part == 0 && oi != NO_OFFSET) {
+            const float lg = LGO[oi];
+            s0[0] += h[0].x;
+            s0[1] += h[0].y;
+            acc[0] += h[0].x * lg;
+            acc[1] += h[0].y * lg;
           }
         }
-        // the previous step's rows are in tensor memory: publish them
+        // the previous step's rows: visible to the tensor cores, then published
         if (pend >= 0) {
-          tmem_wait_st();
+          fence_async_smem();
           tc_fence_before();
           __syncwarp();
           if (lane == 0) mbar_arrive(full0 + 8 * pend);
         }
-        // tcgen05.st is warp-collective: the warp writes when any of its rows
-        // changes (new data, or zeros over data)
-        const bool need = ha || !((zmask >> s) & 1);
-        if (__any_sync(~0u, need)) {
-          const uint32_t acol = lane_base + L::A_COL + (uint32_t)(s * 2 * K) + 8 * part;
-          tmem_st8(acol, hi);
-          tmem_st8(acol + K, lw);
+        {
+          char* A = smem + L::A0 + (size_t)s * 2 * L::SA;
+          store_split4(A, A + L::SA, r, 8 * part, K, t[0], t[1], t[2], t[3]);
+          store_split4(A, A + L::SA, r, 8 * part + 4, K, t[4], t[5], t[6], t[7]);
         }
-        zmask = ha ? (zmask & ~(1 << s)) : (zmask | (1 << s));
+        if (rd) {
+          tmem_wait_ld();
+          take(y, (int)((oring >> (6 * s)) & 63u));
+        }
+        oring = (oring & ~(63u << (6 * s))) | ((uint32_t)oi << (6 * s));
         pend = s;
         ++g;
-        oa = ob;
-        ha = hb;
-        ob = ocn;
-        hb = hc;
+        ea = eb;
+        eb = ec;
         va[0] = vb[0];
         va[1] = vb[1];
         vb[0] = vc[0];
         vb[1] = vc[1];
       }
       if (pend >= 0) {
-        tmem_wait_st();
+        fence_async_smem();
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(full0 + 8 * pend);
       }
+      // the tile's last (up to 4) products, in order as their commits complete
+      for (uint32_t x = g - min(nsteps, (uint32_t)OT_STAGES); x < g; x++) {
+        const int s = (int)(x % OT_STAGES);
+        if (!*s_fail && !mbar_wait(empty0 + 8 * s, (x / OT_STAGES) & 1)) *s_fail = 1;
+        tc_fence_after();
+        float y[8];
+        tmem_ld8(lane_base + (uint32_t)(s * N + 8 * part), y);
+        tmem_wait_ld();
+        take(y, (int)((oring >> (6 * s)) & 63u));
+      }
+      if (nsteps > 0 && valid && !*s_fail) {
+        const unsigned tb = (unsigned)tbox[ti];
+        double2* out = lo + ((size_t)(tb & 0x3FFFFFFu) * P + 4 * part) * ND + d;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (4 * part + q < P) {
+            double2 v = out[(size_t)q * ND];
+            v.x += (double)acc[2 * q];
+            v.y += (double)acc[2 * q + 1];
+            if (q == 0 && part == 0) {
+              // the level term L_0 += log(bs) sum h_0, in FP64
+              const double lg = LGL[tb >> 26];
+              v.x += lg * (double)s0[0];
+              v.y += lg * (double)s0[1];
+            }
+            out[(size_t)q * ND] = v;
+          }
+        }
+      }
     } else if (lane == 0) {
       // MMA issuer.  After the blocking wait for the next stage it also takes
       // the following stages that are already full, so that one tcgen05 fence
-      // covers several steps (the fence costs a few hundred clocks), and it
-      // reads the next step's class ahead of time.
+      // covers several steps (the fence costs a few hundred clocks).
       const uint32_t idesc = idesc_tf32(TC_ROWS, N);
-      unsigned touched = 0;
+      const uint64_t bh = umma_desc(sbase + L::B0, 128, (uint32_t)K * 32);
+      const uint64_t bl = bh + (L::SB >> 4);
       bool fail = *s_fail != 0;
-      unsigned long long mm = mask;
-      int cl_next = mm ? CLS[__ffsll((long long)mm) - 1] : 255;
       uint32_t left = nsteps;
       while (left > 0) {
         if (!fail && !mbar_wait(full0 + 8 * (g % OT_STAGES), (g / OT_STAGES) & 1)) fail = true;
@@ -523,28 +523,21 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         }
         tc_fence_after();
         for (uint32_t q = 0; q < ready; q++) {
-          mm &= mm - 1;
-          const int cl = cl_next;
-          cl_next = mm ? CLS[__ffsll((long long)mm) - 1] : 255;
           const int s = (int)(g % OT_STAGES);
-          if (cl == 255) fail = true;  // not an interaction offset: its MMA is not issued
           if (!fail) {
-            const int m = cl & 3;
-            const uint32_t a_hi = taddr + L::A_COL + (uint32_t)(s * 2 * K), a_lo = a_hi + K;
-            // descriptors of the matrix's hi and lo tiles; a K step of 8 columns
-            // advances the start address by 256 bytes (16 in descriptor units)
-            const uint64_t bh = umma_desc(sbase + L::B0 + (uint32_t)(cl >> 2) * 2 * L::SB, 128,
-                                          (uint32_t)K * 32);
-            const uint64_t bl = bh + (L::SB >> 4);
-            const uint32_t dt = taddr + (uint32_t)(m * N);
-            const uint32_t acc0 = ((touched >> m) & 1u) ? 1u : 0u;
+            const uint32_t dt = taddr + (uint32_t)(s * N);
+            // a K step of 8 columns advances a start address by 256 bytes
+            // (16 in descriptor units)
+            const uint64_t ah =
+                umma_desc(sbase + L::A0 + (uint32_t)s * 2 * L::SA, 128, (uint32_t)K * 32);
+            const uint64_t al = ah + (L::SA >> 4);
 #pragma unroll
-            for (int ks = 0; ks < K / 8; ks++) {
-              umma_tf32_ts(dt, a_hi + 8 * ks, bh + 16 * ks, idesc, ks == 0 ? acc0 : 1u);
-              umma_tf32_ts(dt, a_hi + 8 * ks, bl + 16 * ks, idesc, 1u);
-              umma_tf32_ts(dt, a_lo + 8 * ks, bh + 16 * ks, idesc, 1u);
-            }
-            touched |= 1u << m;
+            for (int ks = 0; ks < K / 8; ks++)
+              umma_tf32(dt, ah + 16 * ks, bl + 16 * ks, idesc, ks == 0 ? 0u : 1u);
+#pragma unroll
+            for (int ks = 0; ks < K / 8; ks++) umma_tf32(dt, al + 16 * ks, bh + 16 * ks, idesc, 1u);
+#pragma unroll
+            for (int ks = 0; ks < K / 8; ks++) umma_tf32(dt, ah + 16 * ks, bh + 16 * ks, idesc, 1u);
           }
           // the commit also releases the stage when nothing was issued
           umma_commit(empty0 + 8 * s);
@@ -555,57 +548,6 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
       if (fail) *s_fail = 1;
     }
     g = g0 + nsteps;
-    // rotation classes present in the tile (the same on every thread)
-    unsigned touched = 0;
-    for (unsigned long long mm = mask; mm; mm &= mm - 1)
-      touched |= 1u << (CLS[__ffsll((long long)mm) - 1] & 3);
-    if (nsteps > 0 && builder) {
-      // epilogue: the last commit of the tile covers all of its MMAs
-      const uint32_t gl = g - 1;
-      if (!mbar_wait(empty0 + 8 * (gl % OT_STAGES), (gl / OT_STAGES) & 1)) *s_fail = 1;
-      tc_fence_after();
-      float acc[8], s0[2] = {0.f, 0.f};
-#pragma unroll
-      for (int i = 0; i < 8; i++) acc[i] = 0.f;
-      for (int m = 0; m < 4; m++) {
-        if (!((touched >> m) & 1u)) continue;
-        float y[8];
-        tmem_ld8(lane_base + (uint32_t)(m * N + 8 * part), y);
-        tmem_wait_ld();
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          // coefficient i = 4 part + q: output phase i^(-m i) = i^(-m q)
-          float a, b;
-          rot_ie(y[2 * q], y[2 * q + 1], (-(m * q)) & 3, a, b);
-          acc[2 * q] += a;
-          acc[2 * q + 1] += b;
-        }
-        if (part == 0) {
-          tmem_ld8(lane_base + (uint32_t)(m * N + 2 * KH), y);
-          tmem_wait_ld();
-          s0[0] += y[0];
-          s0[1] += y[1];
-        }
-      }
-      if (valid && !*s_fail) {
-        const unsigned tb = (unsigned)tbox[ti];
-        if (part == 0) {
-          const float lg = LGL[tb >> 26];
-          acc[0] += lg * s0[0];
-          acc[1] += lg * s0[1];
-        }
-        double2* out = lo + ((size_t)(tb & 0x3FFFFFFu) * P + 4 * part) * ND + d;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          if (4 * part + q < P) {
-            double2 v = out[(size_t)q * ND];
-            v.x += (double)acc[2 * q];
-            v.y += (double)acc[2 * q + 1];
-            out[(size_t)q * ND] = v;
-          }
-        }
-      }
-    }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -623,55 +565,53 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
   if (tid == 0 && *s_fail) atomicExch(err, 1);
 }
 
-// B image of the 14 resident operators (7 base offsets, each as is and
-// conjugated): [matrix][hi, lo][N x K canonical layout], interleaved columns.
-__global__ void k_m2l_btab(int KH, int N, int P, const double* __restrict__ binom,
-                           float* __restrict__ out) {
+// Table image for KH coefficients (P used): G in the canonical K-major
+// layout as TF32 hi and lo tiles (B[n][kc] = G_ik for n = 2i + c, kc = 2k + c:
+// real G acting on Re and Im alike), then (-u)^k and u^i per offset index and
+// log|o| (FP32).  G_00 = 0, G_0k = 1, G_i0 = -1/i, G_ik = C(i+k-1, k-1).
+__global__ void k_m2l_tab(int KH, int N, int P, const double* __restrict__ binom,
+                          float* __restrict__ out) {
   const int K = 2 * KH;
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= NBMAT * N * K) return;
-  const int mat = e / (N * K), rem = e % (N * K), n = rem / K, kc = rem % K;
-  const int b = mat >> 1;
-  const bool conj = mat & 1;
-  const double ox = base_ox(b), oy = base_oy(b), den = ox * ox + oy * oy;
-  const double ur = ox / den, ui = -oy / den;  // u = 1/o
-  double v = 0.0;
-  if (n < 2 * KH) {
+  if (e < N * K) {
+    const int n = e / K, kc = e % K;
+    double v = 0.0;
     const int i = n >> 1, k = kc >> 1;
-    const bool im_out = n & 1, im_in = kc & 1;
-    if (i < P && k < P) {
-      double tr, tim;
-      if (i == 0 && k == 0) {
-        tr = 0.5 * log(den);
-        tim = 0.0;
-      } else {
-        double gik;
-        if (i == 0)
-          gik = 1.0;
-        else if (k == 0)
-          gik = -1.0 / i;
-        else
-          gik = binom[(size_t)(i + k - 1) * BINOM_N + (k - 1)];
-        double pr = 1.0, pi = 0.0;  // u^(i+k)
-        for (int q = 0; q < i + k; q++) {
-          const double t = pr * ur - pi * ui;
-          pi = pr * ui + pi * ur;
-          pr = t;
-        }
-        const double sg = (k & 1) ? -gik : gik;  // u^i (-u)^k
-        tr = sg * pr;
-        tim = sg * pi;
-      }
-      if (conj) tim = -tim;
-      v = (im_out == im_in) ? tr : (im_out ? tim : -tim);
+    if (n < 2 * KH && (n & 1) == (kc & 1) && i < P && k < P) {
+      if (i == 0)
+        v = k == 0 ? 0.0 : 1.0;
+      else if (k == 0)
+        v = -1.0 / i;
+      else
+        v = binom[(size_t)(i + k - 1) * BINOM_N + (k - 1)];
     }
-  } else if ((n == 2 * KH && kc == 0) || (n == 2 * KH + 1 && kc == 1)) {
-    v = 1.0;
+    const float hi = tf32_rna((float)v), lw = tf32_rna((float)(v - (double)hi));
+    const uint32_t o = tile_off(n, kc, K) / 4;
+    out[o] = hi;
+    out[(size_t)N * K + o] = lw;
+    return;
   }
-  const float hi = tf32_rna((float)v), lw = (float)(v - (double)hi);
-  const uint32_t o = tile_off(n, kc, K) / 4;
-  out[(size_t)mat * 2 * N * K + o] = hi;
-  out[(size_t)mat * 2 * N * K + (size_t)N * K + o] = lw;
+  const int f = e - N * K;
+  float2* up = reinterpret_cast<float2*>(out + 2L * N * K);
+  float2* uo = up + NOFF * KH;
+  float* lg = reinterpret_cast<float*>(uo + NOFF * KH);
+  if (f < NOFF * KH) {
+    const int oi = f / KH, k = f % KH;
+    const int ox = oi / 7 - 3, oy = oi % 7 - 3;
+    double2 p = make_double2(0.0, 0.0);
+    if (ox != 0 || oy != 0) {
+      const double den = (double)ox * ox + (double)oy * oy;
+      const double ur = ox / den, ui = -oy / den;  // u = 1/o
+      p = make_double2(1.0, 0.0);
+      for (int q = 0; q < k; q++) p = make_double2(p.x * ur - p.y * ui, p.x * ui + p.y * ur);
+    }
+    uo[f] = make_float2((float)p.x, (float)p.y);
+    const double sg = (k & 1) ? -1.0 : 1.0;
+    up[f] = make_float2((float)(sg * p.x), (float)(sg * p.y));
+    if (k == 0) lg[oi] = (ox != 0 || oy != 0) ? (float)log(hypot((double)ox, (double)oy)) : 0.f;
+  } else if (f < NOFF * KH + 64 - NOFF) {
+    lg[NOFF + (f - NOFF * KH)] = 0.f;
+  }
 }
 
 // FP32 copy of one density chunk's multipoles, [box][ND][KH] (zero beyond P).
@@ -769,18 +709,17 @@ __global__ void k_m2l_count(TV t, const int* __restrict__ box, int ntgt, int* __
   if (i < ntgt) cnt[i] = t.nl2[box[i]];
 }
 
-// Target boxes and their list-2 entries sorted by offset index.
+// Target boxes and their list-2 entries (source | offset index << 26),
+// sorted by offset index.
 __global__ void k_m2l_fill(TV t, const int* __restrict__ box, int ntgt, const int* __restrict__ cnt,
                            const int* __restrict__ offs, int* __restrict__ tbox,
-                           int* __restrict__ tstart, unsigned long long* __restrict__ tmask,
-                           int* __restrict__ ent) {
+                           int* __restrict__ tstart, int* __restrict__ ent) {
   const int ti = blockIdx.x * blockDim.x + threadIdx.x;
   if (ti >= ntgt) return;
   const int b = box[ti], n2 = cnt[ti];
   const double2 cb = t.center[b];
   const double rinv = 1.0 / t.boxsize[t.level[b]];
   unsigned key[MNLIST2];
-  unsigned long long mask = 0;
   for (int e = 0; e < n2; e++) {
     const int jb = t.l2[(size_t)MNLIST2 * b + e];
     const double2 cj = t.center[jb];
@@ -793,51 +732,24 @@ __global__ void k_m2l_fill(TV t, const int* __restrict__ box, int ntgt, const in
       q--;
     }
     key[q] = k;
-    mask |= 1ull << oi;
   }
   const int o = offs[ti];
   for (int e = 0; e < n2; e++) ent[o + e] = (int)key[e];
   tbox[ti] = (int)((unsigned)b | ((unsigned)t.level[b] << 26));
   tstart[ti] = o;
-  tmask[ti] = mask;
 }
 
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
-// Offset-steps of all tiles of 128/ND targets (the issued tensor-core work).
-__global__ void k_m2l_steps(const unsigned long long* __restrict__ tmask, long ntgt, int tpt,
+// Steps of all tiles of tpt targets (the issued tensor-core work): the
+// longest list-2 of each tile.
+__global__ void k_m2l_steps(const int* __restrict__ tstart, long ntgt, int tpt,
                             unsigned long long* __restrict__ out) {
   const long tile = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (tile * tpt >= ntgt) return;
-  unsigned long long m = 0;
-  for (long q = tile * tpt; q < min(ntgt, (tile + 1) * tpt); q++) m |= tmask[q];
-  atomicAdd(out, (unsigned long long)__popcll(m));
-}
-
-// Offset o = i^m b or i^m conj(b) for a base offset b: resident matrix
-// 2 b (+1 for the conjugate) and rotation class m.
-OffsetClasses offset_classes() {
-  OffsetClasses oc;
-  for (auto& c : oc.c) c = 255;
-  for (int oi = 0; oi < 49; oi++) {
-    const int ox = oi / 7 - 3, oy = oi % 7 - 3;
-    if (std::max(std::abs(ox), std::abs(oy)) < 2) continue;
-    bool found = false;
-    for (int b = 0; b < NBASE && !found; b++)
-      for (int c = 0; c < 2 && !found; c++) {
-        int x = base_ox(b), y = c ? -base_oy(b) : base_oy(b);
-        for (int m = 0; m < 4 && !found; m++) {
-          if (x == ox && y == oy) {
-            oc.c[oi] = (unsigned char)((2 * b + c) * 4 + m);
-            found = true;
-          }
-          const int t = x;  // times i
-          x = -y;
-          y = t;
-        }
-      }
-  }
-  return oc;
+  int m = 0;
+  for (long q = tile * tpt; q < min(ntgt, (tile + 1) * tpt); q++) m = max(m, tstart[q + 1] - tstart[q]);
+  atomicAdd(out, (unsigned long long)m);
 }
 
 int m2l_kh(int P) { return (P + 3) / 4 * 4; }
@@ -899,21 +811,21 @@ void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P,
   L.npairs = (long)h[0] + h[1];
   L.tbox.alloc(L.ntgt, st);
   L.tstart.alloc(L.ntgt + 1, st);
-  L.tmask.alloc(L.ntgt, st);
   L.ent.alloc(std::max<long>(L.npairs, 1), st);
   k_m2l_fill<<<ceil_div(ntgt, 128), 128, 0, st>>>(t, sbox.p, ntgt, cnt.p, offs.p, L.tbox.p,
-                                                  L.tstart.p, L.tmask.p, L.ent.p);
+                                                  L.tstart.p, L.ent.p);
   B2_LAUNCH_CHECK();
   k_set_int<<<1, 1, 0, st>>>(L.tstart.p + L.ntgt, (int)L.npairs);
   B2_LAUNCH_CHECK();
-  const int KH = m2l_kh(P), K = 2 * KH, N = (2 * KH + 2 + 15) / 16 * 16;
-  L.btab.alloc((size_t)NBMAT * 2 * N * K, st);
-  k_m2l_btab<<<ceil_div(NBMAT * N * K, 256), 256, 0, st>>>(KH, N, P, device_binomials(), L.btab.p);
+  const int KH = m2l_kh(P), K = 2 * KH, N = (2 * KH + 15) / 16 * 16;
+  L.tab.alloc(m2l_tab_floats(KH), st);
+  k_m2l_tab<<<ceil_div(N * K + NOFF * KH + 64, 256), 256, 0, st>>>(KH, N, P, device_binomials(),
+                                                                    L.tab.p);
   B2_LAUNCH_CHECK();
   L.steps.alloc(1, st);
   L.steps.zero(1);
   const int tpt = 128 / chunk;
-  k_m2l_steps<<<ceil_div(ceil_div(L.ntgt, tpt), 128), 128, 0, st>>>(L.tmask.p, L.ntgt, tpt,
+  k_m2l_steps<<<ceil_div(ceil_div(L.ntgt, tpt), 128), 128, 0, st>>>(L.tstart.p, L.ntgt, tpt,
                                                                     L.steps.p);
   B2_LAUNCH_CHECK();
   // the temporaries above are freed (stream-ordered) when this returns
@@ -938,18 +850,18 @@ int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long 
   const long nconv = (long)nboxes * ND * KH;
   k_mp_to_f32<<<ceil_div(nconv, 256), 256, 0, st>>>(mp, nboxes, P, ND, KH, mp32);
   B2_LAUNCH_CHECK();
-  const OffsetClasses oc = offset_classes();
   const long ntiles = (L.ntgt + (128 >> ndsh) - 1) / (128 >> ndsh);
   auto launch = [&](auto kern, uint32_t total, uint32_t tmem_cols, int threads) {
-    // CTAs that can share an SM's 512 tensor-memory columns; the shared
-    // memory request keeps more from being resident (an allocation would wait)
-    const int per_sm = 512 / (int)tmem_cols;
+    // CTAs that can share an SM (tensor-memory columns and shared memory);
+    // the shared memory request keeps more from being resident (a tensor
+    // memory allocation would wait)
+    const int per_sm = std::max(1, std::min(512 / (int)tmem_cols, 232448 / (int)(total + 1024)));
     const size_t sm = std::max<size_t>(total, (size_t)(233472 / (per_sm + 1)) + 1024);
     set_smem_attr(kern, sm);
     const int grid = (int)std::min<long>(ntiles, (long)nsm * per_sm);
-    kern<<<grid, threads, sm, st>>>(L.tbox.p, L.tstart.p, L.tmask.p, L.ent.p, (int)L.ntgt, ndsh,
-                                    P, reinterpret_cast<const float4*>(L.btab.p), oc, boxsize,
-                                    nlev, reinterpret_cast<const float4*>(mp32), lo, err_dev);
+    kern<<<grid, threads, sm, st>>>(L.tbox.p, L.tstart.p, L.ent.p, (int)L.ntgt, ndsh, P,
+                                    reinterpret_cast<const float4*>(L.tab.p), boxsize, nlev,
+                                    reinterpret_cast<const float4*>(mp32), lo, err_dev);
     B2_LAUNCH_CHECK();
   };
 #define B2_OT(KHV) \

@@ -1,20 +1,19 @@
-// Mixed-precision Laplace M2L on the sm_100a tensor cores (tcgen05, TF32
-// split products accumulated in FP32 in tensor memory).
+// Mixed-precision Laplace M2L on the sm_100a tensor cores (tcgen05, split
+// TF32 products in FP32 in tensor memory, summed in registers).
 #pragma once
 #include "lap_common.cuh"
 
 namespace b2 {
 
 // M2L targets (boxes of levels >= 2 with list-2 boxes and evaluation
-// points, in box order) and their list-2 entries sorted by offset index:
-// the input of the offset-accumulating tensor-core kernel.
+// points, grouped by their position in the parent box) and their list-2
+// entries: the input of the tensor-core kernel.
 struct M2LPairs {
   DBuf<int> tbox;                   // box | level << 26
   DBuf<int> tstart;                 // ntgt + 1 offsets into ent
-  DBuf<unsigned long long> tmask;   // bit o: a list-2 box at offset index o
   DBuf<int> ent;                    // source | offset index << 26
-  DBuf<float> btab;                 // resident operator image (7 base offsets)
-  DBuf<unsigned long long> steps;   // offset steps of all tiles (tensor-core work)
+  DBuf<float> tab;                  // G (TF32 hi, lo) and the per-offset tables
+  DBuf<unsigned long long> steps;   // steps of all tiles (tensor-core work)
   long ntgt = 0, npairs = 0;
   int P = 0;
   bool usable = false;  // false: box indices do not fit the packed format or P too large
