@@ -189,6 +189,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float* v) {
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
+// 4 consecutive FP32 columns of this thread's tensor-memory lane.
+__device__ __forceinline__ void tmem_ld4(uint32_t addr, float* v) {
+  uint32_t r[4];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(addr)
+               : "memory");
+#pragma unroll
+  for (int i = 0; i < 4; i++) v[i] = __uint_as_float(r[i]);
+}
 // 8 consecutive FP32 columns of this thread's tensor-memory lane.
 __device__ __forceinline__ void tmem_ld8(uint32_t addr, float* v) {
   uint32_t r[8];
@@ -243,19 +253,21 @@ __device__ __forceinline__ void issue_split_mma(uint32_t d_tmem, uint32_t a_hi, 
 // ---------------------------------------------------------------------------
 // M2L on the tensor cores
 // ---------------------------------------------------------------------------
-constexpr int OT_STAGES = 4;  // pipeline stages (power of 2)
-constexpr int NOFF = 49;      // offset index (ox + 3) * 7 + (oy + 3), |ox|, |oy| <= 3
-constexpr int NO_OFFSET = 63; // a row without a list-2 entry at this step
+constexpr int OT_STAGES = 4;  // A stages in shared memory (power of 2)
+constexpr int OT_DBUF = 8;    // product buffers in tensor memory (power of 2)
+constexpr int NOFF = 64;      // table rows: offset index (ox + 3) * 7 + (oy + 3) < 49, rest zero
+constexpr int NO_OFFSET = 63; // a row without a list-2 entry at this step (zero table row)
 
 // Sizes and layouts for KH complex coefficients per row.  Columns of A and
 // of the products interleave real and imaginary parts: A col 2k + c =
-// (Re, Im) t_k, D col 2i + c = (Re, Im) y_i.
+// (Re, Im) t_k, D col 2i + c = (Re, Im) y_i, D cols 2 KH, 2 KH + 1 = (Re, Im)
+// S0 = t_0.  Two builder threads per row take C = KH / 2 coefficients each.
 template <int KH>
 struct OT {
   static constexpr int K = 2 * KH;                   // A columns
-  static constexpr int N = (2 * KH + 15) / 16 * 16;  // product columns
-  static constexpr int PARTS = KH / 4;               // builder threads per row
-  static constexpr int BUILDERS = 128 * PARTS;
+  static constexpr int N = (2 * KH + 2 + 15) / 16 * 16;  // product columns (+ S0)
+  static constexpr int C = KH / 2;                   // coefficients per builder thread
+  static constexpr int BUILDERS = 256;
   static constexpr int BWARPS = BUILDERS / 32;
   static constexpr int THREADS = BUILDERS + 32;      // + the MMA issuer warp
   static constexpr uint32_t SA = 128u * K * 4;       // one A tile (hi or lo)
@@ -264,87 +276,110 @@ struct OT {
   static constexpr uint32_t B0 = OT_STAGES * 2 * SA; // G: [hi, lo]
   static constexpr uint32_t UP = B0 + 2 * SB;        // float2 [NOFF][KH]: (-u)^k
   static constexpr uint32_t UO = UP + NOFF * KH * 8; // float2 [NOFF][KH]: u^i
-  static constexpr uint32_t LGO = UO + NOFF * KH * 8;  // float [64]: log|o|
-  static constexpr uint32_t LGL = LGO + 256;         // double [64]: log(box size) by level
-  static constexpr uint32_t MISC = LGL + 512;        // mbarriers, tmem address, flags
+  static constexpr uint32_t LGO = UO + NOFF * KH * 8;  // float [NOFF]: log|o|
+  static constexpr uint32_t LGL = LGO + NOFF * 4;    // double [64]: log(box size) by level
+  static constexpr uint32_t RING = LGL + 512;        // int [8][BUILDERS]: last-entry marks
+  static constexpr uint32_t MISC = RING + 8 * BUILDERS * 4;  // mbarriers, tmem address, flags
   static constexpr uint32_t TOTAL = MISC + 128;
-  // tensor memory: one product D per stage
-  static constexpr uint32_t TMEM_USED = OT_STAGES * N;
+  // tensor memory: a ring of OT_DBUF products, step g in buffer g % OT_DBUF
+  static constexpr uint32_t TMEM_USED = OT_DBUF * N;
   static constexpr uint32_t TMEM_COLS =
-      TMEM_USED <= 32 ? 32 : (TMEM_USED <= 64 ? 64 : (TMEM_USED <= 128 ? 128 : 256));
+      TMEM_USED <= 128 ? 128 : (TMEM_USED <= 256 ? 256 : 512);
 };
 
 // float elements of the table image: G (hi, lo), then (-u)^k and u^i per
-// offset (float2), then log|o| (64 floats).
+// offset index (float2), then log|o|.
 __host__ __device__ constexpr long m2l_tab_floats(int KH) {
-  return 2L * ((2 * KH + 15) / 16 * 16) * (2 * KH) + 4L * NOFF * KH + 64;
+  return 2L * ((2 * KH + 2 + 15) / 16 * 16) * (2 * KH) + 4L * NOFF * KH + NOFF;
 }
 
-// This thread's 4 coefficients of the row's j-th list-2 source multipole
-// (entry e = source | offset index << 26; none: e = ~0).
+// Round to TF32 (10 mantissa bits), to nearest with ties away from zero:
+// add half a TF32 unit to the magnitude bits and clear the 13 low bits.
+__device__ __forceinline__ float tf32_round(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+// The row's j-th list-2 entry (source | offset index << 26; none: NO_OFFSET << 26).
+__device__ __forceinline__ unsigned ot_entry(int j, int ep, int ee, const int* __restrict__ ent) {
+  return ep + j < ee ? (unsigned)ent[ep + j] : (unsigned)NO_OFFSET << 26;
+}
+
+// This thread's C coefficients of the multipole of entry e (zero for none).
 template <int KH>
-__device__ __forceinline__ void ot_fetch(int j, int ep, int ee, const int* __restrict__ ent,
-                                         const float4* __restrict__ mp32, int ND, int d, int part,
-                                         unsigned& e, float4 (&v)[2]) {
-  if (ep + j < ee) {
-    e = (unsigned)ent[ep + j];
-    const float4* h = mp32 + ((size_t)(e & 0x3FFFFFFu) * ND + d) * (KH / 2) + 2 * part;
-    v[0] = h[0];
-    v[1] = h[1];
+__device__ __forceinline__ void ot_fetch(unsigned e, const float4* __restrict__ mp32, int ND, int d,
+                                         int part, float4 (&v)[KH / 4]) {
+  constexpr int NV = KH / 4;  // float4 = 2 coefficients
+  if ((e >> 26) != (unsigned)NO_OFFSET) {
+    const float4* h = mp32 + ((size_t)(e & 0x3FFFFFFu) * ND + d) * (KH / 2) + NV * part;
+#pragma unroll
+    for (int m = 0; m < NV; m++) v[m] = h[m];
   } else {
-    e = 0xFFFFFFFFu;
+#pragma unroll
+    for (int m = 0; m < NV; m++) v[m] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// 2C consecutive FP32 columns of this thread's tensor-memory lane (2C a
+// multiple of 4, addr 4-column aligned), as 4-column loads.
+template <int C>
+__device__ __forceinline__ void tmem_ld_cols(uint32_t addr, float (&y)[2 * C]) {
+#pragma unroll
+  for (int m = 0; m < C / 2; m++) tmem_ld4(addr + 4 * m, y + 4 * m);
 }
 
-// One CTA per SM (persistent); a tile = 128 rows = 128/ND target boxes x ND
-// densities.  tbox: box | level << 26 per target; tstart: CSR offsets into
-// ent (source | offset index << 26); tab: the table image; mp32: FP32
-// multipoles [box][ND][KH] (zero beyond P); lo: FP64 locals [box][P][ND].
+// One CTA per SM (persistent).  Rows are (target, density) pairs; 128 rows =
+// R = 128/ND row groups.  A super-tile is R T consecutive targets of the
+// order built by m2l_tc_build: row group q of the super-tile takes a
+// contiguous run of about T targets (interleaved from the length-sorted
+// order, so the runs have similar lengths) and walks their list-2 entries
+// back to back, one per step.  ent: per entry (source | offset index << 26,
+// target box | level << 26 on the last entry of a target, else -1); tstart:
+// ntgt + 1 entry offsets; tab: the table image; mp32: FP32 multipoles
+// [box][ND][KH] (zero beyond P); lo: FP64 locals [box][P][ND].
 //
-// Step j of a tile handles the j-th list-2 entry of every row (rows with
-// fewer entries get zeros), so a tile runs max(list-2 size) <= 27 steps.
 // Per step, with o the row's offset and u = 1/o:
 //     t_k = h_k (-u)^k                        (builders, FP32)
-//     y   = G t                               (tensor cores, split TF32)
-//     L_i += u^i y_i,  L_0 += h_0 log|o|      (builders, FP32 registers)
-// and at the end of the tile L_0 += log(bs) sum h_0 and the FP64 update.
+//     y   = G t, S0 = t_0 = h_0               (tensor cores, split TF32)
+//     L_i += u^i y_i,  L_0 += S0 log|o|       (builders, FP32 registers)
+// and after the last entry of a target L_0 += log(bs) sum S0 and an FP64
+// atomic add of the row's locals (each local has one writer).
 //
-// Pipeline: the builder warps write the A rows (hi, lo) of step g into
-// shared-memory stage g % 4 once the MMAs of step g - 4 have released it
-// (empty barrier, tcgen05.commit); before that they read back the product of
-// step g - 4 from the stage's tensor-memory columns (tcgen05.ld).  They
-// arrive on the stage's full barrier one step later (after the proxy fence
-// and the wait for the read), and the issuer thread then issues the step's
-// MMAs: A_hi B_lo (starting the product), A_lo B_hi, A_hi B_hi.  The tensor
-// cores truncate each instruction's FP32 sum toward zero; with the two small
-// terms first only the K/8 instructions of the main term truncate at full
-// magnitude, and the steps are summed with round-to-nearest in registers.
+// Pipeline: the builder warps (two threads per row, C coefficients each)
+// write the A rows (hi, lo) of step g into shared-memory stage g % 4 once the
+// MMAs of step g - 4 have released it (empty barrier, tcgen05.commit), and
+// arrive on the stage's full barrier; the issuer thread then issues the
+// step's MMAs into product buffer g % 8: A_hi B_lo (starting the product),
+// A_lo B_hi, A_hi B_hi.  After the arrival the builders read back the
+// product of step g - 4 (tcgen05.ld; its buffer is rewritten by step g + 4)
+// and add it to their registers.  Loads run ahead: list entries three steps,
+// multipoles two.  The tensor cores truncate each instruction's FP32 sum
+// toward zero; with the two small terms first only the K/8 instructions of
+// the main term truncate at full magnitude, and the steps are summed with
+// round-to-nearest in registers.  The pipeline drains only at the end of a
+// super-tile.
 template <int KH>
 __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
-    k_m2l_tc(const int* __restrict__ tbox, const int* __restrict__ tstart,
-             const int* __restrict__ ent, int ntgt, int ndsh, int P,
-             const float4* __restrict__ tab, const double* __restrict__ boxsize, int nlev,
-             const float4* __restrict__ mp32, double2* __restrict__ lo, int* __restrict__ err) {
+    k_m2l_tc(const int* __restrict__ tstart, const int2* __restrict__ ent, int ntgt, int T,
+             int ndsh, int P, const float4* __restrict__ tab, const double* __restrict__ boxsize,
+             int nlev, const float4* __restrict__ mp32, double2* __restrict__ lo,
+             int* __restrict__ err) {
   using L = OT<KH>;
-  constexpr int K = L::K, N = L::N;
+  constexpr int K = L::K, N = L::N, C = L::C, NV = KH / 4;
   extern __shared__ __align__(1024) char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int r = tid & 127, part = tid >> 7;
-  const int ND = 1 << ndsh, tpt = 128 >> ndsh, d = r & (ND - 1);
+  const int ND = 1 << ndsh, R = 128 >> ndsh, d = r & (ND - 1), rg = r >> ndsh;
   uint32_t* misc = reinterpret_cast<uint32_t*>(smem + L::MISC);
   // full[OT_STAGES], empty[OT_STAGES] mbarriers, 8 bytes apart
   const uint32_t full0 = smem_u32(misc), empty0 = full0 + 8 * OT_STAGES;
   volatile uint32_t* s_taddr = misc + 4 * OT_STAGES;
   volatile int* s_fail = reinterpret_cast<volatile int*>(misc + 4 * OT_STAGES + 1);
   volatile int* s_wmax = reinterpret_cast<volatile int*>(misc + 4 * OT_STAGES + 2);  // [4]
-  const float2* UP = reinterpret_cast<const float2*>(smem + L::UP);
-  const float2* UO = reinterpret_cast<const float2*>(smem + L::UO);
+  const float4* UP4 = reinterpret_cast<const float4*>(smem + L::UP);
+  const float4* UO4 = reinterpret_cast<const float4*>(smem + L::UO);
   const float* LGO = reinterpret_cast<const float*>(smem + L::LGO);
   double* LGL = reinterpret_cast<double*>(smem + L::LGL);
+  int* RING = reinterpret_cast<int*>(smem + L::RING);  // [8][BUILDERS]: last-entry marks
 
   {
     // G and the offset tables are contiguous in the image and in shared memory
@@ -369,17 +404,24 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
   const uint32_t taddr = *s_taddr;
   const uint32_t lane_base = taddr + ((uint32_t)((warp & 3) * 32) << 16);
   const uint32_t sbase = smem_u32(smem);
-  const long ntiles = (ntgt + tpt - 1) / tpt;
+  const long per_st = (long)R * T;
+  const long nst = (ntgt + per_st - 1) / per_st;
   const bool builder = warp < L::BWARPS;
-  uint32_t g = 0;  // steps of this CTA so far; stage g % OT_STAGES
+  // this thread's A columns 2 C part .. : C / 2 groups of 4, 128 bytes apart
+  const uint32_t aoff = tile_off(r, 2 * C * part, K);
+  uint32_t g = 0;  // steps of this CTA so far; stage g % OT_STAGES, buffer g % OT_DBUF
 
-  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long ti = tile * tpt + (r >> ndsh);
-    const bool valid = builder && ti < ntgt;
+  for (long st = blockIdx.x; st < nst; st += gridDim.x) {
+    // this row group's run of targets in the super-tile
+    const long base = st * per_st;
+    const int c = (int)min(per_st, (long)ntgt - base);
+    const int q0 = c / R, rem = c % R;
+    const int nr = builder ? q0 + (rg < rem ? 1 : 0) : 0;
     int ep = 0, ee = 0;
-    if (valid) {
-      ep = tstart[ti];
-      ee = tstart[ti + 1];
+    if (nr > 0) {
+      const long first = base + (long)rg * q0 + min(rg, rem);
+      ep = tstart[first];
+      ee = tstart[first + nr];
     }
     {
       const int m = __reduce_max_sync(~0u, ee - ep);
@@ -392,117 +434,138 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         (uint32_t)max(max(s_wmax[0], s_wmax[1]), max(s_wmax[2], s_wmax[3]));
 
     if (builder) {
-      // this thread's coefficients i = 4 part + q of the tile's locals, and
-      // (part 0) the sum of h_0 for the level term
-      float acc[8], s0[2] = {0.f, 0.f};
+      // this thread's coefficients i = C part + q of the current target's
+      // locals, and (part 0) the sum of S0 for the level term
+      float acc[2 * C], s0x = 0.f, s0y = 0.f;
 #pragma unroll
-      for (int q = 0; q < 8; q++) acc[q] = 0.f;
-      uint32_t oring = 0;  // bits 6s .. 6s + 5: offset index of the step in stage s
-      auto take = [&](const float (&y)[8], int oi) {
-        if (oi == NO_OFFSET) return;
+      for (int q = 0; q < 2 * C; q++) acc[q] = 0.f;
+      // offset index of step x in bits 6 (x % 8) .. + 5
+      unsigned long long oring = 0;
+      auto oring_get = [&](uint32_t x) { return (int)((oring >> (6 * (x % 8))) & 63u); };
+      auto dcol = [&](uint32_t x) {
+        return lane_base + (uint32_t)((x % OT_DBUF) * N + 2 * C * part);
+      };
+      // add the product of step x; after the last entry of a target, flush
+      auto take = [&](uint32_t x) {
+        float y[2 * C];
+        tmem_ld_cols<C>(dcol(x), y);
+        float z[4];
+        if (part == 0) tmem_ld4(lane_base + (uint32_t)((x % OT_DBUF) * N + 2 * KH), z);
+        tmem_wait_ld();
+        const int op = oring_get(x);
+        const float4* uo = UO4 + (op * KH + C * part) / 2;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const float2 v = cmulf(make_float2(y[2 * q], y[2 * q + 1]), UO[oi * KH + 4 * part + q]);
-          acc[2 * q] += v.x;
-          acc[2 * q + 1] += v.y;
+        for (int m = 0; m < NV; m++) {
+          const float4 w = uo[m];  // u^i for two coefficients
+          acc[4 * m] = fmaf(y[4 * m], w.x, fmaf(-y[4 * m + 1], w.y, acc[4 * m]));
+          acc[4 * m + 1] = fmaf(y[4 * m], w.y, fmaf(y[4 * m + 1], w.x, acc[4 * m + 1]));
+          acc[4 * m + 2] = fmaf(y[4 * m + 2], w.z, fmaf(-y[4 * m + 3], w.w, acc[4 * m + 2]));
+          acc[4 * m + 3] = fmaf(y[4 * m + 2], w.w, fmaf(y[4 * m + 3], w.z, acc[4 * m + 3]));
+        }
+        if (part == 0) {
+          const float lg = LGO[op];
+          acc[0] = fmaf(z[0], lg, acc[0]);
+          acc[1] = fmaf(z[1], lg, acc[1]);
+          s0x += z[0];
+          s0y += z[1];
+        }
+        // -1: not the last entry of a target (a mark is box | level << 26 with
+        // box < 2^26 - 1, never all ones)
+        const int tb = RING[(x % 8) * L::BUILDERS + tid];
+        if (tb != -1) {
+          if (!*s_fail) {
+            double* out = reinterpret_cast<double*>(
+                lo + ((size_t)((unsigned)tb & 0x3FFFFFFu) * P + C * part) * ND + d);
+#pragma unroll
+            for (int q = 0; q < C; q++) {
+              if (C * part + q < P) {
+                double vx = (double)acc[2 * q], vy = (double)acc[2 * q + 1];
+                if (q == 0 && part == 0) {
+                  // the level term L_0 += log(bs) sum S0, in FP64
+                  const double lg = LGL[(unsigned)tb >> 26];
+                  vx += lg * (double)s0x;
+                  vy += lg * (double)s0y;
+                }
+                atomicAdd(out + 2 * (size_t)q * ND, vx);
+                atomicAdd(out + 2 * (size_t)q * ND + 1, vy);
+              }
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 2 * C; q++) acc[q] = 0.f;
+          s0x = s0y = 0.f;
         }
       };
-      unsigned ea, eb, ec;
-      float4 va[2], vb[2], vc[2];
-      ot_fetch<KH>(0, ep, ee, ent, mp32, ND, d, part, ea, va);
-      ot_fetch<KH>(1, ep, ee, ent, mp32, ND, d, part, eb, vb);
-      int pend = -1;  // stage whose rows are written but not yet published
-      for (uint32_t j = 0; j < nsteps; j++) {
-        ot_fetch<KH>((int)j + 2, ep, ee, ent, mp32, ND, d, part, ec, vc);
+      // Step j from the fetched entry (ecur, vcur).  The multipole of step
+      // j + 2 (entry en, read one step earlier) goes to (ef, vf) and the entry
+      // of step j + 3 to en, so no load waits for another.  The rows are
+      // computed before the wait for the stage, so only the split, the
+      // stores, the proxy fence and the arrival follow the release; the
+      // product of step g - 4 is read after the arrival.
+      const int2 none = make_int2(NO_OFFSET << 26, -1);
+      auto entry = [&](uint32_t j) { return ep + (int)j < ee ? ent[ep + j] : none; };
+      int2 en;
+      auto body = [&](uint32_t j, int2 ecur, const float4 (&vcur)[NV], int2& ef,
+                      float4 (&vf)[NV]) {
+        ef = en;
+        ot_fetch<KH>((unsigned)ef.x, mp32, ND, d, part, vf);
+        en = entry(j + 3);
         const int s = (int)(g % OT_STAGES);
+        const int oi = (int)((unsigned)ecur.x >> 26);
+        // t = h (-u)^k
+        float4 t[NV];
+        {
+          const float4* up = UP4 + (oi * KH + C * part) / 2;
+#pragma unroll
+          for (int m = 0; m < NV; m++) {
+            const float4 w = up[m];  // (-u)^k for two coefficients
+            const float4 h = vcur[m];
+            t[m] = make_float4(h.x * w.x - h.y * w.y, h.x * w.y + h.y * w.x,
+                               h.z * w.z - h.w * w.w, h.z * w.w + h.w * w.z);
+          }
+        }
+        RING[(g % 8) * L::BUILDERS + tid] = ecur.y;
         if (g >= OT_STAGES && !*s_fail) {
           if (!mbar_wait_backoff(empty0 + 8 * s, (g / OT_STAGES - 1) & 1)) *s_fail = 1;
           tc_fence_after();
         }
-        // the product of step g - 4 when that step is this tile's
-        const bool rd = g >= g0 + OT_STAGES;
-        float y[8];
-        if (rd) tmem_ld8(lane_base + (uint32_t)(s * N + 8 * part), y);
-        const int oi = ea == 0xFFFFFFFFu ? NO_OFFSET : (int)(ea >> 26);
-        float t[8];
+        // TF32 hi (rounded) and lo (the MMA keeps its leading 11 bits)
         {
-          const float2 h[4] = {make_float2(va[0].x, va[0].y), make_float2(va[0].z, va[0].w),
-                               make_float2(va[1].x, va[1].y), make_float2(va[1].z, va[1].w)};
+          char* A = smem + L::A0 + (size_t)s * 2 * L::SA + aoff;
 #pragma unroll
-          for (int q = 0; q < 4; q++) {
-            float2 v = make_float2(0.f, 0.f);
-            if (oi != NO_OFFSET) v = cmulf(h[q], UP[oi * KH + 4 * part + q]);
-            t[2 * q] = v.x;
-            t[2 * q + 1] = v.y;
-          }
-          if (part == 0 && oi != NO_OFFSET) {
-            const float lg = LGO[oi];
-            s0[0] += h[0].x;
-            s0[1] += h[0].y;
-            acc[0] += h[0].x * lg;
-            acc[1] += h[0].y * lg;
+          for (int m = 0; m < NV; m++) {
+            const float4 hi = make_float4(tf32_round(t[m].x), tf32_round(t[m].y),
+                                          tf32_round(t[m].z), tf32_round(t[m].w));
+            *reinterpret_cast<float4*>(A + 128 * m) = hi;
+            *reinterpret_cast<float4*>(A + L::SA + 128 * m) =
+                make_float4(t[m].x - hi.x, t[m].y - hi.y, t[m].z - hi.z, t[m].w - hi.w);
           }
         }
-        // the previous step's rows: visible to the tensor cores, then published
-        if (pend >= 0) {
-          fence_async_smem();
-          tc_fence_before();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(full0 + 8 * pend);
-        }
-        {
-          char* A = smem + L::A0 + (size_t)s * 2 * L::SA;
-          store_split4(A, A + L::SA, r, 8 * part, K, t[0], t[1], t[2], t[3]);
-          store_split4(A, A + L::SA, r, 8 * part + 4, K, t[4], t[5], t[6], t[7]);
-        }
-        if (rd) {
-          tmem_wait_ld();
-          take(y, (int)((oring >> (6 * s)) & 63u));
-        }
-        oring = (oring & ~(63u << (6 * s))) | ((uint32_t)oi << (6 * s));
-        pend = s;
-        ++g;
-        ea = eb;
-        eb = ec;
-        va[0] = vb[0];
-        va[1] = vb[1];
-        vb[0] = vc[0];
-        vb[1] = vc[1];
-      }
-      if (pend >= 0) {
+        // visible to the tensor cores, then published
         fence_async_smem();
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(full0 + 8 * pend);
+        if (lane == 0) mbar_arrive(full0 + 8 * s);
+        if (g >= g0 + OT_STAGES) take(g - OT_STAGES);
+        oring = (oring & ~(63ull << (6 * (g % 8)))) | ((unsigned long long)oi << (6 * (g % 8)));
+        ++g;
+      };
+      int2 e0 = entry(0), e1 = entry(1), e2;
+      en = entry(2);
+      float4 v0[NV], v1[NV], v2[NV];
+      ot_fetch<KH>((unsigned)e0.x, mp32, ND, d, part, v0);
+      ot_fetch<KH>((unsigned)e1.x, mp32, ND, d, part, v1);
+      for (uint32_t j = 0; j < nsteps; j += 3) {
+        body(j, e0, v0, e2, v2);
+        if (j + 1 < nsteps) body(j + 1, e1, v1, e0, v0);
+        if (j + 2 < nsteps) body(j + 2, e2, v2, e1, v1);
       }
-      // the tile's last (up to 4) products, in order as their commits complete
+      // the super-tile's last (up to 4) products, in order as their commits complete
       for (uint32_t x = g - min(nsteps, (uint32_t)OT_STAGES); x < g; x++) {
-        const int s = (int)(x % OT_STAGES);
-        if (!*s_fail && !mbar_wait(empty0 + 8 * s, (x / OT_STAGES) & 1)) *s_fail = 1;
+        if (!*s_fail && !mbar_wait(empty0 + 8 * (x % OT_STAGES), (x / OT_STAGES) & 1))
+          *s_fail = 1;
         tc_fence_after();
-        float y[8];
-        tmem_ld8(lane_base + (uint32_t)(s * N + 8 * part), y);
-        tmem_wait_ld();
-        take(y, (int)((oring >> (6 * s)) & 63u));
-      }
-      if (nsteps > 0 && valid && !*s_fail) {
-        const unsigned tb = (unsigned)tbox[ti];
-        double2* out = lo + ((size_t)(tb & 0x3FFFFFFu) * P + 4 * part) * ND + d;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          if (4 * part + q < P) {
-            double2 v = out[(size_t)q * ND];
-            v.x += (double)acc[2 * q];
-            v.y += (double)acc[2 * q + 1];
-            if (q == 0 && part == 0) {
-              // the level term L_0 += log(bs) sum h_0, in FP64
-              const double lg = LGL[tb >> 26];
-              v.x += lg * (double)s0[0];
-              v.y += lg * (double)s0[1];
-            }
-            out[(size_t)q * ND] = v;
-          }
-        }
+        take(x);
       }
     } else if (lane == 0) {
       // MMA issuer.  After the blocking wait for the next stage it also takes
@@ -525,7 +588,7 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         for (uint32_t q = 0; q < ready; q++) {
           const int s = (int)(g % OT_STAGES);
           if (!fail) {
-            const uint32_t dt = taddr + (uint32_t)(s * N);
+            const uint32_t dt = taddr + (uint32_t)((g % OT_DBUF) * N);
             // a K step of 8 columns advances a start address by 256 bytes
             // (16 in descriptor units)
             const uint64_t ah =
@@ -567,8 +630,10 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
 
 // Table image for KH coefficients (P used): G in the canonical K-major
 // layout as TF32 hi and lo tiles (B[n][kc] = G_ik for n = 2i + c, kc = 2k + c:
-// real G acting on Re and Im alike), then (-u)^k and u^i per offset index and
-// log|o| (FP32).  G_00 = 0, G_0k = 1, G_i0 = -1/i, G_ik = C(i+k-1, k-1).
+// real G acting on Re and Im alike; rows 2 KH + c pick t_0), then (-u)^k and
+// u^i per offset index and log|o| (FP32; zero rows for the indices that are
+// not offsets).
+// G_00 = 0, G_0k = 1, G_i0 = -1/i, G_ik = C(i+k-1, k-1).
 __global__ void k_m2l_tab(int KH, int N, int P, const double* __restrict__ binom,
                           float* __restrict__ out) {
   const int K = 2 * KH;
@@ -584,6 +649,8 @@ __global__ void k_m2l_tab(int KH, int N, int P, const double* __restrict__ binom
         v = -1.0 / i;
       else
         v = binom[(size_t)(i + k - 1) * BINOM_N + (k - 1)];
+    } else if (kc < 2 && n == 2 * KH + kc) {
+      v = 1.0;  // S0 = t_0 (rows 2 KH, 2 KH + 1; columns 0, 1)
     }
     const float hi = tf32_rna((float)v), lw = tf32_rna((float)(v - (double)hi));
     const uint32_t o = tile_off(n, kc, K) / 4;
@@ -592,26 +659,25 @@ __global__ void k_m2l_tab(int KH, int N, int P, const double* __restrict__ binom
     return;
   }
   const int f = e - N * K;
+  if (f >= NOFF * KH) return;
   float2* up = reinterpret_cast<float2*>(out + 2L * N * K);
   float2* uo = up + NOFF * KH;
   float* lg = reinterpret_cast<float*>(uo + NOFF * KH);
-  if (f < NOFF * KH) {
-    const int oi = f / KH, k = f % KH;
-    const int ox = oi / 7 - 3, oy = oi % 7 - 3;
-    double2 p = make_double2(0.0, 0.0);
-    if (ox != 0 || oy != 0) {
-      const double den = (double)ox * ox + (double)oy * oy;
-      const double ur = ox / den, ui = -oy / den;  // u = 1/o
-      p = make_double2(1.0, 0.0);
-      for (int q = 0; q < k; q++) p = make_double2(p.x * ur - p.y * ui, p.x * ui + p.y * ur);
-    }
-    uo[f] = make_float2((float)p.x, (float)p.y);
-    const double sg = (k & 1) ? -1.0 : 1.0;
-    up[f] = make_float2((float)(sg * p.x), (float)(sg * p.y));
-    if (k == 0) lg[oi] = (ox != 0 || oy != 0) ? (float)log(hypot((double)ox, (double)oy)) : 0.f;
-  } else if (f < NOFF * KH + 64 - NOFF) {
-    lg[NOFF + (f - NOFF * KH)] = 0.f;
+  const int oi = f / KH, k = f % KH;
+  const int ox = oi / 7 - 3, oy = oi % 7 - 3;
+  double2 p = make_double2(0.0, 0.0);
+  double l = 0.0;
+  if (oi < 49 && (ox != 0 || oy != 0)) {
+    const double den = (double)ox * ox + (double)oy * oy;
+    const double ur = ox / den, ui = -oy / den;  // u = 1/o
+    p = make_double2(1.0, 0.0);
+    for (int q = 0; q < k; q++) p = make_double2(p.x * ur - p.y * ui, p.x * ui + p.y * ur);
+    l = 0.5 * log(den);
   }
+  uo[f] = make_float2((float)p.x, (float)p.y);
+  const double sg = (k & 1) ? -1.0 : 1.0;
+  up[f] = make_float2((float)(sg * p.x), (float)(sg * p.y));
+  if (k == 0) lg[oi] = (float)l;
 }
 
 // FP32 copy of one density chunk's multipoles, [box][ND][KH] (zero beyond P).
@@ -686,21 +752,16 @@ __global__ void k_m2l_flag(TV t, int first, int n, int* __restrict__ flag) {
   flag[i] = (t.has_eval_pts(b) && t.nl2[b] > 0) ? 1 : 0;
 }
 
-// Compact the targets with their child position (parity of the box's grid
-// coordinates at its level), which fixes the set of list-2 offsets a box
-// can have: targets grouped by it make tiles of at most 27 offsets.
+// Compact the targets with their list-2 length as the sort key: a tile runs
+// as many steps as its longest list, so tiles of equal lengths keep every
+// row busy.
 __global__ void k_m2l_compact(TV t, int first, int n, const int* __restrict__ flag,
                               const int* __restrict__ tix, int* __restrict__ key,
                               int* __restrict__ box) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !flag[i]) return;
   const int b = first + i;
-  const double bs = t.boxsize[t.level[b]];
-  const double2 c = t.center[b], c0 = t.center[0];
-  const double h0 = 0.5 * t.boxsize[0];
-  const long ix = __double2ll_rn((c.x - c0.x + h0) / bs - 0.5);
-  const long iy = __double2ll_rn((c.y - c0.y + h0) / bs - 0.5);
-  key[tix[i]] = (int)((ix & 1) | ((iy & 1) << 1));
+  key[tix[i]] = t.nl2[b];
   box[tix[i]] = b;
 }
 
@@ -709,11 +770,12 @@ __global__ void k_m2l_count(TV t, const int* __restrict__ box, int ntgt, int* __
   if (i < ntgt) cnt[i] = t.nl2[box[i]];
 }
 
-// Target boxes and their list-2 entries (source | offset index << 26),
-// sorted by offset index.
+// Target boxes in kernel order and their list-2 entries, sorted by offset
+// index: (source | offset index << 26, target box | level << 26 on the last
+// entry of a target, else -1).
 __global__ void k_m2l_fill(TV t, const int* __restrict__ box, int ntgt, const int* __restrict__ cnt,
-                           const int* __restrict__ offs, int* __restrict__ tbox,
-                           int* __restrict__ tstart, int* __restrict__ ent) {
+                           const int* __restrict__ offs, int* __restrict__ tstart,
+                           int2* __restrict__ ent) {
   const int ti = blockIdx.x * blockDim.x + threadIdx.x;
   if (ti >= ntgt) return;
   const int b = box[ti], n2 = cnt[ti];
@@ -734,21 +796,42 @@ __global__ void k_m2l_fill(TV t, const int* __restrict__ box, int ntgt, const in
     key[q] = k;
   }
   const int o = offs[ti];
-  for (int e = 0; e < n2; e++) ent[o + e] = (int)key[e];
-  tbox[ti] = (int)((unsigned)b | ((unsigned)t.level[b] << 26));
+  const int tb = (int)((unsigned)b | ((unsigned)t.level[b] << 26));
+  for (int e = 0; e < n2; e++) ent[o + e] = make_int2((int)key[e], e == n2 - 1 ? tb : -1);
   tstart[ti] = o;
+}
+
+// Kernel order of the length-sorted targets: super-tiles of R T targets, in
+// which row group q takes a contiguous run of the targets q, q + R, q + 2R,
+// ... of the super-tile (runs of similar total length).
+__global__ void k_m2l_perm(const int* __restrict__ sbox, int ntgt, int R, int T,
+                           int* __restrict__ pbox) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntgt) return;
+  const long per = (long)R * T, base = i / per * per;
+  const int ip = (int)(i - base);
+  const int c = (int)min(per, (long)ntgt - base), q0 = c / R, rem = c % R;
+  const int rg = ip % R, k = ip / R;
+  pbox[base + (long)rg * q0 + min(rg, rem) + k] = sbox[i];
 }
 
 __global__ void k_set_int(int* p, int v) { *p = v; }
 
-// Steps of all tiles of tpt targets (the issued tensor-core work): the
-// longest list-2 of each tile.
-__global__ void k_m2l_steps(const int* __restrict__ tstart, long ntgt, int tpt,
+// Steps of all super-tiles (the issued tensor-core work): the longest run
+// of list-2 entries over the row groups of each super-tile.
+__global__ void k_m2l_steps(const int* __restrict__ tstart, long ntgt, int R, int T,
                             unsigned long long* __restrict__ out) {
-  const long tile = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (tile * tpt >= ntgt) return;
+  const long stl = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long per = (long)R * T, base = stl * per;
+  if (base >= ntgt) return;
+  const int c = (int)min(per, ntgt - base), q0 = c / R, rem = c % R;
   int m = 0;
-  for (long q = tile * tpt; q < min(ntgt, (tile + 1) * tpt); q++) m = max(m, tstart[q + 1] - tstart[q]);
+  for (int rg = 0; rg < R; rg++) {
+    const int nr = q0 + (rg < rem ? 1 : 0);
+    if (nr == 0) continue;
+    const long first = base + (long)rg * q0 + min(rg, rem);
+    m = max(m, tstart[first + nr] - tstart[first]);
+  }
   atomicAdd(out, (unsigned long long)m);
 }
 
@@ -780,7 +863,7 @@ void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P,
   B2_CHECK(cudaStreamSynchronize(st));
   const int ntgt = h[0] + h[1];
   if (ntgt == 0) return;
-  // targets grouped by child position (stable: box order inside a group)
+  // targets sorted by list-2 length
   DBuf<int> key(st), box(st), skey(st), sbox(st), cnt(st), offs(st);
   key.alloc(ntgt, st);
   box.alloc(ntgt, st);
@@ -789,15 +872,27 @@ void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P,
   k_m2l_compact<<<ceil_div(n, 256), 256, 0, st>>>(t, first, n, flag.p, tix.p, key.p, box.p);
   B2_LAUNCH_CHECK();
   size_t tb2 = 0;
-  B2_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key.p, skey.p, box.p, sbox.p, ntgt, 0, 2,
+  // list lengths are <= MNLIST2 < 32: 5 key bits (stable: box order inside a length)
+  static_assert(MNLIST2 < 32, "list-2 length key");
+  B2_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key.p, skey.p, box.p, sbox.p, ntgt, 0, 5,
                                            st));
   DBuf<char> tmp2(st);
   tmp2.alloc(tb2, st);
-  B2_CHECK(cub::DeviceRadixSort::SortPairs(tmp2.p, tb2, key.p, skey.p, box.p, sbox.p, ntgt, 0, 2,
+  B2_CHECK(cub::DeviceRadixSort::SortPairs(tmp2.p, tb2, key.p, skey.p, box.p, sbox.p, ntgt, 0, 5,
                                            st));
+  // super-tiles: about 4 per SM for the main density chunk
+  int dev = 0, nsm = 148;
+  B2_CHECK(cudaGetDevice(&dev));
+  B2_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int R = 128 / chunk;
+  L.T = (int)std::max<long>(1, ((long)ntgt + R - 1) / R / (4L * nsm));
+  DBuf<int> pbox(st);
+  pbox.alloc(ntgt, st);
+  k_m2l_perm<<<ceil_div(ntgt, 256), 256, 0, st>>>(sbox.p, ntgt, R, L.T, pbox.p);
+  B2_LAUNCH_CHECK();
   cnt.alloc(ntgt, st);
   offs.alloc(ntgt, st);
-  k_m2l_count<<<ceil_div(ntgt, 256), 256, 0, st>>>(t, sbox.p, ntgt, cnt.p);
+  k_m2l_count<<<ceil_div(ntgt, 256), 256, 0, st>>>(t, pbox.p, ntgt, cnt.p);
   B2_LAUNCH_CHECK();
   size_t tb3 = 0;
   B2_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, cnt.p, offs.p, ntgt, st));
@@ -809,24 +904,22 @@ void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P,
   B2_CHECK(cudaStreamSynchronize(st));
   L.ntgt = ntgt;
   L.npairs = (long)h[0] + h[1];
-  L.tbox.alloc(L.ntgt, st);
   L.tstart.alloc(L.ntgt + 1, st);
   L.ent.alloc(std::max<long>(L.npairs, 1), st);
-  k_m2l_fill<<<ceil_div(ntgt, 128), 128, 0, st>>>(t, sbox.p, ntgt, cnt.p, offs.p, L.tbox.p,
-                                                  L.tstart.p, L.ent.p);
+  k_m2l_fill<<<ceil_div(ntgt, 128), 128, 0, st>>>(t, pbox.p, ntgt, cnt.p, offs.p, L.tstart.p,
+                                                  L.ent.p);
   B2_LAUNCH_CHECK();
   k_set_int<<<1, 1, 0, st>>>(L.tstart.p + L.ntgt, (int)L.npairs);
   B2_LAUNCH_CHECK();
-  const int KH = m2l_kh(P), K = 2 * KH, N = (2 * KH + 15) / 16 * 16;
+  const int KH = m2l_kh(P), K = 2 * KH, N = (2 * KH + 2 + 15) / 16 * 16;
   L.tab.alloc(m2l_tab_floats(KH), st);
-  k_m2l_tab<<<ceil_div(N * K + NOFF * KH + 64, 256), 256, 0, st>>>(KH, N, P, device_binomials(),
-                                                                    L.tab.p);
+  k_m2l_tab<<<ceil_div(N * K + NOFF * KH, 256), 256, 0, st>>>(KH, N, P, device_binomials(),
+                                                               L.tab.p);
   B2_LAUNCH_CHECK();
   L.steps.alloc(1, st);
   L.steps.zero(1);
-  const int tpt = 128 / chunk;
-  k_m2l_steps<<<ceil_div(ceil_div(L.ntgt, tpt), 128), 128, 0, st>>>(L.tstart.p, L.ntgt, tpt,
-                                                                    L.steps.p);
+  const long nst = ((long)L.ntgt + (long)R * L.T - 1) / ((long)R * L.T);
+  k_m2l_steps<<<ceil_div(nst, 128), 128, 0, st>>>(L.tstart.p, L.ntgt, R, L.T, L.steps.p);
   B2_LAUNCH_CHECK();
   // the temporaries above are freed (stream-ordered) when this returns
 }
@@ -850,7 +943,7 @@ int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long 
   const long nconv = (long)nboxes * ND * KH;
   k_mp_to_f32<<<ceil_div(nconv, 256), 256, 0, st>>>(mp, nboxes, P, ND, KH, mp32);
   B2_LAUNCH_CHECK();
-  const long ntiles = (L.ntgt + (128 >> ndsh) - 1) / (128 >> ndsh);
+  const long nst = (L.ntgt + (long)(128 >> ndsh) * L.T - 1) / ((long)(128 >> ndsh) * L.T);
   auto launch = [&](auto kern, uint32_t total, uint32_t tmem_cols, int threads) {
     // CTAs that can share an SM (tensor-memory columns and shared memory);
     // the shared memory request keeps more from being resident (a tensor
@@ -858,8 +951,8 @@ int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long 
     const int per_sm = std::max(1, std::min(512 / (int)tmem_cols, 232448 / (int)(total + 1024)));
     const size_t sm = std::max<size_t>(total, (size_t)(233472 / (per_sm + 1)) + 1024);
     set_smem_attr(kern, sm);
-    const int grid = (int)std::min<long>(ntiles, (long)nsm * per_sm);
-    kern<<<grid, threads, sm, st>>>(L.tbox.p, L.tstart.p, L.ent.p, (int)L.ntgt, ndsh, P,
+    const int grid = (int)std::min<long>(nst, (long)nsm * per_sm);
+    kern<<<grid, threads, sm, st>>>(L.tstart.p, L.ent.p, (int)L.ntgt, L.T, ndsh, P,
                                     reinterpret_cast<const float4*>(L.tab.p), boxsize, nlev,
                                     reinterpret_cast<const float4*>(mp32), lo, err_dev);
     B2_LAUNCH_CHECK();

@@ -6,16 +6,16 @@
 namespace b2 {
 
 // M2L targets (boxes of levels >= 2 with list-2 boxes and evaluation
-// points, grouped by their position in the parent box) and their list-2
-// entries: the input of the tensor-core kernel.
+// points, sorted by list-2 length and interleaved into super-tiles of
+// 128/ND x T targets) and their list-2 entries: the input of the
+// tensor-core kernel.
 struct M2LPairs {
-  DBuf<int> tbox;                   // box | level << 26
   DBuf<int> tstart;                 // ntgt + 1 offsets into ent
-  DBuf<int> ent;                    // source | offset index << 26
+  DBuf<int2> ent;                   // (source | offset index << 26, last-entry mark)
   DBuf<float> tab;                  // G (TF32 hi, lo) and the per-offset tables
-  DBuf<unsigned long long> steps;   // steps of all tiles (tensor-core work)
+  DBuf<unsigned long long> steps;   // steps of all super-tiles (tensor-core work)
   long ntgt = 0, npairs = 0;
-  int P = 0;
+  int P = 0, T = 1;
   bool usable = false;  // false: box indices do not fit the packed format or P too large
 };
 
