@@ -253,13 +253,22 @@ class ClockSampler:
         self.path = os.path.join("/tmp", f"b2fmm_clocks_{os.getpid()}.csv")
 
     def start(self):
+        """Starts sampling and returns once the first sample is written (at most
+        a few seconds), so that nvidia-smi's start-up, which holds driver locks
+        for a while, lies before the timed region."""
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-i", str(self.gpu), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -425,15 +434,16 @@ def main():
             raise RuntimeError(f"b2fmm_lfmm2d_dev ier={ier.value}")
 
     def timed(precision, steps, warmup, with_clocks=False):
+        # the clock sampler runs from before the warm-up to after the timed steps
+        sampler = ClockSampler(local) if with_clocks else None
+        if sampler:
+            sampler.start()
         for _ in range(warmup):
             step(precision)
         tis = np.zeros(8)
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
-        sampler = ClockSampler(local) if with_clocks else None
-        if sampler:
-            sampler.start()
         L0 = L.b2fmm_kernel_launches()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
