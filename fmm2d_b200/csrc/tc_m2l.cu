@@ -274,9 +274,12 @@ struct OT {
   static constexpr uint32_t SB = (uint32_t)N * K * 4;  // one B tile (hi or lo)
   static constexpr uint32_t A0 = 0;                  // A stages: [stage][hi, lo]
   static constexpr uint32_t B0 = OT_STAGES * 2 * SA; // G: [hi, lo]
-  static constexpr uint32_t UP = B0 + 2 * SB;        // float2 [NOFF][KH]: (-u)^k
-  static constexpr uint32_t UO = UP + NOFF * KH * 8; // float2 [NOFF][KH]: u^i
-  static constexpr uint32_t LGO = UO + NOFF * KH * 8;  // float [NOFF]: log|o|
+  // offset tables, rows of KH + 2 float2: the 16-byte pad spreads the rows of
+  // different offsets over all 8 groups of 16-byte shared-memory banks
+  static constexpr int TS = KH + 2;
+  static constexpr uint32_t UP = B0 + 2 * SB;        // float2 [NOFF][TS]: (-u)^k
+  static constexpr uint32_t UO = UP + NOFF * TS * 8; // float2 [NOFF][TS]: u^i
+  static constexpr uint32_t LGO = UO + NOFF * TS * 8;  // float [NOFF]: log|o|
   static constexpr uint32_t LGL = LGO + NOFF * 4;    // double [64]: log(box size) by level
   static constexpr uint32_t RING = LGL + 512;        // int [8][BUILDERS]: last-entry marks
   static constexpr uint32_t MISC = RING + 8 * BUILDERS * 4;  // mbarriers, tmem address, flags
@@ -290,7 +293,7 @@ struct OT {
 // float elements of the table image: G (hi, lo), then (-u)^k and u^i per
 // offset index (float2), then log|o|.
 __host__ __device__ constexpr long m2l_tab_floats(int KH) {
-  return 2L * ((2 * KH + 2 + 15) / 16 * 16) * (2 * KH) + 4L * NOFF * KH + NOFF;
+  return 2L * ((2 * KH + 2 + 15) / 16 * 16) * (2 * KH) + 4L * NOFF * (KH + 2) + NOFF;
 }
 
 // Round to TF32 (10 mantissa bits), to nearest with ties away from zero:
@@ -453,7 +456,7 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         if (part == 0) tmem_ld4(lane_base + (uint32_t)((x % OT_DBUF) * N + 2 * KH), z);
         tmem_wait_ld();
         const int op = oring_get(x);
-        const float4* uo = UO4 + (op * KH + C * part) / 2;
+        const float4* uo = UO4 + (op * L::TS + C * part) / 2;
 #pragma unroll
         for (int m = 0; m < NV; m++) {
           const float4 w = uo[m];  // u^i for two coefficients
@@ -515,7 +518,7 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         // t = h (-u)^k
         float4 t[NV];
         {
-          const float4* up = UP4 + (oi * KH + C * part) / 2;
+          const float4* up = UP4 + (oi * L::TS + C * part) / 2;
 #pragma unroll
           for (int m = 0; m < NV; m++) {
             const float4 w = up[m];  // (-u)^k for two coefficients
@@ -658,12 +661,18 @@ __global__ void k_m2l_tab(int KH, int N, int P, const double* __restrict__ binom
     out[(size_t)N * K + o] = lw;
     return;
   }
+  // tables: rows of TS = KH + 2 float2 (the last two are padding, zero)
+  const int TS = KH + 2;
   const int f = e - N * K;
-  if (f >= NOFF * KH) return;
+  if (f >= NOFF * TS) return;
   float2* up = reinterpret_cast<float2*>(out + 2L * N * K);
-  float2* uo = up + NOFF * KH;
-  float* lg = reinterpret_cast<float*>(uo + NOFF * KH);
-  const int oi = f / KH, k = f % KH;
+  float2* uo = up + NOFF * TS;
+  float* lg = reinterpret_cast<float*>(uo + NOFF * TS);
+  const int oi = f / TS, k = f % TS;
+  if (k >= KH) {
+    up[f] = uo[f] = make_float2(0.f, 0.f);
+    return;
+  }
   const int ox = oi / 7 - 3, oy = oi % 7 - 3;
   double2 p = make_double2(0.0, 0.0);
   double l = 0.0;
@@ -913,7 +922,7 @@ void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P,
   B2_LAUNCH_CHECK();
   const int KH = m2l_kh(P), K = 2 * KH, N = (2 * KH + 2 + 15) / 16 * 16;
   L.tab.alloc(m2l_tab_floats(KH), st);
-  k_m2l_tab<<<ceil_div(N * K + NOFF * KH, 256), 256, 0, st>>>(KH, N, P, device_binomials(),
+  k_m2l_tab<<<ceil_div(N * K + NOFF * (KH + 2), 256), 256, 0, st>>>(KH, N, P, device_binomials(),
                                                                L.tab.p);
   B2_LAUNCH_CHECK();
   L.steps.alloc(1, st);
