@@ -242,25 +242,72 @@ def fortran_layout(src, q, d, v):
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during timing."""
+    """SM clock and clock-event (throttle) reasons of the timed GPU, sampled
+    every 100 ms from before the warm-up to after the timed steps.  In-process
+    NVML reads (pynvml) in a background thread; the GPU is found by its UUID,
+    so the sample is of the device the process runs on whatever
+    CUDA_VISIBLE_DEVICES maps.  Falls back to an nvidia-smi subprocess when
+    pynvml is missing (its periodic queries hold driver locks for some
+    milliseconds, which shows in short timed regions)."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
+        self.thread = None
+        self.samples = []
         self.path = os.path.join("/tmp", f"b2fmm_clocks_{os.getpid()}.csv")
 
+    def _uuid(self):
+        try:
+            import torch
+            u = torch.cuda.get_device_properties(self.gpu).uuid
+            s = str(u)
+            return s if s.startswith("GPU-") else "GPU-" + s
+        except Exception:
+            return None
+
     def start(self):
-        """Starts sampling and returns once the first sample is written (at most
-        a few seconds), so that nvidia-smi's start-up, which holds driver locks
-        for a while, lies before the timed region."""
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            uid = self._uuid()
+            h = (nv.nvmlDeviceGetHandleByUUID(uid) if uid
+                 else nv.nvmlDeviceGetHandleByIndex(self.gpu))
+            self.nv, self.h = nv, h
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            self.stop_flag = threading.Event()
+
+            def loop():
+                while not self.stop_flag.is_set():
+                    try:
+                        mhz = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((mhz, [k for k, b in bits.items() if r & b]))
+                    except Exception:
+                        pass
+                    self.stop_flag.wait(0.1)
+
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.f = open(self.path, "w")
+            uid = self._uuid()
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-i", uid if uid else str(self.gpu), "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
             return
@@ -271,6 +318,19 @@ class ClockSampler:
             time.sleep(0.02)
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
+            if not self.samples:
+                return None
+            reasons = sorted({r for _, rs in self.samples for r in rs})
+            return {"sm_mhz": statistics.median([m for m, _ in self.samples]),
+                    "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(self.samples), "source": "nvml"}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -280,7 +340,6 @@ class ClockSampler:
             self.proc.kill()
         self.f.close()
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             p = [x.strip() for x in line.split(",")]
             if len(p) < 9:
@@ -290,14 +349,14 @@ class ClockSampler:
                 mx.append(float(p[2]))
             except ValueError:
                 continue
-            for nm, val in zip(names, p[5:9]):
+            for nm, val in zip(self.NAMES, p[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         os.unlink(self.path)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def max_over_ranks(x, dist, device):
