@@ -256,13 +256,36 @@ __global__ void __launch_bounds__(128) k_far_mixed(
       f[d] = L[(P - 1) * ND + d];
       f1[d] = f2[d] = make_double2(0, 0);
     }
-    for (int m = P - 2; m >= 0; m--) {
+    // Horner steps in groups of four whose coefficient loads are issued
+    // together (one load latency per group instead of per step)
+    auto step = [&](const double2 (&c)[ND]) {
 #pragma unroll
       for (int d = 0; d < ND; d++) {
         if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], zz), f1[d]);
         if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], zz), f[d]);
-        f[d] = cadd(cmul(f[d], zz), L[m * ND + d]);
+        f[d] = cadd(cmul(f[d], zz), c[d]);
       }
+    };
+    int m = P - 2;
+    for (; m >= 3; m -= 4) {
+      double2 c0[ND], c1[ND], c2[ND], c3[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        c0[d] = L[m * ND + d];
+        c1[d] = L[(m - 1) * ND + d];
+        c2[d] = L[(m - 2) * ND + d];
+        c3[d] = L[(m - 3) * ND + d];
+      }
+      step(c0);
+      step(c1);
+      step(c2);
+      step(c3);
+    }
+    for (; m >= 0; m--) {
+      double2 c0[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) c0[d] = L[m * ND + d];
+      step(c0);
     }
     double ri = 1.0 / r;
 #pragma unroll
@@ -289,13 +312,34 @@ __global__ void __launch_bounds__(128) k_far_mixed(
       f[d] = M[(P - 1) * ND + d];
       f1[d] = f2[d] = make_double2(0, 0);
     }
-    for (int m = P - 2; m >= 1; m--) {
+    auto mstep = [&](const double2 (&c)[ND]) {
 #pragma unroll
       for (int d = 0; d < ND; d++) {
         if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], w), f1[d]);
         if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], w), f[d]);
-        f[d] = cadd(cmul(f[d], w), M[m * ND + d]);
+        f[d] = cadd(cmul(f[d], w), c[d]);
       }
+    };
+    int m = P - 2;
+    for (; m >= 4; m -= 4) {
+      double2 c0[ND], c1[ND], c2[ND], c3[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        c0[d] = M[m * ND + d];
+        c1[d] = M[(m - 1) * ND + d];
+        c2[d] = M[(m - 2) * ND + d];
+        c3[d] = M[(m - 3) * ND + d];
+      }
+      mstep(c0);
+      mstep(c1);
+      mstep(c2);
+      mstep(c3);
+    }
+    for (; m >= 1; m--) {
+      double2 c0[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) c0[d] = M[m * ND + d];
+      mstep(c0);
     }
     double2 w2 = cmul(w, w);
 #pragma unroll
