@@ -99,6 +99,18 @@ void configure_mempool(int device) {
   done[device] = true;
 }
 
+// One long-lived non-blocking stream per device for the plans' own work
+// (construction, status reads, release).  A stream per plan, kept for the
+// plan's lifetime, made each new plan slower with the number of live plans
+// (1 ms for the first, ~25 ms after 256 in the stream-ordered allocator).
+cudaStream_t plan_stream(int device) {
+  static std::mutex mu;
+  static cudaStream_t streams[128] = {};
+  std::lock_guard<std::mutex> g(mu);
+  if (!streams[device]) B2_CHECK(cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking));
+  return streams[device];
+}
+
 namespace {
 
 using namespace lapk;
@@ -944,7 +956,7 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
 struct LapPlan {
   LapArgs a;                      // geometry and flags (density/output pointers unused)
   cudaStream_t st = nullptr;      // stream owning the buffers
-  bool own = false;               // st was created by the plan
+  bool own = false;               // st is the shared plan stream (not the caller's)
   int nd = 1, ndc = 1, P = 0, chunk = 1;
   long ns = 0, nt = 0;
   bool fc = false, fd = false, mixed = false;
@@ -1025,7 +1037,7 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   p.fc = a.charge != nullptr;
   p.fd = a.dipstr != nullptr;
   if (own_stream) {
-    B2_CHECK(cudaStreamCreateWithFlags(&p.st, cudaStreamNonBlocking));
+    p.st = plan_stream(dev);
     p.own = true;
     // the plan's stream starts after the work already queued on the caller's
     cudaEvent_t e;
@@ -1212,10 +1224,7 @@ void lap_plan_free(LapPlan* p) {
   bool own = p->own;
   if (own) cudaDeviceSynchronize();  // evaluations may have run on other streams
   delete p;                          // buffers are released on the plan's stream
-  if (own) {
-    cudaStreamSynchronize(st);
-    cudaStreamDestroy(st);
-  }
+  if (own) cudaStreamSynchronize(st);
 }
 
 int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
