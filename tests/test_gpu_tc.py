@@ -93,9 +93,9 @@ def test_mixed_tc_vs_direct_4_densities(gpu, tc_on):
 @pytest.mark.parametrize("eps", [0.1, 0.01, 1e-3, 1e-4, 1e-6, 3e-7])
 @pytest.mark.parametrize("kind", ["cfmm_nd1", "lfmm_nd4"])
 def test_tc_every_expansion_length(gpu, tc_on, eps, kind):
-    """All operator sizes of the offset-accumulating kernel (P = 4, 7, 10,
-    13, 19 -> 4, 8, 12, 16, 20 coefficients per half row) with 1 and 8
-    densities per tile row group; P = 21 (eps 3e-7) runs the CUDA-core M2L.
+    """All operator sizes of the tensor-core kernel (P = 4, 7, 10, 13, 19 ->
+    KH = 4, 8, 12, 16, 20 coefficients per row) with 1 and 8 densities per
+    row group; P = 21 (eps 3e-7) runs the CUDA-core M2L.
     The tensor-core result equals the CUDA-core FP32 M2L and the FP64 FMM to
     FP32 accuracy."""
     src, q, d, v = _cloud(11, 30000)
@@ -123,7 +123,11 @@ def test_tc_super_tiles(gpu, tc_on):
     targets per row group (T > 1), each row walks its targets' list-2
     entries back to back and flushes a target's locals after its last
     entry.  The result equals the FP64 FMM to FP32 accuracy, and the steps
-    issued stay within 2 % of the translations x densities / 128 rows."""
+    issued stay within 2 % of the translations x densities / 128 rows.
+    Accuracy against the CUDA-core FP32 M2L: the tensor cores truncate each
+    MMA's FP32 sum, and an accumulator kept across the offsets of a tile
+    made the error ~5x that of the FP32 M2L; per-step products summed with
+    round-to-nearest keep it within 2x."""
     n = 1_200_000
     src, q, d, v = _cloud(21, n)
     kw = dict(eps=1e-6, sources=src, charges=q, dipstr=d, dipvec=v, pg=2)
@@ -132,10 +136,17 @@ def test_tc_super_tiles(gpu, tc_on):
     out_tc = fmm.lfmm2d(**kw, precision="mixed")
     L.b2fmm_set_stats(0)
     st = fmm._lib.get_stats()
+    L.b2fmm_set_m2l_tensor_cores(0)
+    out_cc = fmm.lfmm2d(**kw, precision="mixed")
+    L.b2fmm_set_m2l_tensor_cores(1)
     out_64 = fmm.lfmm2d(**kw, precision="fp64")
-    assert out_tc.ier == 0 and out_64.ier == 0
+    assert out_tc.ier == 0 and out_cc.ier == 0 and out_64.ier == 0
     assert rel_l2(out_tc.pot, out_64.pot) < 1e-6
     assert rel_l2(out_tc.grad, out_64.grad) < 1e-6
+    for k in ("pot", "grad"):
+        e_tc = rel_l2(getattr(out_tc, k), getattr(out_64, k))
+        e_cc = rel_l2(getattr(out_cc, k), getattr(out_64, k))
+        assert e_tc < 2.0 * e_cc + 1e-9, (k, e_tc, e_cc)
     rows = st["m2l_pairs"] * 2  # lfmm2d: 2 Cauchy densities per target
     assert st["m2l_tc_steps"] >= rows / 128
     assert st["m2l_tc_steps"] <= 1.02 * rows / 128 + 4 * 148
