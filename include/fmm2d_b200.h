@@ -307,7 +307,8 @@ uint64_t b2fmm_kernel_launches(void);
  * thread; b2fmm_get_stats copies up to n of: nboxes, nlevels, nleaves,
  * nterms+1, P2P pairs, M2L translations, M2P evaluations, P2L sources,
  * evaluation points, tree build ms, FMM ms after the tree, Cauchy densities,
- * tensor-core M2L offset steps (tiles x offsets; 0 when not used). */
+ * tensor-core M2L steps (128-row MMA steps over all super-tiles; 0 when not
+ * used). */
 void b2fmm_set_stats(int on);
 void b2fmm_get_stats(double* out, int n);
 
