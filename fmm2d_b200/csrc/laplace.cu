@@ -203,8 +203,9 @@ __global__ void __launch_bounds__(64) k_p2m(TV t, int first, int n, const double
 // z0 = child - parent; t_j = h_j (r1/z0)^j;
 // H_0 = t_0, H_i = (-t_0/i + sum_{j=1..i} t_j C(i-1, j-1)) (z0/r2)^i
 // One warp per parent: the lanes first stage t for all four children at
-// once (lane = (child, j)), so the children's loads overlap, then each lane
-// sums its coefficients over the children.
+// once (lane = (child, j)), so the children's loads overlap, then lane =
+// (child, coefficient group) forms the child's terms and shuffles sum the
+// children.
 // ---------------------------------------------------------------------------
 template <int ND>
 __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
@@ -242,41 +243,48 @@ __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
         T[(c * P + j) * ND + d] = has ? cmul(mp[((size_t)k * P + j) * ND + d], a) : make_double2(0, 0);
     }
     __syncwarp();
+    // lane = (child c, group g): the child's contributions to the coefficients
+    // i = g, g + 8, ... (the triangular sums over j are spread over 32 lanes
+    // instead of P), summed over the four children by two xor shuffles
+    const int c = lane >> 3, g = lane & 7;
+    const double2 w2 = W2[c];
+    const double2* tc = T + (size_t)c * P * ND;
+    for (int i0 = 0; i0 < P; i0 += 8) {
+      const int i = i0 + g;
+      double2 v[ND];
 #pragma unroll
-    for (int s = 0; s < 2; s++) {
-      int i = lane + 32 * s;
-      if (i >= P) break;
-      double2 acc[ND];
+      for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
+      if (i == 0) {
 #pragma unroll
-      for (int d = 0; d < ND; d++) acc[d] = make_double2(0, 0);
-      const double* crow = binom + (size_t)(i > 0 ? i - 1 : 0) * BINOM_N;
-      for (int c = 0; c < 4; c++) {
-        if (i == 0) {
-#pragma unroll
-          for (int d = 0; d < ND; d++) acc[d] = cadd(acc[d], T[c * P * ND + d]);
-          continue;
-        }
-        const double2 w2 = W2[c];
-        if (w2.x == 0.0 && w2.y == 0.0) continue;  // child without sources
-        const double2* tc = T + (size_t)c * P * ND;
-        double2 v[ND];
+        for (int d = 0; d < ND; d++) v[d] = tc[d];
+      } else if (i < P && !(w2.x == 0.0 && w2.y == 0.0)) {  // a child without sources adds 0
+        const double* crow = binom + (size_t)(i - 1) * BINOM_N;
 #pragma unroll
         for (int d = 0; d < ND; d++) v[d] = make_double2(-tc[d].x / i, -tc[d].y / i);
         for (int j = 1; j <= i; j++) {
-          double cb = crow[j - 1];
+          const double cb = crow[j - 1];
 #pragma unroll
           for (int d = 0; d < ND; d++) {
-            double2 tj = tc[j * ND + d];
+            const double2 tj = tc[j * ND + d];
             v[d].x += tj.x * cb;
             v[d].y += tj.y * cb;
           }
         }
-        double2 bi_ = cpow_int(w2, i);
+        const double2 bi_ = cpow_int(w2, i);
 #pragma unroll
-        for (int d = 0; d < ND; d++) cfma(acc[d], v[d], bi_);
+        for (int d = 0; d < ND; d++) v[d] = cmul(v[d], bi_);
       }
 #pragma unroll
-      for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = acc[d];
+      for (int d = 0; d < ND; d++) {
+        v[d].x += __shfl_xor_sync(~0u, v[d].x, 8);
+        v[d].y += __shfl_xor_sync(~0u, v[d].y, 8);
+        v[d].x += __shfl_xor_sync(~0u, v[d].x, 16);
+        v[d].y += __shfl_xor_sync(~0u, v[d].y, 16);
+      }
+      if (c == 0 && i < P) {
+#pragma unroll
+        for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = v[d];
+      }
     }
   }
 }
