@@ -498,7 +498,8 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
 // step 5: L2L (laprouts2d.f:1020-1123), z0 = child - parent:
 // t_j = l_j (z0/r1)^j, L_i += (sum_{j>=i} t_j C(j, i)) (r2/z0)^i
 // One warp per parent: lanes stage t for all four children at once (lane =
-// (child, j)), then each lane produces one (child, i) coefficient.
+// (child, j)), then each lane produces (child, i) coefficients, dealt so
+// that the lanes' work is balanced.
 // ---------------------------------------------------------------------------
 template <int ND>
 __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int P,
@@ -528,8 +529,12 @@ __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int P,
       for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(lo[((size_t)b * P + j) * ND + d], a);
     }
     __syncwarp();
-    for (int e = lane; e < 4 * P; e += 32) {
-      const int c = e / P, i = e % P;
+    // items (child, i) cost P - i: dealt in decreasing cost, snaking over the
+    // lanes, so that the lanes' totals come out nearly equal
+    for (int r = 0; r * 32 < 4 * P; r++) {
+      const int e = r * 32 + ((r & 1) ? 31 - lane : lane);
+      if (e >= 4 * P) continue;
+      const int c = e & 3, i = e >> 2;
       const int k = c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
       double2 v[ND];
 #pragma unroll
