@@ -800,12 +800,14 @@ __global__ void k_gather_dens(int fe, int nd, int ndc, const int* __restrict__ p
 
 // Sorted Cauchy results -> caller layout and order (lfmm2d.f:169-223,
 // rfmm2d.f:158-212; cfmm2d.f:399-432 for the inverse permutation).
-__global__ void k_unpack(int fe, int nd, int ndc, int ifl, const int* __restrict__ perm, long n,
+__global__ void k_unpack(int fe, int nd, int ndc, int ifl, const int* __restrict__ inv, long n,
                          const double2* __restrict__ P1, const double2* __restrict__ G1,
                          const double2* __restrict__ H1, double* pot, double* grad, double* hess) {
-  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  size_t i = perm[k];
+  // one output point per thread (caller order), read from its tree position:
+  // the writes are contiguous, the reads gathered
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t k = inv[i];
   for (int j = 0; j < nd; j++) {
     if (fe == FE_CAUCHY) {
       ((double2*)pot)[i * nd + j] = P1[k * ndc + j];
@@ -840,6 +842,12 @@ __global__ void k_unpack(int fe, int nd, int ndc, int ifl, const int* __restrict
       }
     }
   }
+}
+
+// inv[perm[k]] = k: tree position of every caller-order point
+__global__ void k_inverse_perm(const int* __restrict__ perm, long n, int* __restrict__ inv) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k < n) inv[perm[k]] = (int)k;
 }
 
 // Work counts for the roofline accounting (enabled by set_stats).
@@ -980,6 +988,7 @@ struct LapPlan {
   DBuf<double> dbs;
   DBuf<double2> xs, xt, qs, ds, ps, gs, hs, pt, gt, ht, mp, lo;
   DBuf<int> err;
+  DBuf<int> inv_s, inv_t;  // tree position of every caller-order source / target
   MixedData MD;
   TV tv{};
   cudaEvent_t ev[8] = {};
@@ -1103,9 +1112,15 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   p.xs.alloc(p.ns, st);
   k_gather_pts<<<ceil_div(p.ns, 256), 256, 0, st>>>(a.src, T.isrc.p, p.ns, p.xs.p);
   B2_LAUNCH_CHECK();
+  p.inv_s.alloc(p.ns, st);
+  k_inverse_perm<<<ceil_div(p.ns, 256), 256, 0, st>>>(T.isrc.p, p.ns, p.inv_s.p);
+  B2_LAUNCH_CHECK();
   if (p.nt > 0) {
     p.xt.alloc(p.nt, st);
     k_gather_pts<<<ceil_div(p.nt, 256), 256, 0, st>>>(a.trg, T.itarg.p, p.nt, p.xt.p);
+    B2_LAUNCH_CHECK();
+    p.inv_t.alloc(p.nt, st);
+    k_inverse_perm<<<ceil_div(p.nt, 256), 256, 0, st>>>(T.itarg.p, p.nt, p.inv_t.p);
     B2_LAUNCH_CHECK();
   }
   const size_t nsd = (size_t)p.ns * p.ndc, ntd = (size_t)p.nt * p.ndc;
@@ -1207,12 +1222,12 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
     d0 += ND;
   }
   if (a.ifpgh > 0) {
-    k_unpack<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpgh, T.isrc.p, ns, p.ps.p,
+    k_unpack<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpgh, p.inv_s.p, ns, p.ps.p,
                                                 p.gs.p, p.hs.p, pot, grad, hess);
     B2_LAUNCH_CHECK();
   }
   if (a.ifpghtarg > 0 && nt > 0) {
-    k_unpack<<<ceil_div(nt, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpghtarg, T.itarg.p, nt, p.pt.p,
+    k_unpack<<<ceil_div(nt, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpghtarg, p.inv_t.p, nt, p.pt.p,
                                                 p.gt.p, p.ht.p, pottarg, gradtarg, hesstarg);
     B2_LAUNCH_CHECK();
   }
