@@ -116,13 +116,13 @@ __global__ void k_bbox_final(const double4* part, int np, double* root) {
 // the child's, cx +/- bs_child/2 (tree_routs2d.f:33-39).
 // ---------------------------------------------------------------------------
 __global__ void k_keys(const double* __restrict__ xy, long n, const double* __restrict__ root,
-                       uint64_t* khi, uint64_t* klo, int* idx) {
+                       int nkey, uint64_t* khi, uint64_t* klo, int* idx) {
   long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   double x = xy[2 * i], y = xy[2 * i + 1];
   double cx = root[0], cy = root[1], bs = root[2];
   uint64_t hi = 0, lo = 0;
-  for (int lev = 1; lev <= NLMAX; lev++) {
+  for (int lev = 1; lev <= nkey; lev++) {
     bs = bs / 2;  // boxsize(lev) = boxsize(lev-1)/2
     double h = bs / 2;
     int sx = (x - cx < 0) ? 0 : 1;
@@ -159,7 +159,9 @@ void sort_by_key(const double* xy, long n, const double* root, bool deep, DBuf<u
   khi.alloc(n, st);
   klo.alloc(n, st);
   idx.alloc(n, st);
-  k_keys<<<ceil_div(n, 256), 256, 0, st>>>(xy, n, root, khi.p, klo.p, idx.p);
+  // a tree of at most 32 levels reads only the first key word; deeper trees
+  // are rebuilt with deep = true
+  k_keys<<<ceil_div(n, 256), 256, 0, st>>>(xy, n, root, deep ? NLMAX : 32, khi.p, klo.p, idx.p);
   B2_LAUNCH_CHECK();
   size_t tb = 0;
   DBuf<char> tmp(st);
@@ -182,7 +184,11 @@ void sort_by_key(const double* xy, long n, const double* root, bool deep, DBuf<u
     B2_CHECK(cub::DeviceRadixSort::SortPairs(tmp.p, tb, tmpk.p, khi_out.p, tmpi.p, idx_out.p,
                                              (int)n, 0, 64, st));
   }
-  k_gather_u64<<<ceil_div(n, 256), 256, 0, st>>>(klo.p, idx_out.p, n, klo_out.p);
+  if (deep) {
+    k_gather_u64<<<ceil_div(n, 256), 256, 0, st>>>(klo.p, idx_out.p, n, klo_out.p);
+  } else {
+    B2_CHECK(cudaMemsetAsync(klo_out.p, 0, sizeof(uint64_t) * n, st));
+  }
   B2_LAUNCH_CHECK();
 }
 
