@@ -616,6 +616,9 @@ void* b2fmm_tree_build(const double* sources_dev, int64_t ns, const double* targ
     h = new TreeHandle();
     build_device_tree(h->T, sources_dev, ns, targ_dev, nt, idivflag, ndiv, nlmax,
                       cudaStreamPerThread);
+    // the lists are still being written on the stream; b2fmm_tree_get copies
+    // synchronously
+    B2_CHECK(cudaStreamSynchronize(cudaStreamPerThread));
     *nlevels = h->T.nlevels;
     *nboxes = h->T.nboxes;
     return (int)IER_OK;

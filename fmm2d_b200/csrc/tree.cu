@@ -1152,7 +1152,11 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   DBuf<TreeCtl> ctl(st);
   ctl.alloc(1, st);
   const int grid = tree_grid();
-  TreeCtl* hc = (TreeCtl*)pinned_bytes(sizeof(TreeCtl));
+  // control block and root box read back together after each build attempt
+  char* hbuf = (char*)pinned_bytes(sizeof(TreeCtl) + 4 * sizeof(double));
+  TreeCtl* hc = (TreeCtl*)hbuf;
+  double* hr = (double*)(hbuf + sizeof(TreeCtl));
+  static_assert(sizeof(TreeCtl) % sizeof(double) == 0, "root after the control block");
   for (;;) {
     alloc_boxes(T, cap);
     DBuf<double2> sc(st);
@@ -1189,6 +1193,7 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
     B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(TB_THREADS),
                                          args, 0, st));
     B2_CHECK(cudaMemcpyAsync(hc, ctl.p, sizeof(TreeCtl), cudaMemcpyDeviceToHost, st));
+    B2_CHECK(cudaMemcpyAsync(hr, T.root.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     B2_CHECK(cudaStreamSynchronize(st));
     if (hc->status == TB_DEEP && !T.deep_sorted) {
       // levels beyond 32 need the points ordered by all key digits
@@ -1211,13 +1216,8 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   T.llast.assign(hc->llast, hc->llast + T.nlevels + 1);
   T.boxsize.assign(hc->bs, hc->bs + T.nlevels + 1);
   T.bs0 = hc->bs[0];
-  {
-    double* hr = (double*)pinned_bytes(3 * sizeof(double));
-    B2_CHECK(cudaMemcpyAsync(hr, T.root.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    B2_CHECK(cudaStreamSynchronize(st));
-    T.cx0 = hr[0];
-    T.cy0 = hr[1];
-  }
+  T.cx0 = hr[0];
+  T.cy0 = hr[1];
   // interaction lists (boxsize(nlevels+1) for the leaf tests is in the control block)
   int nb = T.nboxes;
   T.nlist1.alloc(nb, st);
@@ -1232,7 +1232,8 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
                                              T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p,
                                              T.nlist4.p, T.list4.p);
   B2_LAUNCH_CHECK();
-  B2_CHECK(cudaStreamSynchronize(st));
+  // no synchronisation: the lists are read by later work on st; the control
+  // block is released (stream-ordered) after k_lists has read its box sizes
 }
 
 }  // namespace b2
