@@ -701,24 +701,58 @@ __device__ bool colleagues_hashed(TreeCtl* C, BoxPtrs& B, const BoxHash& H, int 
     }
     const uint64_t pk = B.pkey[b];
     const long ix = compact_bits(pk), iy = compact_bits(pk >> 1), side = 1L << l;
+    // the 3x3 neighbourhood (q = 3 (dy + 1) + dx + 1): the eight lookups are
+    // independent, so their probes advance together, one round of loads at a
+    // time (st: 0 probing, 1 found at slot hs, 2 absent; q = 4 is b itself)
+    uint64_t nk[9], hk[9];
+    unsigned hs[9];
+    int st[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+      const long x = ix + q % 3 - 1, y = iy + q / 3 - 1;
+      const bool in = !(x < 0 || y < 0 || x >= side || y >= side);
+      nk[q] = in ? ((spread_bits((uint32_t)y) << 1) | spread_bits((uint32_t)x)) : 0;
+      hk[q] = hash_key(l, nk[q]);
+      hs[q] = hash_slot(hk[q], H.mask);
+      st[q] = !in ? 2 : (q == 4 ? 1 : 0);
+    }
+    for (unsigned it = 0; it <= H.mask; it++) {
+      unsigned long long v[9];
+#pragma unroll
+      for (int q = 0; q < 9; q++) v[q] = st[q] == 0 ? H.key[hs[q]] : 0ull;
+      bool more = false;
+#pragma unroll
+      for (int q = 0; q < 9; q++) {
+        if (st[q] != 0) continue;
+        if (v[q] == hk[q]) {
+          st[q] = 1;
+        } else if (v[q] == 0ull) {
+          st[q] = 2;
+        } else {
+          hs[q] = (hs[q] + 1) & H.mask;
+          more = true;
+        }
+      }
+      if (!more) break;
+    }
+    int fbx[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) fbx[q] = q == 4 ? b : (st[q] == 1 ? H.box[hs[q]] : -1);
+    // the found neighbours in key order
     uint64_t fk[9];
     int fb[9], cnt = 0;
-    for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) {
-        const long x = ix + dx, y = iy + dy;
-        if (x < 0 || y < 0 || x >= side || y >= side) continue;
-        const uint64_t nk = (spread_bits((uint32_t)y) << 1) | spread_bits((uint32_t)x);
-        const int nbx = (dx == 0 && dy == 0) ? b : hash_find(H, hash_key(l, nk));
-        if (nbx < 0) continue;
-        int q = cnt++;
-        while (q > 0 && fk[q - 1] > nk) {
-          fk[q] = fk[q - 1];
-          fb[q] = fb[q - 1];
-          q--;
-        }
-        fk[q] = nk;
-        fb[q] = nbx;
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+      if (st[q] != 1) continue;
+      int r = cnt++;
+      while (r > 0 && fk[r - 1] > nk[q]) {
+        fk[r] = fk[r - 1];
+        fb[r] = fb[r - 1];
+        r--;
       }
+      fk[r] = nk[q];
+      fb[r] = fbx[q];
+    }
     for (int q = 0; q < 9; q++) cl[q] = q < cnt ? fb[q] : -1;
     B.ncoll[b] = cnt;
   }
