@@ -219,6 +219,7 @@ BoxPtrs ptrs(DeviceTree& T) {
 constexpr int TB_MAXG = 1024;    // most blocks of the build kernel
 constexpr int TB_THREADS = 512;  // threads per block (one block per SM)
 constexpr int TB_GROUPS = 8;     // first-level arrival counters of the grid barrier
+constexpr int TB_BIG = 16384;    // points of a refined box split by a warp
 struct TreeCtl {
   int nboxes, nlevels, cap, status;
   int lfirst[NLMAX + 2], llast[NLMAX + 2];
@@ -412,6 +413,58 @@ __device__ void split_children(BoxPtrs& B, int b, int lev_child, const uint64_t*
   for (int j = 0; j < 4; j++) {
     B.srng[cc[j]] = make_int2(bs_[j], bs_[j + 1]);
     B.trng[cc[j]] = make_int2(bt_[j], bt_[j + 1]);
+  }
+}
+
+// split_children by one warp, for refined boxes with many points: lanes
+// 0..29 run the six searches as 6-way searches (5 probes per search and
+// round, combined by a ballot), log_6 instead of log_2 rounds of dependent
+// loads.  Each search ends at the same boundary as the binary search.
+__device__ void split_children_warp(BoxPtrs& B, int b, int lev_child, const uint64_t* skhi,
+                                    const uint64_t* sklo, const uint64_t* tkhi,
+                                    const uint64_t* tklo) {
+  const int lane = threadIdx.x & 31, q = lane / 5, k = lane % 5;
+  const int2 rs = B.srng[b], rt = B.trng[b];
+  int lo = 0, hi = 0;
+  if (q < 6) {
+    lo = q < 3 ? rs.x : rt.x;
+    hi = q < 3 ? rs.y : rt.y;
+  }
+  const int t = (q % 3) + 1;
+  for (;;) {
+    const int n = hi - lo;
+    const bool active = n > 0;
+    if (!__any_sync(~0u, active)) break;
+    bool pred = false;
+    if (active) {
+      const int p = lo + (int)(((long long)n * (k + 1)) / 6);  // in [lo, hi)
+      const int dg = q < 3 ? key_digit(skhi[p], sklo[p], lev_child)
+                           : key_digit(tkhi[p], tklo[p], lev_child);
+      pred = dg >= t;
+    }
+    const unsigned m = __ballot_sync(~0u, pred);
+    if (active) {
+      const unsigned gm = (m >> (q * 5)) & 0x1Fu;
+      const int ks = gm ? __ffs(gm) - 1 : 5;  // first probe at or past the boundary
+      const int nhi = ks < 5 ? lo + (int)(((long long)n * (ks + 1)) / 6) : hi;
+      const int nlo = ks > 0 ? lo + (int)(((long long)n * ks) / 6) + 1 : lo;
+      lo = nlo;
+      hi = nhi;
+    }
+  }
+  int bd[6];
+#pragma unroll
+  for (int j = 0; j < 6; j++) bd[j] = __shfl_sync(~0u, lo, j * 5);
+  if (lane == 0) {
+    const int4 ch = B.child[b];
+    const int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    const int bs_[5] = {rs.x, bd[0], bd[1], bd[2], rs.y};
+    const int bt_[5] = {rt.x, bd[3], bd[4], bd[5], rt.y};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      B.srng[cc[j]] = make_int2(bs_[j], bs_[j + 1]);
+      B.trng[cc[j]] = make_int2(bt_[j], bt_[j + 1]);
+    }
   }
 }
 
@@ -789,6 +842,8 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
   __shared__ int wsum[32];
   __shared__ int red[2];
   __shared__ int newf[NLMAX + 2];
+  __shared__ int bigl[TB_THREADS];  // refined boxes of the chunk split by warps
+  __shared__ int nbig;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gs = gridDim.x * blockDim.x;
   const int cap = C->cap;
   BoxPtrs cur = B, alt = S;
@@ -827,6 +882,10 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
       return;
     }
     const double bsc = C->bs[lev] / 2;
+    // boxes with many points are split by a warp each after the loop (their
+    // binary searches would be long chains of dependent loads)
+    if (threadIdx.x == 0) nbig = 0;
+    __syncthreads();
     int run = pre;
     for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
       const int i = i0 + threadIdx.x;
@@ -834,10 +893,24 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
       int s;
       const int r = block_excl_scan(fl, wsum, &s);
       if (fl) {
-        create_children(cur, f + i, nb + 4 * (run + r), bsc, lev + 1, 0);
-        split_children(cur, f + i, lev + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
+        const int b = f + i;
+        create_children(cur, b, nb + 4 * (run + r), bsc, lev + 1, 0);
+        const int2 rs = cur.srng[b], rt = cur.trng[b];
+        int slot = -1;
+        if (rs.y - rs.x + rt.y - rt.x > TB_BIG) {
+          slot = atomicAdd(&nbig, 1);
+          if (slot < TB_THREADS) bigl[slot] = b;
+        }
+        if (slot < 0 || slot >= TB_THREADS)
+          split_children(cur, b, lev + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
       }
       run += s;
+    }
+    __syncthreads();
+    {
+      const int nw = min(nbig, TB_THREADS);
+      for (int w = threadIdx.x >> 5; w < nw; w += TB_THREADS / 32)
+        split_children_warp(cur, bigl[w], lev + 1, K.skhi, K.sklo, K.tkhi, K.tklo);
     }
     if (gt == 0) {
       C->bs[lev + 1] = bsc;
