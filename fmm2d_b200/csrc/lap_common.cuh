@@ -23,6 +23,18 @@ __device__ __forceinline__ double2 cpow_int(double2 w, int e) {
 
 __device__ __forceinline__ double2 cneg(double2 a) { return make_double2(-a.x, -a.y); }
 
+// Asynchronous 16-byte copy global -> shared (both 16-byte aligned); the
+// issuing thread's copies are complete after cp_async_wait_all().
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+__device__ __forceinline__ int child_of(int4 ch, int c) {
+  return c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
+}
+
 // Box and list arrays of the device tree, passed by value to kernels.
 struct TV {
   const double2* center;

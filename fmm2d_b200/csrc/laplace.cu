@@ -124,34 +124,62 @@ using namespace lapk;
 // step 1: P2M (laprouts2d.f:84-282) at leaves of level >= 2; every other leaf
 // gets a zero expansion so that list 2 / list 3 reads are well defined.
 // m_0 += q,  m_n += -q w^n / n + (d/r) w^(n-1),  w = (x - c) / r
+// A warp takes 32 of its boxes at a time (stride = the grid's warps): each
+// lane loads one box's child count, level, sources and centre, ballots mark
+// the leaves, and the warp then works through them with the box data
+// shuffled from the lane that loaded it (one round of loads per 32 boxes
+// instead of a chain of rounds per box).
 template <int ND>
 __global__ void __launch_bounds__(64) k_p2m(TV t, int first, int n, const double2* __restrict__ xs,
                                             Dens D, int P, double2* __restrict__ mp) {
   extern __shared__ double2 smem[];
-  WARP_LOOP(n) {
-    double2* W = smem + (size_t)wib * (32 * P + 64 * ND);
-    double2* Q = W + 32 * P;
-    double2* Dd = Q + 32 * ND;
-    int b = first + bi;
-    if (t.nchild[b] != 0) continue;
-    double2 acc[2][ND];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  double2* W = smem + (size_t)wib * (32 * P + 64 * ND);
+  double2* Q = W + 32 * P;
+  double2* Dd = Q + 32 * ND;
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
+    const int mine = base + lane * nw;
+    int nc = 1, lev = 0;
+    int2 sr = make_int2(0, 0);
+    double2 cen = make_double2(0, 0);
+    if (mine < n) {
+      const int b = first + mine;
+      nc = t.nchild[b];
+      lev = t.level[b];
+      sr = t.srng[b];
+      cen = t.center[b];
+    }
+    const bool work = nc == 0 && lev >= 2 && sr.y > sr.x;
+    unsigned zm = __ballot_sync(~0u, mine < n && nc == 0 && !work);
+    unsigned wm = __ballot_sync(~0u, mine < n && work);
+    while (zm) {
+      const int src = __ffs(zm) - 1;
+      zm &= zm - 1;
+      const size_t b = (size_t)first + base + src * nw;
+      for (int e = lane; e < P * ND; e += 32) mp[b * P * ND + e] = make_double2(0, 0);
+    }
+    while (wm) {
+      const int src = __ffs(wm) - 1;
+      wm &= wm - 1;
+      const int b = first + base + src * nw;
+      const int2 srb = make_int2(__shfl_sync(~0u, sr.x, src), __shfl_sync(~0u, sr.y, src));
+      const double2 c = make_double2(__shfl_sync(~0u, cen.x, src), __shfl_sync(~0u, cen.y, src));
+      const double r = t.boxsize[__shfl_sync(~0u, lev, src)];
+      const double ri = 1.0 / r;
+      double2 acc[2][ND];
 #pragma unroll
-    for (int s = 0; s < 2; s++)
+      for (int s = 0; s < 2; s++)
 #pragma unroll
-      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
-    int lev = t.level[b];
-    int2 sr = t.srng[b];
-    if (lev >= 2 && sr.y > sr.x) {
-      double r = t.boxsize[lev];
-      double ri = 1.0 / r;
-      double2 c = t.center[b];
-      for (int s0 = sr.x; s0 < sr.y; s0 += 32) {
-        int m = min(32, sr.y - s0);
+        for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+      for (int s0 = srb.x; s0 < srb.y; s0 += 32) {
+        const int m = min(32, srb.y - s0);
         __syncwarp();
         if (lane < m) {
-          int j = s0 + lane;
-          double2 x = xs[j];
-          double2 w = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
+          const int j = s0 + lane;
+          const double2 x = xs[j];
+          const double2 w = make_double2((x.x - c.x) / r, (x.y - c.y) / r);
           double2 pw = make_double2(1.0, 0.0);
           for (int k = 0; k < P; k++) {
             W[lane * P + k] = pw;
@@ -167,17 +195,17 @@ __global__ void __launch_bounds__(64) k_p2m(TV t, int first, int n, const double
         __syncwarp();
 #pragma unroll
         for (int s = 0; s < 2; s++) {
-          int k = lane + 32 * s;
+          const int k = lane + 32 * s;
           if (k >= P) break;
           if (k == 0) {
             for (int j = 0; j < m; j++)
 #pragma unroll
               for (int d = 0; d < ND; d++) acc[s][d] = cadd(acc[s][d], Q[j * ND + d]);
           } else {
-            double mik = -1.0 / k;
+            const double mik = -1.0 / k;
             for (int j = 0; j < m; j++) {
-              double2 wk = W[j * P + k], wk1 = W[j * P + k - 1];
-              double2 cq = cscale(wk, mik);
+              const double2 wk = W[j * P + k], wk1 = W[j * P + k - 1];
+              const double2 cq = cscale(wk, mik);
 #pragma unroll
               for (int d = 0; d < ND; d++) {
                 cfma(acc[s][d], Q[j * ND + d], cq);
@@ -187,103 +215,156 @@ __global__ void __launch_bounds__(64) k_p2m(TV t, int first, int n, const double
           }
         }
       }
-    }
 #pragma unroll
-    for (int s = 0; s < 2; s++) {
-      int k = lane + 32 * s;
-      if (k >= P) break;
+      for (int s = 0; s < 2; s++) {
+        const int k = lane + 32 * s;
+        if (k >= P) break;
 #pragma unroll
-      for (int d = 0; d < ND; d++) mp[((size_t)b * P + k) * ND + d] = acc[s][d];
+        for (int d = 0; d < ND; d++) mp[((size_t)b * P + k) * ND + d] = acc[s][d];
+      }
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// Parents of a level, found without a round of loads per box: a warp takes
+// 32 of its boxes at a time (stride = the grid's warps, so the boxes are
+// dealt as by a warp-per-box loop), each lane loads one box's child count,
+// centre and children, a ballot marks the parents, and the warp then works
+// through them with the box data shuffled from the lane that loaded it.
+// ---------------------------------------------------------------------------
+struct ParentScan {
+  int nchild;
+  int4 child;
+  double2 center;
+  int2 srng, trng;
+};
+
+__device__ __forceinline__ ParentScan scan_box(const TV& t, int b, bool want_eval) {
+  ParentScan s;
+  s.nchild = t.nchild[b];
+  s.child = t.child[b];
+  s.center = t.center[b];
+  if (want_eval) {
+    s.srng = t.srng[b];
+    s.trng = t.trng[b];
+  }
+  return s;
+}
+
+__device__ __forceinline__ double2 shfl_d2(double2 v, int src) {
+  return make_double2(__shfl_sync(~0u, v.x, src), __shfl_sync(~0u, v.y, src));
+}
+__device__ __forceinline__ int4 shfl_i4(int4 v, int src) {
+  return make_int4(__shfl_sync(~0u, v.x, src), __shfl_sync(~0u, v.y, src),
+                   __shfl_sync(~0u, v.z, src), __shfl_sync(~0u, v.w, src));
 }
 
 // ---------------------------------------------------------------------------
 // step 3: M2M (laprouts2d.f:905-1015) from the children with sources.
 // z0 = child - parent; t_j = h_j (r1/z0)^j;
 // H_0 = t_0, H_i = (-t_0/i + sum_{j=1..i} t_j C(i-1, j-1)) (z0/r2)^i
-// One warp per parent: the lanes first stage t for all four children at
-// once (lane = (child, j)), so the children's loads overlap, then lane =
-// (child, coefficient group) forms the child's terms and shuffles sum the
-// children.
+// One warp per parent: one round of loads brings the children's boxes and
+// (by cp.async, lane = (child, j)) all four children's coefficients into
+// shared memory; the lanes scale them to t, then lane = (child, coefficient
+// group) forms the child's terms and shuffles sum the children.
 // ---------------------------------------------------------------------------
 template <int ND>
-__global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
+__global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int lev, int P,
                                              const double* __restrict__ binom,
                                              double2* __restrict__ mp) {
   extern __shared__ double2 smem[];
-  WARP_LOOP(n) {
-    // per warp: t[child][j][density] (zero for children without sources),
-    // then z0 / r2 of each child
-    double2* T = smem + (size_t)wib * (4 * P * ND + 4);
-    double2* W2 = T + 4 * P * ND;
-    int b = first + bi;
-    if (t.nchild[b] == 0) continue;
-    int lev = t.level[b];
-    double r2 = t.boxsize[lev], r1 = t.boxsize[lev + 1];
-    double2 c2 = t.center[b];
-    int4 ch = t.child[b];
-    __syncwarp();
-    for (int e = lane; e < 4 * P; e += 32) {
-      const int c = e / P, j = e % P;
-      const int k = c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
-      const bool has = t.srng[k].y > t.srng[k].x;
-      double2 a = make_double2(0, 0);
-      if (has) {
-        double2 c1 = t.center[k];
-        double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
-        double2 w1 = crcp(make_double2(z0.x / r1, z0.y / r1));
-        a = cpow_int(w1, j);
-        if (j == 0) W2[c] = make_double2(z0.x / r2, z0.y / r2);
-      } else if (j == 0) {
-        W2[c] = make_double2(0, 0);
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const double r2 = t.boxsize[lev], r1 = t.boxsize[lev + 1];
+  // per warp: t[child][j][density], then r1 / z0 and z0 / r2 of each child
+  // (both 0 for a child without sources)
+  double2* T = smem + (size_t)wib * (4 * P * ND + 8);
+  double2* W1 = T + 4 * P * ND;
+  double2* W2 = W1 + 4;
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
+    const int mine = base + lane * nw;
+    ParentScan s{};
+    if (mine < n) s = scan_box(t, first + mine, false);
+    unsigned pm = __ballot_sync(~0u, mine < n && s.nchild != 0);
+    while (pm) {
+      const int src = __ffs(pm) - 1;
+      pm &= pm - 1;
+      const int b = first + base + src * nw;
+      const double2 c2 = shfl_d2(s.center, src);
+      const int4 ch = shfl_i4(s.child, src);
+      __syncwarp();  // the previous parent's reads of T are done
+      for (int e = lane; e < 4 * P; e += 32) {
+        const int c = e / P, j = e - c * P;
+        const int k = child_of(ch, c);
+#pragma unroll
+        for (int d = 0; d < ND; d++) cp_async16(&T[(c * P + j) * ND + d], &mp[((size_t)k * P + j) * ND + d]);
       }
+      if (lane < 4) {
+        const int k = child_of(ch, lane);
+        const int2 sr = t.srng[k];
+        const double2 c1 = t.center[k];
+        const double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
+        const bool has = sr.y > sr.x;
+        W1[lane] = has ? crcp(make_double2(z0.x / r1, z0.y / r1)) : make_double2(0, 0);
+        W2[lane] = has ? make_double2(z0.x / r2, z0.y / r2) : make_double2(0, 0);
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      for (int e = lane; e < 4 * P; e += 32) {
+        const int c = e / P, j = e - c * P;
+        const double2 w2 = W2[c];
+        const bool has = !(w2.x == 0.0 && w2.y == 0.0);
+        const double2 a = has ? cpow_int(W1[c], j) : make_double2(0, 0);
 #pragma unroll
-      for (int d = 0; d < ND; d++)
-        T[(c * P + j) * ND + d] = has ? cmul(mp[((size_t)k * P + j) * ND + d], a) : make_double2(0, 0);
-    }
-    __syncwarp();
-    // lane = (child c, group g): the child's contributions to the coefficients
-    // i = g, g + 8, ... (the triangular sums over j are spread over 32 lanes
-    // instead of P), summed over the four children by two xor shuffles
-    const int c = lane >> 3, g = lane & 7;
-    const double2 w2 = W2[c];
-    const double2* tc = T + (size_t)c * P * ND;
-    for (int i0 = 0; i0 < P; i0 += 8) {
-      const int i = i0 + g;
-      double2 v[ND];
+        for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(T[(c * P + j) * ND + d], a);
+      }
+      __syncwarp();
+      // lane = (child c, group g): the child's contributions to the
+      // coefficients i = g, g + 8, ... (the triangular sums over j are spread
+      // over 32 lanes instead of P), summed over the four children by two xor
+      // shuffles
+      const int c = lane >> 3, g = lane & 7;
+      const double2 w2 = W2[c];
+      const double2* tc = T + (size_t)c * P * ND;
+      for (int i0 = 0; i0 < P; i0 += 8) {
+        const int i = i0 + g;
+        double2 v[ND];
 #pragma unroll
-      for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
-      if (i == 0) {
+        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
+        if (i == 0) {
 #pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = tc[d];
-      } else if (i < P && !(w2.x == 0.0 && w2.y == 0.0)) {  // a child without sources adds 0
-        const double* crow = binom + (size_t)(i - 1) * BINOM_N;
+          for (int d = 0; d < ND; d++) v[d] = tc[d];
+        } else if (i < P && !(w2.x == 0.0 && w2.y == 0.0)) {  // a child without sources adds 0
+          const double* crow = binom + (size_t)(i - 1) * BINOM_N;
+          const double mri = -1.0 / i;
 #pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = make_double2(-tc[d].x / i, -tc[d].y / i);
-        for (int j = 1; j <= i; j++) {
-          const double cb = crow[j - 1];
+          for (int d = 0; d < ND; d++) v[d] = make_double2(tc[d].x * mri, tc[d].y * mri);
+          for (int j = 1; j <= i; j++) {
+            const double cb = crow[j - 1];
 #pragma unroll
-          for (int d = 0; d < ND; d++) {
-            const double2 tj = tc[j * ND + d];
-            v[d].x += tj.x * cb;
-            v[d].y += tj.y * cb;
+            for (int d = 0; d < ND; d++) {
+              const double2 tj = tc[j * ND + d];
+              v[d].x += tj.x * cb;
+              v[d].y += tj.y * cb;
+            }
           }
+          const double2 bi_ = cpow_int(w2, i);
+#pragma unroll
+          for (int d = 0; d < ND; d++) v[d] = cmul(v[d], bi_);
         }
-        const double2 bi_ = cpow_int(w2, i);
 #pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = cmul(v[d], bi_);
-      }
+        for (int d = 0; d < ND; d++) {
+          v[d].x += __shfl_xor_sync(~0u, v[d].x, 8);
+          v[d].y += __shfl_xor_sync(~0u, v[d].y, 8);
+          v[d].x += __shfl_xor_sync(~0u, v[d].x, 16);
+          v[d].y += __shfl_xor_sync(~0u, v[d].y, 16);
+        }
+        if (c == 0 && i < P) {
 #pragma unroll
-      for (int d = 0; d < ND; d++) {
-        v[d].x += __shfl_xor_sync(~0u, v[d].x, 8);
-        v[d].y += __shfl_xor_sync(~0u, v[d].y, 8);
-        v[d].x += __shfl_xor_sync(~0u, v[d].x, 16);
-        v[d].y += __shfl_xor_sync(~0u, v[d].y, 16);
-      }
-      if (c == 0 && i < P) {
-#pragma unroll
-        for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = v[d];
+          for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = v[d];
+        }
       }
     }
   }
@@ -292,101 +373,133 @@ __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int P,
 // ---------------------------------------------------------------------------
 // step 2: P2L from list 4 (laprouts2d.f:501-690), z0 = x - c, w = r/z0:
 // l_0 += q log|z0| - d/z0,  l_n += -q w^n/n - (d/z0) w^n.
-// The sources of the (at most 5) list-4 boxes are taken 32 at a time from
-// their concatenation; each lane computes 1/z0, log|z0| and the powers of
-// its source once.
+// A warp takes 32 of its boxes at a time (as in P2M) and ballots those with
+// a list 4 and evaluation points.  The sources of the (at most 5) list-4
+// boxes are taken 32 at a time from their concatenation; each lane computes
+// 1/z0, log|z0| and the powers of its source once.  The locals are zero
+// before this kernel (each box is written by one warp), so they are stored,
+// not updated.
 // ---------------------------------------------------------------------------
 template <int ND>
 __global__ void __launch_bounds__(64) k_p2l(TV t, int first, int n, const double2* __restrict__ xs,
                                             Dens D, int P, double2* __restrict__ lo) {
   extern __shared__ double2 smem[];
-  WARP_LOOP(n) {
-    double2* W = smem + (size_t)wib * (32 * P + 64 * ND + 32);
-    double2* Q = W + 32 * P;
-    double2* Dd = Q + 32 * ND;
-    double* LG = (double*)(Dd + 32 * ND);
-    int b = first + bi;
-    int n4 = t.nl4[b];
-    if (n4 == 0 || !t.has_eval_pts(b)) continue;
-    int lev = t.level[b];
-    double r = t.boxsize[lev];
-    double2 c = t.center[b];
-    int bs[5], be[5], tot = 0;
-    for (int e = 0; e < 5; e++) {
-      bs[e] = be[e] = 0;
-      if (e < n4) {
-        int2 sr = t.srng[t.l4[(size_t)MNLIST4 * b + e]];
-        bs[e] = sr.x;
-        be[e] = tot;  // offset of box e in the concatenation
-        tot += sr.y - sr.x;
-      }
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  double2* W = smem + (size_t)wib * (32 * P + 64 * ND + 32);
+  double2* Q = W + 32 * P;
+  double2* Dd = Q + 32 * ND;
+  double* LG = (double*)(Dd + 32 * ND);
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
+    const int mine = base + lane * nw;
+    int n4 = 0, lev = 0;
+    double2 cen = make_double2(0, 0);
+    if (mine < n) {
+      const int b = first + mine;
+      n4 = t.nl4[b];
+      lev = t.level[b];
+      cen = t.center[b];
+      int ne = 0;
+      if (t.ifpghtarg > 0) ne += t.trng[b].y - t.trng[b].x;
+      if (t.ifpgh > 0) ne += t.srng[b].y - t.srng[b].x;
+      if (ne == 0) n4 = 0;
     }
-    double2 acc[2][ND];
+    unsigned wm = __ballot_sync(~0u, n4 > 0);
+    while (wm) {
+      const int src = __ffs(wm) - 1;
+      wm &= wm - 1;
+      const int b = first + base + src * nw;
+      const int nb4 = __shfl_sync(~0u, n4, src);
+      const double2 c = make_double2(__shfl_sync(~0u, cen.x, src), __shfl_sync(~0u, cen.y, src));
+      const double r = t.boxsize[__shfl_sync(~0u, lev, src)];
+      // lanes e < nb4: the list-4 box e, its first source and its offset in
+      // the concatenation (exclusive scan of the counts)
+      int2 sr = make_int2(0, 0);
+      if (lane < nb4) sr = t.srng[t.l4[(size_t)MNLIST4 * b + lane]];
+      int cnt = sr.y - sr.x, inc = cnt;
 #pragma unroll
-    for (int s = 0; s < 2; s++)
+      for (int o = 1; o < 8; o <<= 1) {
+        const int v = __shfl_up_sync(~0u, inc, o);
+        if (lane >= o) inc += v;
+      }
+      const int tot = __shfl_sync(~0u, inc, MNLIST4 - 1);
+      int bs[MNLIST4], be[MNLIST4];
 #pragma unroll
-      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
-    for (int g0 = 0; g0 < tot; g0 += 32) {
-      int m = min(32, tot - g0);
-      __syncwarp();
-      if (lane < m) {
-        int g = g0 + lane, e = 0;
-        while (e + 1 < n4 && g >= be[e + 1]) e++;
-        int j = bs[e] + (g - be[e]);
-        double2 x = xs[j];
-        double2 z0 = make_double2(x.x - c.x, x.y - c.y);
-        double2 zi = crcp(z0);
-        double2 w = make_double2(r * zi.x, r * zi.y);
-        double2 pw = make_double2(1.0, 0.0);
-        for (int k = 0; k < P; k++) {
-          W[lane * P + k] = pw;
-          pw = cmul(pw, w);
+      for (int e = 0; e < MNLIST4; e++) {
+        bs[e] = __shfl_sync(~0u, sr.x, e);
+        be[e] = __shfl_sync(~0u, inc - cnt, e);
+      }
+      double2 acc[2][ND];
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+      for (int g0 = 0; g0 < tot; g0 += 32) {
+        const int m = min(32, tot - g0);
+        __syncwarp();
+        if (lane < m) {
+          const int g = g0 + lane;
+          int js = bs[0], jb = be[0];
+#pragma unroll
+          for (int e = 1; e < MNLIST4; e++)
+            if (e < nb4 && g >= be[e]) {
+              js = bs[e];
+              jb = be[e];
+            }
+          const int j = js + (g - jb);
+          const double2 x = xs[j];
+          const double2 z0 = make_double2(x.x - c.x, x.y - c.y);
+          const double2 zi = crcp(z0);
+          const double2 w = make_double2(r * zi.x, r * zi.y);
+          double2 pw = make_double2(1.0, 0.0);
+          for (int k = 0; k < P; k++) {
+            W[lane * P + k] = pw;
+            pw = cmul(pw, w);
+          }
+          LG[lane] = log(hypot(z0.x, z0.y));
+          const double2 mzi = cneg(zi);
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            Q[lane * ND + d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+            Dd[lane * ND + d] = D.d ? cmul(D.d[(size_t)j * D.ndc + D.d0 + d], mzi) : make_double2(0, 0);
+          }
         }
-        LG[lane] = log(hypot(z0.x, z0.y));
-        double2 mzi = cneg(zi);
+        __syncwarp();
 #pragma unroll
-        for (int d = 0; d < ND; d++) {
-          Q[lane * ND + d] = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
-          Dd[lane * ND + d] = D.d ? cmul(D.d[(size_t)j * D.ndc + D.d0 + d], mzi) : make_double2(0, 0);
+        for (int s = 0; s < 2; s++) {
+          const int k = lane + 32 * s;
+          if (k >= P) break;
+          if (k == 0) {
+            for (int j = 0; j < m; j++) {
+              const double lg = LG[j];
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                const double2 q = Q[j * ND + d];
+                acc[s][d].x += q.x * lg + Dd[j * ND + d].x;
+                acc[s][d].y += q.y * lg + Dd[j * ND + d].y;
+              }
+            }
+          } else {
+            const double mik = -1.0 / k;
+            for (int j = 0; j < m; j++) {
+              const double2 wk = W[j * P + k];
+              const double2 cq = cscale(wk, mik);
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                cfma(acc[s][d], Q[j * ND + d], cq);
+                cfma(acc[s][d], Dd[j * ND + d], wk);
+              }
+            }
+          }
         }
       }
-      __syncwarp();
 #pragma unroll
       for (int s = 0; s < 2; s++) {
-        int k = lane + 32 * s;
+        const int k = lane + 32 * s;
         if (k >= P) break;
-        if (k == 0) {
-          for (int j = 0; j < m; j++) {
-            double lg = LG[j];
 #pragma unroll
-            for (int d = 0; d < ND; d++) {
-              double2 q = Q[j * ND + d];
-              acc[s][d].x += q.x * lg + Dd[j * ND + d].x;
-              acc[s][d].y += q.y * lg + Dd[j * ND + d].y;
-            }
-          }
-        } else {
-          double mik = -1.0 / k;
-          for (int j = 0; j < m; j++) {
-            double2 wk = W[j * P + k];
-            double2 cq = cscale(wk, mik);
-#pragma unroll
-            for (int d = 0; d < ND; d++) {
-              cfma(acc[s][d], Q[j * ND + d], cq);
-              cfma(acc[s][d], Dd[j * ND + d], wk);
-            }
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int s = 0; s < 2; s++) {
-      int k = lane + 32 * s;
-      if (k >= P) break;
-#pragma unroll
-      for (int d = 0; d < ND; d++) {
-        size_t o = ((size_t)b * P + k) * ND + d;
-        lo[o] = cadd(lo[o], acc[s][d]);
+        for (int d = 0; d < ND; d++) lo[((size_t)b * P + k) * ND + d] = acc[s][d];
       }
     }
   }
@@ -497,65 +610,96 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
 // ---------------------------------------------------------------------------
 // step 5: L2L (laprouts2d.f:1020-1123), z0 = child - parent:
 // t_j = l_j (z0/r1)^j, L_i += (sum_{j>=i} t_j C(j, i)) (r2/z0)^i
-// One warp per parent: lanes stage t for all four children at once (lane =
-// (child, j)), then each lane produces (child, i) coefficients, dealt so
-// that the lanes' work is balanced.
+// One warp per parent: one round of loads brings the children's boxes and
+// (by cp.async) the parent's coefficients and the four children's current
+// locals into shared memory; the lanes scale the parent's coefficients to t
+// per child (lane = (child, j)), then each lane produces (child, i)
+// coefficients, dealt so that the lanes' work is balanced.
 // ---------------------------------------------------------------------------
 template <int ND>
-__global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int P,
+__global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, int P,
                                              const double* __restrict__ binom,
                                              double2* __restrict__ lo) {
   extern __shared__ double2 smem[];
-  WARP_LOOP(n) {
-    // per warp: t[child][j][density], then r2 / z0 of each child
-    double2* T = smem + (size_t)wib * (4 * P * ND + 4);
-    double2* W2 = T + 4 * P * ND;
-    int b = first + bi;
-    if (t.nchild[b] == 0 || !t.has_eval_pts(b)) continue;
-    int lev = t.level[b];
-    double r1 = t.boxsize[lev], r2 = t.boxsize[lev + 1];
-    double2 c1 = t.center[b];
-    int4 ch = t.child[b];
-    __syncwarp();
-    for (int e = lane; e < 4 * P; e += 32) {
-      const int c = e / P, j = e % P;
-      const int k = c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
-      double2 ck = t.center[k];
-      double2 z0 = make_double2(ck.x - c1.x, ck.y - c1.y);
-      double2 w1 = make_double2(z0.x / r1, z0.y / r1);
-      if (j == 0) W2[c] = crcp(make_double2(z0.x / r2, z0.y / r2));
-      double2 a = cpow_int(w1, j);
-#pragma unroll
-      for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(lo[((size_t)b * P + j) * ND + d], a);
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const double r1 = t.boxsize[lev], r2 = t.boxsize[lev + 1];
+  // per warp: the parent's l[j][density], t[child][j][density], the
+  // children's locals U[child][i][density], then z0 / r1 and r2 / z0 of
+  // each child
+  const int PN = P * ND;
+  double2* L = smem + (size_t)wib * (9 * PN + 8);
+  double2* T = L + PN;
+  double2* U = T + 4 * PN;
+  double2* W1 = U + 4 * PN;
+  double2* W2 = W1 + 4;
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
+    const int mine = base + lane * nw;
+    ParentScan s{};
+    bool want = false;
+    if (mine < n) {
+      s = scan_box(t, first + mine, true);
+      int ne = 0;
+      if (t.ifpghtarg > 0) ne += s.trng.y - s.trng.x;
+      if (t.ifpgh > 0) ne += s.srng.y - s.srng.x;
+      want = s.nchild != 0 && ne > 0;
     }
-    __syncwarp();
-    // items (child, i) cost P - i: dealt in decreasing cost, snaking over the
-    // lanes, so that the lanes' totals come out nearly equal
-    for (int r = 0; r * 32 < 4 * P; r++) {
-      const int e = r * 32 + ((r & 1) ? 31 - lane : lane);
-      if (e >= 4 * P) continue;
-      const int c = e & 3, i = e >> 2;
-      const int k = c == 0 ? ch.x : (c == 1 ? ch.y : (c == 2 ? ch.z : ch.w));
-      double2 v[ND];
+    unsigned pm = __ballot_sync(~0u, want);
+    while (pm) {
+      const int src = __ffs(pm) - 1;
+      pm &= pm - 1;
+      const int b = first + base + src * nw;
+      const double2 c1 = shfl_d2(s.center, src);
+      const int4 ch = shfl_i4(s.child, src);
+      __syncwarp();  // the previous parent's reads of shared memory are done
+      for (int e = lane; e < PN; e += 32) cp_async16(&L[e], &lo[(size_t)b * PN + e]);
+      for (int e = lane; e < 4 * PN; e += 32) {
+        const int c = e / PN;
+        cp_async16(&U[e], &lo[(size_t)child_of(ch, c) * PN + (e - c * PN)]);
+      }
+      if (lane < 4) {
+        const double2 ck = t.center[child_of(ch, lane)];
+        const double2 z0 = make_double2(ck.x - c1.x, ck.y - c1.y);
+        W1[lane] = make_double2(z0.x / r1, z0.y / r1);
+        W2[lane] = crcp(make_double2(z0.x / r2, z0.y / r2));
+      }
+      cp_async_wait_all();
+      __syncwarp();
+      for (int e = lane; e < 4 * P; e += 32) {
+        const int c = e / P, j = e - c * P;
+        const double2 a = cpow_int(W1[c], j);
 #pragma unroll
-      for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
-      const double2* tc = T + (size_t)c * P * ND;
-      for (int j = i; j < P; j++) {
-        double cb = binom[(size_t)j * BINOM_N + i];
+        for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(L[j * ND + d], a);
+      }
+      __syncwarp();
+      // items (child, i) cost P - i: dealt in decreasing cost, snaking over
+      // the lanes, so that the lanes' totals come out nearly equal
+      for (int r = 0; r * 32 < 4 * P; r++) {
+        const int e = r * 32 + ((r & 1) ? 31 - lane : lane);
+        if (e >= 4 * P) continue;
+        const int c = e & 3, i = e >> 2;
+        const int k = child_of(ch, c);
+        double2 v[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
+        const double2* tc = T + (size_t)c * PN;
+        for (int j = i; j < P; j++) {
+          const double cb = binom[(size_t)j * BINOM_N + i];
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            const double2 tj = tc[j * ND + d];
+            v[d].x += tj.x * cb;
+            v[d].y += tj.y * cb;
+          }
+        }
+        const double2 bi_ = cpow_int(W2[c], i);
 #pragma unroll
         for (int d = 0; d < ND; d++) {
-          double2 tj = tc[j * ND + d];
-          v[d].x += tj.x * cb;
-          v[d].y += tj.y * cb;
+          double2 cur = U[(c * P + i) * ND + d];
+          cfma(cur, v[d], bi_);
+          lo[((size_t)k * P + i) * ND + d] = cur;
         }
-      }
-      double2 bi_ = cpow_int(W2[c], i);
-#pragma unroll
-      for (int d = 0; d < ND; d++) {
-        size_t o = ((size_t)k * P + i) * ND + d;
-        double2 cur = lo[o];
-        cfma(cur, v[d], bi_);
-        lo[o] = cur;
       }
     }
   }
@@ -910,12 +1054,18 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, 0, nb, xs, D, P, mp);
   B2_LAUNCH_CHECK();
   B2_CHECK(cudaEventRecord(ev[1], st));
-  const size_t sm_m2m = sizeof(double2) * (4 * (size_t)P * ND + 4) * 4, sm_l2l = sm_m2m;
+  // shared memory per warp of M2M / L2L; up to 4 warps per block, fewer for
+  // high orders with many densities
+  const size_t wm2m = sizeof(double2) * (4 * (size_t)P * ND + 8);
+  const size_t wl2l = sizeof(double2) * (9 * (size_t)P * ND + 8);
+  const int wpb_m2m = (int)std::max<size_t>(1, std::min<size_t>(4, (200 << 10) / wm2m));
+  const int wpb_l2l = (int)std::max<size_t>(1, std::min<size_t>(4, (200 << 10) / wl2l));
+  const size_t sm_m2m = wm2m * wpb_m2m, sm_l2l = wl2l * wpb_l2l;
   set_smem_attr(k_m2m<ND>, sm_m2m);
   set_smem_attr(k_l2l<ND>, sm_l2l);
   for (int l = nl - 1; l >= 1; l--) {
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    k_m2m<ND><<<warp_grid(n, 4), 128, sm_m2m, st>>>(tv, f, n, P, binom, mp);
+    k_m2m<ND><<<warp_grid(n, wpb_m2m), 32 * wpb_m2m, sm_m2m, st>>>(tv, f, n, l, P, binom, mp);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[2], st));
@@ -940,7 +1090,7 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   B2_CHECK(cudaEventRecord(ev[4], st));
   for (int l = 1; l <= nl - 1; l++) {
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    k_l2l<ND><<<warp_grid(n, 4), 128, sm_l2l, st>>>(tv, f, n, P, binom, lo);
+    k_l2l<ND><<<warp_grid(n, wpb_l2l), 32 * wpb_l2l, sm_l2l, st>>>(tv, f, n, l, P, binom, lo);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[5], st));
