@@ -142,10 +142,10 @@ __host__ __device__ __forceinline__ void cfma(double2& a, double2 b, double2 c) 
   a.x += b.x * c.x - b.y * c.y;
   a.y += b.x * c.y + b.y * c.x;
 }
-// complex reciprocal 1/z
+// complex reciprocal 1/z (one division: conj(z) * (1 / |z|^2))
 __host__ __device__ __forceinline__ double2 crcp(double2 z) {
-  double d = z.x * z.x + z.y * z.y;
-  return make_double2(z.x / d, -z.y / d);
+  const double id = 1.0 / (z.x * z.x + z.y * z.y);
+  return make_double2(z.x * id, -z.y * id);
 }
 __host__ __device__ __forceinline__ double2 cdiv(double2 a, double2 b) { return cmul(a, crcp(b)); }
 

@@ -284,6 +284,8 @@ __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int lev, in
   const int wib = threadIdx.x >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const double r2 = t.boxsize[lev], r1 = t.boxsize[lev + 1];
+  const double ir2 = 1.0 / r2, ir1 = 1.0 / r1;
+  const int PN = P * ND;
   // per warp: t[child][j][density], then r1 / z0 and z0 / r2 of each child
   // (both 0 for a child without sources)
   double2* T = smem + (size_t)wib * (4 * P * ND + 8);
@@ -301,11 +303,10 @@ __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int lev, in
       const double2 c2 = shfl_d2(s.center, src);
       const int4 ch = shfl_i4(s.child, src);
       __syncwarp();  // the previous parent's reads of T are done
-      for (int e = lane; e < 4 * P; e += 32) {
-        const int c = e / P, j = e - c * P;
-        const int k = child_of(ch, c);
 #pragma unroll
-        for (int d = 0; d < ND; d++) cp_async16(&T[(c * P + j) * ND + d], &mp[((size_t)k * P + j) * ND + d]);
+      for (int c = 0; c < 4; c++) {
+        const size_t k = (size_t)child_of(ch, c);
+        for (int x = lane; x < PN; x += 32) cp_async16(&T[c * PN + x], &mp[k * PN + x]);
       }
       if (lane < 4) {
         const int k = child_of(ch, lane);
@@ -313,13 +314,13 @@ __global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int lev, in
         const double2 c1 = t.center[k];
         const double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
         const bool has = sr.y > sr.x;
-        W1[lane] = has ? crcp(make_double2(z0.x / r1, z0.y / r1)) : make_double2(0, 0);
-        W2[lane] = has ? make_double2(z0.x / r2, z0.y / r2) : make_double2(0, 0);
+        W1[lane] = has ? crcp(make_double2(z0.x * ir1, z0.y * ir1)) : make_double2(0, 0);
+        W2[lane] = has ? make_double2(z0.x * ir2, z0.y * ir2) : make_double2(0, 0);
       }
       cp_async_wait_all();
       __syncwarp();
       for (int e = lane; e < 4 * P; e += 32) {
-        const int c = e / P, j = e - c * P;
+        const int c = (e >= P) + (e >= 2 * P) + (e >= 3 * P), j = e - c * P;
         const double2 w2 = W2[c];
         const bool has = !(w2.x == 0.0 && w2.y == 0.0);
         const double2 a = has ? cpow_int(W1[c], j) : make_double2(0, 0);
@@ -631,6 +632,7 @@ __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, in
   const int wib = threadIdx.x >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const double r1 = t.boxsize[lev], r2 = t.boxsize[lev + 1];
+  const double ir1 = 1.0 / r1, ir2 = 1.0 / r2;
   // per warp: the parent's l[j][density], t[child][j][density], the
   // children's locals U[child][i][density], then z0 / r1 and r2 / z0 of
   // each child
@@ -660,20 +662,21 @@ __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, in
       const int4 ch = shfl_i4(s.child, src);
       __syncwarp();  // the previous parent's reads of shared memory are done
       for (int e = lane; e < PN; e += 32) cp_async16(&L[e], &lo[(size_t)b * PN + e]);
-      for (int e = lane; e < 4 * PN; e += 32) {
-        const int c = e / PN;
-        cp_async16(&U[e], &lo[(size_t)child_of(ch, c) * PN + (e - c * PN)]);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        const size_t k = (size_t)child_of(ch, c);
+        for (int x = lane; x < PN; x += 32) cp_async16(&U[c * PN + x], &lo[k * PN + x]);
       }
       if (lane < 4) {
         const double2 ck = t.center[child_of(ch, lane)];
         const double2 z0 = make_double2(ck.x - c1.x, ck.y - c1.y);
-        W1[lane] = make_double2(z0.x / r1, z0.y / r1);
-        W2[lane] = crcp(make_double2(z0.x / r2, z0.y / r2));
+        W1[lane] = make_double2(z0.x * ir1, z0.y * ir1);
+        W2[lane] = crcp(make_double2(z0.x * ir2, z0.y * ir2));
       }
       cp_async_wait_all();
       __syncwarp();
       for (int e = lane; e < 4 * P; e += 32) {
-        const int c = e / P, j = e - c * P;
+        const int c = (e >= P) + (e >= 2 * P) + (e >= 3 * P), j = e - c * P;
         const double2 a = cpow_int(W1[c], j);
 #pragma unroll
         for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(L[j * ND + d], a);
