@@ -229,12 +229,18 @@ __global__ void k_point_leaf(TV t, int nb, int use_targets, int* __restrict__ le
   for (int k = r.x; k < r.y; k++) leaf[k] = b;
 }
 
+// Blocks of 128 threads per SM asked of the register allocator for the far
+// field: 8 (at most 64 registers a thread) for one or two densities without
+// hessians, where the extra warps hide the coefficient loads (leaf phase
+// 2.59 -> 2.50 ms at 4M points); the compiler's choice otherwise.
+#define FAR_MIN_BLOCKS(ND, IFPGH) ((ND) <= 2 && (IFPGH) <= 2 ? 8 : 1)
+
 // Far field of one evaluation point per thread, FP64: L2P from the local
 // expansion of its leaf and M2P from the leaf's list-3 boxes (the
 // coefficients of one box are shared by the neighbouring threads of the same
 // leaf through the L1 cache).  Writes pot / grad / hess of the point.
 template <int ND, int IFPGH>
-__global__ void __launch_bounds__(128) k_far_mixed(
+__global__ void __launch_bounds__(128, FAR_MIN_BLOCKS(ND, IFPGH)) k_far_mixed(
     TV t, long n, const int* __restrict__ leaf, const double2* __restrict__ xe64, int ndc, int d0,
     int P, const double2* __restrict__ mp, const double2* __restrict__ lo,
     double2* __restrict__ pot, double2* __restrict__ grad, double2* __restrict__ hess) {
