@@ -1151,8 +1151,11 @@ struct LapPlan {
   MixedData MD;
   TV tv{};
   cudaEvent_t ev[8] = {};
+  cudaEvent_t tree_ev[2] = {};  // start / end of the tree build (plans on the caller's stream)
   ~LapPlan() {
     for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : tree_ev)
       if (e) cudaEventDestroy(e);
   }
 };
@@ -1311,10 +1314,18 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
     }
   }
   device_binomials();
-  B2_CHECK(cudaStreamSynchronize(st));
-  B2_CHECK(cudaEventElapsedTime(&p.tree_ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (p.own) {
+    // the plan is evaluated on other streams: finish its construction here
+    B2_CHECK(cudaStreamSynchronize(st));
+    B2_CHECK(cudaEventElapsedTime(&p.tree_ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  } else {
+    // evaluated on the caller's stream right after: no wait here; the tree
+    // time is read when the statistics are
+    p.tree_ev[0] = e0;
+    p.tree_ev[1] = e1;
+  }
   *out = pl.release();
   return IER_OK;
 }
@@ -1452,6 +1463,10 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
     S.m2p_evals = (double)hs6[3];
     S.p2l_sources = (double)hs6[4];
     S.npts_eval = (double)hs6[5];
+    if (p->tree_ev[1]) {
+      B2_CHECK(cudaEventSynchronize(p->tree_ev[1]));
+      B2_CHECK(cudaEventElapsedTime(&p->tree_ms, p->tree_ev[0], p->tree_ev[1]));
+    }
     S.tree_ms = p->tree_ms;
     S.fmm_ms = t2;
     S.nd_cauchy = p->ndc;
