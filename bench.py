@@ -563,7 +563,7 @@ def main():
     nd2 = st["nd_cauchy"]
     P = st["nterms1"]
     # algorithmic flops (FMA = 2): P2P charge+dipole pot+grad per pair 15 + 28*nd2
-    # (SURVEY 8d accounting); M2L per translation 2*P*P real MACs x 2 (re,im) x nd2
+    # (per pair: 15 real flops for the kernel terms, 28 per density); M2L per translation 2*P*P real MACs x 2 (re,im) x nd2
     flops = {"leaf_eval(l2p+m2p+p2p)": st["p2p_pairs"] * (15 + 28 * nd2)
              + st["npts_eval"] * 16 * P * nd2 + st["m2p_evals"] * 16 * P * nd2,
              "m2l": st["m2l_pairs"] * 4 * P * P * nd2}
