@@ -7,16 +7,17 @@
 //     baseline, because no Fortran compiler exists in this image.
 // The product path (fmm2d_b200/) never links, loads or calls this file.
 //
-// Parity pin.  The reference cannot be compiled or imported here (Fortran
-// only, no gfortran/flang/f2c).  This restatement is pinned by
-//   (1) the reference's own pass/fail criterion: FMM output vs. direct sum,
-//       relative l2 error < eps, on the reference test inputs
-//       (test/laplace/test_lfmm2d.f:30-101 with hkrand/dlaran restated below,
-//       python/test/test_lfmm.py:10-60), and
-//   (2) independent direct sums (numpy / mpmath golden fixtures under
-//       tests/golden/) for the kernels themselves.
-// Reference outputs themselves are unavailable, so tree/list identity with
-// the reference is argued from the restated algorithm, not measured.
+// Parity pin.  The reference is Fortran and no Fortran compiler exists in
+// this image, so oracle/f77c.py translates the reference's own source files
+// to C and gcc compiles them (make -C oracle ref -> _ref/libfmm2d_ref.so,
+// front end oracle/ref.py).  tests/test_ref_pin.py requires this restatement
+// to equal that build of the reference: trees, point sorts and lists 1-4
+// array for array (uniform, 16-Gaussian, graded-curve, target and duplicate
+// point cases, idivflag 0-2), lfmm2d / rfmm2d / cfmm2d / hfmm2d outputs
+// within 1e-12 relative l2 on the reference's test inputs
+// (test/laplace/test_lfmm2d.f:30-101, test/helmholtz/test_hfmm2d.f:19-51,
+// with hkrand/dlaran restated below), the direct sums and the ndiv / nterms
+// tables.  Independent checks: mpmath direct sums (tests/golden/).
 //
 // Conventions: 0-based box and point indices, -1 for "none"; complex arrays
 // are interleaved (re, im) doubles in the reference's column-major (nd, n)

@@ -21,6 +21,17 @@ def oracle():
 
 
 @pytest.fixture(scope="session")
+def ref():
+    """The reference itself (its Fortran translated to C, oracle/ref.py)."""
+    from oracle import ref as R
+    R.build()
+    if not R.available():
+        pytest.fail("oracle/_ref/libfmm2d_ref.so missing: run `make -C oracle ref` where the "
+                    "reference's sources are")
+    return R
+
+
+@pytest.fixture(scope="session")
 def gpu():
     import torch
     if not torch.cuda.is_available():
