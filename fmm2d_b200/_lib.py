@@ -15,7 +15,8 @@ P = c_void_p  # all array arguments are raw pointers
 
 class Options(C.Structure):
     """Mirror of ``b2fmm_options``."""
-    _fields_ = [("ndiv", c_int), ("idivflag", c_int), ("ifnear", c_int), ("precision", c_int)]
+    _fields_ = [("ndiv", c_int), ("idivflag", c_int), ("ifnear", c_int), ("precision", c_int),
+                ("async_call", c_int)]
 
 
 PREC = {"auto": 0, "fp64": 1, "mixed": 2}
@@ -55,6 +56,8 @@ SIGNATURES = {
     "b2fmm_tree_free": [P],
     "b2fmm_kernel_launches": [],
     "b2fmm_set_stats": [c_int],
+    "b2fmm_set_device_ranges": [c_int],
+    "b2fmm_async_status": [P, P],
     "b2fmm_get_stats": [P, c_int],
     "b2fmm_fma_peak": [c_int],
     "b2fmm_set_m2l_tensor_cores": [c_int],
@@ -112,7 +115,8 @@ def lib():
 
 
 STAT_KEYS = ["nboxes", "nlevels", "nleaves", "nterms1", "p2p_pairs", "m2l_pairs", "m2p_evals",
-             "p2l_sources", "npts_eval", "tree_ms", "fmm_ms", "nd_cauchy", "m2l_tc_steps"]
+             "p2l_sources", "npts_eval", "tree_ms", "fmm_ms", "nd_cauchy", "m2l_tc_steps",
+             "tl_pre", "tl_tree", "tl_setup", "tl_fmm", "tl_post"]
 
 
 def get_stats():

@@ -66,6 +66,7 @@ LapArgs make_args(int fe, int nd, double eps, int64_t ns, const double* sources,
     a.idivflag = o->idivflag;
     a.ifnear = o->ifnear;
     a.precision = o->precision;
+    a.async_call = o->async_call == 1;
   }
   a.timeinfo = timeinfo;
   return a;
@@ -151,19 +152,42 @@ int lap_host(LapArgs h) {
   a.pottarg = h.ifpghtarg >= 1 ? mk(pt, nq * nt) : nullptr;
   a.gradtarg = h.ifpghtarg >= 2 ? mk(gt, nq * gw * nt) : nullptr;
   a.hesstarg = h.ifpghtarg >= 3 ? mk(ht, nq * hw * nt) : nullptr;
-  int r = lap_fmm_device(a, st, ss.copies_done);
-  if (r != IER_OK) return r;
   auto down = [&](double* hp, const double* dpp, size_t n) {
     if (hp && dpp && n) B2_CHECK(cudaMemcpyAsync(hp, dpp, n * sizeof(double), cudaMemcpyDeviceToHost, st));
   };
-  down(h.pot, a.pot, nq * ns);
-  down(h.grad, a.grad, nq * gw * ns);
-  down(h.hess, a.hess, nq * hw * ns);
-  down(h.pottarg, a.pottarg, nq * nt);
-  down(h.gradtarg, a.gradtarg, nq * gw * nt);
-  down(h.hesstarg, a.hesstarg, nq * hw * nt);
+  auto down_all = [&] {
+    down(h.pot, a.pot, nq * ns);
+    down(h.grad, a.grad, nq * gw * ns);
+    down(h.hess, a.hess, nq * hw * ns);
+    down(h.pottarg, a.pottarg, nq * nt);
+    down(h.gradtarg, a.gradtarg, nq * gw * nt);
+    down(h.hesstarg, a.hesstarg, nq * hw * nt);
+  };
+  // the whole call (copies in, FMM, copies out) is queued before the one
+  // wait; the FMM's outcome comes back in the call's own status word
+  DBuf<int> status(st);
+  status.alloc(1, st);
+  status.zero(1);
+  a.async_call = !h.timeinfo;
+  a.status_word = status.p;
+  int r = lap_fmm_device(a, st, ss.copies_done);
+  if (r != IER_OK) return r;
+  down_all();
+  int* hs = pinned_ints(1);
+  B2_CHECK(cudaMemcpyAsync(hs, status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   B2_CHECK(cudaStreamSynchronize(st));
-  return IER_OK;
+  const int code = a.async_call ? hs[0] : IER_OK;
+  if (code == IER_TREE_LIMIT) {
+    // the tree needs the build with read-back: run the FMM again that way
+    a.async_call = false;
+    a.status_word = nullptr;
+    r = lap_fmm_device(a, st, nullptr);
+    if (r != IER_OK) return r;
+    down_all();
+    B2_CHECK(cudaStreamSynchronize(st));
+    return IER_OK;
+  }
+  return code;
 }
 
 HelmArgs make_hargs(int nd, double eps, double zkr, double zki, int64_t ns, const double* sources,
@@ -677,13 +701,20 @@ uint64_t b2fmm_kernel_launches(void) { return g_launches.load(); }
 
 void b2fmm_set_stats(int on) { set_stats(on != 0); }
 
+void b2fmm_set_device_ranges(int on) { set_device_ranges(on != 0); }
+
+void b2fmm_async_status(void* stream, int* ier) {
+  guarded(ier, [&] { return lap_async_status((cudaStream_t)stream); });
+}
+
 void b2fmm_get_stats(double* out, int n) {
   const LapStats& S = last_stats();
-  const double v[13] = {S.nboxes,    S.nlevels,     S.nleaves,   S.nterms1,
+  const double v[18] = {S.nboxes,    S.nlevels,     S.nleaves,   S.nterms1,
                         S.p2p_pairs, S.m2l_pairs,   S.m2p_evals, S.p2l_sources,
                         S.npts_eval, S.tree_ms,     S.fmm_ms,    S.nd_cauchy,
-                        S.m2l_tc_steps};
-  for (int i = 0; i < n && i < 13; i++) out[i] = v[i];
+                        S.m2l_tc_steps, S.tl_pre,   S.tl_tree,   S.tl_setup,
+                        S.tl_fmm,    S.tl_post};
+  for (int i = 0; i < n && i < 18; i++) out[i] = v[i];
 }
 
 double b2fmm_fma_peak(int fp64) { return fma_peak_flops(fp64 != 0); }

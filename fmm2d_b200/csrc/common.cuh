@@ -23,7 +23,9 @@ enum {
   IER_BADARG = 100,  // invalid argument (sizes, flags)
   IER_CUDA = 101,    // CUDA runtime error
   IER_TIMEOUT = 102,  // a bounded device wait gave up
-  IER_NOALLOC_TOO_LARGE = 103  // problem exceeds a fixed static scratch array
+  IER_NOALLOC_TOO_LARGE = 103,  // problem exceeds a fixed static scratch array
+  IER_TREE_LIMIT = 104  // an asynchronous call's tree needed more boxes or levels than a
+                        // call without read-back allows: repeat it synchronously
 };
 
 struct CudaError : public std::runtime_error {

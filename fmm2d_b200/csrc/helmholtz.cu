@@ -1212,7 +1212,7 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
   if (a.ifpghtarg >= 3 && nt) ht.alloc((size_t)nt * 3 * nd, st);
   TV tv{T.center.p, T.level.p, T.nchild.p, T.child.p, T.srng.p, T.trng.p, T.nlist1.p, T.list1.p,
         T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p, dbs.p, a.ifpgh,
-        nt > 0 ? a.ifpghtarg : 0};
+        nt > 0 ? a.ifpghtarg : 0, T.ctl.p};
   const double thresh = zkabs * T.bs0 * std::ldexp(1.0, -51);
   // leaf box of every sorted point, for the one-point-per-thread leaf kernels
   DBuf<int> leafs(st), leaft(st);

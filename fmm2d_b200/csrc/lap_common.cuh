@@ -53,6 +53,7 @@ struct TV {
   const int* l4;
   const double* boxsize;  // nlevels + 2 entries
   int ifpgh, ifpghtarg;
+  const TreeCtl* ctl;     // the tree's device control block (level table)
   __device__ __forceinline__ bool has_eval_pts(int b) const {
     int n = 0;
     if (ifpghtarg > 0) n += trng[b].y - trng[b].x;
@@ -60,6 +61,40 @@ struct TV {
     return n > 0;
   }
 };
+
+// Box range of a pass.  first >= 0: [first, first + n) as the host knows
+// it.  The negative codes read the range from the tree's device control
+// block instead (calls that do not wait for the tree on the host): all
+// boxes, the boxes of levels >= 2, or the boxes of level `lev`.  After a
+// failed build every range is empty.
+constexpr int RANGE_ALL = -1, RANGE_FROM2 = -2, RANGE_LEVEL = -3;
+
+__device__ __forceinline__ void resolve_range(const TV& t, int& first, int& n, int lev = 0) {
+  if (first >= 0) return;
+  const TreeCtl* c = t.ctl;
+  const int code = first;
+  first = 0;
+  n = 0;
+  if (c->status != TB_OK) return;
+  const int nb = c->nboxes, nl = c->nlevels;
+  if (code == RANGE_ALL) {
+    n = nb;
+  } else if (code == RANGE_FROM2) {
+    if (nl >= 2) {
+      first = c->lfirst[2];
+      n = nb - first;
+    }
+  } else if (lev >= 0 && lev <= nl) {
+    first = c->lfirst[lev];
+    n = c->llast[lev] - first + 1;
+  }
+}
+
+// The self-interaction threshold of the near field, boxsize(0) 2^-51
+// (cfmm2d.f:1276), when the host passes a negative value.
+__device__ __forceinline__ double near_thresh(const TV& t, double thresh) {
+  return thresh >= 0 ? thresh : t.boxsize[0] * 0x1p-51;
+}
 
 struct Dens {
   const double2* q;  // sorted charges (ndc per point) or null

@@ -77,6 +77,7 @@ __global__ void __launch_bounds__(128) k_m2l_f32(TV t, int first, int n, int P, 
   float4* G4 = (float4*)(wbase + 4 * warp_floats);  // [P][RB]: rows 4rb..4rb+3 of column j
   float2* U = (float2*)(G4 + (size_t)P * RB);      // [49][P]
   float* LG = (float*)(U + 49 * P);                // [49]
+  resolve_range(t, first, n);
   for (int e = threadIdx.x; e < P * RB * 4; e += blockDim.x) {
     int j = e / (RB * 4), i = e % (RB * 4);
     float g = 0.f;
@@ -224,6 +225,10 @@ __global__ void __launch_bounds__(128) k_m2l_f32(TV t, int first, int n, int P, 
 // Leaf box of every evaluation point (points are in tree order).
 __global__ void k_point_leaf(TV t, int nb, int use_targets, int* __restrict__ leaf) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nb < 0) {
+    int f = RANGE_ALL;
+    resolve_range(t, f, nb);
+  }
   if (b >= nb || t.nchild[b] != 0) return;
   int2 r = use_targets ? t.trng[b] : t.srng[b];
   for (int k = r.x; k < r.y; k++) leaf[k] = b;
@@ -249,7 +254,8 @@ __global__ void __launch_bounds__(128, FAR_MIN_BLOCKS(ND, IFPGH)) k_far_mixed(
     int P, const double2* __restrict__ mp, const double2* __restrict__ lo,
     double2* __restrict__ pot, double2* __restrict__ grad, double2* __restrict__ hess) {
   long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (k >= n) return;
+  // after a failed tree build the leaf map is not written
+  if (k >= n || t.ctl->status != TB_OK) return;
   const int b = leaf[k];
   const int lev = t.level[b];
   const double r = t.boxsize[lev];
@@ -393,7 +399,11 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_mixed(
     const float2* __restrict__ d32, int ndc, int d0, float th2, double2* __restrict__ pot,
     double2* __restrict__ grad, double2* __restrict__ hess) {
   long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (k >= n) return;
+  if (k >= n || t.ctl->status != TB_OK) return;
+  if (th2 < 0.f) {
+    const double thr = near_thresh(t, -1.0);
+    th2 = (float)(thr * thr);
+  }
   const bool hq = q32 != nullptr, hd = d32 != nullptr;
   const int b = leaf[k];
   const double2 z = xe64[k];
@@ -513,7 +523,8 @@ void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const
   B2_LAUNCH_CHECK();
   if (!ifnear) return;
   k_p2p_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(
-      t, n, leaf, M.xs64, xe64, M.q.p, M.d.p, ndc, d0, (float)(thresh * thresh), pot, grad, hess);
+      t, n, leaf, M.xs64, xe64, M.q.p, M.d.p, ndc, d0,
+      thresh >= 0 ? (float)(thresh * thresh) : -1.f, pot, grad, hess);
   B2_LAUNCH_CHECK();
 }
 
@@ -548,15 +559,16 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
   B2_LAUNCH_CHECK();
 }
 
-void lap_mixed_leaves(MixedData& M, const TV& t, int nb, long ns, long nt, cudaStream_t st) {
+void lap_mixed_leaves(MixedData& M, const TV& t, int nb, bool dev, long ns, long nt,
+                      cudaStream_t st) {
   M.ns = ns;
   M.nt = nt;
   M.leaf_s.alloc(ns, st);
-  k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, nb, 0, M.leaf_s.p);
+  k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, dev ? -1 : nb, 0, M.leaf_s.p);
   B2_LAUNCH_CHECK();
   if (nt > 0) {
     M.leaf_t.alloc(nt, st);
-    k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, nb, 1, M.leaf_t.p);
+    k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, dev ? -1 : nb, 1, M.leaf_t.p);
     B2_LAUNCH_CHECK();
   }
 }

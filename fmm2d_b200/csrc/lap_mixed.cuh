@@ -34,8 +34,10 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
                        bool has_q, bool has_d, int ndc, double cx0, double cy0, int P,
                        cudaStream_t st);
 
-// Leaf box of every sorted evaluation point (once per tree).
-void lap_mixed_leaves(MixedData& M, const lapk::TV& t, int nb, long ns, long nt, cudaStream_t st);
+// Leaf box of every sorted evaluation point (once per tree); nb boxes at
+// most, the box count read from the tree's device control block when dev.
+void lap_mixed_leaves(MixedData& M, const lapk::TV& t, int nb, bool dev, long ns, long nt,
+                      cudaStream_t st);
 
 // FP32 copies of the sorted densities (every evaluation).
 void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, long ns, int ndc,

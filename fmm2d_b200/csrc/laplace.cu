@@ -31,6 +31,7 @@ namespace b2 {
 
 namespace {
 std::atomic<bool> g_stats_on{false};
+std::atomic<bool> g_device_ranges{true};
 thread_local LapStats g_last_stats;
 }  // namespace
 
@@ -142,6 +143,7 @@ __global__ void __launch_bounds__(64, P2M_MIN_BLOCKS(ND)) k_p2m(TV t, int first,
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
+  resolve_range(t, first, n);
   double2* W = smem + (size_t)wib * (P2M_CHUNK * P + 2 * P2M_CHUNK * ND);
   double2* Q = W + P2M_CHUNK * P;
   double2* Dd = Q + P2M_CHUNK * ND;
@@ -276,9 +278,9 @@ __device__ __forceinline__ int4 shfl_i4(int4 v, int src) {
 // group) forms the child's terms and shuffles sum the children.
 // ---------------------------------------------------------------------------
 template <int ND>
-__global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int lev, int P,
-                                             const double* __restrict__ binom,
-                                             double2* __restrict__ mp) {
+__device__ __forceinline__ void m2m_level(const TV& t, int first, int n, int lev, int P,
+                                          const double* __restrict__ binom,
+                                          double2* __restrict__ mp) {
   extern __shared__ double2 smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -394,6 +396,7 @@ __global__ void __launch_bounds__(64) k_p2l(TV t, int first, int n, const double
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int nw = (gridDim.x * blockDim.x) >> 5;
+  resolve_range(t, first, n);
   double2* W = smem + (size_t)wib * (32 * P + 64 * ND + 32);
   double2* Q = W + 32 * P;
   double2* Dd = Q + 32 * ND;
@@ -526,6 +529,7 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
                                              const double2* __restrict__ mp,
                                              double2* __restrict__ lo) {
   extern __shared__ double2 smem[];
+  resolve_range(t, first, n);
   double* G = (double*)smem;  // G[j * P + i]
   for (int e = threadIdx.x; e < P * P; e += blockDim.x) {
     int j = e / P, i = e % P;
@@ -624,9 +628,9 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
 // coefficients, dealt so that the lanes' work is balanced.
 // ---------------------------------------------------------------------------
 template <int ND>
-__global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, int P,
-                                             const double* __restrict__ binom,
-                                             double2* __restrict__ lo) {
+__device__ __forceinline__ void l2l_level(const TV& t, int first, int n, int lev, int P,
+                                          const double* __restrict__ binom,
+                                          double2* __restrict__ lo) {
   extern __shared__ double2 smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -714,6 +718,62 @@ __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, in
   }
 }
 
+// One level of M2M / L2L per launch (the host knows the level's boxes).
+// (first = RANGE_LEVEL: the level's boxes from the device level table).
+template <int ND>
+__global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int lev, int P,
+                                             const double* __restrict__ binom,
+                                             double2* __restrict__ mp) {
+  resolve_range(t, first, n, lev);
+  m2m_level<ND>(t, first, n, lev, P, binom, mp);
+}
+template <int ND>
+__global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, int P,
+                                             const double* __restrict__ binom,
+                                             double2* __restrict__ lo) {
+  resolve_range(t, first, n, lev);
+  l2l_level<ND>(t, first, n, lev, P, binom, lo);
+}
+
+// The levels >= lev_min in one cooperative launch, the boxes of every level
+// from the tree's device level table and a grid barrier between levels: the
+// upward pass finest parents first, the downward pass coarsest first.  The
+// host launches the levels below lev_min one by one; this kernel takes the
+// part of a tree deeper than the host expected (nothing when the guess was
+// right).  A barrier that gives up sets *err (the call reports IER_TIMEOUT).
+template <int ND>
+__global__ void __launch_bounds__(128) k_m2m_all(TV t, int P, const double* __restrict__ binom,
+                                                 double2* __restrict__ mp, GridBar* gb,
+                                                 int* err, int lev_min) {
+  const TreeCtl* c = t.ctl;
+  if (c->status != TB_OK) return;
+  const int nl = c->nlevels, lo_lev = max(lev_min, 1);
+  for (int lev = nl - 1; lev >= lo_lev; lev--) {
+    const int first = c->lfirst[lev];
+    m2m_level<ND>(t, first, c->llast[lev] - first + 1, lev, P, binom, mp);
+    if (lev > lo_lev && !grid_barrier(gb, 1)) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      return;
+    }
+  }
+}
+template <int ND>
+__global__ void __launch_bounds__(128) k_l2l_all(TV t, int P, const double* __restrict__ binom,
+                                                 double2* __restrict__ lo, GridBar* gb,
+                                                 int* err, int lev_min) {
+  const TreeCtl* c = t.ctl;
+  if (c->status != TB_OK) return;
+  const int nl = c->nlevels;
+  for (int lev = max(lev_min, 1); lev <= nl - 1; lev++) {
+    const int first = c->lfirst[lev];
+    l2l_level<ND>(t, first, c->llast[lev] - first + 1, lev, P, binom, lo);
+    if (lev < nl - 1 && !grid_barrier(gb, 1)) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      return;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // steps 6-8 fused per leaf: for 32 evaluation points at a time,
 //   L2P  (laprouts2d.f:696-897)   Horner in (z - c)/r with derivatives
@@ -739,7 +799,9 @@ __global__ void __launch_bounds__(64) k_leaf(TV t, int first, int n, int use_tar
                                             double2* __restrict__ grad,
                                             double2* __restrict__ hess) {
   extern __shared__ double2 smem[];
-  const double th2 = thresh * thresh;
+  resolve_range(t, first, n);
+  const double thr = near_thresh(t, thresh);
+  const double th2 = thr * thr;
   WARP_LOOP(n) {
     LeafSmem<ND>* S = (LeafSmem<ND>*)smem + wib;
     int b = first + bi;
@@ -1006,6 +1068,10 @@ __global__ void k_inverse_perm(const int* __restrict__ perm, long n, int* __rest
 // Work counts for the roofline accounting (enabled by set_stats).
 __global__ void k_stats(TV t, int nb, unsigned long long* out) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nb < 0) {
+    int f = RANGE_ALL;
+    resolve_range(t, f, nb);
+  }
   unsigned long long c[6] = {0, 0, 0, 0, 0, 0};
   if (b < nb) {
     long ne = 0;
@@ -1039,6 +1105,20 @@ __global__ void k_stats(TV t, int nb, unsigned long long* out) {
   }
 }
 
+// Outputs are zero when every source and target coincides (a tree of one
+// box of size 0): all interactions are omitted self-interactions.  Checked on
+// the device for calls that did not read the tree back.
+__global__ void k_zero_if_point_tree(const TreeCtl* c, double* a0, long n0, double* a1, long n1,
+                                     double* a2, long n2, double* a3, long n3, double* a4,
+                                     long n4, double* a5, long n5) {
+  if (c->status != TB_OK || c->bs[0] != 0.0) return;
+  const long g = blockIdx.x * (long)blockDim.x + threadIdx.x, gs = (long)gridDim.x * blockDim.x;
+  double* a[6] = {a0, a1, a2, a3, a4, a5};
+  const long n[6] = {n0, n1, n2, n3, n4, n5};
+  for (int q = 0; q < 6; q++)
+    for (long i = g; i < n[q]; i += gs) a[q][i] = 0.0;
+}
+
 // ---------------------------------------------------------------------------
 // host driver
 // ---------------------------------------------------------------------------
@@ -1047,20 +1127,62 @@ int warp_grid(long nitems, int warps_per_block) {
   return (int)std::max(1L, std::min(blocks, 148L * 64));
 }
 
+// Blocks of a cooperative launch of `kernel` (all resident): as many per SM
+// as registers and shared memory allow, up to g_coop_blocks_per_sm.
+std::atomic<int> g_coop_blocks_per_sm{8};
+
+template <typename K>
+int coop_grid(K kernel, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<const void*, size_t>, int>> done[128];
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) throw CudaError("device ordinal beyond 127", IER_CUDA);
+  std::lock_guard<std::mutex> g(mu);
+  const size_t key = smem * 64 + (size_t)g_coop_blocks_per_sm.load();
+  for (auto& e : done[dev])
+    if (e.first.first == (const void*)kernel && e.first.second == key) return e.second;
+  int nsm = 0, per = 0, coop = 0;
+  B2_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  B2_CHECK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+  if (!coop) throw CudaError("cooperative launch not supported", IER_CUDA);
+  B2_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+  if (per < 1) throw CudaError("cooperative pass does not fit an SM", IER_CUDA);
+  const int grid = std::min(per, g_coop_blocks_per_sm.load()) * nsm;
+  done[dev].push_back({{(const void*)kernel, key}, grid});
+  return grid;
+}
+
+// Launch context of one evaluation: the box count to size grids by (the
+// capacity when the host did not read the tree back), whether ranges come
+// from the device level table, the grid barrier of the all-level passes and
+// the evaluation's error flag.
+struct Launch {
+  int nb;
+  bool dev;
+  GridBar* gb;
+  int* err;
+  int lev_hint;  // levels the host launches one by one (device ranges)
+};
+
 template <int ND>
 void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int P,
                const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
-               double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, double thresh,
+               double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, const Launch& X,
                cudaStream_t st, cudaEvent_t* ev, const MixedData* M) {
   const double* binom = device_binomials();
-  const int nb = T.nboxes;
-  const int nl = T.nlevels;
+  const int nb = X.nb;
+  const bool dev = X.dev;
+  const int nl = dev ? 0 : T.nlevels;
+  const int all = dev ? RANGE_ALL : 0;
+  const int from2 = dev ? RANGE_FROM2 : (nl >= 2 ? T.lfirst[2] : 0);
+  const int n_from2 = dev ? nb : (nl >= 2 ? nb - T.lfirst[2] : 0);
   B2_CHECK(cudaEventRecord(ev[0], st));
   size_t sm_p2m = sizeof(double2) * 2 * (P2M_CHUNK * (size_t)P + 2 * P2M_CHUNK * ND);
   size_t sm_p2l = sizeof(double2) * 2 * (32 * (size_t)P + 64 * ND + 32);
   set_smem_attr(k_p2m<ND>, sm_p2m);
   set_smem_attr(k_p2l<ND>, sm_p2l);
-  k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, 0, nb, xs, D, P, mp);
+  k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, all, nb, xs, D, P, mp);
   B2_LAUNCH_CHECK();
   B2_CHECK(cudaEventRecord(ev[1], st));
   // shared memory per warp of M2M / L2L; up to 4 warps per block, fewer for
@@ -1072,38 +1194,78 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   const size_t sm_m2m = wm2m * wpb_m2m, sm_l2l = wl2l * wpb_l2l;
   set_smem_attr(k_m2m<ND>, sm_m2m);
   set_smem_attr(k_l2l<ND>, sm_l2l);
-  for (int l = nl - 1; l >= 1; l--) {
-    int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    k_m2m<ND><<<warp_grid(n, wpb_m2m), 32 * wpb_m2m, sm_m2m, st>>>(tv, f, n, l, P, binom, mp);
+  TV tvc = tv;
+  // boxes at level l: at most 4^l and the capacity (grids of the levels the
+  // host launches without knowing their size)
+  auto level_bound = [&](int l) { return (int)std::min<long>(nb, l < 15 ? 1L << (2 * l) : nb); };
+  if (dev) {
+    // the part deeper than the expected depth first, then level by level
+    set_smem_attr(k_m2m_all<ND>, sm_m2m);
+    const int grid = coop_grid(k_m2m_all<ND>, 32 * wpb_m2m, sm_m2m);
+    int Pv = P, lmin = X.lev_hint;
+    GridBar* gb = X.gb;
+    int* err = X.err;
+    void* args[] = {&tvc, &Pv, (void*)&binom, &mp, &gb, &err, &lmin};
+    B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_m2m_all<ND>, dim3(grid),
+                                         dim3(32 * wpb_m2m), args, sm_m2m, st));
     B2_LAUNCH_CHECK();
+    for (int l = X.lev_hint - 1; l >= 1; l--) {
+      const int nbl = level_bound(l);
+      k_m2m<ND><<<warp_grid(nbl, wpb_m2m), 32 * wpb_m2m, sm_m2m, st>>>(tv, RANGE_LEVEL, nbl, l,
+                                                                      P, binom, mp);
+      B2_LAUNCH_CHECK();
+    }
+  } else {
+    for (int l = nl - 1; l >= 1; l--) {
+      int f = T.lfirst[l], n = T.llast[l] - f + 1;
+      k_m2m<ND><<<warp_grid(n, wpb_m2m), 32 * wpb_m2m, sm_m2m, st>>>(tv, f, n, l, P, binom, mp);
+      B2_LAUNCH_CHECK();
+    }
   }
   B2_CHECK(cudaEventRecord(ev[2], st));
   B2_CHECK(cudaMemsetAsync(lo, 0, sizeof(double2) * (size_t)nb * P * ND, st));
-  if (nl >= 2) {
-    int f = T.lfirst[2], n = nb - f;
-    k_p2l<ND><<<warp_grid(n, 2), 64, sm_p2l, st>>>(tv, f, n, xs, D, P, lo);
+  if (n_from2 > 0) {
+    k_p2l<ND><<<warp_grid(n_from2, 2), 64, sm_p2l, st>>>(tv, from2, n_from2, xs, D, P, lo);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[3], st));
-  if (nl >= 2 && M) {
-    int f = T.lfirst[2], n = nb - f;
-    lap_mixed_m2l(ND, tv, f, n, P, binom, *M, mp, lo, st);
-  } else if (nl >= 2) {
-    int f = T.lfirst[2], n = nb - f;
+  if (n_from2 > 0 && M) {
+    lap_mixed_m2l(ND, tv, from2, n_from2, P, binom, *M, mp, lo, st);
+  } else if (n_from2 > 0) {
     size_t sm = sizeof(double) * (P * P + 1) + sizeof(double2) * 4 * P * ND;
     if (sm > 48 * 1024)
       set_smem_attr(k_m2l<ND>, sm);
-    k_m2l<ND><<<warp_grid(n, 4), 128, sm, st>>>(tv, f, n, P, binom, mp, lo);
+    k_m2l<ND><<<warp_grid(n_from2, 4), 128, sm, st>>>(tv, from2, n_from2, P, binom, mp, lo);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[4], st));
-  for (int l = 1; l <= nl - 1; l++) {
-    int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    k_l2l<ND><<<warp_grid(n, wpb_l2l), 32 * wpb_l2l, sm_l2l, st>>>(tv, f, n, l, P, binom, lo);
+  if (dev) {
+    for (int l = 1; l <= X.lev_hint - 1; l++) {
+      const int nbl = level_bound(l);
+      k_l2l<ND><<<warp_grid(nbl, wpb_l2l), 32 * wpb_l2l, sm_l2l, st>>>(tv, RANGE_LEVEL, nbl, l,
+                                                                      P, binom, lo);
+      B2_LAUNCH_CHECK();
+    }
+    set_smem_attr(k_l2l_all<ND>, sm_l2l);
+    const int grid = coop_grid(k_l2l_all<ND>, 32 * wpb_l2l, sm_l2l);
+    int Pv = P, lmin = X.lev_hint;
+    GridBar* gb = X.gb;
+    int* err = X.err;
+    void* args[] = {&tvc, &Pv, (void*)&binom, &lo, &gb, &err, &lmin};
+    B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_l2l_all<ND>, dim3(grid),
+                                         dim3(32 * wpb_l2l), args, sm_l2l, st));
     B2_LAUNCH_CHECK();
+  } else {
+    for (int l = 1; l <= nl - 1; l++) {
+      int f = T.lfirst[l], n = T.llast[l] - f + 1;
+      k_l2l<ND><<<warp_grid(n, wpb_l2l), 32 * wpb_l2l, sm_l2l, st>>>(tv, f, n, l, P, binom, lo);
+      B2_LAUNCH_CHECK();
+    }
   }
   B2_CHECK(cudaEventRecord(ev[5], st));
   size_t sm_leaf = sizeof(LeafSmem<ND>) * 2;
+  // near-field threshold boxsize(0) 2^-51, taken on the device from the tree
+  const double thresh = -1.0;
   auto leaf = [&](int use_t, int ifl, const double2* xe, double2* po, double2* gr, double2* he) {
     if (ifl <= 0) return;
     if (M) {
@@ -1113,16 +1275,16 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
     }
     if (ifl == 1) {
       set_smem_attr(k_leaf<ND, 1>, sm_leaf);
-      k_leaf<ND, 1><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
-                                                          thresh, a.ifnear, po, gr, he);
+      k_leaf<ND, 1><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, all, nb, use_t, xs, xe, D, P, mp,
+                                                          lo, thresh, a.ifnear, po, gr, he);
     } else if (ifl == 2) {
       set_smem_attr(k_leaf<ND, 2>, sm_leaf);
-      k_leaf<ND, 2><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
-                                                          thresh, a.ifnear, po, gr, he);
+      k_leaf<ND, 2><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, all, nb, use_t, xs, xe, D, P, mp,
+                                                          lo, thresh, a.ifnear, po, gr, he);
     } else {
       set_smem_attr(k_leaf<ND, 3>, sm_leaf);
-      k_leaf<ND, 3><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, 0, nb, use_t, xs, xe, D, P, mp, lo,
-                                                          thresh, a.ifnear, po, gr, he);
+      k_leaf<ND, 3><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, all, nb, use_t, xs, xe, D, P, mp,
+                                                          lo, thresh, a.ifnear, po, gr, he);
     }
     B2_LAUNCH_CHECK();
   };
@@ -1137,16 +1299,16 @@ struct LapPlan {
   LapArgs a;                      // geometry and flags (density/output pointers unused)
   cudaStream_t st = nullptr;      // stream owning the buffers
   bool own = false;               // st is the shared plan stream (not the caller's)
-  int nd = 1, ndc = 1, P = 0, chunk = 1;
+  bool dev = false;               // box ranges from the device (tree not read back)
+  int nd = 1, ndc = 1, P = 0, chunk = 1, ndiv = 0;
   long ns = 0, nt = 0;
   bool fc = false, fd = false, mixed = false;
   bool zero = false;              // nothing interacts: every output is zero
-  double thresh = 0;
   float tree_ms = 0;
   DeviceTree T;
-  DBuf<double> dbs;
   DBuf<double2> xs, xt, qs, ds, ps, gs, hs, pt, gt, ht, mp, lo;
   DBuf<int> err;
+  DBuf<GridBar> gbar;      // grid barrier of the all-level M2M / L2L passes
   DBuf<int> inv_s, inv_t;  // tree position of every caller-order source / target
   MixedData MD;
   TV tv{};
@@ -1182,11 +1344,36 @@ OutSizes out_sizes(const LapPlan& p) {
   return o;
 }
 
-// Reads and clears the plan's device error flag after `st` has finished.
-int read_err(LapPlan& p, cudaStream_t st) {
-  int* h = pinned_ints(1);
+// Levels of the upward and downward passes the host launches one by one
+// without reading the tree back (see k_m2m_all): the depth of the last tree
+// of this size, else that of a uniform cloud.
+int level_hint(long npts, int ndiv) {
+  int nb = 0, nl = 0;
+  if (tree_shape(npts, ndiv, &nb, &nl)) return nl;
+  int l = 1;
+  for (double boxes = (double)npts / std::max(ndiv, 1); boxes > 1 && l < NLMAX; boxes /= 4) l++;
+  return l;
+}
+
+// The end-of-call check, one small readback after `st` has finished: the
+// evaluation's error flag and, when the host did not read the tree back, the
+// tree's box count and status.  IER_RETRY: the tree needs the build with
+// read-back (more boxes than the capacity, or more than 32 levels).
+constexpr int IER_RETRY = -1;
+
+int finish(LapPlan& p, cudaStream_t st) {
+  int* h = pinned_ints(8);
   B2_CHECK(cudaMemcpyAsync(h, p.err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  const bool dev = p.dev && p.T.ctl.p;
+  if (dev)  // nboxes, nlevels, cap, status: the head of the control block
+    B2_CHECK(cudaMemcpyAsync(h + 4, p.T.ctl.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, st));
   B2_CHECK(cudaStreamSynchronize(st));
+  if (dev) {
+    const int status = h[7];
+    if (status == TB_OVERFLOW || status == TB_DEEP) return IER_RETRY;
+    if (status != TB_OK) return IER_TIMEOUT;
+    note_tree_shape(p.ns + p.nt, p.ndiv, h[4], h[5]);
+  }
   if (h[0]) {
     B2_CHECK(cudaMemsetAsync(p.err.p, 0, sizeof(int), st));
     B2_CHECK(cudaStreamSynchronize(st));
@@ -1197,7 +1384,8 @@ int read_err(LapPlan& p, cudaStream_t st) {
 
 }  // namespace
 
-int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPlan** out) {
+int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPlan** out,
+                    bool device_ranges) {
   *out = nullptr;
   if (a.nd < 1 || a.ns < 0 || a.nt < 0 || a.ifpgh < 0 || a.ifpgh > 3 || a.ifpghtarg < 0 ||
       a.ifpghtarg > 3 || a.ns > (1L << 30) || a.nt > (1L << 30) || a.fe < 0 || a.fe > 2)
@@ -1238,12 +1426,13 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   p.err.zero(1);
   if (p.ns == 0 || (!p.fc && !p.fd)) {
     p.zero = true;
-    B2_CHECK(cudaStreamSynchronize(st));
+    if (own_stream) B2_CHECK(cudaStreamSynchronize(st));
     *out = pl.release();
     return IER_OK;
   }
   int ndiv = a.ndiv > 0 ? a.ndiv : lap_ndiv(a.eps);
   if (ndiv <= 0) ndiv = (int)std::min<long>(p.ns + p.nt, 1L << 30);
+  p.ndiv = ndiv;
   p.P = lap_nterms(a.eps) + 1;
   if (p.P > 64) return IER_NTERMS;
   p.mixed = a.precision == PREC_MIXED || (a.precision == PREC_AUTO && a.eps >= 1e-6);
@@ -1252,25 +1441,26 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   B2_CHECK(cudaEventCreate(&e0));
   B2_CHECK(cudaEventCreate(&e1));
   B2_CHECK(cudaEventRecord(e0, st));
-  build_device_tree(p.T, a.src, p.ns, a.trg, p.nt, a.idivflag, ndiv, NLMAX, st);
+  p.dev = device_ranges && !own_stream;
+  if (p.dev)
+    build_device_tree_async(p.T, a.src, p.ns, a.trg, p.nt, a.idivflag, ndiv, NLMAX,
+                            tree_capacity_guess(p.ns + p.nt, ndiv, a.async_call ? 1.25 : 1.1),
+                            st);
+  else
+    build_device_tree(p.T, a.src, p.ns, a.trg, p.nt, a.idivflag, ndiv, NLMAX, st);
   B2_CHECK(cudaEventRecord(e1, st));
   DeviceTree& T = p.T;
-  if (T.bs0 == 0.0) {
+  if (!p.dev && T.bs0 == 0.0) {
     // every source and target coincides: all interactions are self
     // interactions, which the reference omits, so every output is zero
     p.zero = true;
-    B2_CHECK(cudaStreamSynchronize(st));
+    if (own_stream) B2_CHECK(cudaStreamSynchronize(st));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     *out = pl.release();
     return IER_OK;
   }
-  const int nb = T.nboxes;
-  std::vector<double> bsx(T.boxsize);
-  bsx.push_back(T.boxsize.back() / 2);
-  p.dbs.alloc(bsx.size(), st);
-  B2_CHECK(cudaMemcpyAsync(p.dbs.p, bsx.data(), sizeof(double) * bsx.size(),
-                           cudaMemcpyHostToDevice, st));
+  const int nb = T.nboxes;  // the capacity when the tree was not read back
   p.xs.alloc(p.ns, st);
   k_gather_pts<<<ceil_div(p.ns, 256), 256, 0, st>>>(a.src, T.isrc.p, p.ns, p.xs.p);
   B2_LAUNCH_CHECK();
@@ -1296,21 +1486,26 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   if (a.ifpghtarg >= 3 && p.nt) p.ht.alloc(ntd, st);
   p.tv = TV{T.center.p, T.level.p, T.nchild.p, T.child.p, T.srng.p, T.trng.p, T.nlist1.p,
             T.list1.p, T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p,
-            p.dbs.p, a.ifpgh, p.nt > 0 ? a.ifpghtarg : 0};
-  p.thresh = T.bs0 * std::ldexp(1.0, -51);
+            &T.ctl.p->bs[0], a.ifpgh, p.nt > 0 ? a.ifpghtarg : 0, T.ctl.p};
   p.chunk = p.ndc >= 8 ? 8 : (p.ndc >= 4 ? 4 : (p.ndc >= 2 ? 2 : 1));
   p.mp.alloc((size_t)nb * p.P * p.chunk, st);
   p.lo.alloc((size_t)nb * p.P * p.chunk, st);
+  p.gbar.alloc(1, st);
+  p.gbar.zero(1);
   if (p.mixed) {
-    lap_mixed_prepare(p.MD, p.xs.p, p.ns, p.xt.p, p.nt, p.fc, p.fd, p.ndc, T.cx0, T.cy0, p.P, st);
+    lap_mixed_prepare(p.MD, p.xs.p, p.ns, p.xt.p, p.nt, p.fc, p.fd, p.ndc, 0.0, 0.0, p.P, st);
     p.MD.err = p.err.p;
-    lap_mixed_leaves(p.MD, p.tv, nb, p.ns, p.nt, st);
-    if (T.nlevels >= 2 && T.nlevels < 64 && m2l_tensor_cores() && m2l_tc_supported(p.P)) {
+    lap_mixed_leaves(p.MD, p.tv, nb, p.dev, p.ns, p.nt, st);
+    const bool levels_ok = p.dev || (T.nlevels >= 2 && T.nlevels < 64);
+    if (levels_ok && m2l_tensor_cores() && m2l_tc_supported(p.P)) {
       p.MD.tc = true;
-      p.MD.nlev = T.nlevels + 1;
+      p.MD.nlev = p.dev ? NLMAX + 3 : T.nlevels + 1;
       p.MD.nboxes = nb;
-      m2l_tc_build(p.MD.pairs, p.tv, T.lfirst[2], nb - T.lfirst[2], nb, p.P, p.chunk, st);
-      if (p.MD.pairs.npairs > 0) p.MD.mp32.alloc(m2l_tc_scratch(p.MD.pairs, nb, p.chunk), st);
+      if (p.dev)
+        m2l_tc_build(p.MD.pairs, p.tv, RANGE_FROM2, nb, nb, p.P, p.chunk, st);
+      else
+        m2l_tc_build(p.MD.pairs, p.tv, T.lfirst[2], nb - T.lfirst[2], nb, p.P, p.chunk, st);
+      if (p.MD.pairs.n > 0) p.MD.mp32.alloc(m2l_tc_scratch(p.MD.pairs, nb, p.chunk), st);
     }
   }
   device_binomials();
@@ -1328,6 +1523,10 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   }
   *out = pl.release();
   return IER_OK;
+}
+
+int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPlan** out) {
+  return lap_plan_create(a, st_in, own_stream, out, false);
 }
 
 int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const double* dipvec,
@@ -1364,17 +1563,20 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
                                                    dipvec, p.qs.p, p.ds.p);
   B2_LAUNCH_CHECK();
   if (p.mixed) lap_mixed_densities(p.MD, p.qs.p, p.ds.p, ns, ndc, st);
+  if (p.dev) B2_CHECK(cudaMemsetAsync(p.gbar.p, 0, sizeof(GridBar), st));
   const MixedData* Mp = p.mixed ? &p.MD : nullptr;
+  const Launch X{T.nboxes, p.dev, p.gbar.p, p.err.p,
+                 p.dev ? level_hint(p.ns + p.nt, p.ndiv) : 0};
   double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int d0 = 0; d0 < ndc;) {
     int left = ndc - d0;
     int ND = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
     Dens D{p.fc ? p.qs.p : nullptr, p.fd ? p.ds.p : nullptr, ndc, d0};
     switch (ND) {
-      case 8: run_chunk<8>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
-      case 4: run_chunk<4>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
-      case 2: run_chunk<2>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
-      default: run_chunk<1>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, p.thresh, st, p.ev, Mp); break;
+      case 8: run_chunk<8>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
+      case 4: run_chunk<4>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
+      case 2: run_chunk<2>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
+      default: run_chunk<1>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
     }
     if (timeinfo) {
       B2_CHECK(cudaEventSynchronize(p.ev[6]));
@@ -1401,19 +1603,22 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
                                                 p.gt.p, p.ht.p, pottarg, gradtarg, hesstarg);
     B2_LAUNCH_CHECK();
   }
+  if (p.dev) {
+    k_zero_if_point_tree<<<148, 256, 0, st>>>(T.ctl.p, pot, (long)o.pot, grad, (long)o.grad,
+                                              hess, (long)o.hess, pottarg, (long)o.pott, gradtarg,
+                                              (long)o.gradt, hesstarg, (long)o.hesst);
+    B2_LAUNCH_CHECK();
+  }
   if (timeinfo)
     for (int i = 0; i < 8; i++) timeinfo[i] = tsum[i];
-  if (sync) {
-    B2_CHECK(cudaStreamSynchronize(st));
-    return read_err(p, st);
-  }
+  if (sync) return finish(p, st);
   return IER_OK;
 }
 
 int lap_plan_status(LapPlan* p) {
   if (!p) return IER_BADARG;
   B2_CHECK(cudaDeviceSynchronize());
-  return read_err(*p, p->st);
+  return finish(*p, p->st);
 }
 
 void lap_plan_free(LapPlan* p) {
@@ -1425,10 +1630,15 @@ void lap_plan_free(LapPlan* p) {
   if (own) cudaStreamSynchronize(st);
 }
 
-int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
-  if ((a.fe == FE_LAPLACE || a.fe == FE_REAL) && a.dipstr && !a.dipvec) return IER_BADARG;
+namespace {
+
+// One call: the plan (box ranges taken on the device when device_ranges, so
+// the host does not wait for the tree), its evaluation and the end-of-call
+// check.
+int fmm_once(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready, bool device_ranges,
+             cudaEvent_t call0) {
   LapPlan* p = nullptr;
-  int r = lap_plan_create(a, st, false, &p);
+  int r = lap_plan_create(a, st, false, &p, device_ranges);
   if (r != IER_OK) return r;
   if (dens_ready) B2_CHECK(cudaStreamWaitEvent(st, dens_ready, 0));
   std::unique_ptr<LapPlan, void (*)(LapPlan*)> guard(p, lap_plan_free);
@@ -1437,7 +1647,8 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
   if (want_stats && !p->zero) {
     dstat.alloc(6, st);
     dstat.zero(6);
-    k_stats<<<ceil_div(p->T.nboxes, 256), 256, 0, st>>>(p->tv, p->T.nboxes, dstat.p);
+    k_stats<<<ceil_div(p->T.nboxes, 256), 256, 0, st>>>(p->tv, p->dev ? -1 : p->T.nboxes,
+                                                        dstat.p);
     B2_LAUNCH_CHECK();
   }
   cudaEvent_t e0, e1;
@@ -1451,11 +1662,13 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
   if (want_stats && !p->zero && r == IER_OK) {
     unsigned long long hs6[6];
     B2_CHECK(cudaMemcpy(hs6, dstat.p, sizeof(hs6), cudaMemcpyDeviceToHost));
+    int hn[2] = {0, 0};
+    B2_CHECK(cudaMemcpy(hn, p->T.ctl.p, sizeof(hn), cudaMemcpyDeviceToHost));
     float t2 = 0;
     B2_CHECK(cudaEventElapsedTime(&t2, e0, e1));
     LapStats& S = g_last_stats;
-    S.nboxes = p->T.nboxes;
-    S.nlevels = p->T.nlevels;
+    S.nboxes = hn[0];
+    S.nlevels = hn[1];
     S.nleaves = (double)hs6[0];
     S.nterms1 = p->P;
     S.p2p_pairs = (double)hs6[1];
@@ -1469,6 +1682,15 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
     }
     S.tree_ms = p->tree_ms;
     S.fmm_ms = t2;
+    auto el = [](cudaEvent_t x, cudaEvent_t y) {
+      float ms = 0;
+      return (x && y && cudaEventElapsedTime(&ms, x, y) == cudaSuccess) ? (double)ms : -1.0;
+    };
+    S.tl_pre = el(call0, p->tree_ev[0]);
+    S.tl_tree = el(p->tree_ev[0], p->tree_ev[1]);
+    S.tl_setup = el(p->tree_ev[1], p->ev[0]);
+    S.tl_fmm = el(p->ev[0], p->ev[6]);
+    S.tl_post = el(p->ev[6], e1);
     S.nd_cauchy = p->ndc;
     S.m2l_tc_steps = 0;
     if (p->mixed && p->MD.tc && p->MD.pairs.steps.p) {
@@ -1481,5 +1703,78 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
   cudaEventDestroy(e1);
   return r;
 }
+
+// Device-wide status word of asynchronous calls: the first failure code.
+int* async_word() {
+  static std::mutex mu;
+  static int* words[128] = {nullptr};
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) throw CudaError("device ordinal beyond 127", IER_CUDA);
+  std::lock_guard<std::mutex> g(mu);
+  if (!words[dev]) {
+    int* w = nullptr;
+    B2_CHECK(cudaMalloc(&w, sizeof(int)));
+    B2_CHECK(cudaMemset(w, 0, sizeof(int)));
+    words[dev] = w;
+  }
+  return words[dev];
+}
+
+__global__ void k_fold_status(const TreeCtl* c, const int* err, int* word) {
+  int code = 0;
+  if (c && c->status != TB_OK) code = c->status == TB_TIMEOUT ? IER_TIMEOUT : IER_TREE_LIMIT;
+  if (!code && *err) code = IER_TIMEOUT;
+  if (code) atomicCAS(word, 0, code);
+}
+
+// One call queued on `st` without any host wait: box ranges on the device,
+// the outcome folded into the device's status word.
+int fmm_async(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
+  LapPlan* p = nullptr;
+  int r = lap_plan_create(a, st, false, &p, true);
+  if (r != IER_OK) return r;
+  if (dens_ready) B2_CHECK(cudaStreamWaitEvent(st, dens_ready, 0));
+  std::unique_ptr<LapPlan, void (*)(LapPlan*)> guard(p, lap_plan_free);
+  r = lap_plan_eval(p, a.charge, a.dipstr, a.dipvec, a.pot, a.grad, a.hess, a.pottarg, a.gradtarg,
+                    a.hesstarg, st, false, nullptr);
+  if (r != IER_OK) return r;
+  k_fold_status<<<1, 1, 0, st>>>(p->zero ? nullptr : p->T.ctl.p, p->err.p,
+                                 a.status_word ? a.status_word : async_word());
+  B2_LAUNCH_CHECK();
+  return IER_OK;  // the plan's buffers are released stream-ordered after the call
+}
+
+}  // namespace
+
+int lap_async_status(cudaStream_t st) {
+  int* w = async_word();
+  B2_CHECK(cudaStreamSynchronize(st));
+  int h = 0;
+  B2_CHECK(cudaMemcpy(&h, w, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) B2_CHECK(cudaMemset(w, 0, sizeof(int)));
+  return h;
+}
+
+// A single call does not wait for its tree on the host: the passes read
+// their box ranges on the device and one check at the end of the call reads
+// the outcome.  A tree that needed more boxes than the capacity guess, or
+// more than 32 levels, makes the call run again with the tree read back.
+int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready) {
+  if ((a.fe == FE_LAPLACE || a.fe == FE_REAL) && a.dipstr && !a.dipvec) return IER_BADARG;
+  // phase times and statistics need the host to wait: those calls are synchronous
+  if (a.async_call && !a.timeinfo && !g_stats_on.load()) return fmm_async(a, st, dens_ready);
+  cudaEvent_t call0 = nullptr;
+  if (g_stats_on.load()) {
+    B2_CHECK(cudaEventCreate(&call0));
+    B2_CHECK(cudaEventRecord(call0, st));
+  }
+  int r = fmm_once(a, st, dens_ready, g_device_ranges.load(), call0);
+  if (r == IER_RETRY) r = fmm_once(a, st, nullptr, false, call0);
+  if (call0) cudaEventDestroy(call0);
+  return r;
+}
+
+void set_device_ranges(bool on) { g_device_ranges.store(on); }
 
 }  // namespace b2

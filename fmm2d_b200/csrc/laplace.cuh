@@ -36,7 +36,16 @@ struct LapArgs {
   int ifnear = 1;
   int precision = PREC_AUTO;
   double* timeinfo = nullptr;  // 8 phase times (s), host memory, may be null
+  // return once the call is queued on the stream (no host wait at all);
+  // device-side failures go to the device's status word (lap_async_status)
+  bool async_call = false;
+  int* status_word = nullptr;  // async: fold the outcome here instead of the device's word
 };
+
+// Waits for `st` and returns (and clears) the first failure of the
+// asynchronous calls queued on this device since the last query (IER_OK,
+// IER_TIMEOUT or IER_TREE_LIMIT).
+int lap_async_status(cudaStream_t st);
 
 // Runs the FMM on device pointers on stream `st`; returns an ier code.
 // dens_ready (optional): an event the evaluation waits for before it reads
@@ -54,6 +63,16 @@ int lap_fmm_device(const LapArgs& a, cudaStream_t st, cudaEvent_t dens_ready = n
 // which densities later evaluations pass (non-null = present).
 struct LapPlan;
 int lap_plan_create(const LapArgs& a, cudaStream_t st, bool own_stream, LapPlan** out);
+// device_ranges: the tree is not read back; the passes take their box ranges
+// from its device control block (a single call on the caller's stream; the
+// end-of-call check reports a tree that needs the read-back build).
+int lap_plan_create(const LapArgs& a, cudaStream_t st, bool own_stream, LapPlan** out,
+                    bool device_ranges);
+
+// Single calls take their box ranges on the device (default on); off makes
+// every call wait for its tree on the host and launch the passes level by
+// level.
+void set_device_ranges(bool on);
 int lap_plan_eval(LapPlan* p, const double* charge, const double* dipstr, const double* dipvec,
                   double* pot, double* grad, double* hess, double* pottarg, double* gradtarg,
                   double* hesstarg, cudaStream_t st, bool sync, double* timeinfo);
@@ -78,6 +97,9 @@ struct LapStats {
   double fmm_ms;                             // everything after the tree
   double nd_cauchy;                          // Cauchy densities
   double m2l_tc_steps;                       // tensor-core M2L: offset steps of all tiles (0: not used)
+  // device timeline of the call (ms): start -> tree start, tree, tree end ->
+  // first FMM pass, FMM passes, last pass -> end of the call
+  double tl_pre, tl_tree, tl_setup, tl_fmm, tl_post;
 };
 void set_stats(bool on);
 const LapStats& last_stats();

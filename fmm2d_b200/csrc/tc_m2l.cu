@@ -362,11 +362,12 @@ __device__ __forceinline__ void tmem_ld_cols(uint32_t addr, float (&y)[2 * C]) {
 // super-tile.
 template <int KH>
 __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
-    k_m2l_tc(const int* __restrict__ tstart, const int2* __restrict__ ent, int ntgt, int T,
-             int ndsh, int P, const float4* __restrict__ tab, const double* __restrict__ boxsize,
-             int nlev, const float4* __restrict__ mp32, double2* __restrict__ lo,
-             int* __restrict__ err) {
+    k_m2l_tc(const int* __restrict__ tstart, const int2* __restrict__ ent,
+             const int* __restrict__ info, int ndsh, int P, const float4* __restrict__ tab,
+             const double* __restrict__ boxsize, int nlev, const float4* __restrict__ mp32,
+             double2* __restrict__ lo, int* __restrict__ err) {
   using L = OT<KH>;
+  const int ntgt = info[0], T = info[1];
   constexpr int K = L::K, N = L::N, C = L::C, NV = KH / 4;
   extern __shared__ __align__(1024) char smem[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -754,29 +755,56 @@ __global__ void __launch_bounds__(128, 1)
   if (warp == 0) tmem_dealloc(taddr, TC_TMEM_COLS);
 }
 
+// Candidate i of the target range (a box of level >= 2 with list-2 boxes
+// and evaluation points); the range may come from the device level table,
+// and n (the scan length) may exceed it.
 __global__ void k_m2l_flag(TV t, int first, int n, int* __restrict__ flag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int b = first + i;
-  flag[i] = (t.has_eval_pts(b) && t.nl2[b] > 0) ? 1 : 0;
+  int f = first, nn = n;
+  resolve_range(t, f, nn);
+  const int b = f + i;
+  flag[i] = (i < nn && t.has_eval_pts(b) && t.nl2[b] > 0) ? 1 : 0;
+}
+
+// Target count (info[0]) and super-tile size T (info[1]): about four
+// super-tiles per SM for R rows.
+__global__ void k_m2l_info(const int* __restrict__ tix, const int* __restrict__ flag, int n,
+                           int R, int nsm, int* __restrict__ info) {
+  const int ntgt = n > 0 ? tix[n - 1] + flag[n - 1] : 0;
+  info[0] = ntgt;
+  const long rows = ((long)ntgt + R - 1) / R;
+  info[1] = (int)max(1L, (rows + 4L * nsm - 1) / (4L * nsm));
 }
 
 // Compact the targets with their list-2 length as the sort key: a tile runs
 // as many steps as its longest list, so tiles of equal lengths keep every
-// row busy.
+// row busy.  Non-targets keep key 31 (set beforehand) and sort last.
 __global__ void k_m2l_compact(TV t, int first, int n, const int* __restrict__ flag,
                               const int* __restrict__ tix, int* __restrict__ key,
                               int* __restrict__ box) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !flag[i]) return;
-  const int b = first + i;
+  int f = first, nn = n;
+  resolve_range(t, f, nn);
+  const int b = f + i;
   key[tix[i]] = t.nl2[b];
   box[tix[i]] = b;
 }
 
-__global__ void k_m2l_count(TV t, const int* __restrict__ box, int ntgt, int* __restrict__ cnt) {
+__global__ void k_m2l_count(TV t, const int* __restrict__ box, int n,
+                            const int* __restrict__ info, int* __restrict__ cnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < ntgt) cnt[i] = t.nl2[box[i]];
+  if (i < n) cnt[i] = i < info[0] ? t.nl2[box[i]] : 0;
+}
+
+// Entry count (info[2]) and the closing offset tstart[ntgt].
+__global__ void k_m2l_total(const int* __restrict__ offs, const int* __restrict__ cnt,
+                            int* __restrict__ info, int* __restrict__ tstart) {
+  const int ntgt = info[0];
+  const int np = ntgt > 0 ? offs[ntgt - 1] + cnt[ntgt - 1] : 0;
+  info[2] = np;
+  tstart[ntgt] = np;
 }
 
 // Target boxes in kernel order and their list-2 entries, sorted by offset
@@ -785,7 +813,8 @@ __global__ void k_m2l_count(TV t, const int* __restrict__ box, int ntgt, int* __
 // rows of neighbouring targets (same child position) tend to take the same
 // offset in the same step, so their table loads coincide (2.13 against
 // 2.25 ms for the M2L at 4M points in list order).
-__global__ void __launch_bounds__(128) k_m2l_fill(TV t, const int* __restrict__ box, int ntgt,
+__global__ void __launch_bounds__(128) k_m2l_fill(TV t, const int* __restrict__ box,
+                                                  const int* __restrict__ info,
                                                   const int* __restrict__ cnt,
                                                   const int* __restrict__ offs,
                                                   int* __restrict__ tstart,
@@ -794,7 +823,7 @@ __global__ void __launch_bounds__(128) k_m2l_fill(TV t, const int* __restrict__ 
   // places its entries in its own 49 slots and emits them in index order
   __shared__ int slot[49][128];
   const int ti = blockIdx.x * blockDim.x + threadIdx.x;
-  if (ti >= ntgt) return;
+  if (ti >= info[0]) return;
   const int b = box[ti], n2 = cnt[ti];
   const double2 cb = t.center[b];
   const double rinv = 1.0 / t.boxsize[t.level[b]];
@@ -821,8 +850,9 @@ __global__ void __launch_bounds__(128) k_m2l_fill(TV t, const int* __restrict__ 
 // Kernel order of the length-sorted targets: super-tiles of R T targets, in
 // which row group q takes a contiguous run of the targets q, q + R, q + 2R,
 // ... of the super-tile (runs of similar total length).
-__global__ void k_m2l_perm(const int* __restrict__ sbox, int ntgt, int R, int T,
+__global__ void k_m2l_perm(const int* __restrict__ sbox, const int* __restrict__ info, int R,
                            int* __restrict__ pbox) {
+  const int ntgt = info[0], T = info[1];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ntgt) return;
   const long per = (long)R * T, base = i / per * per;
@@ -832,12 +862,12 @@ __global__ void k_m2l_perm(const int* __restrict__ sbox, int ntgt, int R, int T,
   pbox[base + (long)rg * q0 + min(rg, rem) + k] = sbox[i];
 }
 
-__global__ void k_set_int(int* p, int v) { *p = v; }
-
 // Steps of all super-tiles (the issued tensor-core work): the longest run
 // of list-2 entries over the row groups of each super-tile.
-__global__ void k_m2l_steps(const int* __restrict__ tstart, long ntgt, int R, int T,
+__global__ void k_m2l_steps(const int* __restrict__ tstart, const int* __restrict__ info, int R,
                             unsigned long long* __restrict__ out) {
+  const long ntgt = info[0];
+  const int T = info[1];
   const long stl = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long per = (long)R * T, base = stl * per;
   if (base >= ntgt) return;
@@ -860,10 +890,15 @@ bool m2l_tc_supported(int P) { return P >= 2 && P <= 20; }
 
 void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P, int chunk,
                   cudaStream_t st) {
-  L.ntgt = L.npairs = 0;
   L.P = P;
+  L.n = 0;
   L.usable = nboxes < (1 << 26) && m2l_tc_supported(P);
   if (!L.usable || n <= 0) return;
+  L.n = n;
+  // every count stays on the device (info: targets, super-tile size,
+  // entries); the arrays are sized for n candidates
+  L.info.alloc(4, st);
+  L.info.zero(4);
   DBuf<int> flag(st), tix(st);
   flag.alloc(n, st);
   tix.alloc(n, st);
@@ -874,59 +909,50 @@ void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P,
   DBuf<char> tmp(st);
   tmp.alloc(tb, st);
   B2_CHECK(cub::DeviceScan::ExclusiveSum(tmp.p, tb, flag.p, tix.p, n, st));
-  int* h = pinned_ints(2);
-  B2_CHECK(cudaMemcpyAsync(h, tix.p + (n - 1), sizeof(int), cudaMemcpyDeviceToHost, st));
-  B2_CHECK(cudaMemcpyAsync(h + 1, flag.p + (n - 1), sizeof(int), cudaMemcpyDeviceToHost, st));
-  B2_CHECK(cudaStreamSynchronize(st));
-  const int ntgt = h[0] + h[1];
-  if (ntgt == 0) return;
-  // targets sorted by list-2 length
-  DBuf<int> key(st), box(st), skey(st), sbox(st), cnt(st), offs(st);
-  key.alloc(ntgt, st);
-  box.alloc(ntgt, st);
-  skey.alloc(ntgt, st);
-  sbox.alloc(ntgt, st);
-  k_m2l_compact<<<ceil_div(n, 256), 256, 0, st>>>(t, first, n, flag.p, tix.p, key.p, box.p);
-  B2_LAUNCH_CHECK();
-  size_t tb2 = 0;
-  // list lengths are <= MNLIST2 < 32: 5 key bits (stable: box order inside a length)
-  static_assert(MNLIST2 < 32, "list-2 length key");
-  B2_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key.p, skey.p, box.p, sbox.p, ntgt, 0, 5,
-                                           st));
-  DBuf<char> tmp2(st);
-  tmp2.alloc(tb2, st);
-  B2_CHECK(cub::DeviceRadixSort::SortPairs(tmp2.p, tb2, key.p, skey.p, box.p, sbox.p, ntgt, 0, 5,
-                                           st));
-  // super-tiles: about 4 per SM for the main density chunk
   int dev = 0, nsm = 148;
   B2_CHECK(cudaGetDevice(&dev));
   B2_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const int R = 128 / chunk;
-  L.T = (int)std::max<long>(1, ((long)ntgt + R - 1) / R / (4L * nsm));
-  DBuf<int> pbox(st);
-  pbox.alloc(ntgt, st);
-  k_m2l_perm<<<ceil_div(ntgt, 256), 256, 0, st>>>(sbox.p, ntgt, R, L.T, pbox.p);
+  k_m2l_info<<<1, 1, 0, st>>>(tix.p, flag.p, n, R, nsm, L.info.p);
   B2_LAUNCH_CHECK();
-  cnt.alloc(ntgt, st);
-  offs.alloc(ntgt, st);
-  k_m2l_count<<<ceil_div(ntgt, 256), 256, 0, st>>>(t, pbox.p, ntgt, cnt.p);
+  // targets sorted by list-2 length (non-targets: key 31, sorted last)
+  DBuf<int> key(st), box(st), skey(st), sbox(st), cnt(st), offs(st);
+  key.alloc(n, st);
+  box.alloc(n, st);
+  skey.alloc(n, st);
+  sbox.alloc(n, st);
+  key.fill_bytes(0x1f, n);
+  box.fill_bytes(0xff, n);
+  k_m2l_compact<<<ceil_div(n, 256), 256, 0, st>>>(t, first, n, flag.p, tix.p, key.p, box.p);
+  B2_LAUNCH_CHECK();
+  size_t tb2 = 0;
+  // list lengths are <= MNLIST2 < 31: 5 key bits (stable: box order inside a length)
+  static_assert(MNLIST2 < 31, "list-2 length key");
+  B2_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, tb2, key.p, skey.p, box.p, sbox.p, n, 0, 5,
+                                           st));
+  DBuf<char> tmp2(st);
+  tmp2.alloc(tb2, st);
+  B2_CHECK(cub::DeviceRadixSort::SortPairs(tmp2.p, tb2, key.p, skey.p, box.p, sbox.p, n, 0, 5,
+                                           st));
+  DBuf<int> pbox(st);
+  pbox.alloc(n, st);
+  k_m2l_perm<<<ceil_div(n, 256), 256, 0, st>>>(sbox.p, L.info.p, R, pbox.p);
+  B2_LAUNCH_CHECK();
+  cnt.alloc(n, st);
+  offs.alloc(n, st);
+  k_m2l_count<<<ceil_div(n, 256), 256, 0, st>>>(t, pbox.p, n, L.info.p, cnt.p);
   B2_LAUNCH_CHECK();
   size_t tb3 = 0;
-  B2_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, cnt.p, offs.p, ntgt, st));
+  B2_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, tb3, cnt.p, offs.p, n, st));
   DBuf<char> tmp3(st);
   tmp3.alloc(tb3, st);
-  B2_CHECK(cub::DeviceScan::ExclusiveSum(tmp3.p, tb3, cnt.p, offs.p, ntgt, st));
-  B2_CHECK(cudaMemcpyAsync(h, offs.p + (ntgt - 1), sizeof(int), cudaMemcpyDeviceToHost, st));
-  B2_CHECK(cudaMemcpyAsync(h + 1, cnt.p + (ntgt - 1), sizeof(int), cudaMemcpyDeviceToHost, st));
-  B2_CHECK(cudaStreamSynchronize(st));
-  L.ntgt = ntgt;
-  L.npairs = (long)h[0] + h[1];
-  L.tstart.alloc(L.ntgt + 1, st);
-  L.ent.alloc(std::max<long>(L.npairs, 1), st);
-  k_m2l_fill<<<ceil_div(ntgt, 128), 128, 0, st>>>(t, pbox.p, ntgt, cnt.p, offs.p, L.tstart.p,
-                                                  L.ent.p);
+  B2_CHECK(cub::DeviceScan::ExclusiveSum(tmp3.p, tb3, cnt.p, offs.p, n, st));
+  L.tstart.alloc((size_t)n + 1, st);
+  L.ent.alloc((size_t)MNLIST2 * n, st);
+  k_m2l_total<<<1, 1, 0, st>>>(offs.p, cnt.p, L.info.p, L.tstart.p);
   B2_LAUNCH_CHECK();
-  k_set_int<<<1, 1, 0, st>>>(L.tstart.p + L.ntgt, (int)L.npairs);
+  k_m2l_fill<<<ceil_div(n, 128), 128, 0, st>>>(t, pbox.p, L.info.p, cnt.p, offs.p, L.tstart.p,
+                                               L.ent.p);
   B2_LAUNCH_CHECK();
   const int KH = m2l_kh(P), K = 2 * KH, N = (2 * KH + 2 + 15) / 16 * 16;
   L.tab.alloc(m2l_tab_floats(KH), st);
@@ -935,8 +961,7 @@ void m2l_tc_build(M2LPairs& L, const TV& t, int first, int n, int nboxes, int P,
   B2_LAUNCH_CHECK();
   L.steps.alloc(1, st);
   L.steps.zero(1);
-  const long nst = ((long)L.ntgt + (long)R * L.T - 1) / ((long)R * L.T);
-  k_m2l_steps<<<ceil_div(nst, 128), 128, 0, st>>>(L.tstart.p, L.ntgt, R, L.T, L.steps.p);
+  k_m2l_steps<<<ceil_div(n / R + 1, 128), 128, 0, st>>>(L.tstart.p, L.info.p, R, L.steps.p);
   B2_LAUNCH_CHECK();
   // the temporaries above are freed (stream-ordered) when this returns
 }
@@ -947,7 +972,7 @@ long m2l_tc_scratch(const M2LPairs& L, int nboxes, int ND) {
 
 int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long nmp32, int nboxes,
                double2* lo, const double* boxsize, int nlev, int* err_dev, cudaStream_t st) {
-  if (L.npairs == 0) return IER_OK;
+  if (L.n == 0) return IER_OK;
   const int P = L.P;
   if (nlev > 64 || !m2l_tc_supported(P) || !(ND == 1 || ND == 2 || ND == 4 || ND == 8))
     return IER_BADARG;
@@ -960,7 +985,6 @@ int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long 
   const long nconv = (long)nboxes * ND * KH;
   k_mp_to_f32<<<ceil_div(nconv, 256), 256, 0, st>>>(mp, nboxes, P, ND, KH, mp32);
   B2_LAUNCH_CHECK();
-  const long nst = (L.ntgt + (long)(128 >> ndsh) * L.T - 1) / ((long)(128 >> ndsh) * L.T);
   auto launch = [&](auto kern, uint32_t total, uint32_t tmem_cols, int threads) {
     // CTAs that can share an SM (tensor-memory columns and shared memory);
     // the shared memory request keeps more from being resident (a tensor
@@ -968,8 +992,9 @@ int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long 
     const int per_sm = std::max(1, std::min(512 / (int)tmem_cols, 232448 / (int)(total + 1024)));
     const size_t sm = std::max<size_t>(total, (size_t)(233472 / (per_sm + 1)) + 1024);
     set_smem_attr(kern, sm);
-    const int grid = (int)std::min<long>(nst, (long)nsm * per_sm);
-    kern<<<grid, threads, sm, st>>>(L.tstart.p, L.ent.p, (int)L.ntgt, L.T, ndsh, P,
+    // persistent: the CTAs take the super-tiles (counted on the device) in turn
+    const int grid = (int)std::min<long>((long)L.n, (long)nsm * per_sm);
+    kern<<<grid, threads, sm, st>>>(L.tstart.p, L.ent.p, L.info.p, ndsh, P,
                                     reinterpret_cast<const float4*>(L.tab.p), boxsize, nlev,
                                     reinterpret_cast<const float4*>(mp32), lo, err_dev);
     B2_LAUNCH_CHECK();

@@ -14,13 +14,16 @@ struct M2LPairs {
   DBuf<int2> ent;                   // (source | offset index << 26, last-entry mark)
   DBuf<float> tab;                  // G (TF32 hi, lo) and the per-offset tables
   DBuf<unsigned long long> steps;   // steps of all super-tiles (tensor-core work)
-  long ntgt = 0, npairs = 0;
-  int P = 0, T = 1;
+  DBuf<int> info;                   // device counts: targets, super-tile size T, entries
+  int n = 0;                        // candidate boxes (the arrays' size); 0: nothing to do
+  int P = 0;
   bool usable = false;  // false: box indices do not fit the packed format or P too large
 };
 
 // Builds L for boxes [first, first+n) (P coefficients; chunk = densities of
-// the main chunk, used only for the step count).
+// the main chunk, which sets the rows of a tile) without waiting on the
+// host: counts stay on the device.  first may be RANGE_FROM2 (boxes of
+// levels >= 2 from the tree's device level table, n = their upper bound).
 void m2l_tc_build(M2LPairs& L, const lapk::TV& t, int first, int n, int nboxes, int P, int chunk,
                   cudaStream_t st);
 

@@ -214,22 +214,7 @@ BoxPtrs ptrs(DeviceTree& T) {
                  nullptr,    T.ncoll.p, T.coll.p,   T.srng.p,   T.trng.p};
 }
 
-// Device control block of the tree build: level table, box count, status
-// and the grid barrier / scan scratch of the persistent build kernel.
-constexpr int TB_MAXG = 1024;    // most blocks of the build kernel
-constexpr int TB_THREADS = 512;  // threads per block (one block per SM)
-constexpr int TB_GROUPS = 8;     // first-level arrival counters of the grid barrier
 constexpr int TB_BIG = 16384;    // points of a refined box split by a warp
-struct TreeCtl {
-  int nboxes, nlevels, cap, status;
-  int lfirst[NLMAX + 2], llast[NLMAX + 2];
-  int tf[NLMAX + 2], tl[NLMAX + 2], lcnt[NLMAX + 2];
-  double bs[NLMAX + 3];
-  unsigned bar_sub[TB_GROUPS * 32];  // one 128-byte line per group
-  unsigned bar_top, bar_gen;
-  int tot[2][TB_MAXG];  // per-block counts of the scans, alternating
-};
-enum : int { TB_OK = 0, TB_OVERFLOW = 1, TB_DEEP = 2, TB_TIMEOUT = 3 };
 
 // Create the four children of parent b as boxes base..base+3 with the
 // reference's child order (-,-), (+,-), (-,+), (+,+).
@@ -502,56 +487,11 @@ __device__ void prefix_ranges(const uint64_t* __restrict__ skhi, int ns,
 // all blocks are resident).  Every wait is bounded; a barrier that gives up
 // sets TB_TIMEOUT, which releases the other blocks too.
 // ---------------------------------------------------------------------------
-constexpr long long TB_BAR_CYCLES = 1LL << 30;  // about half a second
-
 __device__ __forceinline__ int ctl_status(const TreeCtl* C) {
   return *reinterpret_cast<const volatile int*>(&C->status);
 }
 
-// Two-level grid barrier with acquire-release ordering at GPU scope: a block
-// arrives on its group counter, the last arrival of a group on the top
-// counter, and the last arrival there advances the generation word the
-// blocks wait on (ld.acquire), so every write made before the barrier by any
-// block is visible to every block after it.
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ unsigned atom_add_acqrel(unsigned* p, unsigned v) {
-  unsigned old;
-  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v)
-               : "memory");
-  return old;
-}
-
-__device__ bool gbar(TreeCtl* C) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned g0 = ld_acquire(&C->bar_gen);
-    const int G = gridDim.x, ng = min(TB_GROUPS, G), grp = blockIdx.x % ng;
-    const unsigned members = (unsigned)((G - grp + ng - 1) / ng);
-    unsigned* sub = &C->bar_sub[grp * 32];
-    if (atom_add_acqrel(sub, 1u) + 1 == members) {
-      *sub = 0;
-      if (atom_add_acqrel(&C->bar_top, 1u) + 1 == (unsigned)ng) {
-        C->bar_top = 0;
-        atom_add_acqrel(&C->bar_gen, 1u);
-      }
-    }
-    if (ld_acquire(&C->bar_gen) == g0) {
-      const long long t0 = clock64();
-      while (ld_acquire(&C->bar_gen) == g0) {
-        if (clock64() - t0 > TB_BAR_CYCLES || ctl_status(C) == TB_TIMEOUT) {
-          atomicExch(&C->status, TB_TIMEOUT);
-          break;
-        }
-      }
-    }
-  }
-  __syncthreads();
-  return ctl_status(C) != TB_TIMEOUT;
-}
+__device__ __forceinline__ bool gbar(TreeCtl* C) { return grid_barrier(C, TB_TIMEOUT); }
 
 // Item i of one box range [f1, f1+n1) or of two concatenated ranges.
 struct Items {
@@ -1092,10 +1032,11 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
 // list 1 starts with the coarser adjacent leaves (which the reference
 // appends while visiting the coarser level, in increasing box number), then
 // its own entries; its list 4 holds the coarser non-adjacent leaves.
-__global__ void k_lists(BoxPtrs B, int nb, const double* boxsize, int* nl1, int* l1, int* nl2,
-                        int* l2, int* nl3, int* l3, int* nl4, int* l4) {
+__global__ void k_lists(BoxPtrs B, const TreeCtl* C, int* nl1, int* l1, int* nl2, int* l2,
+                        int* nl3, int* l3, int* nl4, int* l4) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nb) return;
+  if (C->status != TB_OK || b >= C->nboxes) return;
+  const double* boxsize = C->bs;
   int n1 = 0, n2 = 0, n3 = 0, n4 = 0;
   int* L1 = l1 + (size_t)MNLIST1 * b;
   int* L2 = l2 + (size_t)MNLIST2 * b;
@@ -1234,72 +1175,167 @@ int tree_grid() {
 int* pinned_ints(int n) { return (int*)pinned_bytes(sizeof(int) * (size_t)n); }
 double* pinned_doubles(int n) { return (double*)pinned_bytes(sizeof(double) * (size_t)n); }
 
-void build_device_tree(DeviceTree& T, const double* src, long ns, const double* trg, long nt,
-                       int idivflag, int ndiv, int nlmax, cudaStream_t st) {
+namespace {
+
+// One build attempt on st with capacity cap: box arrays, hash table and
+// scratch, the root, the persistent build kernel.  Outcome in T.ctl.
+void launch_tree_attempt(DeviceTree& T, long ns, long nt, int idivflag, int ndiv, int nlmax,
+                         int cap, cudaStream_t st) {
+  alloc_boxes(T, cap);
+  DBuf<double2> sc(st);
+  DBuf<int> sl(st), sp(st), sn(st), sf(st), flag(st);
+  DBuf<int4> sch(st);
+  DBuf<uint64_t> pk1(st), pk2(st);
+  DBuf<unsigned long long> hkey(st);
+  DBuf<int> hbox(st);
+  unsigned hcap = 1;
+  while (hcap < 2u * (unsigned)cap) hcap <<= 1;
+  hkey.alloc(hcap, st);
+  hbox.alloc(hcap, st);
+  BoxHash H{hkey.p, hbox.p, hcap - 1};
+  sc.alloc(cap, st);
+  sl.alloc(cap, st);
+  sp.alloc(cap, st);
+  sn.alloc(cap, st);
+  sf.alloc(cap, st);
+  sch.alloc(cap, st);
+  flag.alloc(cap, st);
+  pk1.alloc(cap, st);
+  pk2.alloc(cap, st);
+  BoxPtrs B = ptrs(T);
+  B.pkey = pk1.p;
+  BoxPtrs S{sc.p, sl.p, sp.p, sn.p, sch.p, sf.p, pk2.p, nullptr, nullptr, nullptr, nullptr};
+  k_init_root<<<1, 1, 0, st>>>(B, T.root.p, (int)ns, (int)nt, T.ctl.p, cap);
+  B2_LAUNCH_CHECK();
+  TreeKeys K{T.skhi.p, T.sklo.p, T.tkhi.p, T.tklo.p};
+  TreeCtl* C = T.ctl.p;
+  int* fp = flag.p;
+  int nsi = (int)ns, nti = (int)nt;
+  int deep = T.deep_sorted ? 1 : 0;
+  void* args[] = {&B, &S, &C, &fp, &K, &H, &nsi, &nti, &idivflag, &ndiv, &nlmax, &deep};
+  B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(tree_grid()),
+                                       dim3(TB_THREADS), args, 0, st));
+  // the scratch above is released stream-ordered after the kernel
+}
+
+// Root box (bounding square of sources and targets) and the point sort by
+// the first 32 key levels.
+void tree_prologue(DeviceTree& T, const double* src, long ns, const double* trg, long nt,
+                   cudaStream_t st) {
   T.st = st;
   T.ns = ns;
   T.nt = nt;
   T.deep_sorted = false;
-  // root box
+  T.host_known = false;
   int nblk = std::max(1, std::min(ceil_div(std::max(ns, nt), 256), 1184));
   DBuf<double4> part(st);
   part.alloc(nblk, st);
   T.root.alloc(3, st);
+  T.ctl.alloc(1, st);
   k_bbox<<<nblk, 256, 0, st>>>(src, ns, trg, nt, part.p);
   B2_LAUNCH_CHECK();
   k_bbox_final<<<1, 256, 0, st>>>(part.p, nblk, T.root.p);
   B2_LAUNCH_CHECK();
-  // sort points along the virtual complete tree
   sort_by_key(src, ns, T.root.p, false, T.skhi, T.sklo, T.isrc, st);
   sort_by_key(trg, nt, T.root.p, false, T.tkhi, T.tklo, T.itarg, st);
-  // boxes: one persistent kernel builds the whole tree; it is re-run with
-  // more capacity (or with the 51-level keys) when it reports that need
+}
+
+// Lists 1-4 for at most nb_alloc boxes; the kernel takes the box count from
+// the control block (nothing after a failed build).
+void launch_lists(DeviceTree& T, int nb_alloc, cudaStream_t st) {
+  const int nb = nb_alloc;
+  T.nlist1.alloc(nb, st);
+  T.list1.alloc((size_t)MNLIST1 * nb, st);
+  T.nlist2.alloc(nb, st);
+  T.list2.alloc((size_t)MNLIST2 * nb, st);
+  T.nlist3.alloc(nb, st);
+  T.list3.alloc((size_t)MNLIST3 * nb, st);
+  T.nlist4.alloc(nb, st);
+  T.list4.alloc((size_t)MNLIST4 * nb, st);
+  k_lists<<<ceil_div(nb, 128), 128, 0, st>>>(ptrs(T), T.ctl.p, T.nlist1.p, T.list1.p,
+                                             T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p,
+                                             T.nlist4.p, T.list4.p);
+  B2_LAUNCH_CHECK();
+}
+
+std::mutex g_shape_mu;
+double g_cap_ratio = 3.0;  // boxes per (points / ndiv) of the largest tree seen
+struct Shape {
+  long npts;
+  int ndiv, nboxes, nlevels;
+};
+std::vector<Shape> g_shapes;  // most recent last, at most 64
+
+}  // namespace
+
+void note_tree_shape(long npts, int ndiv, int nboxes, int nlevels) {
+  if (npts <= 0) return;
+  const double r = (double)nboxes / ((double)npts / std::max(ndiv, 1));
+  std::lock_guard<std::mutex> g(g_shape_mu);
+  g_cap_ratio = std::max(g_cap_ratio, std::min(r, 64.0));
+  for (auto& e : g_shapes)
+    if (e.npts == npts && e.ndiv == ndiv) {
+      e.nboxes = nboxes;
+      e.nlevels = nlevels;
+      return;
+    }
+  if (g_shapes.size() >= 64) g_shapes.erase(g_shapes.begin());
+  g_shapes.push_back({npts, ndiv, nboxes, nlevels});
+}
+
+bool tree_shape(long npts, int ndiv, int* nboxes, int* nlevels) {
+  std::lock_guard<std::mutex> g(g_shape_mu);
+  for (auto& e : g_shapes)
+    if (e.npts == npts && e.ndiv == ndiv) {
+      *nboxes = e.nboxes;
+      *nlevels = e.nlevels;
+      return true;
+    }
+  return false;
+}
+
+int tree_capacity_guess(long npts, int ndiv, double margin) {
+  int nb = 0, nl = 0;
+  double c;
+  if (tree_shape(npts, ndiv, &nb, &nl)) {
+    c = margin * nb + 64;
+  } else {
+    double r;
+    {
+      std::lock_guard<std::mutex> g(g_shape_mu);
+      r = g_cap_ratio;
+    }
+    c = std::max(4.0, 1.15 * r) * ((double)npts / std::max(ndiv, 1)) + 64;
+  }
+  return (int)std::min(c, (double)(1 << 29));
+}
+
+void build_device_tree_async(DeviceTree& T, const double* src, long ns, const double* trg,
+                             long nt, int idivflag, int ndiv, int nlmax, int cap,
+                             cudaStream_t st) {
+  tree_prologue(T, src, ns, trg, nt, st);
+  cap = std::max(cap, 64);
+  launch_tree_attempt(T, ns, nt, idivflag, ndiv, nlmax, cap, st);
+  T.nboxes = cap;  // an upper bound until read back
+  T.nlevels = -1;
+  launch_lists(T, cap, st);
+}
+
+void build_device_tree(DeviceTree& T, const double* src, long ns, const double* trg, long nt,
+                       int idivflag, int ndiv, int nlmax, cudaStream_t st) {
+  tree_prologue(T, src, ns, trg, nt, st);
+  // one persistent kernel builds the whole tree; it is re-run with more
+  // capacity (or with the 51-level keys) when it reports that need
   int cap = (int)std::min<long>(8 + 3 * (ns + nt) / std::max(ndiv, 1), 1L << 30);
   cap = std::max(cap, 64);
-  DBuf<TreeCtl> ctl(st);
-  ctl.alloc(1, st);
-  const int grid = tree_grid();
   // control block and root box read back together after each build attempt
   char* hbuf = (char*)pinned_bytes(sizeof(TreeCtl) + 4 * sizeof(double));
   TreeCtl* hc = (TreeCtl*)hbuf;
   double* hr = (double*)(hbuf + sizeof(TreeCtl));
   static_assert(sizeof(TreeCtl) % sizeof(double) == 0, "root after the control block");
   for (;;) {
-    alloc_boxes(T, cap);
-    DBuf<double2> sc(st);
-    DBuf<int> sl(st), sp(st), sn(st), sf(st), flag(st);
-    DBuf<int4> sch(st);
-    DBuf<uint64_t> pk1(st), pk2(st);
-    DBuf<unsigned long long> hkey(st);
-    DBuf<int> hbox(st);
-    unsigned hcap = 1;
-    while (hcap < 2u * (unsigned)cap) hcap <<= 1;
-    hkey.alloc(hcap, st);
-    hbox.alloc(hcap, st);
-    BoxHash H{hkey.p, hbox.p, hcap - 1};
-    sc.alloc(cap, st);
-    sl.alloc(cap, st);
-    sp.alloc(cap, st);
-    sn.alloc(cap, st);
-    sf.alloc(cap, st);
-    sch.alloc(cap, st);
-    flag.alloc(cap, st);
-    pk1.alloc(cap, st);
-    pk2.alloc(cap, st);
-    BoxPtrs B = ptrs(T);
-    B.pkey = pk1.p;
-    BoxPtrs S{sc.p, sl.p, sp.p, sn.p, sch.p, sf.p, pk2.p, nullptr, nullptr, nullptr, nullptr};
-    k_init_root<<<1, 1, 0, st>>>(B, T.root.p, (int)ns, (int)nt, ctl.p, cap);
-    B2_LAUNCH_CHECK();
-    TreeKeys K{T.skhi.p, T.sklo.p, T.tkhi.p, T.tklo.p};
-    TreeCtl* C = ctl.p;
-    int* fp = flag.p;
-    int nsi = (int)ns, nti = (int)nt;
-    int deep = T.deep_sorted ? 1 : 0;
-    void* args[] = {&B, &S, &C, &fp, &K, &H, &nsi, &nti, &idivflag, &ndiv, &nlmax, &deep};
-    B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(grid), dim3(TB_THREADS),
-                                         args, 0, st));
-    B2_CHECK(cudaMemcpyAsync(hc, ctl.p, sizeof(TreeCtl), cudaMemcpyDeviceToHost, st));
+    launch_tree_attempt(T, ns, nt, idivflag, ndiv, nlmax, cap, st);
+    B2_CHECK(cudaMemcpyAsync(hc, T.ctl.p, sizeof(TreeCtl), cudaMemcpyDeviceToHost, st));
     B2_CHECK(cudaMemcpyAsync(hr, T.root.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     B2_CHECK(cudaStreamSynchronize(st));
     if (hc->status == TB_DEEP && !T.deep_sorted) {
@@ -1317,6 +1353,7 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
     if (hc->status != TB_OK) throw CudaError("tree build: grid barrier timed out", IER_TIMEOUT);
     break;
   }
+  T.host_known = true;
   T.nlevels = hc->nlevels;
   T.nboxes = hc->nboxes;
   T.lfirst.assign(hc->lfirst, hc->lfirst + T.nlevels + 1);
@@ -1325,22 +1362,8 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   T.bs0 = hc->bs[0];
   T.cx0 = hr[0];
   T.cy0 = hr[1];
-  // interaction lists (boxsize(nlevels+1) for the leaf tests is in the control block)
-  int nb = T.nboxes;
-  T.nlist1.alloc(nb, st);
-  T.list1.alloc((size_t)MNLIST1 * nb, st);
-  T.nlist2.alloc(nb, st);
-  T.list2.alloc((size_t)MNLIST2 * nb, st);
-  T.nlist3.alloc(nb, st);
-  T.list3.alloc((size_t)MNLIST3 * nb, st);
-  T.nlist4.alloc(nb, st);
-  T.list4.alloc((size_t)MNLIST4 * nb, st);
-  k_lists<<<ceil_div(nb, 128), 128, 0, st>>>(ptrs(T), nb, &ctl.p->bs[0], T.nlist1.p, T.list1.p,
-                                             T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p,
-                                             T.nlist4.p, T.list4.p);
-  B2_LAUNCH_CHECK();
-  // no synchronisation: the lists are read by later work on st; the control
-  // block is released (stream-ordered) after k_lists has read its box sizes
+  note_tree_shape(ns + nt, ndiv, T.nboxes, T.nlevels);
+  launch_lists(T, T.nboxes, st);
 }
 
 }  // namespace b2

@@ -34,6 +34,11 @@ typedef struct b2fmm_options {
   int idivflag;  /* 0: subdivide on sources, 1: targets, 2: max of both    */
   int ifnear;    /* 1: include list-1 near field (P2P), 0: far field only  */
   int precision; /* 0 auto (mixed when eps >= 1e-6), 1 FP64, 2 mixed        */
+  int async_call; /* b2fmm_{c,l,r}fmm2d_dev only (no counterpart in the
+                     reference): 1 returns once the whole call is queued on
+                     the stream, with no host wait; device-side failures are
+                     reported by b2fmm_async_status.  Ignored (synchronous)
+                     when timeinfo or statistics are requested. */
 } b2fmm_options;
 
 /* Library version string. */
@@ -308,9 +313,25 @@ uint64_t b2fmm_kernel_launches(void);
  * nterms+1, P2P pairs, M2L translations, M2P evaluations, P2L sources,
  * evaluation points, tree build ms, FMM ms after the tree, Cauchy densities,
  * tensor-core M2L steps (128-row MMA steps over all super-tiles; 0 when not
- * used). */
+ * used), then the device timeline of the call in ms: start to tree start,
+ * tree, tree end to the first FMM pass, the FMM passes, last pass to the end
+ * of the call. */
 void b2fmm_set_stats(int on);
 void b2fmm_get_stats(double* out, int n);
+
+/* Waits for `stream` and returns in *ier the first failure of the
+ * asynchronous calls (options.async_call = 1) queued on the current device
+ * since the last query, then clears it: 0, 102 (a bounded device wait gave
+ * up) or 104 (a call's tree needed more boxes or levels than a call without
+ * read-back allows: repeat it synchronously).  No counterpart in the
+ * reference, whose calls are all blocking. */
+void b2fmm_async_status(void* stream, int* ier);
+
+/* Laplace / Cauchy calls take their box ranges from the tree's device
+ * level table, so the host does not wait for the tree in the middle of a
+ * call (1, the default); 0 reads every tree back first and launches the
+ * upward and downward passes level by level.  Results are the same. */
+void b2fmm_set_device_ranges(int on);
 
 /* Measured fused-multiply-add throughput of this GPU in flop/s (FP64 when
  * fp64 != 0, else FP32), from a dependent-free FMA loop over all SMs. */
