@@ -8,13 +8,23 @@ and gradient at the sources); seeded synthetic data (numpy default_rng(1)).
 
 A step is one complete FMM call (tree, lists, all passes, caller-order
 results).  ``value`` times it with inputs resident in HBM (device-pointer C
-ABI b2fmm_lfmm2d_dev) in the mixed-precision mode; ``fp64_value`` is the
-plain FP64 GPU FMM on the same inputs; ``e2e`` calls the reference-named host
-entry point b2fmm_lfmm2d with pinned host buffers (H2D + FMM + D2H per step).
-Every run reports the relative l2 error of pot+grad against the FP64 direct
-sum over 1000 random sources.  ``--impl reference`` times the CPU oracle (the
-C++ restatement of the reference algorithm; the Fortran reference cannot be
-built here) on a bounded sample of the same workload with all host threads.
+ABI b2fmm_lfmm2d_dev) in the mixed-precision mode; the K timed calls are
+queued back to back (options.async_call: no host wait inside or between
+them) and their device status is checked after the timing.  ``fp64_value``
+is the plain FP64 GPU FMM on the same inputs, timed the same way; ``e2e``
+calls the host-pointer entry point b2fmm_lfmm2d_ex with pinned host buffers
+(H2D + FMM + D2H per step, one wait per call).  Every run reports the
+relative l2 error of pot+grad against the FP64 direct sum over 1000 random
+sources.  ``--impl reference`` times the reference itself (its Fortran
+translated to C by oracle/f77c.py, gcc -O3 -fopenmp; no Fortran compiler
+exists here) on a bounded sample of the same workload with all host
+threads; ``cpu_baseline`` is the same code on a 1M-point sample.
+
+Lines printed before the headline line: ``lfmm2d_eps_sweep`` (the headline
+workload at eps 1e-3, mixed, and 1e-9, FP64, with their errors);
+``rfmm2d_c1`` (plain rfmm2d, 100,000 uniform sources, real N(0,1) charges,
+eps 1e-6, pg 2: FP64 and mixed GPU time, the reference on the host cores and
+the FP64 GPU result against the reference's); ``roofline_detail``.
 
 ``helmholtz_c4`` adds the Helmholtz configuration: hfmm2d with zk = 40 on
 2,000,000 sources at uniform random angles on the curve
@@ -377,39 +387,52 @@ def dist_info():
     return rank, world, local
 
 
-def cpu_baseline(n_sample, reps=1):
-    """Oracle (C++ restatement of the reference algorithm) on a bounded sample."""
+REF_KIND = ("the reference's own Fortran (src/laplace, src/common), translated to C by "
+            "oracle/f77c.py and compiled with gcc -O3 -funroll-loops -fopenmp")
+
+
+def _ref_module():
+    """The reference itself (oracle/_ref) when built, else the C++ restatement."""
+    from oracle import ref as R
+    if R.available():
+        return R, "reference"
     from oracle import oracle as O
     O.build()
-    O.set_num_threads(os.cpu_count() or 1)
+    return O, "port"
+
+
+def cpu_baseline(n_sample, reps=1):
+    """The reference's lfmm2d on a bounded sample, all host threads."""
+    M, kind = _ref_module()
+    M.set_num_threads(os.cpu_count() or 1)
     src, q, d, v = make_inputs(n_sample, seed=1)
-    O.lfmm2d(1e-6, src[:, :20000], charges=q[:20000], dipstr=d[:20000], dipvec=v[:, :20000],
+    M.lfmm2d(1e-6, src[:, :20000], charges=q[:20000], dipstr=d[:20000], dipvec=v[:, :20000],
              ifpgh=2)  # warm-up
     ts = []
     for _ in range(reps):
         t0 = time.perf_counter()
-        O.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
+        M.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
         ts.append(time.perf_counter() - t0)
     t = min(ts)
-    return {"value": n_sample / t, "unit": "points/s", "cores": O.num_threads(), "kind": "port",
+    return {"value": n_sample / t, "unit": "points/s", "cores": M.num_threads(), "kind": kind,
             "sample": f"{n_sample} points of the same 16-Gaussian mixture (seed 1), one lfmm2d "
-                      f"call, eps=1e-6, pg=2; {t:.2f} s"}
+                      f"call, eps=1e-6, pg=2; {t:.2f} s"
+                      + (f"; {REF_KIND}" if kind == "reference" else "")}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     n_sample = args.ref_sample
-    from oracle import oracle as O
-    O.build()
-    O.set_num_threads(os.cpu_count() or 1)
+    M, kind = _ref_module()
+    M.set_num_threads(os.cpu_count() or 1)
     src, q, d, v = make_inputs(n_sample, seed=1)
     for _ in range(args.warmup):
-        O.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
+        M.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
     ts = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        O.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
+        M.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
         ts.append(time.perf_counter() - t0)
     t = sum(ts) / len(ts)
     val = n_sample / t
@@ -418,20 +441,150 @@ def run_reference(args, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": WORKLOAD + f"; bounded sample n={n_sample}",
                                             "n_points": n_sample, "eps": 1e-6},
-            "cpu_baseline": {"value": val, "unit": "points/s", "cores": O.num_threads(),
-                             "kind": "port",
-                             "sample": f"{n_sample} points of the same mixture per step"},
+            "cpu_baseline": {"value": val, "unit": "points/s", "cores": M.num_threads(),
+                             "kind": kind,
+                             "sample": f"{n_sample} points of the same mixture per step"
+                                       + (f"; {REF_KIND}" if kind == "reference" else "")},
             "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def _lfmm_dev(L, n, ds, dq, dd, dv, pot, grad, stream, eps, precision, async_call=0,
+              timeinfo=None):
+    from fmm2d_b200 import _lib
+    o = _lib.Options()
+    o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, _lib.PREC[precision]
+    o.async_call = async_call
+    ier = C.c_int(0)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    ti = timeinfo.ctypes.data_as(C.c_void_p) if timeinfo is not None else None
+    L.b2fmm_lfmm2d_dev(1, C.c_double(eps), C.c_int64(n), ptr(ds), 1, ptr(dq), 1, ptr(dd),
+                       ptr(dv), 2, ptr(pot), ptr(grad), None, C.c_int64(0), None, 0, None,
+                       None, None, C.byref(o), ti, C.c_void_p(stream.cuda_stream), C.byref(ier))
+    if ier.value != 0:
+        raise RuntimeError(f"b2fmm_lfmm2d_dev ier={ier.value}")
+
+
+def async_status(L, stream):
+    ier = C.c_int(-1)
+    L.b2fmm_async_status(C.c_void_p(stream.cuda_stream), C.byref(ier))
+    if ier.value != 0:
+        raise RuntimeError(f"asynchronous FMM calls failed: ier={ier.value}")
+
+
+def rel_err_vs_direct(L, ds, dq, dd, dv, src, n, pot, grad, stream, dev, seed=99):
+    """comperr-style relative l2 error of pot+grad against the FP64 direct sum
+    over 1000 random sources."""
+    import torch
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(n, 1000, replace=False))
+    tsel = torch.as_tensor(np.ascontiguousarray(src[:, idx].T), device=dev)
+    ep = torch.empty((1000, 1), dtype=torch.complex128, device=dev)
+    eg = torch.empty((1000, 2, 1), dtype=torch.complex128, device=dev)
+    ier = C.c_int(0)
+    L.b2fmm_lap_direct_dev(1, 1, C.c_int64(n), ptr(ds), ptr(dq), ptr(dd), ptr(dv),
+                           C.c_int64(1000), ptr(tsel), 2, ptr(ep), ptr(eg), None,
+                           C.c_double(1e-16), C.c_void_p(stream.cuda_stream), C.byref(ier))
+    ia = torch.as_tensor(idx, device=dev)
+    a_p, a_g = pot[ia, 0].cpu().numpy(), grad[ia, :, 0].cpu().numpy()
+    e_p, e_g = ep[:, 0].cpu().numpy(), eg[:, :, 0].cpu().numpy()
+    return float(np.sqrt((np.linalg.norm(a_p - e_p) ** 2 + np.linalg.norm(a_g - e_g) ** 2)
+                         / (np.linalg.norm(e_p) ** 2 + np.linalg.norm(e_g) ** 2)))
+
+
+def c2_eps_sweep(L, n, ds, dq, dd, dv, src, pot, grad, stream, dev, steps=5):
+    """The headline workload at eps 1e-3 and 1e-9: mixed (1e-3) and FP64
+    (1e-9, below the mixed path's range) device time and error."""
+    import torch
+    out = {}
+    for eps in (1e-3, 1e-9):
+        precision = "mixed" if eps >= 1e-6 else "fp64"
+        for _ in range(2):
+            _lfmm_dev(L, n, ds, dq, dd, dv, pot, grad, stream, eps, precision)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            _lfmm_dev(L, n, ds, dq, dd, dv, pot, grad, stream, eps, precision, async_call=1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        async_status(L, stream)
+        ms = e0.elapsed_time(e1) / steps
+        out[f"eps_{eps:g}"] = {"precision": precision, "ms_per_step": ms,
+                               "value": n / (ms * 1e-3), "unit": "points/s", "eps": eps,
+                               "rel_l2_err": rel_err_vs_direct(L, ds, dq, dd, dv, src, n, pot,
+                                                               grad, stream, dev)}
+    return out
+
+
+def rfmm_c1(L, dev, stream, steps=20, cpu=True):
+    """Plain rfmm2d: 100,000 uniform sources, real N(0,1) charges, eps 1e-6,
+    pg 2, no targets; FP64 and mixed GPU device time, and the reference's own
+    CPU code on the same inputs with all host threads."""
+    import torch
+    from fmm2d_b200 import _lib
+    n = 100_000
+    rng = np.random.default_rng(0)
+    src = rng.uniform(0, 1, (2, n))
+    q = rng.normal(size=n)
+    ds = torch.as_tensor(np.ascontiguousarray(src.T), device=dev)
+    dq = torch.as_tensor(q.reshape(n, 1), device=dev)
+    pot = torch.empty((n, 1), dtype=torch.float64, device=dev)
+    grad = torch.empty((n, 2, 1), dtype=torch.float64, device=dev)
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    res = {"workload": "rfmm2d 100,000 uniform sources, real N(0,1) charges, eps=1e-6, pg=2",
+           "n": n, "unit": "points/s"}
+
+    def call(precision, async_call):
+        o = _lib.Options()
+        o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, _lib.PREC[precision]
+        o.async_call = async_call
+        ier = C.c_int(0)
+        L.b2fmm_rfmm2d_dev(1, C.c_double(1e-6), C.c_int64(n), ptr(ds), 1, ptr(dq), 0, None, None,
+                           2, ptr(pot), ptr(grad), None, C.c_int64(0), None, 0, None, None, None,
+                           C.byref(o), None, C.c_void_p(stream.cuda_stream), C.byref(ier))
+        if ier.value != 0:
+            raise RuntimeError(f"b2fmm_rfmm2d_dev ier={ier.value}")
+
+    for precision in ("fp64", "mixed"):
+        for _ in range(3):
+            call(precision, 0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            call(precision, 1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        async_status(L, stream)
+        ms = e0.elapsed_time(e1) / steps
+        res[precision] = {"ms_per_step": ms, "value": n / (ms * 1e-3)}
+    if cpu:
+        M, kind = _ref_module()
+        M.set_num_threads(os.cpu_count() or 1)
+        M.rfmm2d(1e-6, src, charges=q, ifpgh=2)
+        ts = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            r = M.rfmm2d(1e-6, src, charges=q, ifpgh=2)
+            ts.append(time.perf_counter() - t0)
+        t = min(ts)
+        res["cpu"] = {"value": n / t, "ms_per_step": t * 1e3, "cores": M.num_threads(),
+                      "kind": kind}
+        # the FP64 GPU result against the reference's own output
+        call("fp64", 0)
+        torch.cuda.synchronize()
+        a = pot[:, 0].cpu().numpy()
+        res["fp64_rel_diff_vs_cpu"] = float(np.linalg.norm(a - r["pot"][0])
+                                            / np.linalg.norm(r["pot"][0]))
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    # 50 calls (~0.6 s timed): the GPU waits on the host a few times a call,
-    # and the shared hosts now and then stall a process for tenths of a
-    # second; a longer timed region keeps one stall from dominating the mean
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -445,6 +598,8 @@ def main():
     ap.add_argument("--c4-scale", type=float, default=1.0)
     ap.add_argument("--no-c3", action="store_true", help="skip the batched configuration")
     ap.add_argument("--no-c5", action="store_true", help="skip the cost-model sweep")
+    ap.add_argument("--no-c1", action="store_true", help="skip the plain rfmm2d configuration")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the eps 1e-3 / 1e-9 runs")
     ap.add_argument("--c3-only", action="store_true", help="run only the batched configuration")
     args = ap.parse_args()
     rank, world, local = dist_info()
@@ -463,14 +618,14 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         pg = dist
     L = _lib.lib()
+    stream = torch.cuda.current_stream(dev)
     if args.c3_only:
         res = batched_c3(L, dev)
         if rank == 0:
             print(json.dumps({"batched_c3": res}), flush=True)
         return
     if args.c4_only:
-        res = helmholtz_c4(L, dev, torch.cuda.current_stream(dev), args.c4_scale,
-                           max(1, args.steps), max(1, args.warmup))
+        res = helmholtz_c4(L, dev, stream, args.c4_scale, max(1, args.steps), max(1, args.warmup))
         if rank == 0:
             print(json.dumps({"helmholtz_c4": res}), flush=True)
         return
@@ -480,22 +635,10 @@ def main():
     ds, dq, dd, dv = (torch.as_tensor(x, device=dev) for x in (hs, hq, hd, hv))
     pot = torch.empty((n, 1), dtype=torch.complex128, device=dev)
     grad = torch.empty((n, 2, 1), dtype=torch.complex128, device=dev)
-    stream = torch.cuda.current_stream(dev)
     ptr = lambda t: C.c_void_p(t.data_ptr())
 
-    def step(precision, timeinfo=None):
-        o = _lib.Options()
-        o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, _lib.PREC[precision]
-        ier = C.c_int(0)
-        # phase times only when asked for: reading them makes the host wait for
-        # each density chunk
-        ti = timeinfo.ctypes.data_as(C.c_void_p) if timeinfo is not None else None
-        L.b2fmm_lfmm2d_dev(1, C.c_double(1e-6), C.c_int64(n), ptr(ds), 1, ptr(dq), 1, ptr(dd),
-                           ptr(dv), 2, ptr(pot), ptr(grad), None, C.c_int64(0), None, 0, None,
-                           None, None, C.byref(o), ti,
-                           C.c_void_p(stream.cuda_stream), C.byref(ier))
-        if ier.value != 0:
-            raise RuntimeError(f"b2fmm_lfmm2d_dev ier={ier.value}")
+    def step(precision, timeinfo=None, async_call=0):
+        _lfmm_dev(L, n, ds, dq, dd, dv, pot, grad, stream, 1e-6, precision, async_call, timeinfo)
 
     def timed(precision, steps, warmup, with_clocks=False):
         # the clock sampler runs from before the warm-up to after the timed steps
@@ -504,21 +647,24 @@ def main():
             sampler.start()
         for _ in range(warmup):
             step(precision)
-        tis = np.zeros(8)
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
         L0 = L.b2fmm_kernel_launches()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        # the steps are queued back to back (asynchronous calls: no host wait
+        # inside or between them); their outcome is checked after the timing
         e0.record(stream)
         for _ in range(steps):
-            step(precision)
+            step(precision, async_call=1)
         e1.record(stream)
         torch.cuda.synchronize()
         launches = L.b2fmm_kernel_launches() - L0
         clocks = sampler.stop() if sampler else None
-        # phase times from three more (untimed) calls
+        async_status(L, stream)
+        # phase times from three more (untimed, synchronous) calls
+        tis = np.zeros(8)
         for _ in range(3):
             ti = np.zeros(8)
             step(precision, ti)
@@ -528,10 +674,9 @@ def main():
 
     prec = args.precision
     # Process warm-up before the first timed loop: in a fresh process the first
-    # few dozen calls run ~1 ms slower each (stream-ordered pool growth, lazily
-    # loaded kernels, clock ramp), which W = 3 warm-up calls do not cover.
-    # About one second of untimed calls is spent here; the W warm-up calls of
-    # timed() follow as usual.
+    # calls run slower (stream-ordered pool growth, lazily loaded kernels, clock
+    # ramp), which W = 3 warm-up calls do not cover.  About one second of
+    # untimed calls is spent here; the W warm-up calls of timed() follow.
     prewarm_s = 1.0
     t_end = time.perf_counter() + prewarm_s
     while time.perf_counter() < t_end:
@@ -563,7 +708,8 @@ def main():
     nd2 = st["nd_cauchy"]
     P = st["nterms1"]
     # algorithmic flops (FMA = 2): P2P charge+dipole pot+grad per pair 15 + 28*nd2
-    # (per pair: 15 real flops for the kernel terms, 28 per density); M2L per translation 2*P*P real MACs x 2 (re,im) x nd2
+    # (per pair: 15 real flops for the kernel terms, 28 per density); M2L per
+    # translation 2*P*P real MACs x 2 (re,im) x nd2
     flops = {"leaf_eval(l2p+m2p+p2p)": st["p2p_pairs"] * (15 + 28 * nd2)
              + st["npts_eval"] * 16 * P * nd2 + st["m2p_evals"] * 16 * P * nd2,
              "m2l": st["m2l_pairs"] * 4 * P * P * nd2}
@@ -615,23 +761,10 @@ def main():
             pass
 
     # accuracy against the FP64 direct sum on 1000 random sources
-    rng = np.random.default_rng(99)
-    idx = np.sort(rng.choice(n, 1000, replace=False))
     step(prec)
-    pot_h = pot[:, 0].cpu().numpy()
-    grad_h = grad[:, :, 0].cpu().numpy()
-    tsel = torch.as_tensor(np.ascontiguousarray(src[:, idx].T), device=dev)
-    ep = torch.empty((1000, 1), dtype=torch.complex128, device=dev)
-    eg = torch.empty((1000, 2, 1), dtype=torch.complex128, device=dev)
-    ier = C.c_int(0)
-    L.b2fmm_lap_direct_dev(1, 1, C.c_int64(n), ptr(ds), ptr(dq), ptr(dd), ptr(dv),
-                           C.c_int64(1000), ptr(tsel), 2, ptr(ep), ptr(eg), None,
-                           C.c_double(1e-16), C.c_void_p(stream.cuda_stream), C.byref(ier))
-    ex_p = ep[:, 0].cpu().numpy()
-    ex_g = eg[:, :, 0].cpu().numpy()
-    num = np.linalg.norm(pot_h[idx] - ex_p) ** 2 + np.linalg.norm(grad_h[idx] - ex_g) ** 2
-    den = np.linalg.norm(ex_p) ** 2 + np.linalg.norm(ex_g) ** 2
-    err = float(np.sqrt(num / den))
+    err = rel_err_vs_direct(L, ds, dq, dd, dv, src, n, pot, grad, stream, dev)
+    step("fp64")
+    err64 = rel_err_vs_direct(L, ds, dq, dd, dv, src, n, pot, grad, stream, dev)
 
     # end to end through the reference-named host entry point, pinned buffers
     hsrc = torch.as_tensor(hs).pin_memory()
@@ -648,7 +781,8 @@ def main():
         L.b2fmm_lfmm2d_ex(1, C.c_double(1e-6), C.c_int64(n), ptr(hsrc), 1, ptr(hq_), 1, ptr(hd_),
                           ptr(hv_), 2, ptr(hpot), ptr(hgrad), None, C.c_int64(0), None, 0, None,
                           None, None, C.byref(o), None, C.byref(ier))
-        return ier.value
+        if ier.value != 0:
+            raise RuntimeError(f"b2fmm_lfmm2d_ex ier={ier.value}")
 
     for _ in range(max(1, args.warmup - 1)):
         e2e_step()
@@ -661,10 +795,18 @@ def main():
     h2d = hsrc.numel() * 8 + hq_.numel() * 16 + hd_.numel() * 16 + hv_.numel() * 8
     d2h = hpot.numel() * 16 + hgrad.numel() * 16
 
-    c3 = None
+    # the other configurations, each on a line of its own before the headline
+    def emit(key, obj):
+        if rank == 0 and obj is not None:
+            print(json.dumps({key: obj}), flush=True)
+
+    if not args.no_sweep:
+        emit("lfmm2d_eps_sweep", c2_eps_sweep(L, n, ds, dq, dd, dv, src, pot, grad, stream, dev))
+    if not args.no_c1:
+        emit("rfmm2d_c1", rfmm_c1(L, dev, stream, cpu=(rank == 0 and world == 1
+                                                      and not args.no_cpu_baseline)))
     if not args.no_c3:
-        c3 = batched_c3(L, dev)
-    c5 = None
+        emit("batched_c3", batched_c3(L, dev))
     if not args.no_c5:
         from fmm2d_b200 import costmodel as cm
         model = cm.CostModel.load()
@@ -674,34 +816,36 @@ def main():
             c5["workload"] = ("40 rfmm2d problems, N log-uniform [1e4, 8e6], uniform / "
                               "16-Gaussian mixture / graded curve, eps in {1e-3, 1e-6}, pg=2")
             c5["ndiv_mlp"] = [r["ndiv_mlp"] for r in res["rows"]]
-    c4 = None
+            emit("costmodel_c5", c5)
     if not args.no_c4:
-        c4 = helmholtz_c4(L, dev, stream, args.c4_scale)
+        emit("helmholtz_c4", helmholtz_c4(L, dev, stream, args.c4_scale))
+    emit("roofline_detail", roofline)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_sample)
 
     if rank == 0:
+        # the headline line last, compact: the sub-configurations are above
+        rl = {k: roofline[k] for k in ("bound", "kernel", "achieved", "peak", "unit", "frac",
+                                       "traffic", "peak_source")}
+        rl["phase_ms"] = phases_ms
         line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "speedup_vs_fp64": value / value64, "fp64_value": value64,
+                "fp64_ms_per_step": ms64, "rel_l2_err": err, "fp64_rel_l2_err": err64,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64" if prec == "mixed" else "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD, "n_points_per_gpu": n, "eps": 1e-6,
                            "precision": prec, "parallelism": f"replicas x{world}",
-                           "m2l_engine": ("tcgen05 split-TF32 (FP32 accumulate in TMEM)"
-                                          if prec == "mixed" else "FP64 CUDA cores"),
-                           "l2_policy": "inputs (256 MB) and expansions larger than L2",
-                           "prewarm_s": prewarm_s},
-                "fp64_value": value64, "fp64_ms_per_step": ms64,
+                           "calls": "queued back to back (asynchronous), checked after",
+                           "l2_policy": "inputs (256 MB) and expansions larger than L2"},
+                "err_ref": "FP64 direct sum over 1000 random sources",
                 "mixed_cuda_core_m2l_ms_per_step": ms_cc,
-                "speedup_vs_fp64": value / value64,
-                "rel_l2_err": err, "err_ref": "FP64 direct sum over 1000 random sources",
                 "e2e": {"value": world * n / te, "unit": "points/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": int(launches),
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
-                "helmholtz_c4": c4, "batched_c3": c3, "costmodel_c5": c5}
+                "roofline": rl, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
