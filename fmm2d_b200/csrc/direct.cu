@@ -238,7 +238,10 @@ namespace b2 {
 // In host code `g_direct_scratch` only names a host-side stand-in, not the
 // device address, so the first call on each device looks the address up with
 // cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture.  All calls share the one array and it
+// first call before any stream capture, and before the device's memory is
+// handed to another allocator: with CUDA's lazy module loading it may be the
+// look-up that loads this module and reserves the array (or set
+// CUDA_MODULE_LOADING=EAGER).  All calls share the one array and it
 // keeps the last call's contents: the first kernel writes every element the
 // second one reads, so nothing needs clearing, but calls that overlap on the
 // GPU (other streams, other host threads) race on it and must be serialised
@@ -255,14 +258,17 @@ double2* g_scratch_addr[128] = {nullptr};
 double2* scratch_address() {
   int dev = 0;
   B2_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) throw CudaError("device ordinal beyond 127", IER_BADARG);
   std::lock_guard<std::mutex> g(g_scratch_mu);
   if (!g_scratch_addr[dev]) {
     void* p = nullptr;
+    // with lazy module loading this first look-up may be what loads the
+    // module and reserves the array: out of memory then is IER_ALLOC
     cudaError_t e = cudaGetSymbolAddress(&p, g_direct_scratch);
     if (e != cudaSuccess || !p)
       throw CudaError(std::string("cudaGetSymbolAddress(g_direct_scratch): ") +
                           cudaGetErrorString(e),
-                      IER_CUDA);
+                      e == cudaErrorMemoryAllocation ? IER_ALLOC : IER_CUDA);
     g_scratch_addr[dev] = (double2*)p;
   }
   return g_scratch_addr[dev];

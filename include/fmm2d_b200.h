@@ -147,9 +147,12 @@ void b2fmm_lap_direct_dev(int kind, int nd, int64_t ns, const double* sources,
  * loads the library holds until exit.  Limit: nt*3 (kind 0) or nt*6
  * (kinds 1, 2) <= 262144, i.e. at most 87381 / 43690 targets per call;
  * larger nt returns ier = 103 without computing.  The first call on a device
- * looks up the array's device address, so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race on it and
- * must be serialised by the caller. */
+ * looks up the array's device address, so make it before any stream capture,
+ * and before the device's memory is handed to another allocator: with lazy
+ * module loading that look-up may be what reserves the array (ier = 4 when
+ * the device has no room left; CUDA_MODULE_LOADING=EAGER reserves it at
+ * load).  All calls share the array: calls that overlap on the GPU race on
+ * it and must be serialised by the caller. */
 void b2fmm_lap_direct_noalloc_dev(int kind, int nd, int64_t ns, const double* sources,
                                   const double* charge, const double* dipstr,
                                   const double* dipvec, int64_t nt, const double* targ,

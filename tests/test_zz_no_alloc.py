@@ -84,3 +84,26 @@ def test_noalloc_rejects_oversize(gpu):
     assert _call(L.b2fmm_lap_direct_noalloc_dev, 1, 1, src, q, d, v, trg, outs, stream) == 103
     torch.cuda.synchronize()
     assert bool((outs[0] == 7.0).all())
+
+
+@pytest.mark.parametrize("kind,limit", [(0, 262144 // 3), (1, 262144 // 6)])
+def test_noalloc_at_the_limit_and_one_beyond(gpu, kind, limit):
+    """Exactly as many targets as the static scratch holds (one slice of
+    partial sums) matches the allocating entry point; one more is refused."""
+    import torch
+    from fmm2d_b200 import _lib
+    L = _lib.lib()
+    stream = torch.cuda.current_stream(gpu).cuda_stream
+    src, trg, q, d, v = _inputs(gpu, kind, 300, limit + 1, 1, seed=20 + kind)
+    ref = _outputs(gpu, kind, limit, 1)
+    got = _outputs(gpu, kind, limit, 1)
+    assert _call(L.b2fmm_lap_direct_dev, kind, 1, src, q, d, v, trg[:limit], ref, stream) == 0
+    assert _call(L.b2fmm_lap_direct_noalloc_dev, kind, 1, src, q, d, v, trg[:limit], got,
+                 stream) == 0
+    torch.cuda.synchronize()
+    for a, b in zip(got, ref):
+        assert _rel(a, b) < TOL
+    over = _outputs(gpu, kind, limit + 1, 1)
+    assert _call(L.b2fmm_lap_direct_noalloc_dev, kind, 1, src, q, d, v, trg, over, stream) == 103
+    torch.cuda.synchronize()
+    assert bool((over[0] == 7.0).all())
