@@ -58,6 +58,8 @@ SIGNATURES = {
     "b2fmm_set_stats": [c_int],
     "b2fmm_set_device_ranges": [c_int],
     "b2fmm_async_status": [P, P],
+    "b2fmm_test_fail_alloc": [c_int],
+    "b2fmm_test_barrier_limit": [C.c_longlong],
     "b2fmm_get_stats": [P, c_int],
     "b2fmm_fma_peak": [c_int],
     "b2fmm_set_m2l_tensor_cores": [c_int],

@@ -16,6 +16,17 @@
 
 namespace b2 {
 std::atomic<unsigned long long> g_launches{0};
+
+// allocation fault injection (b2fmm_test_fail_alloc): -1 off, else the
+// number of allocations that still succeed before one fails
+std::atomic<int> g_fail_after{-1};
+bool alloc_fault_due() {
+  int v = g_fail_after.load(std::memory_order_relaxed);
+  while (v >= 0) {
+    if (g_fail_after.compare_exchange_weak(v, v - 1)) return v == 0;
+  }
+  return false;
+}
 }
 
 using namespace b2;
@@ -702,6 +713,10 @@ uint64_t b2fmm_kernel_launches(void) { return g_launches.load(); }
 void b2fmm_set_stats(int on) { set_stats(on != 0); }
 
 void b2fmm_set_device_ranges(int on) { set_device_ranges(on != 0); }
+
+void b2fmm_test_fail_alloc(int after) { b2::g_fail_after.store(after < 0 ? -1 : after); }
+
+void b2fmm_test_barrier_limit(long long cycles) { set_tree_barrier_limit(cycles); }
 
 void b2fmm_async_status(void* stream, int* ier) {
   guarded(ier, [&] { return lap_async_status((cudaStream_t)stream); });

@@ -52,6 +52,10 @@ extern std::atomic<unsigned long long> g_launches;
     B2_CHECK(cudaGetLastError());                                 \
   } while (0)
 
+// Test hook: true exactly once, on the allocation that b2fmm_test_fail_alloc
+// asked to fail (the library then reports IER_ALLOC as for a real failure).
+bool alloc_fault_due();
+
 // Stream-ordered device buffer (cudaMallocAsync from the device's default pool).
 template <typename T>
 struct DBuf {
@@ -81,12 +85,16 @@ struct DBuf {
     release();
     s = st;
     n = count;
-    if (count) B2_CHECK(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+    if (count) {
+      if (alloc_fault_due()) throw CudaError("injected allocation failure (test hook)", IER_ALLOC);
+      B2_CHECK(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+    }
   }
   // grow to at least `count` elements keeping the first `keep` elements
   void grow(size_t count, size_t keep) {
     if (count <= n) return;
     T* q = nullptr;
+    if (alloc_fault_due()) throw CudaError("injected allocation failure (test hook)", IER_ALLOC);
     B2_CHECK(cudaMallocAsync((void**)&q, count * sizeof(T), s));
     if (p && keep) B2_CHECK(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
     if (p) cudaFreeAsync(p, s);

@@ -1371,6 +1371,7 @@ int finish(LapPlan& p, cudaStream_t st) {
   if (dev) {
     const int status = h[7];
     if (status == TB_OVERFLOW || status == TB_DEEP) return IER_RETRY;
+    if (status == TB_BADPTS) return IER_BADARG;
     if (status != TB_OK) return IER_TIMEOUT;
     note_tree_shape(p.ns + p.nt, p.ndiv, h[4], h[5]);
   }
@@ -1723,7 +1724,9 @@ int* async_word() {
 
 __global__ void k_fold_status(const TreeCtl* c, const int* err, int* word) {
   int code = 0;
-  if (c && c->status != TB_OK) code = c->status == TB_TIMEOUT ? IER_TIMEOUT : IER_TREE_LIMIT;
+  if (c && c->status != TB_OK)
+    code = c->status == TB_TIMEOUT ? IER_TIMEOUT
+                                   : (c->status == TB_BADPTS ? IER_BADARG : IER_TREE_LIMIT);
   if (!code && *err) code = IER_TIMEOUT;
   if (code) atomicCAS(word, 0, code);
 }

@@ -32,6 +32,8 @@ namespace {
 thread_local void* g_pinned = nullptr;
 thread_local size_t g_pinned_bytes = 0;
 
+std::atomic<long long> g_tree_bar_cycles{0};
+
 void* pinned_bytes(size_t b) {
   if (b > g_pinned_bytes) {
     if (g_pinned) cudaFreeHost(g_pinned);
@@ -83,13 +85,16 @@ __global__ void k_bbox(const double* __restrict__ src, long ns, const double* __
                        long nt, double4* part) {
   double4 v = make_double4(DBL_MAX, -DBL_MAX, DBL_MAX, -DBL_MAX);
   long stride = (long)gridDim.x * blockDim.x;
+  // a coordinate that is not finite widens the box to infinity, which
+  // k_init_root reports as TB_BADPTS
+  const double4 bad = make_double4(-INFINITY, INFINITY, -INFINITY, INFINITY);
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < ns; i += stride) {
     double x = src[2 * i], y = src[2 * i + 1];
-    minmax4(v, make_double4(x, x, y, y));
+    minmax4(v, isfinite(x) && isfinite(y) ? make_double4(x, x, y, y) : bad);
   }
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nt; i += stride) {
     double x = trg[2 * i], y = trg[2 * i + 1];
-    minmax4(v, make_double4(x, x, y, y));
+    minmax4(v, isfinite(x) && isfinite(y) ? make_double4(x, x, y, y) : bad);
   }
   v = block_minmax(v);
   if (threadIdx.x == 0) part[blockIdx.x] = v;
@@ -239,7 +244,8 @@ __device__ __forceinline__ void create_children(BoxPtrs& B, int b, int base, dou
   B.child[b] = make_int4(base, base + 1, base + 2, base + 3);
 }
 
-__global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt, TreeCtl* C, int cap) {
+__global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt, TreeCtl* C, int cap,
+                            long long bar_cycles) {
   B.center[0] = make_double2(root[0], root[1]);
   B.level[0] = 0;
   B.parent[0] = -1;
@@ -255,7 +261,8 @@ __global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt, TreeC
   C->nboxes = 1;
   C->nlevels = 0;
   C->cap = cap;
-  C->status = TB_OK;
+  C->status = isfinite(root[2]) ? TB_OK : TB_BADPTS;
+  C->bar_cycles = bar_cycles;
   C->lfirst[0] = 0;
   C->llast[0] = 0;
   C->bs[0] = root[2];
@@ -788,6 +795,7 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
   const int cap = C->cap;
   BoxPtrs cur = B, alt = S;
   int buf = 0;  // tot[] buffer of the next scan
+  if (C->status != TB_OK) return;  // non-finite coordinates (every block sees it)
   // A zero-size root (all points coincide) cannot be subdivided: the
   // children would coincide with it forever.  Keep the root as the only box.
   if (C->bs[0] == 0.0) nlmax = 0;
@@ -1205,7 +1213,8 @@ void launch_tree_attempt(DeviceTree& T, long ns, long nt, int idivflag, int ndiv
   BoxPtrs B = ptrs(T);
   B.pkey = pk1.p;
   BoxPtrs S{sc.p, sl.p, sp.p, sn.p, sch.p, sf.p, pk2.p, nullptr, nullptr, nullptr, nullptr};
-  k_init_root<<<1, 1, 0, st>>>(B, T.root.p, (int)ns, (int)nt, T.ctl.p, cap);
+  k_init_root<<<1, 1, 0, st>>>(B, T.root.p, (int)ns, (int)nt, T.ctl.p, cap,
+                               g_tree_bar_cycles.load());
   B2_LAUNCH_CHECK();
   TreeKeys K{T.skhi.p, T.sklo.p, T.tkhi.p, T.tklo.p};
   TreeCtl* C = T.ctl.p;
@@ -1294,6 +1303,8 @@ bool tree_shape(long npts, int ndiv, int* nboxes, int* nlevels) {
   return false;
 }
 
+void set_tree_barrier_limit(long long cycles) { g_tree_bar_cycles.store(cycles); }
+
 int tree_capacity_guess(long npts, int ndiv, double margin) {
   int nb = 0, nl = 0;
   double c;
@@ -1350,6 +1361,8 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
       cap = (int)std::min<long>(2L * cap, 1L << 30);
       continue;
     }
+    if (hc->status == TB_BADPTS)
+      throw CudaError("a source or target coordinate is not finite", IER_BADARG);
     if (hc->status != TB_OK) throw CudaError("tree build: grid barrier timed out", IER_TIMEOUT);
     break;
   }

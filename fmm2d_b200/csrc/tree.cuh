@@ -12,7 +12,8 @@ constexpr int NLMAX = 51;                                               // cfmm2
 constexpr int TB_MAXG = 1024;    // most blocks of the persistent build kernel
 constexpr int TB_THREADS = 512;  // threads per block (one block per SM)
 constexpr int TB_GROUPS = 8;     // first-level arrival counters of a grid barrier
-enum : int { TB_OK = 0, TB_OVERFLOW = 1, TB_DEEP = 2, TB_TIMEOUT = 3 };
+// TB_BADPTS: a source or target coordinate is not finite
+enum : int { TB_OK = 0, TB_OVERFLOW = 1, TB_DEEP = 2, TB_TIMEOUT = 3, TB_BADPTS = 4 };
 
 // Device control block of the tree build: box count, level table (box range
 // of every level), box sizes and status, followed by the grid barrier and
@@ -27,6 +28,7 @@ struct TreeCtl {
   double bs[NLMAX + 3];
   unsigned bar_sub[TB_GROUPS * 32];  // one 128-byte line per group
   unsigned bar_top, bar_gen;
+  long long bar_cycles;  // wait limit of the grid barrier (<= 0: GRID_BAR_CYCLES)
   int tot[2][TB_MAXG];  // per-block counts of the scans, alternating
 };
 
@@ -34,6 +36,7 @@ struct TreeCtl {
 struct GridBar {
   unsigned bar_sub[TB_GROUPS * 32];
   unsigned bar_top, bar_gen;
+  long long bar_cycles;  // wait limit (<= 0: GRID_BAR_CYCLES)
   int status;  // 0, or the timeout code once a barrier gave up
 };
 
@@ -74,9 +77,10 @@ __device__ bool grid_barrier(Ctl* C, int timeout_code) {
       }
     }
     if (ld_acquire_u32(&C->bar_gen) == g0) {
+      const long long lim = C->bar_cycles > 0 ? C->bar_cycles : GRID_BAR_CYCLES;
       const long long t0 = clock64();
       while (ld_acquire_u32(&C->bar_gen) == g0) {
-        if (clock64() - t0 > GRID_BAR_CYCLES ||
+        if (clock64() - t0 > lim ||
             *reinterpret_cast<const volatile int*>(&C->status) == timeout_code) {
           atomicExch(&C->status, timeout_code);
           break;
@@ -141,6 +145,10 @@ void build_device_tree_async(DeviceTree& T, const double* src, long ns, const do
 // the remembered count for a size seen before, else a generous multiple of
 // points / ndiv (raised by the largest ratio seen).
 void note_tree_shape(long npts, int ndiv, int nboxes, int nlevels);
+
+// Test hook: wait limit (clock cycles) of the tree build's grid barrier for
+// later builds; <= 0 restores the default of about half a second.
+void set_tree_barrier_limit(long long cycles);
 bool tree_shape(long npts, int ndiv, int* nboxes, int* nlevels);
 int tree_capacity_guess(long npts, int ndiv, double margin);
 

@@ -330,6 +330,17 @@ void b2fmm_get_stats(double* out, int n);
  * reference, whose calls are all blocking. */
 void b2fmm_async_status(void* stream, int* ier);
 
+/* Test hooks for the error paths (no counterpart in the reference; they
+ * inject failures on the host side only).  b2fmm_test_fail_alloc(k): the
+ * (k+1)-th device allocation of the library from now on fails as if the
+ * device were out of memory, so the call in progress returns ier = 4; k < 0
+ * switches the injection off.  b2fmm_test_barrier_limit(c): later tree
+ * builds give up a grid-barrier wait after c clock cycles instead of about
+ * half a second, and their calls return ier = 102 (c <= 0 restores the
+ * default); the device stays usable. */
+void b2fmm_test_fail_alloc(int after);
+void b2fmm_test_barrier_limit(long long cycles);
+
 /* Laplace / Cauchy calls take their box ranges from the tree's device
  * level table, so the host does not wait for the tree in the middle of a
  * call (1, the default); 0 reads every tree back first and launches the
