@@ -2,8 +2,11 @@
 
 Every ``csrc/*.cu`` is compiled for sm_100a with nvcc (objects under
 ``fmm2d_b200/_build/``) and linked into one shared library exporting the C ABI
-of ``include/fmm2d_b200.h``.  Run ``python -m fmm2d_b200.build`` or call
-``build()``; ``verbose_ptxas=True`` adds ``-Xptxas -v`` (registers, spills).
+of ``include/fmm2d_b200.h``.  ``csrc/fortran_abi.c`` becomes
+``fmm2d_b200/libfmm2d.so``: the reference library's own Fortran and C entry
+points (``include/fmm2d_f77.h``), linked against the first.  Run
+``python -m fmm2d_b200.build`` or call ``build()``; ``verbose_ptxas=True``
+adds ``-Xptxas -v`` (registers, spills).
 """
 import concurrent.futures as cf
 import os
@@ -14,6 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libfmm2d_b200.so")
+F77_SRC = os.path.join(CSRC, "fortran_abi.c")
+F77_LIB = os.path.join(HERE, "libfmm2d.so")
+INCLUDE = os.path.join(HERE, "..", "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xcompiler", "-Wno-unused-function", "-diag-suppress", "177,550"]
@@ -77,7 +83,23 @@ def build(force=False, verbose_ptxas=False, jobs=None):
         if p.returncode != 0:
             sys.stderr.write(p.stdout + p.stderr)
             raise RuntimeError("link failed")
+    _build_f77(force)
     return LIB
+
+
+def _build_f77(force):
+    """libfmm2d.so from csrc/fortran_abi.c (gcc), resolving the B200 library
+    beside it at run time."""
+    deps = [LIB, os.path.join(INCLUDE, "fmm2d_f77.h"), os.path.join(INCLUDE, "fmm2d_b200.h")]
+    if not force and not _stale(F77_LIB, F77_SRC, deps):
+        return
+    cmd = [os.environ.get("CC", "gcc"), "-std=c11", "-O2", "-fPIC", "-shared", "-Wall",
+           "-Werror", "-I", INCLUDE, F77_SRC, "-o", F77_LIB, "-L", HERE, "-l:libfmm2d_b200.so",
+           "-Wl,-rpath,$ORIGIN", "-Wl,--no-undefined"]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    if p.returncode != 0:
+        sys.stderr.write(p.stdout + p.stderr)
+        raise RuntimeError("libfmm2d.so failed to build")
 
 
 if __name__ == "__main__":

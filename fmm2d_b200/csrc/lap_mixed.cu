@@ -596,7 +596,7 @@ bool m2l_tensor_cores() { return g_m2l_tc.load(); }
 void lap_mixed_m2l(int ND, const TV& t, int first, int n, int P, const double* binom,
                    const MixedData& M, const double2* mp, double2* lo, cudaStream_t st) {
   if (M.tc && M.pairs.usable && M.pairs.P == P && M.err) {
-    int r = m2l_tc_run(ND, M.pairs, mp, M.mp32.p, (long)M.mp32.n, M.nboxes, lo, t.boxsize,
+    int r = m2l_tc_run(ND, M.pairs, mp, M.mp32.p, (long)M.mp32.n, M.nboxes, t.ctl, lo, t.boxsize,
                        M.nlev, M.err, st);
     if (r != IER_OK) throw CudaError("tensor-core M2L: invalid arguments", r);
     return;

@@ -690,21 +690,34 @@ __global__ void k_m2l_tab(int KH, int N, int P, const double* __restrict__ binom
   if (k == 0) lg[oi] = (float)l;
 }
 
-// FP32 copy of one density chunk's multipoles, [box][ND][KH] (zero beyond P).
-__global__ void k_mp_to_f32(const double2* __restrict__ mp, long nbox, int P, int ND, int KH,
-                            float2* __restrict__ out) {
-  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (e >= nbox * ND * KH) return;
-  const int k = (int)(e % KH);
-  const long bd = e / KH;
-  const int d = (int)(bd % ND);
-  const long box = bd / ND;
-  float2 v = make_float2(0.f, 0.f);
-  if (k < P) {
-    const double2 x = mp[((size_t)box * P + k) * ND + d];
-    v = make_float2((float)x.x, (float)x.y);
+// FP32 copy of one density chunk's multipoles, [box][ND][KH] (zero beyond P),
+// two coefficients per thread; only the boxes the tree holds (its count read
+// from the control block when there is one), grid-stride.
+__global__ void k_mp_to_f32(const double2* __restrict__ mp, long nbox, const TreeCtl* ctl, int P,
+                            int ND, int KH, float4* __restrict__ out) {
+  const long nb = ctl ? min((long)ctl->nboxes, nbox) : nbox;
+  const int KH2 = KH >> 1;
+  const long total = nb * ND * KH2;
+  for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total;
+       e += (long)gridDim.x * blockDim.x) {
+    const int k = (int)(e % KH2) * 2;
+    const long bd = e / KH2;
+    const int d = (int)(bd % ND);
+    const long box = bd / ND;
+    const double2* src = mp + ((size_t)box * P + k) * ND + d;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (k < P) {
+      const double2 x = src[0];
+      v.x = (float)x.x;
+      v.y = (float)x.y;
+    }
+    if (k + 1 < P) {
+      const double2 x = src[ND];
+      v.z = (float)x.x;
+      v.w = (float)x.y;
+    }
+    out[e] = v;
   }
-  out[e] = v;
 }
 
 __global__ void __launch_bounds__(128, 1)
@@ -971,7 +984,7 @@ long m2l_tc_scratch(const M2LPairs& L, int nboxes, int ND) {
 }
 
 int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long nmp32, int nboxes,
-               double2* lo, const double* boxsize, int nlev, int* err_dev, cudaStream_t st) {
+               const TreeCtl* ctl, double2* lo, const double* boxsize, int nlev, int* err_dev, cudaStream_t st) {
   if (L.n == 0) return IER_OK;
   const int P = L.P;
   if (nlev > 64 || !m2l_tc_supported(P) || !(ND == 1 || ND == 2 || ND == 4 || ND == 8))
@@ -982,8 +995,9 @@ int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long 
   int dev = 0, nsm = 148;
   B2_CHECK(cudaGetDevice(&dev));
   B2_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const long nconv = (long)nboxes * ND * KH;
-  k_mp_to_f32<<<ceil_div(nconv, 256), 256, 0, st>>>(mp, nboxes, P, ND, KH, mp32);
+  const long nconv = (long)nboxes * ND * (KH / 2);
+  k_mp_to_f32<<<(int)std::min<long>(ceil_div(nconv, 256), (long)nsm * 8), 256, 0, st>>>(
+      mp, nboxes, ctl, P, ND, KH, reinterpret_cast<float4*>(mp32));
   B2_LAUNCH_CHECK();
   auto launch = [&](auto kern, uint32_t total, uint32_t tmem_cols, int threads) {
     // CTAs that can share an SM (tensor-memory columns and shared memory);

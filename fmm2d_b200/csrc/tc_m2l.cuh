@@ -40,7 +40,7 @@ long m2l_tc_scratch(const M2LPairs& L, int nboxes, int ND);
 // cores that gives up sets *err_dev to 1 (the caller reports IER_TIMEOUT
 // after synchronising).
 int m2l_tc_run(int ND, const M2LPairs& L, const double2* mp, float2* mp32, long nmp32, int nboxes,
-               double2* lo, const double* boxsize, int nlev, int* err_dev, cudaStream_t st);
+               const TreeCtl* ctl, double2* lo, const double* boxsize, int nlev, int* err_dev, cudaStream_t st);
 
 // Probe of the tensor-core tile path: D = A B^T for a 128 x K (A) and an
 // N x K (B) FP32 matrix (row-major, device pointers), K in {8,16,24,32},
