@@ -517,6 +517,46 @@ void b2fmm_hfmm2d_dev(int nd, double eps, double zk_re, double zk_im, int64_t ns
   });
 }
 
+void b2fmm_hfmm2d_mps(int nd, double eps, double zk_re, double zk_im, int64_t nmpole,
+                      const double* cmpole, const double* rmpole, const int* mterms,
+                      int64_t ntot, const double* mpole, const int* impole, double* local,
+                      int* ier) {
+  guarded(ier, [&] {
+    if (nd < 1 || nmpole < 0 || ntot < 0) return (int)IER_BADARG;
+    if (nmpole == 0) return (int)IER_OK;
+    if (!cmpole || !rmpole || !mterms || !mpole || !impole || !local) return (int)IER_BADARG;
+    // every (nd, -m..m) block inside the coefficient arrays
+    int mmax = 0;
+    for (int64_t i = 0; i < nmpole; i++) {
+      const int64_t m = mterms[i], o = (int64_t)impole[i] - 1;
+      if (m < 0 || o < 0 || o + (int64_t)nd * (2 * m + 1) > ntot) return (int)IER_BADARG;
+      mmax = std::max(mmax, (int)m);
+    }
+    cudaStream_t st = cudaStreamPerThread;
+    DBuf<double> c(st), r(st), mp(st), lo(st);
+    DBuf<int> mt(st), im(st);
+    c.alloc(2 * (size_t)nmpole, st);
+    r.alloc(nmpole, st);
+    mt.alloc(nmpole, st);
+    im.alloc(nmpole, st);
+    mp.alloc(2 * (size_t)ntot, st);
+    lo.alloc(2 * (size_t)ntot, st);
+    B2_CHECK(cudaMemcpyAsync(c.p, cmpole, sizeof(double) * 2 * nmpole, cudaMemcpyHostToDevice, st));
+    B2_CHECK(cudaMemcpyAsync(r.p, rmpole, sizeof(double) * nmpole, cudaMemcpyHostToDevice, st));
+    B2_CHECK(cudaMemcpyAsync(mt.p, mterms, sizeof(int) * nmpole, cudaMemcpyHostToDevice, st));
+    B2_CHECK(cudaMemcpyAsync(im.p, impole, sizeof(int) * nmpole, cudaMemcpyHostToDevice, st));
+    B2_CHECK(cudaMemcpyAsync(mp.p, mpole, sizeof(double) * 2 * ntot, cudaMemcpyHostToDevice, st));
+    // entries outside every block keep the caller's values, as in the reference
+    B2_CHECK(cudaMemcpyAsync(lo.p, local, sizeof(double) * 2 * ntot, cudaMemcpyHostToDevice, st));
+    int rc = helm_mps_device(nd, eps, zk_re, zk_im, nmpole, c.p, r.p, mt.p, im.p, ntot, mp.p,
+                             lo.p, mmax, st);
+    if (rc != IER_OK) return rc;
+    B2_CHECK(cudaMemcpyAsync(local, lo.p, sizeof(double) * 2 * ntot, cudaMemcpyDeviceToHost, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+    return (int)IER_OK;
+  });
+}
+
 void b2fmm_h2ddir_dev(int nd, double zk_re, double zk_im, int64_t ns, const double* sources,
                       const double* charge, const double* dipstr, const double* dipvec,
                       int64_t nt, const double* targ, int ifpgh, double* pot, double* grad,

@@ -143,6 +143,13 @@ void hfmm2d_ndiv_(const int* nd, const double* eps, const double* zk, const int*
                     hesstarg, *ndiv, *idivflag, *ifnear, timeinfo, ier);
 }
 
+void hfmm2d_mps_(const int* nd, const double* eps, const double* zk, const int* nmpole,
+                 const double* cmpole, const double* rmpole, const int* mterms, const int* ntot,
+                 const double* mpole, const int* impole, double* local, int* ier) {
+  b2fmm_hfmm2d_mps(*nd, *eps, zk[0], zk[1], *nmpole, cmpole, rmpole, mterms, *ntot, mpole,
+                   impole, local, ier);
+}
+
 /* ------------------------------------------------------------ flag wrappers */
 
 #define ZK_c NULL

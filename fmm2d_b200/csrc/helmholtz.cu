@@ -999,6 +999,73 @@ int grid_w(long nitems, int wpb) {
   return (int)std::max(1L, std::min(blocks, 148L * 32));
 }
 
+// Per-level expansion orders and scales, the expansion layout and the
+// translation tables of one tree (hfmm2d.f:317-326 for orders and scales).
+struct HelmLevels {
+  std::vector<HLev> hl;
+  int maxp = 0;  // largest order at levels >= 2
+  long off = 0;  // expansion storage per density (double2 units)
+  DBuf<HLev> dlv;
+  DBuf<double2> tabs;
+  DBuf<double> dbs;  // box sizes, one level past the deepest
+  explicit HelmLevels(cudaStream_t st) : dlv(st), tabs(st), dbs(st) {}
+};
+
+// ier 13: an order above HMAXP; 20: a level where translations run has
+// boxes larger than 16 wavelengths (hfmm2d.f:1001-1013, the wideband path).
+int helm_levels(const DeviceTree& T, double zkr, double zki, double eps, HelmLevels& H,
+                cudaStream_t st) {
+  const int nl = T.nlevels;
+  const double pi = 4 * std::atan(1.0);
+  const double zkabs = std::hypot(zkr, zki);
+  std::vector<HLev>& hl = H.hl;
+  hl.assign(nl + 1, HLev{});
+  int maxp = 0, ier = 0;
+  for (int l = 0; l <= nl; l++) {
+    double bs = T.boxsize[l];
+    hl[l].lfirst = T.lfirst[l];
+    hl[l].rs = std::min(zkabs * bs / (2.0 * pi), 1.0);
+    hl[l].bs = bs;
+    hl[l].p = helm_nterms(bs, zkr, zki, eps, &ier);
+    hl[l].P = 2 * hl[l].p + 1;
+    hl[l].ok = (zki * bs < 40.0) ? 1 : 0;
+    if (hl[l].ok && l >= 1 && bs / (1.0 / (zkr / (2.0 * pi))) > 16.0) return IER_HIGHFREQ;
+    if (l >= 2) maxp = std::max(maxp, hl[l].p);
+  }
+  if (ier) return ier;
+  if (maxp > HMAXP) return IER_NTERMS;
+  H.maxp = maxp;
+  // expansion and table layout
+  long off = 0, toff = 0;
+  for (int l = 0; l <= nl; l++) {
+    hl[l].off = off;
+    off += (long)(T.llast[l] - T.lfirst[l] + 1) * hl[l].P;
+    hl[l].nsh = l < nl ? hl[l].p + hl[l + 1].p : 0;
+    hl[l].tm2l = toff;
+    if (l >= 2) toff += 49L * (4 * hl[l].p + 1);
+    hl[l].tm2m = toff;
+    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
+    hl[l].tl2l = toff;
+    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
+  }
+  H.off = off;
+  H.dlv.alloc(nl + 1, st);
+  B2_CHECK(cudaMemcpyAsync(H.dlv.p, hl.data(), sizeof(HLev) * (nl + 1), cudaMemcpyHostToDevice, st));
+  DBuf<double2> scratch(st);
+  H.tabs.alloc(std::max(toff, 1L), st);
+  const int nthreads = (nl + 1) * 57, sstride = 2 * (2 * HMAXP) + 8;
+  scratch.alloc((size_t)nthreads * sstride, st);
+  k_h_tables<<<ceil_div(nthreads, 64), 64, 0, st>>>(H.dlv.p, nl, zkr, zki, H.tabs.p, scratch.p,
+                                                    sstride);
+  B2_LAUNCH_CHECK();
+  std::vector<double> bsx(T.boxsize);
+  bsx.push_back(T.boxsize.back() / 2);
+  H.dbs.alloc(bsx.size(), st);
+  B2_CHECK(cudaMemcpyAsync(H.dbs.p, bsx.data(), sizeof(double) * bsx.size(), cudaMemcpyHostToDevice,
+                           st));
+  return IER_OK;
+}
+
 template <int ND>
 void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
                 const HLev* dlv, const std::vector<HLev>& hl, int maxp, const double2* tabs,
@@ -1077,6 +1144,300 @@ void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
   B2_CHECK(cudaEventRecord(ev[6], st));
 }
 
+
+// ---------------------------------------------------------------------------
+// FMM over multipole sources (hfmm2d_mps, src/helmholtz/hfmm2d_mps.f:19-1025).
+// The tree is built on the expansion centres (ndiv 1).  Box-to-box steps are
+// the kernels above; the steps that start or end at an expansion of its own
+// centre, scale and order translate one expansion at a time:
+//   step 1  expansion -> leaf multipole (h2dmpmp)       k_mps_boxes
+//   step 2  list-4 expansions -> box local (h2dmploc)   k_mps_boxes
+//   step 6  list-3 multipoles -> expansion (h2dmploc)   k_mps_locals
+//   step 7  leaf local -> expansion (h2dlocloc)         k_mps_locals
+//   step 8  list-1 expansions -> expansion (h2dmploc)   k_mps_locals
+// ---------------------------------------------------------------------------
+enum { X_MPMP = 0, X_MPLOC = 1, X_LOCLOC = 2 };
+
+// Expansions in tree order: centre, scale, order, offset of (nd, -m..m) in
+// the caller's coefficient arrays.
+struct MpsExp {
+  const double2* c;
+  const double* rs;
+  const int* m;
+  const long* off;
+};
+
+// Warp-private shared scratch of the translations: Z[nt + 4], T[2 nt + 1],
+// R[max order + 1].
+struct XScr {
+  double2* Z;
+  double2* T;
+  double* R;
+};
+
+// dst(i) += sum_j src(j) T(i-j) f(i,j), i = -n2..n2, j = -n1..n1, with the
+// (value, phase) table T of the centre shift c2 - c1 (J_n(zk r)/rs1^n for the
+// shifts, H_n(zk r) rs1^n for multipole to local; theta - pi as in
+// h2dmpmp / h2dmploc / h2dlocloc, helmrouts2d.f:967-1378) and the rscale
+// factors of each operator:
+//   mpmp:   (rs1/rs2)^|i| rs1^(2e), e = max(0,|j|-|i|) for j of the sign of i, else |j|
+//   mploc:  (rs2/rs1)^|i| rs1^(2 min(|i|,|j|)) for j of the sign of i, else (rs2/rs1)^|i|
+//   locloc: 1 for i = 0; (rs1 rs2)^|i| for j = 0 or of the other sign;
+//           (rs2/rs1)^|i| rs1^(2 max(0,|i|-|j|)) for j of the sign of i.
+// src and dst hold ND densities per coefficient at strides ss and ds.
+template <int ND>
+__device__ void warp_xlate(int kind, double2 zk, double rs1, double2 c1, const double2* src, int ss,
+                           int n1, double rs2, double2 c2, double2* dst, int ds, int n2,
+                           const XScr& S, int lane) {
+  const int nt = n1 + n2;
+  const double pi = 3.14159265358979323846;
+  const double x = c2.x - c1.x, y = c2.y - c1.y;
+  const double th = atan2(y, x) - pi;
+  if (lane == 0) {
+    const double r = sqrt(x * x + y * y);
+    const double2 z = make_double2(zk.x * r, zk.y * r);
+    if (kind == X_MPLOC)
+      hscaled(nt + 1, z, rs1, S.Z);
+    else
+      jscaled(nt + 3, z, rs1, S.Z);
+  }
+  const int mx = n1 > n2 ? n1 : n2;
+  for (int k = lane; k <= mx; k += 32) S.R[k] = pow(rs1, 2.0 * k);
+  __syncwarp();
+  for (int j = lane; j <= nt; j += 32) {
+    double sn, cs;
+    sincos(j * th, &sn, &cs);
+    const double2 e = make_double2(cs, -sn);  // exp(-i theta)^j
+    const double2 zj = S.Z[j];
+    S.T[nt + j] = cmul(e, zj);
+    if (j > 0) {
+      double2 t = cmul(make_double2(cs, sn), zj);  // conj(e)^j Z_j
+      if (j & 1) t = make_double2(-t.x, -t.y);
+      S.T[nt - j] = t;
+    }
+  }
+  __syncwarp();
+  const double2* T = S.T + nt;
+  for (int i = lane - n2; i <= n2; i += 32) {
+    const int ai = i < 0 ? -i : i;
+    double2 a0[ND], a1[ND];  // a0: unit factor, a1: the second factor class
+#pragma unroll
+    for (int d = 0; d < ND; d++) a0[d] = a1[d] = make_double2(0, 0);
+    for (int j = -n1; j <= n1; j++) {
+      const int aj = j < 0 ? -j : j;
+      const bool same = i != 0 && j != 0 && ((i > 0) == (j > 0));
+      double f = 1.0;
+      bool second = false;
+      if (kind == X_MPMP) {
+        f = S.R[same ? (aj > ai ? aj - ai : 0) : aj];
+      } else if (kind == X_MPLOC) {
+        if (same) f = S.R[ai < aj ? ai : aj];
+      } else if (i != 0) {
+        if (same)
+          f = S.R[ai > aj ? ai - aj : 0];
+        else
+          second = true;
+      }
+      const double2 t = cscale(T[i - j], f);
+      const double2* sj = src + (size_t)(j + n1) * ss;
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        if (second)
+          cfma(a1[d], sj[d], t);
+        else
+          cfma(a0[d], sj[d], t);
+      }
+    }
+    double g0 = 1.0, g1 = 0.0;
+    if (kind == X_MPMP) {
+      g0 = pow(rs1 / rs2, (double)ai);
+    } else if (kind == X_MPLOC) {
+      g0 = pow(rs2 / rs1, (double)ai);
+    } else if (i != 0) {
+      g0 = pow(rs2 / rs1, (double)ai);
+      g1 = pow(rs1 * rs2, (double)ai);
+    }
+    double2* di = dst + (size_t)(i + n2) * ds;
+#pragma unroll
+    for (int d = 0; d < ND; d++)
+      di[d] = cadd(di[d], cadd(cscale(a0[d], g0), cscale(a1[d], g1)));
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ XScr warp_scratch(char* base, int maxnt, int wib) {
+  const size_t zn = (size_t)maxnt + 4, tn = 2 * (size_t)maxnt + 1, rn = (size_t)maxnt + 2;
+  const size_t per = (zn + tn) * sizeof(double2) + rn * sizeof(double);
+  char* w = base + per * wib;
+  XScr S;
+  S.Z = reinterpret_cast<double2*>(w);
+  S.T = S.Z + zn;
+  S.R = reinterpret_cast<double*>(S.T + tn);
+  return S;
+}
+
+// Steps 1 and 2, one warp per box of levels >= 2 (boxes first .. first+n-1).
+template <int ND>
+__global__ void __launch_bounds__(128) k_mps_boxes(TV t, const HLev* __restrict__ lv, int first,
+                                                   int n, MpsExp E, const double2* __restrict__ mpole,
+                                                   int nd, int d0, double2 zk, double2* mp,
+                                                   double2* lo, int maxnt) {
+  extern __shared__ __align__(16) char xsm[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const XScr S = warp_scratch(xsm, maxnt, wib);
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int w = blockIdx.x * (blockDim.x >> 5) + wib; w < n; w += nw) {
+    const int b = first + w;
+    const HLev L = lv[t.level[b]];
+    if (!L.ok) continue;
+    const double2 cb = t.center[b];
+    if (t.nchild[b] == 0) {
+      const int2 r = t.srng[b];
+      double2* M = hexp(mp, L, b, ND);
+      for (int k = r.x; k < r.y; k++)
+        warp_xlate<ND>(X_MPMP, zk, E.rs[k], E.c[k], mpole + E.off[k] + d0, nd, E.m[k], L.rs, cb,
+                       M, ND, L.p, S, lane);
+    }
+    double2* Lo = hexp(lo, L, b, ND);
+    const int n4 = t.nl4[b];
+    for (int e = 0; e < n4; e++) {
+      const int jb = t.l4[(size_t)MNLIST4 * b + e];
+      const int2 r = t.srng[jb];
+      for (int k = r.x; k < r.y; k++)
+        warp_xlate<ND>(X_MPLOC, zk, E.rs[k], E.c[k], mpole + E.off[k] + d0, nd, E.m[k], L.rs, cb,
+                       Lo, ND, L.p, S, lane);
+    }
+  }
+}
+
+// Steps 6-8, one warp per expansion (tree order), accumulating into the
+// caller's local array (zeroed here first, as hfmm2dmain_mps zeroes it).
+template <int ND>
+__global__ void __launch_bounds__(128) k_mps_locals(TV t, const HLev* __restrict__ lv, int nlev,
+                                                    const int* __restrict__ leaf, long nexp,
+                                                    MpsExp E, const double2* __restrict__ mpole,
+                                                    int nd, int d0, double2 zk,
+                                                    const double2* __restrict__ mp,
+                                                    const double2* __restrict__ lo,
+                                                    double2* __restrict__ local, double thresh,
+                                                    int maxnt) {
+  extern __shared__ __align__(16) char xsm[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const XScr S = warp_scratch(xsm, maxnt, wib);
+  const long nw = (long)gridDim.x * (blockDim.x >> 5);
+  for (long j = blockIdx.x * (long)(blockDim.x >> 5) + wib; j < nexp; j += nw) {
+    const int m2 = E.m[j];
+    const double rs2 = E.rs[j];
+    const double2 c2 = E.c[j];
+    double2* dst = local + E.off[j] + d0;
+    for (int e = lane; e < 2 * m2 + 1; e += 32)
+#pragma unroll
+      for (int d = 0; d < ND; d++) dst[(size_t)e * nd + d] = make_double2(0, 0);
+    __syncwarp();
+    const int B = leaf[j];
+    const int lb = t.level[B];
+    // step 6: multipoles of list-3 boxes (one level down)
+    const int n3 = t.nl3[B];
+    for (int e = 0; e < n3; e++) {
+      const int jb = t.l3[(size_t)MNLIST3 * B + e];
+      const HLev LJ = lv[t.level[jb]];
+      if (!LJ.ok) continue;
+      warp_xlate<ND>(X_MPLOC, zk, LJ.rs, t.center[jb], hexp(const_cast<double2*>(mp), LJ, jb, ND),
+                     ND, LJ.p, rs2, c2, dst, nd, m2, S, lane);
+    }
+    // step 7: the leaf's local expansion (zero above level 2, where no
+    // translation reaches)
+    const HLev L = lv[lb];
+    if (L.ok && lb >= 2)
+      warp_xlate<ND>(X_LOCLOC, zk, L.rs, t.center[B], hexp(const_cast<double2*>(lo), L, B, ND), ND,
+                     L.p, rs2, c2, dst, nd, m2, S, lane);
+    // step 8: expansions of list-1 boxes, except coincident centres
+    const int n1 = t.nl1[B];
+    for (int e = 0; e < n1; e++) {
+      const int jb = t.l1[(size_t)MNLIST1 * B + e];
+      const int2 r = t.srng[jb];
+      for (int k = r.x; k < r.y; k++) {
+        const double2 ck = E.c[k];
+        const double dx = ck.x - c2.x, dy = ck.y - c2.y;
+        if (!(sqrt(dx * dx + dy * dy) > thresh)) continue;
+        warp_xlate<ND>(X_MPLOC, zk, E.rs[k], ck, mpole + E.off[k] + d0, nd, E.m[k], rs2, c2, dst,
+                       nd, m2, S, lane);
+      }
+    }
+  }
+  (void)nlev;
+}
+
+// Expansion data in tree order; off = (impole - 1) / 1 in double2 units.
+__global__ void k_mps_gather(const double* __restrict__ cen, const double* __restrict__ rsc,
+                             const int* __restrict__ mt, const int* __restrict__ impole,
+                             const int* __restrict__ perm, long n, double2* c, double* rs, int* m,
+                             long* off) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const long i = perm[k];
+  c[k] = make_double2(cen[2 * i], cen[2 * i + 1]);
+  rs[k] = rsc[i];
+  m[k] = mt[i];
+  off[k] = (long)impole[i] - 1;
+}
+
+size_t mps_smem(int maxnt, int warps) {
+  const size_t zn = (size_t)maxnt + 4, tn = 2 * (size_t)maxnt + 1, rn = (size_t)maxnt + 2;
+  return ((zn + tn) * sizeof(double2) + rn * sizeof(double)) * warps;
+}
+
+template <int ND>
+void mps_chunk(const TV& tv, const DeviceTree& T, const HelmLevels& H, const MpsExp& E,
+               const double2* mpole, int nd, int d0, double2 zk, double2* mp, double2* lo,
+               const int* leaf, long nc, double2* local, double thresh, int maxnt,
+               cudaStream_t st) {
+  const int nb = T.nboxes, nl = T.nlevels;
+  const std::vector<HLev>& hl = H.hl;
+  const size_t xs = mps_smem(maxnt, 4);
+  B2_CHECK(cudaMemsetAsync(mp, 0, sizeof(double2) * (size_t)H.off * ND, st));
+  B2_CHECK(cudaMemsetAsync(lo, 0, sizeof(double2) * (size_t)H.off * ND, st));
+  if (nl >= 2) {
+    const int f = T.lfirst[2], n = nb - f;
+    set_smem(k_mps_boxes<ND>, xs);
+    k_mps_boxes<ND><<<(int)std::min<long>(ceil_div(n, 4), 148L * 8), 128, xs, st>>>(
+        tv, H.dlv.p, f, n, E, mpole, nd, d0, zk, mp, lo, maxnt);
+    B2_LAUNCH_CHECK();
+  }
+  for (int l = nl - 1; l >= 2; l--) {
+    if (!hl[l].ok) continue;
+    int f = T.lfirst[l], n = T.llast[l] - f + 1;
+    size_t sm = sizeof(double2) * (2 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
+                sizeof(double) * (HMAXP + 1);
+    set_smem(k_h_m2m<ND>, sm);
+    k_h_m2m<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                   H.tabs.p, mp);
+    B2_LAUNCH_CHECK();
+  }
+  if (nl >= 2) {
+    int f = T.lfirst[2], n = nb - f;
+    size_t sm = sizeof(double2) * (2 * (2 * H.maxp + 1) * ND + 4 * H.maxp + 1) +
+                sizeof(double) * (H.maxp + 1);
+    set_smem(k_h_m2l<ND>, sm);
+    k_h_m2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, f, n, H.tabs.p,
+                                                                   mp, lo, H.maxp);
+    B2_LAUNCH_CHECK();
+  }
+  for (int l = 2; l <= nl - 1; l++) {
+    if (!hl[l].ok) continue;
+    int f = T.lfirst[l], n = T.llast[l] - f + 1;
+    size_t sm = sizeof(double2) * ((2 * hl[l].p + 1) * ND + 4 * (2 * hl[l].nsh + 1)) +
+                sizeof(double) * (HMAXP + 1);
+    set_smem(k_h_l2l<ND>, sm);
+    k_h_l2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                   H.tabs.p, lo);
+    B2_LAUNCH_CHECK();
+  }
+  set_smem(k_mps_locals<ND>, xs);
+  k_mps_locals<ND><<<(int)std::min<long>(ceil_div(nc, 4), 148L * 8), 128, xs, st>>>(
+      tv, H.dlv.p, nl, leaf, nc, E, mpole, nd, d0, zk, mp, lo, local, thresh, maxnt);
+  B2_LAUNCH_CHECK();
+}
 }  // namespace
 
 int helm_nterms(double bsize, double zkr, double zki, double eps, int* ier) {
@@ -1138,53 +1499,15 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
     zero_outputs();
     return IER_OK;
   }
-  const int nl = T.nlevels;
-  const double pi = 4 * std::atan(1.0);
   const double zkabs = std::hypot(a.zkr, a.zki);
-  // per-level order and scale (hfmm2d.f:317-326), high-frequency test
-  // (hfmm2d.f:1001-1013): box > 16 wavelengths needs the wideband path
-  std::vector<HLev> hl(nl + 1);
-  int maxp = 0, ier = 0;
-  for (int l = 0; l <= nl; l++) {
-    double bs = T.boxsize[l];
-    hl[l].lfirst = T.lfirst[l];
-    hl[l].rs = std::min(zkabs * bs / (2.0 * pi), 1.0);
-    hl[l].bs = bs;
-    hl[l].p = helm_nterms(bs, a.zkr, a.zki, a.eps, &ier);
-    hl[l].P = 2 * hl[l].p + 1;
-    hl[l].ok = (a.zki * bs < 40.0) ? 1 : 0;
-    if (hl[l].ok && l >= 1 && bs / (1.0 / (a.zkr / (2.0 * pi))) > 16.0) return IER_HIGHFREQ;
-    if (l >= 2) maxp = std::max(maxp, hl[l].p);
-  }
-  if (ier) return ier;
-  if (maxp > HMAXP) return IER_NTERMS;
-  // expansion and table layout
-  long off = 0, toff = 0;
-  for (int l = 0; l <= nl; l++) {
-    hl[l].off = off;
-    off += (long)(T.llast[l] - T.lfirst[l] + 1) * hl[l].P;
-    hl[l].nsh = l < nl ? hl[l].p + hl[l + 1].p : 0;
-    hl[l].tm2l = toff;
-    if (l >= 2) toff += 49L * (4 * hl[l].p + 1);
-    hl[l].tm2m = toff;
-    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
-    hl[l].tl2l = toff;
-    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
-  }
-  DBuf<HLev> dlv(st);
-  dlv.alloc(nl + 1, st);
-  B2_CHECK(cudaMemcpyAsync(dlv.p, hl.data(), sizeof(HLev) * (nl + 1), cudaMemcpyHostToDevice, st));
-  DBuf<double2> tabs(st), scratch(st);
-  tabs.alloc(std::max(toff, 1L), st);
-  const int nthreads = (nl + 1) * 57, sstride = 2 * (2 * HMAXP) + 8;
-  scratch.alloc((size_t)nthreads * sstride, st);
-  k_h_tables<<<ceil_div(nthreads, 64), 64, 0, st>>>(dlv.p, nl, a.zkr, a.zki, tabs.p, scratch.p, sstride);
-  B2_LAUNCH_CHECK();
-  std::vector<double> bsx(T.boxsize);
-  bsx.push_back(T.boxsize.back() / 2);
-  DBuf<double> dbs(st);
-  dbs.alloc(bsx.size(), st);
-  B2_CHECK(cudaMemcpyAsync(dbs.p, bsx.data(), sizeof(double) * bsx.size(), cudaMemcpyHostToDevice, st));
+  HelmLevels H(st);
+  if (int r = helm_levels(T, a.zkr, a.zki, a.eps, H, st)) return r;
+  const std::vector<HLev>& hl = H.hl;
+  const int maxp = H.maxp;
+  const long off = H.off;
+  DBuf<HLev>& dlv = H.dlv;
+  DBuf<double2>& tabs = H.tabs;
+  DBuf<double>& dbs = H.dbs;
   // sorted inputs
   DBuf<double2> xs(st), xt(st), qs(st), ds(st);
   DBuf<double> vs(st);
@@ -1269,6 +1592,65 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
   if (a.timeinfo)
     for (int i = 0; i < 8; i++) a.timeinfo[i] = tsum[i];
   for (int i = 0; i < 8; i++) cudaEventDestroy(ev[i]);
+  return IER_OK;
+}
+
+int helm_mps_device(int nd, double eps, double zkr, double zki, long nc, const double* centers,
+                    const double* rscales, const int* mterms, const int* impole, long ntot,
+                    const double* mpole, double* local, int max_mterms, cudaStream_t st) {
+  if (nd < 1 || nc < 0 || ntot < 0 || nc > (1L << 30) || max_mterms < 0) return IER_BADARG;
+  if (max_mterms > HMAXP) return IER_NTERMS;
+  if (nc == 0) return IER_OK;
+  if (!centers || !rscales || !mterms || !impole || !mpole || !local) return IER_BADARG;
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  configure_mempool(dev);
+  ensure_device_tables();
+  // tree on the centres, one per leaf (hfmm2d_mps.f:106-143: idivflag 0, ndiv 1)
+  DeviceTree T;
+  build_device_tree(T, centers, nc, nullptr, 0, 0, 1, NLMAX, st);
+  HelmLevels H(st);
+  if (int r = helm_levels(T, zkr, zki, eps, H, st)) return r;
+  const int maxnt = 2 * std::max(H.maxp, max_mterms);
+  DBuf<double2> ec(st);
+  DBuf<double> ers(st);
+  DBuf<int> em(st), leaf(st);
+  DBuf<long> eoff(st);
+  ec.alloc(nc, st);
+  ers.alloc(nc, st);
+  em.alloc(nc, st);
+  eoff.alloc(nc, st);
+  k_mps_gather<<<ceil_div(nc, 256), 256, 0, st>>>(centers, rscales, mterms, impole, T.isrc.p, nc,
+                                                  ec.p, ers.p, em.p, eoff.p);
+  B2_LAUNCH_CHECK();
+  TV tv{T.center.p, T.level.p, T.nchild.p, T.child.p, T.srng.p, T.trng.p, T.nlist1.p, T.list1.p,
+        T.nlist2.p, T.list2.p, T.nlist3.p, T.list3.p, T.nlist4.p, T.list4.p, H.dbs.p, 1, 0,
+        T.ctl.p};
+  leaf.alloc(nc, st);
+  k_h_point_leaf<<<ceil_div(T.nboxes, 128), 128, 0, st>>>(tv, T.nboxes, 0, leaf.p);
+  B2_LAUNCH_CHECK();
+  // interactions closer than this are skipped (hfmm2d_mps.f:960)
+  const double thresh = std::hypot(zkr, zki) * T.bs0 * std::ldexp(1.0, -51);
+  // the offsets count complex entries of (nd, -m..m) blocks
+  MpsExp E{ec.p, ers.p, em.p, eoff.p};
+  const double2 zk = make_double2(zkr, zki);
+  const int chunk = nd >= 4 ? 4 : (nd >= 2 ? 2 : 1);
+  DBuf<double2> mp(st), lo(st);
+  mp.alloc((size_t)H.off * chunk, st);
+  lo.alloc((size_t)H.off * chunk, st);
+  auto* mpc = reinterpret_cast<const double2*>(mpole);
+  auto* loc = reinterpret_cast<double2*>(local);
+  for (int d0 = 0; d0 < nd;) {
+    const int left = nd - d0;
+    const int ND = left >= 4 ? 4 : (left >= 2 ? 2 : 1);
+    switch (ND) {
+      case 4: mps_chunk<4>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, leaf.p, nc, loc, thresh, maxnt, st); break;
+      case 2: mps_chunk<2>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, leaf.p, nc, loc, thresh, maxnt, st); break;
+      default: mps_chunk<1>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, leaf.p, nc, loc, thresh, maxnt, st); break;
+    }
+    d0 += ND;
+  }
+  B2_CHECK(cudaStreamSynchronize(st));
   return IER_OK;
 }
 

@@ -34,6 +34,18 @@ int helm_direct_device(int nd, double zkr, double zki, long ns, const double* sr
                        const double* trg, int ifpgh, double* pot, double* grad, double* hess,
                        double thresh, cudaStream_t st);
 
+// FMM over multipole expansions (hfmm2d_mps, src/helmholtz/hfmm2d_mps.f:19-286):
+// the local expansion at each of nc centres due to all the other
+// expansions.  Device pointers: centers (2, nc), rscales (nc), mterms (nc),
+// impole (nc, 1-based offsets into the complex arrays as in the
+// reference), mpole and local complex (ntot); expansion i is the (nd,
+// -m..m) block at impole(i), m = mterms(i) <= max_mterms.  ier 13 when
+// max_mterms exceeds the supported order (63), 20 in the high-frequency
+// regime (as helm_fmm_device).
+int helm_mps_device(int nd, double eps, double zkr, double zki, long nc, const double* centers,
+                    const double* rscales, const int* mterms, const int* impole, long ntot,
+                    const double* mpole, double* local, int max_mterms, cudaStream_t st);
+
 // Expansion order of a box of size bsize (h2dterms, src/helmholtz/h2dterms.f:35-97).
 int helm_nterms(double bsize, double zkr, double zki, double eps, int* ier);
 

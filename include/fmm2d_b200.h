@@ -189,6 +189,18 @@ void b2fmm_hfmm2d_dev(int nd, double eps, double zk_re, double zk_im, int64_t ns
                       double* pottarg, double* gradtarg, double* hesstarg,
                       const b2fmm_options* opts, double* timeinfo, void* stream, int* ier);
 
+/* hfmm2d_mps: src/helmholtz/hfmm2d_mps.f:19-22.  Host arrays: cmpole (2,
+ * nmpole), rmpole (nmpole), mterms (nmpole), impole (nmpole, 1-based
+ * offsets into the complex arrays), mpole and local complex (ntot).
+ * Expansion i is the (nd, -m..m) block at impole(i) with m = mterms(i) <= 63.
+ * On return local holds, at each block, the local expansion about that
+ * centre due to all the other expansions.  ier 100 when a block lies
+ * outside ntot, 13 for an order above 63, 20 in the high-frequency regime. */
+void b2fmm_hfmm2d_mps(int nd, double eps, double zk_re, double zk_im, int64_t nmpole,
+                      const double* cmpole, const double* rmpole, const int* mterms,
+                      int64_t ntot, const double* mpole, const int* impole, double* local,
+                      int* ier);
+
 /* h2d_direct{c,d,cd}{p,g,h}: src/helmholtz/helmkernels2d.f:3-904.  Device
  * pointers; charge / dipstr NULL when absent; pairs with |zk r| < thresh
  * (<= for the charge potential-only kernel) are skipped.  Outputs are

@@ -11,6 +11,7 @@
  *   core      cfmm2d_, lfmm2d_, rfmm2d_, hfmm2d_       src/laplace/cfmm2d.f:23-26,
  *             lfmm2d.f:29-32, rfmm2d.f:27-30, src/helmholtz/hfmm2d.f:19-22
  *   tuning    cfmm2d_ndiv_ ... hfmm2d_ndiv_            cfmm2d_ndiv.f:23-26 etc.
+ *   sources   hfmm2d_mps_ (multipole expansions)       src/helmholtz/hfmm2d_mps.f:19-22
  *   flags     {c,l,r,h}fmm2d_{s,t,st}_{c,d,cd}_{p,g,h}[_vec]_   (27 + 27 per family)
  *             src/laplace/{l,r,c}fmm2dwrap.f, {l,r,c}fmm2dwrap_vec.f,
  *             src/helmholtz/hfmm2dwrap.f, hfmm2dwrap_vec.f
@@ -84,6 +85,13 @@ void hfmm2d_ndiv_(const int* nd, const double* eps, const double* zk, const int*
                   const int* nt, const double* targ, const int* ifpghtarg, double* pottarg,
                   double* gradtarg, double* hesstarg, const int* ndiv, const int* idivflag,
                   const int* ifnear, double* timeinfo, int* ier);
+
+/* ---- FMM over multipole expansions (src/helmholtz/hfmm2d_mps.f:19-22):
+ * cmpole(2,nmpole), rmpole(nmpole), mterms(nmpole), mpole/local(ntot)
+ * complex, impole(nmpole) 1-based offsets of the (nd,-m:m) blocks. */
+void hfmm2d_mps_(const int* nd, const double* eps, const double* zk, const int* nmpole,
+                 const double* cmpole, const double* rmpole, const int* mterms, const int* ntot,
+                 const double* mpole, const int* impole, double* local, int* ier);
 
 /* ---- flag wrappers.  Argument lists, in order:
  *   [nd,] eps, [zk,] ns, sources, <densities>, <source outputs>, [nt, targ, <target outputs>,] ier
