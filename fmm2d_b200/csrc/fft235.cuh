@@ -26,7 +26,7 @@ struct Plan {
 };
 
 // Factorisation of a 5-smooth n (false otherwise).
-inline bool plan(int n, Plan& P) {
+__host__ __device__ inline bool plan(int n, Plan& P) {
   P.n = n;
   P.nf = 0;
   if (n < 1) return false;
@@ -40,7 +40,7 @@ inline bool plan(int n, Plan& P) {
 
 // Smallest even 5-smooth integer >= n (src/common/next235.f: the search
 // starts at 2 ceil(n / 2) and steps by 2).
-inline int next235(int n) {
+__host__ __device__ inline int next235(int n) {
   int k = 2 * ((n + 1) / 2);
   if (k <= 0) k = 2;
   for (;; k += 2) {

@@ -19,6 +19,7 @@
 #include <cmath>
 #include <mutex>
 
+#include "fft235.cuh"
 #include "helm_special.cuh"
 #include "lap_common.cuh"
 #include "laplace.cuh"
@@ -74,7 +75,8 @@ void ensure_device_tables() {
   done[dev] = true;
 }
 
-constexpr int HMAXP = 63;  // largest supported expansion order (2p+1 <= 4 x 32 lanes)
+constexpr int HMAXP = 63;      // largest order of the coefficient-per-lane translations
+constexpr int HF_MAXSIG = 7000;  // longest signature (2 x 7000 x 16 B of shared memory)
 
 struct HLev {
   int lfirst, p, P, ok;  // ok: expansions formed at this level (zkiupbound test)
@@ -82,6 +84,12 @@ struct HLev {
   long off;              // expansion offset (double2 units, times ND inside kernels)
   int nsh;               // half width of the M2M/L2L tables towards level l+1
   long tm2l, tm2m, tl2l; // table offsets (double2 units)
+  // wideband: translations of this level (M2L, and the shifts between it
+  // and level l+1) run on signatures, FFTs of the expansions
+  int wide;
+  int nsig, nsig_sh;      // signature lengths: M2L, shifts towards l+1
+  long sig_off;           // per-box M2L signatures (double2 units, times ND)
+  long tv_m2l, tv_mm, tv_ll;  // diagonal translation operators (double2 units)
 };
 
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
@@ -115,7 +123,7 @@ __global__ void k_h_tables(const HLev* __restrict__ lv, int nl, double zkr, doub
   double2* Z = scratch + (size_t)tid * scratch_stride;
   HLev L = lv[l];
   if (k < 49) {
-    if (l < 2 || !L.ok) return;
+    if (l < 2 || !L.ok || L.wide) return;
     int ox = k / 7 - 3, oy = k % 7 - 3;
     if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) return;
     // z0 = c_tgt - c_src = o bs; theta - pi as in h2dmploc
@@ -126,7 +134,7 @@ __global__ void k_h_tables(const HLev* __restrict__ lv, int nl, double zkr, doub
     phase_table(nt, th, Z, tabs + L.tm2l + (size_t)k * (2 * nt + 1));
     return;
   }
-  if (l >= nl || l < 2) return;  // shifts run between levels >= 2
+  if (l >= nl || l < 2 || L.wide) return;  // shifts run between levels >= 2
   HLev C = lv[l + 1];
   int slot = (k - 49) % 4, kind = (k - 49) / 4;  // kind 0: M2M, 1: L2L
   if (!(kind == 0 ? C.ok : L.ok)) return;
@@ -201,12 +209,12 @@ __device__ __forceinline__ double2 src_term(int n, const double2* Z, const doubl
 template <int ND>
 __device__ void form_from_sources(int lane, double2* Zs, double2* Es, double* Ps, int sbeg,
                                   int send, const double2* __restrict__ xs, const HDens& D,
-                                  double2 c, double2 zk, double rs, int p, bool mpole,
-                                  double2 acc[4][ND]) {
+                                  double2 c, double2 zk, double rs, int p, bool mpole, int n0,
+                                  int SB, double2 acc[4][ND]) {
   const int W = p + 3;  // table width (orders 0..p+2)
   const bool hq = D.q != nullptr, hd = D.d != nullptr;
-  for (int s0 = sbeg; s0 < send; s0 += 16) {
-    int m = min(16, send - s0);
+  for (int s0 = sbeg; s0 < send; s0 += SB) {
+    int m = min(SB, send - s0);
     __syncwarp();
     if (lane < m) {
       int j = s0 + lane;
@@ -240,7 +248,7 @@ __device__ void form_from_sources(int lane, double2* Zs, double2* Es, double* Ps
     double rsd = mpole ? rs : 1.0 / rs;
 #pragma unroll
     for (int sl = 0; sl < 4; sl++) {
-      int n = lane + 32 * sl - p;
+      int n = n0 + lane + 32 * sl;
       if (n > p) break;
       for (int jj = 0; jj < m; jj++) {
         const double* Pp = Ps + jj * (4 * ND + 2 * ND);
@@ -267,11 +275,19 @@ __device__ __forceinline__ double2* hexp(double2* base, const HLev& L, int b, in
   return base + (L.off + (size_t)(b - L.lfirst) * L.P) * ND;
 }
 
-// step 1: P2M at leaves of levels >= 2 (zero expansions elsewhere)
+// Shared memory of one warp of the expansion-forming kernels: tables of SB
+// sources (Z and E, orders 0..maxp+2) and their densities.
+__device__ __forceinline__ double2* form_smem(double2* base, int wib, int maxp, int SB, int ND) {
+  return base + (size_t)wib * SB * (2 * (maxp + 3) + 3 * ND);
+}
+
+// step 1: P2M at leaves of levels >= 2 (zero expansions elsewhere), 128
+// coefficients at a time
 template <int ND>
 __global__ void __launch_bounds__(64) k_h_p2m(TV t, const HLev* __restrict__ lv, int nb,
                                               const double2* __restrict__ xs, HDens D, double zkr,
-                                              double zki, double2* __restrict__ mp, int maxp) {
+                                              double zki, double2* __restrict__ mp, int maxp,
+                                              int SB) {
   extern __shared__ double2 hsm[];
   HLOOP(nb) {
     int b = bi;
@@ -280,25 +296,27 @@ __global__ void __launch_bounds__(64) k_h_p2m(TV t, const HLev* __restrict__ lv,
     if (lev < 2) continue;  // multipoles of levels 0 and 1 are never used
     HLev L = lv[lev];
     int W = L.p + 3;
-    double2* Zs = hsm + (size_t)wib * (32 * (maxp + 3) + 16 * 3 * ND);
-    double2* Es = Zs + 16 * W;
-    double* Ps = (double*)(Es + 16 * W);
-    double2 acc[4][ND];
-#pragma unroll
-    for (int s = 0; s < 4; s++)
-#pragma unroll
-      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+    double2* Zs = form_smem(hsm, wib, maxp, SB, ND);
+    double2* Es = Zs + SB * W;
+    double* Ps = (double*)(Es + SB * W);
     int2 sr = t.srng[b];
-    if (L.ok && sr.y > sr.x)
-      form_from_sources<ND>(lane, Zs, Es, Ps, sr.x, sr.y, xs, D, t.center[b],
-                            make_double2(zkr, zki), L.rs, L.p, true, acc);
     double2* M = hexp(mp, L, b, ND);
+    for (int n0 = -L.p; n0 <= L.p; n0 += 128) {
+      double2 acc[4][ND];
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      int n = lane + 32 * s - L.p;
-      if (n > L.p) break;
+      for (int s = 0; s < 4; s++)
 #pragma unroll
-      for (int d = 0; d < ND; d++) M[(n + L.p) * ND + d] = acc[s][d];
+        for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+      if (L.ok && sr.y > sr.x)
+        form_from_sources<ND>(lane, Zs, Es, Ps, sr.x, sr.y, xs, D, t.center[b],
+                              make_double2(zkr, zki), L.rs, L.p, true, n0, SB, acc);
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        int n = n0 + lane + 32 * s;
+        if (n > L.p) break;
+#pragma unroll
+        for (int d = 0; d < ND; d++) M[(n + L.p) * ND + d] = acc[s][d];
+      }
     }
   }
 }
@@ -307,7 +325,8 @@ __global__ void __launch_bounds__(64) k_h_p2m(TV t, const HLev* __restrict__ lv,
 template <int ND>
 __global__ void __launch_bounds__(64) k_h_p2l(TV t, const HLev* __restrict__ lv, int first, int n,
                                               const double2* __restrict__ xs, HDens D, double zkr,
-                                              double zki, double2* __restrict__ lo, int maxp) {
+                                              double zki, double2* __restrict__ lo, int maxp,
+                                              int SB) {
   extern __shared__ double2 hsm[];
   HLOOP(n) {
     int b = first + bi;
@@ -317,26 +336,29 @@ __global__ void __launch_bounds__(64) k_h_p2l(TV t, const HLev* __restrict__ lv,
     HLev L = lv[lev];
     if (!L.ok) continue;
     int W = L.p + 3;
-    double2* Zs = hsm + (size_t)wib * (32 * (maxp + 3) + 16 * 3 * ND);
-    double2* Es = Zs + 16 * W;
-    double* Ps = (double*)(Es + 16 * W);
-    double2 acc[4][ND];
-#pragma unroll
-    for (int s = 0; s < 4; s++)
-#pragma unroll
-      for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
-    for (int e = 0; e < n4; e++) {
-      int2 sr = t.srng[t.l4[(size_t)MNLIST4 * b + e]];
-      form_from_sources<ND>(lane, Zs, Es, Ps, sr.x, sr.y, xs, D, t.center[b],
-                            make_double2(zkr, zki), L.rs, L.p, false, acc);
-    }
+    double2* Zs = form_smem(hsm, wib, maxp, SB, ND);
+    double2* Es = Zs + SB * W;
+    double* Ps = (double*)(Es + SB * W);
     double2* Lo = hexp(lo, L, b, ND);
+    for (int n0 = -L.p; n0 <= L.p; n0 += 128) {
+      double2 acc[4][ND];
 #pragma unroll
-    for (int s = 0; s < 4; s++) {
-      int nn = lane + 32 * s - L.p;
-      if (nn > L.p) break;
+      for (int s = 0; s < 4; s++)
 #pragma unroll
-      for (int d = 0; d < ND; d++) Lo[(nn + L.p) * ND + d] = cadd(Lo[(nn + L.p) * ND + d], acc[s][d]);
+        for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+      for (int e = 0; e < n4; e++) {
+        int2 sr = t.srng[t.l4[(size_t)MNLIST4 * b + e]];
+        form_from_sources<ND>(lane, Zs, Es, Ps, sr.x, sr.y, xs, D, t.center[b],
+                              make_double2(zkr, zki), L.rs, L.p, false, n0, SB, acc);
+      }
+#pragma unroll
+      for (int s = 0; s < 4; s++) {
+        int nn = n0 + lane + 32 * s;
+        if (nn > L.p) break;
+#pragma unroll
+        for (int d = 0; d < ND; d++)
+          Lo[(nn + L.p) * ND + d] = cadd(Lo[(nn + L.p) * ND + d], acc[s][d]);
+      }
     }
   }
 }
@@ -442,7 +464,7 @@ __global__ void __launch_bounds__(128) k_h_m2l(TV t, const HLev* __restrict__ lv
     if (n2 == 0 || !t.has_eval_pts(b)) continue;
     const int lev = t.level[b];
     const HLev L = lv[lev];
-    if (!L.ok) continue;
+    if (!L.ok || L.wide) continue;
     const int p = L.p, np = 2 * p + 1, nt = 2 * p;
     const int i = tid - p;
     const bool act = tid < np;
@@ -568,6 +590,211 @@ __global__ void __launch_bounds__(128) k_h_l2l(TV t, const HLev* __restrict__ lv
         double2 v = cadd(acc[d], cadd(cscale(accc[d], Cf), cscale(acca[d], A)));
         J2[(i + p2) * ND + d] = cadd(J2[(i + p2) * ND + d], v);
       }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wideband levels (src/helmholtz/wideband2d.f, hfmm2d.f:1051-1097,
+// 1124-1208, 1279-1285).  With unit scales every translation is the linear
+// convolution out(i) = sum_j in(j) T(i-j) of the expansion with the shift's
+// table T(k), k = -nt..nt.  An expansion placed at indices k mod nsig
+// (nsig >= 2 nt + 1, 5-smooth) and Fourier transformed is its signature;
+// the translation is then a pointwise product with the transformed table
+// (divided by nsig), and the backward transform gives the expansion back.
+// ---------------------------------------------------------------------------
+struct TvJob {
+  long out;
+  int nsig, nt, bessel;  // bessel: J tables (shifts), else H (M2L)
+  double x, y;           // centre shift c2 - c1
+};
+
+// One block per operator (h2d_mkm2ltrans / h2d_mkmpshift).
+__global__ void __launch_bounds__(256) k_hf_transvec(const TvJob* __restrict__ jobs, double zkr,
+                                                     double zki, double2* __restrict__ tabs) {
+  extern __shared__ __align__(16) double2 fsm[];
+  const TvJob J = jobs[blockIdx.x];
+  fft::Plan P;
+  fft::plan(J.nsig, P);
+  double2* X = fsm;
+  double2* Y = X + J.nsig;  // holds the values Z_k first (nt + 2 <= nsig)
+  const double pi = 3.14159265358979323846;
+  if (threadIdx.x == 0) {
+    const double r = sqrt(J.x * J.x + J.y * J.y);
+    const double2 z = make_double2(zkr * r, zki * r);
+    if (J.bessel)
+      jscaled(J.nt, z, 1.0, Y);
+    else
+      hscaled(J.nt + 1, z, 1.0, Y);
+  }
+  const double th = atan2(J.y, J.x) - pi;
+  const double inv = 1.0 / J.nsig;
+  for (int k = threadIdx.x; k < J.nsig; k += blockDim.x) X[k] = make_double2(0, 0);
+  __syncthreads();
+  for (int j = threadIdx.x; j <= J.nt; j += blockDim.x) {
+    double sn, cs;
+    sincos(j * th, &sn, &cs);
+    const double2 zj = cscale(Y[j], inv);
+    X[j] = cmul(make_double2(cs, -sn), zj);  // exp(-i theta)^j Z_j
+    if (j > 0) {
+      double2 t = cmul(make_double2(cs, sn), zj);  // (-conj e)^j Z_j
+      if (j & 1) t = make_double2(-t.x, -t.y);
+      X[J.nsig - j] = t;
+    }
+  }
+  const double2* R = fft::block_fft(P, X, Y, -1);
+  for (int k = threadIdx.x; k < J.nsig; k += blockDim.x) tabs[J.out + k] = R[k];
+}
+
+// x[k mod nsig] = E(k), k = -p..p (density d), zero elsewhere.
+__device__ __forceinline__ void hf_pack(const double2* __restrict__ E, int p, int ND, int d,
+                                        double2* x, int nsig) {
+  for (int k = threadIdx.x; k < nsig; k += blockDim.x) {
+    int i = k <= p ? k : (k >= nsig - p ? k - nsig : p + 1);
+    x[k] = i <= p ? E[(size_t)(i + p) * ND + d] : make_double2(0, 0);
+  }
+}
+
+// E(i) += x[i mod nsig], i = -p..p (density d).
+__device__ __forceinline__ void hf_unpack_add(const double2* x, int nsig, double2* E, int p,
+                                              int ND, int d) {
+  for (int i = (int)threadIdx.x - p; i <= p; i += blockDim.x) {
+    const int k = i >= 0 ? i : nsig + i;
+    double2* e = E + (size_t)(i + p) * ND + d;
+    *e = cadd(*e, x[k]);
+  }
+}
+
+// Signatures of the multipoles of one wideband level (h2d_mptosig).
+template <int ND>
+__global__ void __launch_bounds__(256) k_hf_tosig(const HLev* __restrict__ lv, int lev, int first,
+                                                  int n, const double2* __restrict__ mp,
+                                                  double2* __restrict__ sig) {
+  extern __shared__ __align__(16) double2 fsm[];
+  const HLev L = lv[lev];
+  fft::Plan P;
+  fft::plan(L.nsig, P);
+  double2* X = fsm;
+  double2* Y = X + L.nsig;
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
+    const double2* E = hexp(const_cast<double2*>(mp), L, b, ND);
+    double2* S = sig + (L.sig_off + (size_t)(b - L.lfirst) * L.nsig) * ND;
+    for (int d = 0; d < ND; d++) {
+      hf_pack(E, L.p, ND, d, X, L.nsig);
+      const double2* R = fft::block_fft(P, X, Y, -1);
+      for (int k = threadIdx.x; k < L.nsig; k += blockDim.x) S[(size_t)k * ND + d] = R[k];
+      __syncthreads();
+    }
+  }
+}
+
+// M2L of one wideband level: products of the list-2 signatures with the
+// offset's operator, summed, transformed back and added to the local
+// expansion (h2d_diagtrans, h2d_sig2exp).
+template <int ND>
+__global__ void __launch_bounds__(256) k_hf_m2l(TV t, const HLev* __restrict__ lv, int lev, int first,
+                                                int n, const double2* __restrict__ sig,
+                                                const double2* __restrict__ tabs,
+                                                double2* __restrict__ lo) {
+  extern __shared__ __align__(16) double2 fsm[];
+  const HLev L = lv[lev];
+  fft::Plan P;
+  fft::plan(L.nsig, P);
+  double2* X = fsm;
+  double2* Y = X + L.nsig;
+  const double rinv = 1.0 / L.bs;
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
+    const int n2 = t.nl2[b];
+    if (n2 == 0 || !t.has_eval_pts(b)) continue;
+    const double2 cb = t.center[b];
+    for (int d = 0; d < ND; d++) {
+      for (int k = threadIdx.x; k < L.nsig; k += blockDim.x) {
+        double2 acc = make_double2(0, 0);
+        for (int e = 0; e < n2; e++) {
+          const int jb = t.l2[(size_t)MNLIST2 * b + e];
+          const double2 cj = t.center[jb];
+          const int ox = __double2int_rn((cb.x - cj.x) * rinv);
+          const int oy = __double2int_rn((cb.y - cj.y) * rinv);
+          const double2 tv = tabs[L.tv_m2l + (size_t)((ox + 3) * 7 + (oy + 3)) * L.nsig + k];
+          const double2 sj = sig[(L.sig_off + (size_t)(jb - L.lfirst) * L.nsig + k) * ND + d];
+          cfma(acc, tv, sj);
+        }
+        X[k] = acc;
+      }
+      const double2* R = fft::block_fft(P, X, Y, +1);
+      hf_unpack_add(R, L.nsig, hexp(lo, L, b, ND), L.p, ND, d);
+      __syncthreads();
+    }
+  }
+}
+
+// One shift between a wideband level and the next through signatures:
+// dst(-p2..p2) += backward(op * forward(src(-p1..p1))).
+template <int ND>
+__device__ void hf_shift(const fft::Plan& P, const double2* src, int p1, const double2* op,
+                         double2* dst, int p2, double2* X, double2* Y) {
+  for (int d = 0; d < ND; d++) {
+    hf_pack(src, p1, ND, d, X, P.n);
+    double2* R = fft::block_fft(P, X, Y, -1);
+    double2* W = R == X ? Y : X;
+    for (int k = threadIdx.x; k < P.n; k += blockDim.x) R[k] = cmul(R[k], op[k]);
+    const double2* B = fft::block_fft(P, R, W, +1);
+    hf_unpack_add(B, P.n, dst, p2, ND, d);
+    __syncthreads();
+  }
+}
+
+// M2M into the parents of one wideband level (h2dmpmphf + h2d_sig2exp).
+template <int ND>
+__global__ void __launch_bounds__(256) k_hf_m2m(TV t, const HLev* __restrict__ lv, int lev, int first,
+                                                int n, const double2* __restrict__ tabs,
+                                                double2* __restrict__ mp) {
+  extern __shared__ __align__(16) double2 fsm[];
+  const HLev L = lv[lev], C = lv[lev + 1];
+  fft::Plan P;
+  fft::plan(L.nsig_sh, P);
+  double2* X = fsm;
+  double2* Y = X + L.nsig_sh;
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
+    if (t.nchild[b] == 0) continue;
+    double2* M = hexp(mp, L, b, ND);
+    for (int e = threadIdx.x; e < L.P * ND; e += blockDim.x) M[e] = make_double2(0, 0);
+    __syncthreads();
+    const int4 ch = t.child[b];
+    const int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    for (int q = 0; q < 4; q++) {
+      const int k = cc[q];
+      if (k < 0 || t.srng[k].y <= t.srng[k].x) continue;
+      hf_shift<ND>(P, hexp(mp, C, k, ND), C.p, tabs + L.tv_mm + (size_t)q * L.nsig_sh, M, L.p, X,
+                   Y);
+    }
+  }
+}
+
+// L2L from the parents of one wideband level (h2dloclochf).
+template <int ND>
+__global__ void __launch_bounds__(256) k_hf_l2l(TV t, const HLev* __restrict__ lv, int lev, int first,
+                                                int n, const double2* __restrict__ tabs,
+                                                double2* __restrict__ lo) {
+  extern __shared__ __align__(16) double2 fsm[];
+  const HLev L = lv[lev], C = lv[lev + 1];
+  fft::Plan P;
+  fft::plan(L.nsig_sh, P);
+  double2* X = fsm;
+  double2* Y = X + L.nsig_sh;
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
+    if (t.nchild[b] == 0 || !t.has_eval_pts(b)) continue;
+    const double2* J1 = hexp(lo, L, b, ND);
+    const int4 ch = t.child[b];
+    const int cc[4] = {ch.x, ch.y, ch.z, ch.w};
+    for (int q = 0; q < 4; q++) {
+      if (cc[q] < 0) continue;
+      hf_shift<ND>(P, J1, L.p, tabs + L.tv_ll + (size_t)q * L.nsig_sh, hexp(lo, C, cc[q], ND), C.p,
+                   X, Y);
     }
   }
 }
@@ -1003,16 +1230,19 @@ int grid_w(long nitems, int wpb) {
 // translation tables of one tree (hfmm2d.f:317-326 for orders and scales).
 struct HelmLevels {
   std::vector<HLev> hl;
-  int maxp = 0;  // largest order at levels >= 2
-  long off = 0;  // expansion storage per density (double2 units)
+  int maxp = 0;      // largest order at levels >= 2 of the coefficient-per-lane kernels
+  int maxp_all = 0;  // largest order at levels >= 2
+  long off = 0;      // expansion storage per density (double2 units)
+  long sig_total = 0;  // M2L signatures of the wideband levels per density
+  int maxsig = 0;      // longest signature
   DBuf<HLev> dlv;
   DBuf<double2> tabs;
   DBuf<double> dbs;  // box sizes, one level past the deepest
   explicit HelmLevels(cudaStream_t st) : dlv(st), tabs(st), dbs(st) {}
 };
 
-// ier 13: an order above HMAXP; 20: a level where translations run has
-// boxes larger than 16 wavelengths (hfmm2d.f:1001-1013, the wideband path).
+// ier 13: an order the kernels do not support (above HMAXP with a scale
+// below 1, or a signature longer than HF_MAXSIG).
 int helm_levels(const DeviceTree& T, double zkr, double zki, double eps, HelmLevels& H,
                 cudaStream_t st) {
   const int nl = T.nlevels;
@@ -1020,7 +1250,7 @@ int helm_levels(const DeviceTree& T, double zkr, double zki, double eps, HelmLev
   const double zkabs = std::hypot(zkr, zki);
   std::vector<HLev>& hl = H.hl;
   hl.assign(nl + 1, HLev{});
-  int maxp = 0, ier = 0;
+  int maxp = 0, maxp_all = 0, ier = 0;
   for (int l = 0; l <= nl; l++) {
     double bs = T.boxsize[l];
     hl[l].lfirst = T.lfirst[l];
@@ -1029,25 +1259,60 @@ int helm_levels(const DeviceTree& T, double zkr, double zki, double eps, HelmLev
     hl[l].p = helm_nterms(bs, zkr, zki, eps, &ier);
     hl[l].P = 2 * hl[l].p + 1;
     hl[l].ok = (zki * bs < 40.0) ? 1 : 0;
-    if (hl[l].ok && l >= 1 && bs / (1.0 / (zkr / (2.0 * pi))) > 16.0) return IER_HIGHFREQ;
-    if (l >= 2) maxp = std::max(maxp, hl[l].p);
+    // boxes above 16 wavelengths take the diagonal (signature) translations
+    // (hfmm2d.f:1001-1013, 1124-1208); so do orders beyond the
+    // coefficient-per-lane kernels, where the scale is 1 as well and the two
+    // forms are the same convolution
+    const bool hf = bs / (1.0 / (zkr / (2.0 * pi))) > 16.0;
+    hl[l].wide = (l >= 2 && hl[l].ok && (hf || hl[l].p > HMAXP)) ? 1 : 0;
+    if (l >= 2 && hl[l].ok) {
+      if (hl[l].wide)
+        maxp_all = std::max(maxp_all, hl[l].p);
+      else
+        maxp = std::max(maxp, hl[l].p);
+    }
   }
   if (ier) return ier;
   if (maxp > HMAXP) return IER_NTERMS;
-  H.maxp = maxp;
-  // expansion and table layout
-  long off = 0, toff = 0;
-  for (int l = 0; l <= nl; l++) {
-    hl[l].off = off;
-    off += (long)(T.llast[l] - T.lfirst[l] + 1) * hl[l].P;
-    hl[l].nsh = l < nl ? hl[l].p + hl[l + 1].p : 0;
-    hl[l].tm2l = toff;
-    if (l >= 2) toff += 49L * (4 * hl[l].p + 1);
-    hl[l].tm2m = toff;
-    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
-    hl[l].tl2l = toff;
-    if (l < nl) toff += 4L * (2 * hl[l].nsh + 1);
+  maxp_all = std::max(maxp_all, maxp);
+  for (int l = 2; l <= nl; l++) {
+    HLev& L = hl[l];
+    if (!L.wide) continue;
+    // the signature form holds for unit scales only (rscale = 1 in
+    // wideband2d.f); shifts also need the child level's scale to be 1
+    if (L.rs != 1.0 || (l < nl && hl[l + 1].ok && hl[l + 1].rs != 1.0)) return IER_NTERMS;
+    L.nsig = fft::next235(2 * (L.p + L.p) + 1);
+    L.nsig_sh = l < nl ? fft::next235(2 * (L.p + hl[l + 1].p) + 1) : 0;
+    if (L.nsig > HF_MAXSIG || L.nsig_sh > HF_MAXSIG) return IER_NTERMS;
   }
+  H.maxp = maxp;
+  H.maxp_all = maxp_all;
+  // expansion and table layout
+  long off = 0, toff = 0, soff = 0;
+  for (int l = 0; l <= nl; l++) {
+    HLev& L = hl[l];
+    const long nbl = (long)(T.llast[l] - T.lfirst[l] + 1);
+    L.off = off;
+    off += nbl * L.P;
+    L.nsh = l < nl ? L.p + hl[l + 1].p : 0;
+    L.tm2l = toff;
+    if (l >= 2 && !L.wide) toff += 49L * (4 * L.p + 1);
+    L.tm2m = toff;
+    if (l < nl && !L.wide) toff += 4L * (2 * L.nsh + 1);
+    L.tl2l = toff;
+    if (l < nl && !L.wide) toff += 4L * (2 * L.nsh + 1);
+    if (L.wide) {
+      L.tv_m2l = toff;
+      toff += 49L * L.nsig;
+      L.tv_mm = toff;
+      if (l < nl) toff += 4L * L.nsig_sh;
+      L.tv_ll = toff;
+      if (l < nl) toff += 4L * L.nsig_sh;
+      L.sig_off = soff;
+      soff += nbl * L.nsig;
+    }
+  }
+  H.sig_total = soff;
   H.off = off;
   H.dlv.alloc(nl + 1, st);
   B2_CHECK(cudaMemcpyAsync(H.dlv.p, hl.data(), sizeof(HLev) * (nl + 1), cudaMemcpyHostToDevice, st));
@@ -1058,6 +1323,41 @@ int helm_levels(const DeviceTree& T, double zkr, double zki, double eps, HelmLev
   k_h_tables<<<ceil_div(nthreads, 64), 64, 0, st>>>(H.dlv.p, nl, zkr, zki, H.tabs.p, scratch.p,
                                                     sstride);
   B2_LAUNCH_CHECK();
+  // diagonal operators of the wideband levels: M2L per offset (target -
+  // source = o bs), M2M per child slot (parent - child), L2L (child - parent)
+  std::vector<TvJob> jobs;
+  int maxsig = 0;
+  for (int l = 2; l <= nl; l++) {
+    const HLev& L = hl[l];
+    if (!L.wide) continue;
+    for (int k = 0; k < 49; k++) {
+      const int ox = k / 7 - 3, oy = k % 7 - 3;
+      if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) continue;
+      jobs.push_back(TvJob{L.tv_m2l + (long)k * L.nsig, L.nsig, 2 * L.p, 0, ox * L.bs, oy * L.bs});
+    }
+    maxsig = std::max(maxsig, L.nsig);
+    if (l < nl) {
+      const double h = L.bs / 4;  // child centre - parent centre
+      for (int q = 0; q < 4; q++) {
+        const double cx = (q & 1) ? h : -h, cy = (q < 2) ? -h : h;
+        const int nt = L.p + hl[l + 1].p;
+        jobs.push_back(TvJob{L.tv_mm + (long)q * L.nsig_sh, L.nsig_sh, nt, 1, -cx, -cy});
+        jobs.push_back(TvJob{L.tv_ll + (long)q * L.nsig_sh, L.nsig_sh, nt, 1, cx, cy});
+      }
+      maxsig = std::max(maxsig, L.nsig_sh);
+    }
+  }
+  if (!jobs.empty()) {
+    DBuf<TvJob> dj(st);
+    dj.alloc(jobs.size(), st);
+    B2_CHECK(cudaMemcpyAsync(dj.p, jobs.data(), sizeof(TvJob) * jobs.size(), cudaMemcpyHostToDevice,
+                             st));
+    const size_t sm = 2 * sizeof(double2) * (size_t)maxsig;
+    set_smem(k_hf_transvec, sm);
+    k_hf_transvec<<<(int)jobs.size(), 256, sm, st>>>(dj.p, zkr, zki, H.tabs.p);
+    B2_LAUNCH_CHECK();
+  }
+  H.maxsig = maxsig;
   std::vector<double> bsx(T.boxsize);
   bsx.push_back(T.boxsize.back() / 2);
   H.dbs.alloc(bsx.size(), st);
@@ -1066,56 +1366,124 @@ int helm_levels(const DeviceTree& T, double zkr, double zki, double eps, HelmLev
   return IER_OK;
 }
 
+// Source batch of the expansion-forming kernels (2 warps per block) and
+// their shared memory: 16 sources at a time, fewer for high orders.
+int form_batch(int maxp, int ND, size_t* bytes) {
+  int SB = 16;
+  auto need = [&](int sb) { return sizeof(double2) * 2 * (size_t)sb * (2 * (maxp + 3) + 3 * ND); };
+  while (SB > 1 && need(SB) > 200 * 1024) SB /= 2;
+  *bytes = need(SB);
+  return SB;
+}
+
+// M2M into levels nl-1 .. 2; signature form at the wideband levels.
 template <int ND>
-void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
-                const HLev* dlv, const std::vector<HLev>& hl, int maxp, const double2* tabs,
-                const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
-                double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, double thresh,
-                const int* leaf_s, const int* leaf_t, long ns_pts, long nt_pts, cudaStream_t st,
-                cudaEvent_t* ev) {
-  const int nb = T.nboxes, nl = T.nlevels;
-  B2_CHECK(cudaEventRecord(ev[0], st));
-  size_t sm_form = sizeof(double2) * 2 * (32 * (size_t)(maxp + 3) + 16 * 3 * ND);
-  set_smem(k_h_p2m<ND>, sm_form);
-  set_smem(k_h_p2l<ND>, sm_form);
-  k_h_p2m<ND><<<grid_w(nb, 2), 64, sm_form, st>>>(tv, dlv, nb, xs, D, a.zkr, a.zki, mp, maxp);
-  B2_LAUNCH_CHECK();
-  B2_CHECK(cudaEventRecord(ev[1], st));
-  for (int l = nl - 1; l >= 2; l--) {
+void upward_pass(const TV& tv, const DeviceTree& T, const HelmLevels& H, double2* mp,
+                 cudaStream_t st) {
+  const std::vector<HLev>& hl = H.hl;
+  for (int l = T.nlevels - 1; l >= 2; l--) {
     if (!hl[l].ok) continue;
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    size_t sm = sizeof(double2) * (2 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
-                sizeof(double) * (HMAXP + 1);
-    set_smem(k_h_m2m<ND>, sm);
-    k_h_m2m<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, dlv, l, f, n, tabs, mp);
+    if (hl[l].wide) {
+      const size_t sm = 2 * sizeof(double2) * (size_t)hl[l].nsig_sh;
+      set_smem(k_hf_m2m<ND>, sm);
+      k_hf_m2m<ND><<<(int)std::min<long>(n, 148L * 4), 256, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                      H.tabs.p, mp);
+    } else {
+      size_t sm = sizeof(double2) * (2 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
+                  sizeof(double) * (HMAXP + 1);
+      set_smem(k_h_m2m<ND>, sm);
+      k_h_m2m<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                     H.tabs.p, mp);
+    }
     B2_LAUNCH_CHECK();
   }
-  B2_CHECK(cudaEventRecord(ev[2], st));
-  if (nl >= 2) {
-    int f = T.lfirst[2], n = nb - f;
-    k_h_p2l<ND><<<grid_w(n, 2), 64, sm_form, st>>>(tv, dlv, f, n, xs, D, a.zkr, a.zki, lo, maxp);
-    B2_LAUNCH_CHECK();
-  }
-  B2_CHECK(cudaEventRecord(ev[3], st));
-  if (nl >= 2) {
+}
+
+// M2L at levels >= 2: tabulated kernels, and signatures at the wideband levels.
+template <int ND>
+void m2l_pass(const TV& tv, const DeviceTree& T, const HelmLevels& H, const double2* mp,
+              double2* lo, double2* sig, cudaStream_t st) {
+  const int nb = T.nboxes, nl = T.nlevels;
+  if (nl < 2) return;
+  const int maxp = H.maxp;
+  {
     int f = T.lfirst[2], n = nb - f;
     size_t sm = sizeof(double2) * (2 * (2 * maxp + 1) * ND + 4 * maxp + 1) +
                 sizeof(double) * (maxp + 1);
     set_smem(k_h_m2l<ND>, sm);
-    k_h_m2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, dlv, f, n, tabs, mp, lo,
-                                                                   maxp);
+    k_h_m2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, f, n, H.tabs.p,
+                                                                   mp, lo, maxp);
     B2_LAUNCH_CHECK();
   }
-  B2_CHECK(cudaEventRecord(ev[4], st));
-  for (int l = 2; l <= nl - 1; l++) {
+  for (int l = 2; l <= nl; l++) {
+    const HLev& L = H.hl[l];
+    if (!L.wide) continue;
+    int f = T.lfirst[l], n = T.llast[l] - f + 1;
+    const size_t sm = 2 * sizeof(double2) * (size_t)L.nsig;
+    set_smem(k_hf_tosig<ND>, sm);
+    k_hf_tosig<ND><<<(int)std::min<long>(n, 148L * 4), 256, sm, st>>>(H.dlv.p, l, f, n, mp, sig);
+    B2_LAUNCH_CHECK();
+    set_smem(k_hf_m2l<ND>, sm);
+    k_hf_m2l<ND><<<(int)std::min<long>(n, 148L * 4), 256, sm, st>>>(tv, H.dlv.p, l, f, n, sig,
+                                                                    H.tabs.p, lo);
+    B2_LAUNCH_CHECK();
+  }
+}
+
+// L2L from levels 2 .. nl-1; signature form at the wideband levels.
+template <int ND>
+void downward_pass(const TV& tv, const DeviceTree& T, const HelmLevels& H, double2* lo,
+                   cudaStream_t st) {
+  const std::vector<HLev>& hl = H.hl;
+  for (int l = 2; l <= T.nlevels - 1; l++) {
     if (!hl[l].ok) continue;
     int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    size_t sm = sizeof(double2) * ((2 * hl[l].p + 1) * ND + 4 * (2 * hl[l].nsh + 1)) +
-                sizeof(double) * (HMAXP + 1);
-    set_smem(k_h_l2l<ND>, sm);
-    k_h_l2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, dlv, l, f, n, tabs, lo);
+    if (hl[l].wide) {
+      const size_t sm = 2 * sizeof(double2) * (size_t)hl[l].nsig_sh;
+      set_smem(k_hf_l2l<ND>, sm);
+      k_hf_l2l<ND><<<(int)std::min<long>(n, 148L * 4), 256, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                      H.tabs.p, lo);
+    } else {
+      size_t sm = sizeof(double2) * ((2 * hl[l].p + 1) * ND + 4 * (2 * hl[l].nsh + 1)) +
+                  sizeof(double) * (HMAXP + 1);
+      set_smem(k_h_l2l<ND>, sm);
+      k_h_l2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                     H.tabs.p, lo);
+    }
     B2_LAUNCH_CHECK();
   }
+}
+
+template <int ND>
+void helm_chunk(const TV& tv, DeviceTree& T, const HelmArgs& a, const HDens& D,
+                const HelmLevels& H, const double2* xs, const double2* xt, double2* mp,
+                double2* lo, double2* sig, double2* ps, double2* gs, double2* hs, double2* pt,
+                double2* gt, double2* ht, double thresh, const int* leaf_s, const int* leaf_t,
+                long ns_pts, long nt_pts, cudaStream_t st, cudaEvent_t* ev) {
+  const int nb = T.nboxes, nl = T.nlevels;
+  const HLev* dlv = H.dlv.p;
+  B2_CHECK(cudaEventRecord(ev[0], st));
+  size_t sm_form = 0;
+  const int SB = form_batch(H.maxp_all, ND, &sm_form);
+  set_smem(k_h_p2m<ND>, sm_form);
+  set_smem(k_h_p2l<ND>, sm_form);
+  k_h_p2m<ND><<<grid_w(nb, 2), 64, sm_form, st>>>(tv, dlv, nb, xs, D, a.zkr, a.zki, mp,
+                                                  H.maxp_all, SB);
+  B2_LAUNCH_CHECK();
+  B2_CHECK(cudaEventRecord(ev[1], st));
+  upward_pass<ND>(tv, T, H, mp, st);
+  B2_CHECK(cudaEventRecord(ev[2], st));
+  if (nl >= 2) {
+    int f = T.lfirst[2], n = nb - f;
+    k_h_p2l<ND><<<grid_w(n, 2), 64, sm_form, st>>>(tv, dlv, f, n, xs, D, a.zkr, a.zki, lo,
+                                                   H.maxp_all, SB);
+    B2_LAUNCH_CHECK();
+  }
+  B2_CHECK(cudaEventRecord(ev[3], st));
+  m2l_pass<ND>(tv, T, H, mp, lo, sig, st);
+  B2_CHECK(cudaEventRecord(ev[4], st));
+  downward_pass<ND>(tv, T, H, lo, st);
   B2_CHECK(cudaEventRecord(ev[5], st));
   auto leaf = [&](int use_t, int ifl, const double2* xe, double2* po, double2* gr, double2* he) {
     const long n = use_t ? nt_pts : ns_pts;
@@ -1390,51 +1758,25 @@ size_t mps_smem(int maxnt, int warps) {
 template <int ND>
 void mps_chunk(const TV& tv, const DeviceTree& T, const HelmLevels& H, const MpsExp& E,
                const double2* mpole, int nd, int d0, double2 zk, double2* mp, double2* lo,
-               const int* leaf, long nc, double2* local, double thresh, int maxnt,
-               cudaStream_t st) {
+               double2* sig, const int* leaf, long nc, double2* local, double thresh, int maxnt,
+               int warps, cudaStream_t st) {
   const int nb = T.nboxes, nl = T.nlevels;
-  const std::vector<HLev>& hl = H.hl;
-  const size_t xs = mps_smem(maxnt, 4);
+  const size_t xs = mps_smem(maxnt, warps);
+  const int thr = 32 * warps;
   B2_CHECK(cudaMemsetAsync(mp, 0, sizeof(double2) * (size_t)H.off * ND, st));
   B2_CHECK(cudaMemsetAsync(lo, 0, sizeof(double2) * (size_t)H.off * ND, st));
   if (nl >= 2) {
     const int f = T.lfirst[2], n = nb - f;
     set_smem(k_mps_boxes<ND>, xs);
-    k_mps_boxes<ND><<<(int)std::min<long>(ceil_div(n, 4), 148L * 8), 128, xs, st>>>(
+    k_mps_boxes<ND><<<(int)std::min<long>(ceil_div(n, warps), 148L * 8), thr, xs, st>>>(
         tv, H.dlv.p, f, n, E, mpole, nd, d0, zk, mp, lo, maxnt);
     B2_LAUNCH_CHECK();
   }
-  for (int l = nl - 1; l >= 2; l--) {
-    if (!hl[l].ok) continue;
-    int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    size_t sm = sizeof(double2) * (2 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
-                sizeof(double) * (HMAXP + 1);
-    set_smem(k_h_m2m<ND>, sm);
-    k_h_m2m<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
-                                                                   H.tabs.p, mp);
-    B2_LAUNCH_CHECK();
-  }
-  if (nl >= 2) {
-    int f = T.lfirst[2], n = nb - f;
-    size_t sm = sizeof(double2) * (2 * (2 * H.maxp + 1) * ND + 4 * H.maxp + 1) +
-                sizeof(double) * (H.maxp + 1);
-    set_smem(k_h_m2l<ND>, sm);
-    k_h_m2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, f, n, H.tabs.p,
-                                                                   mp, lo, H.maxp);
-    B2_LAUNCH_CHECK();
-  }
-  for (int l = 2; l <= nl - 1; l++) {
-    if (!hl[l].ok) continue;
-    int f = T.lfirst[l], n = T.llast[l] - f + 1;
-    size_t sm = sizeof(double2) * ((2 * hl[l].p + 1) * ND + 4 * (2 * hl[l].nsh + 1)) +
-                sizeof(double) * (HMAXP + 1);
-    set_smem(k_h_l2l<ND>, sm);
-    k_h_l2l<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
-                                                                   H.tabs.p, lo);
-    B2_LAUNCH_CHECK();
-  }
+  upward_pass<ND>(tv, T, H, mp, st);
+  m2l_pass<ND>(tv, T, H, mp, lo, sig, st);
+  downward_pass<ND>(tv, T, H, lo, st);
   set_smem(k_mps_locals<ND>, xs);
-  k_mps_locals<ND><<<(int)std::min<long>(ceil_div(nc, 4), 148L * 8), 128, xs, st>>>(
+  k_mps_locals<ND><<<(int)std::min<long>(ceil_div(nc, warps), 148L * 8), thr, xs, st>>>(
       tv, H.dlv.p, nl, leaf, nc, E, mpole, nd, d0, zk, mp, lo, local, thresh, maxnt);
   B2_LAUNCH_CHECK();
 }
@@ -1446,7 +1788,9 @@ int helm_nterms(double bsize, double zkr, double zki, double eps, int* ier) {
   double2 zb = make_double2(zkr * bsize, zki * bsize);
   double rscale = 1.0;
   if (std::hypot(zb.x, zb.y) < pi2) rscale = std::hypot(zb.x, zb.y);
-  const int NT = 400;
+  // the criterion is met near order 1.5 |zk bsize| + (digits); the
+  // reference scans up to 50000 orders
+  const int NT = (int)std::min(50000.0, std::max(400.0, 2.0 * std::hypot(zb.x, zb.y) + 200.0));
   std::vector<double2> hf(NT + 1), jf(NT + 1);
   helm::hscaled(NT, make_double2(1.5 * zb.x, 1.5 * zb.y), rscale, hf.data());
   double c = std::sqrt(2.0) / 2.0;
@@ -1502,11 +1846,7 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
   const double zkabs = std::hypot(a.zkr, a.zki);
   HelmLevels H(st);
   if (int r = helm_levels(T, a.zkr, a.zki, a.eps, H, st)) return r;
-  const std::vector<HLev>& hl = H.hl;
-  const int maxp = H.maxp;
   const long off = H.off;
-  DBuf<HLev>& dlv = H.dlv;
-  DBuf<double2>& tabs = H.tabs;
   DBuf<double>& dbs = H.dbs;
   // sorted inputs
   DBuf<double2> xs(st), xt(st), qs(st), ds(st);
@@ -1548,9 +1888,10 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
     B2_LAUNCH_CHECK();
   }
   int chunk = nd >= 4 ? 4 : (nd >= 2 ? 2 : 1);
-  DBuf<double2> mp(st), lo(st);
+  DBuf<double2> mp(st), lo(st), sig(st);
   mp.alloc((size_t)off * chunk, st);
   lo.alloc((size_t)off * chunk, st);
+  if (H.sig_total > 0) sig.alloc((size_t)H.sig_total * chunk, st);
   cudaEvent_t ev[8];
   for (int i = 0; i < 8; i++) B2_CHECK(cudaEventCreate(&ev[i]));
   double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -1560,9 +1901,9 @@ int helm_fmm_device(const HelmArgs& a, cudaStream_t st) {
     HDens D{fc ? qs.p : nullptr, fd ? ds.p : nullptr, fd ? vs.p : nullptr, nd, d0};
     B2_CHECK(cudaMemsetAsync(lo.p, 0, sizeof(double2) * (size_t)off * ND, st));
     switch (ND) {
-      case 4: helm_chunk<4>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
-      case 2: helm_chunk<2>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
-      default: helm_chunk<1>(tv, T, a, D, dlv.p, hl, maxp, tabs.p, xs.p, xt.p, mp.p, lo.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
+      case 4: helm_chunk<4>(tv, T, a, D, H, xs.p, xt.p, mp.p, lo.p, sig.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
+      case 2: helm_chunk<2>(tv, T, a, D, H, xs.p, xt.p, mp.p, lo.p, sig.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
+      default: helm_chunk<1>(tv, T, a, D, H, xs.p, xt.p, mp.p, lo.p, sig.p, ps.p, gs.p, hs.p, pt.p, gt.p, ht.p, thresh, leafs.p, leaft.p, ns, nt, st, ev); break;
     }
     if (a.timeinfo) {
       B2_CHECK(cudaEventSynchronize(ev[6]));
@@ -1611,7 +1952,11 @@ int helm_mps_device(int nd, double eps, double zkr, double zki, long nc, const d
   build_device_tree(T, centers, nc, nullptr, 0, 0, 1, NLMAX, st);
   HelmLevels H(st);
   if (int r = helm_levels(T, zkr, zki, eps, H, st)) return r;
-  const int maxnt = 2 * std::max(H.maxp, max_mterms);
+  const int maxnt = 2 * std::max(H.maxp_all, max_mterms);
+  // warps per block of the per-expansion kernels (their translation scratch)
+  int warps = 4;
+  while (warps > 1 && mps_smem(maxnt, warps) > 200 * 1024) warps /= 2;
+  if (mps_smem(maxnt, warps) > 200 * 1024) return IER_NTERMS;
   DBuf<double2> ec(st);
   DBuf<double> ers(st);
   DBuf<int> em(st), leaf(st);
@@ -1635,18 +1980,19 @@ int helm_mps_device(int nd, double eps, double zkr, double zki, long nc, const d
   MpsExp E{ec.p, ers.p, em.p, eoff.p};
   const double2 zk = make_double2(zkr, zki);
   const int chunk = nd >= 4 ? 4 : (nd >= 2 ? 2 : 1);
-  DBuf<double2> mp(st), lo(st);
+  DBuf<double2> mp(st), lo(st), sig(st);
   mp.alloc((size_t)H.off * chunk, st);
   lo.alloc((size_t)H.off * chunk, st);
+  if (H.sig_total > 0) sig.alloc((size_t)H.sig_total * chunk, st);
   auto* mpc = reinterpret_cast<const double2*>(mpole);
   auto* loc = reinterpret_cast<double2*>(local);
   for (int d0 = 0; d0 < nd;) {
     const int left = nd - d0;
     const int ND = left >= 4 ? 4 : (left >= 2 ? 2 : 1);
     switch (ND) {
-      case 4: mps_chunk<4>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, leaf.p, nc, loc, thresh, maxnt, st); break;
-      case 2: mps_chunk<2>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, leaf.p, nc, loc, thresh, maxnt, st); break;
-      default: mps_chunk<1>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, leaf.p, nc, loc, thresh, maxnt, st); break;
+      case 4: mps_chunk<4>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, sig.p, leaf.p, nc, loc, thresh, maxnt, warps, st); break;
+      case 2: mps_chunk<2>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, sig.p, leaf.p, nc, loc, thresh, maxnt, warps, st); break;
+      default: mps_chunk<1>(tv, T, H, E, mpc, nd, d0, zk, mp.p, lo.p, sig.p, leaf.p, nc, loc, thresh, maxnt, warps, st); break;
     }
     d0 += ND;
   }

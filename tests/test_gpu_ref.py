@@ -194,12 +194,14 @@ def test_host_entry_points_vs_reference(gpu, ref):
         assert rel_l2(a.transpose(2, 1, 0), r[k]) < TOL_HELM, k
 
 
-@pytest.mark.parametrize("zk", [10.0, 3 + 0.5j])
+@pytest.mark.parametrize("zk", [10.0, 3 + 0.5j, 500.0])
 @pytest.mark.parametrize("pg", [1, 2, 3])
 def test_hfmm_reference_inputs(gpu, ref, zk, pg):
     """test/helmholtz/test_hfmm2d.f:19-51 inputs (1000 sources, 1001 targets),
     eps 0.51e-8, through the reference-named host entry b2fmm_hfmm2d (the
-    python front end, like fmm2dpy's, stops at pg 2)."""
+    python front end, like fmm2dpy's, stops at pg 2).  zk = 500 is
+    test/helmholtz/test_hfmm2d_hf.f: boxes of 40 and 20 wavelengths at levels
+    1 and 2 take the wideband (signature) translations."""
     from fmm2d_b200 import _lib
     src, trg, q, d, v = hk_inputs(ref, 1000, 1001)
     n, nt = src.shape[1], trg.shape[1]
@@ -295,3 +297,31 @@ def test_batch_graph_vs_reference(gpu, ref, precision):
     g.close()
     for p in plans:
         p.close()
+
+
+@pytest.mark.parametrize("case", ["uniform", "curve"])
+def test_hfmm_wideband_vs_reference(gpu, ref, case):
+    """Larger wideband problems: wideband and tabulated levels in one tree,
+    nd = 2, sources and targets, pg = pgt = 2."""
+    rng = np.random.default_rng(60)
+    if case == "uniform":
+        ns, nt, zk = 40000, 10000, 600.0
+        src = rng.uniform(0, 1, (2, ns))
+    else:
+        ns, nt, zk = 60000, 10000, 150.0 + 2.0j
+        th = rng.uniform(0, 2 * np.pi, ns)
+        r0 = 0.3 * (1 + 0.2 * np.cos(5 * th))
+        src = np.stack([0.5 + r0 * np.cos(th), 0.5 + r0 * np.sin(th)])
+    trg = rng.uniform(0, 1, (2, nt))
+    nd = 2
+    q = rng.normal(size=(nd, ns)) + 1j * rng.normal(size=(nd, ns))
+    d = rng.normal(size=(nd, ns)) + 1j * rng.normal(size=(nd, ns))
+    ph = rng.uniform(0, 2 * np.pi, (nd, ns))
+    v = np.stack([np.cos(ph), np.sin(ph)], axis=1)
+    out = fmm.hfmm2d(eps=1e-9, zk=zk, sources=src, charges=q, dipstr=d, dipvec=v, targets=trg,
+                     pg=2, pgt=2, nd=nd)
+    assert out.ier == 0
+    r = ref.hfmm2d(1e-9, zk, src, charges=q, dipstr=d, dipvec=v, targets=trg, ifpgh=2,
+                   ifpghtarg=2, nd=nd)
+    for k in ("pot", "grad", "pottarg", "gradtarg"):
+        assert rel_l2(getattr(out, k), r[k]) < TOL_HELM, k
