@@ -47,6 +47,17 @@ SIGNATURES = {
     "b2fmm_hfmm2d": _HELM_HOST + [c_int] + _PGH + [P],
     "b2fmm_hfmm2d_ndiv": _HELM_HOST + [c_int] + _PGH + [c_int, c_int, c_int, P, P],
     "b2fmm_hfmm2d_dev": _HELM_HOST + _PGH + [P, P, P, P],
+    "b2fmm_bhfmm2d": [c_int, c_double, c_int64, P, c_int, P, c_int, P, c_int, c_int, P, P, P,
+                      c_int64, P, c_int, P, P, P, P],
+    "b2fmm_bhfmm2d_dev": [c_int, c_double, c_int64, P, c_int, P, c_int, P, c_int, P, P, c_int64,
+                          P, c_int, P, P, P, P],
+    "b2fmm_bh2ddir_dev": [c_int, c_int64, P, P, P, c_int64, P, c_int, P, P, c_double, P, P],
+    "b2fmm_stfmm2d": [c_int, c_double, c_int64, P, c_int, P, c_int, P, P, c_int, P, P, P, c_int64,
+                      P, c_int, P, P, P, P],
+    "b2fmm_stfmm2d_dev": [c_int, c_double, c_int64, P, c_int, P, c_int, P, P, c_int, P, P, P,
+                          c_int64, P, c_int, P, P, P, P, P],
+    "b2fmm_st2ddir_dev": [c_int, c_int64, P, c_int, P, c_int, P, P, c_int64, P, c_int, P, P, P,
+                          c_double, P, P],
     "b2fmm_hfmm2d_mps": [c_int, c_double, c_double, c_double, c_int64, P, P, P, c_int64, P, P, P,
                          P],
     "b2fmm_h2ddir_dev": [c_int, c_double, c_double, c_int64, P, P, P, P, c_int64, P, c_int, P,

@@ -13,7 +13,16 @@ eps, and every training run is checked against the FP64 direct sum.
 
 Usage on a GPU:
     python -m fmm2d_b200.costmodel train  [--out fmm2d_b200/costmodel_weights.json]
+    python -m fmm2d_b200.costmodel train --from-samples   # refit on the committed samples
     python -m fmm2d_b200.costmodel evaluate
+
+``train`` times every candidate ndiv on the training problems and writes the
+samples to fmm2d_b200/costmodel_samples.json (committed, so the fit is
+reproducible without re-timing) together with the weights.  Beside the
+network it records the best single constant ndiv per eps on the same
+training timings (the smallest total time over the training problems): the
+third arm of ``evaluate``, which separates what the network learned about
+the point distribution from "larger leaves than the table".
 """
 import argparse
 import ctypes as C
@@ -30,6 +39,7 @@ NIN, H1, H2 = 9, 32, 32
 CANDIDATES = [4, 6, 8, 11, 15, 20, 28, 40, 56, 80, 112]
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "costmodel_weights.json")
+SAMPLES = os.path.join(HERE, "costmodel_samples.json")
 
 
 def table_ndiv(eps):
@@ -87,10 +97,16 @@ def model_inputs(feat, cands=CANDIDATES):
 # the model
 # ---------------------------------------------------------------------------
 class CostModel:
-    def __init__(self, params, ymean=0.0, ystd=1.0):
+    def __init__(self, params, ymean=0.0, ystd=1.0, best_constant=None):
         self.params = np.asarray(params, dtype=np.float32)
         self.ymean, self.ystd = float(ymean), float(ystd)
+        self.best_constant = dict(best_constant or {})  # eps (str) -> ndiv
         assert self.params.size == _lib.lib().b2fmm_mlp_param_count(NIN, H1, H2)
+
+    def constant_ndiv(self, eps):
+        """The best constant ndiv of the training timings for eps (the table's
+        value when eps was not in the training set)."""
+        return self.best_constant.get(repr(float(eps)), table_ndiv(eps))
 
     @staticmethod
     def init(seed=0):
@@ -122,7 +138,7 @@ class CostModel:
 
     def save(self, path=WEIGHTS):
         json.dump({"nin": NIN, "h1": H1, "h2": H2, "candidates": CANDIDATES,
-                   "ymean": self.ymean, "ystd": self.ystd,
+                   "ymean": self.ymean, "ystd": self.ystd, "best_constant": self.best_constant,
                    "params": [float(v) for v in self.params]}, open(path, "w"))
 
     @staticmethod
@@ -132,7 +148,7 @@ class CostModel:
         d = json.load(open(path))
         if (d["nin"], d["h1"], d["h2"]) != (NIN, H1, H2):
             return None
-        return CostModel(d["params"], d["ymean"], d["ystd"])
+        return CostModel(d["params"], d["ymean"], d["ystd"], d.get("best_constant"))
 
 
 def train(X, y, steps=3000, lr=3e-3, seed=0):
@@ -263,6 +279,29 @@ def collect(problems, cands=CANDIDATES, reps=2, check=True):
     return np.array(X, dtype=np.float32), np.array(y, dtype=np.float64), rec
 
 
+def best_constant(rec):
+    """Per eps, the candidate with the smallest total time over the problems
+    timed in rec (every problem is timed at every candidate)."""
+    out = {}
+    for eps in sorted({r["eps"] for r in rec}):
+        tot = {}
+        for r in rec:
+            if r["eps"] == eps:
+                tot[r["ndiv"]] = tot.get(r["ndiv"], 0.0) + r["ms"]
+        out[repr(float(eps))] = int(min(tot, key=tot.get))
+    return out
+
+
+def save_samples(X, y, rec, path=SAMPLES):
+    json.dump({"nin": NIN, "candidates": CANDIDATES, "X": np.asarray(X).tolist(),
+               "y": np.asarray(y).tolist(), "runs": rec}, open(path, "w"))
+
+
+def load_samples(path=SAMPLES):
+    d = json.load(open(path))
+    return np.array(d["X"], dtype=np.float32), np.array(d["y"], dtype=np.float64), d["runs"]
+
+
 def sweep_problems(count, seed0, nmin=1e4, nmax=8e6):
     """count problems: N log-uniform, distribution and eps cycling."""
     rng = np.random.default_rng(seed0)
@@ -287,19 +326,26 @@ def evaluate(model, problems):
         nd_m = model.choose_ndiv(features_from_hist(histogram(ts), eps))
         choose_ms = (time.perf_counter() - t0) * 1e3
         nd_t = table_ndiv(eps)
+        nd_c = model.constant_ndiv(eps)
         ms_t, pt, gt = time_rfmm(ts, tq, eps, nd_t)
         err_t = direct_error(ts, tq, pt, gt)
         ms_m, pm, gm = time_rfmm(ts, tq, eps, nd_m)
         err_m = direct_error(ts, tq, pm, gm)
+        ms_c, pc, gc = time_rfmm(ts, tq, eps, nd_c)
+        err_c = direct_error(ts, tq, pc, gc)
         rows.append({"kind": kind, "n": n, "eps": eps, "ndiv_table": nd_t, "ndiv_mlp": nd_m,
-                     "ms_table": ms_t, "ms_mlp": ms_m, "err_table": err_t, "err_mlp": err_m,
-                     "choose_ms": choose_ms})
+                     "ndiv_constant": nd_c, "ms_table": ms_t, "ms_mlp": ms_m,
+                     "ms_constant": ms_c, "err_table": err_t, "err_mlp": err_m,
+                     "err_constant": err_c, "choose_ms": choose_ms})
     tt = sum(r["ms_table"] for r in rows)
     tm = sum(r["ms_mlp"] for r in rows)
+    tc = sum(r["ms_constant"] for r in rows)
     return {"problems": len(rows), "total_ms_table": tt, "total_ms_mlp": tm,
-            "speedup": tt / tm,
+            "total_ms_constant": tc, "speedup": tt / tm, "speedup_vs_constant": tc / tm,
+            "best_constant": model.best_constant,
             "max_err_over_eps_table": max(r["err_table"] / r["eps"] for r in rows),
             "max_err_over_eps_mlp": max(r["err_mlp"] / r["eps"] for r in rows),
+            "max_err_over_eps_constant": max(r["err_constant"] / r["eps"] for r in rows),
             "rows": rows}
 
 
@@ -309,16 +355,23 @@ def main():
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--train-problems", type=int, default=60)
     ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--from-samples", action="store_true",
+                    help="refit on fmm2d_b200/costmodel_samples.json instead of timing")
     args = ap.parse_args()
     if args.cmd == "train":
-        probs = sweep_problems(args.train_problems, seed0=1000, nmax=2e6)
-        X, y, rec = collect(probs)
-        bad = [r for r in rec if r["err"] > r["eps"]]
+        if args.from_samples:
+            X, y, rec = load_samples()
+        else:
+            probs = sweep_problems(args.train_problems, seed0=1000, nmax=2e6)
+            X, y, rec = collect(probs)
+            save_samples(X, y, rec)
+        bad = [r for r in rec if r["err"] is not None and r["err"] > r["eps"]]
         m, hist = train(X, y, steps=args.steps)
+        m.best_constant = best_constant(rec)
         m.save(args.out)
         print(json.dumps({"samples": len(y), "loss_first": float(hist[0]),
                           "loss_last": float(hist[-1]), "runs_over_eps": len(bad),
-                          "weights": args.out}))
+                          "best_constant": m.best_constant, "weights": args.out}))
     else:
         m = CostModel.load(args.out)
         print(json.dumps({k: v for k, v in evaluate(m, sweep_problems(40, seed0=5000)).items()

@@ -4,6 +4,7 @@
 
 #include "../../include/fmm2d_b200.h"
 #include "batch.cuh"
+#include "biharmonic.cuh"
 #include "direct.cuh"
 #include "helm_special.cuh"
 #include "helmholtz.cuh"
@@ -514,6 +515,195 @@ void b2fmm_hfmm2d_dev(int nd, double eps, double zk_re, double zk_im, int64_t ns
                                       ifdipole, dipstr, dipvec, ifpgh, pot, grad, hess, nt, targ,
                                       ifpghtarg, pottarg, gradtarg, hesstarg, opts, timeinfo),
                            (cudaStream_t)stream);
+  });
+}
+
+namespace {
+// Host arrays in, device copies, a device call, results back: inputs (host
+// pointer, doubles) and outputs (host pointer, doubles); null entries skip.
+struct HostIO {
+  cudaStream_t st = cudaStreamPerThread;
+  std::vector<DBuf<double>*> bufs;
+  std::vector<std::pair<double*, const double*>> outs;  // host, device
+  std::vector<size_t> out_n;
+  ~HostIO() {
+    for (auto* b : bufs) delete b;
+  }
+  const double* in(const double* h, size_t n) {
+    if (!h || n == 0) return nullptr;
+    auto* b = new DBuf<double>(st);
+    bufs.push_back(b);
+    b->alloc(n, st);
+    B2_CHECK(cudaMemcpyAsync(b->p, h, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    return b->p;
+  }
+  double* out(double* h, size_t n) {
+    if (!h || n == 0) return nullptr;
+    auto* b = new DBuf<double>(st);
+    bufs.push_back(b);
+    b->alloc(n, st);
+    outs.push_back({h, b->p});
+    out_n.push_back(n);
+    return b->p;
+  }
+  void finish() {
+    for (size_t k = 0; k < outs.size(); k++)
+      B2_CHECK(cudaMemcpyAsync(outs[k].first, outs[k].second, out_n[k] * sizeof(double),
+                               cudaMemcpyDeviceToHost, st));
+    B2_CHECK(cudaStreamSynchronize(st));
+  }
+};
+
+BhArgs bh_args(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+               const double* charge, int ifdipole, const double* dip, int ifpgh, double* pot,
+               double* grad, int64_t nt, const double* targ, int ifpghtarg, double* pottarg,
+               double* gradtarg) {
+  BhArgs b;
+  b.nd = nd;
+  b.eps = eps;
+  b.ns = ns;
+  b.src = sources;
+  b.charge = ifcharge == 1 ? charge : nullptr;
+  b.dip = ifdipole == 1 ? dip : nullptr;
+  b.ifpgh = ifpgh;
+  b.pot = pot;
+  b.grad = grad;
+  b.nt = nt;
+  b.trg = targ;
+  b.ifpghtarg = ifpghtarg;
+  b.pottarg = pottarg;
+  b.gradtarg = gradtarg;
+  return b;
+}
+
+StArgs st_args(int nd, double eps, int64_t ns, const double* sources, int ifstoklet,
+               const double* stoklet, int ifstrslet, const double* strslet, const double* strsvec,
+               int ifppreg, double* pot, double* pre, double* grad, int64_t nt, const double* targ,
+               int ifppregtarg, double* pottarg, double* pretarg, double* gradtarg) {
+  StArgs a;
+  a.nd = nd;
+  a.eps = eps;
+  a.ns = ns;
+  a.src = sources;
+  a.stoklet = ifstoklet == 1 ? stoklet : nullptr;
+  a.strslet = ifstrslet == 1 ? strslet : nullptr;
+  a.strsvec = ifstrslet == 1 ? strsvec : nullptr;
+  a.ifppreg = ifppreg;
+  a.pot = pot;
+  a.pre = pre;
+  a.grad = grad;
+  a.nt = nt;
+  a.trg = targ;
+  a.ifppregtarg = ifppregtarg;
+  a.pottarg = pottarg;
+  a.pretarg = pretarg;
+  a.gradtarg = gradtarg;
+  return a;
+}
+}  // namespace
+
+void b2fmm_bhfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dip, int ifpgh,
+                       double* pot, double* grad, int64_t nt, const double* targ, int ifpghtarg,
+                       double* pottarg, double* gradtarg, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return bh_device(bh_args(nd, eps, ns, sources, ifcharge, charge, ifdipole, dip, ifpgh, pot,
+                             grad, nt, targ, ifpghtarg, pottarg, gradtarg),
+                     (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_bh2ddir_dev(int nd, int64_t ns, const double* sources, const double* charge,
+                       const double* dip, int64_t nt, const double* targ, int ifpgh, double* pot,
+                       double* grad, double thresh, void* stream, int* ier) {
+  guarded(ier, [&] {
+    BhArgs b = bh_args(nd, 0.0, ns, sources, charge ? 1 : 0, charge, dip ? 1 : 0, dip, 0, nullptr,
+                       nullptr, nt, targ, ifpgh, pot, grad);
+    b.direct = true;
+    b.thresh = thresh;
+    return bh_device(b, (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_bhfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                   const double* charge, int ifdipole, const double* dip, int iper, int ifpgh,
+                   double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                   int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg, int* ier) {
+  (void)iper;
+  (void)hess;
+  (void)hesstarg;
+  guarded(ier, [&] {
+    if (nd < 1 || ns < 0 || nt < 0) return (int)IER_BADARG;
+    HostIO io;
+    const size_t n2 = 2 * (size_t)nd;  // doubles per complex density
+    const int ifs = std::min(ifpgh, 2), ift = std::min(ifpghtarg, 2);
+    const long ntt = ift > 0 ? nt : 0;
+    BhArgs b = bh_args(
+        nd, eps, ns, io.in(sources, 2 * (size_t)ns), ifcharge,
+        ifcharge == 1 ? io.in(charge, n2 * 2 * ns) : nullptr, ifdipole,
+        ifdipole == 1 ? io.in(dip, n2 * 3 * ns) : nullptr, ifs,
+        ifs >= 1 ? io.out(pot, n2 * ns) : nullptr, ifs >= 2 ? io.out(grad, n2 * 3 * ns) : nullptr,
+        ntt, io.in(targ, 2 * (size_t)ntt), ift, ift >= 1 ? io.out(pottarg, n2 * ntt) : nullptr,
+        ift >= 2 ? io.out(gradtarg, n2 * 3 * ntt) : nullptr);
+    int r = bh_device(b, io.st);
+    if (r != IER_OK) return r;
+    io.finish();
+    return (int)IER_OK;
+  });
+}
+
+void b2fmm_stfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifstoklet,
+                       const double* stoklet, int ifstrslet, const double* strslet,
+                       const double* strsvec, int ifppreg, double* pot, double* pre, double* grad,
+                       int64_t nt, const double* targ, int ifppregtarg, double* pottarg,
+                       double* pretarg, double* gradtarg, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return stokes_device(st_args(nd, eps, ns, sources, ifstoklet, stoklet, ifstrslet, strslet,
+                                 strsvec, ifppreg, pot, pre, grad, nt, targ, ifppregtarg, pottarg,
+                                 pretarg, gradtarg),
+                         (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_st2ddir_dev(int nd, int64_t ns, const double* sources, int ifstoklet,
+                       const double* stoklet, int ifstrslet, const double* strslet,
+                       const double* strsvec, int64_t nt, const double* targ, int ifppreg,
+                       double* pot, double* pre, double* grad, double thresh, void* stream,
+                       int* ier) {
+  guarded(ier, [&] {
+    StArgs a = st_args(nd, 0.0, ns, sources, ifstoklet, stoklet, ifstrslet, strslet, strsvec, 0,
+                       nullptr, nullptr, nullptr, nt, targ, ifppreg, pot, pre, grad);
+    a.direct = true;
+    a.thresh = thresh;
+    return stokes_device(a, (cudaStream_t)stream);
+  });
+}
+
+void b2fmm_stfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifstoklet,
+                   const double* stoklet, int ifstrslet, const double* strslet,
+                   const double* strsvec, int ifppreg, double* pot, double* pre, double* grad,
+                   int64_t nt, const double* targ, int ifppregtarg, double* pottarg,
+                   double* pretarg, double* gradtarg, int* ier) {
+  guarded(ier, [&] {
+    if (nd < 1 || ns < 0 || nt < 0) return (int)IER_BADARG;
+    HostIO io;
+    const size_t nn = (size_t)nd;
+    const int ifs = std::min(ifppreg, 3), ift = std::min(ifppregtarg, 3);
+    const long ntt = ift > 0 ? nt : 0;
+    StArgs a = st_args(
+        nd, eps, ns, io.in(sources, 2 * (size_t)ns), ifstoklet,
+        ifstoklet == 1 ? io.in(stoklet, nn * 2 * ns) : nullptr, ifstrslet,
+        ifstrslet == 1 ? io.in(strslet, nn * 2 * ns) : nullptr,
+        ifstrslet == 1 ? io.in(strsvec, nn * 2 * ns) : nullptr, ifs,
+        ifs >= 1 ? io.out(pot, nn * 2 * ns) : nullptr, ifs >= 2 ? io.out(pre, nn * ns) : nullptr,
+        ifs >= 3 ? io.out(grad, nn * 4 * ns) : nullptr, ntt, io.in(targ, 2 * (size_t)ntt), ift,
+        ift >= 1 ? io.out(pottarg, nn * 2 * ntt) : nullptr,
+        ift >= 2 ? io.out(pretarg, nn * ntt) : nullptr,
+        ift >= 3 ? io.out(gradtarg, nn * 4 * ntt) : nullptr);
+    int r = stokes_device(a, io.st);
+    if (r != IER_OK) return r;
+    io.finish();
+    return (int)IER_OK;
   });
 }
 

@@ -150,6 +150,26 @@ void hfmm2d_mps_(const int* nd, const double* eps, const double* zk, const int* 
                    impole, local, ier);
 }
 
+void bhfmm2d_(const int* nd, const double* eps, const int* ns, const double* sources,
+              const int* ifcharge, const double* charge, const int* ifdipole, const double* dip,
+              const int* iper, const int* ifpgh, double* pot, double* grad, double* hess,
+              const int* nt, const double* targ, const int* ifpghtarg, double* pottarg,
+              double* gradtarg, double* hesstarg, int* ier) {
+  b2fmm_bhfmm2d(*nd, *eps, *ns, sources, *ifcharge, charge, *ifdipole, dip, *iper, *ifpgh, pot,
+                grad, hess, *nt, targ, *ifpghtarg, pottarg, gradtarg, hesstarg, ier);
+}
+
+void stfmm2d_(const int* nd, const double* eps, const int* nsource, const double* source,
+              const int* ifstoklet, const double* stoklet, const int* ifstrslet,
+              const double* strslet, const double* strsvec, const int* ifppreg, double* pot,
+              double* pre, double* grad, const int* ntarg, const double* targ,
+              const int* ifppregtarg, double* pottarg, double* pretarg, double* gradtarg,
+              int* ier) {
+  b2fmm_stfmm2d(*nd, *eps, *nsource, source, *ifstoklet, stoklet, *ifstrslet, strslet, strsvec,
+                *ifppreg, pot, pre, grad, *ntarg, targ, *ifppregtarg, pottarg, pretarg, gradtarg,
+                ier);
+}
+
 /* ------------------------------------------------------------ flag wrappers */
 
 #define ZK_c NULL

@@ -1,6 +1,7 @@
-// Helmholtz FMM on B200 (FP64): the low-frequency path of hfmm2dmain
-// (src/helmholtz/hfmm2d.f:456-1580) with the operators of
-// src/helmholtz/helmrouts2d.f and the near field of helmkernels2d.f.
+// Helmholtz FMM on B200 (FP64): hfmm2dmain (src/helmholtz/hfmm2d.f:456-1580)
+// with the operators of src/helmholtz/helmrouts2d.f, the wideband
+// translations of wideband2d.f and the near field of helmkernels2d.f; and
+// the FMM over multipole sources hfmm2d_mps (hfmm2d_mps.f).
 //
 // Expansions have 2p_l+1 coefficients (n = -p_l..p_l) per density, with a
 // per-level order p_l (h2dterms) and scale rs_l = min(|zk bs_l / 2pi|, 1);

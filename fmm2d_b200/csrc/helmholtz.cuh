@@ -1,4 +1,4 @@
-// Helmholtz FMM engine (the low-frequency path of src/helmholtz/hfmm2d.f).
+// Helmholtz FMM engine (src/helmholtz/hfmm2d.f, wideband levels included).
 #pragma once
 #include "common.cuh"
 
@@ -24,8 +24,8 @@ struct HelmArgs {
   double* timeinfo = nullptr;
 };
 
-// ier: 0 ok, 13 expansion order too large, 20 the problem needs the
-// high-frequency (box larger than 16 wavelengths) translations.
+// ier: 0 ok, 13 expansion order too large (or one the kernels do not
+// support: above 63 with a scale below 1, a signature above 7000 points).
 int helm_fmm_device(const HelmArgs& a, cudaStream_t st);
 
 // All-pairs Helmholtz sums (h2d_direct*, src/helmholtz/helmkernels2d.f).
@@ -40,8 +40,7 @@ int helm_direct_device(int nd, double zkr, double zki, long ns, const double* sr
 // impole (nc, 1-based offsets into the complex arrays as in the
 // reference), mpole and local complex (ntot); expansion i is the (nd,
 // -m..m) block at impole(i), m = mterms(i) <= max_mterms.  ier 13 when
-// max_mterms exceeds the supported order (63), 20 in the high-frequency
-// regime (as helm_fmm_device).
+// max_mterms exceeds the supported order (63).
 int helm_mps_device(int nd, double eps, double zkr, double zki, long nc, const double* centers,
                     const double* rscales, const int* mterms, const int* impole, long ntot,
                     const double* mpole, double* local, int max_mterms, cudaStream_t st);

@@ -495,6 +495,226 @@ def h2ddir(*, zk, sources, targets, charges=None, dipstr=None, dipvec=None, pgt=
 # ---------------------------------------------------------------------------
 # relative l2 error of the first ntest values (fmm2d.py:2017-2139)
 # ---------------------------------------------------------------------------
+def _fortran_dev(a, shape, dtype):
+    """A user array of the reference's shape (nd, k, n) as a CUDA tensor in
+    column-major (Fortran) element order."""
+    import torch
+    t = _to_dev(a, dtype).reshape(shape)
+    return t.permute(*reversed(range(len(shape)))).contiguous()
+
+
+def _user(t, torch_mode, squeeze):
+    """Device output in column-major order (n, ..., nd) back to the
+    reference's (nd, ..., n) shape (without nd when squeeze)."""
+    if t is None:
+        return None
+    r = t.permute(*reversed(range(t.dim())))
+    if squeeze:
+        r = r[0]
+    return r if torch_mode else r.cpu().numpy()
+
+
+def _bh_check(sources, charges, dipoles, nd, ns):
+    """Shape assertions of the reference's bhfmm2d / bh2ddir front ends."""
+    if charges is not None:
+        if nd == 1 and ns > 1:
+            assert charges.shape[0] == 2 and charges.shape[1] == ns, \
+                "Charges must be of shape [2, number of source]"
+        if nd == 1 and ns == 1:
+            assert charges.shape[0] == 2, "Charges must of shape [2, number of sources]"
+        if nd > 1:
+            assert charges.shape[0] == nd and charges.shape[1] == 2 and charges.shape[2] == ns, \
+                "Charges must be of shape [nd,2,ns] where nd is number of densities, and ns " \
+                "is number of sources"
+    if dipoles is not None:
+        if nd == 1 and ns > 1:
+            assert dipoles.shape[0] == 3 and dipoles.shape[1] == ns, \
+                "Dipole must of shape [3, number of sources]"
+        if nd == 1 and ns == 1:
+            assert dipoles.shape[0] == 3, "Dipole must of shape [3, number of sources]"
+        if nd > 1:
+            assert dipoles.shape[0] == nd and dipoles.shape[1] == 3 and dipoles.shape[2] == ns, \
+                "Dipole must of shape [nd,2, number of sources]"
+
+
+def _bh_run(eps, sources, charges, dipoles, targets, pg, pgt, nd, direct=False, thresh=1e-16):
+    import torch
+    torch_mode = _is_torch(sources)
+    ns = _ns_of(sources)
+    s = _fortran_dev(sources, (2, ns), torch.float64)
+    q = None if charges is None else _fortran_dev(charges, (nd, 2, ns), torch.complex128)
+    d = None if dipoles is None else _fortran_dev(dipoles, (nd, 3, ns), torch.complex128)
+    nt = 0
+    t = None
+    if targets is not None and pgt > 0:
+        nt = _ns_of(targets)
+        t = _fortran_dev(targets, (2, nt), torch.float64)
+    z = lambda *sh: torch.zeros(sh, dtype=torch.complex128, device="cuda")
+    pot = z(ns, nd) if pg >= 1 else None
+    grad = z(ns, 3, nd) if pg >= 2 else None
+    pott = z(nt, nd) if pgt >= 1 and nt else None
+    gradt = z(nt, 3, nd) if pgt >= 2 and nt else None
+    ier = C.c_int(0)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    L = _lib.lib()
+    if direct:
+        L.b2fmm_bh2ddir_dev(nd, ns, _ptr(s), _ptr(q), _ptr(d), nt, _ptr(t), pgt, _ptr(pott),
+                            _ptr(gradt), C.c_double(thresh), stream, C.byref(ier))
+    else:
+        L.b2fmm_bhfmm2d_dev(nd, C.c_double(eps), ns, _ptr(s), int(q is not None), _ptr(q),
+                            int(d is not None), _ptr(d), pg, _ptr(pot), _ptr(grad), nt, _ptr(t),
+                            pgt, _ptr(pott), _ptr(gradt), stream, C.byref(ier))
+    out = Output()
+    out.ier = ier.value
+    sq = nd == 1
+    out.pot, out.grad = _user(pot, torch_mode, sq), _user(grad, torch_mode, sq)
+    out.pottarg, out.gradtarg = _user(pott, torch_mode, sq), _user(gradt, torch_mode, sq)
+    return out
+
+
+def bhfmm2d(*, eps, sources, charges=None, dipoles=None, targets=None, pg=0, pgt=0, nd=1):
+    """Biharmonic FMM (python/fmm2dpy/fmm2d.py bhfmm2d, src/biharmonic/bhfmm2d.f):
+    u(x) = sum 2 c1 log|x-x_j| + c2 (x-x_j)/conj(x-x_j) + d1/(x-x_j)
+    + d3/conj(x-x_j) + d2 (x-x_j)/conj(x-x_j)^2; grad the three derivatives
+    (d/dz, its conj(z) part, d/dconj(z)).  charges (nd,2,n), dipoles (nd,3,n)."""
+    out = Output()
+    assert sources.shape[0] == 2, "The first dimension of sources must be 2"
+    ns = _ns_of(sources)
+    if pg == 0 and pgt == 0:
+        print("Nothing to compute, set either pg or pgt to non-zero")
+        return out
+    _bh_check(sources, charges, dipoles, nd, ns)
+    if targets is not None:
+        assert targets.shape[0] == 2, "The first dimension of targets must be 2"
+    return _bh_run(eps, sources, charges, dipoles, targets, pg, pgt, nd)
+
+
+def bh2ddir(*, sources, targets, charges=None, dipoles=None, pgt=0, nd=1, thresh=1e-16):
+    """All-pairs biharmonic sums at the targets (fmm2d.py bh2ddir)."""
+    out = Output()
+    assert sources.shape[0] == 2, "The first dimension of sources must be 2"
+    ns = _ns_of(sources)
+    if pgt == 0:
+        print("Nothing to compute, set either pg or pgt to non-zero")
+        return out
+    _bh_check(sources, charges, dipoles, nd, ns)
+    assert targets.shape[0] == 2, "The first dimension of targets must be 2"
+    return _bh_run(0.0, sources, charges, dipoles, targets, 0, pgt, nd, direct=True,
+                   thresh=thresh)
+
+
+def _st_check(stoklet, strslet, strsvec, nd, ns):
+    if stoklet is not None:
+        if nd == 1 and ns > 1:
+            assert stoklet.shape[0] == 2 and stoklet.shape[1] == ns, \
+                "stoklet vectors must be of shape [2,number of sources]"
+        if nd == 1 and ns == 1:
+            assert stoklet.shape[0] == 2, "stoklet vectors must be of shape [2,number of sources]"
+        if nd > 1:
+            assert stoklet.shape[0] == nd and stoklet.shape[1] == 2 and stoklet.shape[2] == ns, \
+                "stoklet vectors must be of shape [nd,2,ns] where nd is number of densities, " \
+                "and ns is number of sources"
+    if strslet is not None and strsvec is not None:
+        if nd == 1 and ns > 1:
+            assert strslet.shape[0] == 2 and strslet.shape[1] == ns, \
+                "strslet vectors must be of shape [2,number of sources]"
+            assert strsvec.shape[0] == 2 and strsvec.shape[1] == ns, \
+                "strsvec vectors must be of shape [2,number of sources]"
+        if nd == 1 and ns == 1:
+            assert strslet.shape[0] == 2, "strslet vectors must be of shape [2,number of sources]"
+            assert strsvec.shape[0] == 2, "strsvec vectors must be of shape [2,number of sources]"
+        if nd > 1:
+            assert strslet.shape[0] == nd and strslet.shape[1] == 2 and strslet.shape[2] == ns, \
+                "strslet vectors must be of shape [nd,2,ns] where nd is number of densities, " \
+                "and ns is number of sources"
+            assert strsvec.shape[0] == nd and strsvec.shape[1] == 2 and strsvec.shape[2] == ns, \
+                "strsvec vectors must be of shape [nd,2,ns] where nd is number of densities, " \
+                "and ns is number of sources"
+
+
+def _st_run(eps, sources, stoklet, strslet, strsvec, targets, ifppreg, ifppregtarg, nd,
+            direct=False, thresh=1e-16):
+    import torch
+    torch_mode = _is_torch(sources)
+    ns = _ns_of(sources)
+    s = _fortran_dev(sources, (2, ns), torch.float64)
+    f = lambda a: None if a is None else _fortran_dev(a, (nd, 2, ns), torch.float64)
+    sk, sl, sv = f(stoklet), f(strslet), f(strsvec)
+    nt = 0
+    t = None
+    if targets is not None and ifppregtarg > 0:
+        nt = _ns_of(targets)
+        t = _fortran_dev(targets, (2, nt), torch.float64)
+    z = lambda *sh: torch.zeros(sh, dtype=torch.float64, device="cuda")
+    bufs = []
+    for n, lev in ((ns, ifppreg), (nt, ifppregtarg)):
+        bufs.append((z(n, 2, nd) if lev >= 1 and n else None,
+                     z(n, nd) if lev >= 2 and n else None,
+                     z(n, 2, 2, nd) if lev >= 3 and n else None))
+    (pot, pre, grad), (pott, pret, gradt) = bufs
+    ier = C.c_int(0)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    L = _lib.lib()
+    ist, isl = int(sk is not None), int(sl is not None)
+    if direct:
+        for tg, n, lev, (po, pr, gr) in ((s, ns, ifppreg, bufs[0]), (t, nt, ifppregtarg, bufs[1])):
+            if lev > 0 and n:
+                L.b2fmm_st2ddir_dev(nd, ns, _ptr(s), ist, _ptr(sk), isl, _ptr(sl), _ptr(sv), n,
+                                    _ptr(tg), lev, _ptr(po), _ptr(pr), _ptr(gr),
+                                    C.c_double(thresh), stream, C.byref(ier))
+    else:
+        L.b2fmm_stfmm2d_dev(nd, C.c_double(eps), ns, _ptr(s), ist, _ptr(sk), isl, _ptr(sl),
+                            _ptr(sv), ifppreg, _ptr(pot), _ptr(pre), _ptr(grad), nt, _ptr(t),
+                            ifppregtarg, _ptr(pott), _ptr(pret), _ptr(gradt), stream,
+                            C.byref(ier))
+    out = Output()
+    out.ier = ier.value
+    out.pot, out.pre, out.grad = (_user(a, torch_mode, False) for a in (pot, pre, grad))
+    out.pottarg, out.pretarg, out.gradtarg = (_user(a, torch_mode, False)
+                                              for a in (pott, pret, gradt))
+    return out
+
+
+def _st_front(eps, sources, stoklet, strslet, strsvec, targets, ifppreg, ifppregtarg, nd,
+              direct, thresh=1e-16):
+    out = Output()
+    if ifppreg == 0 and ifppregtarg == 0:
+        print("Nothing to compute, set either ifppreg or ifppregtarg to non-zero")
+        return out
+    if stoklet is None and strslet is None and strsvec is None:
+        print("Nothing to compute, set either stoklet or strslet+strsvec to non-None")
+        return out
+    if strslet is not None and strsvec is None:
+        print("strslet and strsvec mush be both None or both not None")
+        return out
+    if strslet is None and strsvec is not None:
+        print("strslet and strsvec mush be both None or both not None")
+        return out
+    assert sources.shape[0] == 2, "The first dimension of sources must be 2"
+    ns = _ns_of(sources)
+    if targets is not None:
+        assert targets.shape[0] == 2, "The first dimension of targets must be 2"
+    _st_check(stoklet, strslet, strsvec, nd, ns)
+    return _st_run(eps, sources, stoklet, strslet, strsvec, targets, ifppreg, ifppregtarg, nd,
+                   direct, thresh)
+
+
+def stfmm2d(*, eps, sources, stoklet=None, strslet=None, strsvec=None, targets=None, ifppreg=0,
+            ifppregtarg=0, nd=1):
+    """Stokes FMM (fmm2d.py stfmm2d, src/stokes/stfmm2d.f): velocity (nd,2,n),
+    pressure (nd,n) and velocity gradient (nd,2,2,n) of stokeslets and
+    stresslets (nd,2,n each)."""
+    return _st_front(eps, sources, stoklet, strslet, strsvec, targets, ifppreg, ifppregtarg, nd,
+                     False)
+
+
+def st2ddir(*, eps, sources, stoklet=None, strslet=None, strsvec=None, targets=None, ifppreg=0,
+            ifppregtarg=0, nd=1, thresh=1e-16):
+    """All-pairs Stokes sums (fmm2d.py st2ddir, stokkernels2d.f)."""
+    return _st_front(eps, sources, stoklet, strslet, strsvec, targets, ifppreg, ifppregtarg, nd,
+                     True, thresh)
+
+
 def _np(a):
     if _is_torch(a):
         return a.detach().cpu().numpy()

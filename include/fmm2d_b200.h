@@ -14,9 +14,10 @@
  * the given CUDA stream (NULL = legacy default stream) and return after the
  * stream has finished the call.
  * ier: 0 ok, 4 device allocation failure, 13 expansion order too large,
- *      20 Helmholtz problem needing the high-frequency (box > 16
- *      wavelengths) translations, 100 invalid argument, 101 CUDA error,
- *      103 problem larger than a fixed static scratch array.
+ *      100 invalid argument (a non-finite coordinate included), 101 CUDA
+ *      error, 102 a bounded device wait gave up, 103 problem larger than a
+ *      fixed static scratch array, 104 (asynchronous calls) the tree needs a
+ *      synchronous call.
  */
 #ifndef FMM2D_B200_H
 #define FMM2D_B200_H
@@ -163,9 +164,9 @@ void b2fmm_lap_direct_noalloc_dev(int kind, int nd, int64_t ns, const double* so
 
 /* hfmm2d: src/helmholtz/hfmm2d.f:19-22.  zk is passed as (zk_re, zk_im);
  * charge, dipstr and all outputs are complex, grad (nd,2,n), hess (nd,3,n),
- * dipvec (nd,2,n) real.  Low-frequency path: ier 20 when a level where
- * translations run has boxes larger than 16 wavelengths
- * (hfmm2d.f:1001-1013, the wideband branch of src/helmholtz/wideband2d.f). */
+ * dipvec (nd,2,n) real.  Levels whose boxes exceed 16 wavelengths
+ * (hfmm2d.f:1001-1013) translate in the diagonal (signature) form of
+ * src/helmholtz/wideband2d.f. */
 void b2fmm_hfmm2d(int nd, double eps, double zk_re, double zk_im, int64_t ns,
                   const double* sources, int ifcharge, const double* charge, int ifdipole,
                   const double* dipstr, const double* dipvec, int iper, int ifpgh, double* pot,
@@ -189,13 +190,63 @@ void b2fmm_hfmm2d_dev(int nd, double eps, double zk_re, double zk_im, int64_t ns
                       double* pottarg, double* gradtarg, double* hesstarg,
                       const b2fmm_options* opts, double* timeinfo, void* stream, int* ier);
 
+/* ------------------------------------------------- biharmonic and Stokes */
+
+/* bhfmm2d: src/biharmonic/bhfmm2d.f:1-4.  Host arrays: charge complex
+ * (nd,2,ns) = (c1, c2), dip complex (nd,3,ns) = (d1, d2, d3); pot complex
+ * (nd,n), grad complex (nd,3,n) (d/dz, its conj(z) part, d/dconj(z)); the
+ * kernel of bhkernels2d.f bh2d_directcdg.  hess and hesstarg are not
+ * computed (as in the reference).  Runs as one FP64 Cauchy FMM over 4 nd
+ * densities. */
+void b2fmm_bhfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                   const double* charge, int ifdipole, const double* dip, int iper, int ifpgh,
+                   double* pot, double* grad, double* hess, int64_t nt, const double* targ,
+                   int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg, int* ier);
+
+/* Device-pointer form of b2fmm_bhfmm2d on `stream` (blocking). */
+void b2fmm_bhfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,
+                       const double* charge, int ifdipole, const double* dip, int ifpgh,
+                       double* pot, double* grad, int64_t nt, const double* targ, int ifpghtarg,
+                       double* pottarg, double* gradtarg, void* stream, int* ier);
+
+/* All-pairs biharmonic sums at nt targets (bh2ddir of the python API,
+ * bhkernels2d.f bh2d_direct*); charge or dip may be null; pairs closer than
+ * thresh are skipped. */
+void b2fmm_bh2ddir_dev(int nd, int64_t ns, const double* sources, const double* charge,
+                       const double* dip, int64_t nt, const double* targ, int ifpgh, double* pot,
+                       double* grad, double thresh, void* stream, int* ier);
+
+/* stfmm2d: src/stokes/stfmm2d.f:3-7.  Host arrays: stoklet, strslet,
+ * strsvec real (nd,2,ns); pot (nd,2,n), pre (nd,n), grad (nd,2,2,n) real;
+ * ifppreg 1 velocity, 2 + pressure, 3 + velocity gradient. */
+void b2fmm_stfmm2d(int nd, double eps, int64_t ns, const double* sources, int ifstoklet,
+                   const double* stoklet, int ifstrslet, const double* strslet,
+                   const double* strsvec, int ifppreg, double* pot, double* pre, double* grad,
+                   int64_t nt, const double* targ, int ifppregtarg, double* pottarg,
+                   double* pretarg, double* gradtarg, int* ier);
+
+/* Device-pointer form of b2fmm_stfmm2d on `stream` (blocking). */
+void b2fmm_stfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifstoklet,
+                       const double* stoklet, int ifstrslet, const double* strslet,
+                       const double* strsvec, int ifppreg, double* pot, double* pre, double* grad,
+                       int64_t nt, const double* targ, int ifppregtarg, double* pottarg,
+                       double* pretarg, double* gradtarg, void* stream, int* ier);
+
+/* All-pairs Stokes sums at nt targets (st2ddir of the python API,
+ * src/stokes/stokkernels2d.f st2ddirectstokstrsg). */
+void b2fmm_st2ddir_dev(int nd, int64_t ns, const double* sources, int ifstoklet,
+                       const double* stoklet, int ifstrslet, const double* strslet,
+                       const double* strsvec, int64_t nt, const double* targ, int ifppreg,
+                       double* pot, double* pre, double* grad, double thresh, void* stream,
+                       int* ier);
+
 /* hfmm2d_mps: src/helmholtz/hfmm2d_mps.f:19-22.  Host arrays: cmpole (2,
  * nmpole), rmpole (nmpole), mterms (nmpole), impole (nmpole, 1-based
  * offsets into the complex arrays), mpole and local complex (ntot).
  * Expansion i is the (nd, -m..m) block at impole(i) with m = mterms(i) <= 63.
  * On return local holds, at each block, the local expansion about that
  * centre due to all the other expansions.  ier 100 when a block lies
- * outside ntot, 13 for an order above 63, 20 in the high-frequency regime. */
+ * outside ntot, 13 for an order above 63. */
 void b2fmm_hfmm2d_mps(int nd, double eps, double zk_re, double zk_im, int64_t nmpole,
                       const double* cmpole, const double* rmpole, const int* mterms,
                       int64_t ntot, const double* mpole, const int* impole, double* local,

@@ -12,6 +12,8 @@
  *             lfmm2d.f:29-32, rfmm2d.f:27-30, src/helmholtz/hfmm2d.f:19-22
  *   tuning    cfmm2d_ndiv_ ... hfmm2d_ndiv_            cfmm2d_ndiv.f:23-26 etc.
  *   sources   hfmm2d_mps_ (multipole expansions)       src/helmholtz/hfmm2d_mps.f:19-22
+ *   kernels   bhfmm2d_, stfmm2d_                       src/biharmonic/bhfmm2d.f:1-4,
+ *                                                      src/stokes/stfmm2d.f:3-7
  *   flags     {c,l,r,h}fmm2d_{s,t,st}_{c,d,cd}_{p,g,h}[_vec]_   (27 + 27 per family)
  *             src/laplace/{l,r,c}fmm2dwrap.f, {l,r,c}fmm2dwrap_vec.f,
  *             src/helmholtz/hfmm2dwrap.f, hfmm2dwrap_vec.f
@@ -85,6 +87,21 @@ void hfmm2d_ndiv_(const int* nd, const double* eps, const double* zk, const int*
                   const int* nt, const double* targ, const int* ifpghtarg, double* pottarg,
                   double* gradtarg, double* hesstarg, const int* ndiv, const int* idivflag,
                   const int* ifnear, double* timeinfo, int* ier);
+
+/* ---- biharmonic (src/biharmonic/bhfmm2d.f:1-4) and Stokes
+ * (src/stokes/stfmm2d.f:3-7) FMMs: charge(nd,2,ns), dip(nd,3,ns) complex;
+ * stoklet, strslet, strsvec (nd,2,ns) real; see fmm2d_b200.h. */
+void bhfmm2d_(const int* nd, const double* eps, const int* ns, const double* sources,
+              const int* ifcharge, const double* charge, const int* ifdipole, const double* dip,
+              const int* iper, const int* ifpgh, double* pot, double* grad, double* hess,
+              const int* nt, const double* targ, const int* ifpghtarg, double* pottarg,
+              double* gradtarg, double* hesstarg, int* ier);
+void stfmm2d_(const int* nd, const double* eps, const int* nsource, const double* source,
+              const int* ifstoklet, const double* stoklet, const int* ifstrslet,
+              const double* strslet, const double* strsvec, const int* ifppreg, double* pot,
+              double* pre, double* grad, const int* ntarg, const double* targ,
+              const int* ifppregtarg, double* pottarg, double* pretarg, double* gradtarg,
+              int* ier);
 
 /* ---- FMM over multipole expansions (src/helmholtz/hfmm2d_mps.f:19-22):
  * cmpole(2,nmpole), rmpole(nmpole), mterms(nmpole), mpole/local(ntot)

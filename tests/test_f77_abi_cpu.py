@@ -1,7 +1,8 @@
 """No-GPU checks of libfmm2d.so, the reference's own entry points served by
 the B200 library: it loads, exports every routine include/fmm2d_f77.h
 declares (the 4 core routines, their 4 _ndiv variants, 27 + 27 flag
-wrappers per family, hfmm2d_mps and the C function hfmm2d_s_c_p), and every Fortran
+wrappers per family, hfmm2d_mps, bhfmm2d, stfmm2d and the C function
+hfmm2d_s_c_p), and every Fortran
 name it exports is one the reference library exports too."""
 import ctypes
 import os
@@ -30,12 +31,12 @@ def expected():
             for d in ("c", "d", "cd"):
                 for o in "pgh":
                     names += [f"{f}fmm2d_{k}_{d}_{o}_", f"{f}fmm2d_{k}_{d}_{o}_vec_"]
-    return sorted(names + ["hfmm2d_s_c_p", "hfmm2d_mps_"])
+    return sorted(names + ["hfmm2d_s_c_p", "hfmm2d_mps_", "bhfmm2d_", "stfmm2d_"])
 
 
 def test_header_declares_the_reference_surface():
     assert declared() == expected()
-    assert len(expected()) == 4 * (2 + 54) + 2
+    assert len(expected()) == 4 * (2 + 54) + 4
 
 
 def test_library_exports_every_declared_routine():
