@@ -355,16 +355,17 @@ def main():
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--train-problems", type=int, default=60)
     ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--samples", default=SAMPLES, help="training samples (written by train)")
     ap.add_argument("--from-samples", action="store_true",
-                    help="refit on fmm2d_b200/costmodel_samples.json instead of timing")
+                    help="refit on the samples file instead of timing")
     args = ap.parse_args()
     if args.cmd == "train":
         if args.from_samples:
-            X, y, rec = load_samples()
+            X, y, rec = load_samples(args.samples)
         else:
             probs = sweep_problems(args.train_problems, seed0=1000, nmax=2e6)
             X, y, rec = collect(probs)
-            save_samples(X, y, rec)
+            save_samples(X, y, rec, args.samples)
         bad = [r for r in rec if r["err"] is not None and r["err"] > r["eps"]]
         m, hist = train(X, y, steps=args.steps)
         m.best_constant = best_constant(rec)

@@ -269,7 +269,8 @@ struct OT {
   static constexpr int C = KH / 2;                   // coefficients per builder thread
   static constexpr int BUILDERS = 256;
   static constexpr int BWARPS = BUILDERS / 32;
-  static constexpr int THREADS = BUILDERS + 32;      // + the MMA issuer warp
+  static constexpr int ISSUERS = OT_STAGES;          // MMA issuer warps (one thread each)
+  static constexpr int THREADS = BUILDERS + 32 * ISSUERS;
   static constexpr uint32_t SA = 128u * K * 4;       // one A tile (hi or lo)
   static constexpr uint32_t SB = (uint32_t)N * K * 4;  // one B tile (hi or lo)
   static constexpr uint32_t A0 = 0;                  // A stages: [stage][hi, lo]
@@ -572,45 +573,39 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
         take(x);
       }
     } else if (lane == 0) {
-      // MMA issuer.  After the blocking wait for the next stage it also takes
-      // the following stages that are already full, so that one tcgen05 fence
-      // covers several steps (the fence costs a few hundred clocks).
+      // MMA issuers: issuer w takes the steps g = w (mod OT_STAGES), i.e.
+      // always stage w, so that the steps of OT_STAGES stages are issued
+      // concurrently (one thread issues a tcgen05.mma only every ~150 SM
+      // clocks; four threads together reach ~40-50).  Each commit covers the
+      // issuing thread's own MMAs: the commit of step g releases stage
+      // g % OT_STAGES and marks product g % OT_DBUF complete.
+      const uint32_t w = (uint32_t)(warp - L::BWARPS);
       const uint32_t idesc = idesc_tf32(TC_ROWS, N);
       const uint64_t bh = umma_desc(sbase + L::B0, 128, (uint32_t)K * 32);
       const uint64_t bl = bh + (L::SB >> 4);
       bool fail = *s_fail != 0;
-      uint32_t left = nsteps;
-      while (left > 0) {
-        if (!fail && !mbar_wait(full0 + 8 * (g % OT_STAGES), (g / OT_STAGES) & 1)) fail = true;
-        uint32_t ready = 1;
-        while (!fail && ready < left && ready < OT_STAGES) {
-          const uint32_t gn = g + ready;
-          if (!mbar_test(full0 + 8 * (gn % OT_STAGES), (gn / OT_STAGES) & 1)) break;
-          ++ready;
-        }
+      const uint32_t first = g0 + ((w + OT_STAGES - g0 % OT_STAGES) % OT_STAGES);
+      for (uint32_t x = first; x < g0 + nsteps; x += OT_STAGES) {
+        const int s = (int)(x % OT_STAGES);
+        if (!fail && !mbar_wait(full0 + 8 * s, (x / OT_STAGES) & 1)) fail = true;
         tc_fence_after();
-        for (uint32_t q = 0; q < ready; q++) {
-          const int s = (int)(g % OT_STAGES);
-          if (!fail) {
-            const uint32_t dt = taddr + (uint32_t)((g % OT_DBUF) * N);
-            // a K step of 8 columns advances a start address by 256 bytes
-            // (16 in descriptor units)
-            const uint64_t ah =
-                umma_desc(sbase + L::A0 + (uint32_t)s * 2 * L::SA, 128, (uint32_t)K * 32);
-            const uint64_t al = ah + (L::SA >> 4);
+        if (!fail) {
+          const uint32_t dt = taddr + (uint32_t)((x % OT_DBUF) * N);
+          // a K step of 8 columns advances a start address by 256 bytes
+          // (16 in descriptor units)
+          const uint64_t ah =
+              umma_desc(sbase + L::A0 + (uint32_t)s * 2 * L::SA, 128, (uint32_t)K * 32);
+          const uint64_t al = ah + (L::SA >> 4);
 #pragma unroll
-            for (int ks = 0; ks < K / 8; ks++)
-              umma_tf32(dt, ah + 16 * ks, bl + 16 * ks, idesc, ks == 0 ? 0u : 1u);
+          for (int ks = 0; ks < K / 8; ks++)
+            umma_tf32(dt, ah + 16 * ks, bl + 16 * ks, idesc, ks == 0 ? 0u : 1u);
 #pragma unroll
-            for (int ks = 0; ks < K / 8; ks++) umma_tf32(dt, al + 16 * ks, bh + 16 * ks, idesc, 1u);
+          for (int ks = 0; ks < K / 8; ks++) umma_tf32(dt, al + 16 * ks, bh + 16 * ks, idesc, 1u);
 #pragma unroll
-            for (int ks = 0; ks < K / 8; ks++) umma_tf32(dt, ah + 16 * ks, bh + 16 * ks, idesc, 1u);
-          }
-          // the commit also releases the stage when nothing was issued
-          umma_commit(empty0 + 8 * s);
-          ++g;
+          for (int ks = 0; ks < K / 8; ks++) umma_tf32(dt, ah + 16 * ks, bh + 16 * ks, idesc, 1u);
         }
-        left -= ready;
+        // the commit also releases the stage when nothing was issued
+        umma_commit(empty0 + 8 * s);
       }
       if (fail) *s_fail = 1;
     }
@@ -619,11 +614,11 @@ __global__ void __launch_bounds__(OT<KH>::THREADS, 1)
     __syncthreads();
     tc_fence_after();
   }
-  if (*s_fail && g > 0) {
+  if (*s_fail && tid == 0) {
     // the tensor cores may still be working: one more bounded wait for the
-    // last commit before the tensor memory is released
-    const uint32_t gl = g - 1;
-    mbar_wait(empty0 + 8 * (gl % OT_STAGES), (gl / OT_STAGES) & 1);
+    // last commit of every stage before the tensor memory is released
+    for (uint32_t gl = g > OT_STAGES ? g - OT_STAGES : 0; gl < g; gl++)
+      mbar_wait(empty0 + 8 * (gl % OT_STAGES), (gl / OT_STAGES) & 1);
   }
   tc_fence_before();
   __syncthreads();
