@@ -523,9 +523,7 @@ __global__ void __launch_bounds__(64) k_p2l(TV t, int first, int n, const double
 // The offset-independent matrix G (G_0j = 1, G_i0 = -1/i, G_ij = C(i+j-1,j-1))
 // sits in shared memory; per pair only the power vectors depend on z0.
 // ---------------------------------------------------------------------------
-// REG (P <= 32): each lane keeps its column of G in registers, so the inner
-// product reads only the broadcast t_j from shared memory.
-template <int ND, bool REG>
+template <int ND>
 __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
                                              const double* __restrict__ binom,
                                              const double2* __restrict__ mp,
@@ -546,12 +544,6 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
   }
   __syncthreads();
   double2* Tbase = smem + (P * P + 1) / 2;
-  double gr[REG ? 32 : 1];
-  if (REG) {
-    const int i = threadIdx.x & 31;
-#pragma unroll
-    for (int j = 0; j < (REG ? 32 : 1); j++) gr[j] = (i < P && j < P) ? G[j * P + i] : 0.0;
-  }
   WARP_LOOP(n) {
     double2* T = Tbase + (size_t)wib * P * ND;
     int b = first + bi;
@@ -592,28 +584,13 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
         double2 y[ND];
 #pragma unroll
         for (int d = 0; d < ND; d++) y[d] = make_double2(0, 0);
-        if (REG) {
+        for (int j = 0; j < P; j++) {
+          double g = G[j * P + i];
 #pragma unroll
-          for (int j = 0; j < (REG ? 32 : 1); j++) {
-            if (j < P) {
-              const double g = gr[j];
-#pragma unroll
-              for (int d = 0; d < ND; d++) {
-                const double2 tj = T[j * ND + d];
-                y[d].x += g * tj.x;
-                y[d].y += g * tj.y;
-              }
-            }
-          }
-        } else {
-          for (int j = 0; j < P; j++) {
-            double g = G[j * P + i];
-#pragma unroll
-            for (int d = 0; d < ND; d++) {
-              double2 tj = T[j * ND + d];
-              y[d].x += g * tj.x;
-              y[d].y += g * tj.y;
-            }
+          for (int d = 0; d < ND; d++) {
+            double2 tj = T[j * ND + d];
+            y[d].x += g * tj.x;
+            y[d].y += g * tj.y;
           }
         }
         if (i == 0) {
@@ -1256,15 +1233,9 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
     lap_mixed_m2l(ND, tv, from2, n_from2, P, binom, *M, mp, lo, st);
   } else if (n_from2 > 0) {
     size_t sm = sizeof(double) * (P * P + 1) + sizeof(double2) * 4 * P * ND;
-    if (P <= 32) {
-      if (sm > 48 * 1024) set_smem_attr(k_m2l<ND, true>, sm);
-      k_m2l<ND, true><<<warp_grid(n_from2, 4), 128, sm, st>>>(tv, from2, n_from2, P, binom, mp,
-                                                              lo);
-    } else {
-      if (sm > 48 * 1024) set_smem_attr(k_m2l<ND, false>, sm);
-      k_m2l<ND, false><<<warp_grid(n_from2, 4), 128, sm, st>>>(tv, from2, n_from2, P, binom, mp,
-                                                               lo);
-    }
+    if (sm > 48 * 1024)
+      set_smem_attr(k_m2l<ND>, sm);
+    k_m2l<ND><<<warp_grid(n_from2, 4), 128, sm, st>>>(tv, from2, n_from2, P, binom, mp, lo);
     B2_LAUNCH_CHECK();
   }
   B2_CHECK(cudaEventRecord(ev[4], st));
