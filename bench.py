@@ -701,8 +701,12 @@ def main():
     step(prec)
     L.b2fmm_set_stats(0)
     st = _lib.get_stats()
-    phases = {"p2m": ti[0], "p2l": ti[1], "m2m": ti[2], "m2l": ti[3], "l2l": ti[4],
-              "leaf_eval(l2p+m2p+p2p)": ti[7]}
+    phases = {"p2m": ti[0], "p2l": ti[1], "m2m": ti[2], "m2l": ti[3], "l2l": ti[4]}
+    if prec == "mixed":
+        # two kernels: k_far_mixed (L2P + M2P, FP64), then k_p2p_mixed (FP32)
+        phases.update({"far(l2p+m2p)": ti[5], "p2p": ti[7]})
+    else:
+        phases["leaf_eval(l2p+m2p+p2p)"] = ti[7]
     phases_ms = {k: round(v * 1e3, 4) for k, v in phases.items()}
     dom = max(phases, key=phases.get)
     fma_peak = L.b2fmm_fma_peak(1 if prec == "fp64" else 0)
@@ -711,8 +715,9 @@ def main():
     # algorithmic flops (FMA = 2): P2P charge+dipole pot+grad per pair 15 + 28*nd2
     # (per pair: 15 real flops for the kernel terms, 28 per density); M2L per
     # translation 2*P*P real MACs x 2 (re,im) x nd2
-    flops = {"leaf_eval(l2p+m2p+p2p)": st["p2p_pairs"] * (15 + 28 * nd2)
-             + st["npts_eval"] * 16 * P * nd2 + st["m2p_evals"] * 16 * P * nd2,
+    far_fl = st["npts_eval"] * 16 * P * nd2 + st["m2p_evals"] * 16 * P * nd2
+    p2p_fl = st["p2p_pairs"] * (15 + 28 * nd2)
+    flops = {"leaf_eval(l2p+m2p+p2p)": p2p_fl + far_fl, "far(l2p+m2p)": far_fl, "p2p": p2p_fl,
              "m2l": st["m2l_pairs"] * 4 * P * P * nd2}
     t_dom = phases[dom]
     achieved = flops.get(dom, 0.0) / t_dom / 1e12 if t_dom > 0 else 0.0
@@ -744,13 +749,13 @@ def main():
                     "frac": achieved / (fma_peak / 1e12), "traffic": None,
                     "peak_source": ("in-run FMA microbenchmark b2fmm_fma_peak "
                                     f"({'FP64' if prec == 'fp64' else 'FP32'})")}
-    t_leaf = phases["leaf_eval(l2p+m2p+p2p)"]
-    p2p_fl = st["p2p_pairs"] * (15 + 28 * nd2)
+    t_p2p = phases.get("p2p", phases.get("leaf_eval(l2p+m2p+p2p)", 0.0))
     roofline["near_field"] = {"bound": "fma", "pairs": st["p2p_pairs"],
-                              "achieved": p2p_fl / t_leaf / 1e12 if t_leaf > 0 else 0.0,
+                              "achieved": p2p_fl / t_p2p / 1e12 if t_p2p > 0 else 0.0,
                               "peak": fma_peak / 1e12, "unit": "TFLOP/s",
-                              "note": "P2P flops over the whole leaf phase (L2P and M2P "
-                                      "included in the time)"}
+                              "note": ("k_p2p_mixed alone (FP32 pair kernel, FP64 pair "
+                                       "differences)" if "p2p" in phases else
+                                       "P2P flops over the whole fused leaf kernel")}
     roofline["near_field"]["frac"] = roofline["near_field"]["achieved"] / (fma_peak / 1e12)
     roofline.update({"phase_ms": phases_ms, "tree_ms": round(st["tree_ms"], 4),
                      "counts": counts})

@@ -513,7 +513,8 @@ void m2l_launch(const TV& t, int first, int n, int P, const double* binom, const
 template <int ND, int IFPGH>
 void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const double2* xe64,
                  int ndc, int d0, int P, const double2* mp, const double2* lo, double thresh,
-                 int ifnear, double2* pot, double2* grad, double2* hess, cudaStream_t st) {
+                 int ifnear, double2* pot, double2* grad, double2* hess, cudaStream_t st,
+                 cudaEvent_t far_done) {
   (void)nb;
   const long n = use_targets ? M.nt : M.ns;
   if (n <= 0) return;
@@ -521,6 +522,7 @@ void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const
   k_far_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(t, n, leaf, xe64, ndc, d0, P, mp, lo,
                                                           pot, grad, hess);
   B2_LAUNCH_CHECK();
+  if (far_done) B2_CHECK(cudaEventRecord(far_done, st));
   if (!ifnear) return;
   k_p2p_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(
       t, n, leaf, M.xs64, xe64, M.q.p, M.d.p, ndc, d0,
@@ -532,13 +534,13 @@ template <int ND>
 void leaf_dispatch(int ifl, const TV& t, int nb, int use_targets, const MixedData& M,
                    const double2* xe64, int ndc, int d0, int P, const double2* mp,
                    const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
-                   double2* hess, cudaStream_t st) {
+                   double2* hess, cudaStream_t st, cudaEvent_t far_done) {
   if (ifl == 1)
-    leaf_launch<ND, 1>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+    leaf_launch<ND, 1>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
   else if (ifl == 2)
-    leaf_launch<ND, 2>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+    leaf_launch<ND, 2>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
   else
-    leaf_launch<ND, 3>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+    leaf_launch<ND, 3>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
 }
 
 }  // namespace
@@ -612,12 +614,12 @@ void lap_mixed_m2l(int ND, const TV& t, int first, int n, int P, const double* b
 void lap_mixed_leaf(int ND, int ifl, const TV& t, int nb, int use_targets, const MixedData& M,
                     const double2* xe64, int ndc, int d0, int P, const double2* mp,
                     const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
-                    double2* hess, cudaStream_t st) {
+                    double2* hess, cudaStream_t st, cudaEvent_t far_done) {
   switch (ND) {
-    case 8: leaf_dispatch<8>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
-    case 4: leaf_dispatch<4>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
-    case 2: leaf_dispatch<2>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
-    default: leaf_dispatch<1>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st); break;
+    case 8: leaf_dispatch<8>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
+    case 4: leaf_dispatch<4>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
+    case 2: leaf_dispatch<2>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
+    default: leaf_dispatch<1>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
   }
 }
 

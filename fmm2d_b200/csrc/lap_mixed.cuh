@@ -47,10 +47,12 @@ void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, lon
 void lap_mixed_m2l(int ND, const lapk::TV& t, int first, int n, int P, const double* binom,
                    const MixedData& M, const double2* mp, double2* lo, cudaStream_t st);
 
-// Fused leaf evaluation (L2P + M2P in FP64, P2P in FP32) for one chunk.
+// Leaf evaluation (L2P + M2P in FP64, then P2P in FP32) for one chunk;
+// far_done (optional) is recorded between the two kernels.
 void lap_mixed_leaf(int ND, int ifl, const lapk::TV& t, int nb, int use_targets,
                     const MixedData& M, const double2* xe64, int ndc, int d0, int P,
                     const double2* mp, const double2* lo, double thresh, int ifnear,
-                    double2* pot, double2* grad, double2* hess, cudaStream_t st);
+                    double2* pot, double2* grad, double2* hess, cudaStream_t st,
+                    cudaEvent_t far_done = nullptr);
 
 }  // namespace b2
