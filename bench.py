@@ -703,7 +703,7 @@ def main():
     st = _lib.get_stats()
     phases = {"p2m": ti[0], "p2l": ti[1], "m2m": ti[2], "m2l": ti[3], "l2l": ti[4]}
     if prec == "mixed":
-        # two kernels: k_far_mixed (L2P + M2P, FP64), then k_p2p_mixed (FP32)
+        # two kernels: k_far_mixed (L2P + M2P, FP64), then k_p2p_leaf (FP32)
         phases.update({"far(l2p+m2p)": ti[5], "p2p": ti[7]})
     else:
         phases["leaf_eval(l2p+m2p+p2p)"] = ti[7]
@@ -753,8 +753,8 @@ def main():
     roofline["near_field"] = {"bound": "fma", "pairs": st["p2p_pairs"],
                               "achieved": p2p_fl / t_p2p / 1e12 if t_p2p > 0 else 0.0,
                               "peak": fma_peak / 1e12, "unit": "TFLOP/s",
-                              "note": ("k_p2p_mixed alone (FP32 pair kernel, FP64 pair "
-                                       "differences)" if "p2p" in phases else
+                              "note": ("k_p2p_leaf alone (FP32 pair kernel, two-float "
+                                       "leaf-relative pair differences)" if "p2p" in phases else
                                        "P2P flops over the whole fused leaf kernel")}
     roofline["near_field"]["frac"] = roofline["near_field"]["achieved"] / (fma_peak / 1e12)
     roofline.update({"phase_ms": phases_ms, "tree_ms": round(st["tree_ms"], 4),

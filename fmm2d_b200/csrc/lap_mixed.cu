@@ -7,16 +7,19 @@
 //   multipole (FP64 -> FP32) and the fixed matrix G(i,j) = C(i+j-1, j-1)
 //   remain.  Local expansions are accumulated in FP32 per target box and
 //   added to the FP64 expansion once.
-// * k_far_mixed / k_p2p_mixed: one evaluation point per thread.  L2P and M2P
-//   in FP64 (as the FP64 path), then the near field in FP32.  The coordinate
-//   difference of a pair is formed in FP64 and rounded once to FP32, so it
-//   keeps the relative accuracy of the FP64 path's difference even for nearly
-//   coincident points (separations of 1e-12 occur in graded distributions);
-//   log and 1/r^2 use the SFU.  Per-pair terms are summed in FP32 over at
-//   most 32 sources and the partial sums in FP64.
+// * k_far_mixed: L2P and M2P in FP64 (as the FP64 path), one evaluation
+//   point per thread.
+// * k_p2p_leaf: the near field in FP32, per work item (up to 32 evaluation
+//   points of one leaf) over sources staged in shared memory as two-float
+//   offsets from the leaf centre, so a pair difference keeps the relative
+//   accuracy of an FP64 difference even for nearly coincident points
+//   (separations of 1e-12 occur in graded distributions); log and 1/r^2 use
+//   the SFU.  Per-pair terms are summed in FP32 over at most 32 sources and
+//   the partial sums in FP64.
 #include "lap_mixed.cuh"
 
 #include <atomic>
+#include <cstddef>
 #include "laplace.cuh"
 
 namespace b2 {
@@ -240,10 +243,6 @@ __global__ void k_point_leaf(TV t, int nb, int use_targets, int* __restrict__ le
 // 2.59 -> 2.50 ms at 4M points); the compiler's choice otherwise.
 #define FAR_MIN_BLOCKS(ND, IFPGH) ((ND) <= 2 && (IFPGH) <= 2 ? 8 : 1)
 
-// The same for the near field: 10 blocks (at most 48 registers a thread) for
-// one or two densities without hessians (leaf phase 2.50 -> 2.43 ms at 4M).
-#define P2P_MIN_BLOCKS(ND, IFPGH) ((ND) <= 2 && (IFPGH) <= 2 ? 10 : 1)
-
 // Far field of one evaluation point per thread, FP64: L2P from the local
 // expansion of its leaf and M2P from the leaf's list-3 boxes (the
 // coefficients of one box are shared by the neighbouring threads of the same
@@ -388,108 +387,373 @@ __global__ void __launch_bounds__(128, FAR_MIN_BLOCKS(ND, IFPGH)) k_far_mixed(
   }
 }
 
-// Near field of one evaluation point per thread, FP32 (cauchykernels2d.f):
-// all sources of the leaf's list-1 boxes; coordinate differences from the
-// hi/lo float pairs, per-pair terms summed in FP32 over at most 32 sources,
-// the partial sums in FP64, added to the far field already in the outputs.
-template <int ND, int IFPGH>
-__global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_mixed(
-    TV t, long n, const int* __restrict__ leaf, const double2* __restrict__ xs64,
-    const double2* __restrict__ xe64, const float2* __restrict__ q32,
-    const float2* __restrict__ d32, int ndc, int d0, float th2, double2* __restrict__ pot,
-    double2* __restrict__ grad, double2* __restrict__ hess) {
-  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (k >= n || t.ctl->status != TB_OK) return;
-  if (th2 < 0.f) {
-    const double thr = near_thresh(t, -1.0);
-    th2 = (float)(thr * thr);
+// Register budget of the near-field pass: 6 blocks of 128 threads per SM
+// (at most 80 registers a thread) for one or two densities without
+// hessians; the compiler's choice otherwise.
+#ifndef P2P_MB
+#define P2P_MB 6
+#endif
+#define P2P_MIN_BLOCKS(ND, IFPGH) ((ND) <= 2 && (IFPGH) <= 2 ? P2P_MB : 1)
+
+// Grid of a persistent pass: every SM filled with as many blocks as fit.
+template <typename K>
+int resident_grid(K kernel, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::vector<std::pair<std::pair<const void*, int>, int>> done;
+  int dev = 0;
+  B2_CHECK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> g(mu);
+  for (auto& e : done)
+    if (e.first.first == (const void*)kernel && e.first.second == dev) return e.second;
+  int nsm = 0, per = 0;
+  B2_CHECK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  B2_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem));
+  const int grid = std::max(1, per) * nsm;
+  done.push_back({{(const void*)kernel, dev}, grid});
+  return grid;
+}
+
+// Near field of the mixed path, FP32 (cauchykernels2d.f c2d_directcdg and
+// relatives), one warp per work item of up to 32 evaluation points of one
+// leaf box (the item list is built once per tree by k_p2p_items; warps take
+// items in turn).  The warp stages the union of the item's list-1 sources in
+// shared memory, up to 128 at a time, as offsets from the leaf
+// centre scaled by a power of two 2^-e close to 1/(box size): x = hi + lo,
+// two floats (48 significant bits of an offset of a few box sizes).  A pair
+// difference is (zh - sh) + (zl - sl), with an absolute error of ~2^-46 in
+// these units; pairs closer than 2^-20 box sizes (rare, but graded
+// distributions have them) are formed again as an FP64 difference of the
+// input coordinates rounded once, so nearly coincident points keep the
+// relative accuracy of the FP64 difference; the pair of a point with itself
+// is skipped by index.  Lane = (target ti, source phase ph): the warp takes
+// the item's ntc targets, 32 / ntc phases each, and the phases of one
+// target are summed by shuffles at the end.
+// Terms use the scaled geometry: log r = log r' + e ln 2, 1/z = 2^-e / z'
+// (dipole strengths are staged times 2^-e, gradients and hessians scaled
+// once per target).
+// Per-pair terms are summed in FP32 over at most 32 sources, those partial
+// sums in FP64, and added to the far field already in the outputs.  KIND: 1
+// charges, 2 dipoles, 3 both.
+#ifndef P2P_CHUNK
+#define P2P_CHUNK 128
+#endif
+constexpr int P2P_CH = P2P_CHUNK;  // staged sources per warp and chunk
+#ifndef P2P_UNR
+#define P2P_UNR 2
+#endif
+constexpr int P2P_UNROLL = P2P_UNR;
+static_assert(MNLIST1 <= 16, "list-1 search below covers 16 boxes");
+
+__device__ __forceinline__ void split_hilo(double x, float& hi, float& lo) {
+  hi = __double2float_rn(x);
+  lo = __double2float_rn(x - (double)hi);
+}
+
+// One staged source: scaled offset (hi x, hi y, lo x, lo y), then its
+// charges and dipole strengths (KIND decides which are present).
+template <int ND, int KIND>
+struct P2PSrc {
+  float4 p;
+  float2 c[ND * ((KIND & 1) + ((KIND >> 1) & 1))];
+};
+
+// A near-field work item (see k_p2p_items).
+struct P2PItem {
+  int b, k0, meta, ex;  // box, first point, points | list-1 length << 8, exponent
+  int S, pad0, pad1, pad2;  // sources in the list-1 boxes
+  double2 c;            // box centre
+  int lst[16];          // list-1 source range starts
+  int lpre[16];         // exclusive prefix of the range lengths
+};
+
+static_assert(offsetof(P2PItem, lpre) == offsetof(P2PItem, lst) + 16 * sizeof(int),
+              "lst and lpre are read as 32 consecutive ints");
+
+// Shared memory of one warp: staged sources, their input indices and one
+// leaf's list-1 ranges.
+template <int ND, int KIND>
+struct P2PWarp {
+  P2PSrc<ND, KIND> s[P2P_CH];
+  int j[P2P_CH];
+  int lst[16];   // list-1 source range starts
+  int lpre[16];  // exclusive prefix of the list-1 range lengths (follows lst)
+};
+using P2PWarp11 = P2PWarp<1, 1>;
+static_assert(offsetof(P2PWarp11, lpre) == offsetof(P2PWarp11, lst) + 16 * sizeof(int),
+              "lst and lpre are written as 32 consecutive ints");
+
+// Near-field work items of one tree, ceil(n / 32) per leaf box with n
+// evaluation points, written once per tree (appended in any order; count[0]
+// ends as the number of items).  An item holds everything the pass needs
+// before it stages sources: the box, its first point and point count, the
+// list-1 length, the binary exponent of the box size, the centre, and the
+// source ranges of the list-1 boxes with their exclusive prefix.
+__global__ void k_p2p_items(TV t, int nb, int use_targets, P2PItem* __restrict__ items,
+                            int* __restrict__ count) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (nb < 0) {
+    int f = RANGE_ALL;
+    resolve_range(t, f, nb);
   }
-  const bool hq = q32 != nullptr, hd = d32 != nullptr;
-  const int b = leaf[k];
-  const double2 z = xe64[k];
-  double2 pt[ND], gr[ND], hs[ND];
+  int ni = 0;
+  int2 tr = make_int2(0, 0);
+  if (b < nb && t.nchild[b] == 0) {
+    tr = use_targets ? t.trng[b] : t.srng[b];
+    ni = tr.y > tr.x ? (tr.y - tr.x + 31) / 32 : 0;
+  }
+  // one atomic per warp
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int inc = ni;
 #pragma unroll
-  for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
-  float2 fp[ND], fg[ND], fh[ND];
-#pragma unroll
-  for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
-  int cnt = 0;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(FULL, inc, o);
+    if (lane >= o) inc += v;
+  }
+  int base = 0;
+  if (lane == 31 && inc > 0) base = atomicAdd(count, inc);
+  base = __shfl_sync(FULL, base, 31) + inc - ni;
+  if (ni == 0) return;
+  P2PItem it;
+  int ex = 0;
+  frexp(t.boxsize[t.level[b]], &ex);
   const int n1 = t.nl1[b];
-  for (int e = 0; e < n1; e++) {
-    int2 sr = t.srng[t.l1[(size_t)MNLIST1 * b + e]];
-    for (int j = sr.x; j < sr.y; j++) {
-      // the difference in FP64 (as the FP64 path forms it), the kernel in FP32:
-      // sources closer than ~1e-15 of the coordinates keep their relative accuracy
-      double2 s = xs64[j];
-      float dx = (float)(z.x - s.x);
-      float dy = (float)(z.y - s.y);
-      float rr = fmaf(dx, dx, dy * dy);
-      // cauchykernels2d.f: <= for potential-only, < otherwise
-      if (!(IFPGH == 1 ? (rr <= th2) : (rr < th2))) {
-        float ir = __fdividef(1.0f, rr);
-        float2 zi = make_float2(dx * ir, -dy * ir);
-        float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
-        if (hq) {
-          float lg = 0.5f * __logf(rr);
+  it.b = b;
+  it.ex = ex;
+  it.c = t.center[b];
+  int S = 0;
+  for (int e = 0; e < 16; e++) {
+    int2 r = make_int2(0, 0);
+    if (e < n1) r = t.srng[t.l1[(size_t)MNLIST1 * b + e]];
+    it.lst[e] = r.x;
+    it.lpre[e] = S;
+    S += r.y - r.x;
+  }
+  it.S = S;
+  it.pad0 = it.pad1 = it.pad2 = 0;
+  const int nt = tr.y - tr.x;
+  for (int i = 0; i < ni; i++) {
+    it.k0 = tr.x + 32 * i;
+    it.meta = min(32, nt - 32 * i) | (n1 << 8);
+    items[base + i] = it;
+  }
+}
+
+template <int ND, int IFPGH, int KIND>
+__global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
+    TV t, const double2* __restrict__ xs64, const double2* __restrict__ xe64,
+    const float2* __restrict__ q32, const float2* __restrict__ d32, int ndc, int d0,
+    double thresh, const P2PItem* __restrict__ items, const int* __restrict__ nitems,
+    int self_pairs, double2* __restrict__ pot, double2* __restrict__ grad,
+    double2* __restrict__ hess) {
+  constexpr bool HQ = KIND & 1, HD = (KIND >> 1) & 1;
+  constexpr int DOFF = HQ ? ND : 0;  // first dipole entry of a staged source
+  extern __shared__ float4 p2p_sm[];
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  P2PWarp<ND, KIND>& W = ((P2PWarp<ND, KIND>*)p2p_sm)[wib];
+  // after a failed tree build the item list is empty
+  const int ni = t.ctl->status == TB_OK ? *nitems : 0;
+  const double thr = near_thresh(t, thresh);
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int it = blockIdx.x * (blockDim.x >> 5) + wib; it < ni; it += nw) {
+    const P2PItem& I = items[it];
+    // the list-1 ranges and their prefix: 32 consecutive ints, one a lane
+    ((int*)W.lst)[lane] = ((const int*)I.lst)[lane];
+    const int4 h = *(const int4*)&I;
+    const int n1 = h.z >> 8, ntc = h.z & 255, ex = h.w;
+    const int S = I.S;
+    const double2 c = I.c;
+    // 32 / ntc and lane / ntc by a float reciprocal (exact: the quotients
+    // are at least 1/64 away from the next integer)
+    const float rn = __frcp_rn((float)ntc);
+    const int nph = __float2int_rz(32.5f * rn);
+    const int ph = __float2int_rz(((float)lane + 0.5f) * rn), ti = lane - ph * ntc;
+    const bool act = ph < nph;
+    const long k = (long)h.y + ti;
+    const double sc = __hiloint2double((1023 - ex) << 20, 0);  // 2^-ex
+    const float scf = (float)sc;
+    const double ts = thr * sc;
+    const float th2 = (float)(ts * ts);
+    // pairs below this squared distance take the careful path (FP64
+    // difference, exclusion test)
+    const float rslow = fmaxf(0x1p-40f, 2.f * th2);
+    const float lsc = (float)((double)ex * 0.69314718055994530942);
+    __syncwarp();
+    // at most 32 sources per lane and chunk: one FP32 partial sum each
+    const int cap = min(P2P_CH, 32 * nph);
+    float2 zh, zl;
+    {
+      const double2 z = xe64[k];
+      split_hilo((z.x - c.x) * sc, zh.x, zl.x);
+      split_hilo((z.y - c.y) * sc, zh.y, zl.y);
+    }
+    double2 pt[ND], gr[ND], hs[ND];
 #pragma unroll
-          for (int d = 0; d < ND; d++) {
-            float2 c = q32[(size_t)j * ndc + d0 + d];
-            fp[d].x = fmaf(lg, c.x, fp[d].x);
-            fp[d].y = fmaf(lg, c.y, fp[d].y);
-            if (IFPGH >= 2) cfmaf_(fg[d], zi, c);
-            if (IFPGH >= 3) cfmaf_(fh[d], z2, c);
-          }
-        }
-        if (hd) {
-          float2 z3 = make_float2(0.f, 0.f);
-          if (IFPGH >= 3) {
-            z3 = cmulf_(z2, zi);
-            z3 = make_float2(-2.f * z3.x, -2.f * z3.y);
-          }
+    for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
+    for (int u0 = 0; u0 < S; u0 += cap) {
+      const int m = min(cap, S - u0);
+      for (int i = lane; i < m; i += 32) {
+        // the list-1 box of source u: the last e with lpre[e] <= u
+        const int u = u0 + i;
+        int e = 0;
 #pragma unroll
-          for (int d = 0; d < ND; d++) {
-            float2 c = d32[(size_t)j * ndc + d0 + d];
-            cfmaf_(fp[d], zi, c);
-            if (IFPGH >= 2) cfmaf_(fg[d], z2, c);
-            if (IFPGH >= 3) cfmaf_(fh[d], z3, c);
+        for (int step = 8; step > 0; step >>= 1)
+          if (e + step < n1 && W.lpre[e + step] <= u) e += step;
+        const int j = W.lst[e] + (u - W.lpre[e]);
+        const double2 sxy = xs64[j];
+        P2PSrc<ND, KIND>& R = W.s[i];
+        float4 p;
+        split_hilo((sxy.x - c.x) * sc, p.x, p.z);
+        split_hilo((sxy.y - c.y) * sc, p.y, p.w);
+        R.p = p;
+        W.j[i] = j;
+        const size_t o = (size_t)j * ndc + d0;
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          if (HQ) R.c[d] = q32[o + d];
+          if (HD) {
+            const float2 v = d32[o + d];
+            R.c[DOFF + d] = make_float2(v.x * scf, v.y * scf);
           }
         }
       }
-      if (++cnt == 32) {
-        cnt = 0;
+      __syncwarp();
+      if (act) {
+        float2 fp[ND], fg[ND], fh[ND];
+#pragma unroll
+        for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
+#pragma unroll P2P_UNROLL
+        for (int u = ph; u < m; u += nph) {
+          const P2PSrc<ND, KIND>& R = W.s[u];
+          const float4 p = R.p;
+          float dx = (zh.x - p.x) + (zl.x - p.z);
+          float dy = (zh.y - p.y) + (zl.y - p.w);
+          float rr = fmaf(dx, dx, dy * dy);
+          if (rr < rslow) {
+            // a point and itself (evaluation points = sources): r = 0, excluded
+            const int js = W.j[u];
+            if (self_pairs && js == k) continue;
+            if (rr < 0x1p-40f) {
+              // nearly coincident: the FP64 difference, rounded once
+              const double2 sxy = xs64[js];
+              const double2 z = xe64[k];
+              dx = __double2float_rn((z.x - sxy.x) * sc);
+              dy = __double2float_rn((z.y - sxy.y) * sc);
+              rr = fmaf(dx, dx, dy * dy);
+            }
+            // cauchykernels2d.f: <= for potential-only, < otherwise
+            if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
+          }
+          const float ir = __fdividef(1.0f, rr);
+          const float2 zi = make_float2(dx * ir, -dy * ir);
+          const float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
+          if (HQ) {
+            const float lg = fmaf(0.5f, __logf(rr), lsc);
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              const float2 v = R.c[d];
+              fp[d].x = fmaf(lg, v.x, fp[d].x);
+              fp[d].y = fmaf(lg, v.y, fp[d].y);
+              if (IFPGH >= 2) cfmaf_(fg[d], zi, v);
+              if (IFPGH >= 3) cfmaf_(fh[d], z2, v);
+            }
+          }
+          if (HD) {
+            float2 z3 = make_float2(0.f, 0.f);
+            if (IFPGH >= 3) {
+              z3 = cmulf_(z2, zi);
+              z3 = make_float2(-2.f * z3.x, -2.f * z3.y);
+            }
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              const float2 v = R.c[DOFF + d];
+              cfmaf_(fp[d], zi, v);
+              if (IFPGH >= 2) cfmaf_(fg[d], z2, v);
+              if (IFPGH >= 3) cfmaf_(fh[d], z3, v);
+            }
+          }
+        }
 #pragma unroll
         for (int d = 0; d < ND; d++) {
           pt[d].x += fp[d].x;
           pt[d].y += fp[d].y;
-          fp[d] = make_float2(0.f, 0.f);
           if (IFPGH >= 2) {
             gr[d].x += fg[d].x;
             gr[d].y += fg[d].y;
-            fg[d] = make_float2(0.f, 0.f);
           }
           if (IFPGH >= 3) {
             hs[d].x += fh[d].x;
             hs[d].y += fh[d].y;
-            fh[d] = make_float2(0.f, 0.f);
+          }
+        }
+      }
+      __syncwarp();
+    }
+    // sum the phases of every target: a tree over ph by shuffles at strides
+    // ntc, 2 ntc, 4 ntc, ... (a lane adds its partner only if that phase
+    // exists)
+    for (int hh = 1; hh < nph; hh <<= 1) {
+      const bool take = (ph & (2 * hh - 1)) == 0 && ph + hh < nph;
+      const int off = hh * ntc;
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        double2 v;
+        v.x = __shfl_down_sync(FULL, pt[d].x, off);
+        v.y = __shfl_down_sync(FULL, pt[d].y, off);
+        if (take) {
+          pt[d].x += v.x;
+          pt[d].y += v.y;
+        }
+        if (IFPGH >= 2) {
+          v.x = __shfl_down_sync(FULL, gr[d].x, off);
+          v.y = __shfl_down_sync(FULL, gr[d].y, off);
+          if (take) {
+            gr[d].x += v.x;
+            gr[d].y += v.y;
+          }
+        }
+        if (IFPGH >= 3) {
+          v.x = __shfl_down_sync(FULL, hs[d].x, off);
+          v.y = __shfl_down_sync(FULL, hs[d].y, off);
+          if (take) {
+            hs[d].x += v.x;
+            hs[d].y += v.y;
           }
         }
       }
     }
-  }
+    if (lane < ntc) {
 #pragma unroll
-  for (int d = 0; d < ND; d++) {
-    size_t o = (size_t)k * ndc + d0 + d;
-    double2 v = pot[o];
-    pot[o] = make_double2(v.x + pt[d].x + fp[d].x, v.y + pt[d].y + fp[d].y);
-    if (IFPGH >= 2) {
-      v = grad[o];
-      grad[o] = make_double2(v.x + gr[d].x + fg[d].x, v.y + gr[d].y + fg[d].y);
-    }
-    if (IFPGH >= 3) {
-      v = hess[o];
-      hess[o] = make_double2(v.x + hs[d].x + fh[d].x, v.y + hs[d].y + fh[d].y);
+      for (int d = 0; d < ND; d++) {
+        const size_t o = (size_t)k * ndc + d0 + d;
+        double2 w = pot[o];
+        pot[o] = make_double2(w.x + pt[d].x, w.y + pt[d].y);
+        if (IFPGH >= 2) {
+          w = grad[o];
+          grad[o] = make_double2(w.x + sc * gr[d].x, w.y + sc * gr[d].y);
+        }
+        if (IFPGH >= 3) {
+          w = hess[o];
+          const double s2 = sc * sc;
+          hess[o] = make_double2(w.x + s2 * hs[d].x, w.y + s2 * hs[d].y);
+        }
+      }
     }
   }
+}
+
+template <int ND, int IFPGH, int KIND>
+void p2p_launch(const TV& t, const MixedData& M, const double2* xe64, int ndc, int d0,
+                double thresh, const P2PItem* items, const int* nitems, double2* pot,
+                double2* grad, double2* hess, cudaStream_t st) {
+  constexpr size_t sm = 4 * sizeof(P2PWarp<ND, KIND>);
+  auto kern = k_p2p_leaf<ND, IFPGH, KIND>;
+  set_smem_attr(kern, sm);
+  kern<<<resident_grid(kern, 128, sm), 128, sm, st>>>(t, M.xs64, xe64, M.q.p, M.d.p, ndc, d0,
+                                                     thresh, items, nitems,
+                                                     xe64 == M.xs64 ? 1 : 0, pot, grad, hess);
+  B2_LAUNCH_CHECK();
 }
 
 int grid_for(long nitems, int wpb) {
@@ -511,11 +775,10 @@ void m2l_launch(const TV& t, int first, int n, int P, const double* binom, const
 }
 
 template <int ND, int IFPGH>
-void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const double2* xe64,
-                 int ndc, int d0, int P, const double2* mp, const double2* lo, double thresh,
-                 int ifnear, double2* pot, double2* grad, double2* hess, cudaStream_t st,
+void leaf_launch(const TV& t, int use_targets, const MixedData& M, const double2* xe64, int ndc,
+                 int d0, int P, const double2* mp, const double2* lo, double thresh, int ifnear,
+                 double2* pot, double2* grad, double2* hess, cudaStream_t st,
                  cudaEvent_t far_done) {
-  (void)nb;
   const long n = use_targets ? M.nt : M.ns;
   if (n <= 0) return;
   const int* leaf = use_targets ? M.leaf_t.p : M.leaf_s.p;
@@ -523,24 +786,29 @@ void leaf_launch(const TV& t, int nb, int use_targets, const MixedData& M, const
                                                           pot, grad, hess);
   B2_LAUNCH_CHECK();
   if (far_done) B2_CHECK(cudaEventRecord(far_done, st));
-  if (!ifnear) return;
-  k_p2p_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(
-      t, n, leaf, M.xs64, xe64, M.q.p, M.d.p, ndc, d0,
-      thresh >= 0 ? (float)(thresh * thresh) : -1.f, pot, grad, hess);
-  B2_LAUNCH_CHECK();
+  const int kind = (M.q.p ? 1 : 0) | (M.d.p ? 2 : 0);
+  if (!ifnear || kind == 0) return;
+  const P2PItem* items = (const P2PItem*)(use_targets ? M.items_t.p : M.items_s.p);
+  const int* nitems = M.nitems.p + (use_targets ? 1 : 0);
+  if (kind == 3)
+    p2p_launch<ND, IFPGH, 3>(t, M, xe64, ndc, d0, thresh, items, nitems, pot, grad, hess, st);
+  else if (kind == 2)
+    p2p_launch<ND, IFPGH, 2>(t, M, xe64, ndc, d0, thresh, items, nitems, pot, grad, hess, st);
+  else
+    p2p_launch<ND, IFPGH, 1>(t, M, xe64, ndc, d0, thresh, items, nitems, pot, grad, hess, st);
 }
 
 template <int ND>
-void leaf_dispatch(int ifl, const TV& t, int nb, int use_targets, const MixedData& M,
+void leaf_dispatch(int ifl, const TV& t, int use_targets, const MixedData& M,
                    const double2* xe64, int ndc, int d0, int P, const double2* mp,
                    const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
                    double2* hess, cudaStream_t st, cudaEvent_t far_done) {
   if (ifl == 1)
-    leaf_launch<ND, 1>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
+    leaf_launch<ND, 1>(t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
   else if (ifl == 2)
-    leaf_launch<ND, 2>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
+    leaf_launch<ND, 2>(t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
   else
-    leaf_launch<ND, 3>(t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
+    leaf_launch<ND, 3>(t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
 }
 
 }  // namespace
@@ -568,9 +836,20 @@ void lap_mixed_leaves(MixedData& M, const TV& t, int nb, bool dev, long ns, long
   M.leaf_s.alloc(ns, st);
   k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, dev ? -1 : nb, 0, M.leaf_s.p);
   B2_LAUNCH_CHECK();
+  M.nitems.alloc(2, st);
+  B2_CHECK(cudaMemsetAsync(M.nitems.p, 0, 2 * sizeof(int), st));
+  // at most one item per leaf plus one per 32 points
+  M.items_s.alloc(((size_t)nb + ns / 32 + 1) * sizeof(P2PItem), st);
+  k_p2p_items<<<ceil_div(nb, 128), 128, 0, st>>>(t, dev ? -1 : nb, 0, (P2PItem*)M.items_s.p,
+                                                  M.nitems.p);
+  B2_LAUNCH_CHECK();
   if (nt > 0) {
     M.leaf_t.alloc(nt, st);
     k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, dev ? -1 : nb, 1, M.leaf_t.p);
+    B2_LAUNCH_CHECK();
+    M.items_t.alloc(((size_t)nb + nt / 32 + 1) * sizeof(P2PItem), st);
+    k_p2p_items<<<ceil_div(nb, 128), 128, 0, st>>>(t, dev ? -1 : nb, 1, (P2PItem*)M.items_t.p,
+                                                    M.nitems.p + 1);
     B2_LAUNCH_CHECK();
   }
 }
@@ -615,11 +894,12 @@ void lap_mixed_leaf(int ND, int ifl, const TV& t, int nb, int use_targets, const
                     const double2* xe64, int ndc, int d0, int P, const double2* mp,
                     const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
                     double2* hess, cudaStream_t st, cudaEvent_t far_done) {
+  (void)nb;
   switch (ND) {
-    case 8: leaf_dispatch<8>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
-    case 4: leaf_dispatch<4>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
-    case 2: leaf_dispatch<2>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
-    default: leaf_dispatch<1>(ifl, t, nb, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
+    case 8: leaf_dispatch<8>(ifl, t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
+    case 4: leaf_dispatch<4>(ifl, t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
+    case 2: leaf_dispatch<2>(ifl, t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
+    default: leaf_dispatch<1>(ifl, t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done); break;
   }
 }
 

@@ -8,7 +8,8 @@
 namespace b2 {
 
 // Data of the mixed-precision kernels: FP32 copies of the sorted densities,
-// offset tables, the tensor-core M2L pair list and per-point leaf maps.
+// offset tables, the tensor-core M2L pair list, per-point leaf maps and
+// near-field work items.
 struct MixedData {
   const double2* xs64 = nullptr;  // sorted sources (FP64, owned by the caller)
   DBuf<float2> q, d;    // all Cauchy densities, ndc per point
@@ -20,7 +21,9 @@ struct MixedData {
   int nlev = 0;         // tree levels + 1
   int nboxes = 0;
   long ns = 0, nt = 0;
-  DBuf<int> leaf_s, leaf_t;  // leaf box of every sorted source / target
+  DBuf<int> leaf_s, leaf_t;     // leaf box of every sorted source / target
+  DBuf<char> items_s, items_t;  // near-field work items (sources, targets)
+  DBuf<int> nitems;              // their counts
   int* err = nullptr;   // device flag set by a tensor-core wait that gave up
 };
 
@@ -34,8 +37,9 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
                        bool has_q, bool has_d, int ndc, double cx0, double cy0, int P,
                        cudaStream_t st);
 
-// Leaf box of every sorted evaluation point (once per tree); nb boxes at
-// most, the box count read from the tree's device control block when dev.
+// Leaf box of every sorted evaluation point and the near-field work items
+// (once per tree); nb boxes at most, the box count read from the tree's
+// device control block when dev.
 void lap_mixed_leaves(MixedData& M, const lapk::TV& t, int nb, bool dev, long ns, long nt,
                       cudaStream_t st);
 
@@ -47,8 +51,8 @@ void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, lon
 void lap_mixed_m2l(int ND, const lapk::TV& t, int first, int n, int P, const double* binom,
                    const MixedData& M, const double2* mp, double2* lo, cudaStream_t st);
 
-// Leaf evaluation (L2P + M2P in FP64, then P2P in FP32) for one chunk;
-// far_done (optional) is recorded between the two kernels.
+// Leaf evaluation (L2P + M2P in FP64, then P2P in FP32) for one density
+// chunk; far_done (optional) is recorded between the two kernels.
 void lap_mixed_leaf(int ND, int ifl, const lapk::TV& t, int nb, int use_targets,
                     const MixedData& M, const double2* xe64, int ndc, int d0, int P,
                     const double2* mp, const double2* lo, double thresh, int ifnear,
