@@ -421,11 +421,12 @@ int resident_grid(K kernel, int threads, size_t smem) {
 // centre scaled by a power of two 2^-e close to 1/(box size): x = hi + lo,
 // two floats (48 significant bits of an offset of a few box sizes).  A pair
 // difference is (zh - sh) + (zl - sl), with an absolute error of ~2^-46 in
-// these units; pairs closer than 2^-20 box sizes (rare, but graded
-// distributions have them) are formed again as an FP64 difference of the
-// input coordinates rounded once, so nearly coincident points keep the
-// relative accuracy of the FP64 difference; the pair of a point with itself
-// is skipped by index.  Lane = (target ti, source phase ph): the warp takes
+// these units.  Pairs closer than 2^-20 box sizes (rare, but graded
+// distributions have them) add nothing in the branch-free pass; the target's
+// lane forms them after it as an FP64 difference of the input coordinates
+// rounded once, so nearly coincident points keep the relative accuracy of
+// the FP64 difference, and skips the pair of a point with itself by index.
+// Lane = (target ti, source phase ph): the warp takes
 // the item's ntc targets, 32 / ntc phases each, and the phases of one
 // target are summed by shuffles at the end.
 // Terms use the scaled geometry: log r = log r' + e ln 2, 1/z = 2^-e / z'
@@ -469,12 +470,10 @@ struct P2PItem {
 static_assert(offsetof(P2PItem, lpre) == offsetof(P2PItem, lst) + 16 * sizeof(int),
               "lst and lpre are read as 32 consecutive ints");
 
-// Shared memory of one warp: staged sources, their input indices and one
-// leaf's list-1 ranges.
+// Shared memory of one warp: staged sources and one leaf's list-1 ranges.
 template <int ND, int KIND>
 struct P2PWarp {
   P2PSrc<ND, KIND> s[P2P_CH];
-  int j[P2P_CH];
   int lst[16];   // list-1 source range starts
   int lpre[16];  // exclusive prefix of the list-1 range lengths (follows lst)
 };
@@ -591,6 +590,7 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
     double2 pt[ND], gr[ND], hs[ND];
 #pragma unroll
     for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
+    int nslow = 0;
     for (int u0 = 0; u0 < S; u0 += cap) {
       const int m = min(cap, S - u0);
       for (int i = lane; i < m; i += 32) {
@@ -607,7 +607,6 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
         split_hilo((sxy.x - c.x) * sc, p.x, p.z);
         split_hilo((sxy.y - c.y) * sc, p.y, p.w);
         R.p = p;
-        W.j[i] = j;
         const size_t o = (size_t)j * ndc + d0;
 #pragma unroll
         for (int d = 0; d < ND; d++) {
@@ -623,36 +622,26 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
         float2 fp[ND], fg[ND], fh[ND];
 #pragma unroll
         for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
+        // branch-free pairs: a pair closer than rslow (the pair of a point
+        // with itself, nearly coincident or excluded pairs) adds nothing
+        // here and is counted; such pairs are formed after the item
+        const P2PSrc<ND, KIND>* const Rend = W.s + m;
 #pragma unroll P2P_UNROLL
-        for (int u = ph; u < m; u += nph) {
-          const P2PSrc<ND, KIND>& R = W.s[u];
-          const float4 p = R.p;
-          float dx = (zh.x - p.x) + (zl.x - p.z);
-          float dy = (zh.y - p.y) + (zl.y - p.w);
-          float rr = fmaf(dx, dx, dy * dy);
-          if (rr < rslow) {
-            // a point and itself (evaluation points = sources): r = 0, excluded
-            const int js = W.j[u];
-            if (self_pairs && js == k) continue;
-            if (rr < 0x1p-40f) {
-              // nearly coincident: the FP64 difference, rounded once
-              const double2 sxy = xs64[js];
-              const double2 z = xe64[k];
-              dx = __double2float_rn((z.x - sxy.x) * sc);
-              dy = __double2float_rn((z.y - sxy.y) * sc);
-              rr = fmaf(dx, dx, dy * dy);
-            }
-            // cauchykernels2d.f: <= for potential-only, < otherwise
-            if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
-          }
-          const float ir = __fdividef(1.0f, rr);
+        for (const P2PSrc<ND, KIND>* R = W.s + ph; R < Rend; R += nph) {
+          const float4 p = R->p;
+          const float dx = (zh.x - p.x) + (zl.x - p.z);
+          const float dy = (zh.y - p.y) + (zl.y - p.w);
+          const float rr = fmaf(dx, dx, dy * dy);
+          const bool fast = rr >= rslow;
+          nslow += fast ? 0 : 1;
+          const float ir = fast ? __fdividef(1.0f, rr) : 0.f;
           const float2 zi = make_float2(dx * ir, -dy * ir);
           const float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
           if (HQ) {
-            const float lg = fmaf(0.5f, __logf(rr), lsc);
+            const float lg = fast ? fmaf(0.5f, __logf(rr), lsc) : 0.f;
 #pragma unroll
             for (int d = 0; d < ND; d++) {
-              const float2 v = R.c[d];
+              const float2 v = R->c[d];
               fp[d].x = fmaf(lg, v.x, fp[d].x);
               fp[d].y = fmaf(lg, v.y, fp[d].y);
               if (IFPGH >= 2) cfmaf_(fg[d], zi, v);
@@ -667,7 +656,7 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
             }
 #pragma unroll
             for (int d = 0; d < ND; d++) {
-              const float2 v = R.c[DOFF + d];
+              const float2 v = R->c[DOFF + d];
               cfmaf_(fp[d], zi, v);
               if (IFPGH >= 2) cfmaf_(fg[d], z2, v);
               if (IFPGH >= 3) cfmaf_(fh[d], z3, v);
@@ -696,6 +685,10 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
     for (int hh = 1; hh < nph; hh <<= 1) {
       const bool take = (ph & (2 * hh - 1)) == 0 && ph + hh < nph;
       const int off = hh * ntc;
+      {
+        const int v = __shfl_down_sync(FULL, nslow, off);
+        if (take) nslow += v;
+      }
 #pragma unroll
       for (int d = 0; d < ND; d++) {
         double2 v;
@@ -719,6 +712,68 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
           if (take) {
             hs[d].x += v.x;
             hs[d].y += v.y;
+          }
+        }
+      }
+    }
+    // the close pairs: beyond the pair of a point with itself (one per
+    // target when the evaluation points are the sources) they are rare; the
+    // target's lane walks its sources again and forms them one by one
+    const bool redo = act && ph == 0 && nslow > (self_pairs ? 1 : 0);
+    if (__any_sync(FULL, redo) && redo) {
+      const double2 z = xe64[k];
+      for (int e = 0; e < n1; e++) {
+        const int j0 = W.lst[e], len = (e + 1 < n1 ? W.lpre[e + 1] : S) - W.lpre[e];
+        for (int j = j0; j < j0 + len; j++) {
+          const double2 sxy = xs64[j];
+          float4 p;
+          split_hilo((sxy.x - c.x) * sc, p.x, p.z);
+          split_hilo((sxy.y - c.y) * sc, p.y, p.w);
+          float dx = (zh.x - p.x) + (zl.x - p.z);
+          float dy = (zh.y - p.y) + (zl.y - p.w);
+          float rr = fmaf(dx, dx, dy * dy);
+          if (rr >= rslow) continue;  // formed in the pass above
+          if (self_pairs && j == k) continue;  // a point and itself: r = 0
+          if (rr < 0x1p-40f) {
+            // nearly coincident: the FP64 difference, rounded once
+            dx = __double2float_rn((z.x - sxy.x) * sc);
+            dy = __double2float_rn((z.y - sxy.y) * sc);
+            rr = fmaf(dx, dx, dy * dy);
+          }
+          // cauchykernels2d.f: <= for potential-only, < otherwise
+          if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
+          const float ir = __fdividef(1.0f, rr);
+          const float2 zi = make_float2(dx * ir, -dy * ir);
+          const float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
+          const float2 z3 = IFPGH >= 3 ? cmulf_(z2, zi) : make_float2(0.f, 0.f);
+          const size_t o = (size_t)j * ndc + d0;
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            float2 fp = make_float2(0.f, 0.f), fg = fp, fh = fp;
+            if (HQ) {
+              const float lg = fmaf(0.5f, __logf(rr), lsc);
+              const float2 v = q32[o + d];
+              fp = make_float2(lg * v.x, lg * v.y);
+              if (IFPGH >= 2) cfmaf_(fg, zi, v);
+              if (IFPGH >= 3) cfmaf_(fh, z2, v);
+            }
+            if (HD) {
+              const float2 v0 = d32[o + d];
+              const float2 v = make_float2(v0.x * scf, v0.y * scf);
+              cfmaf_(fp, zi, v);
+              if (IFPGH >= 2) cfmaf_(fg, z2, v);
+              if (IFPGH >= 3) cfmaf_(fh, make_float2(-2.f * z3.x, -2.f * z3.y), v);
+            }
+            pt[d].x += fp.x;
+            pt[d].y += fp.y;
+            if (IFPGH >= 2) {
+              gr[d].x += fg.x;
+              gr[d].y += fg.y;
+            }
+            if (IFPGH >= 3) {
+              hs[d].x += fh.x;
+              hs[d].y += fh.y;
+            }
           }
         }
       }
