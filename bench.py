@@ -45,10 +45,11 @@ the graph's results against the sequential ones.
 ``costmodel_c5`` is the learned-cost-model sweep: 40 rfmm2d problems with N
 log-uniform in [1e4, 8e6] over three distributions (uniform; the 16-Gaussian
 mixture; the curve above with density graded over 1e3), real N(0,1)
-charges, eps in {1e-3, 1e-6}, pg = 2: total time with the leaf size chosen by
-the trained network (fmm2d_b200/costmodel.py) against the lndiv2d table and
-against the best single constant leaf size per eps of the training timings,
-all three error-checked against the FP64 direct sum.
+charges, eps in {1e-3, 1e-6}, pg = 2: total time with the leaf size and level
+balance chosen by the trained network (fmm2d_b200/costmodel.py) against the
+lndiv2d table, the best single constant leaf size per eps of the training
+timings, and the network's leaf size alone at balance 0, all four
+error-checked against the FP64 direct sum.
 
 Multi-GPU (torchrun): every rank evaluates its own independent problem of the
 same size (replicas, no collective in the data path); timings are the max over
@@ -822,6 +823,7 @@ def main():
             c5["workload"] = ("40 rfmm2d problems, N log-uniform [1e4, 8e6], uniform / "
                               "16-Gaussian mixture / graded curve, eps in {1e-3, 1e-6}, pg=2")
             c5["ndiv_mlp"] = [r["ndiv_mlp"] for r in res["rows"]]
+            c5["balance_mlp"] = [r["balance_mlp"] for r in res["rows"]]
             c5["ndiv_constant"] = sorted({r["ndiv_constant"] for r in res["rows"]})
             emit("costmodel_c5", c5)
     if not args.no_c4:

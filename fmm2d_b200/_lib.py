@@ -16,7 +16,7 @@ P = c_void_p  # all array arguments are raw pointers
 class Options(C.Structure):
     """Mirror of ``b2fmm_options``."""
     _fields_ = [("ndiv", c_int), ("idivflag", c_int), ("ifnear", c_int), ("precision", c_int),
-                ("async_call", c_int)]
+                ("async_call", c_int), ("level_balance", c_double)]
 
 
 PREC = {"auto": 0, "fp64": 1, "mixed": 2}

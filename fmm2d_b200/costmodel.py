@@ -1,28 +1,39 @@
-"""Learned cost model for the leaf size (ndiv) of the Laplace FMM.
+"""Learned cost model for the leaf size (ndiv) and the per-level
+near-field / expansion balance of the Laplace FMM.
 
-The reference picks ndiv from a fixed table of eps (lndiv2d.f:1-39).  Here a
-small MLP, trained on timings the FMM itself produces, predicts the log run
-time of one rfmm2d / lfmm2d / cfmm2d call from cheap point-distribution
-statistics and a candidate ndiv; ``choose_ndiv`` returns the candidate with
-the smallest prediction.  The network's forward, backward and Adam kernels
-are hand-written CUDA (include/fmm2d_b200.h: b2fmm_mlp_*); the point
-statistics come from a GPU histogram (b2fmm_point_stats).  The table stays
-the fallback when no trained weights are present, and accuracy is never
-traded: ndiv changes only the tree depth, the expansion order still follows
-eps, and every training run is checked against the FP64 direct sum.
+The reference picks ndiv from a fixed table of eps (lndiv2d.f:1-39) and uses
+it at every level.  Here a small MLP, trained on timings the FMM itself
+produces, predicts the log run time of one rfmm2d / lfmm2d / cfmm2d call from
+cheap point-distribution statistics, a candidate ndiv and a candidate level
+balance b (the leaf capacity at level l is ndiv 2^(b (lp - l)), lp the level
+whose boxes hold ndiv points of a uniform cloud: b > 0 keeps more points in
+the leaves above lp, as P2P work, and splits the boxes below it sooner, into
+more M2L work; b < 0 the reverse).  ``choose_ndiv`` returns the candidate
+ndiv with the smallest prediction at b = 0; ``choose_tree`` keeps it unless
+a balance at one of the three best ndiv (where the training timings sample
+the balances) is predicted faster by more than 2 %.
+The network's forward, backward and Adam kernels are hand-written CUDA
+(include/fmm2d_b200.h: b2fmm_mlp_*); the point statistics come from a GPU
+histogram (b2fmm_point_stats).  The table stays the fallback when no trained
+weights are present, and accuracy is never traded: ndiv and the balance
+change only the tree, the expansion order still follows eps, and every
+training run is checked against the FP64 direct sum.
 
 Usage on a GPU:
     python -m fmm2d_b200.costmodel train  [--out fmm2d_b200/costmodel_weights.json]
     python -m fmm2d_b200.costmodel train --from-samples   # refit on the committed samples
     python -m fmm2d_b200.costmodel evaluate
 
-``train`` times every candidate ndiv on the training problems and writes the
-samples to fmm2d_b200/costmodel_samples.json (committed, so the fit is
-reproducible without re-timing) together with the weights.  Beside the
-network it records the best single constant ndiv per eps on the same
-training timings (the smallest total time over the training problems): the
-third arm of ``evaluate``, which separates what the network learned about
-the point distribution from "larger leaves than the table".
+``train`` times every candidate ndiv at balance 0 on the training problems,
+then the three fastest of them at the other balances, and writes the samples
+to fmm2d_b200/costmodel_samples.json (committed, so the fit is reproducible
+without re-timing) together with the weights.  Beside the network it records
+the best single constant ndiv per eps on the same training timings (the
+smallest total time over the training problems).  ``evaluate`` times four
+arms on held-out problems: the table, that constant (which separates what the
+network learned about the point distribution from "larger leaves than the
+table"), the network's ndiv at balance 0, and its (ndiv, balance) pair (the
+difference between the last two is what the level balance gains).
 """
 import argparse
 import ctypes as C
@@ -35,8 +46,9 @@ import numpy as np
 
 from . import _lib
 
-NIN, H1, H2 = 9, 32, 32
+NIN, H1, H2 = 10, 32, 32
 CANDIDATES = [4, 6, 8, 11, 15, 20, 28, 40, 56, 80, 112]
+BALANCES = [-0.5, -0.25, 0.0, 0.25, 0.5]
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "costmodel_weights.json")
 SAMPLES = os.path.join(HERE, "costmodel_samples.json")
@@ -86,11 +98,18 @@ def features_from_hist(hist, eps):
     return np.array(f, dtype=np.float32)
 
 
-def model_inputs(feat, cands=CANDIDATES):
+def model_inputs(feat, cands=CANDIDATES, balances=None):
+    """Network inputs for candidate leaf sizes cands at level balances
+    (default 0 for every candidate)."""
     x = np.zeros((len(cands), NIN), dtype=np.float32)
     x[:, :8] = feat
     x[:, 8] = np.log2(np.asarray(cands, dtype=np.float64)) / 7.0
+    if balances is not None:
+        x[:, 9] = 2.0 * np.asarray(balances, dtype=np.float64)
     return x
+
+
+
 
 
 # ---------------------------------------------------------------------------
@@ -134,10 +153,23 @@ class CostModel:
         return ty.cpu().numpy() * self.ystd + self.ymean
 
     def choose_ndiv(self, feat):
+        """Best predicted ndiv at level balance 0."""
         return CANDIDATES[int(np.argmin(self.predict(model_inputs(feat))))]
+
+    def choose_tree(self, feat, top=3, margin=0.02):
+        """(ndiv, level balance): the best predicted ndiv at balance 0 unless
+        a balance at one of the `top` best ndiv (the region the training
+        timings cover) is predicted faster by more than `margin`."""
+        p0 = self.predict(model_inputs(feat))
+        best = (CANDIDATES[int(np.argmin(p0))], 0.0)
+        g = [(CANDIDATES[i], b) for i in np.argsort(p0)[:top] for b in BALANCES if b != 0.0]
+        p = self.predict(model_inputs(feat, [c[0] for c in g], [c[1] for c in g]))
+        j = int(np.argmin(p))
+        return g[j] if p[j] < float(np.min(p0)) - math.log1p(margin) else best
 
     def save(self, path=WEIGHTS):
         json.dump({"nin": NIN, "h1": H1, "h2": H2, "candidates": CANDIDATES,
+                   "balances": BALANCES,
                    "ymean": self.ymean, "ystd": self.ystd, "best_constant": self.best_constant,
                    "params": [float(v) for v in self.params]}, open(path, "w"))
 
@@ -176,14 +208,15 @@ def train(X, y, steps=3000, lr=3e-3, seed=0):
 _MODEL = None
 
 
-def auto_ndiv(src_dev, trg_dev, eps):
-    """ndiv chosen by the trained model, or the lndiv2d table without one."""
+def auto_tree(src_dev, trg_dev, eps):
+    """(ndiv, level balance) chosen by the trained model, or the lndiv2d
+    table and balance 0 without one."""
     global _MODEL
     if _MODEL is None:
         _MODEL = CostModel.load() or False
     if not _MODEL:
-        return table_ndiv(eps)
-    return _MODEL.choose_ndiv(features_from_hist(histogram(src_dev, trg_dev), eps))
+        return table_ndiv(eps), 0.0
+    return _MODEL.choose_tree(features_from_hist(histogram(src_dev, trg_dev), eps))
 
 
 # ---------------------------------------------------------------------------
@@ -210,7 +243,7 @@ def make_problem(kind, n, seed):
     return src, q
 
 
-def time_rfmm(ts, tq, eps, ndiv, reps=2):
+def time_rfmm(ts, tq, eps, ndiv, reps=2, balance=0.0):
     """Device time (ms, min of reps) of one rfmm2d call (pg = 2) and its
     potential / gradient."""
     import torch
@@ -219,6 +252,7 @@ def time_rfmm(ts, tq, eps, ndiv, reps=2):
     grad = torch.empty((n, 2, 1), dtype=torch.float64, device="cuda")
     o = _lib.Options()
     o.ndiv, o.idivflag, o.ifnear, o.precision = int(ndiv), 0, 1, 0
+    o.level_balance = float(balance)
     st = torch.cuda.current_stream()
     best = float("inf")
     for _ in range(reps + 1):
@@ -260,9 +294,10 @@ def direct_error(ts, tq, pot, grad, m=200, seed=0):
     return float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
 
 
-def collect(problems, cands=CANDIDATES, reps=2, check=True):
-    """Rows (features + log2 ndiv), targets (log ms) and the largest error of
-    every (problem, candidate) run."""
+def collect(problems, cands=CANDIDATES, reps=2, check=True, nbest=3):
+    """Rows (features, log2 ndiv, balance), targets (log ms) and the error of
+    every (problem, candidate) run: every ndiv at balance 0, then the nbest
+    fastest of those at the other balances."""
     import torch
     X, y, rec = [], [], []
     for kind, n, eps, seed in problems:
@@ -270,23 +305,35 @@ def collect(problems, cands=CANDIDATES, reps=2, check=True):
         ts = torch.as_tensor(np.ascontiguousarray(src.T), device="cuda")
         tq = torch.as_tensor(q.reshape(n, 1), device="cuda")
         feat = features_from_hist(histogram(ts), eps)
-        for nd in cands:
-            ms, pot, grad = time_rfmm(ts, tq, eps, nd, reps)
+        times = {}
+
+        def run(nd, b):
+            ms, pot, grad = time_rfmm(ts, tq, eps, nd, reps, b)
             err = direct_error(ts, tq, pot, grad) if check else None
-            X.append(model_inputs(feat, [nd])[0])
+            X.append(model_inputs(feat, [nd], [b])[0])
             y.append(math.log(ms))
-            rec.append({"kind": kind, "n": n, "eps": eps, "ndiv": nd, "ms": ms, "err": err})
+            rec.append({"kind": kind, "n": n, "eps": eps, "ndiv": nd, "balance": b, "ms": ms,
+                        "err": err})
+            return ms
+
+        for nd in cands:
+            times[nd] = run(nd, 0.0)
+        for nd in sorted(times, key=times.get)[:nbest]:
+            for b in BALANCES:
+                if b != 0.0:
+                    run(nd, b)
     return np.array(X, dtype=np.float32), np.array(y, dtype=np.float64), rec
 
 
 def best_constant(rec):
     """Per eps, the candidate with the smallest total time over the problems
-    timed in rec (every problem is timed at every candidate)."""
+    timed in rec at level balance 0 (every problem is timed at every
+    candidate there)."""
     out = {}
     for eps in sorted({r["eps"] for r in rec}):
         tot = {}
         for r in rec:
-            if r["eps"] == eps:
+            if r["eps"] == eps and r.get("balance", 0.0) == 0.0:
                 tot[r["ndiv"]] = tot.get(r["ndiv"], 0.0) + r["ms"]
         out[repr(float(eps))] = int(min(tot, key=tot.get))
     return out
@@ -298,8 +345,13 @@ def save_samples(X, y, rec, path=SAMPLES):
 
 
 def load_samples(path=SAMPLES):
+    """Samples file; rows written before the level balance input read as
+    balance 0."""
     d = json.load(open(path))
-    return np.array(d["X"], dtype=np.float32), np.array(d["y"], dtype=np.float64), d["runs"]
+    X = np.array(d["X"], dtype=np.float32)
+    if X.shape[1] < NIN:
+        X = np.concatenate([X, np.zeros((X.shape[0], NIN - X.shape[1]), np.float32)], axis=1)
+    return X, np.array(d["y"], dtype=np.float64), d["runs"]
 
 
 def sweep_problems(count, seed0, nmin=1e4, nmax=8e6):
@@ -314,8 +366,9 @@ def sweep_problems(count, seed0, nmin=1e4, nmax=8e6):
 
 
 def evaluate(model, problems):
-    """MLP-chosen ndiv against the table on the same problems, both
-    error-checked against the direct sum."""
+    """The network's (ndiv, level balance) against the lndiv2d table, the
+    best constant ndiv and the network's ndiv alone (balance 0) on the same
+    problems, every run error-checked against the direct sum."""
     import torch
     rows = []
     for kind, n, eps, seed in problems:
@@ -323,30 +376,30 @@ def evaluate(model, problems):
         ts = torch.as_tensor(np.ascontiguousarray(src.T), device="cuda")
         tq = torch.as_tensor(q.reshape(n, 1), device="cuda")
         t0 = time.perf_counter()
-        nd_m = model.choose_ndiv(features_from_hist(histogram(ts), eps))
+        feat = features_from_hist(histogram(ts), eps)
+        nd_m, b_m = model.choose_tree(feat)
         choose_ms = (time.perf_counter() - t0) * 1e3
+        nd_n = model.choose_ndiv(feat)
         nd_t = table_ndiv(eps)
         nd_c = model.constant_ndiv(eps)
-        ms_t, pt, gt = time_rfmm(ts, tq, eps, nd_t)
-        err_t = direct_error(ts, tq, pt, gt)
-        ms_m, pm, gm = time_rfmm(ts, tq, eps, nd_m)
-        err_m = direct_error(ts, tq, pm, gm)
-        ms_c, pc, gc = time_rfmm(ts, tq, eps, nd_c)
-        err_c = direct_error(ts, tq, pc, gc)
-        rows.append({"kind": kind, "n": n, "eps": eps, "ndiv_table": nd_t, "ndiv_mlp": nd_m,
-                     "ndiv_constant": nd_c, "ms_table": ms_t, "ms_mlp": ms_m,
-                     "ms_constant": ms_c, "err_table": err_t, "err_mlp": err_m,
-                     "err_constant": err_c, "choose_ms": choose_ms})
-    tt = sum(r["ms_table"] for r in rows)
-    tm = sum(r["ms_mlp"] for r in rows)
-    tc = sum(r["ms_constant"] for r in rows)
-    return {"problems": len(rows), "total_ms_table": tt, "total_ms_mlp": tm,
-            "total_ms_constant": tc, "speedup": tt / tm, "speedup_vs_constant": tc / tm,
-            "best_constant": model.best_constant,
-            "max_err_over_eps_table": max(r["err_table"] / r["eps"] for r in rows),
-            "max_err_over_eps_mlp": max(r["err_mlp"] / r["eps"] for r in rows),
-            "max_err_over_eps_constant": max(r["err_constant"] / r["eps"] for r in rows),
-            "rows": rows}
+        row = {"kind": kind, "n": n, "eps": eps, "ndiv_table": nd_t, "ndiv_mlp": nd_m,
+               "balance_mlp": b_m, "ndiv_mlp_alone": nd_n, "ndiv_constant": nd_c,
+               "choose_ms": choose_ms}
+        for arm, nd, b in (("table", nd_t, 0.0), ("mlp", nd_m, b_m), ("mlp_ndiv", nd_n, 0.0),
+                           ("constant", nd_c, 0.0)):
+            ms, p, g = time_rfmm(ts, tq, eps, nd, balance=b)
+            row["ms_" + arm] = ms
+            row["err_" + arm] = direct_error(ts, tq, p, g)
+        rows.append(row)
+    tot = {a: sum(r["ms_" + a] for r in rows) for a in ("table", "mlp", "mlp_ndiv", "constant")}
+    out = {"problems": len(rows), "best_constant": model.best_constant, "rows": rows}
+    for a, v in tot.items():
+        out["total_ms_" + a] = v
+        out["max_err_over_eps_" + a] = max(r["err_" + a] / r["eps"] for r in rows)
+    out["speedup"] = tot["table"] / tot["mlp"]
+    out["speedup_vs_constant"] = tot["constant"] / tot["mlp"]
+    out["speedup_of_balance"] = tot["mlp_ndiv"] / tot["mlp"]
+    return out
 
 
 def main():

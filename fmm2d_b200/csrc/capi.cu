@@ -75,6 +75,7 @@ LapArgs make_args(int fe, int nd, double eps, int64_t ns, const double* sources,
   a.hesstarg = hesstarg;
   if (o) {
     a.ndiv = o->ndiv;
+    a.lbal = o->level_balance;
     a.idivflag = o->idivflag;
     a.ifnear = o->ifnear;
     a.precision = o->precision;
@@ -777,6 +778,7 @@ void* b2fmm_plan_create(int fe, int nd, double eps, int64_t ns, const double* so
     a.ifpghtarg = ifpghtarg;
     if (opts) {
       a.ndiv = opts->ndiv;
+      a.lbal = opts->level_balance;
       a.idivflag = opts->idivflag;
       a.ifnear = opts->ifnear;
       a.precision = opts->precision;

@@ -238,8 +238,8 @@ namespace b2 {
 // In host code `g_direct_scratch` only names a host-side stand-in, not the
 // device address, so the first call on each device looks the address up with
 // cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture, and before the device's memory is
-// handed to another allocator: with CUDA's lazy module loading it may be the
+// first call before the device's memory is handed to another allocator: with
+// CUDA's lazy module loading it may be the
 // look-up that loads this module and reserves the array (or set
 // CUDA_MODULE_LOADING=EAGER).  All calls share the one array and it
 // keeps the last call's contents: the first kernel writes every element the

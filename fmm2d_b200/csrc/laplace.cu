@@ -1448,13 +1448,15 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   B2_CHECK(cudaEventCreate(&e0));
   B2_CHECK(cudaEventCreate(&e1));
   B2_CHECK(cudaEventRecord(e0, st));
-  p.dev = device_ranges && !own_stream;
+  // a level-balanced tree has no cached shape to size a one-attempt build:
+  // it is built with the host in the loop
+  p.dev = device_ranges && !own_stream && a.lbal == 0.0;
   if (p.dev)
     build_device_tree_async(p.T, a.src, p.ns, a.trg, p.nt, a.idivflag, ndiv, NLMAX,
                             tree_capacity_guess(p.ns + p.nt, ndiv, a.async_call ? 1.25 : 1.1),
                             st);
   else
-    build_device_tree(p.T, a.src, p.ns, a.trg, p.nt, a.idivflag, ndiv, NLMAX, st);
+    build_device_tree(p.T, a.src, p.ns, a.trg, p.nt, a.idivflag, ndiv, NLMAX, st, a.lbal);
   B2_CHECK(cudaEventRecord(e1, st));
   DeviceTree& T = p.T;
   if (!p.dev && T.bs0 == 0.0) {

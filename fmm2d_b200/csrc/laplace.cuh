@@ -32,6 +32,7 @@ struct LapArgs {
   double *pottarg = nullptr, *gradtarg = nullptr, *hesstarg = nullptr;
   // tuning (cfmm2d_ndiv.f:23-26)
   int ndiv = 0;  // <= 0: lndiv2d table
+  double lbal = 0.0;  // level balance of the leaf capacity (0: ndiv at every level)
   int idivflag = 0;
   int ifnear = 1;
   int precision = PREC_AUTO;

@@ -16,6 +16,8 @@
 // once, then builds the lists with one more kernel.
 #include "tree.cuh"
 
+#include <cmath>
+
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -274,6 +276,17 @@ __global__ void k_init_root(BoxPtrs B, const double* root, int ns, int nt, TreeC
 // ---------------------------------------------------------------------------
 // per-box steps of the build (pts_tree2d.f, tree_routs2d.f)
 // ---------------------------------------------------------------------------
+// Leaf capacity at level lev: ndiv (pts_tree2d.f), or, with a level balance
+// lbal != 0, ndiv 2^(lbal (lpiv - lev)) rounded (at least 1), lpiv the level
+// whose boxes would hold ndiv points of a uniform cloud: lbal > 0 lets
+// leaves above that level hold more points and splits boxes below it
+// sooner (more M2L, less P2P deep down), lbal < 0 the reverse.
+__device__ __forceinline__ int level_ndiv(int ndiv, float lbal, float lpiv, int lev) {
+  if (lbal == 0.f) return ndiv;
+  const float v = (float)ndiv * exp2f(lbal * (lpiv - (float)lev));
+  return v >= 2e9f ? 2000000000 : max(1, (int)(v + 0.5f));
+}
+
 // refine if the relevant count exceeds ndiv (pts_tree2d.f:538-560)
 __device__ __forceinline__ int refine_flag(const BoxPtrs& B, int b, int idivflag, int ndiv) {
   int nss = B.srng[b].y - B.srng[b].x, ntt = B.trng[b].y - B.trng[b].x;
@@ -785,7 +798,7 @@ __device__ bool colleagues_all(TreeCtl* C, BoxPtrs& B, int nl, int nb, F extra) 
 // C->cap boxes; TB_DEEP: levels beyond 32 need the 51-level keys).
 __global__ void __launch_bounds__(TB_THREADS, 1)
     k_tree_build(BoxPtrs B, BoxPtrs S, TreeCtl* C, int* flag, TreeKeys K, BoxHash H, int ns,
-                 int nt, int idivflag, int ndiv, int nlmax, int deep) {
+                 int nt, int idivflag, int ndiv, int nlmax, int deep, float lbal, float lpiv) {
   __shared__ int wsum[32];
   __shared__ int red[2];
   __shared__ int newf[NLMAX + 2];
@@ -805,11 +818,12 @@ __global__ void __launch_bounds__(TB_THREADS, 1)
     // phase A: refine flags and counts of own chunk
     const bool more = lev < nlmax;
     const Chunk ch = chunk_of(n);
+    const int ndl = level_ndiv(ndiv, lbal, lpiv, lev);
     int cnt = 0;
     if (more)
       for (int i0 = ch.c0; i0 < ch.c1; i0 += blockDim.x) {
         const int i = i0 + threadIdx.x;
-        const int fl = i < ch.c1 ? refine_flag(cur, f + i, idivflag, ndiv) : 0;
+        const int fl = i < ch.c1 ? refine_flag(cur, f + i, idivflag, ndl) : 0;
         if (i < ch.c1) flag[i] = fl;
         cnt += __syncthreads_count(fl);
       }
@@ -1188,7 +1202,7 @@ namespace {
 // One build attempt on st with capacity cap: box arrays, hash table and
 // scratch, the root, the persistent build kernel.  Outcome in T.ctl.
 void launch_tree_attempt(DeviceTree& T, long ns, long nt, int idivflag, int ndiv, int nlmax,
-                         int cap, cudaStream_t st) {
+                         int cap, cudaStream_t st, double lbal) {
   alloc_boxes(T, cap);
   DBuf<double2> sc(st);
   DBuf<int> sl(st), sp(st), sn(st), sf(st), flag(st);
@@ -1221,7 +1235,13 @@ void launch_tree_attempt(DeviceTree& T, long ns, long nt, int idivflag, int ndiv
   int* fp = flag.p;
   int nsi = (int)ns, nti = (int)nt;
   int deep = T.deep_sorted ? 1 : 0;
-  void* args[] = {&B, &S, &C, &fp, &K, &H, &nsi, &nti, &idivflag, &ndiv, &nlmax, &deep};
+  // pivot level of the level balance: where boxes of a uniform cloud of the
+  // counted points hold ndiv of them
+  const long npiv = idivflag == 0 ? ns : (idivflag == 1 ? nt : std::max(ns, nt));
+  float fl_bal = (float)lbal;
+  float fl_piv = (float)(0.5 * std::log2(std::max(1.0, (double)npiv / std::max(ndiv, 1))));
+  void* args[] = {&B, &S, &C, &fp, &K, &H, &nsi, &nti, &idivflag, &ndiv, &nlmax, &deep,
+                  &fl_bal, &fl_piv};
   B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_tree_build, dim3(tree_grid()),
                                        dim3(TB_THREADS), args, 0, st));
   // the scratch above is released stream-ordered after the kernel
@@ -1323,17 +1343,17 @@ int tree_capacity_guess(long npts, int ndiv, double margin) {
 
 void build_device_tree_async(DeviceTree& T, const double* src, long ns, const double* trg,
                              long nt, int idivflag, int ndiv, int nlmax, int cap,
-                             cudaStream_t st) {
+                             cudaStream_t st, double lbal) {
   tree_prologue(T, src, ns, trg, nt, st);
   cap = std::max(cap, 64);
-  launch_tree_attempt(T, ns, nt, idivflag, ndiv, nlmax, cap, st);
+  launch_tree_attempt(T, ns, nt, idivflag, ndiv, nlmax, cap, st, lbal);
   T.nboxes = cap;  // an upper bound until read back
   T.nlevels = -1;
   launch_lists(T, cap, st);
 }
 
 void build_device_tree(DeviceTree& T, const double* src, long ns, const double* trg, long nt,
-                       int idivflag, int ndiv, int nlmax, cudaStream_t st) {
+                       int idivflag, int ndiv, int nlmax, cudaStream_t st, double lbal) {
   tree_prologue(T, src, ns, trg, nt, st);
   // one persistent kernel builds the whole tree; it is re-run with more
   // capacity (or with the 51-level keys) when it reports that need
@@ -1345,7 +1365,7 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   double* hr = (double*)(hbuf + sizeof(TreeCtl));
   static_assert(sizeof(TreeCtl) % sizeof(double) == 0, "root after the control block");
   for (;;) {
-    launch_tree_attempt(T, ns, nt, idivflag, ndiv, nlmax, cap, st);
+    launch_tree_attempt(T, ns, nt, idivflag, ndiv, nlmax, cap, st, lbal);
     B2_CHECK(cudaMemcpyAsync(hc, T.ctl.p, sizeof(TreeCtl), cudaMemcpyDeviceToHost, st));
     B2_CHECK(cudaMemcpyAsync(hr, T.root.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     B2_CHECK(cudaStreamSynchronize(st));
@@ -1375,7 +1395,8 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
   T.bs0 = hc->bs[0];
   T.cx0 = hr[0];
   T.cy0 = hr[1];
-  note_tree_shape(ns + nt, ndiv, T.nboxes, T.nlevels);
+  // the shape cache is keyed by (points, ndiv): level-balanced trees stay out
+  if (lbal == 0.0) note_tree_shape(ns + nt, ndiv, T.nboxes, T.nlevels);
   launch_lists(T, T.nboxes, st);
 }
 

@@ -127,8 +127,11 @@ struct DeviceTree {
 // Build the level-restricted tree of sources `src` (2*ns doubles, x/y
 // interleaved) and targets `trg` on stream `st`.  idivflag 0/1/2 subdivides
 // on sources / targets / max of both, as in the reference.
+// lbal: level balance of the leaf capacity (0: ndiv at every level, as the
+// reference; otherwise ndiv 2^(lbal (lpiv - level)), lpiv the level whose
+// boxes hold ndiv points of a uniform cloud of the counted points).
 void build_device_tree(DeviceTree& T, const double* src, long ns, const double* trg, long nt,
-                       int idivflag, int ndiv, int nlmax, cudaStream_t st);
+                       int idivflag, int ndiv, int nlmax, cudaStream_t st, double lbal = 0.0);
 
 // The same build enqueued on `st` without any host synchronisation: one
 // attempt with capacity `cap` boxes and the first 32 key levels.  The tree
@@ -136,7 +139,8 @@ void build_device_tree(DeviceTree& T, const double* src, long ns, const double* 
 // TB_DEEP (more than 32 levels) need build_device_tree instead, and every
 // pass that reads its ranges from T.ctl does nothing after such a failure.
 void build_device_tree_async(DeviceTree& T, const double* src, long ns, const double* trg,
-                             long nt, int idivflag, int ndiv, int nlmax, int cap, cudaStream_t st);
+                             long nt, int idivflag, int ndiv, int nlmax, int cap, cudaStream_t st,
+                             double lbal = 0.0);
 
 // Shapes of earlier trees by (points, leaf size): the box count and depth a
 // call can expect without reading its tree back.  note_tree_shape records a

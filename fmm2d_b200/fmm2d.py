@@ -11,8 +11,11 @@ in ``libfmm2d_b200.so`` on the GPU; there is no CPU fallback.
 Optional keyword extensions (not in the reference, defaults reproduce it):
 ``precision`` ('auto' = mixed when eps >= 1e-6, 'fp64', 'mixed'), ``ndiv``
 (leaf capacity override, or 'auto' for the learned cost model of
-fmm2d_b200/costmodel.py) and ``timeinfo`` (a length-8 float64 numpy array
-that receives the per-step device times).
+fmm2d_b200/costmodel.py, which then also picks the level balance),
+``level_balance`` (Laplace: the leaf capacity at level l is
+ndiv 2^(b (lp - l)), lp the level whose boxes hold ndiv points of a uniform
+cloud; 0, the default, keeps ndiv at every level) and ``timeinfo`` (a
+length-8 float64 numpy array that receives the per-step device times).
 """
 import ctypes as C
 
@@ -89,17 +92,18 @@ class _TH:
         return a.permute(*perm)
 
 
-def _options(precision, ndiv):
+def _options(precision, ndiv, level_balance=0.0):
     o = _lib.Options()
     o.ndiv = int(ndiv) if ndiv else 0
     o.idivflag = 0
     o.ifnear = 1
     o.precision = _lib.PREC[precision]
+    o.level_balance = float(level_balance or 0.0)
     return o
 
 
 def _lap_run(fe, eps, sources, charges, dipstr, dipvec, targets, ifpgh, ifpghtarg, nd,
-             precision="auto", ndiv=None, timeinfo=None):
+             precision="auto", ndiv=None, timeinfo=None, level_balance=0.0):
     """One Cauchy-engine FMM call; returns user-shaped outputs and ier."""
     torch_mode = _is_torch(sources)
     B = _TH if torch_mode else _NP
@@ -126,13 +130,14 @@ def _lap_run(fe, eps, sources, charges, dipstr, dipvec, targets, ifpgh, ifpghtar
     gradt = B.empty(gshape(nt), dt, **kw) if ifpghtarg >= 2 and nt else None
     hesst = B.empty(hshape(nt), dt, **kw) if ifpghtarg >= 3 and nt else None
     if ndiv == "auto":
-        # leaf size from the learned cost model (lndiv2d table without weights)
+        # leaf size and level balance from the learned cost model (lndiv2d
+        # table, balance 0, without weights)
         import torch
         from . import costmodel
         dsrc = s if torch_mode else torch.as_tensor(s, device="cuda")
         dtrg = None if t is None else (t if torch_mode else torch.as_tensor(t, device="cuda"))
-        ndiv = costmodel.auto_ndiv(dsrc, dtrg, eps)
-    opts = _options(precision, ndiv)
+        ndiv, level_balance = costmodel.auto_tree(dsrc, dtrg, eps)
+    opts = _options(precision, ndiv, level_balance)
     ti = np.zeros(8) if timeinfo is None else timeinfo
     ier = C.c_int(0)
     L = _lib.lib()

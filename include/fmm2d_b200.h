@@ -40,6 +40,13 @@ typedef struct b2fmm_options {
                      the stream, with no host wait; device-side failures are
                      reported by b2fmm_async_status.  Ignored (synchronous)
                      when timeinfo or statistics are requested. */
+  double level_balance; /* Laplace only (no counterpart in the reference):
+                     0 keeps the leaf capacity ndiv at every level; otherwise
+                     a box of level l is split above ndiv 2^(b (lp - l))
+                     points (rounded, at least 1), lp the level whose boxes
+                     hold ndiv points of a uniform cloud of the counted
+                     points: b > 0 lets leaves above lp hold more points and
+                     splits boxes below it sooner, b < 0 the reverse. */
 } b2fmm_options;
 
 /* Library version string. */
@@ -148,8 +155,8 @@ void b2fmm_lap_direct_dev(int kind, int nd, int64_t ns, const double* sources,
  * loads the library holds until exit.  Limit: nt*3 (kind 0) or nt*6
  * (kinds 1, 2) <= 262144, i.e. at most 87381 / 43690 targets per call;
  * larger nt returns ier = 103 without computing.  The first call on a device
- * looks up the array's device address, so make it before any stream capture,
- * and before the device's memory is handed to another allocator: with lazy
+ * looks up the array's device address, so make it before the device's memory
+ * is handed to another allocator: with lazy
  * module loading that look-up may be what reserves the array (ier = 4 when
  * the device has no room left; CUDA_MODULE_LOADING=EAGER reserves it at
  * load).  All calls share the array: calls that overlap on the GPU race on

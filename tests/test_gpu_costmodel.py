@@ -135,3 +135,30 @@ def test_front_end_auto_ndiv(gpu):
     b = fmm.rfmm2d(eps=1e-6, sources=src, charges=q, pg=2)
     assert a.ier == 0
     assert rel_l2(a.pot, b.pot) < 1e-6 and rel_l2(a.grad, b.grad) < 1e-6
+
+
+@pytest.mark.parametrize("balance", [-0.5, 0.5])
+def test_level_balance_changes_the_tree_not_the_accuracy(gpu, balance):
+    """A nonzero level balance builds a different tree (the leaf capacity
+    varies by level) and the FMM stays within eps of the FP64 direct sum,
+    for the mixed and the FP64 path."""
+    import torch
+    import fmm2d_b200 as fmm
+    from conftest import rel_l2
+    src, q = cm.make_problem("mixture", 120000, 5)
+    L = _lib.lib()
+    boxes = {}
+    for b in (0.0, balance):
+        L.b2fmm_set_stats(1)
+        out = fmm.rfmm2d(eps=1e-6, sources=src, charges=q, pg=2, level_balance=b)
+        L.b2fmm_set_stats(0)
+        boxes[b] = _lib.get_stats()["nboxes"]
+        assert out.ier == 0
+        idx = np.sort(np.random.default_rng(1).choice(src.shape[1], 300, replace=False))
+        ex = fmm.r2ddir(sources=src, targets=src[:, idx], charges=q, pgt=2)
+        assert rel_l2(out.pot[idx], ex.pottarg) < 1e-6
+        assert rel_l2(out.grad[:, idx], ex.gradtarg) < 1e-6
+        o64 = fmm.rfmm2d(eps=1e-6, sources=src, charges=q, pg=2, level_balance=b,
+                         precision="fp64")
+        assert rel_l2(o64.pot[idx], ex.pottarg) < 1e-6
+    assert boxes[balance] != boxes[0.0]
