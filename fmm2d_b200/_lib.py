@@ -76,6 +76,8 @@ SIGNATURES = {
     "b2fmm_get_stats": [P, c_int],
     "b2fmm_fma_peak": [c_int],
     "b2fmm_set_m2l_tensor_cores": [c_int],
+    "b2fmm_set_p2p_shape": [c_int, c_int],
+    "b2fmm_get_p2p_shape": [c_int],
     "b2fmm_mlp_param_count": [c_int, c_int, c_int],
     "b2fmm_mlp_forward": [P, c_int, c_int, c_int, c_int, P, P, P, P],
     "b2fmm_mlp_gradient": [P, P, c_int, c_int, c_int, c_int, P, P, P, P, P],
@@ -125,7 +127,12 @@ def lib():
         L.b2fmm_batch_graph_create.restype = c_void_p
         L.b2fmm_batch_graph_status.restype = c_int
         L.b2fmm_batch_graph_nodes.restype = C.c_int64
+        L.b2fmm_set_p2p_shape.restype = c_int
+        L.b2fmm_get_p2p_shape.restype = c_int
         _lib = L
+        # the autotuner's committed near-field tile shapes (fmm2d_b200/autotune.py)
+        from . import autotune
+        autotune.apply(autotune.load(), L)
     return _lib
 
 

@@ -998,6 +998,10 @@ void b2fmm_point_stats(const double* sources, int64_t ns, const double* targ, in
 
 void b2fmm_set_m2l_tensor_cores(int on) { set_m2l_tensor_cores(on != 0); }
 
+int b2fmm_set_p2p_shape(int leaf_class, int shape) { return set_p2p_shape(leaf_class, shape); }
+
+int b2fmm_get_p2p_shape(int leaf_class) { return p2p_shape(leaf_class); }
+
 void b2fmm_tc_gemm_probe(const float* a_dev, const float* b_dev, int k, int n, float* d_dev,
                          void* stream, int* ier) {
   guarded(ier, [&] { return tc_gemm_probe(a_dev, b_dev, k, n, d_dev, (cudaStream_t)stream); });

@@ -387,13 +387,20 @@ __global__ void __launch_bounds__(128, FAR_MIN_BLOCKS(ND, IFPGH)) k_far_mixed(
   }
 }
 
-// Register budget of the near-field pass: 6 blocks of 128 threads per SM
-// (at most 80 registers a thread) for one or two densities without
-// hessians; the compiler's choice otherwise.
-#ifndef P2P_MB
-#define P2P_MB 6
-#endif
-#define P2P_MIN_BLOCKS(ND, IFPGH) ((ND) <= 2 && (IFPGH) <= 2 ? P2P_MB : 1)
+// Tile shapes of the near-field pass (k_p2p_leaf), chosen per leaf-size
+// class by the autotuner (fmm2d_b200/autotune.py, b2fmm_set_p2p_shape):
+// sources staged per warp and chunk, unrolling of the pair loop, and the
+// resident blocks of 128 threads per SM asked of the register allocator
+// (for one or two densities without hessians; the compiler's choice and
+// shape 0 otherwise).
+struct P2PShape {
+  int chunk, unroll, min_blocks;
+};
+constexpr P2PShape P2P_SHAPES[] = {{128, 2, 6}, {64, 2, 8}, {128, 4, 5}};
+constexpr int P2P_NSHAPES = 3;
+static_assert(P2P_NSHAPES == B2FMM_P2P_SHAPES, "shape table and C ABI agree");
+constexpr bool p2p_tuned(int ND, int IFPGH) { return ND <= 2 && IFPGH <= 2; }
+#define P2P_MIN_BLOCKS(ND, IFPGH, V) (p2p_tuned(ND, IFPGH) ? P2P_SHAPES[V].min_blocks : 1)
 
 // Grid of a persistent pass: every SM filled with as many blocks as fit.
 template <typename K>
@@ -435,14 +442,6 @@ int resident_grid(K kernel, int threads, size_t smem) {
 // Per-pair terms are summed in FP32 over at most 32 sources, those partial
 // sums in FP64, and added to the far field already in the outputs.  KIND: 1
 // charges, 2 dipoles, 3 both.
-#ifndef P2P_CHUNK
-#define P2P_CHUNK 128
-#endif
-constexpr int P2P_CH = P2P_CHUNK;  // staged sources per warp and chunk
-#ifndef P2P_UNR
-#define P2P_UNR 2
-#endif
-constexpr int P2P_UNROLL = P2P_UNR;
 static_assert(MNLIST1 <= 16, "list-1 search below covers 16 boxes");
 
 __device__ __forceinline__ void split_hilo(double x, float& hi, float& lo) {
@@ -471,13 +470,13 @@ static_assert(offsetof(P2PItem, lpre) == offsetof(P2PItem, lst) + 16 * sizeof(in
               "lst and lpre are read as 32 consecutive ints");
 
 // Shared memory of one warp: staged sources and one leaf's list-1 ranges.
-template <int ND, int KIND>
+template <int ND, int KIND, int CH>
 struct P2PWarp {
-  P2PSrc<ND, KIND> s[P2P_CH];
+  P2PSrc<ND, KIND> s[CH];
   int lst[16];   // list-1 source range starts
   int lpre[16];  // exclusive prefix of the list-1 range lengths (follows lst)
 };
-using P2PWarp11 = P2PWarp<1, 1>;
+using P2PWarp11 = P2PWarp<1, 1, 64>;
 static_assert(offsetof(P2PWarp11, lpre) == offsetof(P2PWarp11, lst) + 16 * sizeof(int),
               "lst and lpre are written as 32 consecutive ints");
 
@@ -538,8 +537,8 @@ __global__ void k_p2p_items(TV t, int nb, int use_targets, P2PItem* __restrict__
   }
 }
 
-template <int ND, int IFPGH, int KIND>
-__global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
+template <int ND, int IFPGH, int KIND, int V>
+__global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH, V)) k_p2p_leaf(
     TV t, const double2* __restrict__ xs64, const double2* __restrict__ xe64,
     const float2* __restrict__ q32, const float2* __restrict__ d32, int ndc, int d0,
     double thresh, const P2PItem* __restrict__ items, const int* __restrict__ nitems,
@@ -550,7 +549,8 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
   extern __shared__ float4 p2p_sm[];
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  P2PWarp<ND, KIND>& W = ((P2PWarp<ND, KIND>*)p2p_sm)[wib];
+  constexpr int CH = P2P_SHAPES[V].chunk, UNROLL = P2P_SHAPES[V].unroll;
+  P2PWarp<ND, KIND, CH>& W = ((P2PWarp<ND, KIND, CH>*)p2p_sm)[wib];
   // after a failed tree build the item list is empty
   const int ni = t.ctl->status == TB_OK ? *nitems : 0;
   const double thr = near_thresh(t, thresh);
@@ -580,7 +580,7 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
     const float lsc = (float)((double)ex * 0.69314718055994530942);
     __syncwarp();
     // at most 32 sources per lane and chunk: one FP32 partial sum each
-    const int cap = min(P2P_CH, 32 * nph);
+    const int cap = min(CH, 32 * nph);
     float2 zh, zl;
     {
       const double2 z = xe64[k];
@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
         // with itself, nearly coincident or excluded pairs) adds nothing
         // here and is counted; such pairs are formed after the item
         const P2PSrc<ND, KIND>* const Rend = W.s + m;
-#pragma unroll P2P_UNROLL
+#pragma unroll UNROLL
         for (const P2PSrc<ND, KIND>* R = W.s + ph; R < Rend; R += nph) {
           const float4 p = R->p;
           const float dx = (zh.x - p.x) + (zl.x - p.z);
@@ -798,17 +798,40 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH)) k_p2p_leaf(
   }
 }
 
-template <int ND, int IFPGH, int KIND>
-void p2p_launch(const TV& t, const MixedData& M, const double2* xe64, int ndc, int d0,
-                double thresh, const P2PItem* items, const int* nitems, double2* pot,
-                double2* grad, double2* hess, cudaStream_t st) {
-  constexpr size_t sm = 4 * sizeof(P2PWarp<ND, KIND>);
-  auto kern = k_p2p_leaf<ND, IFPGH, KIND>;
+std::atomic<int> g_p2p_shape[B2FMM_P2P_CLASSES] = {};
+
+template <int ND, int IFPGH, int KIND, int V>
+void p2p_launch_v(const TV& t, const MixedData& M, const double2* xe64, int ndc, int d0,
+                  double thresh, const P2PItem* items, const int* nitems, double2* pot,
+                  double2* grad, double2* hess, cudaStream_t st) {
+  constexpr size_t sm = 4 * sizeof(P2PWarp<ND, KIND, P2P_SHAPES[V].chunk>);
+  auto kern = k_p2p_leaf<ND, IFPGH, KIND, V>;
   set_smem_attr(kern, sm);
   kern<<<resident_grid(kern, 128, sm), 128, sm, st>>>(t, M.xs64, xe64, M.q.p, M.d.p, ndc, d0,
                                                      thresh, items, nitems,
                                                      xe64 == M.xs64 ? 1 : 0, pot, grad, hess);
   B2_LAUNCH_CHECK();
+}
+
+template <int ND, int IFPGH, int KIND>
+void p2p_launch(const TV& t, const MixedData& M, const double2* xe64, int ndc, int d0,
+                double thresh, const P2PItem* items, const int* nitems, double2* pot,
+                double2* grad, double2* hess, cudaStream_t st) {
+  const int v = p2p_tuned(ND, IFPGH) ? g_p2p_shape[p2p_leaf_class(M.ndiv)].load() : 0;
+  if constexpr (p2p_tuned(ND, IFPGH)) {
+    if (v == 1) {
+      p2p_launch_v<ND, IFPGH, KIND, 1>(t, M, xe64, ndc, d0, thresh, items, nitems, pot, grad,
+                                       hess, st);
+      return;
+    }
+    if (v == 2) {
+      p2p_launch_v<ND, IFPGH, KIND, 2>(t, M, xe64, ndc, d0, thresh, items, nitems, pot, grad,
+                                       hess, st);
+      return;
+    }
+  }
+  p2p_launch_v<ND, IFPGH, KIND, 0>(t, M, xe64, ndc, d0, thresh, items, nitems, pot, grad, hess,
+                                   st);
 }
 
 int grid_for(long nitems, int wpb) {
@@ -884,10 +907,11 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
   B2_LAUNCH_CHECK();
 }
 
-void lap_mixed_leaves(MixedData& M, const TV& t, int nb, bool dev, long ns, long nt,
+void lap_mixed_leaves(MixedData& M, const TV& t, int nb, bool dev, long ns, long nt, int ndiv,
                       cudaStream_t st) {
   M.ns = ns;
   M.nt = nt;
+  M.ndiv = ndiv;
   M.leaf_s.alloc(ns, st);
   k_point_leaf<<<ceil_div(nb, 128), 128, 0, st>>>(t, dev ? -1 : nb, 0, M.leaf_s.p);
   B2_LAUNCH_CHECK();
@@ -924,6 +948,19 @@ void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, lon
 
 namespace {
 std::atomic<bool> g_m2l_tc{true};
+}
+
+int p2p_leaf_class(int ndiv) { return ndiv <= 20 ? 0 : (ndiv <= 56 ? 1 : 2); }
+
+int set_p2p_shape(int leaf_class, int shape) {
+  if (leaf_class < 0 || leaf_class >= B2FMM_P2P_CLASSES || shape < 0 || shape >= P2P_NSHAPES)
+    return IER_BADARG;
+  g_p2p_shape[leaf_class].store(shape);
+  return IER_OK;
+}
+
+int p2p_shape(int leaf_class) {
+  return leaf_class < 0 || leaf_class >= B2FMM_P2P_CLASSES ? -1 : g_p2p_shape[leaf_class].load();
 }
 
 void set_m2l_tensor_cores(bool on) { g_m2l_tc.store(on); }

@@ -3,6 +3,7 @@
 // differences; expansions, shifts, L2P and M2P stay FP64.
 #pragma once
 #include "lap_common.cuh"
+#include "../../include/fmm2d_b200.h"
 #include "tc_m2l.cuh"
 
 namespace b2 {
@@ -21,6 +22,7 @@ struct MixedData {
   int nlev = 0;         // tree levels + 1
   int nboxes = 0;
   long ns = 0, nt = 0;
+  int ndiv = 0;         // leaf capacity of the tree (selects the near-field tile shape)
   DBuf<int> leaf_s, leaf_t;     // leaf box of every sorted source / target
   DBuf<char> items_s, items_t;  // near-field work items (sources, targets)
   DBuf<int> nitems;              // their counts
@@ -41,7 +43,13 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
 // (once per tree); nb boxes at most, the box count read from the tree's
 // device control block when dev.
 void lap_mixed_leaves(MixedData& M, const lapk::TV& t, int nb, bool dev, long ns, long nt,
-                      cudaStream_t st);
+                      int ndiv, cudaStream_t st);
+
+// Near-field tile shape per leaf-size class (0: ndiv <= 20, 1: <= 56,
+// 2: larger); set_p2p_shape returns IER_BADARG for an unknown class or shape.
+int p2p_leaf_class(int ndiv);
+int set_p2p_shape(int leaf_class, int shape);
+int p2p_shape(int leaf_class);
 
 // FP32 copies of the sorted densities (every evaluation).
 void lap_mixed_densities(MixedData& M, const double2* qs, const double2* ds, long ns, int ndc,

@@ -1504,7 +1504,7 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   if (p.mixed) {
     lap_mixed_prepare(p.MD, p.xs.p, p.ns, p.xt.p, p.nt, p.fc, p.fd, p.ndc, 0.0, 0.0, p.P, st);
     p.MD.err = p.err.p;
-    lap_mixed_leaves(p.MD, p.tv, nb, p.dev, p.ns, p.nt, st);
+    lap_mixed_leaves(p.MD, p.tv, nb, p.dev, p.ns, p.nt, p.ndiv, st);
     const bool levels_ok = p.dev || (T.nlevels >= 2 && T.nlevels < 64);
     if (levels_ok && m2l_tensor_cores() && m2l_tc_supported(p.P)) {
       p.MD.tc = true;

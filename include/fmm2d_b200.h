@@ -343,6 +343,22 @@ void b2fmm_mlp_train(const float* x, const float* target, int batch, int nin, in
 void b2fmm_point_stats(const double* sources, int64_t ns, const double* targ, int64_t nt,
                        unsigned* hist, void* stream, int* ier);
 
+/* ------------------------------------------------ near-field tile shapes (no reference counterpart) */
+
+/* The mixed-precision near-field kernel comes in B2FMM_P2P_SHAPES tile
+ * shapes (0: 128 staged sources per warp, pair loop unrolled twice, 6 blocks
+ * per SM; 1: 64 sources, twice, 8 blocks; 2: 128 sources, four times, 5
+ * blocks), one chosen per leaf-size class (0: ndiv <= 20, 1: ndiv <= 56, 2:
+ * larger).  Shape 0 everywhere until set; fmm2d_b200/autotune.py times the
+ * shapes and the Python package applies its committed choice at load.
+ * Results of different shapes agree to FP32 round-off (the staged chunk
+ * bounds the FP32 partial sums).  Process-wide; set returns 0 or 100 (an
+ * unknown class or shape), get returns the shape or -1. */
+#define B2FMM_P2P_SHAPES 3
+#define B2FMM_P2P_CLASSES 3
+int b2fmm_set_p2p_shape(int leaf_class, int shape);
+int b2fmm_get_p2p_shape(int leaf_class);
+
 /* ------------------------------------------------- tensor-core M2L (no reference counterpart) */
 
 /* Mixed-precision Laplace M2L engine switch: 1 (default) runs the list-2

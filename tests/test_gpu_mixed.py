@@ -112,3 +112,36 @@ def test_mixed_close_pairs_duplicates_and_targets(gpu, oracle):
     ext = oracle.l2ddir(src, trg, charges=q, dipstr=d, dipvec=v, ifpgh=2)
     assert rel_l2(out.pottarg, ext["pottarg"][0]) < 1e-6
     assert rel_l2(out.gradtarg, ext["gradtarg"][0]) < 1e-6
+
+
+def test_near_field_tile_shapes_agree(gpu, oracle):
+    """Every near-field tile shape, on every leaf-size class, gives the same
+    result as shape 0 to FP32 round-off and stays within eps of the oracle;
+    unknown classes or shapes are refused."""
+    from fmm2d_b200 import _lib, autotune
+    L = _lib.lib()
+    saved = [L.b2fmm_get_p2p_shape(c) for c in range(autotune.NCLASSES)]
+    assert L.b2fmm_set_p2p_shape(3, 0) == 100 and L.b2fmm_set_p2p_shape(0, 3) == 100
+    assert L.b2fmm_get_p2p_shape(-1) == -1
+    rng = np.random.default_rng(12)
+    n = 30000
+    src = _gauss16(rng, n)
+    q = rng.normal(size=n) + 1j * rng.normal(size=n)
+    d = rng.normal(size=n) + 1j * rng.normal(size=n)
+    v = rng.uniform(-1, 1, (2, n))
+    ref = oracle.lfmm2d(1e-6, src, charges=q, dipstr=d, dipvec=v, ifpgh=2)
+    try:
+        for c, nd in enumerate(autotune.CLASS_NDIV):
+            outs = []
+            for s in range(len(autotune.SHAPES)):
+                assert L.b2fmm_set_p2p_shape(c, s) == 0 and L.b2fmm_get_p2p_shape(c) == s
+                o = fmm.lfmm2d(eps=1e-6, sources=src, charges=q, dipstr=d, dipvec=v, pg=2,
+                               precision="mixed", ndiv=nd)
+                assert o.ier == 0
+                outs.append(o)
+            for o in outs:
+                assert rel_l2(o.pot, outs[0].pot) < 1e-7 and rel_l2(o.grad, outs[0].grad) < 1e-7
+            assert rel_l2(outs[0].grad, ref["grad"]) < 1e-6
+    finally:
+        for c, s in enumerate(saved):
+            L.b2fmm_set_p2p_shape(c, s)
