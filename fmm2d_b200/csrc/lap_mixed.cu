@@ -20,6 +20,7 @@
 
 #include <atomic>
 #include <cstddef>
+#include <type_traits>
 #include "laplace.cuh"
 
 namespace b2 {
@@ -401,6 +402,164 @@ constexpr int P2P_NSHAPES = 3;
 static_assert(P2P_NSHAPES == B2FMM_P2P_SHAPES, "shape table and C ABI agree");
 constexpr bool p2p_tuned(int ND, int IFPGH) { return ND <= 2 && IFPGH <= 2; }
 #define P2P_MIN_BLOCKS(ND, IFPGH, V) (p2p_tuned(ND, IFPGH) ? P2P_SHAPES[V].min_blocks : 1)
+
+// Far field of the mixed path in FP32, one evaluation point per thread:
+// L2P from the leaf's local expansion (FP64, rounded to FP32 on load) and
+// M2P from the FP32 copy of the multipoles that the tensor-core M2L makes
+// (mp32: [box][ND][KH] complex, zero beyond P).  Point-to-centre
+// differences are formed in FP64 and rounded once; Horner, the complex
+// reciprocal and log|z - c| (SFU) in FP32; the sums go to FP64 outputs.
+// Relative error ~1e-7 of the far field, below the eps >= 1e-6 the mixed
+// path serves.  Writes pot / grad / hess of the point.
+__device__ __forceinline__ float2 f2_(double2 a) { return make_float2((float)a.x, (float)a.y); }
+__device__ __forceinline__ float2 caddf_(float2 a, float2 b) {
+  return make_float2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ float2 cmaf_(float2 a, float2 b, float2 c) {  // a b + c
+  return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+
+template <int ND, int IFPGH>
+__global__ void __launch_bounds__(128, FAR_MIN_BLOCKS(ND, IFPGH)) k_far_f32(
+    TV t, long n, const int* __restrict__ leaf, const double2* __restrict__ xe64, int ndc, int d0,
+    int P, int KH, const float2* __restrict__ mp32, const double2* __restrict__ lo,
+    double2* __restrict__ pot, double2* __restrict__ grad, double2* __restrict__ hess) {
+  long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n || t.ctl->status != TB_OK) return;
+  const int b = leaf[k];
+  const int lev = t.level[b];
+  const double r = t.boxsize[lev];
+  const double2 cb = t.center[b];
+  const double2 z = xe64[k];
+  float2 pt[ND], gr[ND], hs[ND];
+  {
+    const double2* L = lo + (size_t)b * P * ND;
+    const double ri = 1.0 / r;
+    const float2 zz = make_float2((float)((z.x - cb.x) * ri), (float)((z.y - cb.y) * ri));
+    float2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      f[d] = f2_(L[(P - 1) * ND + d]);
+      f1[d] = f2[d] = make_float2(0.f, 0.f);
+    }
+    auto step = [&](const float2 (&c)[ND]) {
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        if (IFPGH >= 3) f2[d] = cmaf_(f2[d], zz, f1[d]);
+        if (IFPGH >= 2) f1[d] = cmaf_(f1[d], zz, f[d]);
+        f[d] = cmaf_(f[d], zz, c[d]);
+      }
+    };
+    int m = P - 2;
+    for (; m >= 3; m -= 4) {
+      float2 c0[ND], c1[ND], c2[ND], c3[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        c0[d] = f2_(L[m * ND + d]);
+        c1[d] = f2_(L[(m - 1) * ND + d]);
+        c2[d] = f2_(L[(m - 2) * ND + d]);
+        c3[d] = f2_(L[(m - 3) * ND + d]);
+      }
+      step(c0);
+      step(c1);
+      step(c2);
+      step(c3);
+    }
+    for (; m >= 0; m--) {
+      float2 c0[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) c0[d] = f2_(L[m * ND + d]);
+      step(c0);
+    }
+    const float rif = (float)ri;
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      pt[d] = f[d];
+      gr[d] = IFPGH >= 2 ? make_float2(f1[d].x * rif, f1[d].y * rif) : make_float2(0.f, 0.f);
+      hs[d] = IFPGH >= 3 ? make_float2(f2[d].x * 2.f * rif * rif, f2[d].y * 2.f * rif * rif)
+                         : make_float2(0.f, 0.f);
+    }
+  }
+  const int n3 = t.nl3[b];
+  const float rj = (float)t.boxsize[lev + 1], irj = 1.f / rj;
+  for (int e = 0; e < n3; e++) {
+    // M2P: c_0 log(z - c) + sum_{m>=1} c_m (r_j / (z - c))^m
+    const int jb = t.l3[(size_t)MNLIST3 * b + e];
+    const double2 cj = t.center[jb];
+    const float2 zc = make_float2((float)(z.x - cj.x), (float)(z.y - cj.y));
+    const float q2 = fmaf(zc.x, zc.x, zc.y * zc.y);
+    const float iq = __fdividef(1.f, q2);
+    const float2 zi = make_float2(zc.x * iq, -zc.y * iq);
+    const float2 w = make_float2(rj * zi.x, rj * zi.y);
+    const float lg = 0.5f * __logf(q2);
+    const float2* M = mp32 + (size_t)jb * ND * KH;
+    float2 f[ND], f1[ND], f2[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      f[d] = M[d * KH + P - 1];
+      f1[d] = f2[d] = make_float2(0.f, 0.f);
+    }
+    auto mstep = [&](const float2 (&c)[ND]) {
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        if (IFPGH >= 3) f2[d] = cmaf_(f2[d], w, f1[d]);
+        if (IFPGH >= 2) f1[d] = cmaf_(f1[d], w, f[d]);
+        f[d] = cmaf_(f[d], w, c[d]);
+      }
+    };
+    int m = P - 2;
+    for (; m >= 4; m -= 4) {
+      float2 c0[ND], c1[ND], c2[ND], c3[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        c0[d] = M[d * KH + m];
+        c1[d] = M[d * KH + m - 1];
+        c2[d] = M[d * KH + m - 2];
+        c3[d] = M[d * KH + m - 3];
+      }
+      mstep(c0);
+      mstep(c1);
+      mstep(c2);
+      mstep(c3);
+    }
+    for (; m >= 1; m--) {
+      float2 c0[ND];
+#pragma unroll
+      for (int d = 0; d < ND; d++) c0[d] = M[d * KH + m];
+      mstep(c0);
+    }
+    const float2 w2 = cmulf_(w, w);
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      const float2 c0 = M[d * KH];
+      const float2 Sv = cmulf_(w, f[d]);
+      const float2 S1 = caddf_(f[d], cmulf_(w, f1[d]));
+      pt[d].x += Sv.x + c0.x * lg;
+      pt[d].y += Sv.y + c0.y * lg;
+      if (IFPGH >= 2) {
+        const float2 gg = cmulf_(S1, w2);
+        gr[d] = caddf_(gr[d], caddf_(make_float2(-gg.x * irj, -gg.y * irj), cmulf_(c0, zi)));
+      }
+      if (IFPGH >= 3) {
+        const float2 S2p = caddf_(f1[d], cmulf_(w, f2[d]));
+        const float2 S2 = make_float2(2.f * S2p.x, 2.f * S2p.y);
+        const float2 w3 = cmulf_(w2, w), w4 = cmulf_(w2, w2);
+        const float2 S1w3 = cmulf_(S1, w3);
+        float2 hh = caddf_(cmulf_(S2, w4), make_float2(2.f * S1w3.x, 2.f * S1w3.y));
+        hh = make_float2(hh.x * irj * irj, hh.y * irj * irj);
+        const float2 c0zz = cmulf_(c0, cmulf_(zi, zi));
+        hs[d] = caddf_(hs[d], make_float2(hh.x - c0zz.x, hh.y - c0zz.y));
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < ND; d++) {
+    const size_t o = (size_t)k * ndc + d0 + d;
+    pot[o] = make_double2(pt[d].x, pt[d].y);
+    if (IFPGH >= 2) grad[o] = make_double2(gr[d].x, gr[d].y);
+    if (IFPGH >= 3) hess[o] = make_double2(hs[d].x, hs[d].y);
+  }
+}
 
 // Grid of a persistent pass: every SM filled with as many blocks as fit.
 template <typename K>
@@ -798,6 +957,178 @@ __global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH, V)) k_p2p_leaf(
   }
 }
 
+// Near field of the FP64 path (cauchykernels2d.f), on the same work items
+// and lane mapping as k_p2p_leaf: sources staged as FP64 coordinates and
+// densities, pair differences, terms and sums in FP64 as the reference, the
+// pairs at r <= thresh (r < thresh with gradients) left out by a select,
+// not a branch.  Adds to the far field already in the outputs.
+template <int ND, int KIND>
+struct P2PSrc64 {
+  double2 p;
+  double2 c[ND * ((KIND & 1) + ((KIND >> 1) & 1))];
+};
+
+template <int ND, int KIND>
+struct P2PWarp64 {
+  P2PSrc64<ND, KIND> s[64];
+  int lst[16];
+  int lpre[16];
+};
+
+template <int ND, int IFPGH, int KIND>
+__global__ void __launch_bounds__(128) k_p2p_leaf64(
+    TV t, const double2* __restrict__ xs64, const double2* __restrict__ xe64,
+    const double2* __restrict__ q64, const double2* __restrict__ d64, int ndc, int d0,
+    double thresh, const P2PItem* __restrict__ items, const int* __restrict__ nitems,
+    double2* __restrict__ pot, double2* __restrict__ grad, double2* __restrict__ hess) {
+  constexpr bool HQ = KIND & 1, HD = (KIND >> 1) & 1;
+  constexpr int DOFF = HQ ? ND : 0;
+  constexpr int CH = 64;
+  extern __shared__ float4 p2p_sm[];
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  P2PWarp64<ND, KIND>& W = ((P2PWarp64<ND, KIND>*)p2p_sm)[wib];
+  const int ni = t.ctl->status == TB_OK ? *nitems : 0;
+  const double thr = near_thresh(t, thresh);
+  const double th2 = thr * thr;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int it = blockIdx.x * (blockDim.x >> 5) + wib; it < ni; it += nw) {
+    const P2PItem& I = items[it];
+    ((int*)W.lst)[lane] = ((const int*)I.lst)[lane];
+    const int4 h = *(const int4*)&I;
+    const int n1 = h.z >> 8, ntc = h.z & 255;
+    const int S = I.S;
+    const float rn = __frcp_rn((float)ntc);
+    const int nph = __float2int_rz(32.5f * rn);
+    const int ph = __float2int_rz(((float)lane + 0.5f) * rn), ti = lane - ph * ntc;
+    const bool act = ph < nph;
+    const long k = (long)h.y + ti;
+    __syncwarp();
+    const double2 z = xe64[k];
+    double2 pt[ND], gr[ND], hs[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
+    for (int u0 = 0; u0 < S; u0 += CH) {
+      const int m = min(CH, S - u0);
+      for (int i = lane; i < m; i += 32) {
+        const int u = u0 + i;
+        int e = 0;
+#pragma unroll
+        for (int step = 8; step > 0; step >>= 1)
+          if (e + step < n1 && W.lpre[e + step] <= u) e += step;
+        const int j = W.lst[e] + (u - W.lpre[e]);
+        P2PSrc64<ND, KIND>& R = W.s[i];
+        R.p = xs64[j];
+        const size_t o = (size_t)j * ndc + d0;
+#pragma unroll
+        for (int d = 0; d < ND; d++) {
+          if (HQ) R.c[d] = q64[o + d];
+          if (HD) R.c[DOFF + d] = d64[o + d];
+        }
+      }
+      __syncwarp();
+      if (act) {
+        for (int u = ph; u < m; u += nph) {
+          const P2PSrc64<ND, KIND>& R = W.s[u];
+          const double dx = z.x - R.p.x, dy = z.y - R.p.y;
+          const double rr = dx * dx + dy * dy;
+          // cauchykernels2d.f: <= for potential-only, < otherwise
+          const bool inc = IFPGH == 1 ? !(rr <= th2) : !(rr < th2);
+          const double ir = inc ? 1.0 / rr : 0.0;
+          const double2 zi = make_double2(dx * ir, -dy * ir);
+          const double2 z2 = cneg(cmul(zi, zi));
+          if (HQ) {
+            const double lg = inc ? 0.5 * log(rr) : 0.0;
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              const double2 c = R.c[d];
+              pt[d].x += lg * c.x;
+              pt[d].y += lg * c.y;
+              if (IFPGH >= 2) cfma(gr[d], zi, c);
+              if (IFPGH >= 3) cfma(hs[d], z2, c);
+            }
+          }
+          if (HD) {
+            const double2 z3 = IFPGH >= 3 ? cscale(cmul(z2, zi), -2.0) : make_double2(0, 0);
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              const double2 c = R.c[DOFF + d];
+              cfma(pt[d], zi, c);
+              if (IFPGH >= 2) cfma(gr[d], z2, c);
+              if (IFPGH >= 3) cfma(hs[d], z3, c);
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+    for (int hh = 1; hh < nph; hh <<= 1) {
+      const bool take = (ph & (2 * hh - 1)) == 0 && ph + hh < nph;
+      const int off = hh * ntc;
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        double2 v;
+        v.x = __shfl_down_sync(FULL, pt[d].x, off);
+        v.y = __shfl_down_sync(FULL, pt[d].y, off);
+        if (take) pt[d] = cadd(pt[d], v);
+        if (IFPGH >= 2) {
+          v.x = __shfl_down_sync(FULL, gr[d].x, off);
+          v.y = __shfl_down_sync(FULL, gr[d].y, off);
+          if (take) gr[d] = cadd(gr[d], v);
+        }
+        if (IFPGH >= 3) {
+          v.x = __shfl_down_sync(FULL, hs[d].x, off);
+          v.y = __shfl_down_sync(FULL, hs[d].y, off);
+          if (take) hs[d] = cadd(hs[d], v);
+        }
+      }
+    }
+    if (lane < ntc) {
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        const size_t o = (size_t)k * ndc + d0 + d;
+        pot[o] = cadd(pot[o], pt[d]);
+        if (IFPGH >= 2) grad[o] = cadd(grad[o], gr[d]);
+        if (IFPGH >= 3) hess[o] = cadd(hess[o], hs[d]);
+      }
+    }
+  }
+}
+
+template <int ND, int IFPGH, int KIND>
+void p2p64_launch(const TV& t, const MixedData& M, const double2* xe64, const Dens& D,
+                  double thresh, const P2PItem* items, const int* nitems, double2* pot,
+                  double2* grad, double2* hess, cudaStream_t st) {
+  constexpr size_t sm = 4 * sizeof(P2PWarp64<ND, KIND>);
+  auto kern = k_p2p_leaf64<ND, IFPGH, KIND>;
+  set_smem_attr(kern, sm);
+  kern<<<resident_grid(kern, 128, sm), 128, sm, st>>>(t, M.xs64, xe64, D.q, D.d, D.ndc, D.d0,
+                                                     thresh, items, nitems, pot, grad, hess);
+  B2_LAUNCH_CHECK();
+}
+
+template <int ND, int IFPGH>
+void leaf64_launch(const TV& t, int use_targets, const MixedData& M, const double2* xe64,
+                   const Dens& D, int P, const double2* mp, const double2* lo, double thresh,
+                   int ifnear, double2* pot, double2* grad, double2* hess, cudaStream_t st) {
+  const long n = use_targets ? M.nt : M.ns;
+  if (n <= 0) return;
+  const int* leaf = use_targets ? M.leaf_t.p : M.leaf_s.p;
+  k_far_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(t, n, leaf, xe64, D.ndc, D.d0, P, mp,
+                                                          lo, pot, grad, hess);
+  B2_LAUNCH_CHECK();
+  const int kind = (D.q ? 1 : 0) | (D.d ? 2 : 0);
+  if (!ifnear || kind == 0) return;
+  const P2PItem* items = (const P2PItem*)(use_targets ? M.items_t.p : M.items_s.p);
+  const int* nitems = M.nitems.p + (use_targets ? 1 : 0);
+  if (kind == 3)
+    p2p64_launch<ND, IFPGH, 3>(t, M, xe64, D, thresh, items, nitems, pot, grad, hess, st);
+  else if (kind == 2)
+    p2p64_launch<ND, IFPGH, 2>(t, M, xe64, D, thresh, items, nitems, pot, grad, hess, st);
+  else
+    p2p64_launch<ND, IFPGH, 1>(t, M, xe64, D, thresh, items, nitems, pot, grad, hess, st);
+}
+
 std::atomic<int> g_p2p_shape[B2FMM_P2P_CLASSES] = {};
 
 template <int ND, int IFPGH, int KIND, int V>
@@ -860,8 +1191,15 @@ void leaf_launch(const TV& t, int use_targets, const MixedData& M, const double2
   const long n = use_targets ? M.nt : M.ns;
   if (n <= 0) return;
   const int* leaf = use_targets ? M.leaf_t.p : M.leaf_s.p;
-  k_far_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(t, n, leaf, xe64, ndc, d0, P, mp, lo,
-                                                          pot, grad, hess);
+  if (M.tc && M.pairs.usable && M.pairs.P == P && M.err && M.pairs.n > 0 && M.mp32.p) {
+    // the FP32 multipoles of this chunk, from the tensor-core M2L
+    k_far_f32<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(t, n, leaf, xe64, ndc, d0, P,
+                                                          m2l_kh(P), M.mp32.p, lo, pot, grad,
+                                                          hess);
+  } else {
+    k_far_mixed<ND, IFPGH><<<ceil_div(n, 128), 128, 0, st>>>(t, n, leaf, xe64, ndc, d0, P, mp, lo,
+                                                            pot, grad, hess);
+  }
   B2_LAUNCH_CHECK();
   if (far_done) B2_CHECK(cudaEventRecord(far_done, st));
   const int kind = (M.q.p ? 1 : 0) | (M.d.p ? 2 : 0);
@@ -979,6 +1317,27 @@ void lap_mixed_m2l(int ND, const TV& t, int first, int n, int P, const double* b
     case 4: m2l_launch<4>(t, first, n, P, binom, M, mp, lo, st); break;
     case 2: m2l_launch<2>(t, first, n, P, binom, M, mp, lo, st); break;
     default: m2l_launch<1>(t, first, n, P, binom, M, mp, lo, st); break;
+  }
+}
+
+void lap_fp64_leaf(int ND, int ifl, const TV& t, int use_targets, const MixedData& M,
+                   const double2* xe64, const Dens& D, int P, const double2* mp,
+                   const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
+                   double2* hess, cudaStream_t st) {
+  auto run = [&](auto nd_tag) {
+    constexpr int N = decltype(nd_tag)::value;
+    if (ifl == 1)
+      leaf64_launch<N, 1>(t, use_targets, M, xe64, D, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+    else if (ifl == 2)
+      leaf64_launch<N, 2>(t, use_targets, M, xe64, D, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+    else
+      leaf64_launch<N, 3>(t, use_targets, M, xe64, D, P, mp, lo, thresh, ifnear, pot, grad, hess, st);
+  };
+  switch (ND) {
+    case 8: run(std::integral_constant<int, 8>()); break;
+    case 4: run(std::integral_constant<int, 4>()); break;
+    case 2: run(std::integral_constant<int, 2>()); break;
+    default: run(std::integral_constant<int, 1>()); break;
   }
 }
 

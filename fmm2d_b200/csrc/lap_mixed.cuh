@@ -45,6 +45,14 @@ void lap_mixed_prepare(MixedData& M, const double2* xs, long ns, const double2* 
 void lap_mixed_leaves(MixedData& M, const lapk::TV& t, int nb, bool dev, long ns, long nt,
                       int ndiv, cudaStream_t st);
 
+// Leaf evaluation of the FP64 path on the same work items: L2P + M2P
+// (k_far_mixed, FP64) then the FP64 near field (k_p2p_leaf64) for one
+// density chunk D (sorted FP64 densities).
+void lap_fp64_leaf(int ND, int ifl, const lapk::TV& t, int use_targets, const MixedData& M,
+                   const double2* xe64, const lapk::Dens& D, int P, const double2* mp,
+                   const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
+                   double2* hess, cudaStream_t st);
+
 // Near-field tile shape per leaf-size class (0: ndiv <= 20, 1: <= 56,
 // 2: larger); set_p2p_shape returns IER_BADARG for an unknown class or shape.
 int p2p_leaf_class(int ndiv);

@@ -14,8 +14,10 @@
 //   k_p2l        list 4 -> local (step 2)
 //   k_m2l        list 2 multipole -> local (step 4)
 //   k_l2l        downward pass, one launch per level (step 5)
-//   k_leaf       per leaf and 32 evaluation points: L2P + M2P (list 3) +
-//                P2P (list 1) fused, one result write per point (steps 6-8)
+//   leaf passes  (steps 6-8, csrc/lap_mixed.cu) on per-tree work items:
+//                L2P + M2P one point per thread (k_far_mixed), then the
+//                near field one warp per item of up to 32 points of a leaf
+//                (k_p2p_leaf64; FP32 k_p2p_leaf on the mixed path)
 //   k_unpack     caller layout (cfmm / lfmm / rfmm) and inverse permutation
 #include "laplace.cuh"
 
@@ -775,205 +777,6 @@ __global__ void __launch_bounds__(128) k_l2l_all(TV t, int P, const double* __re
 }
 
 // ---------------------------------------------------------------------------
-// steps 6-8 fused per leaf: for 32 evaluation points at a time,
-//   L2P  (laprouts2d.f:696-897)   Horner in (z - c)/r with derivatives
-//   M2P  (laprouts2d.f:289-500)   for each list-3 box, Horner in w = r/(z-c)
-//   P2P  (cauchykernels2d.f)      for each list-1 box, sources staged in smem
-// and one store of pot / grad / hess per point (tree order).
-// ---------------------------------------------------------------------------
-template <int ND>
-struct LeafSmem {
-  double2 coef[64 * ND];  // local or multipole coefficients
-  double2 sx[32];
-  double2 sq[32 * ND];
-  double2 sd[32 * ND];
-};
-
-// Resident blocks the FP64 leaf kernel asks the register allocator for (the
-// common ND <= 2, pot + grad case; at 110 registers only 9 fit an SM: 12
-// (80 registers, a few spilled) run the 4M FP64 call 29.7 -> 28.5 ms).
-#define LEAF_MIN_BLOCKS(ND, IFPGH) ((ND) <= 2 && (IFPGH) <= 2 ? 12 : 1)
-
-template <int ND, int IFPGH>
-__global__ void __launch_bounds__(64, LEAF_MIN_BLOCKS(ND, IFPGH)) k_leaf(TV t, int first, int n, int use_targets,
-                                            const double2* __restrict__ xs,
-                                            const double2* __restrict__ xe, Dens D, int P,
-                                            const double2* __restrict__ mp,
-                                            const double2* __restrict__ lo, double thresh,
-                                            int ifnear, double2* __restrict__ pot,
-                                            double2* __restrict__ grad,
-                                            double2* __restrict__ hess) {
-  extern __shared__ double2 smem[];
-  resolve_range(t, first, n);
-  const double thr = near_thresh(t, thresh);
-  const double th2 = thr * thr;
-  WARP_LOOP(n) {
-    LeafSmem<ND>* S = (LeafSmem<ND>*)smem + wib;
-    int b = first + bi;
-    if (t.nchild[b] != 0) continue;
-    int2 er = use_targets ? t.trng[b] : t.srng[b];
-    if (er.y <= er.x) continue;
-    int lev = t.level[b];
-    double r = t.boxsize[lev];
-    double2 cb = t.center[b];
-    int n3 = t.nl3[b], n1 = ifnear ? t.nl1[b] : 0;
-    for (int k0 = er.x; k0 < er.y; k0 += 32) {
-      int k = k0 + lane;
-      bool act = k < er.y;
-      double2 z = act ? xe[k] : cb;
-      double2 pt[ND], gr[ND], hs[ND];
-#pragma unroll
-      for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
-      // L2P
-      __syncwarp();
-      for (int e = lane; e < P * ND; e += 32) S->coef[e] = lo[(size_t)b * P * ND + e];
-      __syncwarp();
-      {
-        double2 zz = make_double2((z.x - cb.x) / r, (z.y - cb.y) / r);
-        double2 f[ND], f1[ND], f2[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          f[d] = S->coef[(P - 1) * ND + d];
-          f1[d] = f2[d] = make_double2(0, 0);
-        }
-        for (int m = P - 2; m >= 0; m--) {
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], zz), f1[d]);
-            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], zz), f[d]);
-            f[d] = cadd(cmul(f[d], zz), S->coef[m * ND + d]);
-          }
-        }
-        double ri = 1.0 / r;
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          pt[d] = f[d];
-          if (IFPGH >= 2) gr[d] = cscale(f1[d], ri);
-          if (IFPGH >= 3) hs[d] = cscale(f2[d], 2.0 * ri * ri);
-        }
-      }
-      // M2P from list 3 (boxes one level finer)
-      for (int e = 0; e < n3; e++) {
-        int jb = t.l3[(size_t)MNLIST3 * b + e];
-        double rj = t.boxsize[lev + 1];
-        double2 cj = t.center[jb];
-        __syncwarp();
-        for (int q = lane; q < P * ND; q += 32) S->coef[q] = mp[(size_t)jb * P * ND + q];
-        __syncwarp();
-        double2 zc = make_double2(z.x - cj.x, z.y - cj.y);
-        double2 zi = crcp(zc);
-        double2 w = make_double2(rj * zi.x, rj * zi.y);
-        double lg = log(hypot(zc.x, zc.y));
-        // S(w) = sum_{m>=1} c_m w^m by Horner, with S' and S''
-        double2 f[ND], f1[ND], f2[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          f[d] = S->coef[(P - 1) * ND + d];
-          f1[d] = f2[d] = make_double2(0, 0);
-        }
-        for (int m = P - 2; m >= 1; m--) {
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            if (IFPGH >= 3) f2[d] = cadd(cmul(f2[d], w), f1[d]);
-            if (IFPGH >= 2) f1[d] = cadd(cmul(f1[d], w), f[d]);
-            f[d] = cadd(cmul(f[d], w), S->coef[m * ND + d]);
-          }
-        }
-        // now f = sum_{m>=1} c_m w^(m-1); shift by one power of w
-        double2 w2 = cmul(w, w);
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          double2 c0 = S->coef[d];
-          // S = w f ; S' = f + w f1 ; S'' = 2 f1 + w f2
-          double2 Sv = cmul(w, f[d]);
-          double2 S1 = cadd(f[d], cmul(w, f1[d]));
-          // f2 holds f''/2 (Horner), so S'' = 2 f' + w f'' = 2 (f1 + w f2)
-          double2 S2 = cscale(cadd(f1[d], cmul(w, f2[d])), 2.0);
-          pt[d].x += Sv.x + c0.x * lg;
-          pt[d].y += Sv.y + c0.y * lg;
-          if (IFPGH >= 2) {
-            // d/dz = S'(w) (-w^2/r) + c0/z
-            double2 g = cmul(S1, w2);
-            g = make_double2(-g.x / rj, -g.y / rj);
-            g = cadd(g, cmul(c0, zi));
-            gr[d] = cadd(gr[d], g);
-          }
-          if (IFPGH >= 3) {
-            // d2/dz2 = S'' w^4/r^2 + S' 2 w^3/r^2 - c0/z^2
-            double2 w3 = cmul(w2, w), w4 = cmul(w2, w2);
-            double ir2 = 1.0 / (rj * rj);
-            double2 h = cadd(cmul(S2, w4), cscale(cmul(S1, w3), 2.0));
-            h = cscale(h, ir2);
-            h = csub(h, cmul(c0, cmul(zi, zi)));
-            hs[d] = cadd(hs[d], h);
-          }
-        }
-      }
-      // P2P from list 1
-      for (int e = 0; e < n1; e++) {
-        int jb = t.l1[(size_t)MNLIST1 * b + e];
-        int2 sr = t.srng[jb];
-        for (int s0 = sr.x; s0 < sr.y; s0 += 32) {
-          int ns = min(32, sr.y - s0);
-          __syncwarp();
-          if (lane < ns) {
-            int j = s0 + lane;
-            S->sx[lane] = xs[j];
-#pragma unroll
-            for (int d = 0; d < ND; d++) {
-              if (D.q) S->sq[lane * ND + d] = D.q[(size_t)j * D.ndc + D.d0 + d];
-              if (D.d) S->sd[lane * ND + d] = D.d[(size_t)j * D.ndc + D.d0 + d];
-            }
-          }
-          __syncwarp();
-          if (act) {
-            for (int j = 0; j < ns; j++) {
-              double2 y = S->sx[j];
-              double dx = z.x - y.x, dy = z.y - y.y;
-              double rr = dx * dx + dy * dy;
-              // cauchykernels2d.f: <= for potential-only, < otherwise
-              if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
-              double ir = 1.0 / rr;
-              double2 zi = make_double2(dx * ir, -dy * ir);
-              double lg = 0.5 * log(rr);
-              double2 z2 = (IFPGH >= 2 || D.d) ? cneg(cmul(zi, zi)) : make_double2(0, 0);
-#pragma unroll
-              for (int d = 0; d < ND; d++) {
-                if (D.q) {
-                  double2 c = S->sq[j * ND + d];
-                  pt[d].x += lg * c.x;
-                  pt[d].y += lg * c.y;
-                  if (IFPGH >= 2) cfma(gr[d], zi, c);
-                  if (IFPGH >= 3) cfma(hs[d], z2, c);
-                }
-                if (D.d) {
-                  double2 c = S->sd[j * ND + d];
-                  cfma(pt[d], zi, c);
-                  if (IFPGH >= 2) cfma(gr[d], z2, c);
-                  if (IFPGH >= 3) {
-                    double2 z3 = cscale(cmul(z2, zi), -2.0);
-                    cfma(hs[d], z3, c);
-                  }
-                }
-              }
-            }
-          }
-        }
-      }
-      if (act) {
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          size_t o = (size_t)k * D.ndc + D.d0 + d;
-          pot[o] = pt[d];
-          if (IFPGH >= 2) grad[o] = gr[d];
-          if (IFPGH >= 3) hess[o] = hs[d];
-        }
-      }
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
 // gather / unpack
 // ---------------------------------------------------------------------------
 __global__ void k_gather_pts(const double* __restrict__ xy, const int* __restrict__ perm, long n,
@@ -1174,7 +977,7 @@ template <int ND>
 void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int P,
                const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
                double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, const Launch& X,
-               cudaStream_t st, cudaEvent_t* ev, const MixedData* M) {
+               cudaStream_t st, cudaEvent_t* ev, const MixedData* M, const MixedData& LD) {
   const double* binom = device_binomials();
   const int nb = X.nb;
   const bool dev = X.dev;
@@ -1268,7 +1071,6 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
     }
   }
   B2_CHECK(cudaEventRecord(ev[5], st));
-  size_t sm_leaf = sizeof(LeafSmem<ND>) * 2;
   // near-field threshold boxsize(0) 2^-51, taken on the device from the tree
   const double thresh = -1.0;
   auto leaf = [&](int use_t, int ifl, const double2* xe, double2* po, double2* gr, double2* he) {
@@ -1279,20 +1081,7 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
                      gr, he, st, use_t == 0 ? ev[7] : nullptr);
       return;
     }
-    if (ifl == 1) {
-      set_smem_attr(k_leaf<ND, 1>, sm_leaf);
-      k_leaf<ND, 1><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, all, nb, use_t, xs, xe, D, P, mp,
-                                                          lo, thresh, a.ifnear, po, gr, he);
-    } else if (ifl == 2) {
-      set_smem_attr(k_leaf<ND, 2>, sm_leaf);
-      k_leaf<ND, 2><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, all, nb, use_t, xs, xe, D, P, mp,
-                                                          lo, thresh, a.ifnear, po, gr, he);
-    } else {
-      set_smem_attr(k_leaf<ND, 3>, sm_leaf);
-      k_leaf<ND, 3><<<warp_grid(nb, 2), 64, sm_leaf, st>>>(tv, all, nb, use_t, xs, xe, D, P, mp,
-                                                          lo, thresh, a.ifnear, po, gr, he);
-    }
-    B2_LAUNCH_CHECK();
+    lap_fp64_leaf(ND, ifl, tv, use_t, LD, xe, D, P, mp, lo, thresh, a.ifnear, po, gr, he, st);
   };
   leaf(0, a.ifpgh, xs, ps, gs, hs);
   leaf(1, a.ifpghtarg, xt, pt, gt, ht);
@@ -1501,6 +1290,11 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
   p.lo.alloc((size_t)nb * p.P * p.chunk, st);
   p.gbar.alloc(1, st);
   p.gbar.zero(1);
+  if (!p.mixed) {
+    // the FP64 leaf passes use the same leaf maps and near-field work items
+    p.MD.xs64 = p.xs.p;
+    lap_mixed_leaves(p.MD, p.tv, nb, p.dev, p.ns, p.nt, p.ndiv, st);
+  }
   if (p.mixed) {
     lap_mixed_prepare(p.MD, p.xs.p, p.ns, p.xt.p, p.nt, p.fc, p.fd, p.ndc, 0.0, 0.0, p.P, st);
     p.MD.err = p.err.p;
@@ -1582,10 +1376,10 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
     int ND = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
     Dens D{p.fc ? p.qs.p : nullptr, p.fd ? p.ds.p : nullptr, ndc, d0};
     switch (ND) {
-      case 8: run_chunk<8>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
-      case 4: run_chunk<4>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
-      case 2: run_chunk<2>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
-      default: run_chunk<1>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp); break;
+      case 8: run_chunk<8>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
+      case 4: run_chunk<4>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
+      case 2: run_chunk<2>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
+      default: run_chunk<1>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
     }
     if (timeinfo) {
       B2_CHECK(cudaEventSynchronize(p.ev[6]));

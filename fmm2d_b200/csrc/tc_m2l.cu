@@ -890,9 +890,9 @@ __global__ void k_m2l_steps(const int* __restrict__ tstart, const int* __restric
   atomicAdd(out, (unsigned long long)m);
 }
 
-int m2l_kh(int P) { return (P + 3) / 4 * 4; }
-
 }  // namespace
+
+int m2l_kh(int P) { return (P + 3) / 4 * 4; }
 
 bool m2l_tc_supported(int P) { return P >= 2 && P <= 20; }
 

@@ -29,6 +29,9 @@ void m2l_tc_build(M2LPairs& L, const lapk::TV& t, int first, int n, int nboxes, 
 
 // True when the tensor-core M2L supports P (expansion length).
 bool m2l_tc_supported(int P);
+// Coefficients per (box, density) of the FP32 multipole copy (P rounded up
+// to a multiple of 4; the entries beyond P are zero).
+int m2l_kh(int P);
 
 // float2 elements of the FP32 multipole scratch for ND densities.
 long m2l_tc_scratch(const M2LPairs& L, int nboxes, int ND);
