@@ -5,8 +5,15 @@
 // independent branches (fork/join through events on a capturing stream), so
 // small problems that cannot fill the GPU on their own run side by side and
 // a whole batch costs one graph launch instead of hundreds of kernel
-// launches per problem.
+// launches per problem.  The mixed near fields of all plans (one density
+// chunk each) run as one persistent pass over the work items of every tree
+// (p2p_batch_launch, one launch per group of density count, output level
+// and density kind) between the plans' far fields and their unsorts:
+//     fork -> plans up to the far field -> join -> batched near field ->
+//     fork -> the plans' unsorts -> join.
 #include "batch.cuh"
+
+#include "lap_mixed.cuh"
 
 #include <algorithm>
 #include <vector>
@@ -17,10 +24,12 @@ struct BatchGraph {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   std::vector<LapPlan*> plans;
+  P2PBatch* near = nullptr;  // the batched near-field pass (null: none deferred)
   size_t nodes = 0;
   ~BatchGraph() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
+    if (near) p2p_batch_free(near);
   }
 };
 
@@ -42,14 +51,21 @@ int batch_graph_create(int n, LapPlan* const* plans, const BatchIO& io, int nbra
     if (fork) cudaEventDestroy(fork);
     if (s0) cudaStreamDestroy(s0);
   };
-  auto eval = [&](int i, cudaStream_t s) {
-    return lap_plan_eval(plans[i], io.charge ? io.charge[i] : nullptr,
-                         io.dipstr ? io.dipstr[i] : nullptr, io.dipvec ? io.dipvec[i] : nullptr,
-                         io.pot ? io.pot[i] : nullptr, io.grad ? io.grad[i] : nullptr,
-                         io.hess ? io.hess[i] : nullptr, io.pottarg ? io.pottarg[i] : nullptr,
-                         io.gradtarg ? io.gradtarg[i] : nullptr,
-                         io.hesstarg ? io.hesstarg[i] : nullptr, s, false, nullptr);
+  auto eval = [&](int i, cudaStream_t s, int part) {
+    return lap_plan_eval_part(
+        plans[i], io.charge ? io.charge[i] : nullptr, io.dipstr ? io.dipstr[i] : nullptr,
+        io.dipvec ? io.dipvec[i] : nullptr, io.pot ? io.pot[i] : nullptr,
+        io.grad ? io.grad[i] : nullptr, io.hess ? io.hess[i] : nullptr,
+        io.pottarg ? io.pottarg[i] : nullptr, io.gradtarg ? io.gradtarg[i] : nullptr,
+        io.hesstarg ? io.hesstarg[i] : nullptr, s, false, nullptr, part);
   };
+  std::vector<char> defer(n, 0);
+  std::vector<P2PBatchEntry> entries;
+  for (int i = 0; i < n; i++)
+    if (lap_plan_defers_near(plans[i])) {
+      defer[i] = 1;
+      lap_plan_near_entries(plans[i], entries);
+    }
   try {
     B2_CHECK(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
     for (auto& s : br) B2_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -58,11 +74,18 @@ int batch_graph_create(int n, LapPlan* const* plans, const BatchIO& io, int nbra
     // one ordinary evaluation of every plan first: checks the arguments and
     // performs every one-time set-up (kernel attributes) outside the capture
     for (int i = 0; i < n; i++) {
-      int r = eval(i, s0);
+      int r = eval(i, s0, 0);
       if (r != IER_OK) {
         cleanup();
         return r;
       }
+    }
+    if (!entries.empty()) {
+      // the batched pass once outside the capture too (its kernel attributes;
+      // it only adds to the plans' tree-order buffers, which every
+      // evaluation rewrites)
+      G->near = p2p_batch_create(entries);
+      p2p_batch_launch(G->near, s0);
     }
     B2_CHECK(cudaStreamSynchronize(s0));
     for (int i = 0; i < n; i++) {
@@ -75,12 +98,24 @@ int batch_graph_create(int n, LapPlan* const* plans, const BatchIO& io, int nbra
     B2_CHECK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
     int rc = IER_OK;
     try {
-      B2_CHECK(cudaEventRecord(fork, s0));
-      for (auto& s : br) B2_CHECK(cudaStreamWaitEvent(s, fork, 0));
-      for (int i = 0; i < n && rc == IER_OK; i++) rc = eval(i, br[i % nbranch]);
-      for (int b = 0; b < nbranch; b++) {
-        B2_CHECK(cudaEventRecord(join[b], br[b]));
-        B2_CHECK(cudaStreamWaitEvent(s0, join[b], 0));
+      auto fork_join = [&](auto body) {
+        B2_CHECK(cudaEventRecord(fork, s0));
+        for (auto& s : br) B2_CHECK(cudaStreamWaitEvent(s, fork, 0));
+        body();
+        for (int b = 0; b < nbranch; b++) {
+          B2_CHECK(cudaEventRecord(join[b], br[b]));
+          B2_CHECK(cudaStreamWaitEvent(s0, join[b], 0));
+        }
+      };
+      fork_join([&] {
+        for (int i = 0; i < n && rc == IER_OK; i++) rc = eval(i, br[i % nbranch], defer[i] ? 1 : 0);
+      });
+      if (G->near && rc == IER_OK) {
+        p2p_batch_launch(G->near, s0);
+        fork_join([&] {
+          for (int i = 0; i < n && rc == IER_OK; i++)
+            if (defer[i]) rc = eval(i, br[i % nbranch], 2);
+        });
       }
     } catch (...) {
       cudaGraph_t g = nullptr;

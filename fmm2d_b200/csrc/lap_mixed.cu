@@ -19,6 +19,7 @@
 #include "lap_mixed.cuh"
 
 #include <atomic>
+#include <memory>
 #include <cstddef>
 #include <type_traits>
 #include "laplace.cuh"
@@ -696,264 +697,332 @@ __global__ void k_p2p_items(TV t, int nb, int use_targets, P2PItem* __restrict__
   }
 }
 
+// One near-field job: the work items of one tree with the arrays they read
+// and the outputs they add to (k_p2p_leaf takes one, k_p2p_batch many).
+struct P2PJob {
+  const TreeCtl* ctl;     // tree status (no items after a failed build)
+  const double* bs;       // box sizes (bs[0]: the root, for the default threshold)
+  const double2* xs64;    // sorted sources
+  const double2* xe64;    // sorted evaluation points
+  const float2* q32;      // FP32 charges, ndc per point, or null
+  const float2* d32;      // FP32 dipole strengths or null
+  const P2PItem* items;
+  const int* nitems;
+  double2 *pot, *grad, *hess;  // tree-order outputs (added to)
+  double thresh;          // < 0: boxsize(0) 2^-51
+  int ndc, d0, self_pairs, pad;
+};
+
+// The near field of one work item (the body of k_p2p_leaf and k_p2p_batch).
 template <int ND, int IFPGH, int KIND, int V>
-__global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH, V)) k_p2p_leaf(
-    TV t, const double2* __restrict__ xs64, const double2* __restrict__ xe64,
-    const float2* __restrict__ q32, const float2* __restrict__ d32, int ndc, int d0,
-    double thresh, const P2PItem* __restrict__ items, const int* __restrict__ nitems,
-    int self_pairs, double2* __restrict__ pot, double2* __restrict__ grad,
-    double2* __restrict__ hess) {
+__device__ __forceinline__ void p2p_item(const P2PJob& J, const P2PItem& I,
+                                         P2PWarp<ND, KIND, P2P_SHAPES[V].chunk>& W, int lane) {
   constexpr bool HQ = KIND & 1, HD = (KIND >> 1) & 1;
   constexpr int DOFF = HQ ? ND : 0;  // first dipole entry of a staged source
-  extern __shared__ float4 p2p_sm[];
   constexpr unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   constexpr int CH = P2P_SHAPES[V].chunk, UNROLL = P2P_SHAPES[V].unroll;
-  P2PWarp<ND, KIND, CH>& W = ((P2PWarp<ND, KIND, CH>*)p2p_sm)[wib];
-  // after a failed tree build the item list is empty
-  const int ni = t.ctl->status == TB_OK ? *nitems : 0;
-  const double thr = near_thresh(t, thresh);
-  const int nw = gridDim.x * (blockDim.x >> 5);
-  for (int it = blockIdx.x * (blockDim.x >> 5) + wib; it < ni; it += nw) {
-    const P2PItem& I = items[it];
-    // the list-1 ranges and their prefix: 32 consecutive ints, one a lane
-    ((int*)W.lst)[lane] = ((const int*)I.lst)[lane];
-    const int4 h = *(const int4*)&I;
-    const int n1 = h.z >> 8, ntc = h.z & 255, ex = h.w;
-    const int S = I.S;
-    const double2 c = I.c;
-    // 32 / ntc and lane / ntc by a float reciprocal (exact: the quotients
-    // are at least 1/64 away from the next integer)
-    const float rn = __frcp_rn((float)ntc);
-    const int nph = __float2int_rz(32.5f * rn);
-    const int ph = __float2int_rz(((float)lane + 0.5f) * rn), ti = lane - ph * ntc;
-    const bool act = ph < nph;
-    const long k = (long)h.y + ti;
-    const double sc = __hiloint2double((1023 - ex) << 20, 0);  // 2^-ex
-    const float scf = (float)sc;
-    const double ts = thr * sc;
-    const float th2 = (float)(ts * ts);
-    // pairs below this squared distance take the careful path (FP64
-    // difference, exclusion test)
-    const float rslow = fmaxf(0x1p-40f, 2.f * th2);
-    const float lsc = (float)((double)ex * 0.69314718055994530942);
-    __syncwarp();
-    // at most 32 sources per lane and chunk: one FP32 partial sum each
-    const int cap = min(CH, 32 * nph);
-    float2 zh, zl;
-    {
-      const double2 z = xe64[k];
-      split_hilo((z.x - c.x) * sc, zh.x, zl.x);
-      split_hilo((z.y - c.y) * sc, zh.y, zl.y);
+  const double thr = J.thresh >= 0 ? J.thresh : J.bs[0] * 0x1p-51;
+  // the previous item's lanes are done with the list-1 ranges (its close
+  // pairs read them after the last chunk)
+  __syncwarp();
+  // the list-1 ranges and their prefix: 32 consecutive ints, one a lane
+  ((int*)W.lst)[lane] = ((const int*)I.lst)[lane];
+  const int4 h = *(const int4*)&I;
+  const int n1 = h.z >> 8, ntc = h.z & 255, ex = h.w;
+  const int S = I.S;
+  const double2 c = I.c;
+  // 32 / ntc and lane / ntc by a float reciprocal (exact: the quotients
+  // are at least 1/64 away from the next integer)
+  const float rn = __frcp_rn((float)ntc);
+  const int nph = __float2int_rz(32.5f * rn);
+  const int ph = __float2int_rz(((float)lane + 0.5f) * rn), ti = lane - ph * ntc;
+  const bool act = ph < nph;
+  const long k = (long)h.y + ti;
+  const double sc = __hiloint2double((1023 - ex) << 20, 0);  // 2^-ex
+  const float scf = (float)sc;
+  const double ts = thr * sc;
+  const float th2 = (float)(ts * ts);
+  // pairs below this squared distance take the careful path (FP64
+  // difference, exclusion test)
+  const float rslow = fmaxf(0x1p-40f, 2.f * th2);
+  const float lsc = (float)((double)ex * 0.69314718055994530942);
+  __syncwarp();
+  // at most 32 sources per lane and chunk: one FP32 partial sum each
+  const int cap = min(CH, 32 * nph);
+  float2 zh, zl;
+  {
+    const double2 z = J.xe64[k];
+    split_hilo((z.x - c.x) * sc, zh.x, zl.x);
+    split_hilo((z.y - c.y) * sc, zh.y, zl.y);
+  }
+  double2 pt[ND], gr[ND], hs[ND];
+#pragma unroll
+  for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
+  int nslow = 0;
+  for (int u0 = 0; u0 < S; u0 += cap) {
+    const int m = min(cap, S - u0);
+    for (int i = lane; i < m; i += 32) {
+      // the list-1 box of source u: the last e with lpre[e] <= u
+      const int u = u0 + i;
+      int e = 0;
+#pragma unroll
+      for (int step = 8; step > 0; step >>= 1)
+        if (e + step < n1 && W.lpre[e + step] <= u) e += step;
+      const int j = W.lst[e] + (u - W.lpre[e]);
+      const double2 sxy = J.xs64[j];
+      P2PSrc<ND, KIND>& R = W.s[i];
+      float4 p;
+      split_hilo((sxy.x - c.x) * sc, p.x, p.z);
+      split_hilo((sxy.y - c.y) * sc, p.y, p.w);
+      R.p = p;
+      const size_t o = (size_t)j * J.ndc + J.d0;
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        if (HQ) R.c[d] = J.q32[o + d];
+        if (HD) {
+          const float2 v = J.d32[o + d];
+          R.c[DOFF + d] = make_float2(v.x * scf, v.y * scf);
+        }
+      }
     }
-    double2 pt[ND], gr[ND], hs[ND];
+    __syncwarp();
+    if (act) {
+      float2 fp[ND], fg[ND], fh[ND];
 #pragma unroll
-    for (int d = 0; d < ND; d++) pt[d] = gr[d] = hs[d] = make_double2(0, 0);
-    int nslow = 0;
-    for (int u0 = 0; u0 < S; u0 += cap) {
-      const int m = min(cap, S - u0);
-      for (int i = lane; i < m; i += 32) {
-        // the list-1 box of source u: the last e with lpre[e] <= u
-        const int u = u0 + i;
-        int e = 0;
+      for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
+      // branch-free pairs: a pair closer than rslow (the pair of a point
+      // with itself, nearly coincident or excluded pairs) adds nothing
+      // here and is counted; such pairs are formed after the item
+      const P2PSrc<ND, KIND>* const Rend = W.s + m;
+#pragma unroll UNROLL
+      for (const P2PSrc<ND, KIND>* R = W.s + ph; R < Rend; R += nph) {
+        const float4 p = R->p;
+        const float dx = (zh.x - p.x) + (zl.x - p.z);
+        const float dy = (zh.y - p.y) + (zl.y - p.w);
+        const float rr = fmaf(dx, dx, dy * dy);
+        const bool fast = rr >= rslow;
+        nslow += fast ? 0 : 1;
+        const float ir = fast ? __fdividef(1.0f, rr) : 0.f;
+        const float2 zi = make_float2(dx * ir, -dy * ir);
+        const float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
+        if (HQ) {
+          const float lg = fast ? fmaf(0.5f, __logf(rr), lsc) : 0.f;
 #pragma unroll
-        for (int step = 8; step > 0; step >>= 1)
-          if (e + step < n1 && W.lpre[e + step] <= u) e += step;
-        const int j = W.lst[e] + (u - W.lpre[e]);
-        const double2 sxy = xs64[j];
-        P2PSrc<ND, KIND>& R = W.s[i];
+          for (int d = 0; d < ND; d++) {
+            const float2 v = R->c[d];
+            fp[d].x = fmaf(lg, v.x, fp[d].x);
+            fp[d].y = fmaf(lg, v.y, fp[d].y);
+            if (IFPGH >= 2) cfmaf_(fg[d], zi, v);
+            if (IFPGH >= 3) cfmaf_(fh[d], z2, v);
+          }
+        }
+        if (HD) {
+          float2 z3 = make_float2(0.f, 0.f);
+          if (IFPGH >= 3) {
+            z3 = cmulf_(z2, zi);
+            z3 = make_float2(-2.f * z3.x, -2.f * z3.y);
+          }
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            const float2 v = R->c[DOFF + d];
+            cfmaf_(fp[d], zi, v);
+            if (IFPGH >= 2) cfmaf_(fg[d], z2, v);
+            if (IFPGH >= 3) cfmaf_(fh[d], z3, v);
+          }
+        }
+      }
+#pragma unroll
+      for (int d = 0; d < ND; d++) {
+        pt[d].x += fp[d].x;
+        pt[d].y += fp[d].y;
+        if (IFPGH >= 2) {
+          gr[d].x += fg[d].x;
+          gr[d].y += fg[d].y;
+        }
+        if (IFPGH >= 3) {
+          hs[d].x += fh[d].x;
+          hs[d].y += fh[d].y;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  // sum the phases of every target: a tree over ph by shuffles at strides
+  // ntc, 2 ntc, 4 ntc, ... (a lane adds its partner only if that phase
+  // exists)
+  for (int hh = 1; hh < nph; hh <<= 1) {
+    const bool take = (ph & (2 * hh - 1)) == 0 && ph + hh < nph;
+    const int off = hh * ntc;
+    {
+      const int v = __shfl_down_sync(FULL, nslow, off);
+      if (take) nslow += v;
+    }
+#pragma unroll
+    for (int d = 0; d < ND; d++) {
+      double2 v;
+      v.x = __shfl_down_sync(FULL, pt[d].x, off);
+      v.y = __shfl_down_sync(FULL, pt[d].y, off);
+      if (take) {
+        pt[d].x += v.x;
+        pt[d].y += v.y;
+      }
+      if (IFPGH >= 2) {
+        v.x = __shfl_down_sync(FULL, gr[d].x, off);
+        v.y = __shfl_down_sync(FULL, gr[d].y, off);
+        if (take) {
+          gr[d].x += v.x;
+          gr[d].y += v.y;
+        }
+      }
+      if (IFPGH >= 3) {
+        v.x = __shfl_down_sync(FULL, hs[d].x, off);
+        v.y = __shfl_down_sync(FULL, hs[d].y, off);
+        if (take) {
+          hs[d].x += v.x;
+          hs[d].y += v.y;
+        }
+      }
+    }
+  }
+  // the close pairs: beyond the pair of a point with itself (one per
+  // target when the evaluation points are the sources) they are rare; the
+  // target's lane walks its sources again and forms them one by one
+  const bool redo = act && ph == 0 && nslow > (J.self_pairs ? 1 : 0);
+  if (__any_sync(FULL, redo) && redo) {
+    const double2 z = J.xe64[k];
+    for (int e = 0; e < n1; e++) {
+      const int j0 = W.lst[e], len = (e + 1 < n1 ? W.lpre[e + 1] : S) - W.lpre[e];
+      for (int j = j0; j < j0 + len; j++) {
+        const double2 sxy = J.xs64[j];
         float4 p;
         split_hilo((sxy.x - c.x) * sc, p.x, p.z);
         split_hilo((sxy.y - c.y) * sc, p.y, p.w);
-        R.p = p;
-        const size_t o = (size_t)j * ndc + d0;
+        float dx = (zh.x - p.x) + (zl.x - p.z);
+        float dy = (zh.y - p.y) + (zl.y - p.w);
+        float rr = fmaf(dx, dx, dy * dy);
+        if (rr >= rslow) continue;  // formed in the pass above
+        if (J.self_pairs && j == k) continue;  // a point and itself: r = 0
+        if (rr < 0x1p-40f) {
+          // nearly coincident: the FP64 difference, rounded once
+          dx = __double2float_rn((z.x - sxy.x) * sc);
+          dy = __double2float_rn((z.y - sxy.y) * sc);
+          rr = fmaf(dx, dx, dy * dy);
+        }
+        // cauchykernels2d.f: <= for potential-only, < otherwise
+        if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
+        const float ir = __fdividef(1.0f, rr);
+        const float2 zi = make_float2(dx * ir, -dy * ir);
+        const float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
+        const float2 z3 = IFPGH >= 3 ? cmulf_(z2, zi) : make_float2(0.f, 0.f);
+        const size_t o = (size_t)j * J.ndc + J.d0;
 #pragma unroll
         for (int d = 0; d < ND; d++) {
-          if (HQ) R.c[d] = q32[o + d];
-          if (HD) {
-            const float2 v = d32[o + d];
-            R.c[DOFF + d] = make_float2(v.x * scf, v.y * scf);
-          }
-        }
-      }
-      __syncwarp();
-      if (act) {
-        float2 fp[ND], fg[ND], fh[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) fp[d] = fg[d] = fh[d] = make_float2(0.f, 0.f);
-        // branch-free pairs: a pair closer than rslow (the pair of a point
-        // with itself, nearly coincident or excluded pairs) adds nothing
-        // here and is counted; such pairs are formed after the item
-        const P2PSrc<ND, KIND>* const Rend = W.s + m;
-#pragma unroll UNROLL
-        for (const P2PSrc<ND, KIND>* R = W.s + ph; R < Rend; R += nph) {
-          const float4 p = R->p;
-          const float dx = (zh.x - p.x) + (zl.x - p.z);
-          const float dy = (zh.y - p.y) + (zl.y - p.w);
-          const float rr = fmaf(dx, dx, dy * dy);
-          const bool fast = rr >= rslow;
-          nslow += fast ? 0 : 1;
-          const float ir = fast ? __fdividef(1.0f, rr) : 0.f;
-          const float2 zi = make_float2(dx * ir, -dy * ir);
-          const float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
+          float2 fp = make_float2(0.f, 0.f), fg = fp, fh = fp;
           if (HQ) {
-            const float lg = fast ? fmaf(0.5f, __logf(rr), lsc) : 0.f;
-#pragma unroll
-            for (int d = 0; d < ND; d++) {
-              const float2 v = R->c[d];
-              fp[d].x = fmaf(lg, v.x, fp[d].x);
-              fp[d].y = fmaf(lg, v.y, fp[d].y);
-              if (IFPGH >= 2) cfmaf_(fg[d], zi, v);
-              if (IFPGH >= 3) cfmaf_(fh[d], z2, v);
-            }
+            const float lg = fmaf(0.5f, __logf(rr), lsc);
+            const float2 v = J.q32[o + d];
+            fp = make_float2(lg * v.x, lg * v.y);
+            if (IFPGH >= 2) cfmaf_(fg, zi, v);
+            if (IFPGH >= 3) cfmaf_(fh, z2, v);
           }
           if (HD) {
-            float2 z3 = make_float2(0.f, 0.f);
-            if (IFPGH >= 3) {
-              z3 = cmulf_(z2, zi);
-              z3 = make_float2(-2.f * z3.x, -2.f * z3.y);
-            }
-#pragma unroll
-            for (int d = 0; d < ND; d++) {
-              const float2 v = R->c[DOFF + d];
-              cfmaf_(fp[d], zi, v);
-              if (IFPGH >= 2) cfmaf_(fg[d], z2, v);
-              if (IFPGH >= 3) cfmaf_(fh[d], z3, v);
-            }
+            const float2 v0 = J.d32[o + d];
+            const float2 v = make_float2(v0.x * scf, v0.y * scf);
+            cfmaf_(fp, zi, v);
+            if (IFPGH >= 2) cfmaf_(fg, z2, v);
+            if (IFPGH >= 3) cfmaf_(fh, make_float2(-2.f * z3.x, -2.f * z3.y), v);
           }
-        }
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          pt[d].x += fp[d].x;
-          pt[d].y += fp[d].y;
+          pt[d].x += fp.x;
+          pt[d].y += fp.y;
           if (IFPGH >= 2) {
-            gr[d].x += fg[d].x;
-            gr[d].y += fg[d].y;
+            gr[d].x += fg.x;
+            gr[d].y += fg.y;
           }
           if (IFPGH >= 3) {
-            hs[d].x += fh[d].x;
-            hs[d].y += fh[d].y;
+            hs[d].x += fh.x;
+            hs[d].y += fh.y;
           }
         }
       }
-      __syncwarp();
     }
-    // sum the phases of every target: a tree over ph by shuffles at strides
-    // ntc, 2 ntc, 4 ntc, ... (a lane adds its partner only if that phase
-    // exists)
-    for (int hh = 1; hh < nph; hh <<= 1) {
-      const bool take = (ph & (2 * hh - 1)) == 0 && ph + hh < nph;
-      const int off = hh * ntc;
-      {
-        const int v = __shfl_down_sync(FULL, nslow, off);
-        if (take) nslow += v;
-      }
+  }
+  if (lane < ntc) {
 #pragma unroll
-      for (int d = 0; d < ND; d++) {
-        double2 v;
-        v.x = __shfl_down_sync(FULL, pt[d].x, off);
-        v.y = __shfl_down_sync(FULL, pt[d].y, off);
-        if (take) {
-          pt[d].x += v.x;
-          pt[d].y += v.y;
-        }
-        if (IFPGH >= 2) {
-          v.x = __shfl_down_sync(FULL, gr[d].x, off);
-          v.y = __shfl_down_sync(FULL, gr[d].y, off);
-          if (take) {
-            gr[d].x += v.x;
-            gr[d].y += v.y;
-          }
-        }
-        if (IFPGH >= 3) {
-          v.x = __shfl_down_sync(FULL, hs[d].x, off);
-          v.y = __shfl_down_sync(FULL, hs[d].y, off);
-          if (take) {
-            hs[d].x += v.x;
-            hs[d].y += v.y;
-          }
-        }
+    for (int d = 0; d < ND; d++) {
+      const size_t o = (size_t)k * J.ndc + J.d0 + d;
+      double2 w = J.pot[o];
+      J.pot[o] = make_double2(w.x + pt[d].x, w.y + pt[d].y);
+      if (IFPGH >= 2) {
+        w = J.grad[o];
+        J.grad[o] = make_double2(w.x + sc * gr[d].x, w.y + sc * gr[d].y);
+      }
+      if (IFPGH >= 3) {
+        w = J.hess[o];
+        const double s2 = sc * sc;
+        J.hess[o] = make_double2(w.x + s2 * hs[d].x, w.y + s2 * hs[d].y);
       }
     }
-    // the close pairs: beyond the pair of a point with itself (one per
-    // target when the evaluation points are the sources) they are rare; the
-    // target's lane walks its sources again and forms them one by one
-    const bool redo = act && ph == 0 && nslow > (self_pairs ? 1 : 0);
-    if (__any_sync(FULL, redo) && redo) {
-      const double2 z = xe64[k];
-      for (int e = 0; e < n1; e++) {
-        const int j0 = W.lst[e], len = (e + 1 < n1 ? W.lpre[e + 1] : S) - W.lpre[e];
-        for (int j = j0; j < j0 + len; j++) {
-          const double2 sxy = xs64[j];
-          float4 p;
-          split_hilo((sxy.x - c.x) * sc, p.x, p.z);
-          split_hilo((sxy.y - c.y) * sc, p.y, p.w);
-          float dx = (zh.x - p.x) + (zl.x - p.z);
-          float dy = (zh.y - p.y) + (zl.y - p.w);
-          float rr = fmaf(dx, dx, dy * dy);
-          if (rr >= rslow) continue;  // formed in the pass above
-          if (self_pairs && j == k) continue;  // a point and itself: r = 0
-          if (rr < 0x1p-40f) {
-            // nearly coincident: the FP64 difference, rounded once
-            dx = __double2float_rn((z.x - sxy.x) * sc);
-            dy = __double2float_rn((z.y - sxy.y) * sc);
-            rr = fmaf(dx, dx, dy * dy);
-          }
-          // cauchykernels2d.f: <= for potential-only, < otherwise
-          if (IFPGH == 1 ? (rr <= th2) : (rr < th2)) continue;
-          const float ir = __fdividef(1.0f, rr);
-          const float2 zi = make_float2(dx * ir, -dy * ir);
-          const float2 z2 = make_float2(-(zi.x * zi.x - zi.y * zi.y), -2.f * zi.x * zi.y);
-          const float2 z3 = IFPGH >= 3 ? cmulf_(z2, zi) : make_float2(0.f, 0.f);
-          const size_t o = (size_t)j * ndc + d0;
-#pragma unroll
-          for (int d = 0; d < ND; d++) {
-            float2 fp = make_float2(0.f, 0.f), fg = fp, fh = fp;
-            if (HQ) {
-              const float lg = fmaf(0.5f, __logf(rr), lsc);
-              const float2 v = q32[o + d];
-              fp = make_float2(lg * v.x, lg * v.y);
-              if (IFPGH >= 2) cfmaf_(fg, zi, v);
-              if (IFPGH >= 3) cfmaf_(fh, z2, v);
-            }
-            if (HD) {
-              const float2 v0 = d32[o + d];
-              const float2 v = make_float2(v0.x * scf, v0.y * scf);
-              cfmaf_(fp, zi, v);
-              if (IFPGH >= 2) cfmaf_(fg, z2, v);
-              if (IFPGH >= 3) cfmaf_(fh, make_float2(-2.f * z3.x, -2.f * z3.y), v);
-            }
-            pt[d].x += fp.x;
-            pt[d].y += fp.y;
-            if (IFPGH >= 2) {
-              gr[d].x += fg.x;
-              gr[d].y += fg.y;
-            }
-            if (IFPGH >= 3) {
-              hs[d].x += fh.x;
-              hs[d].y += fh.y;
-            }
-          }
-        }
+  }
+}
+
+template <int ND, int IFPGH, int KIND, int V>
+__global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH, V)) k_p2p_leaf(P2PJob J) {
+  extern __shared__ float4 p2p_sm[];
+  constexpr int CH = P2P_SHAPES[V].chunk;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  P2PWarp<ND, KIND, CH>& W = ((P2PWarp<ND, KIND, CH>*)p2p_sm)[wib];
+  // after a failed tree build the item list is empty
+  const int ni = J.ctl->status == TB_OK ? *J.nitems : 0;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int it = blockIdx.x * (blockDim.x >> 5) + wib; it < ni; it += nw)
+    p2p_item<ND, IFPGH, KIND, V>(J, J.items[it], W, lane);
+}
+
+// Item offsets of the jobs of a batch (jobs of failed trees count none);
+// one block of 256 threads.
+__global__ void k_p2p_batch_prefix(const P2PJob* __restrict__ jobs, int njobs,
+                                   int* __restrict__ prefix) {
+  __shared__ int cnt[256];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < njobs; base += 256) {
+    const int j = base + threadIdx.x;
+    cnt[threadIdx.x] = j < njobs && jobs[j].ctl->status == TB_OK ? *jobs[j].nitems : 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int s = carry;
+      for (int q = 0; q < 256 && base + q < njobs; q++) {
+        prefix[base + q] = s;
+        s += cnt[q];
       }
+      carry = s;
     }
-    if (lane < ntc) {
-#pragma unroll
-      for (int d = 0; d < ND; d++) {
-        const size_t o = (size_t)k * ndc + d0 + d;
-        double2 w = pot[o];
-        pot[o] = make_double2(w.x + pt[d].x, w.y + pt[d].y);
-        if (IFPGH >= 2) {
-          w = grad[o];
-          grad[o] = make_double2(w.x + sc * gr[d].x, w.y + sc * gr[d].y);
-        }
-        if (IFPGH >= 3) {
-          w = hess[o];
-          const double s2 = sc * sc;
-          hess[o] = make_double2(w.x + s2 * hs[d].x, w.y + s2 * hs[d].y);
-        }
-      }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) prefix[njobs] = carry;
+}
+
+// The near field of many trees in one persistent launch: warps take the
+// items of all jobs in turn (the job of an item by a binary search of the
+// prefix).
+template <int ND, int IFPGH, int KIND, int V>
+__global__ void __launch_bounds__(128, P2P_MIN_BLOCKS(ND, IFPGH, V)) k_p2p_batch(
+    const P2PJob* __restrict__ jobs, int njobs, const int* __restrict__ prefix) {
+  extern __shared__ float4 p2p_sm[];
+  constexpr int CH = P2P_SHAPES[V].chunk;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  P2PWarp<ND, KIND, CH>& W = ((P2PWarp<ND, KIND, CH>*)p2p_sm)[wib];
+  const int ni = prefix[njobs];
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int it = blockIdx.x * (blockDim.x >> 5) + wib; it < ni; it += nw) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= it) lo = mid; else hi = mid - 1;
     }
+    const P2PJob J = jobs[lo];
+    p2p_item<ND, IFPGH, KIND, V>(J, J.items[it - prefix[lo]], W, lane);
   }
 }
 
@@ -1138,9 +1207,9 @@ void p2p_launch_v(const TV& t, const MixedData& M, const double2* xe64, int ndc,
   constexpr size_t sm = 4 * sizeof(P2PWarp<ND, KIND, P2P_SHAPES[V].chunk>);
   auto kern = k_p2p_leaf<ND, IFPGH, KIND, V>;
   set_smem_attr(kern, sm);
-  kern<<<resident_grid(kern, 128, sm), 128, sm, st>>>(t, M.xs64, xe64, M.q.p, M.d.p, ndc, d0,
-                                                     thresh, items, nitems,
-                                                     xe64 == M.xs64 ? 1 : 0, pot, grad, hess);
+  const P2PJob J{t.ctl, t.boxsize, M.xs64, xe64, M.q.p, M.d.p, items, nitems, pot, grad, hess,
+                 thresh, ndc, d0, xe64 == M.xs64 ? 1 : 0, 0};
+  kern<<<resident_grid(kern, 128, sm), 128, sm, st>>>(J);
   B2_LAUNCH_CHECK();
 }
 
@@ -1225,6 +1294,42 @@ void leaf_dispatch(int ifl, const TV& t, int use_targets, const MixedData& M,
     leaf_launch<ND, 2>(t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
   else
     leaf_launch<ND, 3>(t, use_targets, M, xe64, ndc, d0, P, mp, lo, thresh, ifnear, pot, grad, hess, st, far_done);
+}
+
+template <int ND, int IFPGH, int KIND, int V>
+void p2p_batch_group(const P2PJob* jobs, int njobs, int* prefix, cudaStream_t st) {
+  constexpr size_t sm = 4 * sizeof(P2PWarp<ND, KIND, P2P_SHAPES[V].chunk>);
+  auto kern = k_p2p_batch<ND, IFPGH, KIND, V>;
+  set_smem_attr(kern, sm);
+  k_p2p_batch_prefix<<<1, 256, 0, st>>>(jobs, njobs, prefix);
+  B2_LAUNCH_CHECK();
+  kern<<<resident_grid(kern, 128, sm), 128, sm, st>>>(jobs, njobs, prefix);
+  B2_LAUNCH_CHECK();
+}
+
+template <int ND, int IFPGH, int KIND>
+void p2p_batch_shape(int v, const P2PJob* jobs, int njobs, int* prefix, cudaStream_t st) {
+  if constexpr (p2p_tuned(ND, IFPGH)) {
+    if (v == 1) return p2p_batch_group<ND, IFPGH, KIND, 1>(jobs, njobs, prefix, st);
+    if (v == 2) return p2p_batch_group<ND, IFPGH, KIND, 2>(jobs, njobs, prefix, st);
+  }
+  p2p_batch_group<ND, IFPGH, KIND, 0>(jobs, njobs, prefix, st);
+}
+
+template <int ND, int IFPGH>
+void p2p_batch_kind(int kind, int v, const P2PJob* jobs, int njobs, int* prefix,
+                    cudaStream_t st) {
+  if (kind == 3) p2p_batch_shape<ND, IFPGH, 3>(v, jobs, njobs, prefix, st);
+  else if (kind == 2) p2p_batch_shape<ND, IFPGH, 2>(v, jobs, njobs, prefix, st);
+  else p2p_batch_shape<ND, IFPGH, 1>(v, jobs, njobs, prefix, st);
+}
+
+template <int ND>
+void p2p_batch_ifl(int ifl, int kind, int v, const P2PJob* jobs, int njobs, int* prefix,
+                   cudaStream_t st) {
+  if (ifl == 1) p2p_batch_kind<ND, 1>(kind, v, jobs, njobs, prefix, st);
+  else if (ifl == 2) p2p_batch_kind<ND, 2>(kind, v, jobs, njobs, prefix, st);
+  else p2p_batch_kind<ND, 3>(kind, v, jobs, njobs, prefix, st);
 }
 
 }  // namespace
@@ -1340,6 +1445,72 @@ void lap_fp64_leaf(int ND, int ifl, const TV& t, int use_targets, const MixedDat
     default: run(std::integral_constant<int, 1>()); break;
   }
 }
+
+struct P2PBatch {
+  struct Group {
+    int ND, ifl, kind, shape, njobs;
+    P2PJob* jobs;  // device
+    int* prefix;   // device, njobs + 1
+  };
+  std::vector<Group> groups;
+  ~P2PBatch() {
+    for (auto& g : groups) {
+      cudaFree(g.jobs);
+      cudaFree(g.prefix);
+    }
+  }
+};
+
+P2PBatch* p2p_batch_create(const std::vector<P2PBatchEntry>& E) {
+  std::unique_ptr<P2PBatch> B(new P2PBatch());
+  std::vector<int> done(E.size(), 0);
+  for (size_t i = 0; i < E.size(); i++) {
+    if (done[i]) continue;
+    const P2PBatchEntry& e = E[i];
+    const int kind = (e.M->q.p ? 1 : 0) | (e.M->d.p ? 2 : 0);
+    if (kind == 0) {
+      done[i] = 1;
+      continue;
+    }
+    // the tile shape each plan's own near field would use
+    auto shape_of = [](const P2PBatchEntry& x) {
+      return x.ND <= 2 && x.ifl <= 2 ? g_p2p_shape[p2p_leaf_class(x.M->ndiv)].load() : 0;
+    };
+    const int shape = shape_of(e);
+    std::vector<P2PJob> jobs;
+    for (size_t k = i; k < E.size(); k++) {
+      const P2PBatchEntry& f = E[k];
+      const int fk = (f.M->q.p ? 1 : 0) | (f.M->d.p ? 2 : 0);
+      if (done[k] || f.ND != e.ND || f.ifl != e.ifl || fk != kind || shape_of(f) != shape)
+        continue;
+      done[k] = 1;
+      jobs.push_back(P2PJob{f.tv->ctl, f.tv->boxsize, f.M->xs64, f.xe64, f.M->q.p, f.M->d.p,
+                            (const P2PItem*)(f.use_targets ? f.M->items_t.p : f.M->items_s.p),
+                            f.M->nitems.p + (f.use_targets ? 1 : 0), f.pot, f.grad, f.hess,
+                            -1.0, f.ndc, 0, f.xe64 == f.M->xs64 ? 1 : 0, 0});
+    }
+    P2PBatch::Group g{e.ND, e.ifl, kind, shape, (int)jobs.size(), nullptr, nullptr};
+    B2_CHECK(cudaMalloc(&g.jobs, sizeof(P2PJob) * jobs.size()));
+    B2_CHECK(cudaMalloc(&g.prefix, sizeof(int) * (jobs.size() + 1)));
+    B->groups.push_back(g);
+    B2_CHECK(cudaMemcpy(g.jobs, jobs.data(), sizeof(P2PJob) * jobs.size(),
+                        cudaMemcpyHostToDevice));
+  }
+  return B.release();
+}
+
+void p2p_batch_launch(const P2PBatch* B, cudaStream_t st) {
+  for (const auto& g : B->groups) {
+    switch (g.ND) {
+      case 8: p2p_batch_ifl<8>(g.ifl, g.kind, g.shape, g.jobs, g.njobs, g.prefix, st); break;
+      case 4: p2p_batch_ifl<4>(g.ifl, g.kind, g.shape, g.jobs, g.njobs, g.prefix, st); break;
+      case 2: p2p_batch_ifl<2>(g.ifl, g.kind, g.shape, g.jobs, g.njobs, g.prefix, st); break;
+      default: p2p_batch_ifl<1>(g.ifl, g.kind, g.shape, g.jobs, g.njobs, g.prefix, st); break;
+    }
+  }
+}
+
+void p2p_batch_free(P2PBatch* B) { delete B; }
 
 void lap_mixed_leaf(int ND, int ifl, const TV& t, int nb, int use_targets, const MixedData& M,
                     const double2* xe64, int ndc, int d0, int P, const double2* mp,

@@ -1,7 +1,10 @@
-// Mixed-precision kernels of the Laplace FMM (used when eps >= 1e-6 or when
-// requested): FP32 M2L and a FP32 near field with double-float coordinate
-// differences; expansions, shifts, L2P and M2P stay FP64.
+// Leaf and M2L kernels of the Laplace FMM.  Mixed precision (eps >= 1e-6 or
+// when requested): M2L on the tensor cores (or FP32 CUDA cores), L2P / M2P
+// in FP32, an FP32 near field over leaf-relative two-float offsets; the
+// expansion coefficients and shifts stay FP64.  The FP64 path's leaf passes
+// (far field, FP64 near field on the same work items) live here too.
 #pragma once
+#include <vector>
 #include "lap_common.cuh"
 #include "../../include/fmm2d_b200.h"
 #include "tc_m2l.cuh"
@@ -52,6 +55,23 @@ void lap_fp64_leaf(int ND, int ifl, const lapk::TV& t, int use_targets, const Mi
                    const double2* xe64, const lapk::Dens& D, int P, const double2* mp,
                    const double2* lo, double thresh, int ifnear, double2* pot, double2* grad,
                    double2* hess, cudaStream_t st);
+
+// The mixed near field of many trees in one persistent launch per group of
+// (ND, pot/grad/hess level, density kind): every entry is the deferred
+// near-field pass of one tree (its far field already in pot / grad / hess,
+// tree order, a single density chunk of ndc <= 8).  create builds the
+// device job tables (outside any capture); launch is stream work only.
+struct P2PBatchEntry {
+  const lapk::TV* tv;
+  const MixedData* M;
+  const double2* xe64;  // sorted evaluation points (M->xs64 for the sources)
+  int use_targets, ndc, ND, ifl;
+  double2 *pot, *grad, *hess;
+};
+struct P2PBatch;
+P2PBatch* p2p_batch_create(const std::vector<P2PBatchEntry>& entries);
+void p2p_batch_launch(const P2PBatch* b, cudaStream_t st);
+void p2p_batch_free(P2PBatch* b);
 
 // Near-field tile shape per leaf-size class (0: ndiv <= 20, 1: <= 56,
 // 2: larger); set_p2p_shape returns IER_BADARG for an unknown class or shape.

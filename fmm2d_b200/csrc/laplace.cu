@@ -977,8 +977,10 @@ template <int ND>
 void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int P,
                const double2* xs, const double2* xt, double2* mp, double2* lo, double2* ps,
                double2* gs, double2* hs, double2* pt, double2* gt, double2* ht, const Launch& X,
-               cudaStream_t st, cudaEvent_t* ev, const MixedData* M, const MixedData& LD) {
+               cudaStream_t st, cudaEvent_t* ev, const MixedData* M, const MixedData& LD,
+               bool skip_near) {
   const double* binom = device_binomials();
+  const int ifnear = skip_near ? 0 : a.ifnear;
   const int nb = X.nb;
   const bool dev = X.dev;
   const int nl = dev ? 0 : T.nlevels;
@@ -1077,11 +1079,11 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
     if (ifl <= 0) return;
     if (M) {
       // ev[7]: between the far-field and near-field kernels of the sources
-      lap_mixed_leaf(ND, ifl, tv, nb, use_t, *M, xe, D.ndc, D.d0, P, mp, lo, thresh, a.ifnear, po,
+      lap_mixed_leaf(ND, ifl, tv, nb, use_t, *M, xe, D.ndc, D.d0, P, mp, lo, thresh, ifnear, po,
                      gr, he, st, use_t == 0 ? ev[7] : nullptr);
       return;
     }
-    lap_fp64_leaf(ND, ifl, tv, use_t, LD, xe, D, P, mp, lo, thresh, a.ifnear, po, gr, he, st);
+    lap_fp64_leaf(ND, ifl, tv, use_t, LD, xe, D, P, mp, lo, thresh, ifnear, po, gr, he, st);
   };
   leaf(0, a.ifpgh, xs, ps, gs, hs);
   leaf(1, a.ifpghtarg, xt, pt, gt, ht);
@@ -1335,7 +1337,16 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
 int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const double* dipvec,
                   double* pot, double* grad, double* hess, double* pottarg, double* gradtarg,
                   double* hesstarg, cudaStream_t st, bool sync, double* timeinfo) {
-  if (!pp) return IER_BADARG;
+  return lap_plan_eval_part(pp, charge, dipstr, dipvec, pot, grad, hess, pottarg, gradtarg,
+                            hesstarg, st, sync, timeinfo, 0);
+}
+
+int lap_plan_eval_part(LapPlan* pp, const double* charge, const double* dipstr,
+                       const double* dipvec, double* pot, double* grad, double* hess,
+                       double* pottarg, double* gradtarg, double* hesstarg, cudaStream_t st,
+                       bool sync, double* timeinfo, int part) {
+  if (!pp || part < 0 || part > 2) return IER_BADARG;
+  if (part != 0 && !lap_plan_defers_near(pp)) return IER_BADARG;
   LapPlan& p = *pp;
   const LapArgs& a = p.a;
   if ((charge != nullptr) != p.fc || (dipstr != nullptr) != p.fd) return IER_BADARG;
@@ -1362,6 +1373,9 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
   DeviceTree& T = p.T;
   const long ns = p.ns, nt = p.nt;
   const int nd = p.nd, ndc = p.ndc, P = p.P;
+  double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // part 2: only the unpack of a near field added by the batched pass
+  if (part != 2) {
   k_gather_dens<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, T.isrc.p, ns, charge, dipstr,
                                                    dipvec, p.qs.p, p.ds.p);
   B2_LAUNCH_CHECK();
@@ -1370,16 +1384,15 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
   const MixedData* Mp = p.mixed ? &p.MD : nullptr;
   const Launch X{T.nboxes, p.dev, p.gbar.p, p.err.p,
                  p.dev ? level_hint(p.ns + p.nt, p.ndiv) : 0};
-  double tsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int d0 = 0; d0 < ndc;) {
     int left = ndc - d0;
     int ND = left >= 8 ? 8 : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
     Dens D{p.fc ? p.qs.p : nullptr, p.fd ? p.ds.p : nullptr, ndc, d0};
     switch (ND) {
-      case 8: run_chunk<8>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
-      case 4: run_chunk<4>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
-      case 2: run_chunk<2>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
-      default: run_chunk<1>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD); break;
+      case 8: run_chunk<8>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD, part == 1); break;
+      case 4: run_chunk<4>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD, part == 1); break;
+      case 2: run_chunk<2>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD, part == 1); break;
+      default: run_chunk<1>(p.tv, T, a, D, P, p.xs.p, p.xt.p, p.mp.p, p.lo.p, p.ps.p, p.gs.p, p.hs.p, p.pt.p, p.gt.p, p.ht.p, X, st, p.ev, Mp, p.MD, part == 1); break;
     }
     if (timeinfo) {
       B2_CHECK(cudaEventSynchronize(p.ev[6]));
@@ -1406,6 +1419,9 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
     }
     d0 += ND;
   }
+  }
+  // part 1: the near field comes from the batched pass, then part 2
+  if (part == 1) return IER_OK;
   if (a.ifpgh > 0) {
     k_unpack<<<ceil_div(ns, 256), 256, 0, st>>>(a.fe, nd, ndc, a.ifpgh, p.inv_s.p, ns, p.ps.p,
                                                 p.gs.p, p.hs.p, pot, grad, hess);
@@ -1426,6 +1442,22 @@ int lap_plan_eval(LapPlan* pp, const double* charge, const double* dipstr, const
     for (int i = 0; i < 8; i++) timeinfo[i] = tsum[i];
   if (sync) return finish(p, st);
   return IER_OK;
+}
+
+bool lap_plan_defers_near(const LapPlan* p) {
+  // one density chunk (ndc 1, 2, 4 or 8), mixed precision, with a near field
+  return p && p->mixed && !p->zero && p->a.ifnear &&
+         (p->ndc == 1 || p->ndc == 2 || p->ndc == 4 || p->ndc == 8);
+}
+
+void lap_plan_near_entries(LapPlan* p, std::vector<P2PBatchEntry>& out) {
+  if (!lap_plan_defers_near(p)) return;
+  if (p->a.ifpgh > 0)
+    out.push_back(P2PBatchEntry{&p->tv, &p->MD, p->xs.p, 0, p->ndc, p->ndc, p->a.ifpgh, p->ps.p,
+                                p->gs.p, p->hs.p});
+  if (p->nt > 0 && p->a.ifpghtarg > 0)
+    out.push_back(P2PBatchEntry{&p->tv, &p->MD, p->xt.p, 1, p->ndc, p->ndc, p->a.ifpghtarg,
+                                p->pt.p, p->gt.p, p->ht.p});
 }
 
 int lap_plan_status(LapPlan* p) {

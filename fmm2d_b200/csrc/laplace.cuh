@@ -1,6 +1,8 @@
 // Cauchy/Laplace FMM engine (the path of src/laplace/cfmm2d.f, lfmm2d.f,
 // rfmm2d.f) on device memory.
 #pragma once
+#include <vector>
+
 #include "common.cuh"
 #include "tree.cuh"
 
@@ -77,6 +79,20 @@ void set_device_ranges(bool on);
 int lap_plan_eval(LapPlan* p, const double* charge, const double* dipstr, const double* dipvec,
                   double* pot, double* grad, double* hess, double* pottarg, double* gradtarg,
                   double* hesstarg, cudaStream_t st, bool sync, double* timeinfo);
+// The same in parts, for batches whose mixed near fields run as one pass
+// (p2p_batch_launch over lap_plan_near_entries): part 1 runs everything up
+// to the far field of the leaves, part 2 only the unsort into the caller's
+// outputs; part 0 is the whole evaluation.  Parts 1 and 2 are for plans
+// with lap_plan_defers_near (IER_BADARG otherwise).
+int lap_plan_eval_part(LapPlan* p, const double* charge, const double* dipstr,
+                       const double* dipvec, double* pot, double* grad, double* hess,
+                       double* pottarg, double* gradtarg, double* hesstarg, cudaStream_t st,
+                       bool sync, double* timeinfo, int part);
+bool lap_plan_defers_near(const LapPlan* p);
+// The plan's deferred near-field passes (sources, targets) as batch entries
+// (P2PBatchEntry: csrc/lap_mixed.cuh).
+struct P2PBatchEntry;
+void lap_plan_near_entries(LapPlan* p, std::vector<P2PBatchEntry>& out);
 // IER_TIMEOUT when a bounded tensor-core wait of an earlier evaluation gave
 // up, else IER_OK; clears the flag.  Synchronises the device.
 int lap_plan_status(LapPlan* p);
