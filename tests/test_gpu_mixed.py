@@ -145,3 +145,26 @@ def test_near_field_tile_shapes_agree(gpu, oracle):
     finally:
         for c, s in enumerate(saved):
             L.b2fmm_set_p2p_shape(c, s)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+@pytest.mark.parametrize("nd", [4, 8, 11])
+def test_many_densities_vs_oracle(gpu, oracle, precision, nd):
+    """nd = 4 and 8 density vectors (one chunk of the widest near-field and
+    far-field kernels) and nd = 11 (chunks of 8, 2 and 1), with hessians:
+    equal to the oracle within eps (mixed) or round-off (FP64)."""
+    rng = np.random.default_rng(40 + nd)
+    n, nt = 9000, 3000
+    src = _gauss16(rng, n)
+    trg = rng.uniform(src.min(), src.max(), (2, nt))
+    q = rng.normal(size=(nd, n)) + 1j * rng.normal(size=(nd, n))
+    d = rng.normal(size=(nd, n)) + 1j * rng.normal(size=(nd, n))
+    out = fmm.cfmm2d(eps=1e-6, sources=src, charges=q, dipstr=d, targets=trg, pg=3, pgt=3,
+                     nd=nd, precision=precision)
+    ref = oracle.cfmm2d(1e-6, src, charges=q, dipstr=d, targets=trg, ifpgh=3, ifpghtarg=3,
+                        nd=nd)
+    tol = 1e-6 if precision == "mixed" else 1e-11
+    for k in ("pot", "grad", "hess"):
+        assert rel_l2(getattr(out, k), ref[k]) < tol, k
+    for k in ("pottarg", "gradtarg", "hesstarg"):
+        assert rel_l2(getattr(out, k), ref[k]) < tol, k
