@@ -12,8 +12,11 @@ ABI b2fmm_lfmm2d_dev) in the mixed-precision mode; the K timed calls are
 queued back to back (options.async_call: no host wait inside or between
 them) and their device status is checked after the timing.  ``fp64_value``
 is the plain FP64 GPU FMM on the same inputs, timed the same way; ``e2e``
-calls the host-pointer entry point b2fmm_lfmm2d_ex with pinned host buffers
-(H2D + FMM + D2H per step, one wait per call).  Every run reports the
+calls the queued host-pointer entry point b2fmm_lfmm2d_host_async with pinned
+host buffers on two streams in turn (every step copies its inputs in and its
+results out; one step's copies overlap the other's FMM; wall clock from the
+first call to both streams finished), ``e2e_blocking`` the blocking
+b2fmm_lfmm2d_ex (one wait per call).  Every run reports the
 relative l2 error of pot+grad against the FP64 direct sum over 1000 random
 sources.  ``--impl reference`` times the reference itself (its Fortran
 translated to C by oracle/f77c.py, gcc -O3 -fopenmp; no Fortran compiler
@@ -800,6 +803,7 @@ def main():
         if ier.value != 0:
             raise RuntimeError(f"b2fmm_lfmm2d_ex ier={ier.value}")
 
+    # blocking calls: copies in, FMM, copies out, one wait per call
     for _ in range(max(1, args.warmup - 1)):
         e2e_step()
     if pg:
@@ -807,7 +811,49 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
+    te_block = max_over_ranks((time.perf_counter() - t0) / args.steps, pg, dev)
+
+    # queued calls (b2fmm_lfmm2d_host_async) on two streams in turn, each
+    # with its own pinned result arrays: one call's copies overlap the other's
+    # FMM; every step still copies its inputs in and its results out
+    streams = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
+    hpot2 = [hpot, torch.empty_like(hpot).pin_memory()]
+    hgrad2 = [hgrad, torch.empty_like(hgrad).pin_memory()]
+
+    def e2e_async(k):
+        ier = C.c_int(0)
+        o = _lib.Options()
+        o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, _lib.PREC[prec]
+        L.b2fmm_lfmm2d_host_async(1, C.c_double(1e-6), C.c_int64(n), ptr(hsrc), 1, ptr(hq_), 1,
+                                  ptr(hd_), ptr(hv_), 2, ptr(hpot2[k % 2]), ptr(hgrad2[k % 2]),
+                                  None, C.c_int64(0), None, 0, None, None, None, C.byref(o),
+                                  C.c_void_p(streams[k % 2].cuda_stream), C.byref(ier))
+        if ier.value != 0:
+            raise RuntimeError(f"b2fmm_lfmm2d_host_async ier={ier.value}")
+
+    def queued_status():
+        for s_ in streams:
+            ier = C.c_int(0)
+            L.b2fmm_async_status(C.c_void_p(s_.cuda_stream), C.byref(ier))
+            if ier.value != 0:
+                raise RuntimeError(f"b2fmm_lfmm2d_host_async: device status {ier.value}")
+
+    for k in range(max(2, args.warmup - 1)):
+        e2e_async(k)
+    torch.cuda.synchronize()
+    queued_status()
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        e2e_async(k)
+    for s_ in streams:
+        s_.synchronize()
     te = max_over_ranks((time.perf_counter() - t0) / args.steps, pg, dev)
+    queued_status()
+    # the queued calls' results against the blocking call's
+    e2e_diff = float(torch.linalg.norm((hpot2[(args.steps - 1) % 2] - hpot).flatten()) /
+                     torch.linalg.norm(hpot.flatten())) if args.steps > 1 else 0.0
     h2d = hsrc.numel() * 8 + hq_.numel() * 16 + hd_.numel() * 16 + hv_.numel() * 8
     d2h = hpot.numel() * 16 + hgrad.numel() * 16
 
@@ -860,8 +906,13 @@ def main():
                            "l2_policy": "inputs (256 MB) and expansions larger than L2"},
                 "err_ref": "FP64 direct sum over 1000 random sources",
                 "mixed_cuda_core_m2l_ms_per_step": ms_cc,
+                "e2e_blocking": {"value": world * n / te_block, "unit": "points/s",
+                                 "ms_per_step": te_block * 1e3,
+                                 "call": "b2fmm_lfmm2d_ex, one wait per call"},
                 "e2e": {"value": world * n / te, "unit": "points/s", "h2d_bytes_per_step": h2d,
-                        "d2h_bytes_per_step": d2h},
+                        "d2h_bytes_per_step": d2h, "ms_per_step": te * 1e3,
+                        "call": "b2fmm_lfmm2d_host_async on two streams in turn",
+                        "rel_diff_vs_blocking_call": e2e_diff},
                 "gpu_launches": int(launches),
                 "roofline": rl, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(line), flush=True)

@@ -37,6 +37,9 @@ SIGNATURES = {
     "b2fmm_cfmm2d_ex": _LAP_HOST + _PGH + [P, P, P],
     "b2fmm_lfmm2d_ex": _LAP_HOST + [P] + _PGH + [P, P, P],
     "b2fmm_rfmm2d_ex": _LAP_HOST + [P] + _PGH + [P, P, P],
+    "b2fmm_cfmm2d_host_async": _LAP_HOST + _PGH + [P, P, P],
+    "b2fmm_lfmm2d_host_async": _LAP_HOST + [P] + _PGH + [P, P, P],
+    "b2fmm_rfmm2d_host_async": _LAP_HOST + [P] + _PGH + [P, P, P],
     "b2fmm_cfmm2d_dev": _LAP_HOST + _PGH + [P, P, P, P],
     "b2fmm_lfmm2d_dev": _LAP_HOST + [P] + _PGH + [P, P, P, P],
     "b2fmm_rfmm2d_dev": _LAP_HOST + [P] + _PGH + [P, P, P, P],

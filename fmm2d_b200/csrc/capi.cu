@@ -110,9 +110,12 @@ SideStream& side_stream() {
 // Host-pointer driver: copies inputs to the device, runs, copies results back.
 // The point coordinates go first on the main stream (the tree needs them);
 // the densities follow on a side stream while the tree is being built, and
-// the evaluation waits for them.
-int lap_host(LapArgs h) {
-  cudaStream_t st = cudaStreamPerThread;
+// the evaluation waits for them.  async: everything is queued on st and the
+// call returns without waiting (device buffers are freed in stream order
+// after the copies back; failures go to the device's status word,
+// lap_async_status); otherwise one wait at the end.
+int lap_host(LapArgs h, cudaStream_t st = cudaStreamPerThread, bool async = false) {
+  if (h.timeinfo) async = false;
   const int nd = h.nd;
   const long ns = h.ns, nt = h.nt;
   const int cw = h.fe == FE_REAL ? 1 : 2;
@@ -176,6 +179,14 @@ int lap_host(LapArgs h) {
     down(h.gradtarg, a.gradtarg, nq * gw * nt);
     down(h.hesstarg, a.hesstarg, nq * hw * nt);
   };
+  if (async) {
+    a.async_call = true;
+    a.status_word = nullptr;  // the device's status word
+    int r = lap_fmm_device(a, st, ss.copies_done);
+    if (r != IER_OK) return r;
+    down_all();
+    return IER_OK;
+  }
   // the whole call (copies in, FMM, copies out) is queued before the one
   // wait; the FMM's outcome comes back in the call's own status word
   DBuf<int> status(st);
@@ -411,6 +422,48 @@ void b2fmm_rfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int 
     return lap_host(make_args(FE_REAL, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
                               dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
                               gradtarg, hesstarg, opts, timeinfo));
+  });
+}
+
+void b2fmm_cfmm2d_host_async(int nd, double eps, int64_t ns, const double* sources,
+                             int ifcharge, const double* charge, int ifdipole,
+                             const double* dipstr, int ifpgh, double* pot, double* grad,
+                             double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                             double* pottarg, double* gradtarg, double* hesstarg,
+                             const b2fmm_options* opts, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_CAUCHY, nd, eps, ns, sources, ifcharge, charge, ifdipole,
+                              dipstr, nullptr, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+                              pottarg, gradtarg, hesstarg, opts, nullptr),
+                    (cudaStream_t)stream, true);
+  });
+}
+
+void b2fmm_lfmm2d_host_async(int nd, double eps, int64_t ns, const double* sources,
+                             int ifcharge, const double* charge, int ifdipole,
+                             const double* dipstr, const double* dipvec, int ifpgh, double* pot,
+                             double* grad, double* hess, int64_t nt, const double* targ,
+                             int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                             const b2fmm_options* opts, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_LAPLACE, nd, eps, ns, sources, ifcharge, charge, ifdipole,
+                              dipstr, dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg,
+                              pottarg, gradtarg, hesstarg, opts, nullptr),
+                    (cudaStream_t)stream, true);
+  });
+}
+
+void b2fmm_rfmm2d_host_async(int nd, double eps, int64_t ns, const double* sources,
+                             int ifcharge, const double* charge, int ifdipole,
+                             const double* dipstr, const double* dipvec, int ifpgh, double* pot,
+                             double* grad, double* hess, int64_t nt, const double* targ,
+                             int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                             const b2fmm_options* opts, void* stream, int* ier) {
+  guarded(ier, [&] {
+    return lap_host(make_args(FE_REAL, nd, eps, ns, sources, ifcharge, charge, ifdipole, dipstr,
+                              dipvec, ifpgh, pot, grad, hess, nt, targ, ifpghtarg, pottarg,
+                              gradtarg, hesstarg, opts, nullptr),
+                    (cudaStream_t)stream, true);
   });
 }
 

@@ -117,6 +117,35 @@ void b2fmm_rfmm2d_ex(int nd, double eps, int64_t ns, const double* sources, int 
                      double* gradtarg, double* hesstarg, const b2fmm_options* opts,
                      double* timeinfo, int* ier);
 
+/* Host-pointer calls that return once queued (no counterpart in the
+ * reference, whose calls are all blocking): the copies in, the FMM and the
+ * copies back are enqueued on `stream` and the call returns; the results are
+ * in the host arrays once the stream has finished (b2fmm_async_status waits
+ * for it and returns the first failure, 104 meaning the call's tree needed
+ * the synchronous build: repeat it with b2fmm_{c,l,r}fmm2d_ex).  The host
+ * arrays must stay valid until then and should be pinned (page-locked), or
+ * the copies run synchronously.  Calls on different streams overlap: one
+ * call's copies with another's FMM.  Same arguments as the _ex calls,
+ * without timeinfo. */
+void b2fmm_cfmm2d_host_async(int nd, double eps, int64_t ns, const double* sources,
+                             int ifcharge, const double* charge, int ifdipole,
+                             const double* dipstr, int ifpgh, double* pot, double* grad,
+                             double* hess, int64_t nt, const double* targ, int ifpghtarg,
+                             double* pottarg, double* gradtarg, double* hesstarg,
+                             const b2fmm_options* opts, void* stream, int* ier);
+void b2fmm_lfmm2d_host_async(int nd, double eps, int64_t ns, const double* sources,
+                             int ifcharge, const double* charge, int ifdipole,
+                             const double* dipstr, const double* dipvec, int ifpgh, double* pot,
+                             double* grad, double* hess, int64_t nt, const double* targ,
+                             int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                             const b2fmm_options* opts, void* stream, int* ier);
+void b2fmm_rfmm2d_host_async(int nd, double eps, int64_t ns, const double* sources,
+                             int ifcharge, const double* charge, int ifdipole,
+                             const double* dipstr, const double* dipvec, int ifpgh, double* pot,
+                             double* grad, double* hess, int64_t nt, const double* targ,
+                             int ifpghtarg, double* pottarg, double* gradtarg, double* hesstarg,
+                             const b2fmm_options* opts, void* stream, int* ier);
+
 /* Device-pointer variants of cfmm2d / lfmm2d / rfmm2d (same argument meaning;
  * opts may be NULL for the reference defaults; timeinfo may be NULL). */
 void b2fmm_cfmm2d_dev(int nd, double eps, int64_t ns, const double* sources, int ifcharge,

@@ -154,3 +154,55 @@ def test_deep_duplicate_tree(gpu, oracle):
     o = oracle.lfmm2d(1e-9, src, charges=call.qh, dipstr=call.dh, dipvec=call.vh, ifpgh=2)
     assert rel_l2(pot.cpu().numpy()[:, 0], o["pot"][0]) < 1e-11
     assert rel_l2(grad.cpu().numpy()[:, :, 0].T, o["grad"][0]) < 1e-11
+
+
+def test_queued_host_calls_on_two_streams(gpu):
+    """b2fmm_lfmm2d_host_async / cfmm2d / rfmm2d with pinned host arrays:
+    four calls queued on two streams in turn give, bit for bit, the blocking
+    host call's results, and b2fmm_async_status reports no failure."""
+    L = _lib.lib()
+    n = 60000
+    call = Call(gauss16(n, 7), 3)
+    pin = lambda a: torch.as_tensor(np.ascontiguousarray(a)).pin_memory()
+    hs, hq, hd, hv = (pin(x.cpu()) for x in (call.s, call.q, call.d, call.v))
+    o = _lib.Options()
+    o.ndiv, o.idivflag, o.ifnear, o.precision = 0, 0, 1, _lib.PREC["mixed"]
+    ier = C.c_int(-1)
+    bpot = torch.empty((n, 1), dtype=torch.complex128).pin_memory()
+    bgrad = torch.empty((n, 2, 1), dtype=torch.complex128).pin_memory()
+    L.b2fmm_lfmm2d_ex(1, C.c_double(1e-6), C.c_int64(n), _p(hs), 1, _p(hq), 1, _p(hd), _p(hv),
+                      2, _p(bpot), _p(bgrad), None, C.c_int64(0), None, 0, None, None, None,
+                      C.byref(o), None, C.byref(ier))
+    assert ier.value == 0
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    outs = [(torch.empty_like(bpot).pin_memory(), torch.empty_like(bgrad).pin_memory())
+            for _ in range(4)]
+    for k, (po, gr) in enumerate(outs):
+        L.b2fmm_lfmm2d_host_async(1, C.c_double(1e-6), C.c_int64(n), _p(hs), 1, _p(hq), 1,
+                                  _p(hd), _p(hv), 2, _p(po), _p(gr), None, C.c_int64(0), None,
+                                  0, None, None, None, C.byref(o),
+                                  C.c_void_p(streams[k % 2].cuda_stream), C.byref(ier))
+        assert ier.value == 0
+    for s in streams:
+        L.b2fmm_async_status(C.c_void_p(s.cuda_stream), C.byref(ier))
+        assert ier.value == 0
+    for po, gr in outs:
+        assert torch.equal(po, bpot) and torch.equal(gr, bgrad)
+    # the Cauchy and real entry points, against their blocking calls
+    hqr = pin(call.q.real.contiguous().cpu())
+    for fn_async, fn_ex, args in (
+            (L.b2fmm_cfmm2d_host_async, L.b2fmm_cfmm2d_ex, [_p(hq), 0, None]),
+            (L.b2fmm_rfmm2d_host_async, L.b2fmm_rfmm2d_ex, [_p(hqr), 0, None, None])):
+        real = fn_ex is L.b2fmm_rfmm2d_ex
+        dt = torch.float64 if real else torch.complex128
+        p1 = torch.empty((n, 1), dtype=dt).pin_memory()
+        p2 = torch.empty((n, 1), dtype=dt).pin_memory()
+        fn_ex(1, C.c_double(1e-6), C.c_int64(n), _p(hs), 1, *args, 1, _p(p1), None, None,
+              C.c_int64(0), None, 0, None, None, None, C.byref(o), None, C.byref(ier))
+        assert ier.value == 0
+        fn_async(1, C.c_double(1e-6), C.c_int64(n), _p(hs), 1, *args, 1, _p(p2), None, None,
+                 C.c_int64(0), None, 0, None, None, None, C.byref(o),
+                 C.c_void_p(streams[0].cuda_stream), C.byref(ier))
+        assert ier.value == 0
+        L.b2fmm_async_status(C.c_void_p(streams[0].cuda_stream), C.byref(ier))
+        assert ier.value == 0 and torch.equal(p1, p2)
