@@ -10,10 +10,11 @@
 //
 // Kernels (one warp per box unless noted):
 //   k_p2m        P2M at leaves (step 1)
-//   k_m2m        upward pass, one launch per level (step 3)
+//   k_m2m        upward pass, one launch per level (step 3; a block per
+//                chunk of boxes, the quadrant-symmetric operators)
 //   k_p2l        list 4 -> local (step 2)
 //   k_m2l        list 2 multipole -> local (step 4)
-//   k_l2l        downward pass, one launch per level (step 5)
+//   k_l2l        downward pass, one launch per level (step 5; as k_m2m)
 //   leaf passes  (steps 6-8, csrc/lap_mixed.cu) on per-tree work items:
 //                L2P + M2P one point per thread (k_far_mixed), then the
 //                near field one warp per item of up to 32 points of a leaf
@@ -66,13 +67,22 @@ int lap_nterms(double eps) {
 void set_stats(bool on) { g_stats_on = on; }
 const LapStats& last_stats() { return g_last_stats; }
 
-const double* device_binomials() {
+namespace {
+struct DeviceTables {
+  double* binom = nullptr;
+  double2* shift = nullptr;
+};
+
+// The binomials and the M2M / L2L tables of the child (+,+) (the formulas at
+// m2m_level), once per device.
+const DeviceTables& device_tables() {
   static std::mutex mu;
-  static double* tab[128] = {nullptr};
+  static DeviceTables tab[128];
   int dev = 0;
   B2_CHECK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) throw CudaError("device ordinal beyond 127", IER_CUDA);
   std::lock_guard<std::mutex> g(mu);
-  if (!tab[dev]) {
+  if (!tab[dev].binom) {
     // Pascal recursion as in init_carray (src/common/fmmcommon2d.f:150-165)
     std::vector<double> c((size_t)BINOM_N * BINOM_N, 0.0);
     for (int l = 0; l < BINOM_N; l++) c[(size_t)l * BINOM_N] = 1.0;
@@ -81,13 +91,42 @@ const double* device_binomials() {
       for (int l = m + 1; l < BINOM_N; l++)
         c[(size_t)l * BINOM_N + m] = c[(size_t)(l - 1) * BINOM_N + m] + c[(size_t)(l - 1) * BINOM_N + m - 1];
     }
+    // (1 + i)^k, Gaussian integers (exact below k = 106)
+    std::vector<double2> pw(BINOM_N);
+    pw[0] = make_double2(1.0, 0.0);
+    for (int k = 1; k < BINOM_N; k++)
+      pw[k] = make_double2(pw[k - 1].x - pw[k - 1].y, pw[k - 1].x + pw[k - 1].y);
+    std::vector<double2> sh(2 * (size_t)SHIFT_TAB);
+    double2* m2m = sh.data();
+    double2* l2l = m2m + SHIFT_TAB;
+    for (int a = 0; a < BINOM_N; a++)
+      for (int b = 0; b <= a; b++) {
+        const size_t o = (size_t)a * (a + 1) / 2 + b;
+        // M2M B[i = a][j = b]
+        double f;
+        if (a == 0) f = 1.0;
+        else if (b == 0) f = -std::ldexp(1.0, -2 * a) / a;
+        else f = c[(size_t)(a - 1) * BINOM_N + (b - 1)] * std::ldexp(1.0, b - 2 * a);
+        m2m[o] = make_double2(pw[a - b].x * f, pw[a - b].y * f);
+        // L2L E[j = a][i = b]
+        const double e = c[(size_t)a * BINOM_N + b] * std::ldexp(1.0, b - 2 * a);
+        l2l[o] = make_double2(pw[a - b].x * e, pw[a - b].y * e);
+      }
     double* d = nullptr;
+    double2* d2 = nullptr;
     B2_CHECK(cudaMalloc(&d, c.size() * sizeof(double)));
     B2_CHECK(cudaMemcpy(d, c.data(), c.size() * sizeof(double), cudaMemcpyHostToDevice));
-    tab[dev] = d;
+    B2_CHECK(cudaMalloc(&d2, sh.size() * sizeof(double2)));
+    B2_CHECK(cudaMemcpy(d2, sh.data(), sh.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    tab[dev].shift = d2;
+    tab[dev].binom = d;
   }
   return tab[dev];
 }
+}  // namespace
+
+const double* device_binomials() { return device_tables().binom; }
+const double2* device_shift_tables() { return device_tables().shift; }
 
 void configure_mempool(int device) {
   static std::mutex mu;
@@ -237,146 +276,136 @@ __global__ void __launch_bounds__(64, P2M_MIN_BLOCKS(ND)) k_p2m(TV t, int first,
 }
 
 // ---------------------------------------------------------------------------
-// Parents of a level, found without a round of loads per box: a warp takes
-// 32 of its boxes at a time (stride = the grid's warps, so the boxes are
-// dealt as by a warp-per-box loop), each lane loads one box's child count,
-// centre and children, a ballot marks the parents, and the warp then works
-// through them with the box data shuffled from the lane that loaded it.
+// M2M and L2L with the quadrant symmetry.  A child's centre is its parent's
+// plus v_c h, h half the child's size, v_c = u_c (1 + i) with u_c = -1, -i,
+// i, 1 for the reference's child order (-,-), (+,-), (-,+), (+,+), so that
+// with the expansions scaled by the box sizes every translation of the tree
+// is one of four operators that differ by the powers u_c^(i-j).  The
+// operators of the child (+,+) are level-independent tables (built once, on
+// the host, in device_binomials):
+//   M2M  B[i][j] = 2^j (1+i)^(i-j) / 4^i * C(i-1, j-1)  (j >= 1),
+//        B[i][0] = -(1+i)^i / (i 4^i),  B[0][0] = 1;
+//   L2L  E[j][i] = C(j, i) 2^i (1+i)^(j-i) / 4^j  (i <= j),
+// both lower-triangular, row a at a (a + 1) / 2, so that the rows below P
+// are a prefix.  The M2M of a parent is then one triangular product with
+// the children's four-point sums S_m[j] = sum_c u_c^m h_c[j]:
+//   H_i = sum_{j <= i} B[i][j] S_{(i-j) mod 4}[j];
+// the L2L one triangular product split by (j - i) mod 4,
+//   A_q[i] = sum_{j >= i, j - i = q mod 4} E[j][i] l_j,
+// and child c adds sum_q u_c^q A_q[i].  This is the reference's recurrence
+// (laprouts2d.f:905-1015, 1020-1123) with the powers of z0 / r exact (the
+// reference forms z0 from the rounded centres) and a quarter of its work.
+// A block scans 2G boxes of the level at a time (G parents make about two
+// (parent, coefficient, density) items a thread), compacts the parents
+// into shared memory and takes them in groups of up to G: a pass over the
+// items stages the inputs, a second one forms the outputs.  Small chunks
+// give a level many blocks: with chunks of 256 boxes, levels of mostly
+// parents ran a dozen groups one after another per block (M2M 1.37 ms,
+// L2L 2.69 ms at 4M points, against 0.82 and 0.83 ms for the warp-per-
+// parent recurrence); chunks of 2G boxes take 0.46 and 0.52 ms.
 // ---------------------------------------------------------------------------
-struct ParentScan {
-  int nchild;
-  int4 child;
-  double2 center;
-  int2 srng, trng;
-};
+constexpr int SHIFT_THREADS = 128;
 
-__device__ __forceinline__ ParentScan scan_box(const TV& t, int b, bool want_eval) {
-  ParentScan s;
-  s.nchild = t.nchild[b];
-  s.child = t.child[b];
-  s.center = t.center[b];
-  if (want_eval) {
-    s.srng = t.srng[b];
-    s.trng = t.trng[b];
+// i^q z
+__device__ __forceinline__ double2 mul_ipow(double2 z, int q) {
+  double2 r = (q & 1) ? make_double2(-z.y, z.x) : z;
+  if (q & 2) r = make_double2(-r.x, -r.y);
+  return r;
+}
+
+// The parents among the level's boxes [c0, min(c0 + CH, end)) (CH <=
+// SHIFT_THREADS), in box order: their numbers and children in shared
+// memory; returns their count.  need_eval: only parents with evaluation
+// points (L2L).
+__device__ __forceinline__ int collect_parents(const TV& t, int c0, int CH, int end,
+                                               bool need_eval, int* box, int4* ch, int* wcnt) {
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int b = c0 + tid;
+  bool isp = false;
+  int4 c = make_int4(-1, -1, -1, -1);
+  if (tid < CH && b < end) {
+    isp = t.nchild[b] != 0;
+    if (isp && need_eval) {
+      int ne = 0;
+      if (t.ifpghtarg > 0) ne += t.trng[b].y - t.trng[b].x;
+      if (t.ifpgh > 0) ne += t.srng[b].y - t.srng[b].x;
+      isp = ne > 0;
+    }
+    if (isp) c = t.child[b];
   }
-  return s;
+  const unsigned m = __ballot_sync(~0u, isp);
+  if (lane == 0) wcnt[w] = __popc(m);
+  __syncthreads();
+  int off = 0, tot = 0;
+#pragma unroll
+  for (int k = 0; k < SHIFT_THREADS / 32; k++) {
+    const int v = wcnt[k];
+    off += k < w ? v : 0;
+    tot += v;
+  }
+  if (isp) {
+    const int pos = off + __popc(m & ((1u << lane) - 1));
+    box[pos] = b;
+    ch[pos] = c;
+  }
+  __syncthreads();
+  return tot;
 }
 
-__device__ __forceinline__ double2 shfl_d2(double2 v, int src) {
-  return make_double2(__shfl_sync(~0u, v.x, src), __shfl_sync(~0u, v.y, src));
-}
-__device__ __forceinline__ int4 shfl_i4(int4 v, int src) {
-  return make_int4(__shfl_sync(~0u, v.x, src), __shfl_sync(~0u, v.y, src),
-                   __shfl_sync(~0u, v.z, src), __shfl_sync(~0u, v.w, src));
+// Shared memory of a block of the M2M / L2L kernels: the table prefix, the
+// staged inputs of G parents (four sums per item for M2M, one coefficient
+// for L2L), the compacted parents.
+__host__ __device__ constexpr size_t shift_smem(int P, int ND, int G, bool m2m) {
+  return sizeof(double2) * ((size_t)P * (P + 1) / 2 + (size_t)G * P * ND * (m2m ? 4 : 1)) +
+         SHIFT_THREADS * (sizeof(int4) + sizeof(int)) + 32 * sizeof(int);
 }
 
-// ---------------------------------------------------------------------------
-// step 3: M2M (laprouts2d.f:905-1015) from the children with sources.
-// z0 = child - parent; t_j = h_j (r1/z0)^j;
-// H_0 = t_0, H_i = (-t_0/i + sum_{j=1..i} t_j C(i-1, j-1)) (z0/r2)^i
-// One warp per parent: one round of loads brings the children's boxes and
-// (by cp.async, lane = (child, j)) all four children's coefficients into
-// shared memory; the lanes scale them to t, then lane = (child, coefficient
-// group) forms the child's terms and shuffles sum the children.
-// ---------------------------------------------------------------------------
+// step 3: M2M of the level's parents (every parent is written; a child
+// without sources holds a zero expansion and adds nothing).
 template <int ND>
-__device__ __forceinline__ void m2m_level(const TV& t, int first, int n, int lev, int P,
-                                          const double* __restrict__ binom,
+__device__ __forceinline__ void m2m_level(const TV& t, int first, int n, int P, int G,
+                                          const double2* __restrict__ tab,
                                           double2* __restrict__ mp) {
   extern __shared__ double2 smem[];
-  const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  const double r2 = t.boxsize[lev], r1 = t.boxsize[lev + 1];
-  const double ir2 = 1.0 / r2, ir1 = 1.0 / r1;
-  const int PN = P * ND;
-  // per warp: t[child][j][density], then r1 / z0 and z0 / r2 of each child
-  // (both 0 for a child without sources)
-  double2* T = smem + (size_t)wib * (4 * P * ND + 8);
-  double2* W1 = T + 4 * P * ND;
-  double2* W2 = W1 + 4;
-  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
-    const int mine = base + lane * nw;
-    ParentScan s{};
-    if (mine < n) s = scan_box(t, first + mine, false);
-    unsigned pm = __ballot_sync(~0u, mine < n && s.nchild != 0);
-    while (pm) {
-      const int src = __ffs(pm) - 1;
-      pm &= pm - 1;
-      const int b = first + base + src * nw;
-      const double2 c2 = shfl_d2(s.center, src);
-      const int4 ch = shfl_i4(s.child, src);
-      __syncwarp();  // the previous parent's reads of T are done
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        const size_t k = (size_t)child_of(ch, c);
-        for (int x = lane; x < PN; x += 32) cp_async16(&T[c * PN + x], &mp[k * PN + x]);
+  const int PN = P * ND, nt = P * (P + 1) / 2;
+  double2* B = smem;
+  double2* S = B + nt;  // [parent][j][density][m]
+  int4* ch = (int4*)(S + (size_t)G * PN * 4);
+  int* box = (int*)(ch + SHIFT_THREADS);
+  int* wcnt = box + SHIFT_THREADS;
+  for (int e = threadIdx.x; e < nt; e += blockDim.x) B[e] = tab[e];
+  const int end = first + n, CH = min(2 * G, SHIFT_THREADS);
+  for (int c0 = first + blockIdx.x * CH; c0 < end; c0 += gridDim.x * CH) {
+    const int np = collect_parents(t, c0, CH, end, false, box, ch, wcnt);
+    for (int g0 = 0; g0 < np; g0 += G) {
+      const int ne = min(G, np - g0) * PN;
+      for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int p = e / PN, r = e - p * PN;
+        const int4 c = ch[g0 + p];
+        const double2 h0 = mp[(size_t)c.x * PN + r], h1 = mp[(size_t)c.y * PN + r];
+        const double2 h2 = mp[(size_t)c.z * PN + r], h3 = mp[(size_t)c.w * PN + r];
+        const double2 a = cadd(h3, h0), b = cadd(h1, h2), s = csub(h3, h0), dd = csub(h2, h1);
+        double2* o = S + (size_t)e * 4;
+        o[0] = cadd(a, b);
+        o[1] = make_double2(s.x - dd.y, s.y + dd.x);  // s + i dd
+        o[2] = csub(a, b);
+        o[3] = make_double2(s.x + dd.y, s.y - dd.x);  // s - i dd
       }
-      if (lane < 4) {
-        const int k = child_of(ch, lane);
-        const int2 sr = t.srng[k];
-        const double2 c1 = t.center[k];
-        const double2 z0 = make_double2(c1.x - c2.x, c1.y - c2.y);
-        const bool has = sr.y > sr.x;
-        W1[lane] = has ? crcp(make_double2(z0.x * ir1, z0.y * ir1)) : make_double2(0, 0);
-        W2[lane] = has ? make_double2(z0.x * ir2, z0.y * ir2) : make_double2(0, 0);
-      }
-      cp_async_wait_all();
-      __syncwarp();
-      for (int e = lane; e < 4 * P; e += 32) {
-        const int c = (e >= P) + (e >= 2 * P) + (e >= 3 * P), j = e - c * P;
-        const double2 w2 = W2[c];
-        const bool has = !(w2.x == 0.0 && w2.y == 0.0);
-        const double2 a = has ? cpow_int(W1[c], j) : make_double2(0, 0);
-#pragma unroll
-        for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(T[(c * P + j) * ND + d], a);
-      }
-      __syncwarp();
-      // lane = (child c, group g): the child's contributions to the
-      // coefficients i = g, g + 8, ... (the triangular sums over j are spread
-      // over 32 lanes instead of P), summed over the four children by two xor
-      // shuffles
-      const int c = lane >> 3, g = lane & 7;
-      const double2 w2 = W2[c];
-      const double2* tc = T + (size_t)c * P * ND;
-      for (int i0 = 0; i0 < P; i0 += 8) {
-        const int i = i0 + g;
-        double2 v[ND];
-#pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
-        if (i == 0) {
-#pragma unroll
-          for (int d = 0; d < ND; d++) v[d] = tc[d];
-        } else if (i < P && !(w2.x == 0.0 && w2.y == 0.0)) {  // a child without sources adds 0
-          const double* crow = binom + (size_t)(i - 1) * BINOM_N;
-          const double mri = -1.0 / i;
-#pragma unroll
-          for (int d = 0; d < ND; d++) v[d] = make_double2(tc[d].x * mri, tc[d].y * mri);
-          for (int j = 1; j <= i; j++) {
-            const double cb = crow[j - 1];
-#pragma unroll
-            for (int d = 0; d < ND; d++) {
-              const double2 tj = tc[j * ND + d];
-              v[d].x += tj.x * cb;
-              v[d].y += tj.y * cb;
-            }
-          }
-          const double2 bi_ = cpow_int(w2, i);
-#pragma unroll
-          for (int d = 0; d < ND; d++) v[d] = cmul(v[d], bi_);
+      __syncthreads();
+      for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int p = e / PN, r = e - p * PN, i = r / ND, d = r - i * ND;
+        const double2* Br = B + i * (i + 1) / 2;
+        const double2* Sp = S + ((size_t)p * PN + d) * 4;
+        double2 acc0 = make_double2(0, 0), acc1 = make_double2(0, 0);
+        int j = 0;
+        for (; j + 1 <= i; j += 2) {
+          cfma(acc0, Br[j], Sp[j * ND * 4 + ((i - j) & 3)]);
+          cfma(acc1, Br[j + 1], Sp[(j + 1) * ND * 4 + ((i - j - 1) & 3)]);
         }
-#pragma unroll
-        for (int d = 0; d < ND; d++) {
-          v[d].x += __shfl_xor_sync(~0u, v[d].x, 8);
-          v[d].y += __shfl_xor_sync(~0u, v[d].y, 8);
-          v[d].x += __shfl_xor_sync(~0u, v[d].x, 16);
-          v[d].y += __shfl_xor_sync(~0u, v[d].y, 16);
-        }
-        if (c == 0 && i < P) {
-#pragma unroll
-          for (int d = 0; d < ND; d++) mp[((size_t)b * P + i) * ND + d] = v[d];
-        }
+        if (j <= i) cfma(acc0, Br[j], Sp[j * ND * 4 + ((i - j) & 3)]);
+        mp[(size_t)box[g0 + p] * PN + r] = cadd(acc0, acc1);
       }
+      __syncthreads();
     }
   }
 }
@@ -621,101 +650,59 @@ __global__ void __launch_bounds__(128) k_m2l(TV t, int first, int n, int P,
 }
 
 // ---------------------------------------------------------------------------
-// step 5: L2L (laprouts2d.f:1020-1123), z0 = child - parent:
-// t_j = l_j (z0/r1)^j, L_i += (sum_{j>=i} t_j C(j, i)) (r2/z0)^i
-// One warp per parent: one round of loads brings the children's boxes and
-// (by cp.async) the parent's coefficients and the four children's current
-// locals into shared memory; the lanes scale the parent's coefficients to t
-// per child (lane = (child, j)), then each lane produces (child, i)
-// coefficients, dealt so that the lanes' work is balanced.
+// step 5: L2L of the level's parents with evaluation points into their four
+// children (the quadrant-symmetric form above).
 // ---------------------------------------------------------------------------
 template <int ND>
-__device__ __forceinline__ void l2l_level(const TV& t, int first, int n, int lev, int P,
-                                          const double* __restrict__ binom,
+__device__ __forceinline__ void l2l_level(const TV& t, int first, int n, int P, int G,
+                                          const double2* __restrict__ tab,
                                           double2* __restrict__ lo) {
   extern __shared__ double2 smem[];
-  const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  const double r1 = t.boxsize[lev], r2 = t.boxsize[lev + 1];
-  const double ir1 = 1.0 / r1, ir2 = 1.0 / r2;
-  // per warp: the parent's l[j][density], t[child][j][density], the
-  // children's locals U[child][i][density], then z0 / r1 and r2 / z0 of
-  // each child
-  const int PN = P * ND;
-  double2* L = smem + (size_t)wib * (9 * PN + 8);
-  double2* T = L + PN;
-  double2* U = T + 4 * PN;
-  double2* W1 = U + 4 * PN;
-  double2* W2 = W1 + 4;
-  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
-    const int mine = base + lane * nw;
-    ParentScan s{};
-    bool want = false;
-    if (mine < n) {
-      s = scan_box(t, first + mine, true);
-      int ne = 0;
-      if (t.ifpghtarg > 0) ne += s.trng.y - s.trng.x;
-      if (t.ifpgh > 0) ne += s.srng.y - s.srng.x;
-      want = s.nchild != 0 && ne > 0;
-    }
-    unsigned pm = __ballot_sync(~0u, want);
-    while (pm) {
-      const int src = __ffs(pm) - 1;
-      pm &= pm - 1;
-      const int b = first + base + src * nw;
-      const double2 c1 = shfl_d2(s.center, src);
-      const int4 ch = shfl_i4(s.child, src);
-      __syncwarp();  // the previous parent's reads of shared memory are done
-      for (int e = lane; e < PN; e += 32) cp_async16(&L[e], &lo[(size_t)b * PN + e]);
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        const size_t k = (size_t)child_of(ch, c);
-        for (int x = lane; x < PN; x += 32) cp_async16(&U[c * PN + x], &lo[k * PN + x]);
+  const int PN = P * ND, nt = P * (P + 1) / 2;
+  double2* E = smem;
+  double2* L = E + nt;  // [parent][j][density]
+  int4* ch = (int4*)(L + (size_t)G * PN);
+  int* box = (int*)(ch + SHIFT_THREADS);
+  int* wcnt = box + SHIFT_THREADS;
+  for (int e = threadIdx.x; e < nt; e += blockDim.x) E[e] = tab[e];
+  const int end = first + n, CH = min(2 * G, SHIFT_THREADS);
+  for (int c0 = first + blockIdx.x * CH; c0 < end; c0 += gridDim.x * CH) {
+    const int np = collect_parents(t, c0, CH, end, true, box, ch, wcnt);
+    for (int g0 = 0; g0 < np; g0 += G) {
+      const int ne = min(G, np - g0) * PN;
+      for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int p = e / PN, r = e - p * PN;
+        L[e] = lo[(size_t)box[g0 + p] * PN + r];
       }
-      if (lane < 4) {
-        const double2 ck = t.center[child_of(ch, lane)];
-        const double2 z0 = make_double2(ck.x - c1.x, ck.y - c1.y);
-        W1[lane] = make_double2(z0.x * ir1, z0.y * ir1);
-        W2[lane] = crcp(make_double2(z0.x * ir2, z0.y * ir2));
-      }
-      cp_async_wait_all();
-      __syncwarp();
-      for (int e = lane; e < 4 * P; e += 32) {
-        const int c = (e >= P) + (e >= 2 * P) + (e >= 3 * P), j = e - c * P;
-        const double2 a = cpow_int(W1[c], j);
+      __syncthreads();
+      for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+        const int p = e / PN, r = e - p * PN, i = r / ND, d = r - i * ND;
+        const int4 c = ch[g0 + p];
+        // the children's locals first: their loads overlap the sums
+        double2 cur[4];
 #pragma unroll
-        for (int d = 0; d < ND; d++) T[(c * P + j) * ND + d] = cmul(L[j * ND + d], a);
-      }
-      __syncwarp();
-      // items (child, i) cost P - i: dealt in decreasing cost, snaking over
-      // the lanes, so that the lanes' totals come out nearly equal
-      for (int r = 0; r * 32 < 4 * P; r++) {
-        const int e = r * 32 + ((r & 1) ? 31 - lane : lane);
-        if (e >= 4 * P) continue;
-        const int c = e & 3, i = e >> 2;
-        const int k = child_of(ch, c);
-        double2 v[ND];
+        for (int k = 0; k < 4; k++) cur[k] = lo[(size_t)child_of(c, k) * PN + r];
+        const double2* Lp = L + (size_t)p * PN + d;
+        double2 A[4];
 #pragma unroll
-        for (int d = 0; d < ND; d++) v[d] = make_double2(0, 0);
-        const double2* tc = T + (size_t)c * PN;
-        for (int j = i; j < P; j++) {
-          const double cb = binom[(size_t)j * BINOM_N + i];
+        for (int q = 0; q < 4; q++) A[q] = make_double2(0, 0);
+        for (int j0 = i; j0 < P; j0 += 4) {
 #pragma unroll
-          for (int d = 0; d < ND; d++) {
-            const double2 tj = tc[j * ND + d];
-            v[d].x += tj.x * cb;
-            v[d].y += tj.y * cb;
+          for (int q = 0; q < 4; q++) {
+            const int j = j0 + q;
+            if (j < P) cfma(A[q], E[j * (j + 1) / 2 + i], Lp[j * ND]);
           }
         }
-        const double2 bi_ = cpow_int(W2[c], i);
+        // child c adds sum_q u_c^q A_q: (+,+) E + F, (-,-) E - F,
+        // (-,+) G + iH, (+,-) G - iH
+        const double2 Ev = cadd(A[0], A[2]), F = cadd(A[1], A[3]);
+        const double2 Gv = csub(A[0], A[2]), H = csub(A[1], A[3]);
+        const double2 add[4] = {csub(Ev, F), make_double2(Gv.x + H.y, Gv.y - H.x),
+                                make_double2(Gv.x - H.y, Gv.y + H.x), cadd(Ev, F)};
 #pragma unroll
-        for (int d = 0; d < ND; d++) {
-          double2 cur = U[(c * P + i) * ND + d];
-          cfma(cur, v[d], bi_);
-          lo[((size_t)k * P + i) * ND + d] = cur;
-        }
+        for (int k = 0; k < 4; k++) lo[(size_t)child_of(c, k) * PN + r] = cadd(cur[k], add[k]);
       }
+      __syncthreads();
     }
   }
 }
@@ -723,18 +710,18 @@ __device__ __forceinline__ void l2l_level(const TV& t, int first, int n, int lev
 // One level of M2M / L2L per launch (the host knows the level's boxes).
 // (first = RANGE_LEVEL: the level's boxes from the device level table).
 template <int ND>
-__global__ void __launch_bounds__(128) k_m2m(TV t, int first, int n, int lev, int P,
-                                             const double* __restrict__ binom,
-                                             double2* __restrict__ mp) {
+__global__ void __launch_bounds__(SHIFT_THREADS) k_m2m(TV t, int first, int n, int lev, int P, int G,
+                                                       const double2* __restrict__ tab,
+                                                       double2* __restrict__ mp) {
   resolve_range(t, first, n, lev);
-  m2m_level<ND>(t, first, n, lev, P, binom, mp);
+  m2m_level<ND>(t, first, n, P, G, tab, mp);
 }
 template <int ND>
-__global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, int P,
-                                             const double* __restrict__ binom,
-                                             double2* __restrict__ lo) {
+__global__ void __launch_bounds__(SHIFT_THREADS) k_l2l(TV t, int first, int n, int lev, int P, int G,
+                                                       const double2* __restrict__ tab,
+                                                       double2* __restrict__ lo) {
   resolve_range(t, first, n, lev);
-  l2l_level<ND>(t, first, n, lev, P, binom, lo);
+  l2l_level<ND>(t, first, n, P, G, tab, lo);
 }
 
 // The levels >= lev_min in one cooperative launch, the boxes of every level
@@ -744,15 +731,16 @@ __global__ void __launch_bounds__(128) k_l2l(TV t, int first, int n, int lev, in
 // part of a tree deeper than the host expected (nothing when the guess was
 // right).  A barrier that gives up sets *err (the call reports IER_TIMEOUT).
 template <int ND>
-__global__ void __launch_bounds__(128) k_m2m_all(TV t, int P, const double* __restrict__ binom,
-                                                 double2* __restrict__ mp, GridBar* gb,
-                                                 int* err, int lev_min) {
+__global__ void __launch_bounds__(SHIFT_THREADS) k_m2m_all(TV t, int P, int G,
+                                                           const double2* __restrict__ tab,
+                                                           double2* __restrict__ mp, GridBar* gb,
+                                                           int* err, int lev_min) {
   const TreeCtl* c = t.ctl;
   if (c->status != TB_OK) return;
   const int nl = c->nlevels, lo_lev = max(lev_min, 1);
   for (int lev = nl - 1; lev >= lo_lev; lev--) {
     const int first = c->lfirst[lev];
-    m2m_level<ND>(t, first, c->llast[lev] - first + 1, lev, P, binom, mp);
+    m2m_level<ND>(t, first, c->llast[lev] - first + 1, P, G, tab, mp);
     if (lev > lo_lev && !grid_barrier(gb, 1)) {
       if (threadIdx.x == 0) atomicExch(err, 1);
       return;
@@ -760,22 +748,22 @@ __global__ void __launch_bounds__(128) k_m2m_all(TV t, int P, const double* __re
   }
 }
 template <int ND>
-__global__ void __launch_bounds__(128) k_l2l_all(TV t, int P, const double* __restrict__ binom,
-                                                 double2* __restrict__ lo, GridBar* gb,
-                                                 int* err, int lev_min) {
+__global__ void __launch_bounds__(SHIFT_THREADS) k_l2l_all(TV t, int P, int G,
+                                                           const double2* __restrict__ tab,
+                                                           double2* __restrict__ lo, GridBar* gb,
+                                                           int* err, int lev_min) {
   const TreeCtl* c = t.ctl;
   if (c->status != TB_OK) return;
   const int nl = c->nlevels;
   for (int lev = max(lev_min, 1); lev <= nl - 1; lev++) {
     const int first = c->lfirst[lev];
-    l2l_level<ND>(t, first, c->llast[lev] - first + 1, lev, P, binom, lo);
+    l2l_level<ND>(t, first, c->llast[lev] - first + 1, P, G, tab, lo);
     if (lev < nl - 1 && !grid_barrier(gb, 1)) {
       if (threadIdx.x == 0) atomicExch(err, 1);
       return;
     }
   }
 }
-
 // ---------------------------------------------------------------------------
 // gather / unpack
 // ---------------------------------------------------------------------------
@@ -995,15 +983,17 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, all, nb, xs, D, P, mp);
   B2_LAUNCH_CHECK();
   B2_CHECK(cudaEventRecord(ev[1], st));
-  // shared memory per warp of M2M / L2L; up to 4 warps per block, fewer for
-  // high orders with many densities
-  const size_t wm2m = sizeof(double2) * (4 * (size_t)P * ND + 8);
-  const size_t wl2l = sizeof(double2) * (9 * (size_t)P * ND + 8);
-  const int wpb_m2m = (int)std::max<size_t>(1, std::min<size_t>(4, (200 << 10) / wm2m));
-  const int wpb_l2l = (int)std::max<size_t>(1, std::min<size_t>(4, (200 << 10) / wl2l));
-  const size_t sm_m2m = wm2m * wpb_m2m, sm_l2l = wl2l * wpb_l2l;
+  // M2M / L2L: parents per group for about two items a thread
+  const double2* tab_m2m = device_shift_tables();
+  const double2* tab_l2l = tab_m2m + SHIFT_TAB;
+  const int g_m2m = std::max(1, std::min(SHIFT_THREADS / 2, 2 * SHIFT_THREADS / (P * ND)));
+  const int g_l2l = g_m2m;
+  const size_t sm_m2m = shift_smem(P, ND, g_m2m, true), sm_l2l = shift_smem(P, ND, g_l2l, false);
   set_smem_attr(k_m2m<ND>, sm_m2m);
   set_smem_attr(k_l2l<ND>, sm_l2l);
+  // one block per chunk of 2G boxes of a level, at most 64 blocks an SM
+  const int shift_ch = std::min(2 * g_m2m, SHIFT_THREADS);
+  auto shift_grid = [&](long n) { return (int)std::max(1L, std::min<long>(ceil_div(n, shift_ch), 148L * 64)); };
   TV tvc = tv;
   // boxes at level l: at most 4^l and the capacity (grids of the levels the
   // host launches without knowing their size)
@@ -1011,24 +1001,24 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   if (dev) {
     // the part deeper than the expected depth first, then level by level
     set_smem_attr(k_m2m_all<ND>, sm_m2m);
-    const int grid = coop_grid(k_m2m_all<ND>, 32 * wpb_m2m, sm_m2m);
-    int Pv = P, lmin = X.lev_hint;
+    const int grid = coop_grid(k_m2m_all<ND>, SHIFT_THREADS, sm_m2m);
+    int Pv = P, Gv = g_m2m, lmin = X.lev_hint;
     GridBar* gb = X.gb;
     int* err = X.err;
-    void* args[] = {&tvc, &Pv, (void*)&binom, &mp, &gb, &err, &lmin};
+    void* args[] = {&tvc, &Pv, &Gv, (void*)&tab_m2m, &mp, &gb, &err, &lmin};
     B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_m2m_all<ND>, dim3(grid),
-                                         dim3(32 * wpb_m2m), args, sm_m2m, st));
+                                         dim3(SHIFT_THREADS), args, sm_m2m, st));
     B2_LAUNCH_CHECK();
     for (int l = X.lev_hint - 1; l >= 1; l--) {
       const int nbl = level_bound(l);
-      k_m2m<ND><<<warp_grid(nbl, wpb_m2m), 32 * wpb_m2m, sm_m2m, st>>>(tv, RANGE_LEVEL, nbl, l,
-                                                                      P, binom, mp);
+      k_m2m<ND><<<shift_grid(nbl), SHIFT_THREADS, sm_m2m, st>>>(tv, RANGE_LEVEL, nbl, l, P, g_m2m,
+                                                                tab_m2m, mp);
       B2_LAUNCH_CHECK();
     }
   } else {
     for (int l = nl - 1; l >= 1; l--) {
       int f = T.lfirst[l], n = T.llast[l] - f + 1;
-      k_m2m<ND><<<warp_grid(n, wpb_m2m), 32 * wpb_m2m, sm_m2m, st>>>(tv, f, n, l, P, binom, mp);
+      k_m2m<ND><<<shift_grid(n), SHIFT_THREADS, sm_m2m, st>>>(tv, f, n, l, P, g_m2m, tab_m2m, mp);
       B2_LAUNCH_CHECK();
     }
   }
@@ -1052,23 +1042,23 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   if (dev) {
     for (int l = 1; l <= X.lev_hint - 1; l++) {
       const int nbl = level_bound(l);
-      k_l2l<ND><<<warp_grid(nbl, wpb_l2l), 32 * wpb_l2l, sm_l2l, st>>>(tv, RANGE_LEVEL, nbl, l,
-                                                                      P, binom, lo);
+      k_l2l<ND><<<shift_grid(nbl), SHIFT_THREADS, sm_l2l, st>>>(tv, RANGE_LEVEL, nbl, l, P, g_l2l,
+                                                                tab_l2l, lo);
       B2_LAUNCH_CHECK();
     }
     set_smem_attr(k_l2l_all<ND>, sm_l2l);
-    const int grid = coop_grid(k_l2l_all<ND>, 32 * wpb_l2l, sm_l2l);
-    int Pv = P, lmin = X.lev_hint;
+    const int grid = coop_grid(k_l2l_all<ND>, SHIFT_THREADS, sm_l2l);
+    int Pv = P, Gv = g_l2l, lmin = X.lev_hint;
     GridBar* gb = X.gb;
     int* err = X.err;
-    void* args[] = {&tvc, &Pv, (void*)&binom, &lo, &gb, &err, &lmin};
+    void* args[] = {&tvc, &Pv, &Gv, (void*)&tab_l2l, &lo, &gb, &err, &lmin};
     B2_CHECK(cudaLaunchCooperativeKernel((const void*)k_l2l_all<ND>, dim3(grid),
-                                         dim3(32 * wpb_l2l), args, sm_l2l, st));
+                                         dim3(SHIFT_THREADS), args, sm_l2l, st));
     B2_LAUNCH_CHECK();
   } else {
     for (int l = 1; l <= nl - 1; l++) {
       int f = T.lfirst[l], n = T.llast[l] - f + 1;
-      k_l2l<ND><<<warp_grid(n, wpb_l2l), 32 * wpb_l2l, sm_l2l, st>>>(tv, f, n, l, P, binom, lo);
+      k_l2l<ND><<<shift_grid(n), SHIFT_THREADS, sm_l2l, st>>>(tv, f, n, l, P, g_l2l, tab_l2l, lo);
       B2_LAUNCH_CHECK();
     }
   }
@@ -1314,6 +1304,7 @@ int lap_plan_create(const LapArgs& a, cudaStream_t st_in, bool own_stream, LapPl
     }
   }
   device_binomials();
+  device_shift_tables();
   if (p.own) {
     // the plan is evaluated on other streams: finish its construction here
     B2_CHECK(cudaStreamSynchronize(st));

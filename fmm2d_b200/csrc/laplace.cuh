@@ -124,5 +124,10 @@ const LapStats& last_stats();
 // Device binomial table C(l, m), 0 <= m <= l < BINOM_N, row-major (BINOM_N^2).
 constexpr int BINOM_N = 128;
 const double* device_binomials();
+// Device tables of the M2M and L2L operators of the child (+,+), each
+// lower-triangular over 0 <= b <= a < BINOM_N at a (a + 1) / 2 + b: M2M
+// first, L2L at + SHIFT_TAB.
+constexpr int SHIFT_TAB = BINOM_N * (BINOM_N + 1) / 2;
+const double2* device_shift_tables();
 
 }  // namespace b2
