@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(64, P2M_MIN_BLOCKS(ND)) k_p2m(TV t, int first,
 // give a level many blocks: with chunks of 256 boxes, levels of mostly
 // parents ran a dozen groups one after another per block (M2M 1.37 ms,
 // L2L 2.69 ms at 4M points, against 0.82 and 0.83 ms for the warp-per-
-// parent recurrence); chunks of 2G boxes take 0.46 and 0.52 ms.
+// parent recurrence); chunks of 2G boxes take 0.47 and 0.50 ms.
 // ---------------------------------------------------------------------------
 constexpr int SHIFT_THREADS = 128;
 
@@ -324,14 +324,16 @@ __device__ __forceinline__ int collect_parents(const TV& t, int c0, int CH, int 
   bool isp = false;
   int4 c = make_int4(-1, -1, -1, -1);
   if (tid < CH && b < end) {
-    isp = t.nchild[b] != 0;
-    if (isp && need_eval) {
+    // a box has children iff its first child number is set (one round of
+    // independent loads, no nchild read before the children)
+    c = t.child[b];
+    isp = c.x >= 0;
+    if (need_eval) {
       int ne = 0;
       if (t.ifpghtarg > 0) ne += t.trng[b].y - t.trng[b].x;
       if (t.ifpgh > 0) ne += t.srng[b].y - t.srng[b].x;
-      isp = ne > 0;
+      isp = isp && ne > 0;
     }
-    if (isp) c = t.child[b];
   }
   const unsigned m = __ballot_sync(~0u, isp);
   if (lane == 0) wcnt[w] = __popc(m);
