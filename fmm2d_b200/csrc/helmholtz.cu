@@ -442,6 +442,101 @@ __global__ void __launch_bounds__(128) k_h_m2m(TV t, const HLev* __restrict__ lv
   }
 }
 
+// The same M2M with the child slots folded together.  The slots' tables
+// differ only by the phases of their offsets' angles, multiples of pi/2
+// apart: T_q(m) = T_3(m) (-i)^(m k_q), k_q = 2, 3, 1, 0 for the slots (-,-),
+// (+,-), (-,+), (+,+).  So sum_q sum_j T_q(i-j) H_q(j) = sum_j T_3(i-j)
+// S_((i-j) mod 4)(j) with the four-point sums S_m = sum_q (-i)^(m k_q) H_q
+// (and their rs1^(2|j|)-scaled copies): one staging round and one pass over
+// j per parent instead of four (a child without sources adds nothing: it
+// is left out of the sums).  For one or two densities (the staged sums take
+// four times the shared memory of one child).
+template <int ND>
+__global__ void __launch_bounds__(128) k_h_m2m_sym(TV t, const HLev* __restrict__ lv, int lev,
+                                                   int first, int n,
+                                                   const double2* __restrict__ tabs,
+                                                   double2* __restrict__ mp) {
+  extern __shared__ double2 hsm[];
+  const HLev L = lv[lev], C = lv[lev + 1];
+  const int p1 = C.p, p2 = L.p, nt = L.nsh, np1 = 2 * p1 + 1, NS = np1 * ND;
+  double2* Sh = hsm;            // [m][np1 ND]
+  double2* Sc = Sh + 4 * NS;    // the same, times rs1^(2|j|)
+  double2* Ts = Sc + 4 * NS;    // slot (+,+)'s table [2 nt + 1]
+  double* R1 = reinterpret_cast<double*>(Ts + 2 * nt + 1);  // rs1^(2k), k <= max(p1, p2)
+  const int tid = threadIdx.x, i = tid - p2;
+  const bool act = tid < 2 * p2 + 1;
+  const int ai = i < 0 ? -i : i;
+  const int kmax = p1 > p2 ? p1 : p2;
+  for (int k = tid; k <= kmax; k += blockDim.x) R1[k] = pow(C.rs, 2.0 * k);
+  for (int e = tid; e <= 2 * nt; e += blockDim.x) Ts[e] = tabs[L.tm2m + 3 * (2 * nt + 1) + e];
+  const double fi = pow(C.rs / L.rs, (double)ai);
+  const double2 z = make_double2(0, 0);
+  for (int bi = blockIdx.x; bi < n; bi += gridDim.x) {
+    const int b = first + bi;
+    if (t.nchild[b] == 0) continue;
+    const int4 ch = t.child[b];
+    const bool h0 = t.srng[ch.x].y > t.srng[ch.x].x, h1 = t.srng[ch.y].y > t.srng[ch.y].x;
+    const bool h2 = t.srng[ch.z].y > t.srng[ch.z].x, h3 = t.srng[ch.w].y > t.srng[ch.w].x;
+    const double2* H0 = hexp(mp, C, ch.x, ND);
+    const double2* H1 = hexp(mp, C, ch.y, ND);
+    const double2* H2 = hexp(mp, C, ch.z, ND);
+    const double2* H3 = hexp(mp, C, ch.w, ND);
+    __syncthreads();  // tables ready / the previous parent is consumed
+    for (int e = tid; e < NS; e += blockDim.x) {
+      const double2 x0 = h0 ? H0[e] : z, x1 = h1 ? H1[e] : z;
+      const double2 x2 = h2 ? H2[e] : z, x3 = h3 ? H3[e] : z;
+      const double2 a = cadd(x3, x0), bb = cadd(x1, x2), c = csub(x3, x0), dd = csub(x1, x2);
+      const double2 s0 = cadd(a, bb), s2 = csub(a, bb);
+      const double2 s1 = make_double2(c.x - dd.y, c.y + dd.x);  // c + i dd
+      const double2 s3 = make_double2(c.x + dd.y, c.y - dd.x);  // c - i dd
+      const int jj = e / ND - p1;
+      const double r = R1[jj < 0 ? -jj : jj];
+      Sh[e] = s0;
+      Sh[NS + e] = s1;
+      Sh[2 * NS + e] = s2;
+      Sh[3 * NS + e] = s3;
+      Sc[e] = cscale(s0, r);
+      Sc[NS + e] = cscale(s1, r);
+      Sc[2 * NS + e] = cscale(s2, r);
+      Sc[3 * NS + e] = cscale(s3, r);
+    }
+    __syncthreads();
+    if (!act) continue;
+    const double2* T = Ts + nt;
+    double2 acc[ND];
+#pragma unroll
+    for (int d = 0; d < ND; d++) acc[d] = make_double2(0, 0);
+    if (i == 0) {
+      for (int jj = -p1; jj <= p1; jj++) {
+        const double2* S = Sc + ((-jj) & 3) * NS + (jj + p1) * ND;
+#pragma unroll
+        for (int d = 0; d < ND; d++) cfma(acc[d], S[d], T[-jj]);
+      }
+    } else {
+      // opposite sign or j = 0: rs1^(2|j|); same sign, |j| <= |i|: 1;
+      // same sign, |j| > |i|: rs1^(2(|j| - |i|))
+      const int sg = i > 0 ? 1 : -1;
+      for (int aj = 0; aj <= p1; aj++) {
+        const int jj = -sg * aj;
+        const double2* S = Sc + ((i - jj) & 3) * NS + (jj + p1) * ND;
+#pragma unroll
+        for (int d = 0; d < ND; d++) cfma(acc[d], S[d], T[i - jj]);
+      }
+      for (int aj = 1; aj <= p1; aj++) {
+        const int jj = sg * aj;
+        double2 tt = T[i - jj];
+        if (aj > ai) tt = cscale(tt, R1[aj - ai]);
+        const double2* S = Sh + ((i - jj) & 3) * NS + (jj + p1) * ND;
+#pragma unroll
+        for (int d = 0; d < ND; d++) cfma(acc[d], S[d], tt);
+      }
+    }
+    double2* M = hexp(mp, L, b, ND);
+#pragma unroll
+    for (int d = 0; d < ND; d++) M[(i + p2) * ND + d] = cscale(acc[d], fi);
+  }
+}
+
 // step 4: M2L over list 2 (same level: rs1 = rs2, (rs2/rs1)^|i| = 1).
 // One block per target box, one thread per output coefficient i; for every
 // list-2 source the block stages its multipole (plain and scaled by
@@ -1391,11 +1486,19 @@ void upward_pass(const TV& tv, const DeviceTree& T, const HelmLevels& H, double2
       k_hf_m2m<ND><<<(int)std::min<long>(n, 148L * 4), 256, sm, st>>>(tv, H.dlv.p, l, f, n,
                                                                       H.tabs.p, mp);
     } else {
-      size_t sm = sizeof(double2) * (2 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
-                  sizeof(double) * (HMAXP + 1);
-      set_smem(k_h_m2m<ND>, sm);
-      k_h_m2m<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
-                                                                     H.tabs.p, mp);
+      if (ND <= 2) {
+        size_t sm = sizeof(double2) * (8 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
+                    sizeof(double) * (HMAXP + 1);
+        set_smem(k_h_m2m_sym<ND>, sm);
+        k_h_m2m_sym<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                           H.tabs.p, mp);
+      } else {
+        size_t sm = sizeof(double2) * (2 * (2 * hl[l + 1].p + 1) * ND + 2 * hl[l].nsh + 1) +
+                    sizeof(double) * (HMAXP + 1);
+        set_smem(k_h_m2m<ND>, sm);
+        k_h_m2m<ND><<<(int)std::min<long>(n, 148L * 16), 128, sm, st>>>(tv, H.dlv.p, l, f, n,
+                                                                       H.tabs.p, mp);
+      }
     }
     B2_LAUNCH_CHECK();
   }
