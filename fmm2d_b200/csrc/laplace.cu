@@ -548,6 +548,163 @@ __global__ void __launch_bounds__(64) k_p2l(TV t, int first, int n, const double
   }
 }
 
+// The mixed path's P2L: the same staging and lane mapping with the
+// per-source terms and the sums over a chunk of 32 sources in FP32, each
+// chunk's partial sums added to FP64 accumulators.  The source offset is
+// formed in FP64 and scaled by the box size first, u = (x - c) / r (O(1)
+// whatever the coordinates' magnitude), so that w = 1/u, d/z0 = (d/r) w and
+// log|z0| = log|u| + log r, the last as log r times the chunk's charge sum
+// in FP64.
+template <int ND>
+__global__ void __launch_bounds__(64) k_p2l_f32(TV t, int first, int n,
+                                                const double2* __restrict__ xs, Dens D, int P,
+                                                double2* __restrict__ lo) {
+  extern __shared__ float2 fsm2[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  resolve_range(t, first, n);
+  float2* W = fsm2 + (size_t)wib * (32 * P + 64 * ND + 16);
+  float2* Q = W + 32 * P;
+  float2* Dd = Q + 32 * ND;
+  float* LG = reinterpret_cast<float*>(Dd + 32 * ND);
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
+    const int mine = base + lane * nw;
+    int n4 = 0, lev = 0;
+    double2 cen = make_double2(0, 0);
+    if (mine < n) {
+      const int b = first + mine;
+      n4 = t.nl4[b];
+      lev = t.level[b];
+      cen = t.center[b];
+      int ne = 0;
+      if (t.ifpghtarg > 0) ne += t.trng[b].y - t.trng[b].x;
+      if (t.ifpgh > 0) ne += t.srng[b].y - t.srng[b].x;
+      if (ne == 0) n4 = 0;
+    }
+    unsigned wm = __ballot_sync(~0u, n4 > 0);
+    while (wm) {
+      const int src = __ffs(wm) - 1;
+      wm &= wm - 1;
+      const int b = first + base + src * nw;
+      const int nb4 = __shfl_sync(~0u, n4, src);
+      const double2 c = make_double2(__shfl_sync(~0u, cen.x, src), __shfl_sync(~0u, cen.y, src));
+      const double r = t.boxsize[__shfl_sync(~0u, lev, src)];
+      const double ri = 1.0 / r, lr = log(r);
+      int2 sr = make_int2(0, 0);
+      if (lane < nb4) sr = t.srng[t.l4[(size_t)MNLIST4 * b + lane]];
+      int cnt = sr.y - sr.x, inc = cnt;
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        const int v = __shfl_up_sync(~0u, inc, o);
+        if (lane >= o) inc += v;
+      }
+      const int tot = __shfl_sync(~0u, inc, MNLIST4 - 1);
+      int bs[MNLIST4], be[MNLIST4];
+#pragma unroll
+      for (int e = 0; e < MNLIST4; e++) {
+        bs[e] = __shfl_sync(~0u, sr.x, e);
+        be[e] = __shfl_sync(~0u, inc - cnt, e);
+      }
+      double2 acc[2][ND];
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+      for (int g0 = 0; g0 < tot; g0 += 32) {
+        const int m = min(32, tot - g0);
+        __syncwarp();
+        if (lane < m) {
+          const int g = g0 + lane;
+          int js = bs[0], jb = be[0];
+#pragma unroll
+          for (int e = 1; e < MNLIST4; e++)
+            if (e < nb4 && g >= be[e]) {
+              js = bs[e];
+              jb = be[e];
+            }
+          const int j = js + (g - jb);
+          const double2 x = xs[j];
+          const float2 u = make_float2((float)((x.x - c.x) * ri), (float)((x.y - c.y) * ri));
+          const float iu2 = 1.0f / (u.x * u.x + u.y * u.y);
+          const float2 w = make_float2(u.x * iu2, -u.y * iu2);  // r / z0
+          float2 pw = make_float2(1.0f, 0.0f);
+          for (int k = 0; k < P; k++) {
+            W[lane * P + k] = pw;
+            pw = cmulf(pw, w);
+          }
+          LG[lane] = -0.5f * logf(iu2);  // log|u|
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            const double2 q = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+            Q[lane * ND + d] = make_float2((float)q.x, (float)q.y);
+            float2 dd = make_float2(0.0f, 0.0f);
+            if (D.d) {
+              const double2 dv = D.d[(size_t)j * D.ndc + D.d0 + d];
+              dd = cmulf(make_float2((float)(dv.x * ri), (float)(dv.y * ri)), w);
+            }
+            Dd[lane * ND + d] = make_float2(-dd.x, -dd.y);  // -d / z0
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          const int k = lane + 32 * s;
+          if (k >= P) break;
+          float2 part[ND];
+#pragma unroll
+          for (int d = 0; d < ND; d++) part[d] = make_float2(0.0f, 0.0f);
+          if (k == 0) {
+            float qs[2 * ND];
+#pragma unroll
+            for (int e = 0; e < 2 * ND; e++) qs[e] = 0.0f;
+            for (int j = 0; j < m; j++) {
+              const float lg = LG[j];
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                const float2 q = Q[j * ND + d];
+                part[d].x += q.x * lg + Dd[j * ND + d].x;
+                part[d].y += q.y * lg + Dd[j * ND + d].y;
+                qs[2 * d] += q.x;
+                qs[2 * d + 1] += q.y;
+              }
+            }
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              acc[s][d].x += (double)part[d].x + lr * (double)qs[2 * d];
+              acc[s][d].y += (double)part[d].y + lr * (double)qs[2 * d + 1];
+            }
+          } else {
+            const float mik = -1.0f / (float)k;
+            for (int j = 0; j < m; j++) {
+              const float2 wk = W[j * P + k];
+              const float2 cq = make_float2(wk.x * mik, wk.y * mik);
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                const float2 q = Q[j * ND + d], dd = Dd[j * ND + d];
+                part[d].x += q.x * cq.x - q.y * cq.y + dd.x * wk.x - dd.y * wk.y;
+                part[d].y += q.x * cq.y + q.y * cq.x + dd.x * wk.y + dd.y * wk.x;
+              }
+            }
+#pragma unroll
+            for (int d = 0; d < ND; d++) {
+              acc[s][d].x += (double)part[d].x;
+              acc[s][d].y += (double)part[d].y;
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        const int k = lane + 32 * s;
+        if (k >= P) break;
+#pragma unroll
+        for (int d = 0; d < ND; d++) lo[((size_t)b * P + k) * ND + d] = acc[s][d];
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // step 4: M2L over list 2 (laprouts2d.f:1130-1244), z0 = c_src - c_tgt,
 // u = r/z0, t_j = h_j (-u)^j:
@@ -1026,7 +1183,12 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   }
   B2_CHECK(cudaEventRecord(ev[2], st));
   B2_CHECK(cudaMemsetAsync(lo, 0, sizeof(double2) * (size_t)nb * P * ND, st));
-  if (n_from2 > 0) {
+  if (n_from2 > 0 && M) {
+    const size_t sm = sizeof(float2) * 2 * (32 * (size_t)P + 64 * ND + 16);
+    set_smem_attr(k_p2l_f32<ND>, sm);
+    k_p2l_f32<ND><<<warp_grid(n_from2, 2), 64, sm, st>>>(tv, from2, n_from2, xs, D, P, lo);
+    B2_LAUNCH_CHECK();
+  } else if (n_from2 > 0) {
     k_p2l<ND><<<warp_grid(n_from2, 2), 64, sm_p2l, st>>>(tv, from2, n_from2, xs, D, P, lo);
     B2_LAUNCH_CHECK();
   }
