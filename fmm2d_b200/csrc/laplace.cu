@@ -12,7 +12,7 @@
 //   k_p2m        P2M at leaves (step 1)
 //   k_m2m        upward pass, one launch per level (step 3; a block per
 //                chunk of boxes, the quadrant-symmetric operators)
-//   k_p2l        list 4 -> local (step 2)
+//   k_p2l        list 4 -> local (step 2; k_p2l_f32 on the mixed path)
 //   k_m2l        list 2 multipole -> local (step 4)
 //   k_l2l        downward pass, one launch per level (step 5; as k_m2m)
 //   leaf passes  (steps 6-8, csrc/lap_mixed.cu) on per-tree work items:
