@@ -9,7 +9,7 @@
 // so the coefficients of one box are contiguous.
 //
 // Kernels (one warp per box unless noted):
-//   k_p2m        P2M at leaves (step 1)
+//   k_p2m        P2M at leaves (step 1; k_p2m_f32 on the mixed path)
 //   k_m2m        upward pass, one launch per level (step 3; a block per
 //                chunk of boxes, the quadrant-symmetric operators)
 //   k_p2l        list 4 -> local (step 2; k_p2l_f32 on the mixed path)
@@ -261,6 +261,122 @@ __global__ void __launch_bounds__(64, P2M_MIN_BLOCKS(ND)) k_p2m(TV t, int first,
                 cfma(acc[s][d], Dd[j * ND + d], wk1);
               }
             }
+          }
+        }
+      }
+#pragma unroll
+      for (int s = 0; s < 2; s++) {
+        const int k = lane + 32 * s;
+        if (k >= P) break;
+#pragma unroll
+        for (int d = 0; d < ND; d++) mp[((size_t)b * P + k) * ND + d] = acc[s][d];
+      }
+    }
+  }
+}
+
+// The mixed path's P2M: the same staging and lane mapping with the
+// per-source terms and the sums over a chunk of sources in FP32, each
+// chunk's partial sums added to FP64 accumulators; w = (x - c) / r is formed
+// in FP64 and rounded once.
+template <int ND>
+__global__ void __launch_bounds__(64, P2M_MIN_BLOCKS(ND)) k_p2m_f32(TV t, int first, int n, const double2* __restrict__ xs,
+                                            Dens D, int P, double2* __restrict__ mp) {
+  extern __shared__ float2 fsm1[];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  resolve_range(t, first, n);
+  float2* W = fsm1 + (size_t)wib * (P2M_CHUNK * P + 2 * P2M_CHUNK * ND);
+  float2* Q = W + P2M_CHUNK * P;
+  float2* Dd = Q + P2M_CHUNK * ND;
+  for (int base = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; base < n; base += 32 * nw) {
+    const int mine = base + lane * nw;
+    int nc = 1, lev = 0;
+    int2 sr = make_int2(0, 0);
+    double2 cen = make_double2(0, 0);
+    if (mine < n) {
+      const int b = first + mine;
+      nc = t.nchild[b];
+      lev = t.level[b];
+      sr = t.srng[b];
+      cen = t.center[b];
+    }
+    const bool work = nc == 0 && lev >= 2 && sr.y > sr.x;
+    unsigned zm = __ballot_sync(~0u, mine < n && nc == 0 && !work);
+    unsigned wm = __ballot_sync(~0u, mine < n && work);
+    while (zm) {
+      const int src = __ffs(zm) - 1;
+      zm &= zm - 1;
+      const size_t b = (size_t)first + base + src * nw;
+      for (int e = lane; e < P * ND; e += 32) mp[b * P * ND + e] = make_double2(0, 0);
+    }
+    while (wm) {
+      const int src = __ffs(wm) - 1;
+      wm &= wm - 1;
+      const int b = first + base + src * nw;
+      const int2 srb = make_int2(__shfl_sync(~0u, sr.x, src), __shfl_sync(~0u, sr.y, src));
+      const double2 c = make_double2(__shfl_sync(~0u, cen.x, src), __shfl_sync(~0u, cen.y, src));
+      const double r = t.boxsize[__shfl_sync(~0u, lev, src)];
+      const double ri = 1.0 / r;
+      double2 acc[2][ND];
+#pragma unroll
+      for (int s = 0; s < 2; s++)
+#pragma unroll
+        for (int d = 0; d < ND; d++) acc[s][d] = make_double2(0, 0);
+      for (int s0 = srb.x; s0 < srb.y; s0 += P2M_CHUNK) {
+        const int m = min(P2M_CHUNK, srb.y - s0);
+        __syncwarp();
+        if (lane < m) {
+          const int j = s0 + lane;
+          const double2 x = xs[j];
+          const float2 w = make_float2((float)((x.x - c.x) * ri), (float)((x.y - c.y) * ri));
+          float2 pw = make_float2(1.0f, 0.0f);
+          for (int k = 0; k < P; k++) {
+            W[lane * P + k] = pw;
+            pw = cmulf(pw, w);
+          }
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            const double2 q = D.q ? D.q[(size_t)j * D.ndc + D.d0 + d] : make_double2(0, 0);
+            const double2 dv =
+                D.d ? cscale(D.d[(size_t)j * D.ndc + D.d0 + d], ri) : make_double2(0, 0);
+            Q[lane * ND + d] = make_float2((float)q.x, (float)q.y);
+            Dd[lane * ND + d] = make_float2((float)dv.x, (float)dv.y);
+          }
+        }
+        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < 2; s++) {
+          const int k = lane + 32 * s;
+          if (k >= P) break;
+          float2 part[ND];
+#pragma unroll
+          for (int d = 0; d < ND; d++) part[d] = make_float2(0.0f, 0.0f);
+          if (k == 0) {
+            for (int j = 0; j < m; j++)
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                part[d].x += Q[j * ND + d].x;
+                part[d].y += Q[j * ND + d].y;
+              }
+          } else {
+            const float mik = -1.0f / (float)k;
+            for (int j = 0; j < m; j++) {
+              const float2 wk = W[j * P + k], wk1 = W[j * P + k - 1];
+              const float2 cq = make_float2(wk.x * mik, wk.y * mik);
+#pragma unroll
+              for (int d = 0; d < ND; d++) {
+                const float2 q = Q[j * ND + d], dd = Dd[j * ND + d];
+                part[d].x += q.x * cq.x - q.y * cq.y + dd.x * wk1.x - dd.y * wk1.y;
+                part[d].y += q.x * cq.y + q.y * cq.x + dd.x * wk1.y + dd.y * wk1.x;
+              }
+            }
+          }
+#pragma unroll
+          for (int d = 0; d < ND; d++) {
+            acc[s][d].x += (double)part[d].x;
+            acc[s][d].y += (double)part[d].y;
           }
         }
       }
@@ -1139,7 +1255,13 @@ void run_chunk(const TV& tv, DeviceTree& T, const LapArgs& a, const Dens& D, int
   size_t sm_p2l = sizeof(double2) * 2 * (32 * (size_t)P + 64 * ND + 32);
   set_smem_attr(k_p2m<ND>, sm_p2m);
   set_smem_attr(k_p2l<ND>, sm_p2l);
-  k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, all, nb, xs, D, P, mp);
+  if (M) {
+    const size_t sm = sizeof(float2) * 2 * (P2M_CHUNK * (size_t)P + 2 * P2M_CHUNK * ND);
+    set_smem_attr(k_p2m_f32<ND>, sm);
+    k_p2m_f32<ND><<<warp_grid(nb, 2), 64, sm, st>>>(tv, all, nb, xs, D, P, mp);
+  } else {
+    k_p2m<ND><<<warp_grid(nb, 2), 64, sm_p2m, st>>>(tv, all, nb, xs, D, P, mp);
+  }
   B2_LAUNCH_CHECK();
   B2_CHECK(cudaEventRecord(ev[1], st));
   // M2M / L2L: parents per group for about two items a thread
